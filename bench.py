@@ -1,0 +1,333 @@
+"""Benchmark: Total-FETI dual solve time to 1e-8 on one B200 (per rank), through FETI4I.
+
+Workload (default): heat conduction on a unit cube, 8x8x8 subdomains x 10x10x10 HEXA8
+elements, log-uniform per-element conductivity on [1,100] (seed 0), T=0 on z=0,
+unit source; lumped preconditioner; Schur complements stored in FP32 inside FP64
+residual replacement (reliable updates); dual PCG to precision 1e-8.
+
+One step = one dual PCG solve on device-resident data (FETI4ISolveResident).
+``e2e`` = one FETI4ISolve call with host buffers (host b/e vectors, H2D, PCG,
+D2H, host primal recovery).  ``roofline`` is the tile SYMV (F apply) kernel:
+algorithmic bytes per launch / CUDA-event launch time on the library stream.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FETI solve time @1e-8 rel err, mixed/batched vs FP64 GPU; F-apply HBM GB/s"
+SCHUR = {"fp64": 0, "fp32": 1, "bf16": 2}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2_heat_512")
+    ap.add_argument("--schur", default="fp32", choices=sorted(SCHUR))
+    ap.add_argument("--precond", type=int, default=1)
+    ap.add_argument("--precision", type=float, default=1e-8)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is None:
+            return
+        time.sleep(0.25)
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                self.samples.append(f)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        mhz = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def dist_init(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return rank, world, local, dist
+
+
+def dist_max(dist, v):
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def cpu_reference_solver(cfg_name, precond):
+    """The oracle restatement of ESPRESO's FP64 dual PCG on the host cores."""
+    from espreso_b200 import problems
+    from oracle import feti as OF
+    from oracle import numbering as ON
+    P = problems.build_config(cfg_name)
+    num = ON.Numbering(P.elem_nodes, P.elem_domain, P.n_nodes, P.dpn, P.dirichlet)
+    OP = OF.FETIProblem(num, P.elem_nodes, P.elem_domain, P.Ke, P.fe, P.coords,
+                        build_dirichlet=(precond == OF.PREC_DIRICHLET))
+    return OP
+
+
+def threaded_apply_F(OP, nthreads):
+    """F apply of the oracle with subdomains spread over host threads (numpy releases the GIL)."""
+    from concurrent.futures import ThreadPoolExecutor
+    pool = ThreadPoolExecutor(nthreads)
+
+    def apply(x):
+        parts = list(pool.map(lambda s: s.S @ x[s.lam], OP.sub))
+        y = np.zeros(OP.n_lambda)
+        for s, yi in zip(OP.sub, parts):
+            np.add.at(y, s.lam, yi)
+        return y
+    return apply
+
+
+def time_cpu_iterations(OP, precond, iters, nthreads, precision):
+    """Time a bounded sample of PCG iterations of the oracle (threaded F apply)."""
+    OP.apply_F = (lambda f: (lambda x, precision="f64": f(x)))(threaded_apply_F(OP, nthreads))
+    t0 = time.perf_counter()
+    OP.solve(precision=precision, max_it=iters, prec=precond)
+    return (time.perf_counter() - t0) / max(1, OP.iterations)
+
+
+def run_reference(args):
+    rank, world, local, dist = dist_init(args)
+    if rank != 0:
+        return
+    from threadpoolctl import threadpool_limits
+    ncores = os.cpu_count() or 1
+    with threadpool_limits(1):
+        OP = cpu_reference_solver(args.config, args.precond)
+        # iteration count of the full solve (untimed), then bounded timed samples
+        hist = []
+        OP.solve(precision=args.precision, max_it=5000, prec=args.precond, history=hist)
+        n_it = OP.iterations
+        for _ in range(args.warmup):
+            time_cpu_iterations(OP, args.precond, 2, ncores, args.precision)
+        per_it = [time_cpu_iterations(OP, args.precond, 5, ncores, args.precision) for _ in range(args.steps)]
+    ms = 1e3 * statistics.median(per_it) * n_it
+    line = {"metric": METRIC, "value": ms, "unit": "ms", "impl": "reference", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.config, "precond": args.precond, "precision": args.precision,
+                       "pcg_iterations": n_it},
+            "cpu_baseline": {"value": ms, "unit": "ms", "cores": ncores, "kind": "port",
+                             "sample": f"5 PCG iterations per step x {n_it} iterations of the full FP64 solve "
+                                       f"(oracle restatement, subdomain F apply over {ncores} threads)"},
+            "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_ours(args):
+    rank, world, local, dist = dist_init(args)
+    import torch
+    torch.cuda.set_device(local)
+    from espreso_b200 import feti4i as F
+    from espreso_b200 import problems
+    t0 = time.time()
+    P = problems.build_config(args.config)
+    rhs = P.rhs()
+    inst = problems.make_instance(P, iopts={F.PRECONDITIONER: args.precond, F.VERBOSE_LEVEL: 0,
+                                            F.MAX_ITERATIONS: 5000},
+                                  ropts={F.PRECISION: args.precision},
+                                  ext={F.EXT_SCHUR_PRECISION: SCHUR[args.schur]})
+    setup_s = time.time() - t0
+    st0 = inst.stats()
+    sol = np.zeros(P.ndofs)
+    # warm-up: full solves through the C ABI (also uploads the right-hand side)
+    for _ in range(max(1, args.warmup)):
+        inst.solve(sol)
+    # FP64 GPU reference solve time (same config, same kernels, FP64 Schur tiles)
+    inst.set_solve_precision(0)
+    inst.solve_resident()
+    fp64_ms = inst.solve_resident()
+    st64 = inst.stats()
+    inst.set_solve_precision(SCHUR[args.schur])
+    inst.solve_resident()
+    # timed region: K device-resident solves
+    dist_barrier(dist)
+    torch.cuda.synchronize()
+    dev_ms = []
+    with Clocks(local) as clk:
+        tw = time.perf_counter()
+        for _ in range(args.steps):
+            dev_ms.append(inst.solve_resident())
+        torch.cuda.synchronize()
+        wall = (time.perf_counter() - tw) * 1e3 / args.steps
+    dist_barrier(dist)
+    st = inst.stats()
+    step_ms = dist_max(dist, float(np.mean(dev_ms)))
+    # end-to-end through FETI4ISolve with host buffers
+    e2e = []
+    for _ in range(max(2, args.steps // 2)):
+        t = time.perf_counter()
+        inst.solve(sol)
+        e2e.append((time.perf_counter() - t) * 1e3)
+    e2e_ms = dist_max(dist, float(np.median(e2e)))
+    NL = int(sum(inst.subdomain_info(d)["rows"] for d in range(int(st["subdomains"]))))
+    nK = int(st["kernel_size"])
+    # roofline of the F apply kernel (events on the library stream)
+    t_f = inst.time_F(SCHUR[args.schur], 20)
+    alg = float(st["fapply_bytes"])
+    achieved = alg / (t_f * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "fapply_traffic.json")
+    if os.path.exists(tp):
+        tj = json.load(open(tp))
+        key = f"{args.config}:{args.schur}"
+        if key in tj:
+            traffic = tj[key]["dram_bytes_per_launch"]
+    fp64_f = inst.time_F(0, 10)
+    alg64 = inst.stats() and None
+    # CPU baseline: oracle port on the host cores (rank 0, N=1 only)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_from_library(inst, P, args)
+    clocks = clk.summary()
+    launches = int(st["kernel_launches"]) * args.steps
+    line = {
+        "metric": METRIC, "value": step_ms, "unit": "ms", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 (fp32 Schur storage)" if args.schur == "fp32" else
+        ("f64 (bf16 Schur storage)" if args.schur == "bf16" else "f64"),
+        "data": "synthetic",
+        "config": {"workload": args.config, "subdomains": int(st["subdomains"]), "dual_size": int(st["dual_size"]),
+                   "kernel_size": nK, "precond": args.precond, "schur": args.schur, "precision": args.precision,
+                   "pcg_iterations": int(st["iterations"]), "replacements": int(st["replacements"]),
+                   "parallelism": f"replicas{world}", "l2": "working set > L2 (Schur tiles "
+                   f"{alg / 1e9:.2f} GB per apply, 126 MB L2)", "wall_ms_per_step": wall,
+                   "setup_s": setup_s, "host_prep_s": st0["prep_seconds"]},
+        "fp64_gpu": {"ms": fp64_ms, "pcg_iterations": int(st64["iterations"]), "speedup_mixed": fp64_ms / step_ms,
+                     "fapply_ms": fp64_f},
+        "solves_per_s": world * 1e3 / step_ms,
+        "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 8 * (NL + nK),
+                "d2h_bytes_per_step": 8 * (NL + nK)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "kernel": "tile_symv_kernel", "launch_ms": t_f, "peak_kind": peak_kind,
+                     "alg_bytes_per_launch": alg},
+        "cpu_baseline": cpu,
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    inst.destroy()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def cpu_baseline_from_library(inst, P, args):
+    """Oracle FP64 PCG iterations on the host cores with the same S_i (bounded sample)."""
+    from threadpoolctl import threadpool_limits
+
+    from oracle import feti as OF
+    from oracle import numbering as ON
+    ncores = os.cpu_count() or 1
+    with threadpool_limits(1):
+        num = ON.Numbering(P.elem_nodes, P.elem_domain, P.n_nodes, P.dpn, P.dirichlet)
+        OP = OF.FETIProblem.__new__(OF.FETIProblem)
+        # light-weight oracle object on the library's operators (no oracle factorisation)
+        OP.num = num
+        OP.coords = P.coords
+        OP.n_lambda = num.n_lambda
+        OP.sub = []
+        diags = None
+        for d in range(num.ndomains):
+            s = OF.Subdomain(K=None, f=None, R=inst.kernel(d), regmat=None, chol=None, lam=num.B[d]["lam"],
+                             dof=num.B[d]["dof"], sign=num.B[d]["sign"], c=num.B[d]["c"], w=None)
+            s.S = np.ascontiguousarray(inst.schur(d))
+            OP.sub.append(s)
+        OP._coarse()
+        apply = threaded_apply_F(OP, ncores)
+        rng = np.random.default_rng(0)
+        x = rng.standard_normal(OP.n_lambda)
+        apply(x)
+        reps = 3
+        t = time.perf_counter()
+        for _ in range(reps):
+            apply(x)
+        per_apply = (time.perf_counter() - t) / reps
+    iters = int(inst.stats()["iterations"])
+    # one PCG iteration = one F apply + projector/preconditioner work (counted as the F apply alone: lower bound)
+    ms = 1e3 * per_apply * iters
+    return {"value": ms, "unit": "ms", "cores": ncores, "kind": "port",
+            "sample": f"{reps} FP64 F applies of the oracle (subdomain S_i @ x over {ncores} threads) x "
+                      f"{iters} PCG iterations; projector and preconditioner not counted (lower bound)"}
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)

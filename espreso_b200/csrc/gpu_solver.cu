@@ -1,0 +1,1166 @@
+// Total-FETI dual PCG on one B200 (sm_100a): tiled Schur-complement SYMV
+// work queue, projector, lumped/Dirichlet preconditioners and the PCG
+// recurrences over replicated local dual vectors, captured in CUDA graphs.
+//
+// Reference behaviour restated here:
+//   PCG recurrences, stop rule ........ src/solver/specific/itersolver.cpp:1406-1724
+//   projector P = I - G^T (GG^T)^-1 G .. src/solver/specific/itersolver.cpp:5541-5623
+//   F apply (explicit S_i) ............ src/solver/specific/cpu/itersolvercpu.cpp:49-70
+//   preconditioners ................... src/solver/specific/cpu/itersolvercpu.cpp:520-602
+//   FP32 Schur path (x->float, float accumulate, y->double)
+//                                       src/solver/generic/SparseMatrix.cpp:1093-1160
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "common.h"
+#include "gpu_solver.h"
+
+#define CUDA_CHECK(x)                                                                              \
+    do {                                                                                           \
+        cudaError_t e_ = (x);                                                                      \
+        if (e_ != cudaSuccess)                                                                     \
+            throw ::feti::Error(std::string("CUDA error ") + cudaGetErrorString(e_) + " in " #x); \
+    } while (0)
+
+namespace feti {
+
+namespace {
+
+constexpr int KMAX = 8;        // kernel dimension bound per subdomain (elasticity: 6)
+constexpr int TPB = 256;       // threads of the per-subdomain kernels
+constexpr int TILE = 32;       // Schur tile edge
+constexpr unsigned FULL = 0xffffffffu;
+
+// ---------------------------------------------------------------------------------------------
+// device state shared by the kernels of one solve
+struct DevState {
+    int conv_iter;      // first iteration whose check passed, -1 while running
+    int iter_base;      // iteration index of slot 0 of the current graph chunk
+    int replace_next;   // mixed precision: recompute the true residual before the next iteration
+    int r_true;         // the residual of the current iteration is a freshly recomputed one
+    int replacements;
+    int max_it;
+    int mixed;
+    int pad;
+    double tol;
+    double precision;
+    double rmax;        // largest projected residual norm since the last replacement
+    double delta;       // replacement threshold
+    double last_norm;
+};
+
+struct DevProblem {
+    int nd, NL, nK, NT;
+    const int *loff;        // nd+1
+    const int *kof;         // nd+1 kernel offsets
+    const int *toff;        // nd+1 T-space offsets
+    const int *partner;     // NL: row of the other owner, -1
+    const int *tidx;        // NL: global T index of the row's DOF
+    const double *ws;       // NL: B1 weight * sign
+    const double *minv;     // NL: 1 / multiplicity
+    const double *Gl;       // NL*KMAX: G coefficients of the row
+    const int *rkof;        // NL: kernel offset of the row's subdomain
+    const int *rnk;         // NL: kernel dimension of the row's subdomain
+    const int *trow_ptr;    // NT+1
+    const int *trow_idx;    // rows of each T index
+    const int *kt_ptr;      // NT+1 lumped: K restricted to T (global T columns)
+    const int *kt_col;
+    const double *kt_val;
+    const double *GGtinv;   // nK*nK
+    const double *bL;       // NL replicated b
+    double *x, *r, *w, *z, *y, *p, *Ap, *uT, *vT, *d, *alpha;
+    double *part_w, *part_rho, *part_b, *rho_hist;
+    DevState *st;
+};
+
+struct TileSetDev {
+    int nitems;
+    int prec;
+    const int4 *items;            // (matrix, k0, k1, -)
+    const int *mat_n, *mat_voff, *mat_tn;
+    const long long *mat_tile0;
+    const unsigned *tile_ij;      // (I << 16) | J
+    const void *tiles;
+    const float *scale;           // BF16 per-tile scale
+    double *item_dot;
+    int *queue;                   // [0] work counter, [1] finished CTAs
+};
+
+// ---------------------------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+
+// block-wide sum; identical result in every thread; fixed order for a given blockDim
+__device__ double block_sum(double v, double *sh) {
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    double s = 0.0;
+    for (int i = 0; i < nw; ++i) s += sh[i];
+    __syncthreads();
+    return s;
+}
+
+// block-wide sum of KMAX values at once
+__device__ void block_sum_k(double (&v)[KMAX], double *sh /* >= 32*KMAX */) {
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k) v[k] = warp_sum(v[k]);
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < KMAX; ++k) sh[wid * KMAX + k] = v[k];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k) {
+        double s = 0.0;
+        for (int i = 0; i < nw; ++i) s += sh[i * KMAX + k];
+        v[k] = s;
+    }
+    __syncthreads();
+}
+
+// sum of an array of partials in a fixed order (same value in every CTA)
+__device__ double array_sum(const double *a, int n, double *sh) {
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s += a[i];
+    return block_sum(s, sh);
+}
+
+__device__ __forceinline__ bool skip_iter(const DevState *st, int iter) {
+    int c = st->conv_iter;
+    return (c >= 0 && iter > c) || iter >= st->max_it;
+}
+
+// (G^T a) at local row e: own coefficients plus the partner's
+__device__ __forceinline__ double gt_alpha(const DevProblem &P, int e, const double *a) {
+    double s = 0.0;
+    int nk = P.rnk[e], ko = P.rkof[e];
+    for (int k = 0; k < nk; ++k) s += P.Gl[(size_t)e * KMAX + k] * a[ko + k];
+    int q = P.partner[e];
+    if (q >= 0) {
+        nk = P.rnk[q];
+        ko = P.rkof[q];
+        for (int k = 0; k < nk; ++k) s += P.Gl[(size_t)q * KMAX + k] * a[ko + k];
+    }
+    return s;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Tile SYMV.  A symmetric matrix of order n is stored as its upper-triangular
+// 32x32 tiles (I <= J), row-major inside a tile; diagonal tiles hold the full
+// symmetric block.  A warp owns one tile at a time: every lane loads
+// 32/EPC 16-byte chunks (coalesced, one 512-byte row segment per instruction),
+// forms partial row sums (S x_J) and column sums (S^T x_I) and finishes both
+// with shuffle reduce-scatters, so each lane ends with one row and one column.
+template <int PREC>
+struct TileT;
+template <>
+struct TileT<SCHUR_FP64> {
+    using Acc = double;
+    static constexpr int EPC = 2;
+};
+template <>
+struct TileT<SCHUR_FP32> {
+    using Acc = float;
+    static constexpr int EPC = 4;
+};
+template <>
+struct TileT<SCHUR_BF16> {
+    using Acc = float;
+    static constexpr int EPC = 8;
+};
+
+__device__ __forceinline__ uint4 ld_stream(const uint4 *p) {
+    uint4 v;
+    asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "l"(p));
+    return v;
+}
+
+template <int PREC>
+__device__ __forceinline__ void unpack(const uint4 &u, typename TileT<PREC>::Acc (&e)[TileT<PREC>::EPC], float sc);
+template <>
+__device__ __forceinline__ void unpack<SCHUR_FP64>(const uint4 &u, double (&e)[2], float) {
+    e[0] = __hiloint2double(u.y, u.x);
+    e[1] = __hiloint2double(u.w, u.z);
+}
+template <>
+__device__ __forceinline__ void unpack<SCHUR_FP32>(const uint4 &u, float (&e)[4], float) {
+    e[0] = __uint_as_float(u.x);
+    e[1] = __uint_as_float(u.y);
+    e[2] = __uint_as_float(u.z);
+    e[3] = __uint_as_float(u.w);
+}
+template <>
+__device__ __forceinline__ void unpack<SCHUR_BF16>(const uint4 &u, float (&e)[8], float sc) {
+    const unsigned w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        e[2 * i] = __uint_as_float(w[i] << 16) * sc;
+        e[2 * i + 1] = __uint_as_float(w[i] & 0xffff0000u) * sc;
+    }
+}
+
+// reduce-scatter over the M lanes that differ in lane bits [SHIFT, SHIFT+log2 M):
+// afterwards v[0] of a lane holds the group sum of entry ((lane >> SHIFT) & (M-1)).
+template <int M, int SHIFT, typename T>
+__device__ __forceinline__ T reduce_scatter(T (&v)[M], int lane) {
+#pragma unroll
+    for (int half = M / 2; half >= 1; half /= 2) {
+        const bool upper = (lane >> SHIFT) & half;
+#pragma unroll
+        for (int i = 0; i < half; ++i) {
+            T send = upper ? v[i] : v[i + half];
+            T keep = upper ? v[i + half] : v[i];
+            v[i] = keep + __shfl_xor_sync(FULL, send, half << SHIFT);
+        }
+    }
+    return v[0];
+}
+
+// MODE 0: x = src (outside the PCG loop)
+// MODE 1: x = src + beta * src2 with beta = rho_k / rho_{k-1} (PCG direction p = y + beta p)
+// MODE 2: x = src inside the PCG loop (skipped after convergence)
+// MODE 3: x = src, only when a residual replacement is pending (mixed precision)
+template <int PREC, int MODE>
+__global__ void __launch_bounds__(256, 2)
+tile_symv_kernel(TileSetDev ts, DevProblem P, const double *src, const double *src2, double *out, int slot) {
+    using Acc = typename TileT<PREC>::Acc;
+    constexpr int EPC = TileT<PREC>::EPC;
+    constexpr int CPR = TILE / EPC;          // 16-byte chunks per tile row (= loads per lane)
+    constexpr int LOG_CPR = (CPR == 16) ? 4 : (CPR == 8) ? 3 : 2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double red[32];
+    __shared__ int s_item;
+    __shared__ double s_beta;
+
+    if (MODE != 0) {
+        const int iter = P.st->iter_base + slot;
+        if (skip_iter(P.st, iter)) return;
+        if (MODE == 3 && !P.st->replace_next) return;
+        if (MODE == 1) {
+            double rho = array_sum(P.part_rho, P.nd, red);
+            if (threadIdx.x == 0) s_beta = (iter == 0) ? 0.0 : rho / P.rho_hist[iter - 1];
+            __syncthreads();
+        }
+    }
+    const double beta = (MODE == 1) ? s_beta : 0.0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int cq = lane % CPR, h = lane / CPR;
+    const int idx = EPC * cq + h;   // row/column handled by this lane after the reductions
+
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(&ts.queue[0], 1);
+        __syncthreads();
+        const int item = s_item;
+        if (item >= ts.nitems) break;
+        const int4 it = ts.items[item];
+        const int m = it.x, k0 = it.y, k1 = it.z;
+        const int n = ts.mat_n[m], voff = ts.mat_voff[m], tn = ts.mat_tn[m];
+        const int np = tn * TILE;
+        Acc *xs = reinterpret_cast<Acc *>(smem_raw);
+        Acc *ys = xs + np;
+        for (int i = threadIdx.x; i < np; i += blockDim.x) {
+            double v = 0.0;
+            if (i < n) v = (MODE == 1) ? src[voff + i] + beta * src2[voff + i] : src[voff + i];
+            xs[i] = (Acc)v;
+            ys[i] = (Acc)0;
+        }
+        __syncthreads();
+
+        const long long tbase = ts.mat_tile0[m];
+        const uint4 *tiles = reinterpret_cast<const uint4 *>(ts.tiles);
+        int curI = -1;
+        Acc racc = 0;
+        for (int k = k0 + warp; k < k1; k += nw) {
+            const long long g = tbase + k;
+            const unsigned ij = ts.tile_ij[g];
+            const int I = ij >> 16, J = ij & 0xffff;
+            uint4 raw[CPR];
+            const uint4 *tp = tiles + (size_t)g * (TILE * CPR);
+#pragma unroll
+            for (int q = 0; q < CPR; ++q) raw[q] = ld_stream(tp + q * 32 + lane);
+            const float sc = (PREC == SCHUR_BF16) ? ts.scale[g] : 1.0f;
+            Acc xc[EPC], xr[CPR], rs[CPR], cs[EPC];
+#pragma unroll
+            for (int j = 0; j < EPC; ++j) { xc[j] = xs[TILE * J + EPC * cq + j]; cs[j] = 0; }
+#pragma unroll
+            for (int q = 0; q < CPR; ++q) { xr[q] = xs[TILE * I + EPC * q + h]; rs[q] = 0; }
+#pragma unroll
+            for (int q = 0; q < CPR; ++q) {
+                Acc e[EPC];
+                unpack<PREC>(raw[q], e, sc);
+#pragma unroll
+                for (int j = 0; j < EPC; ++j) {
+                    rs[q] += e[j] * xc[j];
+                    cs[j] += e[j] * xr[q];
+                }
+            }
+            Acc rsum = reduce_scatter<CPR, 0>(rs, lane);
+            if (I != curI) {
+                if (curI >= 0) atomicAdd(&ys[TILE * curI + idx], racc);
+                curI = I;
+                racc = 0;
+            }
+            racc += rsum;
+            if (I != J) {
+                Acc csum = reduce_scatter<EPC, LOG_CPR>(cs, lane);
+                atomicAdd(&ys[TILE * J + idx], csum);
+            }
+        }
+        if (curI >= 0) atomicAdd(&ys[TILE * curI + idx], racc);
+        __syncthreads();
+
+        // item output: partial y and its dot with x
+        const bool whole = (k0 == 0) && (k1 == tn * (tn + 1) / 2);
+        double dot = 0.0;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            double yv = (double)ys[i];
+            dot += (double)xs[i] * yv;
+            if (whole) out[voff + i] = yv;
+            else atomicAdd(&out[voff + i], yv);
+        }
+        dot = block_sum(dot, red);
+        if (threadIdx.x == 0 && ts.item_dot) ts.item_dot[item] = dot;
+        __syncthreads();
+    }
+    // the last CTA to finish resets the work queue for the next launch
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        int done = atomicAdd(&ts.queue[1], 1);
+        if (done == (int)gridDim.x - 1) {
+            ts.queue[0] = 0;
+            ts.queue[1] = 0;
+            __threadfence();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// coarse problem: out = (GG^T)^-1 in   (dense symmetric, one warp per row)
+__global__ void coarse_kernel(DevProblem P, const double *in, double *out, int slot, int looped) {
+    if (looped) {
+        int iter = P.st->iter_base + slot;
+        if (skip_iter(P.st, iter)) return;
+    }
+    int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    int lane = threadIdx.x & 31;
+    if (row >= P.nK) return;
+    const double *col = P.GGtinv + (size_t)row * P.nK;
+    double s = 0.0;
+    for (int b = lane; b < P.nK; b += 32) s += col[b] * in[b];
+    s = warp_sum(s);
+    if (lane == 0) out[row] = s;
+}
+
+// x = G^T alpha (initial lambda_0 = G^T (GG^T)^-1 e)
+__global__ void gt_kernel(DevProblem P, const double *a, double *xout) {
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < P.NL) xout[e] = gt_alpha(P, e, a);
+}
+
+__global__ void zero_kernel(double *v, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = 0.0;
+}
+
+// r = b - assemble(Ap); d = G r per subdomain; ||b||^2 partials.  One CTA per subdomain.
+__global__ void r0_kernel(DevProblem P, double *Ax, int replace_mode, int slot) {
+    __shared__ double sh[32 * KMAX];
+    if (replace_mode) {
+        const int iter = P.st->iter_base + slot;
+        if (skip_iter(P.st, iter) || !P.st->replace_next) return;
+    }
+    const int dsub = blockIdx.x;
+    const int e0 = P.loff[dsub], e1 = P.loff[dsub + 1];
+    double gk[KMAX];
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k) gk[k] = 0.0;
+    double bb = 0.0;
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+        int q = P.partner[e];
+        double a = Ax[e] + (q >= 0 ? Ax[q] : 0.0);
+        double rv = P.bL[e] - a;
+        P.r[e] = rv;
+        bb += P.bL[e] * P.bL[e] * P.minv[e];
+#pragma unroll
+        for (int k = 0; k < KMAX; ++k) gk[k] += P.Gl[(size_t)e * KMAX + k] * rv;
+    }
+    block_sum_k(gk, sh);
+    double bsum = block_sum(bb, sh);
+    if (threadIdx.x == 0) {
+        int nk = P.kof[dsub + 1] - P.kof[dsub];
+        for (int k = 0; k < nk; ++k) P.d[P.kof[dsub] + k] = gk[k];
+        if (!replace_mode) P.part_b[dsub] = bsum;
+    }
+}
+
+// ||P r||^2 partials with alpha = (GG^T)^-1 G r  (initial stop tolerance)
+__global__ void pnorm_kernel(DevProblem P) {
+    __shared__ double sh[32];
+    const int dsub = blockIdx.x;
+    double s = 0.0;
+    for (int e = P.loff[dsub] + threadIdx.x; e < P.loff[dsub + 1]; e += blockDim.x) {
+        double u = P.r[e] - gt_alpha(P, e, P.alpha);
+        s += u * u * P.minv[e];
+    }
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) P.part_w[dsub] = s;
+}
+
+__global__ void tol_kernel(DevProblem P) {
+    __shared__ double sh[32];
+    double un = array_sum(P.part_w, P.nd, sh);
+    double bn = array_sum(P.part_b, P.nd, sh);
+    if (threadIdx.x == 0) {
+        double tol = P.st->precision * fmin(sqrt(un), sqrt(bn));
+        P.st->tol = tol;
+        P.st->rmax = sqrt(un);
+    }
+}
+
+// w = r - G^T alpha, ||w||^2 partials, u_T = B^T (W w) and, for the lumped
+// preconditioner, v_T = K_TT u_T.  With no preconditioner y = w and the rho
+// partials are taken here.  One CTA per subdomain.
+template <int PRECOND>
+__global__ void w_prec_kernel(DevProblem P, int slot) {
+    extern __shared__ double sm[];
+    __shared__ double sh[32];
+    const int iter = P.st->iter_base + slot;
+    if (skip_iter(P.st, iter)) return;
+    const int dsub = blockIdx.x;
+    const int e0 = P.loff[dsub], e1 = P.loff[dsub + 1];
+    double ww = 0.0;
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+        double wv = P.r[e] - gt_alpha(P, e, P.alpha);
+        P.w[e] = wv;
+        if (PRECOND == PREC_NONE) P.y[e] = wv;
+        ww += wv * wv * P.minv[e];
+    }
+    ww = block_sum(ww, sh);
+    if (threadIdx.x == 0) {
+        P.part_w[dsub] = ww;
+        if (PRECOND == PREC_NONE) P.part_rho[dsub] = ww;
+    }
+    if (PRECOND == PREC_NONE) return;
+    __syncthreads();
+    const int t0 = P.toff[dsub], t1 = P.toff[dsub + 1], nt = t1 - t0;
+    double *u = sm;
+    for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+        double s = 0.0;
+        for (int j = P.trow_ptr[t0 + t]; j < P.trow_ptr[t0 + t + 1]; ++j) {
+            int e = P.trow_idx[j];
+            s += P.ws[e] * P.w[e];
+        }
+        if (PRECOND == PREC_LUMPED) u[t] = s;
+        else P.uT[t0 + t] = s;
+        if (PRECOND == PREC_WEIGHT) P.vT[t0 + t] = s;
+    }
+    if (PRECOND != PREC_LUMPED) return;
+    __syncthreads();
+    for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+        double s = 0.0;
+        for (int j = P.kt_ptr[t0 + t]; j < P.kt_ptr[t0 + t + 1]; ++j) s += P.kt_val[j] * u[P.kt_col[j] - t0];
+        P.vT[t0 + t] = s;
+    }
+}
+
+// z = assemble(W B v_T); d = G z.  One CTA per subdomain.
+__global__ void z_kernel(DevProblem P, int slot) {
+    __shared__ double sh[32 * KMAX];
+    const int iter = P.st->iter_base + slot;
+    if (skip_iter(P.st, iter)) return;
+    const int dsub = blockIdx.x;
+    double gk[KMAX];
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k) gk[k] = 0.0;
+    for (int e = P.loff[dsub] + threadIdx.x; e < P.loff[dsub + 1]; e += blockDim.x) {
+        double zv = P.ws[e] * P.vT[P.tidx[e]];
+        int q = P.partner[e];
+        if (q >= 0) zv += P.ws[q] * P.vT[P.tidx[q]];
+        P.z[e] = zv;
+#pragma unroll
+        for (int k = 0; k < KMAX; ++k) gk[k] += P.Gl[(size_t)e * KMAX + k] * zv;
+    }
+    block_sum_k(gk, sh);
+    if (threadIdx.x == 0) {
+        int nk = P.kof[dsub + 1] - P.kof[dsub];
+        for (int k = 0; k < nk; ++k) P.d[P.kof[dsub] + k] = gk[k];
+    }
+}
+
+// y = z - G^T alpha, rho partials = y.w; zero the F-apply accumulator.
+__global__ void y_kernel(DevProblem P, int slot) {
+    __shared__ double sh[32];
+    const int iter = P.st->iter_base + slot;
+    if (skip_iter(P.st, iter)) return;
+    const int dsub = blockIdx.x;
+    double s = 0.0;
+    for (int e = P.loff[dsub] + threadIdx.x; e < P.loff[dsub + 1]; e += blockDim.x) {
+        double yv = P.z[e] - gt_alpha(P, e, P.alpha);
+        P.y[e] = yv;
+        s += yv * P.w[e] * P.minv[e];
+        P.Ap[e] = 0.0;
+    }
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) P.part_rho[dsub] = s;
+}
+
+__global__ void zero_vT_kernel(DevProblem P, int slot) {
+    const int iter = P.st->iter_base + slot;
+    if (skip_iter(P.st, iter)) return;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < P.NT; t += gridDim.x * blockDim.x) P.vT[t] = 0.0;
+}
+
+// p = y + beta p, x += alpha p, r -= alpha assemble(Ap), d = G r, convergence check.
+__global__ void update_kernel(DevProblem P, const double *item_dot, int nitems, int slot) {
+    __shared__ double sh[32 * KMAX];
+    const int iter = P.st->iter_base + slot;
+    if (skip_iter(P.st, iter)) return;
+    const double rho = array_sum(P.part_rho, P.nd, sh);
+    const double pAp = array_sum(item_dot, nitems, sh);
+    const double wn2 = array_sum(P.part_w, P.nd, sh);
+    const double beta = (iter == 0) ? 0.0 : rho / P.rho_hist[iter - 1];
+    const double alpha = rho / pAp;
+    const int dsub = blockIdx.x;
+    double gk[KMAX];
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k) gk[k] = 0.0;
+    for (int e = P.loff[dsub] + threadIdx.x; e < P.loff[dsub + 1]; e += blockDim.x) {
+        double pv = P.y[e] + beta * P.p[e];
+        P.p[e] = pv;
+        P.x[e] += alpha * pv;
+        int q = P.partner[e];
+        double a = P.Ap[e] + (q >= 0 ? P.Ap[q] : 0.0);
+        double rv = P.r[e] - alpha * a;
+        P.r[e] = rv;
+#pragma unroll
+        for (int k = 0; k < KMAX; ++k) gk[k] += P.Gl[(size_t)e * KMAX + k] * rv;
+    }
+    block_sum_k(gk, sh);
+    if (threadIdx.x == 0) {
+        int nk = P.kof[dsub + 1] - P.kof[dsub];
+        for (int k = 0; k < nk; ++k) P.d[P.kof[dsub] + k] = gk[k];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        DevState *st = P.st;
+        P.rho_hist[iter] = rho;
+        double wn = sqrt(wn2);
+        st->last_norm = wn;
+        if (!st->mixed) {
+            if (wn < st->tol && st->conv_iter < 0) st->conv_iter = iter;
+        } else {
+            // reliable updates: converge only on a recomputed residual, replace the
+            // iterated residual when it dropped by `delta` since the last replacement
+            if (wn < st->tol) {
+                if (st->r_true) {
+                    if (st->conv_iter < 0) st->conv_iter = iter;
+                } else {
+                    st->replace_next = 1;
+                }
+            } else if (wn < st->delta * st->rmax) {
+                st->replace_next = 1;
+            }
+            st->r_true = 0;
+        }
+    }
+}
+
+// after a replacement r = b - F64 x: reset the reliable-update bookkeeping
+__global__ void replace_done_kernel(DevProblem P, int slot) {
+    const int iter = P.st->iter_base + slot;
+    if (skip_iter(P.st, iter)) return;
+    DevState *st = P.st;
+    if (!st->replace_next) return;
+    st->replace_next = 0;
+    st->r_true = 1;
+    st->replacements += 1;
+}
+
+// clear the F64 accumulator after a residual replacement consumed it
+__global__ void zero_cond_kernel(DevProblem P, double *v, int slot) {
+    const int iter = P.st->iter_base + slot;
+    if (skip_iter(P.st, iter) || !P.st->replace_next) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.NL; i += gridDim.x * blockDim.x) v[i] = 0.0;
+}
+
+__global__ void chunk_end_kernel(DevProblem P, int chunk) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) P.st->iter_base += chunk;
+}
+
+// rmax tracking for reliable updates: after the w norm of an iteration is known
+__global__ void rmax_kernel(DevProblem P, int slot) {
+    const int iter = P.st->iter_base + slot;
+    if (skip_iter(P.st, iter)) return;
+    __shared__ double sh[32];
+    double wn2 = array_sum(P.part_w, P.nd, sh);
+    if (threadIdx.x == 0) {
+        DevState *st = P.st;
+        double wn = sqrt(wn2);
+        if (st->r_true) st->rmax = wn;
+        else st->rmax = fmax(st->rmax, wn);
+    }
+}
+
+}  // namespace
+
+// =============================================================================================
+struct TileSetHost {
+    int prec = -1;
+    int nitems = 0;
+    size_t bytes = 0;          // stored bytes
+    double alg_bytes = 0.0;    // algorithmic bytes of one apply (triangle + vectors)
+    int4 *items = nullptr;
+    int *mat_n = nullptr, *mat_voff = nullptr, *mat_tn = nullptr;
+    long long *mat_tile0 = nullptr;
+    unsigned *tile_ij = nullptr;
+    void *tiles = nullptr;
+    float *scale = nullptr;
+    double *item_dot = nullptr;
+    int *queue = nullptr;
+    TileSetDev dev() const {
+        TileSetDev t;
+        t.nitems = nitems; t.prec = prec; t.items = items; t.mat_n = mat_n; t.mat_voff = mat_voff; t.mat_tn = mat_tn;
+        t.mat_tile0 = mat_tile0; t.tile_ij = tile_ij; t.tiles = tiles; t.scale = scale; t.item_dot = item_dot;
+        t.queue = queue;
+        return t;
+    }
+};
+
+struct GpuSolver::Impl {
+    int device = 0;
+    int nsm = 148;
+    cudaStream_t stream = nullptr;
+    SolveOptions opt;
+    std::vector<void *> allocs;
+    size_t bytes = 0;
+    DevProblem P{};
+    DevState *st = nullptr;
+    TileSetHost F64, Flow, Dir;
+    int max_tn = 0, max_tn_dir = 0, max_nt = 0;
+    std::vector<int> h_lam;       // L row -> lambda
+    std::vector<int> h_loff;
+    int n_lambda = 0;
+    cudaGraphExec_t graph = nullptr;
+    int graph_chunk = 0, graph_prec = -1, graph_precond = -1;
+    double *Ax64 = nullptr;   // F apply output outside the iteration operator (initial, replacement, tests)
+    double *e_dev = nullptr;
+    int rho_cap = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    template <typename T>
+    T *alloc(size_t n) {
+        void *p = nullptr;
+        if (n == 0) n = 1;
+        CUDA_CHECK(cudaMalloc(&p, n * sizeof(T)));
+        allocs.push_back(p);
+        bytes += n * sizeof(T);
+        return (T *)p;
+    }
+    template <typename T>
+    T *upload(const std::vector<T> &v) {
+        T *p = alloc<T>(v.size());
+        if (!v.empty()) CUDA_CHECK(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+        return p;
+    }
+    ~Impl() {
+        if (graph) cudaGraphExecDestroy(graph);
+        for (void *p : allocs) cudaFree(p);
+        if (stream) cudaStreamDestroy(stream);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+    }
+
+    void build_tiles(TileSetHost &T, int prec, const std::vector<const double *> &mats, const std::vector<int> &ns,
+                     const std::vector<int> &voffs, int tiles_per_item);
+    void launch_tiles(const TileSetHost &T, int mode, const double *src, const double *src2, double *out, int slot);
+    void capture_chunk(int chunk);
+    void launch_iteration(int slot);
+    int kernels_per_iteration() const;
+};
+
+void GpuSolver::Impl::build_tiles(TileSetHost &T, int prec, const std::vector<const double *> &mats,
+                                  const std::vector<int> &ns, const std::vector<int> &voffs, int tiles_per_item) {
+    const int nm = (int)mats.size();
+    const size_t esz = prec == SCHUR_FP64 ? 8 : prec == SCHUR_FP32 ? 4 : 2;
+    const size_t tbytes = (size_t)TILE * TILE * esz;
+    std::vector<int> mn(nm), mv(nm), mt(nm);
+    std::vector<long long> m0(nm);
+    long long total = 0;
+    double alg = 0.0;
+    for (int m = 0; m < nm; ++m) {
+        mn[m] = ns[m];
+        mv[m] = voffs[m];
+        mt[m] = (ns[m] + TILE - 1) / TILE;
+        m0[m] = total;
+        total += (long long)mt[m] * (mt[m] + 1) / 2;
+        alg += (double)ns[m] * (ns[m] + 1) / 2 * (double)esz + (double)ns[m] * (4 + 8 + 8);
+    }
+    std::vector<unsigned> ij(total);
+    std::vector<unsigned char> data((size_t)total * tbytes);
+    std::vector<float> sc(prec == SCHUR_BF16 ? total : 0);
+    for (int m = 0; m < nm; ++m) {
+        const double *S = mats[m];
+        const int n = ns[m], tn = mt[m];
+        long long g = m0[m];
+        for (int I = 0; I < tn; ++I)
+            for (int J = I; J < tn; ++J, ++g) {
+                ij[g] = ((unsigned)I << 16) | (unsigned)J;
+                unsigned char *dst = data.data() + (size_t)g * tbytes;
+                double amax = 0.0;
+                if (prec == SCHUR_BF16)
+                    for (int r = 0; r < TILE; ++r)
+                        for (int c = 0; c < TILE; ++c) {
+                            int gr = TILE * I + r, gc = TILE * J + c;
+                            if (gr < n && gc < n) amax = std::max(amax, std::fabs(S[(size_t)gc * n + gr]));
+                        }
+                float s = (amax > 0) ? (float)amax : 1.0f;
+                if (prec == SCHUR_BF16) sc[g] = s;
+                for (int r = 0; r < TILE; ++r)
+                    for (int c = 0; c < TILE; ++c) {
+                        int gr = TILE * I + r, gc = TILE * J + c;
+                        double v = (gr < n && gc < n) ? S[(size_t)gc * n + gr] : 0.0;
+                        size_t o = (size_t)r * TILE + c;
+                        if (prec == SCHUR_FP64) ((double *)dst)[o] = v;
+                        else if (prec == SCHUR_FP32) ((float *)dst)[o] = (float)v;
+                        else ((__nv_bfloat16 *)dst)[o] = __float2bfloat16_rn((float)(v / s));
+                    }
+            }
+    }
+    // work items: up to tiles_per_item tiles of one matrix; largest matrices first
+    std::vector<int> order(nm);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return mt[a] > mt[b]; });
+    std::vector<int4> items;
+    for (int m : order) {
+        int nt = mt[m] * (mt[m] + 1) / 2;
+        int pieces = std::max(1, (nt + tiles_per_item - 1) / tiles_per_item);
+        for (int k = 0; k < pieces; ++k) {
+            int a = (int)((long long)nt * k / pieces), b = (int)((long long)nt * (k + 1) / pieces);
+            items.push_back(make_int4(m, a, b, 0));
+        }
+    }
+    T.prec = prec;
+    T.nitems = (int)items.size();
+    T.bytes = data.size();
+    T.alg_bytes = alg;
+    T.items = upload(items);
+    T.mat_n = upload(mn);
+    T.mat_voff = upload(mv);
+    T.mat_tn = upload(mt);
+    T.mat_tile0 = upload(m0);
+    T.tile_ij = upload(ij);
+    T.tiles = upload(data);
+    T.scale = prec == SCHUR_BF16 ? upload(sc) : nullptr;
+    T.item_dot = alloc<double>(items.size());
+    T.queue = alloc<int>(2);
+    CUDA_CHECK(cudaMemset(T.queue, 0, 2 * sizeof(int)));
+}
+
+static size_t tile_smem(int prec, int max_tn) {
+    size_t acc = prec == SCHUR_FP64 ? 8 : 4;
+    return 2 * acc * (size_t)max_tn * TILE;
+}
+
+void GpuSolver::Impl::launch_tiles(const TileSetHost &T, int mode, const double *src, const double *src2, double *out,
+                                   int slot) {
+    int mtn = (&T == &Dir) ? max_tn_dir : max_tn;
+    size_t sm = tile_smem(T.prec, mtn);
+    int grid = std::max(1, std::min(T.nitems, nsm * 2));
+    TileSetDev td = T.dev();
+#define LAUNCH(PR, MD) tile_symv_kernel<PR, MD><<<grid, 256, sm, stream>>>(td, P, src, src2, out, slot)
+#define LAUNCH_MODES(PR)                                   \
+    switch (mode) {                                        \
+    case 0: LAUNCH(PR, 0); break;                          \
+    case 1: LAUNCH(PR, 1); break;                          \
+    case 2: LAUNCH(PR, 2); break;                          \
+    default: LAUNCH(PR, 3); break;                         \
+    }
+    FETI_CHECK(mode != 1 || src2 != nullptr, "internal: PCG direction update without a previous direction");
+    if (T.prec == SCHUR_FP64) { LAUNCH_MODES(SCHUR_FP64) }
+    else if (T.prec == SCHUR_FP32) { LAUNCH_MODES(SCHUR_FP32) }
+    else { LAUNCH_MODES(SCHUR_BF16) }
+#undef LAUNCH_MODES
+#undef LAUNCH
+    CUDA_CHECK(cudaGetLastError());
+}
+
+template <int PR>
+static void set_tile_limits(int v) {
+    cudaFuncSetAttribute(tile_symv_kernel<PR, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+    cudaFuncSetAttribute(tile_symv_kernel<PR, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+    cudaFuncSetAttribute(tile_symv_kernel<PR, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+    cudaFuncSetAttribute(tile_symv_kernel<PR, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+}
+
+static void set_smem_limits() {
+    static bool done = false;
+    if (done) return;
+    const int v = 200 * 1024;
+    set_tile_limits<SCHUR_FP64>(v);
+    set_tile_limits<SCHUR_FP32>(v);
+    set_tile_limits<SCHUR_BF16>(v);
+    cudaFuncSetAttribute(w_prec_kernel<PREC_LUMPED>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+    done = true;
+}
+
+// One PCG iteration (reference order: w = P r, z = M w, y = P z, p, F p, update).
+void GpuSolver::Impl::launch_iteration(int slot) {
+    const int nd = P.nd;
+    const int cgrid = (P.nK + 7) / 8;
+    const bool mixed = opt.schur_precision != SCHUR_FP64;
+    const TileSetHost &Fop = mixed ? Flow : F64;
+    if (mixed) {
+        // residual replacement r = b - F64 x when the previous update asked for it
+        launch_tiles(F64, 3, P.x, nullptr, Ax64, slot);
+        r0_kernel<<<nd, TPB, 0, stream>>>(P, Ax64, 1, slot);
+        zero_cond_kernel<<<std::max(1, std::min(1024, (P.NL + 255) / 256)), 256, 0, stream>>>(P, Ax64, slot);
+        replace_done_kernel<<<1, 32, 0, stream>>>(P, slot);
+    }
+    coarse_kernel<<<cgrid, 256, 0, stream>>>(P, P.d, P.alpha, slot, 1);
+    const size_t tsm = sizeof(double) * (size_t)std::max(1, max_nt);
+    switch (opt.precond) {
+    case PREC_NONE: w_prec_kernel<PREC_NONE><<<nd, TPB, 0, stream>>>(P, slot); break;
+    case PREC_LUMPED: w_prec_kernel<PREC_LUMPED><<<nd, TPB, tsm, stream>>>(P, slot); break;
+    case PREC_WEIGHT: w_prec_kernel<PREC_WEIGHT><<<nd, TPB, 0, stream>>>(P, slot); break;
+    default: w_prec_kernel<PREC_DIRICHLET><<<nd, TPB, 0, stream>>>(P, slot); break;
+    }
+    if (mixed) rmax_kernel<<<1, 256, 0, stream>>>(P, slot);
+    if (opt.precond != PREC_NONE) {
+        if (opt.precond == PREC_DIRICHLET) {
+            zero_vT_kernel<<<std::max(1, std::min(1024, (P.NT + 255) / 256)), 256, 0, stream>>>(P, slot);
+            launch_tiles(Dir, 2, P.uT, nullptr, P.vT, slot);
+        }
+        z_kernel<<<nd, TPB, 0, stream>>>(P, slot);
+        coarse_kernel<<<cgrid, 256, 0, stream>>>(P, P.d, P.alpha, slot, 1);
+        y_kernel<<<nd, TPB, 0, stream>>>(P, slot);
+    } else {
+        zero_kernel<<<(P.NL + 255) / 256, 256, 0, stream>>>(P.Ap, P.NL);
+    }
+    launch_tiles(Fop, 1, P.y, P.p, P.Ap, slot);
+    update_kernel<<<nd, TPB, 0, stream>>>(P, Fop.item_dot, Fop.nitems, slot);
+    CUDA_CHECK(cudaGetLastError());
+}
+
+int GpuSolver::Impl::kernels_per_iteration() const {
+    const bool mixed = opt.schur_precision != SCHUR_FP64;
+    int k = 3;  // coarse, w/prec, update
+    k += 1;     // F apply
+    if (mixed) k += 5;
+    if (opt.precond != PREC_NONE) k += 3 + (opt.precond == PREC_DIRICHLET ? 2 : 0);
+    else k += 1;
+    return k;
+}
+
+void GpuSolver::Impl::capture_chunk(int chunk) {
+    if (graph && graph_chunk == chunk && graph_prec == opt.schur_precision && graph_precond == opt.precond) return;
+    if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+    cudaGraph_t g;
+    CUDA_CHECK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    for (int j = 0; j < chunk; ++j) launch_iteration(j);
+    chunk_end_kernel<<<1, 32, 0, stream>>>(P, chunk);
+    CUDA_CHECK(cudaStreamEndCapture(stream, &g));
+    CUDA_CHECK(cudaGraphInstantiate(&graph, g, 0));
+    cudaGraphDestroy(g);
+    graph_chunk = chunk;
+    graph_prec = opt.schur_precision;
+    graph_precond = opt.precond;
+}
+
+GpuSolver::GpuSolver() : impl(new Impl) {}
+GpuSolver::~GpuSolver() { delete impl; }
+size_t GpuSolver::device_bytes() const { return impl->bytes; }
+int GpuSolver::device_id() const { return impl->device; }
+void GpuSolver::set_options(const SolveOptions &opt) {
+    FETI_CHECK(opt.schur_precision == SCHUR_FP64 || impl->Flow.prec == opt.schur_precision,
+               "FETI4I: the requested Schur precision was not prepared on the device");
+    FETI_CHECK(opt.precond == impl->opt.precond, "FETI4I: the preconditioner is fixed at instance creation");
+    int tpi = impl->opt.tiles_per_item;
+    impl->opt = opt;
+    impl->opt.tiles_per_item = tpi;
+}
+
+bool cuda_available(std::string &why) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        why = (e != cudaSuccess) ? cudaGetErrorString(e) : "no CUDA device";
+        return false;
+    }
+    return true;
+}
+
+void GpuSolver::upload(const Decomposition &dec, const Prep &prep, const SolveOptions &opt) {
+    Impl &I = *impl;
+    I.opt = opt;
+    std::string why;
+    FETI_CHECK(cuda_available(why), "FETI4I: no usable CUDA device (" + why + "); the dual solver runs on the GPU only");
+    CUDA_CHECK(cudaGetDevice(&I.device));
+    cudaDeviceProp prop;
+    CUDA_CHECK(cudaGetDeviceProperties(&prop, I.device));
+    FETI_CHECK(prop.major == 10, "FETI4I: this build targets sm_100a (B200); found compute capability " +
+                                     std::to_string(prop.major) + "." + std::to_string(prop.minor));
+    I.nsm = prop.multiProcessorCount;
+    CUDA_CHECK(cudaStreamCreateWithFlags(&I.stream, cudaStreamNonBlocking));
+    CUDA_CHECK(cudaEventCreate(&I.ev0));
+    CUDA_CHECK(cudaEventCreate(&I.ev1));
+    set_smem_limits();
+
+    const int nd = dec.ndom;
+    std::vector<int> loff(nd + 1, 0), kof(nd + 1, 0), toff(nd + 1, 0);
+    for (int d = 0; d < nd; ++d) {
+        loff[d + 1] = loff[d] + prep.sub[d].ni;
+        kof[d + 1] = kof[d] + prep.sub[d].nk;
+        toff[d + 1] = toff[d] + prep.sub[d].t;
+        FETI_CHECK(prep.sub[d].nk <= KMAX, "FETI4I: kernel dimension above the supported bound");
+    }
+    const int NL = loff[nd], NT = toff[nd];
+    I.n_lambda = dec.n_lambda;
+    I.h_loff = loff;
+    I.h_lam.resize(NL);
+    std::vector<int> partner(NL, -1), tidx(NL), rkof(NL), rnk(NL);
+    std::vector<double> ws(NL), minv(NL), Gl((size_t)NL * KMAX, 0.0);
+    for (int d = 0; d < nd; ++d) {
+        const DomainRows &D = dec.dom[d];
+        const SubPrep &S = prep.sub[d];
+        for (int r = 0; r < S.ni; ++r) {
+            int e = loff[d] + r;
+            int l = D.lam[r];
+            I.h_lam[e] = l;
+            int d0 = prep.own_dom[2 * (size_t)l], d1 = prep.own_dom[2 * (size_t)l + 1];
+            int r0 = prep.own_row[2 * (size_t)l], r1 = prep.own_row[2 * (size_t)l + 1];
+            if (d1 >= 0) partner[e] = (d0 == d && r0 == r) ? loff[d1] + r1 : loff[d0] + r0;
+            tidx[e] = toff[d] + S.trow[r];
+            ws[e] = D.w[r] * D.sign[r];
+            minv[e] = d1 >= 0 ? 0.5 : 1.0;
+            rkof[e] = kof[d];
+            rnk[e] = S.nk;
+            for (int k = 0; k < S.nk; ++k) Gl[(size_t)e * KMAX + k] = S.G[(size_t)k * S.ni + r];
+        }
+    }
+    // T space: rows of each touched DOF, lumped K_TT in global T indices
+    std::vector<int> trow_ptr(NT + 1, 0), trow_idx(NL);
+    for (int e = 0; e < NL; ++e) trow_ptr[tidx[e] + 1]++;
+    for (int t = 0; t < NT; ++t) trow_ptr[t + 1] += trow_ptr[t];
+    {
+        std::vector<int> fill(trow_ptr.begin(), trow_ptr.end() - 1);
+        for (int e = 0; e < NL; ++e) trow_idx[fill[tidx[e]]++] = e;
+    }
+    std::vector<int> kt_ptr(NT + 1, 0), kt_col;
+    std::vector<double> kt_val;
+    I.max_nt = 0;
+    for (int d = 0; d < nd; ++d) {
+        const SubPrep &S = prep.sub[d];
+        I.max_nt = std::max(I.max_nt, S.t);
+        if (opt.precond == PREC_LUMPED) {
+            for (int t = 0; t < S.t; ++t) {
+                for (int j = S.KT_ptr[t]; j < S.KT_ptr[t + 1]; ++j) {
+                    kt_col.push_back(toff[d] + S.KT_col[j]);
+                    kt_val.push_back(S.KT_val[j]);
+                }
+                kt_ptr[toff[d] + t + 1] = (int)kt_col.size();
+            }
+        }
+    }
+    if (opt.precond == PREC_LUMPED)
+        FETI_CHECK(sizeof(double) * (size_t)I.max_nt <= 200 * 1024, "FETI4I: subdomain interface too large for the lumped kernel");
+
+    DevProblem &P = I.P;
+    P.nd = nd; P.NL = NL; P.nK = prep.n_kern; P.NT = NT;
+    P.loff = I.upload(loff); P.kof = I.upload(kof); P.toff = I.upload(toff);
+    P.partner = I.upload(partner); P.tidx = I.upload(tidx); P.ws = I.upload(ws); P.minv = I.upload(minv);
+    P.Gl = I.upload(Gl); P.rkof = I.upload(rkof); P.rnk = I.upload(rnk);
+    P.trow_ptr = I.upload(trow_ptr); P.trow_idx = I.upload(trow_idx);
+    P.kt_ptr = I.upload(kt_ptr); P.kt_col = I.upload(kt_col); P.kt_val = I.upload(kt_val);
+    P.GGtinv = I.upload(prep.GGt_inv);
+    P.bL = I.alloc<double>(NL);
+    P.x = I.alloc<double>(NL); P.r = I.alloc<double>(NL); P.w = I.alloc<double>(NL); P.z = I.alloc<double>(NL);
+    P.y = I.alloc<double>(NL); P.p = I.alloc<double>(NL); P.Ap = I.alloc<double>(NL);
+    I.Ax64 = I.alloc<double>(NL);
+    P.uT = I.alloc<double>(NT); P.vT = I.alloc<double>(NT);
+    P.d = I.alloc<double>(prep.n_kern); P.alpha = I.alloc<double>(prep.n_kern);
+    I.e_dev = I.alloc<double>(prep.n_kern);
+    P.part_w = I.alloc<double>(nd); P.part_rho = I.alloc<double>(nd); P.part_b = I.alloc<double>(nd);
+    P.rho_hist = I.alloc<double>((size_t)opt.max_iterations + 64);
+    I.st = I.alloc<DevState>(1);
+    P.st = I.st;
+    CUDA_CHECK(cudaMemset(P.Ap, 0, sizeof(double) * NL));
+    CUDA_CHECK(cudaMemset(I.Ax64, 0, sizeof(double) * NL));
+    CUDA_CHECK(cudaMemset(P.p, 0, sizeof(double) * NL));
+    I.rho_cap = opt.max_iterations + 64;
+
+    // Schur tiles: FP64 always (true residuals, FP64 path), low precision on request
+    std::vector<const double *> mats(nd);
+    std::vector<int> ns(nd), voffs(nd);
+    I.max_tn = 0;
+    for (int d = 0; d < nd; ++d) {
+        mats[d] = prep.sub[d].S.data();
+        ns[d] = prep.sub[d].ni;
+        voffs[d] = loff[d];
+        I.max_tn = std::max(I.max_tn, (ns[d] + TILE - 1) / TILE);
+    }
+    FETI_CHECK(tile_smem(SCHUR_FP64, I.max_tn) <= 200 * 1024, "FETI4I: a Schur complement is too large for the tile kernel");
+    I.build_tiles(I.F64, SCHUR_FP64, mats, ns, voffs, opt.tiles_per_item);
+    if (opt.schur_precision != SCHUR_FP64) I.build_tiles(I.Flow, opt.schur_precision, mats, ns, voffs, opt.tiles_per_item);
+    if (opt.precond == PREC_DIRICHLET) {
+        std::vector<const double *> dm(nd);
+        std::vector<int> dn(nd), dv(nd);
+        I.max_tn_dir = 0;
+        for (int d = 0; d < nd; ++d) {
+            dm[d] = prep.sub[d].Sdir.data();
+            dn[d] = prep.sub[d].t;
+            dv[d] = toff[d];
+            I.max_tn_dir = std::max(I.max_tn_dir, (dn[d] + TILE - 1) / TILE);
+        }
+        FETI_CHECK(tile_smem(SCHUR_FP64, I.max_tn_dir) <= 200 * 1024, "FETI4I: a Dirichlet block is too large for the tile kernel");
+        I.build_tiles(I.Dir, SCHUR_FP64, dm, dn, dv, opt.tiles_per_item);
+    }
+    CUDA_CHECK(cudaDeviceSynchronize());
+}
+
+void GpuSolver::set_rhs(const std::vector<double> &b, const std::vector<double> &e) {
+    Impl &I = *impl;
+    std::vector<double> bL(I.h_lam.size());
+    for (size_t i = 0; i < bL.size(); ++i) bL[i] = b[I.h_lam[i]];
+    CUDA_CHECK(cudaMemcpyAsync((void *)I.P.bL, bL.data(), bL.size() * sizeof(double), cudaMemcpyHostToDevice, I.stream));
+    CUDA_CHECK(cudaMemcpyAsync(I.e_dev, e.data(), e.size() * sizeof(double), cudaMemcpyHostToDevice, I.stream));
+    CUDA_CHECK(cudaStreamSynchronize(I.stream));
+}
+
+void GpuSolver::solve(SolveStats &stats) {
+    Impl &I = *impl;
+    DevProblem &P = I.P;
+    FETI_CHECK(I.opt.max_iterations + 64 <= I.rho_cap, "FETI4I: max_iterations grew after instance creation");
+    const bool mixed = I.opt.schur_precision != SCHUR_FP64;
+    DevState h{};
+    h.conv_iter = -1;
+    h.iter_base = 0;
+    h.replace_next = 0;
+    h.r_true = 1;
+    h.replacements = 0;
+    h.max_it = I.opt.max_iterations;
+    h.mixed = mixed ? 1 : 0;
+    h.precision = I.opt.precision;
+    h.delta = I.opt.reliable_delta;
+    const int nd = P.nd;
+    const int cgrid = (P.nK + 7) / 8;
+    CUDA_CHECK(cudaEventRecord(I.ev0, I.stream));
+    CUDA_CHECK(cudaMemcpyAsync(I.st, &h, sizeof(h), cudaMemcpyHostToDevice, I.stream));
+    // lambda_0 = G^T (GG^T)^-1 e ; r_0 = b - F lambda_0 ; tol = precision * min(|P r_0|, |b|)
+    coarse_kernel<<<cgrid, 256, 0, I.stream>>>(P, I.e_dev, P.alpha, 0, 0);
+    gt_kernel<<<(P.NL + 255) / 256, 256, 0, I.stream>>>(P, P.alpha, P.x);
+    zero_kernel<<<(P.NL + 255) / 256, 256, 0, I.stream>>>(P.p, P.NL);
+    I.launch_tiles(I.F64, 0, P.x, nullptr, I.Ax64, 0);
+    r0_kernel<<<nd, TPB, 0, I.stream>>>(P, I.Ax64, 0, 0);
+    zero_kernel<<<(P.NL + 255) / 256, 256, 0, I.stream>>>(I.Ax64, P.NL);
+    coarse_kernel<<<cgrid, 256, 0, I.stream>>>(P, P.d, P.alpha, 0, 0);
+    pnorm_kernel<<<nd, TPB, 0, I.stream>>>(P);
+    tol_kernel<<<1, 256, 0, I.stream>>>(P);
+    CUDA_CHECK(cudaGetLastError());
+    int launches = 9;
+    const int chunk = std::max(1, I.opt.chunk);
+    if (I.opt.use_graph) I.capture_chunk(chunk);
+    DevState hs{};
+    for (int done = 0; done < I.opt.max_iterations; done += chunk) {
+        if (I.opt.use_graph) {
+            CUDA_CHECK(cudaGraphLaunch(I.graph, I.stream));
+        } else {
+            for (int j = 0; j < chunk; ++j) I.launch_iteration(j);
+            chunk_end_kernel<<<1, 32, 0, I.stream>>>(P, chunk);
+        }
+        launches += chunk * I.kernels_per_iteration() + 1;
+        CUDA_CHECK(cudaMemcpyAsync(&hs, I.st, sizeof(hs), cudaMemcpyDeviceToHost, I.stream));
+        CUDA_CHECK(cudaStreamSynchronize(I.stream));
+        if (hs.conv_iter >= 0) break;
+    }
+    // amplitudes alpha = (GG^T)^-1 G r (d holds G r of the last update)
+    coarse_kernel<<<cgrid, 256, 0, I.stream>>>(P, P.d, P.alpha, 0, 0);
+    launches += 1;
+    CUDA_CHECK(cudaEventRecord(I.ev1, I.stream));
+    CUDA_CHECK(cudaMemcpyAsync(&hs, I.st, sizeof(hs), cudaMemcpyDeviceToHost, I.stream));
+    CUDA_CHECK(cudaStreamSynchronize(I.stream));
+    float ms = 0.f;
+    CUDA_CHECK(cudaEventElapsedTime(&ms, I.ev0, I.ev1));
+    stats.t_solve_ms = ms;
+    stats.converged = hs.conv_iter >= 0;
+    stats.iterations = stats.converged ? hs.conv_iter + 1 : std::min(hs.iter_base, I.opt.max_iterations);
+    stats.replacements = hs.replacements;
+    stats.tol = hs.tol;
+    stats.final_norm = hs.last_norm;
+    stats.kernel_launches = launches;
+    const TileSetHost &Fop = mixed ? I.Flow : I.F64;
+    stats.fapply_bytes = Fop.alg_bytes;
+}
+
+void GpuSolver::get_solution(std::vector<double> &lambda, std::vector<double> &alpha) {
+    Impl &I = *impl;
+    std::vector<double> xL(I.h_lam.size());
+    CUDA_CHECK(cudaMemcpy(xL.data(), I.P.x, xL.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    lambda.assign(I.n_lambda, 0.0);
+    for (size_t e = 0; e < xL.size(); ++e) lambda[I.h_lam[e]] = xL[e];
+    alpha.resize(I.P.nK);
+    CUDA_CHECK(cudaMemcpy(alpha.data(), I.P.alpha, alpha.size() * sizeof(double), cudaMemcpyDeviceToHost));
+}
+
+void GpuSolver::apply_F(const double *x_lambda, double *y_lambda, int precision) {
+    Impl &I = *impl;
+    const TileSetHost &T = precision == SCHUR_FP64 ? I.F64 : I.Flow;
+    FETI_CHECK(T.prec == precision, "FETI4I: the requested Schur precision was not prepared on the device");
+    const int NL = I.P.NL;
+    std::vector<double> xL(NL), yL(NL);
+    for (int e = 0; e < NL; ++e) xL[e] = x_lambda[I.h_lam[e]];
+    CUDA_CHECK(cudaMemcpyAsync(I.P.w, xL.data(), NL * sizeof(double), cudaMemcpyHostToDevice, I.stream));
+    zero_kernel<<<(NL + 255) / 256, 256, 0, I.stream>>>(I.Ax64, NL);
+    I.launch_tiles(T, 0, I.P.w, nullptr, I.Ax64, 0);
+    CUDA_CHECK(cudaMemcpyAsync(yL.data(), I.Ax64, NL * sizeof(double), cudaMemcpyDeviceToHost, I.stream));
+    zero_kernel<<<(NL + 255) / 256, 256, 0, I.stream>>>(I.Ax64, NL);
+    CUDA_CHECK(cudaStreamSynchronize(I.stream));
+    for (int l = 0; l < I.n_lambda; ++l) y_lambda[l] = 0.0;
+    for (int e = 0; e < NL; ++e) y_lambda[I.h_lam[e]] += yL[e];
+}
+
+double GpuSolver::time_F(int precision, int reps) {
+    Impl &I = *impl;
+    const TileSetHost &T = precision == SCHUR_FP64 ? I.F64 : I.Flow;
+    FETI_CHECK(T.prec == precision, "FETI4I: the requested Schur precision was not prepared on the device");
+    const int NL = I.P.NL;
+    for (int i = 0; i < 3; ++i) {
+        zero_kernel<<<(NL + 255) / 256, 256, 0, I.stream>>>(I.Ax64, NL);
+        I.launch_tiles(T, 0, I.P.w, nullptr, I.Ax64, 0);
+    }
+    float total = 0.f;
+    for (int i = 0; i < reps; ++i) {
+        zero_kernel<<<(NL + 255) / 256, 256, 0, I.stream>>>(I.Ax64, NL);
+        CUDA_CHECK(cudaEventRecord(I.ev0, I.stream));
+        I.launch_tiles(T, 0, I.P.w, nullptr, I.Ax64, 0);
+        CUDA_CHECK(cudaEventRecord(I.ev1, I.stream));
+        CUDA_CHECK(cudaEventSynchronize(I.ev1));
+        float ms = 0.f;
+        CUDA_CHECK(cudaEventElapsedTime(&ms, I.ev0, I.ev1));
+        total += ms;
+    }
+    zero_kernel<<<(NL + 255) / 256, 256, 0, I.stream>>>(I.Ax64, NL);
+    CUDA_CHECK(cudaStreamSynchronize(I.stream));
+    return total / reps;
+}
+
+double GpuSolver::fapply_bytes(int precision) const {
+    const TileSetHost &T = precision == SCHUR_FP64 ? impl->F64 : impl->Flow;
+    return T.alg_bytes;
+}
+
+}  // namespace feti

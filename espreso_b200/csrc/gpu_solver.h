@@ -1,0 +1,68 @@
+// Device-resident Total-FETI dual iteration on one B200 (sm_100a).
+//
+// Dual vectors live in the replicated local layout: subdomain d owns rows
+// loff[d]..loff[d+1] (its local multipliers, i.e. rows of B_i); a multiplier
+// shared by two subdomains appears twice and both copies hold the same value.
+// Assembly of a sum over subdomains is "own value + partner value".
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "decompose.h"
+#include "prep.h"
+
+namespace feti {
+
+enum SchurPrecision { SCHUR_FP64 = 0, SCHUR_FP32 = 1, SCHUR_BF16 = 2 };
+
+struct SolveOptions {
+    double precision = 1e-5;
+    int max_iterations = 200;
+    int precond = PREC_DIRICHLET;
+    int schur_precision = SCHUR_FP64;  // storage of the iteration operator
+    int chunk = 16;                    // iterations per captured CUDA graph
+    int tiles_per_item = 48;           // work-queue granularity of the tile SYMV
+    double reliable_delta = 0.1;       // residual replacement threshold (mixed precision)
+    bool use_graph = true;
+};
+
+struct SolveStats {
+    int iterations = 0;
+    int replacements = 0;
+    double tol = 0.0;
+    double final_norm = 0.0;
+    double t_solve_ms = 0.0;       // device time of the dual PCG (events)
+    double t_fapply_ms = 0.0;      // average device time of one F apply (operator precision)
+    double fapply_bytes = 0.0;     // algorithmic bytes of one F apply
+    int fapply_launches = 0;
+    int kernel_launches = 0;       // kernels launched by the last solve
+    bool converged = false;
+};
+
+class GpuSolver {
+public:
+    GpuSolver();
+    ~GpuSolver();
+    void upload(const Decomposition &dec, const Prep &prep, const SolveOptions &opt);
+    // Dual PCG on device-resident b (lambda space), e (kernel space); outputs lambda and alpha.
+    void set_rhs(const std::vector<double> &b, const std::vector<double> &e);
+    void solve(SolveStats &st);
+    void get_solution(std::vector<double> &lambda, std::vector<double> &alpha);
+    // y = F x in lambda space with the given operator precision (tests, benchmarks)
+    void apply_F(const double *x_lambda, double *y_lambda, int precision);
+    // average device time of `reps` F applies (inputs resident), returns ms
+    double time_F(int precision, int reps);
+    double fapply_bytes(int precision) const;
+    size_t device_bytes() const;
+    int device_id() const;
+    void set_options(const SolveOptions &opt);
+
+    struct Impl;
+    Impl *impl;
+};
+
+bool cuda_available(std::string &why);
+
+}  // namespace feti

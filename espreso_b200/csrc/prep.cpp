@@ -1,0 +1,444 @@
+// Host preprocessing: subdomain K assembly, partial Cholesky with the fix
+// DOFs last, algebraic kernel detection on the fix-DOF Schur block, explicit
+// Schur complements S_i = B_i K_reg^-1 B_i^T, Dirichlet/lumped preconditioner
+// data and the coarse problem (GG^T)^-1.
+#include "prep.h"
+
+#include <omp.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <deque>
+#include <numeric>
+
+#include "common.h"
+#include "dense.h"
+
+namespace feti {
+
+namespace {
+
+// Breadth-first distances on the subdomain node graph (nodes sharing an element).
+std::vector<int> bfs(const std::vector<std::vector<int>> &adj, int src) {
+    std::vector<int> dist(adj.size(), -1);
+    std::deque<int> q;
+    dist[src] = 0;
+    q.push_back(src);
+    while (!q.empty()) {
+        int v = q.front();
+        q.pop_front();
+        for (int w : adj[v])
+            if (dist[w] < 0) { dist[w] = dist[v] + 1; q.push_back(w); }
+    }
+    return dist;
+}
+
+// Three mutually distant nodes whose DOFs are all touched by B: the fix set
+// on which the kernel of K is detected (the algebraic regularisation of
+// src/solver/generic/SparseMatrix.cpp:3540-4495 works on a Schur complement
+// of K onto a small DOF set in the same way).
+std::vector<int> choose_fix_nodes(const std::vector<std::vector<int>> &adj, const std::vector<char> &cand) {
+    int n = (int)adj.size();
+    int a = -1;
+    for (int i = 0; i < n; ++i)
+        if (cand[i]) { a = i; break; }
+    FETI_CHECK(a >= 0, "FETI4I: a subdomain has no DOF glued to other subdomains or fixed by Dirichlet conditions");
+    std::vector<int> fix{a};
+    std::vector<int> da = bfs(adj, a);
+    int b = -1;
+    for (int i = 0; i < n; ++i)
+        if (cand[i] && i != a && (b < 0 || da[i] > da[b])) b = i;
+    if (b < 0) return fix;
+    fix.push_back(b);
+    std::vector<int> db = bfs(adj, b);
+    int c = -1;
+    for (int i = 0; i < n; ++i) {
+        if (!cand[i] || i == a || i == b) continue;
+        if (c < 0 || std::min(da[i], db[i]) > std::min(da[c], db[c])) c = i;
+    }
+    if (c >= 0) fix.push_back(c);
+    return fix;
+}
+
+void orthonormalize(std::vector<double> &R, int n, int k) {
+    for (int pass = 0; pass < 2; ++pass)
+        for (int j = 0; j < k; ++j) {
+            double *rj = R.data() + (size_t)j * n;
+            for (int i = 0; i < j; ++i) {
+                const double *ri = R.data() + (size_t)i * n;
+                double s = 0.0;
+                for (int p = 0; p < n; ++p) s += ri[p] * rj[p];
+                for (int p = 0; p < n; ++p) rj[p] -= s * ri[p];
+            }
+            double nr = 0.0;
+            for (int p = 0; p < n; ++p) nr += rj[p] * rj[p];
+            nr = std::sqrt(nr);
+            FETI_CHECK(nr > 0.0, "FETI4I: degenerate kernel basis");
+            for (int p = 0; p < n; ++p) rj[p] /= nr;
+        }
+}
+
+}  // namespace
+
+void SubPrep::kplus(double *x) const {
+    std::vector<double> y(n);
+    for (int i = 0; i < n; ++i) y[pos[i]] = x[i];
+    dense::trsv_packed_lower(Lp.data(), n, y.data());
+    dense::trsv_packed_lower_t(Lp.data(), n, y.data());
+    for (int i = 0; i < n; ++i) x[i] = y[pos[i]];
+}
+
+static void prep_subdomain(const ElementData &el, const Decomposition &dec, int d, const PrepOptions &opt, SubPrep &S) {
+    const DomainRows &D = dec.dom[d];
+    const int dpn = dec.dpn;
+    const int n = D.ndofs;
+    const int nn = (int)D.nodes.size();
+    const auto &g2l = dec.g2l[d];
+    S.n = n;
+    S.ni = (int)D.lam.size();
+
+    // element local DOFs
+    std::vector<std::vector<int>> adj(nn);
+    std::vector<int> eldof;
+    // touched DOFs and candidate fix nodes
+    std::vector<char> touched(n, 0);
+    for (int r = 0; r < S.ni; ++r) touched[D.dof[r]] = 1;
+    std::vector<char> cand(nn, 0);
+    for (int a = 0; a < nn; ++a) {
+        bool all = true;
+        for (int c = 0; c < dpn; ++c) all = all && touched[dpn * a + c];
+        cand[a] = all;
+    }
+    for (int e : D.elems) {
+        int64_t nb = el.node_ptr[e], ne_ = el.node_ptr[e + 1];
+        for (int64_t i = nb; i < ne_; ++i)
+            for (int64_t j = nb; j < ne_; ++j)
+                if (i != j) adj[g2l.at(el.nodes[i])].push_back(g2l.at(el.nodes[j]));
+    }
+    for (auto &v : adj) { std::sort(v.begin(), v.end()); v.erase(std::unique(v.begin(), v.end()), v.end()); }
+    S.fix_nodes = choose_fix_nodes(adj, cand);
+    std::vector<char> isfix(n, 0);
+    std::vector<int> fixdofs;
+    for (int a : S.fix_nodes)
+        for (int c = 0; c < dpn; ++c) { isfix[dpn * a + c] = 1; fixdofs.push_back(dpn * a + c); }
+    const int ns = (int)fixdofs.size();
+
+    // factor order: [untouched | touched, not fix | fix]
+    S.pos.assign(n, -1);
+    int p = 0;
+    for (int i = 0; i < n; ++i) if (!touched[i]) S.pos[i] = p++;
+    const int n1 = p;
+    for (int i = 0; i < n; ++i) if (touched[i] && !isfix[i]) S.pos[i] = p++;
+    for (int i : fixdofs) S.pos[i] = p++;
+    S.t = n - n1;
+    S.tdof.resize(S.t);
+    for (int i = 0; i < n; ++i) if (S.pos[i] >= n1) S.tdof[S.pos[i] - n1] = i;
+    S.trow.resize(S.ni);
+    for (int r = 0; r < S.ni; ++r) S.trow[r] = S.pos[D.dof[r]] - n1;
+
+    // dense K in factor order and sparse K in T order
+    std::vector<double> A((size_t)n * n, 0.0);
+    std::vector<double> diag(n, 0.0);
+    S.f.assign(n, 0.0);
+    std::vector<std::vector<std::pair<int, double>>> KT(S.t);
+    for (int e : D.elems) {
+        int nd = (int)(el.dof_ptr[e + 1] - el.dof_ptr[e]);
+        eldof.resize(nd);
+        for (int k = 0; k < nd; ++k) {
+            int dof = el.dofs[el.dof_ptr[e] + k];
+            eldof[k] = dpn * g2l.at(dec.dof_node[dof]) + dec.dof_comp[dof];
+        }
+        const double *Ke = el.vals.data() + el.val_ptr[e];
+        for (int a = 0; a < nd; ++a) {
+            int pa = S.pos[eldof[a]];
+            for (int b = 0; b < nd; ++b) {
+                double v = Ke[(size_t)a * nd + b];
+                A[(size_t)S.pos[eldof[b]] * n + pa] += v;
+            }
+            diag[eldof[a]] += Ke[(size_t)a * nd + a];
+            if (pa >= n1)
+                for (int b = 0; b < nd; ++b) {
+                    int pb = S.pos[eldof[b]];
+                    if (pb >= n1) KT[pa - n1].emplace_back(pb - n1, Ke[(size_t)a * nd + b]);
+                }
+        }
+    }
+    if (opt.precond == PREC_LUMPED) {
+        S.KT_ptr.assign(S.t + 1, 0);
+        for (int i = 0; i < S.t; ++i) {
+            auto &row = KT[i];
+            std::sort(row.begin(), row.end(), [](auto &x, auto &y) { return x.first < y.first; });
+            int last = -1;
+            for (auto &kv : row) {
+                if (kv.first == last) { S.KT_val.back() += kv.second; continue; }
+                S.KT_col.push_back(kv.first);
+                S.KT_val.push_back(kv.second);
+                last = kv.first;
+            }
+            S.KT_ptr[i + 1] = (int)S.KT_col.size();
+        }
+    }
+    KT.clear();
+    KT.shrink_to_fit();
+    // Frobenius norm of K for the kernel check
+    double knorm = 0.0;
+    for (size_t i = 0; i < A.size(); ++i) knorm += A[i] * A[i];
+    knorm = std::sqrt(knorm);
+    std::vector<double> Kfix((size_t)n * ns);  // original columns of K at the fix DOFs (factor order rows)
+    for (int j = 0; j < ns; ++j)
+        std::memcpy(&Kfix[(size_t)j * n], &A[(size_t)(n - ns + j) * n], sizeof(double) * n);
+
+    // 1) eliminate the untouched DOFs: trailing block = Schur complement onto T
+    int info = dense::potrf_lower(A.data(), n, n, n1);
+    FETI_CHECK(info == 0, "FETI4I: interior block of a subdomain stiffness matrix is not positive definite");
+    if (opt.precond == PREC_DIRICHLET) {
+        S.Sdir.assign((size_t)S.t * S.t, 0.0);
+        for (int j = 0; j < S.t; ++j)
+            for (int i = j; i < S.t; ++i) {
+                double v = A[(size_t)(n1 + j) * n + n1 + i];
+                S.Sdir[(size_t)j * S.t + i] = v;
+                S.Sdir[(size_t)i * S.t + j] = v;
+            }
+    }
+    // 2) eliminate the touched, non-fix DOFs
+    double *At = A.data() + (size_t)n1 * n + n1;
+    info = dense::potrf_lower(At, S.t, n, S.t - ns);
+    FETI_CHECK(info == 0, "FETI4I: fix-node choice does not remove the rigid-body modes of a subdomain");
+    // 3) kernel of the fix-DOF Schur block
+    double *Ass = A.data() + (size_t)(n - ns) * n + (n - ns);
+    std::vector<double> Sss((size_t)ns * ns), ev(ns), V((size_t)ns * ns);
+    for (int j = 0; j < ns; ++j)
+        for (int i = 0; i < ns; ++i) Sss[(size_t)j * ns + i] = (i >= j) ? Ass[(size_t)j * n + i] : Ass[(size_t)i * n + j];
+    dense::jacobi_eigen(Sss.data(), ns, ev.data(), V.data());
+    S.ss_eigs = ev;
+    // defect: the last eigenvalue before a jump of more than 1e5 (SparseMatrix.cpp:3657-3661)
+    int defect = 0;
+    double scale = std::fabs(ev[ns - 1]);
+    for (int k = ns - 2; k >= 0; --k)
+        if (std::fabs(ev[k]) < 1e-5 * std::fabs(ev[k + 1])) { defect = k + 1; break; }
+    if (defect == 0 && scale > 0 && std::fabs(ev[0]) < 1e-10 * scale) defect = 1;
+    FETI_CHECK(defect > 0, "FETI4I: subdomain stiffness matrix is not singular (Total FETI expects floating subdomains)");
+    S.nk = defect;
+    double rho = *std::max_element(diag.begin(), diag.end());
+    for (int j = 0; j < ns; ++j)
+        for (int i = j; i < ns; ++i) {
+            double r = 0.0;
+            for (int k = 0; k < defect; ++k) r += V[(size_t)k * ns + i] * V[(size_t)k * ns + j];
+            Ass[(size_t)j * n + i] += rho * r;
+        }
+    info = dense::potrf_lower(Ass, ns, n, ns);
+    FETI_CHECK(info == 0, "FETI4I: regularised fix block is not positive definite");
+
+    // 4) kernel R = [-K_rr^-1 K_rs N; N] via the factor: R_r = -L_rr^-T (L_sr^T N)
+    const int nr = n - ns;
+    std::vector<double> Rp((size_t)n * defect, 0.0);
+    for (int k = 0; k < defect; ++k) {
+        double *x = &Rp[(size_t)k * n];
+        for (int s = 0; s < ns; ++s) {
+            double v = V[(size_t)k * ns + s];
+            x[nr + s] = v;
+            const double *Lrow = A.data() + (n - ns + s);  // row (nr+s), column j at Lrow[j*n]
+            for (int j = 0; j < nr; ++j) x[j] += Lrow[(size_t)j * n] * v;
+        }
+        for (int j = nr - 1; j >= 0; --j) {
+            const double *cj = A.data() + (size_t)j * n;
+            double s = x[j];
+            for (int i = j + 1; i < nr; ++i) s -= cj[i] * x[i];
+            x[j] = s / cj[j];
+        }
+        for (int j = 0; j < nr; ++j) x[j] = -x[j];
+    }
+    S.R.assign((size_t)n * defect, 0.0);
+    for (int k = 0; k < defect; ++k)
+        for (int i = 0; i < n; ++i) S.R[(size_t)k * n + i] = Rp[(size_t)k * n + S.pos[i]];
+    // kernel check on the fix columns: (K R) rows at the fix DOFs use the saved columns
+    {
+        double res = 0.0;
+        for (int k = 0; k < defect; ++k)
+            for (int j = 0; j < ns; ++j) {
+                double s = 0.0;
+                for (int i = 0; i < n; ++i) s += Kfix[(size_t)j * n + i] * Rp[(size_t)k * n + i];
+                res += s * s;
+            }
+        double rn = 0.0;
+        for (double v : Rp) rn += v * v;
+        S.kernel_residual = std::sqrt(res) / (knorm * std::sqrt(rn));
+    }
+    orthonormalize(S.R, n, defect);
+
+    // 5) S_i = B (K_reg^-1)_TT B^T with (K_reg^-1)_TT = W^T W, W = L_TT^-1
+    std::vector<double> W((size_t)S.t * S.t, 0.0), KiTT((size_t)S.t * S.t);
+    for (int j = 0; j < S.t; ++j)
+        for (int i = j; i < S.t; ++i) W[(size_t)j * S.t + i] = A[(size_t)(n1 + j) * n + n1 + i];
+    dense::trtri_lower(W.data(), S.t, S.t);
+    dense::lauum_lower(W.data(), S.t, S.t, KiTT.data(), S.t);
+    S.S.assign((size_t)S.ni * S.ni, 0.0);
+    for (int k = 0; k < S.ni; ++k)
+        for (int j = 0; j < S.ni; ++j)
+            S.S[(size_t)k * S.ni + j] = D.sign[j] * D.sign[k] * KiTT[(size_t)S.trow[k] * S.t + S.trow[j]];
+
+    // G_i = -(B_i R_i)^T (row-major nk x ni)
+    S.G.assign((size_t)defect * S.ni, 0.0);
+    for (int k = 0; k < defect; ++k)
+        for (int j = 0; j < S.ni; ++j) S.G[(size_t)k * S.ni + j] = -D.sign[j] * S.R[(size_t)k * n + D.dof[j]];
+
+    // packed factor for host K^+ solves
+    S.Lp.resize((size_t)n * (n + 1) / 2);
+    dense::pack_lower(A.data(), n, n, S.Lp.data());
+}
+
+void preprocess(const ElementData &el, Decomposition &dec, const std::vector<double> &rhs, const PrepOptions &opt,
+                Prep &out) {
+    const int dpn = dec.dpn;
+    double t0 = now_s();
+    // K diagonals for the B1 scaling (diagonal of each subdomain matrix)
+    std::vector<std::vector<double>> diags(dec.ndom);
+    for (int d = 0; d < dec.ndom; ++d) {
+        diags[d].assign(dec.dom[d].ndofs, 0.0);
+        for (int e : dec.dom[d].elems) {
+            int nd = (int)(el.dof_ptr[e + 1] - el.dof_ptr[e]);
+            const double *Ke = el.vals.data() + el.val_ptr[e];
+            for (int a = 0; a < nd; ++a) {
+                int dof = el.dofs[el.dof_ptr[e] + a];
+                diags[d][dpn * dec.g2l[d].at(dec.dof_node[dof]) + dec.dof_comp[dof]] += Ke[(size_t)a * nd + a];
+            }
+        }
+    }
+    compute_weights(dec, opt.scaling ? &diags : nullptr);
+
+    out.sub.assign(dec.ndom, SubPrep());
+    out.n_lambda = dec.n_lambda;
+    // largest subdomains first
+    std::vector<int> order(dec.ndom);
+    std::iota(order.begin(), order.end(), 0);
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return dec.dom[a].ndofs > dec.dom[b].ndofs; });
+    int nthreads = opt.threads > 0 ? opt.threads : omp_get_max_threads();
+    std::vector<std::string> errors(dec.ndom);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+    for (int k = 0; k < dec.ndom; ++k) {
+        int d = order[k];
+        try {
+            prep_subdomain(el, dec, d, opt, out.sub[d]);
+        } catch (const std::exception &ex) {
+            errors[d] = ex.what();
+        }
+    }
+    for (int d = 0; d < dec.ndom; ++d)
+        if (!errors[d].empty()) throw Error(errors[d] + " (subdomain " + std::to_string(d) + ")");
+
+    // subdomain right-hand sides: caller DOF value divided by its multiplicity
+    for (int d = 0; d < dec.ndom; ++d) {
+        SubPrep &S = out.sub[d];
+        const DomainRows &D = dec.dom[d];
+        for (int a = 0; a < (int)D.nodes.size(); ++a)
+            for (int c = 0; c < dpn; ++c) {
+                int dof = dec.node_dof[(size_t)D.nodes[a] * dpn + c];
+                double v = (dof >= 0 && dof < (int)rhs.size()) ? rhs[dof] : 0.0;
+                S.f[dpn * a + c] = v / dec.node_ndom[D.nodes[a]];
+            }
+    }
+    out.t_factor = now_s() - t0;
+
+    // coarse problem: kernel offsets, owners of every multiplier, GG^T and its inverse
+    double t1 = now_s();
+    out.kofs.assign(dec.ndom + 1, 0);
+    for (int d = 0; d < dec.ndom; ++d) out.kofs[d + 1] = out.kofs[d] + out.sub[d].nk;
+    out.n_kern = out.kofs[dec.ndom];
+    out.own_dom.assign((size_t)2 * dec.n_lambda, -1);
+    out.own_row.assign((size_t)2 * dec.n_lambda, -1);
+    for (int d = 0; d < dec.ndom; ++d)
+        for (int r = 0; r < (int)dec.dom[d].lam.size(); ++r) {
+            int l = dec.dom[d].lam[r];
+            int slot = out.own_dom[2 * (size_t)l] < 0 ? 0 : 1;
+            FETI_CHECK(out.own_dom[2 * (size_t)l + slot] < 0, "FETI4I: a multiplier is shared by more than two subdomains");
+            out.own_dom[2 * (size_t)l + slot] = d;
+            out.own_row[2 * (size_t)l + slot] = r;
+        }
+    const int nK = out.n_kern;
+    std::vector<double> GG((size_t)nK * nK, 0.0);
+    for (int l = 0; l < dec.n_lambda; ++l) {
+        for (int s1 = 0; s1 < 2; ++s1) {
+            int d1 = out.own_dom[2 * (size_t)l + s1];
+            if (d1 < 0) continue;
+            int r1 = out.own_row[2 * (size_t)l + s1];
+            const SubPrep &A1 = out.sub[d1];
+            for (int s2 = 0; s2 < 2; ++s2) {
+                int d2 = out.own_dom[2 * (size_t)l + s2];
+                if (d2 < 0) continue;
+                int r2 = out.own_row[2 * (size_t)l + s2];
+                const SubPrep &A2 = out.sub[d2];
+                for (int a = 0; a < A1.nk; ++a)
+                    for (int b = 0; b < A2.nk; ++b)
+                        GG[(size_t)(out.kofs[d2] + b) * nK + out.kofs[d1] + a] +=
+                            A1.G[(size_t)a * A1.ni + r1] * A2.G[(size_t)b * A2.ni + r2];
+            }
+        }
+    }
+    int info = dense::potrf_lower(GG.data(), nK, nK, nK);
+    FETI_CHECK(info == 0, "FETI4I: the coarse problem G G^T is singular");
+    std::vector<double> Wc((size_t)nK * nK, 0.0);
+    for (int j = 0; j < nK; ++j)
+        for (int i = j; i < nK; ++i) Wc[(size_t)j * nK + i] = GG[(size_t)j * nK + i];
+    dense::trtri_lower(Wc.data(), nK, nK);
+    out.GGt_inv.assign((size_t)nK * nK, 0.0);
+    dense::lauum_lower(Wc.data(), nK, nK, out.GGt_inv.data(), nK);
+    out.t_coarse = now_s() - t1;
+}
+
+void make_rhs_vectors(const Decomposition &dec, const Prep &prep, std::vector<double> &b, std::vector<double> &e) {
+    b.assign(dec.n_lambda, 0.0);
+    e.assign(prep.n_kern, 0.0);
+    const int nd = dec.ndom;
+    std::vector<std::vector<double>> kf(nd);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int d = 0; d < nd; ++d) {
+        const SubPrep &S = prep.sub[d];
+        kf[d] = S.f;
+        S.kplus(kf[d].data());
+        for (int k = 0; k < S.nk; ++k) {
+            double s = 0.0;
+            for (int i = 0; i < S.n; ++i) s += S.R[(size_t)k * S.n + i] * S.f[i];
+            e[prep.kofs[d] + k] = -s;
+        }
+    }
+    for (int d = 0; d < nd; ++d) {
+        const DomainRows &D = dec.dom[d];
+        for (size_t r = 0; r < D.lam.size(); ++r) b[D.lam[r]] += D.sign[r] * kf[d][D.dof[r]] - D.c[r];
+    }
+}
+
+void primal_solution(const Decomposition &dec, const Prep &prep, const double *lambda, const double *alpha,
+                     double *solution, int solution_size) {
+    const int dpn = dec.dpn;
+    const int nd = dec.ndom;
+    std::vector<std::vector<double>> u(nd);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int d = 0; d < nd; ++d) {
+        const SubPrep &S = prep.sub[d];
+        const DomainRows &D = dec.dom[d];
+        u[d] = S.f;
+        for (size_t r = 0; r < D.lam.size(); ++r) u[d][D.dof[r]] -= D.sign[r] * lambda[D.lam[r]];
+        S.kplus(u[d].data());
+        for (int k = 0; k < S.nk; ++k) {
+            double a = alpha[prep.kofs[d] + k];
+            for (int i = 0; i < S.n; ++i) u[d][i] += S.R[(size_t)k * S.n + i] * a;
+        }
+    }
+    std::vector<double> cnt(solution_size, 0.0);
+    for (int i = 0; i < solution_size; ++i) solution[i] = 0.0;
+    for (int d = 0; d < nd; ++d) {
+        const DomainRows &D = dec.dom[d];
+        for (int a = 0; a < (int)D.nodes.size(); ++a)
+            for (int c = 0; c < dpn; ++c) {
+                int dof = dec.node_dof[(size_t)D.nodes[a] * dpn + c];
+                if (dof < 0 || dof >= solution_size) continue;
+                solution[dof] += u[d][dpn * a + c];
+                cnt[dof] += 1.0;
+            }
+    }
+    for (int i = 0; i < solution_size; ++i)
+        if (cnt[i] > 0) solution[i] /= cnt[i];
+}
+
+}  // namespace feti

@@ -1,0 +1,68 @@
+// Host preprocessing of one Total-FETI problem: subdomain factorisations,
+// algebraic kernels, explicit Schur complements, preconditioner data and the
+// coarse problem.  Timed separately from the GPU dual iteration.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "decompose.h"
+
+namespace feti {
+
+enum Precond { PREC_NONE = 0, PREC_LUMPED = 1, PREC_WEIGHT = 2, PREC_DIRICHLET = 3 };
+
+struct SubPrep {
+    int n = 0;              // local DOFs
+    int ni = 0;             // local multipliers (rows of B_i)
+    int nk = 0;             // kernel dimension (defect)
+    int t = 0;              // touched DOFs (columns of B_i, fix DOFs included)
+    std::vector<int> pos;   // local DOF -> factor position
+    std::vector<int> tdof;  // T index -> local DOF (factor order of the tail)
+    std::vector<int> trow;  // local multiplier row -> T index
+    std::vector<double> Lp; // packed lower Cholesky factor of K_reg (factor order)
+    std::vector<double> R;  // n x nk, local DOF order, orthonormal columns
+    std::vector<double> S;  // ni x ni, column-major, B K_reg^-1 B^T
+    std::vector<double> Sdir;  // t x t Schur complement of K onto T (Dirichlet preconditioner)
+    std::vector<int> KT_ptr, KT_col;  // K restricted to T (lumped preconditioner), CSR in T order
+    std::vector<double> KT_val;
+    std::vector<double> f;  // subdomain right-hand side
+    std::vector<double> G;  // nk x ni, row-major: G_i = -(B_i R_i)^T
+    std::vector<int> fix_nodes;
+    double kernel_residual = 0.0;  // ||K R||_F / (||K||_F) check of the detected kernel
+    std::vector<double> ss_eigs;   // eigenvalues of the fix-DOF Schur block
+
+    // x := K_reg^{-1} x (local DOF order)
+    void kplus(double *x) const;
+};
+
+struct Prep {
+    std::vector<SubPrep> sub;
+    int n_lambda = 0;
+    int n_kern = 0;
+    std::vector<int> kofs;          // kernel offset per subdomain
+    std::vector<double> GGt_inv;    // n_kern x n_kern, dense symmetric inverse
+    std::vector<int> lam_owner;     // 2 per multiplier: (domain, row) packed as domain*2^20+row? (see owners)
+    std::vector<int> own_dom, own_row;  // 2 entries per multiplier, -1 if absent
+    double t_factor = 0.0, t_coarse = 0.0;
+};
+
+struct PrepOptions {
+    int precond = PREC_DIRICHLET;
+    bool scaling = true;
+    bool keep_dirichlet = false;
+    int threads = 0;
+};
+
+// rhs: caller DOF vector (size >= max DOF + 1); split per subdomain by multiplicity.
+void preprocess(const ElementData &el, Decomposition &dec, const std::vector<double> &rhs, const PrepOptions &opt,
+                Prep &out);
+
+// Right-hand-side dependent vectors: b = sum_i B_i K_i^+ f_i - c (lambda space), e = -R^T f.
+void make_rhs_vectors(const Decomposition &dec, const Prep &prep, std::vector<double> &b, std::vector<double> &e);
+
+// Primal recovery u_i = K_i^+ (f_i - B_i^T lambda) + R_i alpha_i, merged to caller DOFs (averaged).
+void primal_solution(const Decomposition &dec, const Prep &prep, const double *lambda, const double *alpha,
+                     double *solution, int solution_size);
+
+}  // namespace feti

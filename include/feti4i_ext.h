@@ -1,0 +1,102 @@
+/*
+ * Extensions of the FETI4I interface for the B200 dual solver.
+ *
+ * All of these are additive: none changes a reference signature.  Options
+ * the reference keeps in its ECF configuration (src/config/ecf/solver/feti.h)
+ * but does not expose through FETI4I (schur precision, scaling, ...) are set
+ * here; data the reference computes with METIS inside API::load (the
+ * subdomain partition, src/input/api/api.cpp:106) is supplied by the caller.
+ */
+#ifndef FETI4I_EXT_H_
+#define FETI4I_EXT_H_
+
+#include "feti4i.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Message of the last failing FETI4I call of this thread ("" if none); the
+ * reference prints and calls exit() instead (src/basis/logging/logging.cpp:103-131). */
+const char *FETI4IGetLastError(void);
+
+/* Element -> subdomain map (size = number of added elements); replaces the
+ * METIS partition of API::load (src/input/api/api.cpp:106).  Without it the
+ * elements are split into FETI4I_SUBDOMAINS contiguous blocks. */
+void FETI4ISetSubdomainPartition(FETI4IMatrix matrix, FETI4IInt size, FETI4IInt *elem2sub);
+
+/* Batched FETI4IAddElement (src/app/apiwrapper/wrapper.cpp:140-165): nelems
+ * elements with the same node/DOF counts, arrays laid out element after element. */
+void FETI4IAddElements(FETI4IMatrix matrix, FETI4IInt type, FETI4IInt nelems, FETI4IInt nodesSize, FETI4IInt *nodes,
+                       FETI4IInt dofsSize, FETI4IInt *dofs, FETI4IReal *values);
+
+/* Extended options, read by FETI4ICreateInstance (process-wide, like the
+ * reference's global ECF configuration). */
+typedef enum {
+    FETI4I_EXT_SCHUR_PRECISION,  /* 0 FP64 (reference DOUBLE), 1 FP32 (reference SINGLE), 2 BF16 + per-tile scale */
+    FETI4I_EXT_SCALING,          /* 1: K-diagonal B1 scaling (reference default), 0: 1/multiplicity */
+    FETI4I_EXT_HOST_ONLY,        /* 1: run the host preprocessing only (no GPU; FETI4ISolve fails) */
+    FETI4I_EXT_TILES_PER_ITEM,   /* work-queue granularity of the Schur SYMV (autotuned default 48) */
+    FETI4I_EXT_GRAPH_CHUNK,      /* PCG iterations per captured CUDA graph (default 16) */
+    FETI4I_EXT_RELIABLE_DELTA,   /* mixed precision: residual replacement threshold (default 0.1) */
+    FETI4I_EXT_HOST_THREADS,     /* OpenMP threads of the preprocessing (0: all) */
+    FETI4I_EXT_OPTIONS_SIZE
+} FETI4IExtOptions;
+void FETI4ISetExtendedOption(FETI4IInt key, FETI4IReal value);
+
+/* Statistics of an instance (indices of FETI4IStatIndex). */
+typedef enum {
+    FETI4I_STAT_ITERATIONS,
+    FETI4I_STAT_CONVERGED,
+    FETI4I_STAT_DUAL_SIZE,
+    FETI4I_STAT_KERNEL_SIZE,
+    FETI4I_STAT_SUBDOMAINS,
+    FETI4I_STAT_PREP_SECONDS,       /* host factorisation + Schur assembly */
+    FETI4I_STAT_UPLOAD_SECONDS,
+    FETI4I_STAT_SOLVE_MS,           /* device time of the dual PCG */
+    FETI4I_STAT_SOLVE_WALL_MS,      /* wall time of the last FETI4ISolve */
+    FETI4I_STAT_FAPPLY_BYTES,       /* algorithmic bytes of one F apply (iteration precision) */
+    FETI4I_STAT_REPLACEMENTS,
+    FETI4I_STAT_KERNEL_LAUNCHES,
+    FETI4I_STAT_DEVICE_BYTES,
+    FETI4I_STAT_FINAL_NORM,
+    FETI4I_STAT_TOLERANCE,
+    FETI4I_STAT_SIZE
+} FETI4IStatIndex;
+void FETI4IGetStats(FETI4IInstance instance, FETI4IInt size, FETI4IReal *stats);
+
+/* Dual solution lambda (dual size) and rigid-body amplitudes (kernel size) of the last solve. */
+void FETI4IGetDualSolution(FETI4IInstance instance, FETI4IReal *lambda, FETI4IReal *amplitudes);
+
+/* Introspection of the preprocessing (host data; used by the parity tests). */
+/* info: [ndofs, rows of B_i, kernel dimension, touched DOFs] */
+void FETI4IGetSubdomainInfo(FETI4IInstance instance, FETI4IInt subdomain, FETI4IInt *info);
+/* per local multiplier: global index, local DOF, sign, B1 scale, Dirichlet value */
+void FETI4IGetSubdomainMultipliers(FETI4IInstance instance, FETI4IInt subdomain, FETI4IInt *lambda, FETI4IInt *dof,
+                                   FETI4IReal *sign, FETI4IReal *weight, FETI4IReal *c);
+/* local node -> caller node */
+void FETI4IGetSubdomainNodes(FETI4IInstance instance, FETI4IInt subdomain, FETI4IInt *nodes);
+/* S_i = B_i K_i^+ B_i^T, rows x rows column-major */
+void FETI4IGetSubdomainSchur(FETI4IInstance instance, FETI4IInt subdomain, FETI4IReal *S);
+/* kernel basis R_i, ndofs x kernel column-major */
+void FETI4IGetSubdomainKernel(FETI4IInstance instance, FETI4IInt subdomain, FETI4IReal *R);
+/* x := K_reg^-1 x for one subdomain (host factor; local DOF order) */
+void FETI4IApplySubdomainKplus(FETI4IInstance instance, FETI4IInt subdomain, FETI4IReal *x);
+/* b (dual size) and e (kernel size) of the current right-hand side */
+void FETI4IGetDualRhs(FETI4IInstance instance, FETI4IReal *b, FETI4IReal *e);
+
+/* y = F x on the GPU with the Schur complements in the given precision (0/1/2). */
+void FETI4IApplyDualOperator(FETI4IInstance instance, FETI4IInt precision, FETI4IReal *x, FETI4IReal *y);
+/* Average device time in ms of one F apply over `reps` launches (inputs resident). */
+FETI4IReal FETI4ITimeDualOperator(FETI4IInstance instance, FETI4IInt precision, FETI4IInt reps);
+/* Solve on device-resident data only (right-hand side already uploaded by a
+ * previous FETI4ISolve): returns the device time in ms of the dual PCG. */
+FETI4IReal FETI4ISolveResident(FETI4IInstance instance);
+/* Select the operator precision of the following solves (must have been prepared). */
+void FETI4ISetSolvePrecision(FETI4IInstance instance, FETI4IInt precision);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FETI4I_EXT_H_ */

@@ -1,0 +1,135 @@
+"""GPU parity: the sm_100a dual iteration (through the FETI4I C ABI) against the oracle.
+
+Tolerances:
+  * F apply, FP64 tiles: 1e-13 relative to the oracle's F with the same S_i
+    (re-association of the FP64 sums only);
+  * F apply, FP32 tiles: 1e-6; BF16 tiles with per-tile scale: 1e-2 (storage precision);
+  * solves: displacements within 1e-8 relative of the oracle's FP64 solve and of
+    a direct solve, for FP64 and for FP32 storage inside
+    FP64 residual replacement.
+"""
+import numpy as np
+import pytest
+
+from espreso_b200 import feti4i as F
+from espreso_b200 import problems
+from oracle import feti as OF
+
+from helpers import direct_u, oracle_problem, with_library_operators
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_instance(P, prec=F.PREC_LUMPED, precision=1e-10, schur=F.FP64, max_it=1000):
+    return problems.make_instance(P, iopts={F.PRECONDITIONER: prec, F.VERBOSE_LEVEL: 0, F.MAX_ITERATIONS: max_it},
+                                  ropts={F.PRECISION: precision}, ext={F.EXT_SCHUR_PRECISION: schur})
+
+
+@pytest.fixture(scope="module")
+def elast():
+    return problems.elasticity_cube(domains=(3, 3, 2), elements=(4, 4, 4))
+
+
+@pytest.fixture(scope="module")
+def heat():
+    return problems.heat_cube(domains=(4, 3, 3), elements=(5, 5, 5), seed=1)
+
+
+@pytest.mark.parametrize("schur,tol", [(F.FP64, 1e-13), (F.FP32, 1e-6), (F.BF16, 2e-2)])
+def test_fapply_parity(elast, schur, tol):
+    inst = gpu_instance(elast, schur=schur)
+    OP = with_library_operators(oracle_problem(elast), inst)
+    rng = np.random.default_rng(1)
+    for _ in range(3):
+        x = rng.standard_normal(OP.n_lambda)
+        ref = OP.apply_F(x)
+        got = inst.apply_F(x, schur)
+        assert np.linalg.norm(got - ref) <= tol * np.linalg.norm(ref)
+    if schur == F.FP32:
+        ref32 = OP.apply_F(x, "f32")
+        assert np.linalg.norm(inst.apply_F(x, schur) - ref32) <= 1e-6 * np.linalg.norm(ref32)
+    inst.destroy()
+
+
+def test_fapply_edge_sizes():
+    """Subdomains whose interface sizes are not multiples of the 32-row tile,
+    single-tile subdomains and a large multi-item subdomain."""
+    P = problems.elasticity_cube(domains=(2, 1, 1), elements=(1, 1, 1))
+    inst = gpu_instance(P)
+    OP = with_library_operators(oracle_problem(P), inst)
+    x = np.random.default_rng(2).standard_normal(OP.n_lambda)
+    np.testing.assert_allclose(inst.apply_F(x), OP.apply_F(x), rtol=1e-12, atol=1e-12 * np.abs(OP.apply_F(x)).max())
+    inst.destroy()
+    P = problems.elasticity_cube(domains=(2, 2, 1), elements=(9, 9, 9))
+    from espreso_b200.feti4i import EXT_TILES_PER_ITEM, set_extended
+    set_extended(EXT_TILES_PER_ITEM, 7)
+    try:
+        inst = gpu_instance(P)
+    finally:
+        set_extended(EXT_TILES_PER_ITEM, 48)
+    OP = with_library_operators(oracle_problem(P), inst)
+    x = np.random.default_rng(3).standard_normal(OP.n_lambda)
+    ref = OP.apply_F(x)
+    assert np.linalg.norm(inst.apply_F(x) - ref) <= 1e-13 * np.linalg.norm(ref)
+    inst.destroy()
+
+
+@pytest.mark.parametrize("prec", [OF.PREC_NONE, OF.PREC_LUMPED, OF.PREC_WEIGHT, OF.PREC_DIRICHLET])
+def test_solve_elasticity(elast, prec):
+    inst = gpu_instance(elast, prec=prec)
+    sol = inst.solve()
+    st = inst.stats()
+    assert st["converged"] == 1.0
+    OP = oracle_problem(elast, dirichlet_prec=True)
+    OP.solve(precision=1e-10, prec=prec)
+    u_or = OP.merge(OP.primal(), elast.n_nodes)
+    u = sol.reshape(-1, 3)
+    assert np.linalg.norm(u - u_or) <= 1e-8 * np.linalg.norm(u_or)
+    ud = direct_u(elast)
+    assert np.linalg.norm(u - ud) <= 1e-8 * np.linalg.norm(ud)
+    # same operator -> same PCG trajectory as the oracle driven by the library's S_i
+    LP = with_library_operators(oracle_problem(elast, dirichlet_prec=True), inst)
+    lam_ref = LP.solve(precision=1e-10, prec=prec)
+    lam, _ = inst.dual_solution()
+    assert abs(LP.iterations - st["iterations"]) <= 1
+    assert np.linalg.norm(lam - lam_ref) <= 1e-7 * np.linalg.norm(lam_ref)
+    inst.destroy()
+
+
+def test_solve_heat_dirichlet(heat):
+    inst = gpu_instance(heat, prec=F.PREC_DIRICHLET)
+    u = inst.solve().reshape(-1, 1)
+    ud = direct_u(heat)
+    assert np.linalg.norm(u - ud) <= 1e-8 * np.linalg.norm(ud)
+    inst.destroy()
+
+
+@pytest.mark.parametrize("schur", [F.FP32, F.BF16])
+def test_mixed_precision_reaches_fp64_accuracy(heat, schur):
+    inst = gpu_instance(heat, prec=F.PREC_LUMPED, schur=schur, precision=1e-10, max_it=3000)
+    u = inst.solve().reshape(-1, 1)
+    st = inst.stats()
+    assert st["converged"] == 1.0
+    assert st["replacements"] >= 1
+    ud = direct_u(heat)
+    assert np.linalg.norm(u - ud) <= 1e-8 * np.linalg.norm(ud)
+    inst.destroy()
+
+
+def test_resolve_after_rhs_update(elast):
+    inst = gpu_instance(elast, prec=F.PREC_DIRICHLET)
+    u1 = inst.solve()
+    inst.update_rhs(-3.0 * elast.rhs())
+    u2 = inst.solve()
+    assert np.linalg.norm(u2 + 3.0 * u1) <= 1e-8 * np.linalg.norm(u2)
+    ms = inst.solve_resident()
+    assert ms > 0
+    inst.destroy()
+
+
+def test_max_iterations_stop(elast):
+    inst = gpu_instance(elast, prec=F.PREC_NONE, max_it=5)
+    inst.solve()
+    st = inst.stats()
+    assert st["converged"] == 0.0 and st["iterations"] == 5
+    inst.destroy()
