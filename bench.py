@@ -248,7 +248,6 @@ def run_ours(args):
         if key in tj:
             traffic = tj[key]["dram_bytes_per_launch"]
     fp64_f = inst.time_F(0, 10)
-    alg64 = inst.stats() and None
     # CPU baseline: oracle port on the host cores (rank 0, N=1 only)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -270,8 +269,8 @@ def run_ours(args):
         "fp64_gpu": {"ms": fp64_ms, "pcg_iterations": int(st64["iterations"]), "speedup_mixed": fp64_ms / step_ms,
                      "fapply_ms": fp64_f},
         "solves_per_s": world * 1e3 / step_ms,
-        "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 8 * (NL + nK),
-                "d2h_bytes_per_step": 8 * (NL + nK)},
+        "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": int(rhs.nbytes),
+                "d2h_bytes_per_step": int(sol.nbytes)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "kernel": "tile_symv_kernel", "launch_ms": t_f, "peak_kind": peak_kind,
                      "alg_bytes_per_launch": alg},
@@ -301,7 +300,6 @@ def cpu_baseline_from_library(inst, P, args):
         OP.coords = P.coords
         OP.n_lambda = num.n_lambda
         OP.sub = []
-        diags = None
         for d in range(num.ndomains):
             s = OF.Subdomain(K=None, f=None, R=inst.kernel(d), regmat=None, chol=None, lam=num.B[d]["lam"],
                              dof=num.B[d]["dof"], sign=num.B[d]["sign"], c=num.B[d]["c"], w=None)

@@ -260,10 +260,15 @@ void FETI4ISolve(FETI4IInstance instance, FETI4IInt solution_size, FETI4IReal *s
     guarded([&] {
         auto *I = check_instance(instance);
         FETI_CHECK(solution_size >= 0 && (solution_size == 0 || solution), "FETI4I: invalid solution array");
+        FETI_CHECK(I->gpu, "FETI4I: instance was created with FETI4I_EXT_HOST_ONLY; no device solver");
         double t0 = now_s();
-        solve_instance(I);
-        primal_solution(I->dec, I->prep, I->lambda.data(), I->alpha.data(), solution, solution_size);
+        I->gpu->solve_full(I->rhs.data(), (int)I->rhs.size(), solution, solution_size, I->stats, true);
+        I->rhs_on_device = true;
         I->t_solve_wall = (now_s() - t0) * 1e3;
+        I->lambda.clear();
+        FETI_LOG(1, "FETI4I: PCG %s after %d iterations (|w| %.3e, tol %.3e), %.3f ms on the device\n",
+                 I->stats.converged ? "converged" : "stopped", I->stats.iterations, I->stats.final_norm, I->stats.tol,
+                 I->stats.t_solve_ms);
     });
 }
 
@@ -273,6 +278,7 @@ FETI4IReal FETI4ISolveResident(FETI4IInstance instance) {
         auto *I = check_instance(instance);
         FETI_CHECK(I->gpu && I->rhs_on_device, "FETI4I: no right-hand side on the device (call FETI4ISolve first)");
         I->gpu->solve(I->stats);
+        I->lambda.clear();
         ms = I->stats.t_solve_ms;
     });
     return ms;
@@ -386,7 +392,8 @@ void FETI4IGetStats(FETI4IInstance instance, FETI4IInt size, FETI4IReal *stats) 
 void FETI4IGetDualSolution(FETI4IInstance instance, FETI4IReal *lambda, FETI4IReal *amplitudes) {
     guarded([&] {
         auto *I = check_instance(instance);
-        FETI_CHECK(!I->lambda.empty(), "FETI4I: no solution yet");
+        FETI_CHECK(I->gpu && I->rhs_on_device, "FETI4I: no solution yet");
+        if (I->lambda.empty()) I->gpu->get_solution(I->lambda, I->alpha);
         if (lambda) std::copy(I->lambda.begin(), I->lambda.end(), lambda);
         if (amplitudes) std::copy(I->alpha.begin(), I->alpha.end(), amplitudes);
     });

@@ -18,6 +18,7 @@
 #include <numeric>
 
 #include "common.h"
+#include "dense.h"
 #include "gpu_solver.h"
 
 #define CUDA_CHECK(x)                                                                              \
@@ -41,8 +42,8 @@ constexpr unsigned FULL = 0xffffffffu;
 struct DevState {
     int conv_iter;      // first iteration whose check passed, -1 while running
     int iter_base;      // iteration index of slot 0 of the current graph chunk
-    int replace_next;   // mixed precision: recompute the true residual before the next iteration
-    int r_true;         // the residual of the current iteration is a freshly recomputed one
+    int replace_iter;   // mixed precision: iteration that starts with r = b - F64 x (-1: none pending)
+    int true_iter;      // iteration whose starting residual was computed in FP64 from x
     int replacements;
     int max_it;
     int mixed;
@@ -55,28 +56,38 @@ struct DevState {
 };
 
 struct DevProblem {
-    int nd, NL, nK, NT;
+    int nd, NL, nK, NT, KS;     // KS: row stride of the G coefficient arrays (max kernel dimension)
     const int *loff;        // nd+1
     const int *kof;         // nd+1 kernel offsets
     const int *toff;        // nd+1 T-space offsets
     const int *partner;     // NL: row of the other owner, -1
     const int *tidx;        // NL: global T index of the row's DOF
+    const int *ptidx;       // NL: T index of the partner row, -1
     const double *ws;       // NL: B1 weight * sign
+    const double *pws;      // NL: partner's weight * sign, 0
     const double *minv;     // NL: 1 / multiplicity
-    const double *Gl;       // NL*KMAX: G coefficients of the row
-    const int *rkof;        // NL: kernel offset of the row's subdomain
-    const int *rnk;         // NL: kernel dimension of the row's subdomain
+    const double *Gl;       // NL*KS: G coefficients of the row
+    const double *Gp;       // NL*KS: G coefficients of the partner row
+    const int *rkof, *rnk;  // NL: kernel offset / dimension of the row's subdomain
+    const int *pkof, *pnk;  // NL: same for the partner's subdomain (pnk = 0 without partner)
     const int *trow_ptr;    // NT+1
     const int *trow_idx;    // rows of each T index
-    const int *kt_ptr;      // NT+1 lumped: K restricted to T (global T columns)
-    const int *kt_col;
-    const double *kt_val;
+    const int *slice0;      // nd+1: lumped K_TT in sliced ELL (32 T rows per slice)
+    const int *ell_ptr;     // per slice: offset of its column-major block
+    const int *ell_w;       // per slice: width
+    const unsigned short *ell_col;  // column (T index inside the subdomain)
+    const double *ell_val;
     const double *GGtinv;   // nK*nK
     const double *bL;       // NL replicated b
     double *x, *r, *w, *z, *y, *p, *Ap, *uT, *vT, *d, *alpha;
     double *part_w, *part_rho, *part_b, *rho_hist;
+    double *scal;           // grid totals (SC_*)
+    int *done;              // completion counters of the last-CTA reductions (DONE_*)
     DevState *st;
 };
+
+enum { SC_RHO = 0, SC_PAP = 1, SC_WN2 = 2, SC_BN2 = 3, SC_PN2 = 4, SC_COUNT = 8 };
+enum { DONE_W = 0, DONE_RHO = 1, DONE_B = 2, DONE_PN = 3, DONE_COUNT = 8 };
 
 struct TileSetDev {
     int nitems;
@@ -131,12 +142,6 @@ __device__ void block_sum_k(double (&v)[KMAX], double *sh /* >= 32*KMAX */) {
     __syncthreads();
 }
 
-// sum of an array of partials in a fixed order (same value in every CTA)
-__device__ double array_sum(const double *a, int n, double *sh) {
-    double s = 0.0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) s += a[i];
-    return block_sum(s, sh);
-}
 
 __device__ __forceinline__ bool skip_iter(const DevState *st, int iter) {
     int c = st->conv_iter;
@@ -146,15 +151,53 @@ __device__ __forceinline__ bool skip_iter(const DevState *st, int iter) {
 // (G^T a) at local row e: own coefficients plus the partner's
 __device__ __forceinline__ double gt_alpha(const DevProblem &P, int e, const double *a) {
     double s = 0.0;
-    int nk = P.rnk[e], ko = P.rkof[e];
-    for (int k = 0; k < nk; ++k) s += P.Gl[(size_t)e * KMAX + k] * a[ko + k];
-    int q = P.partner[e];
-    if (q >= 0) {
-        nk = P.rnk[q];
-        ko = P.rkof[q];
-        for (int k = 0; k < nk; ++k) s += P.Gl[(size_t)q * KMAX + k] * a[ko + k];
-    }
+    const int nk = P.rnk[e], ko = P.rkof[e], pn = P.pnk[e], po = P.pkof[e];
+    const double *g = P.Gl + (size_t)e * P.KS, *gp = P.Gp + (size_t)e * P.KS;
+    for (int k = 0; k < nk; ++k) s += g[k] * a[ko + k];
+    for (int k = 0; k < pn; ++k) s += gp[k] * a[po + k];
     return s;
+}
+
+// Every CTA contributes v (valid in thread 0); the last CTA to arrive adds the
+// partials in index order and stores the total.  No CTA waits for another.
+__device__ void grid_total(double v, double *partials, int *counter, double *out, double *sh) {
+    __shared__ int s_last;
+    __syncthreads();  // s_last may still be read from a previous call
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = v;
+        __threadfence();
+        s_last = (atomicAdd(counter, 1) == (int)gridDim.x - 1);
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        double t = 0.0;
+        for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) t += __ldcg(&partials[i]);
+        t = block_sum(t, sh);
+        if (threadIdx.x == 0) {
+            *out = t;
+            *counter = 0;
+        }
+    }
+}
+
+// G_i v over the rows [e0, e1) of one subdomain, written to d[kof..]
+__device__ void g_dot(const DevProblem &P, int dsub, const double *v, double *sh) {
+    const int e0 = P.loff[dsub], e1 = P.loff[dsub + 1];
+    const int nk = P.kof[dsub + 1] - P.kof[dsub];
+    double gk[KMAX];
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k) gk[k] = 0.0;
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+        const double ve = v[e - e0];
+        const double *g = P.Gl + (size_t)e * P.KS;
+#pragma unroll
+        for (int k = 0; k < KMAX; ++k)
+            if (k < nk) gk[k] += g[k] * ve;
+    }
+    block_sum_k(gk, sh);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < nk; ++k) P.d[P.kof[dsub] + k] = gk[k];
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -231,6 +274,56 @@ __device__ __forceinline__ T reduce_scatter(T (&v)[M], int lane) {
     return v[0];
 }
 
+template <int CPR>
+__device__ __forceinline__ void load_tile(uint4 (&raw)[CPR], const uint4 *tiles, long long g, int lane) {
+    const uint4 *tp = tiles + (size_t)g * (TILE * CPR);
+#pragma unroll
+    for (int q = 0; q < CPR; ++q) raw[q] = ld_stream(tp + q * 32 + lane);
+}
+
+// one 32x32 tile: row sums into the running accumulator of tile row I, column
+// sums (off-diagonal tiles) straight into the shared y
+template <int PREC>
+__device__ __forceinline__ void tile_fma(const uint4 (&raw)[TILE / TileT<PREC>::EPC], const TileSetDev &ts, long long g,
+                                         const typename TileT<PREC>::Acc *xs, typename TileT<PREC>::Acc *ys, int lane,
+                                         int &curI, typename TileT<PREC>::Acc &racc) {
+    using Acc = typename TileT<PREC>::Acc;
+    constexpr int EPC = TileT<PREC>::EPC;
+    constexpr int CPR = TILE / EPC;
+    constexpr int LOG_CPR = (CPR == 16) ? 4 : (CPR == 8) ? 3 : 2;
+    const int cq = lane % CPR, h = lane / CPR;
+    const int idx = EPC * cq + h;
+    const unsigned ij = ts.tile_ij[g];
+    const int I = ij >> 16, J = ij & 0xffff;
+    const float sc = (PREC == SCHUR_BF16) ? ts.scale[g] : 1.0f;
+    Acc xc[EPC], xr[CPR], rs[CPR], cs[EPC];
+#pragma unroll
+    for (int j = 0; j < EPC; ++j) { xc[j] = xs[TILE * J + EPC * cq + j]; cs[j] = 0; }
+#pragma unroll
+    for (int q = 0; q < CPR; ++q) { xr[q] = xs[TILE * I + EPC * q + h]; rs[q] = 0; }
+#pragma unroll
+    for (int q = 0; q < CPR; ++q) {
+        Acc e[EPC];
+        unpack<PREC>(raw[q], e, sc);
+#pragma unroll
+        for (int j = 0; j < EPC; ++j) {
+            rs[q] += e[j] * xc[j];
+            cs[j] += e[j] * xr[q];
+        }
+    }
+    Acc rsum = reduce_scatter<CPR, 0>(rs, lane);
+    if (I != curI) {
+        if (curI >= 0) atomicAdd(&ys[TILE * curI + idx], racc);
+        curI = I;
+        racc = 0;
+    }
+    racc += rsum;
+    if (I != J) {
+        Acc csum = reduce_scatter<EPC, LOG_CPR>(cs, lane);
+        atomicAdd(&ys[TILE * J + idx], csum);
+    }
+}
+
 // MODE 0: x = src (outside the PCG loop)
 // MODE 1: x = src + beta * src2 with beta = rho_k / rho_{k-1} (PCG direction p = y + beta p)
 // MODE 2: x = src inside the PCG loop (skipped after convergence)
@@ -241,7 +334,6 @@ tile_symv_kernel(TileSetDev ts, DevProblem P, const double *src, const double *s
     using Acc = typename TileT<PREC>::Acc;
     constexpr int EPC = TileT<PREC>::EPC;
     constexpr int CPR = TILE / EPC;          // 16-byte chunks per tile row (= loads per lane)
-    constexpr int LOG_CPR = (CPR == 16) ? 4 : (CPR == 8) ? 3 : 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red[32];
     __shared__ int s_item;
@@ -250,17 +342,15 @@ tile_symv_kernel(TileSetDev ts, DevProblem P, const double *src, const double *s
     if (MODE != 0) {
         const int iter = P.st->iter_base + slot;
         if (skip_iter(P.st, iter)) return;
-        if (MODE == 3 && !P.st->replace_next) return;
+        if (MODE == 3 && P.st->replace_iter != iter) return;
         if (MODE == 1) {
-            double rho = array_sum(P.part_rho, P.nd, red);
-            if (threadIdx.x == 0) s_beta = (iter == 0) ? 0.0 : rho / P.rho_hist[iter - 1];
+            if (threadIdx.x == 0) s_beta = (iter == 0) ? 0.0 : P.scal[SC_RHO] / P.rho_hist[iter - 1];
             __syncthreads();
         }
     }
     const double beta = (MODE == 1) ? s_beta : 0.0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const int cq = lane % CPR, h = lane / CPR;
-    const int idx = EPC * cq + h;   // row/column handled by this lane after the reductions
+    const int idx = EPC * (lane % CPR) + lane / CPR;   // row/column of this lane after the reductions
 
     for (;;) {
         if (threadIdx.x == 0) s_item = atomicAdd(&ts.queue[0], 1);
@@ -285,40 +375,27 @@ tile_symv_kernel(TileSetDev ts, DevProblem P, const double *src, const double *s
         const uint4 *tiles = reinterpret_cast<const uint4 *>(ts.tiles);
         int curI = -1;
         Acc racc = 0;
-        for (int k = k0 + warp; k < k1; k += nw) {
-            const long long g = tbase + k;
-            const unsigned ij = ts.tile_ij[g];
-            const int I = ij >> 16, J = ij & 0xffff;
-            uint4 raw[CPR];
-            const uint4 *tp = tiles + (size_t)g * (TILE * CPR);
-#pragma unroll
-            for (int q = 0; q < CPR; ++q) raw[q] = ld_stream(tp + q * 32 + lane);
-            const float sc = (PREC == SCHUR_BF16) ? ts.scale[g] : 1.0f;
-            Acc xc[EPC], xr[CPR], rs[CPR], cs[EPC];
-#pragma unroll
-            for (int j = 0; j < EPC; ++j) { xc[j] = xs[TILE * J + EPC * cq + j]; cs[j] = 0; }
-#pragma unroll
-            for (int q = 0; q < CPR; ++q) { xr[q] = xs[TILE * I + EPC * q + h]; rs[q] = 0; }
-#pragma unroll
-            for (int q = 0; q < CPR; ++q) {
-                Acc e[EPC];
-                unpack<PREC>(raw[q], e, sc);
-#pragma unroll
-                for (int j = 0; j < EPC; ++j) {
-                    rs[q] += e[j] * xc[j];
-                    cs[j] += e[j] * xr[q];
-                }
+        int k = k0 + warp;
+        if (PREC == SCHUR_FP64) {
+            // 8 KB per tile and warp already keep enough bytes in flight
+            for (; k < k1; k += nw) {
+                uint4 raw[CPR];
+                load_tile<CPR>(raw, tiles, tbase + k, lane);
+                tile_fma<PREC>(raw, ts, tbase + k, xs, ys, lane, curI, racc);
             }
-            Acc rsum = reduce_scatter<CPR, 0>(rs, lane);
-            if (I != curI) {
-                if (curI >= 0) atomicAdd(&ys[TILE * curI + idx], racc);
-                curI = I;
-                racc = 0;
-            }
-            racc += rsum;
-            if (I != J) {
-                Acc csum = reduce_scatter<EPC, LOG_CPR>(cs, lane);
-                atomicAdd(&ys[TILE * J + idx], csum);
+        } else {
+            // software pipeline: the next tile of this warp is in flight while one is reduced
+            uint4 ra[CPR], rb[CPR];
+            if (k < k1) load_tile<CPR>(ra, tiles, tbase + k, lane);
+            for (;;) {
+                if (k >= k1) break;
+                if (k + nw < k1) load_tile<CPR>(rb, tiles, tbase + k + nw, lane);
+                tile_fma<PREC>(ra, ts, tbase + k, xs, ys, lane, curI, racc);
+                k += nw;
+                if (k >= k1) break;
+                if (k + nw < k1) load_tile<CPR>(ra, tiles, tbase + k + nw, lane);
+                tile_fma<PREC>(rb, ts, tbase + k, xs, ys, lane, curI, racc);
+                k += nw;
             }
         }
         if (curI >= 0) atomicAdd(&ys[TILE * curI + idx], racc);
@@ -337,12 +414,24 @@ tile_symv_kernel(TileSetDev ts, DevProblem P, const double *src, const double *s
         if (threadIdx.x == 0 && ts.item_dot) ts.item_dot[item] = dot;
         __syncthreads();
     }
-    // the last CTA to finish resets the work queue for the next launch
+    // the last CTA to finish resets the work queue for the next launch and, in
+    // the PCG loop, adds the item dot products p.Ap in item order
+    __shared__ int s_last;
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
-        int done = atomicAdd(&ts.queue[1], 1);
-        if (done == (int)gridDim.x - 1) {
+        s_last = (atomicAdd(&ts.queue[1], 1) == (int)gridDim.x - 1);
+    }
+    __syncthreads();
+    if (s_last) {
+        if (MODE == 1) {
+            __threadfence();
+            double t = 0.0;
+            for (int i = threadIdx.x; i < ts.nitems; i += blockDim.x) t += __ldcg(&ts.item_dot[i]);
+            t = block_sum(t, red);
+            if (threadIdx.x == 0) P.scal[SC_PAP] = t;
+        }
+        if (threadIdx.x == 0) {
             ts.queue[0] = 0;
             ts.queue[1] = 0;
             __threadfence();
@@ -378,38 +467,36 @@ __global__ void zero_kernel(double *v, int n) {
     if (i < n) v[i] = 0.0;
 }
 
-// r = b - assemble(Ap); d = G r per subdomain; ||b||^2 partials.  One CTA per subdomain.
+__global__ void zero2_kernel(double *a, double *b, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) { a[i] = 0.0; b[i] = 0.0; }
+}
+
+// r = b - assemble(Ax); d = G r per subdomain; ||b||^2 total (initial call).  One CTA per subdomain.
 __global__ void r0_kernel(DevProblem P, double *Ax, int replace_mode, int slot) {
+    extern __shared__ double rv_s[];
     __shared__ double sh[32 * KMAX];
     if (replace_mode) {
         const int iter = P.st->iter_base + slot;
-        if (skip_iter(P.st, iter) || !P.st->replace_next) return;
+        if (skip_iter(P.st, iter) || P.st->replace_iter != iter) return;
     }
     const int dsub = blockIdx.x;
     const int e0 = P.loff[dsub], e1 = P.loff[dsub + 1];
-    double gk[KMAX];
-#pragma unroll
-    for (int k = 0; k < KMAX; ++k) gk[k] = 0.0;
     double bb = 0.0;
     for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-        int q = P.partner[e];
-        double a = Ax[e] + (q >= 0 ? Ax[q] : 0.0);
-        double rv = P.bL[e] - a;
+        const int q = P.partner[e];
+        const double a = Ax[e] + (q >= 0 ? Ax[q] : 0.0);
+        const double rv = P.bL[e] - a;
         P.r[e] = rv;
+        rv_s[e - e0] = rv;
         bb += P.bL[e] * P.bL[e] * P.minv[e];
-#pragma unroll
-        for (int k = 0; k < KMAX; ++k) gk[k] += P.Gl[(size_t)e * KMAX + k] * rv;
     }
-    block_sum_k(gk, sh);
-    double bsum = block_sum(bb, sh);
-    if (threadIdx.x == 0) {
-        int nk = P.kof[dsub + 1] - P.kof[dsub];
-        for (int k = 0; k < nk; ++k) P.d[P.kof[dsub] + k] = gk[k];
-        if (!replace_mode) P.part_b[dsub] = bsum;
-    }
+    __syncthreads();
+    g_dot(P, dsub, rv_s, sh);
+    if (!replace_mode) grid_total(block_sum(bb, sh), P.part_b, P.done + DONE_B, P.scal + SC_BN2, sh);
 }
 
-// ||P r||^2 partials with alpha = (GG^T)^-1 G r  (initial stop tolerance)
+// ||P r||^2 with alpha = (GG^T)^-1 G r (initial stop tolerance)
 __global__ void pnorm_kernel(DevProblem P) {
     __shared__ double sh[32];
     const int dsub = blockIdx.x;
@@ -418,24 +505,20 @@ __global__ void pnorm_kernel(DevProblem P) {
         double u = P.r[e] - gt_alpha(P, e, P.alpha);
         s += u * u * P.minv[e];
     }
-    s = block_sum(s, sh);
-    if (threadIdx.x == 0) P.part_w[dsub] = s;
+    grid_total(block_sum(s, sh), P.part_w, P.done + DONE_PN, P.scal + SC_PN2, sh);
 }
 
 __global__ void tol_kernel(DevProblem P) {
-    __shared__ double sh[32];
-    double un = array_sum(P.part_w, P.nd, sh);
-    double bn = array_sum(P.part_b, P.nd, sh);
     if (threadIdx.x == 0) {
-        double tol = P.st->precision * fmin(sqrt(un), sqrt(bn));
-        P.st->tol = tol;
-        P.st->rmax = sqrt(un);
+        const double un = sqrt(P.scal[SC_PN2]), bn = sqrt(P.scal[SC_BN2]);
+        P.st->tol = P.st->precision * fmin(un, bn);
+        P.st->rmax = un;
     }
 }
 
-// w = r - G^T alpha, ||w||^2 partials, u_T = B^T (W w) and, for the lumped
-// preconditioner, v_T = K_TT u_T.  With no preconditioner y = w and the rho
-// partials are taken here.  One CTA per subdomain.
+// w = r - G^T alpha (||w||^2 total), u_T = B^T (W w) and, for the lumped
+// preconditioner, v_T = K_TT u_T (sliced ELL).  With no preconditioner y = w
+// and rho = y.w is taken here.  One CTA per subdomain.
 template <int PRECOND>
 __global__ void w_prec_kernel(DevProblem P, int slot) {
     extern __shared__ double sm[];
@@ -444,27 +527,28 @@ __global__ void w_prec_kernel(DevProblem P, int slot) {
     if (skip_iter(P.st, iter)) return;
     const int dsub = blockIdx.x;
     const int e0 = P.loff[dsub], e1 = P.loff[dsub + 1];
+    const int t0 = P.toff[dsub], t1 = P.toff[dsub + 1], nt = t1 - t0;
+    double *wsm = sm;              // w of the subdomain rows
+    double *u = sm + (e1 - e0);    // B^T W w on the touched DOFs
     double ww = 0.0;
     for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-        double wv = P.r[e] - gt_alpha(P, e, P.alpha);
+        const double wv = P.r[e] - gt_alpha(P, e, P.alpha);
         P.w[e] = wv;
+        wsm[e - e0] = wv;
         if (PRECOND == PREC_NONE) P.y[e] = wv;
         ww += wv * wv * P.minv[e];
     }
-    ww = block_sum(ww, sh);
-    if (threadIdx.x == 0) {
-        P.part_w[dsub] = ww;
-        if (PRECOND == PREC_NONE) P.part_rho[dsub] = ww;
+    ww = block_sum(ww, sh);  // also a barrier for wsm
+    grid_total(ww, P.part_w, P.done + DONE_W, P.scal + SC_WN2, sh);
+    if (PRECOND == PREC_NONE) {
+        grid_total(ww, P.part_rho, P.done + DONE_RHO, P.scal + SC_RHO, sh);
+        return;
     }
-    if (PRECOND == PREC_NONE) return;
-    __syncthreads();
-    const int t0 = P.toff[dsub], t1 = P.toff[dsub + 1], nt = t1 - t0;
-    double *u = sm;
     for (int t = threadIdx.x; t < nt; t += blockDim.x) {
         double s = 0.0;
         for (int j = P.trow_ptr[t0 + t]; j < P.trow_ptr[t0 + t + 1]; ++j) {
-            int e = P.trow_idx[j];
-            s += P.ws[e] * P.w[e];
+            const int e = P.trow_idx[j];
+            s += P.ws[e] * wsm[e - e0];
         }
         if (PRECOND == PREC_LUMPED) u[t] = s;
         else P.uT[t0 + t] = s;
@@ -472,52 +556,53 @@ __global__ void w_prec_kernel(DevProblem P, int slot) {
     }
     if (PRECOND != PREC_LUMPED) return;
     __syncthreads();
+    const int sl0 = P.slice0[dsub];
     for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+        const int sl = sl0 + (t >> 5), ln = t & 31;
+        const int base = P.ell_ptr[sl], wd = P.ell_w[sl];
         double s = 0.0;
-        for (int j = P.kt_ptr[t0 + t]; j < P.kt_ptr[t0 + t + 1]; ++j) s += P.kt_val[j] * u[P.kt_col[j] - t0];
+        for (int j = 0; j < wd; ++j) {
+            const int o = base + j * 32 + ln;
+            s += P.ell_val[o] * u[P.ell_col[o]];
+        }
         P.vT[t0 + t] = s;
     }
 }
 
 // z = assemble(W B v_T); d = G z.  One CTA per subdomain.
 __global__ void z_kernel(DevProblem P, int slot) {
+    extern __shared__ double zs[];
     __shared__ double sh[32 * KMAX];
     const int iter = P.st->iter_base + slot;
     if (skip_iter(P.st, iter)) return;
     const int dsub = blockIdx.x;
-    double gk[KMAX];
-#pragma unroll
-    for (int k = 0; k < KMAX; ++k) gk[k] = 0.0;
-    for (int e = P.loff[dsub] + threadIdx.x; e < P.loff[dsub + 1]; e += blockDim.x) {
+    const int e0 = P.loff[dsub], e1 = P.loff[dsub + 1];
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+        const int pt = P.ptidx[e];
         double zv = P.ws[e] * P.vT[P.tidx[e]];
-        int q = P.partner[e];
-        if (q >= 0) zv += P.ws[q] * P.vT[P.tidx[q]];
+        if (pt >= 0) zv += P.pws[e] * P.vT[pt];
         P.z[e] = zv;
-#pragma unroll
-        for (int k = 0; k < KMAX; ++k) gk[k] += P.Gl[(size_t)e * KMAX + k] * zv;
+        zs[e - e0] = zv;
     }
-    block_sum_k(gk, sh);
-    if (threadIdx.x == 0) {
-        int nk = P.kof[dsub + 1] - P.kof[dsub];
-        for (int k = 0; k < nk; ++k) P.d[P.kof[dsub] + k] = gk[k];
-    }
+    __syncthreads();
+    g_dot(P, dsub, zs, sh);
 }
 
-// y = z - G^T alpha, rho partials = y.w; zero the F-apply accumulator.
-__global__ void y_kernel(DevProblem P, int slot) {
+// y = z - G^T alpha, rho = y.w total; clear the F apply accumulators.
+__global__ void y_kernel(DevProblem P, double *Ax64, int slot) {
     __shared__ double sh[32];
     const int iter = P.st->iter_base + slot;
     if (skip_iter(P.st, iter)) return;
     const int dsub = blockIdx.x;
     double s = 0.0;
     for (int e = P.loff[dsub] + threadIdx.x; e < P.loff[dsub + 1]; e += blockDim.x) {
-        double yv = P.z[e] - gt_alpha(P, e, P.alpha);
+        const double yv = P.z[e] - gt_alpha(P, e, P.alpha);
         P.y[e] = yv;
         s += yv * P.w[e] * P.minv[e];
         P.Ap[e] = 0.0;
+        Ax64[e] = 0.0;
     }
-    s = block_sum(s, sh);
-    if (threadIdx.x == 0) P.part_rho[dsub] = s;
+    grid_total(block_sum(s, sh), P.part_rho, P.done + DONE_RHO, P.scal + SC_RHO, sh);
 }
 
 __global__ void zero_vT_kernel(DevProblem P, int slot) {
@@ -527,92 +612,234 @@ __global__ void zero_vT_kernel(DevProblem P, int slot) {
 }
 
 // p = y + beta p, x += alpha p, r -= alpha assemble(Ap), d = G r, convergence check.
-__global__ void update_kernel(DevProblem P, const double *item_dot, int nitems, int slot) {
+__global__ void update_kernel(DevProblem P, int slot) {
+    extern __shared__ double rs_s[];
     __shared__ double sh[32 * KMAX];
     const int iter = P.st->iter_base + slot;
     if (skip_iter(P.st, iter)) return;
-    const double rho = array_sum(P.part_rho, P.nd, sh);
-    const double pAp = array_sum(item_dot, nitems, sh);
-    const double wn2 = array_sum(P.part_w, P.nd, sh);
+    const double rho = P.scal[SC_RHO];
+    const double pAp = P.scal[SC_PAP];
+    const double wn2 = P.scal[SC_WN2];
     const double beta = (iter == 0) ? 0.0 : rho / P.rho_hist[iter - 1];
     const double alpha = rho / pAp;
     const int dsub = blockIdx.x;
-    double gk[KMAX];
-#pragma unroll
-    for (int k = 0; k < KMAX; ++k) gk[k] = 0.0;
-    for (int e = P.loff[dsub] + threadIdx.x; e < P.loff[dsub + 1]; e += blockDim.x) {
-        double pv = P.y[e] + beta * P.p[e];
+    const int e0 = P.loff[dsub], e1 = P.loff[dsub + 1];
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+        const double pv = P.y[e] + beta * P.p[e];
         P.p[e] = pv;
         P.x[e] += alpha * pv;
-        int q = P.partner[e];
-        double a = P.Ap[e] + (q >= 0 ? P.Ap[q] : 0.0);
-        double rv = P.r[e] - alpha * a;
+        const int q = P.partner[e];
+        const double a = P.Ap[e] + (q >= 0 ? P.Ap[q] : 0.0);
+        const double rv = P.r[e] - alpha * a;
         P.r[e] = rv;
-#pragma unroll
-        for (int k = 0; k < KMAX; ++k) gk[k] += P.Gl[(size_t)e * KMAX + k] * rv;
+        rs_s[e - e0] = rv;
     }
-    block_sum_k(gk, sh);
-    if (threadIdx.x == 0) {
-        int nk = P.kof[dsub + 1] - P.kof[dsub];
-        for (int k = 0; k < nk; ++k) P.d[P.kof[dsub] + k] = gk[k];
-    }
+    __syncthreads();
+    g_dot(P, dsub, rs_s, sh);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         DevState *st = P.st;
         P.rho_hist[iter] = rho;
-        double wn = sqrt(wn2);
+        const double wn = sqrt(wn2);
         st->last_norm = wn;
         if (!st->mixed) {
             if (wn < st->tol && st->conv_iter < 0) st->conv_iter = iter;
         } else {
-            // reliable updates: converge only on a recomputed residual, replace the
-            // iterated residual when it dropped by `delta` since the last replacement
+            // reliable updates (residual replacement): converge only on a residual
+            // recomputed in FP64, replace the iterated residual once it dropped by
+            // `delta` below the largest norm seen since the last replacement
+            const bool fresh = st->true_iter == iter;
+            st->rmax = fresh ? wn : fmax(st->rmax, wn);
+            bool replace = false;
             if (wn < st->tol) {
-                if (st->r_true) {
+                if (fresh) {
                     if (st->conv_iter < 0) st->conv_iter = iter;
                 } else {
-                    st->replace_next = 1;
+                    replace = true;
                 }
             } else if (wn < st->delta * st->rmax) {
-                st->replace_next = 1;
+                replace = true;
             }
-            st->r_true = 0;
+            if (replace) {
+                st->replace_iter = iter + 1;
+                st->true_iter = iter + 1;
+                st->replacements += 1;
+            }
         }
     }
-}
-
-// after a replacement r = b - F64 x: reset the reliable-update bookkeeping
-__global__ void replace_done_kernel(DevProblem P, int slot) {
-    const int iter = P.st->iter_base + slot;
-    if (skip_iter(P.st, iter)) return;
-    DevState *st = P.st;
-    if (!st->replace_next) return;
-    st->replace_next = 0;
-    st->r_true = 1;
-    st->replacements += 1;
-}
-
-// clear the F64 accumulator after a residual replacement consumed it
-__global__ void zero_cond_kernel(DevProblem P, double *v, int slot) {
-    const int iter = P.st->iter_base + slot;
-    if (skip_iter(P.st, iter) || !P.st->replace_next) return;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.NL; i += gridDim.x * blockDim.x) v[i] = 0.0;
 }
 
 __global__ void chunk_end_kernel(DevProblem P, int chunk) {
     if (threadIdx.x == 0 && blockIdx.x == 0) P.st->iter_base += chunk;
 }
 
-// rmax tracking for reliable updates: after the w norm of an iteration is known
-__global__ void rmax_kernel(DevProblem P, int slot) {
-    const int iter = P.st->iter_base + slot;
-    if (skip_iter(P.st, iter)) return;
-    __shared__ double sh[32];
-    double wn2 = array_sum(P.part_w, P.nd, sh);
-    if (threadIdx.x == 0) {
-        DevState *st = P.st;
-        double wn = sqrt(wn2);
-        if (st->r_true) st->rmax = wn;
-        else st->rmax = fmax(st->rmax, wn);
+
+
+// ---------------------------------------------------------------------------------------------
+// K^+ on the device: forward/backward substitution with the Cholesky factor of
+// K_reg (factor order), stored as 32x32 lower tiles (I >= J), block column by
+// block column.  One CTA per subdomain; diagonal blocks are solved by warp 0
+// with shuffles, off-diagonal blocks are applied by all warps.
+struct KplusDev {
+    int nd;
+    const int *n;            // DOFs per subdomain
+    const int *tn;           // 32-blocks per subdomain
+    const int *doff;         // local-DOF offsets (nd+1)
+    const long long *tile0;  // first tile of each subdomain
+    const int *pos;          // local DOF -> factor position (concatenated)
+    const double *L;         // tiles
+};
+
+__device__ __forceinline__ long long ltile(int T, int I, int J) {
+    return (long long)J * T - (long long)J * (J - 1) / 2 + (I - J);
+}
+
+__global__ void __launch_bounds__(256) kplus_kernel(KplusDev K, const double *in, double *out) {
+    extern __shared__ double v[];
+    __shared__ double part[8][32];
+    const int d = blockIdx.x;
+    const int n = K.n[d], T = K.tn[d], o = K.doff[d];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int *pos = K.pos + o;
+    const uint4 *tiles = reinterpret_cast<const uint4 *>(K.L) + (size_t)K.tile0[d] * (TILE * 16);
+    const double *dtiles = K.L + (size_t)K.tile0[d] * TILE * TILE;
+    for (int i = threadIdx.x; i < TILE * T; i += blockDim.x) v[i] = 0.0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) v[pos[i]] = in[o + i];
+    __syncthreads();
+    const int cq = lane % 16, h = lane / 16, idx = 2 * cq + h;
+    // forward: L y = f
+    for (int J = 0; J < T; ++J) {
+        if (warp == 0) {
+            const double *row = dtiles + (size_t)ltile(T, J, J) * TILE * TILE + lane * TILE;
+            double Lr[TILE];
+#pragma unroll
+            for (int k = 0; k < TILE; ++k) Lr[k] = row[k];
+            double vr = v[TILE * J + lane];
+#pragma unroll
+            for (int k = 0; k < TILE; ++k) {
+                double xk = __shfl_sync(FULL, vr / Lr[k], k);
+                if (lane == k) vr = xk;
+                else if (lane > k) vr -= Lr[k] * xk;
+            }
+            v[TILE * J + lane] = vr;
+        }
+        __syncthreads();
+        for (int I = J + 1 + warp; I < T; I += nw) {
+            const uint4 *tp = tiles + (size_t)ltile(T, I, J) * (TILE * 16);
+            double rs[16];
+            const double x0 = v[TILE * J + 2 * cq], x1 = v[TILE * J + 2 * cq + 1];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                uint4 u = ld_stream(tp + q * 32 + lane);
+                rs[q] = __hiloint2double(u.y, u.x) * x0 + __hiloint2double(u.w, u.z) * x1;
+            }
+            double r = reduce_scatter<16, 0>(rs, lane);
+            v[TILE * I + idx] -= r;
+        }
+        __syncthreads();
+    }
+    // backward: L^T x = y
+    for (int J = T - 1; J >= 0; --J) {
+        double cp = 0.0;
+        for (int I = J + 1 + warp; I < T; I += nw) {
+            const uint4 *tp = tiles + (size_t)ltile(T, I, J) * (TILE * 16);
+            double cs[2] = {0.0, 0.0};
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                uint4 u = ld_stream(tp + q * 32 + lane);
+                double xr = v[TILE * I + 2 * q + h];
+                cs[0] += __hiloint2double(u.y, u.x) * xr;
+                cs[1] += __hiloint2double(u.w, u.z) * xr;
+            }
+            cp += reduce_scatter<2, 4>(cs, lane);
+        }
+        part[warp][idx] = cp;
+        __syncthreads();
+        if (warp == 0) {
+            double vc = v[TILE * J + lane];
+            for (int w = 0; w < nw; ++w) vc -= part[w][lane];
+            const double *tile = dtiles + (size_t)ltile(T, J, J) * TILE * TILE;
+            double Lc[TILE];
+#pragma unroll
+            for (int k = 0; k < TILE; ++k) Lc[k] = tile[k * TILE + lane];
+#pragma unroll
+            for (int k = TILE - 1; k >= 0; --k) {
+                double xk = __shfl_sync(FULL, vc / Lc[k], k);
+                if (lane == k) vc = xk;
+                else if (lane < k) vc -= Lc[k] * xk;
+            }
+            v[TILE * J + lane] = vc;
+        }
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) out[o + i] = v[pos[i]];
+}
+
+// subdomain loads f_i = rhs(caller DOF) / multiplicity
+__global__ void split_rhs_kernel(const double *rhs, const int *gdof, const double *invm, double *f, int ntot) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < ntot) {
+        int g = gdof[i];
+        f[i] = g >= 0 ? rhs[g] * invm[i] : 0.0;
+    }
+}
+
+// e = -R^T f per subdomain
+__global__ void evec_kernel(DevProblem P, const int *doff, const int *rofs, const double *R, const double *f, double *e) {
+    __shared__ double sh[32 * KMAX];
+    const int d = blockIdx.x;
+    const int n = doff[d + 1] - doff[d], nk = P.kof[d + 1] - P.kof[d];
+    const double *Rd = R + rofs[d];
+    double acc[KMAX];
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k) acc[k] = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double fi = f[doff[d] + i];
+        for (int k = 0; k < nk; ++k) acc[k] += Rd[(size_t)k * n + i] * fi;
+    }
+    block_sum_k(acc, sh);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < nk; ++k) e[P.kof[d] + k] = -acc[k];
+}
+
+// b at every local row: own (s K^+ f)[dof] - c plus the partner's
+__global__ void bvec_kernel(DevProblem P, const int *rdof, const double *rsign, const double *rc, const double *kf,
+                            double *bL) {
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= P.NL) return;
+    double b = rsign[e] * kf[rdof[e]] - rc[e];
+    int q = P.partner[e];
+    if (q >= 0) b += rsign[q] * kf[rdof[q]] - rc[q];
+    bL[e] = b;
+}
+
+// g = f - B^T lambda (local DOF space), gathered through the touched-DOF rows
+__global__ void primal_rhs_kernel(DevProblem P, const int *tdof_g, const double *rsign, const double *f, double *g,
+                                  int ntot) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ntot; i += gridDim.x * blockDim.x) g[i] = f[i];
+}
+__global__ void primal_bt_kernel(DevProblem P, const int *tdof_g, const double *rsign, double *g) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.NT) return;
+    double s = 0.0;
+    for (int j = P.trow_ptr[t]; j < P.trow_ptr[t + 1]; ++j) {
+        int e = P.trow_idx[j];
+        s += rsign[e] * P.x[e];
+    }
+    g[tdof_g[t]] -= s;
+}
+
+// u += R alpha, merged into the caller's DOF vector (average over subdomains)
+__global__ void primal_merge_kernel(DevProblem P, const int *doff, const int *rofs, const double *R, const double *u,
+                                    const int *gdof, const double *invm, double *sol) {
+    const int d = blockIdx.x;
+    const int n = doff[d + 1] - doff[d], nk = P.kof[d + 1] - P.kof[d];
+    const double *Rd = R + rofs[d];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double val = u[doff[d] + i];
+        for (int k = 0; k < nk; ++k) val += Rd[(size_t)k * n + i] * P.alpha[P.kof[d] + k];
+        int g = gdof[doff[d] + i];
+        if (g >= 0) atomicAdd(&sol[g], val * invm[doff[d] + i]);
     }
 }
 
@@ -651,13 +878,21 @@ struct GpuSolver::Impl {
     DevProblem P{};
     DevState *st = nullptr;
     TileSetHost F64, Flow, Dir;
-    int max_tn = 0, max_tn_dir = 0, max_nt = 0;
+    int max_tn = 0, max_tn_dir = 0, max_nt = 0, max_ni = 0;
     std::vector<int> h_lam;       // L row -> lambda
     std::vector<int> h_loff;
     int n_lambda = 0;
     cudaGraphExec_t graph = nullptr;
     int graph_chunk = 0, graph_prec = -1, graph_precond = -1;
     double *Ax64 = nullptr;   // F apply output outside the iteration operator (initial, replacement, tests)
+    // device K^+ and the right-hand-side / primal vectors
+    KplusDev KP{};
+    int max_T = 0, ntot = 0, n_caller = 0;
+    int *d_doff = nullptr, *d_rofs = nullptr, *d_gdof = nullptr, *d_rdof = nullptr, *d_tdof_g = nullptr;
+    double *d_invm = nullptr, *d_R = nullptr, *d_rsign = nullptr, *d_rc = nullptr;
+    double *d_f = nullptr, *d_kf = nullptr, *d_g = nullptr, *d_rhs = nullptr, *d_sol = nullptr;
+    double *h_pinned = nullptr;
+    size_t h_pinned_n = 0;
     double *e_dev = nullptr;
     int rho_cap = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -678,6 +913,7 @@ struct GpuSolver::Impl {
         return p;
     }
     ~Impl() {
+        if (h_pinned) cudaFreeHost(h_pinned);
         if (graph) cudaGraphExecDestroy(graph);
         for (void *p : allocs) cudaFree(p);
         if (stream) cudaStreamDestroy(stream);
@@ -691,7 +927,100 @@ struct GpuSolver::Impl {
     void capture_chunk(int chunk);
     void launch_iteration(int slot);
     int kernels_per_iteration() const;
+    void upload_kplus(const Decomposition &dec, const Prep &prep, const std::vector<int> &loff,
+                      const std::vector<int> &toff);
+    void launch_kplus(const double *in, double *out);
 };
+
+void GpuSolver::Impl::launch_kplus(const double *in, double *out) {
+    size_t sm = sizeof(double) * TILE * (size_t)max_T;
+    kplus_kernel<<<P.nd, 256, sm, stream>>>(KP, in, out);
+    CUDA_CHECK(cudaGetLastError());
+}
+
+void GpuSolver::Impl::upload_kplus(const Decomposition &dec, const Prep &prep, const std::vector<int> &loff,
+                                   const std::vector<int> &toff) {
+    const int nd = dec.ndom;
+    const int dpn = dec.dpn;
+    std::vector<int> n(nd), tn(nd), doff(nd + 1, 0), rofs(nd + 1, 0);
+    std::vector<long long> tile0(nd + 1, 0);
+    max_T = 0;
+    for (int d = 0; d < nd; ++d) {
+        n[d] = prep.sub[d].n;
+        tn[d] = (n[d] + TILE - 1) / TILE;
+        max_T = std::max(max_T, tn[d]);
+        doff[d + 1] = doff[d] + n[d];
+        rofs[d + 1] = rofs[d] + n[d] * prep.sub[d].nk;
+        tile0[d + 1] = tile0[d] + (long long)tn[d] * (tn[d] + 1) / 2;
+    }
+    FETI_CHECK(sizeof(double) * TILE * (size_t)max_T <= 200 * 1024, "FETI4I: subdomain too large for the device K+ kernel");
+    ntot = doff[nd];
+    std::vector<int> pos(ntot), gdof(ntot), tdof_g(toff[nd]);
+    std::vector<double> invm(ntot), R(rofs[nd]);
+    std::vector<double> L((size_t)tile0[nd] * TILE * TILE, 0.0);
+    n_caller = 0;
+    for (int d = 0; d < nd; ++d) {
+        const SubPrep &S = prep.sub[d];
+        const DomainRows &D = dec.dom[d];
+        for (int i = 0; i < n[d]; ++i) pos[doff[d] + i] = S.pos[i];
+        for (int a = 0; a < (int)D.nodes.size(); ++a)
+            for (int c = 0; c < dpn; ++c) {
+                int g = dec.node_dof[(size_t)D.nodes[a] * dpn + c];
+                gdof[doff[d] + dpn * a + c] = g;
+                invm[doff[d] + dpn * a + c] = 1.0 / dec.node_ndom[D.nodes[a]];
+                n_caller = std::max(n_caller, g + 1);
+            }
+        std::copy(S.R.begin(), S.R.end(), R.begin() + rofs[d]);
+        for (int t = 0; t < S.t; ++t) tdof_g[toff[d] + t] = doff[d] + S.tdof[t];
+        const int T = tn[d], nn = n[d];
+        for (int J = 0; J < T; ++J)
+            for (int I = J; I < T; ++I) {
+                double *tile = L.data() + (size_t)(tile0[d] + (long long)J * T - (long long)J * (J - 1) / 2 + (I - J)) * TILE * TILE;
+                for (int r = 0; r < TILE; ++r)
+                    for (int c = 0; c < TILE; ++c) {
+                        int gr = TILE * I + r, gc = TILE * J + c;
+                        double v = 0.0;
+                        if (gr < nn && gc < nn) { if (gr >= gc) v = S.Lp[dense::packed_index(nn, gr, gc)]; }
+                        else if (gr == gc) v = 1.0;
+                        tile[r * TILE + c] = v;
+                    }
+            }
+    }
+    // per local multiplier row: DOF in the concatenated local space, sign, Dirichlet value
+    const int NL = loff[nd];
+    std::vector<int> rdof(NL);
+    std::vector<double> rsign(NL), rc(NL);
+    for (int d = 0; d < nd; ++d) {
+        const DomainRows &D = dec.dom[d];
+        for (size_t r = 0; r < D.lam.size(); ++r) {
+            rdof[loff[d] + r] = doff[d] + D.dof[r];
+            rsign[loff[d] + r] = D.sign[r];
+            rc[loff[d] + r] = D.c[r];
+        }
+    }
+    KP.nd = nd;
+    KP.n = upload(n);
+    KP.tn = upload(tn);
+    d_doff = upload(doff);
+    KP.doff = d_doff;
+    KP.tile0 = upload(tile0);
+    KP.pos = upload(pos);
+    KP.L = upload(L);
+    d_rofs = upload(rofs);
+    d_gdof = upload(gdof);
+    d_invm = upload(invm);
+    d_R = upload(R);
+    d_rdof = upload(rdof);
+    d_rsign = upload(rsign);
+    d_rc = upload(rc);
+    d_tdof_g = upload(tdof_g);
+    d_f = alloc<double>(ntot);
+    d_kf = alloc<double>(ntot);
+    d_g = alloc<double>(ntot);
+    d_rhs = alloc<double>(std::max(1, n_caller));
+    d_sol = alloc<double>(std::max(1, n_caller));
+    cudaFuncSetAttribute(kplus_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+}
 
 void GpuSolver::Impl::build_tiles(TileSetHost &T, int prec, const std::vector<const double *> &mats,
                                   const std::vector<int> &ns, const std::vector<int> &voffs, int tiles_per_item) {
@@ -814,7 +1143,13 @@ static void set_smem_limits() {
     set_tile_limits<SCHUR_FP64>(v);
     set_tile_limits<SCHUR_FP32>(v);
     set_tile_limits<SCHUR_BF16>(v);
+    cudaFuncSetAttribute(w_prec_kernel<PREC_NONE>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
     cudaFuncSetAttribute(w_prec_kernel<PREC_LUMPED>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+    cudaFuncSetAttribute(w_prec_kernel<PREC_WEIGHT>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+    cudaFuncSetAttribute(w_prec_kernel<PREC_DIRICHLET>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+    cudaFuncSetAttribute(r0_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+    cudaFuncSetAttribute(z_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+    cudaFuncSetAttribute(update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
     done = true;
 }
 
@@ -827,32 +1162,29 @@ void GpuSolver::Impl::launch_iteration(int slot) {
     if (mixed) {
         // residual replacement r = b - F64 x when the previous update asked for it
         launch_tiles(F64, 3, P.x, nullptr, Ax64, slot);
-        r0_kernel<<<nd, TPB, 0, stream>>>(P, Ax64, 1, slot);
-        zero_cond_kernel<<<std::max(1, std::min(1024, (P.NL + 255) / 256)), 256, 0, stream>>>(P, Ax64, slot);
-        replace_done_kernel<<<1, 32, 0, stream>>>(P, slot);
+        r0_kernel<<<nd, TPB, sizeof(double) * max_ni, stream>>>(P, Ax64, 1, slot);
     }
     coarse_kernel<<<cgrid, 256, 0, stream>>>(P, P.d, P.alpha, slot, 1);
-    const size_t tsm = sizeof(double) * (size_t)std::max(1, max_nt);
+    const size_t tsm = sizeof(double) * (size_t)(max_ni + max_nt);
     switch (opt.precond) {
-    case PREC_NONE: w_prec_kernel<PREC_NONE><<<nd, TPB, 0, stream>>>(P, slot); break;
+    case PREC_NONE: w_prec_kernel<PREC_NONE><<<nd, TPB, tsm, stream>>>(P, slot); break;
     case PREC_LUMPED: w_prec_kernel<PREC_LUMPED><<<nd, TPB, tsm, stream>>>(P, slot); break;
-    case PREC_WEIGHT: w_prec_kernel<PREC_WEIGHT><<<nd, TPB, 0, stream>>>(P, slot); break;
-    default: w_prec_kernel<PREC_DIRICHLET><<<nd, TPB, 0, stream>>>(P, slot); break;
+    case PREC_WEIGHT: w_prec_kernel<PREC_WEIGHT><<<nd, TPB, tsm, stream>>>(P, slot); break;
+    default: w_prec_kernel<PREC_DIRICHLET><<<nd, TPB, tsm, stream>>>(P, slot); break;
     }
-    if (mixed) rmax_kernel<<<1, 256, 0, stream>>>(P, slot);
     if (opt.precond != PREC_NONE) {
         if (opt.precond == PREC_DIRICHLET) {
             zero_vT_kernel<<<std::max(1, std::min(1024, (P.NT + 255) / 256)), 256, 0, stream>>>(P, slot);
             launch_tiles(Dir, 2, P.uT, nullptr, P.vT, slot);
         }
-        z_kernel<<<nd, TPB, 0, stream>>>(P, slot);
+        z_kernel<<<nd, TPB, sizeof(double) * max_ni, stream>>>(P, slot);
         coarse_kernel<<<cgrid, 256, 0, stream>>>(P, P.d, P.alpha, slot, 1);
-        y_kernel<<<nd, TPB, 0, stream>>>(P, slot);
+        y_kernel<<<nd, TPB, 0, stream>>>(P, Ax64, slot);
     } else {
-        zero_kernel<<<(P.NL + 255) / 256, 256, 0, stream>>>(P.Ap, P.NL);
+        zero2_kernel<<<(P.NL + 255) / 256, 256, 0, stream>>>(P.Ap, Ax64, P.NL);
     }
     launch_tiles(Fop, 1, P.y, P.p, P.Ap, slot);
-    update_kernel<<<nd, TPB, 0, stream>>>(P, Fop.item_dot, Fop.nitems, slot);
+    update_kernel<<<nd, TPB, sizeof(double) * max_ni, stream>>>(P, slot);
     CUDA_CHECK(cudaGetLastError());
 }
 
@@ -860,7 +1192,7 @@ int GpuSolver::Impl::kernels_per_iteration() const {
     const bool mixed = opt.schur_precision != SCHUR_FP64;
     int k = 3;  // coarse, w/prec, update
     k += 1;     // F apply
-    if (mixed) k += 5;
+    if (mixed) k += 2;
     if (opt.precond != PREC_NONE) k += 3 + (opt.precond == PREC_DIRICHLET ? 2 : 0);
     else k += 1;
     return k;
@@ -932,11 +1264,15 @@ void GpuSolver::upload(const Decomposition &dec, const Prep &prep, const SolveOp
     I.n_lambda = dec.n_lambda;
     I.h_loff = loff;
     I.h_lam.resize(NL);
+    int KS = 1;
+    for (int d = 0; d < nd; ++d) KS = std::max(KS, prep.sub[d].nk);
     std::vector<int> partner(NL, -1), tidx(NL), rkof(NL), rnk(NL);
-    std::vector<double> ws(NL), minv(NL), Gl((size_t)NL * KMAX, 0.0);
+    std::vector<double> ws(NL), minv(NL), Gl((size_t)NL * KS, 0.0);
+    I.max_ni = 0;
     for (int d = 0; d < nd; ++d) {
         const DomainRows &D = dec.dom[d];
         const SubPrep &S = prep.sub[d];
+        I.max_ni = std::max(I.max_ni, S.ni);
         for (int r = 0; r < S.ni; ++r) {
             int e = loff[d] + r;
             int l = D.lam[r];
@@ -949,10 +1285,22 @@ void GpuSolver::upload(const Decomposition &dec, const Prep &prep, const SolveOp
             minv[e] = d1 >= 0 ? 0.5 : 1.0;
             rkof[e] = kof[d];
             rnk[e] = S.nk;
-            for (int k = 0; k < S.nk; ++k) Gl[(size_t)e * KMAX + k] = S.G[(size_t)k * S.ni + r];
+            for (int k = 0; k < S.nk; ++k) Gl[(size_t)e * KS + k] = S.G[(size_t)k * S.ni + r];
         }
     }
-    // T space: rows of each touched DOF, lumped K_TT in global T indices
+    // partner data of every row (shortens the dependent-load chains of the assembly)
+    std::vector<int> ptidx(NL, -1), pkof(NL, 0), pnk(NL, 0);
+    std::vector<double> pws(NL, 0.0), Gp((size_t)NL * KS, 0.0);
+    for (int e = 0; e < NL; ++e) {
+        int q = partner[e];
+        if (q < 0) continue;
+        ptidx[e] = tidx[q];
+        pws[e] = ws[q];
+        pkof[e] = rkof[q];
+        pnk[e] = rnk[q];
+        for (int k = 0; k < KS; ++k) Gp[(size_t)e * KS + k] = Gl[(size_t)q * KS + k];
+    }
+    // T space: rows of each touched DOF
     std::vector<int> trow_ptr(NT + 1, 0), trow_idx(NL);
     for (int e = 0; e < NL; ++e) trow_ptr[tidx[e] + 1]++;
     for (int t = 0; t < NT; ++t) trow_ptr[t + 1] += trow_ptr[t];
@@ -960,32 +1308,50 @@ void GpuSolver::upload(const Decomposition &dec, const Prep &prep, const SolveOp
         std::vector<int> fill(trow_ptr.begin(), trow_ptr.end() - 1);
         for (int e = 0; e < NL; ++e) trow_idx[fill[tidx[e]]++] = e;
     }
-    std::vector<int> kt_ptr(NT + 1, 0), kt_col;
-    std::vector<double> kt_val;
+    // lumped preconditioner: K_TT of each subdomain in sliced ELL (32 rows, column-major)
+    std::vector<int> slice0(nd + 1, 0), ell_ptr, ell_w;
+    std::vector<unsigned short> ell_col;
+    std::vector<double> ell_val;
     I.max_nt = 0;
     for (int d = 0; d < nd; ++d) {
         const SubPrep &S = prep.sub[d];
         I.max_nt = std::max(I.max_nt, S.t);
-        if (opt.precond == PREC_LUMPED) {
-            for (int t = 0; t < S.t; ++t) {
+        slice0[d + 1] = slice0[d];
+        if (opt.precond != PREC_LUMPED) continue;
+        FETI_CHECK(S.t < 65536, "FETI4I: too many interface DOFs in one subdomain for the lumped kernel");
+        for (int t0 = 0; t0 < S.t; t0 += 32) {
+            int w = 0;
+            for (int t = t0; t < std::min(S.t, t0 + 32); ++t) w = std::max(w, S.KT_ptr[t + 1] - S.KT_ptr[t]);
+            ell_ptr.push_back((int)ell_val.size());
+            ell_w.push_back(w);
+            size_t base = ell_val.size();
+            ell_val.resize(base + (size_t)32 * w, 0.0);
+            ell_col.resize(base + (size_t)32 * w, 0);
+            for (int t = t0; t < std::min(S.t, t0 + 32); ++t)
                 for (int j = S.KT_ptr[t]; j < S.KT_ptr[t + 1]; ++j) {
-                    kt_col.push_back(toff[d] + S.KT_col[j]);
-                    kt_val.push_back(S.KT_val[j]);
+                    size_t o = base + (size_t)(j - S.KT_ptr[t]) * 32 + (t - t0);
+                    ell_val[o] = S.KT_val[j];
+                    ell_col[o] = (unsigned short)S.KT_col[j];
                 }
-                kt_ptr[toff[d] + t + 1] = (int)kt_col.size();
-            }
+            slice0[d + 1]++;
         }
     }
-    if (opt.precond == PREC_LUMPED)
-        FETI_CHECK(sizeof(double) * (size_t)I.max_nt <= 200 * 1024, "FETI4I: subdomain interface too large for the lumped kernel");
+    FETI_CHECK(sizeof(double) * (size_t)(I.max_nt + I.max_ni) <= 200 * 1024,
+               "FETI4I: subdomain interface too large for the preconditioner kernel");
 
     DevProblem &P = I.P;
-    P.nd = nd; P.NL = NL; P.nK = prep.n_kern; P.NT = NT;
+    P.nd = nd; P.NL = NL; P.nK = prep.n_kern; P.NT = NT; P.KS = KS;
     P.loff = I.upload(loff); P.kof = I.upload(kof); P.toff = I.upload(toff);
-    P.partner = I.upload(partner); P.tidx = I.upload(tidx); P.ws = I.upload(ws); P.minv = I.upload(minv);
-    P.Gl = I.upload(Gl); P.rkof = I.upload(rkof); P.rnk = I.upload(rnk);
+    P.partner = I.upload(partner); P.tidx = I.upload(tidx); P.ptidx = I.upload(ptidx);
+    P.ws = I.upload(ws); P.pws = I.upload(pws); P.minv = I.upload(minv);
+    P.Gl = I.upload(Gl); P.Gp = I.upload(Gp);
+    P.rkof = I.upload(rkof); P.rnk = I.upload(rnk); P.pkof = I.upload(pkof); P.pnk = I.upload(pnk);
     P.trow_ptr = I.upload(trow_ptr); P.trow_idx = I.upload(trow_idx);
-    P.kt_ptr = I.upload(kt_ptr); P.kt_col = I.upload(kt_col); P.kt_val = I.upload(kt_val);
+    P.slice0 = I.upload(slice0); P.ell_ptr = I.upload(ell_ptr); P.ell_w = I.upload(ell_w);
+    P.ell_col = I.upload(ell_col); P.ell_val = I.upload(ell_val);
+    P.scal = I.alloc<double>(SC_COUNT);
+    P.done = I.alloc<int>(DONE_COUNT);
+    CUDA_CHECK(cudaMemset(P.done, 0, sizeof(int) * DONE_COUNT));
     P.GGtinv = I.upload(prep.GGt_inv);
     P.bL = I.alloc<double>(NL);
     P.x = I.alloc<double>(NL); P.r = I.alloc<double>(NL); P.w = I.alloc<double>(NL); P.z = I.alloc<double>(NL);
@@ -1029,7 +1395,46 @@ void GpuSolver::upload(const Decomposition &dec, const Prep &prep, const SolveOp
         FETI_CHECK(tile_smem(SCHUR_FP64, I.max_tn_dir) <= 200 * 1024, "FETI4I: a Dirichlet block is too large for the tile kernel");
         I.build_tiles(I.Dir, SCHUR_FP64, dm, dn, dv, opt.tiles_per_item);
     }
+    I.upload_kplus(dec, prep, loff, toff);
     CUDA_CHECK(cudaDeviceSynchronize());
+}
+
+void GpuSolver::solve_full(const double *rhs, int rhs_size, double *solution, int solution_size, SolveStats &stats,
+                           bool upload_rhs) {
+    Impl &I = *impl;
+    DevProblem &P = I.P;
+    const int nd = P.nd;
+    const size_t need = std::max<size_t>({(size_t)rhs_size, (size_t)solution_size, (size_t)1});
+    if (I.h_pinned_n < need) {
+        if (I.h_pinned) cudaFreeHost(I.h_pinned);
+        CUDA_CHECK(cudaMallocHost(&I.h_pinned, need * sizeof(double)));
+        I.h_pinned_n = need;
+    }
+    if (upload_rhs) {
+        CUDA_CHECK(cudaMemsetAsync(I.d_rhs, 0, sizeof(double) * std::max(1, I.n_caller), I.stream));
+        const int ncp = std::min(rhs_size, I.n_caller);
+        std::memcpy(I.h_pinned, rhs, sizeof(double) * ncp);
+        CUDA_CHECK(cudaMemcpyAsync(I.d_rhs, I.h_pinned, sizeof(double) * ncp, cudaMemcpyHostToDevice, I.stream));
+        split_rhs_kernel<<<(I.ntot + 255) / 256, 256, 0, I.stream>>>(I.d_rhs, I.d_gdof, I.d_invm, I.d_f, I.ntot);
+        I.launch_kplus(I.d_f, I.d_kf);
+        evec_kernel<<<nd, TPB, 0, I.stream>>>(P, I.d_doff, I.d_rofs, I.d_R, I.d_f, I.e_dev);
+        bvec_kernel<<<(P.NL + 255) / 256, 256, 0, I.stream>>>(P, I.d_rdof, I.d_rsign, I.d_rc, I.d_kf, (double *)P.bL);
+        CUDA_CHECK(cudaGetLastError());
+    }
+    solve(stats);
+    // primal: u = K^+ (f - B^T lambda) + R alpha, averaged into the caller's DOFs
+    primal_rhs_kernel<<<std::max(1, std::min(4096, (I.ntot + 255) / 256)), 256, 0, I.stream>>>(P, I.d_tdof_g, I.d_rsign, I.d_f, I.d_g, I.ntot);
+    primal_bt_kernel<<<(P.NT + 255) / 256, 256, 0, I.stream>>>(P, I.d_tdof_g, I.d_rsign, I.d_g);
+    I.launch_kplus(I.d_g, I.d_kf);
+    CUDA_CHECK(cudaMemsetAsync(I.d_sol, 0, sizeof(double) * std::max(1, I.n_caller), I.stream));
+    primal_merge_kernel<<<nd, TPB, 0, I.stream>>>(P, I.d_doff, I.d_rofs, I.d_R, I.d_kf, I.d_gdof, I.d_invm, I.d_sol);
+    CUDA_CHECK(cudaGetLastError());
+    const int ncp = std::min(solution_size, I.n_caller);
+    CUDA_CHECK(cudaMemcpyAsync(I.h_pinned, I.d_sol, sizeof(double) * std::max(0, ncp), cudaMemcpyDeviceToHost, I.stream));
+    CUDA_CHECK(cudaStreamSynchronize(I.stream));
+    std::memcpy(solution, I.h_pinned, sizeof(double) * std::max(0, ncp));
+    for (int i = std::max(0, ncp); i < solution_size; ++i) solution[i] = 0.0;
+    stats.kernel_launches += 10;
 }
 
 void GpuSolver::set_rhs(const std::vector<double> &b, const std::vector<double> &e) {
@@ -1049,8 +1454,8 @@ void GpuSolver::solve(SolveStats &stats) {
     DevState h{};
     h.conv_iter = -1;
     h.iter_base = 0;
-    h.replace_next = 0;
-    h.r_true = 1;
+    h.replace_iter = -1;
+    h.true_iter = 0;
     h.replacements = 0;
     h.max_it = I.opt.max_iterations;
     h.mixed = mixed ? 1 : 0;
@@ -1065,7 +1470,7 @@ void GpuSolver::solve(SolveStats &stats) {
     gt_kernel<<<(P.NL + 255) / 256, 256, 0, I.stream>>>(P, P.alpha, P.x);
     zero_kernel<<<(P.NL + 255) / 256, 256, 0, I.stream>>>(P.p, P.NL);
     I.launch_tiles(I.F64, 0, P.x, nullptr, I.Ax64, 0);
-    r0_kernel<<<nd, TPB, 0, I.stream>>>(P, I.Ax64, 0, 0);
+    r0_kernel<<<nd, TPB, sizeof(double) * I.max_ni, I.stream>>>(P, I.Ax64, 0, 0);
     zero_kernel<<<(P.NL + 255) / 256, 256, 0, I.stream>>>(I.Ax64, P.NL);
     coarse_kernel<<<cgrid, 256, 0, I.stream>>>(P, P.d, P.alpha, 0, 0);
     pnorm_kernel<<<nd, TPB, 0, I.stream>>>(P);

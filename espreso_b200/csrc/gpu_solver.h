@@ -50,6 +50,11 @@ public:
     void set_rhs(const std::vector<double> &b, const std::vector<double> &e);
     void solve(SolveStats &st);
     void get_solution(std::vector<double> &lambda, std::vector<double> &alpha);
+    // Whole solve on the device: caller right-hand side -> f_i, K^+ f_i, b, e, dual PCG,
+    // primal recovery u_i = K^+ (f_i - B_i^T lambda) + R_i alpha_i, averaged into `solution`.
+    // With upload_rhs == false the right-hand side of the previous call is reused.
+    void solve_full(const double *rhs, int rhs_size, double *solution, int solution_size, SolveStats &st,
+                    bool upload_rhs = true);
     // y = F x in lambda space with the given operator precision (tests, benchmarks)
     void apply_F(const double *x_lambda, double *y_lambda, int precision);
     // average device time of `reps` F applies (inputs resident), returns ms
