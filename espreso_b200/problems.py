@@ -203,6 +203,8 @@ CONFIGS = {
     # configs of the benchmark definition; sizes as stated there
     "c1_elasticity_64": dict(kind="elasticity", domains=(4, 4, 4), elements=(8, 8, 8)),
     "c2_heat_512": dict(kind="heat", domains=(8, 8, 8), elements=(10, 10, 10)),
+    # smaller variant of the heat workload (profiling captures; a few GB on the device)
+    "c2_heat_216": dict(kind="heat", domains=(6, 6, 6), elements=(10, 10, 10)),
 }
 
 
