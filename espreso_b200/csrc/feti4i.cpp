@@ -487,4 +487,14 @@ FETI4IReal FETI4ITimeDualOperator(FETI4IInstance instance, FETI4IInt precision, 
     return ms;
 }
 
+int FETI4ITiledSymvNoAlloc(const FETI4IReal *tiles, const long long *tile_offset, const FETI4IInt *order,
+                           const FETI4IInt *vector_offset, FETI4IInt nmatrices, FETI4IInt max_order,
+                           const FETI4IReal *x, FETI4IReal *y, FETI4IReal *dot, void *stream) {
+    int rc = -1;
+    guarded([&] {
+        rc = tiled_symv_noalloc(tiles, tile_offset, order, vector_offset, nmatrices, max_order, x, y, dot, stream);
+    });
+    return rc;
+}
+
 }  // extern "C"

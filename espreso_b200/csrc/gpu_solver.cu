@@ -1569,3 +1569,158 @@ double GpuSolver::fapply_bytes(int precision) const {
 }
 
 }  // namespace feti
+
+// =============================================================================================
+// Allocation-free batched tile SYMV (FETI4ITiledSymvNoAlloc).
+//
+// For callers that own every byte of device memory themselves (a finite-element
+// code that reserves HBM in its own pool at start-up and must not allocate while
+// it runs): the caller passes the tiles, descriptors, x and y; the only scratch
+// the kernel needs (work-queue counters and one dot partial per matrix) lives in
+// the file-scope array below, NOALLOC_MAX_MATRICES matrices at most.  Every GPU
+// that loads the library holds this array until the process exits.  All calls
+// share it and it keeps the last call's contents, so each call clears its
+// counters first, and calls that overlap on the GPU (different streams) race.
+namespace feti {
+namespace {
+
+constexpr int NOALLOC_MAX_MATRICES = 16384;
+constexpr int NOALLOC_MAX_ORDER = 3200;   // 2 * 32 * ceil(order/32) doubles of shared memory per CTA
+
+struct NoAllocScratch {
+    int queue;      // next matrix to take
+    int done;       // CTAs that finished
+    int pad[62];
+    double dots[NOALLOC_MAX_MATRICES];
+};
+
+static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
+
+// one 32x32 tile with known block coordinates (I, J), FP64
+__device__ __forceinline__ void tile_fma_noalloc(const uint4 (&raw)[16], int I, int J, const double *xs, double *ys,
+                                                 int lane) {
+    const int cq = lane % 16, h = lane / 16, idx = 2 * cq + h;
+    double xc[2], xr[16], rs[16], cs[2];
+    xc[0] = xs[TILE * J + 2 * cq];
+    xc[1] = xs[TILE * J + 2 * cq + 1];
+    cs[0] = cs[1] = 0.0;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) { xr[q] = xs[TILE * I + 2 * q + h]; rs[q] = 0.0; }
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+        const double e0 = __hiloint2double(raw[q].y, raw[q].x), e1 = __hiloint2double(raw[q].w, raw[q].z);
+        rs[q] += e0 * xc[0] + e1 * xc[1];
+        cs[0] += e0 * xr[q];
+        cs[1] += e1 * xr[q];
+    }
+    atomicAdd(&ys[TILE * I + idx], reduce_scatter<16, 0>(rs, lane));
+    if (I != J) atomicAdd(&ys[TILE * J + idx], reduce_scatter<2, 4>(cs, lane));
+}
+
+__global__ void __launch_bounds__(256, 2)
+tile_symv_noalloc_kernel(const double *tiles, const long long *tile0, const int *order, const int *voff, int nmat,
+                         int max_order, const double *x, double *y, double *dot_out, NoAllocScratch *scr) {
+    extern __shared__ __align__(16) double nsm[];
+    __shared__ double red[32];
+    __shared__ int s_m, s_last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const uint4 *tl = reinterpret_cast<const uint4 *>(tiles);
+    for (;;) {
+        if (threadIdx.x == 0) s_m = atomicAdd(&scr->queue, 1);
+        __syncthreads();
+        const int m = s_m;
+        if (m >= nmat) break;
+        const int n = order[m];
+        if (n > max_order || n < 0) {   // violates the caller's stated bound: skip, output untouched
+            if (threadIdx.x == 0) scr->dots[m] = 0.0;
+            __syncthreads();
+            continue;
+        }
+        const int T = (n + TILE - 1) / TILE, o = voff[m];
+        double *xs = nsm, *ys = nsm + TILE * T;
+        for (int i = threadIdx.x; i < TILE * T; i += blockDim.x) {
+            xs[i] = i < n ? x[o + i] : 0.0;
+            ys[i] = 0.0;
+        }
+        __syncthreads();
+        const int ntiles = T * (T + 1) / 2;
+        // tiles k = warp, warp + nw, ...; (I, J) followed incrementally along the upper triangle
+        int I = 0, off = warp;
+        while (I < T && off >= T - I) { off -= T - I; ++I; }
+        for (int k = warp; k < ntiles; k += nw) {
+            uint4 raw[16];
+            const uint4 *tp = tl + (size_t)(tile0[m] + k) * (TILE * 16);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) raw[q] = ld_stream(tp + q * 32 + lane);
+            tile_fma_noalloc(raw, I, I + off, xs, ys, lane);
+            off += nw;
+            while (I < T && off >= T - I) { off -= T - I; ++I; }
+        }
+        __syncthreads();
+        double dot = 0.0;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            y[o + i] = ys[i];
+            dot += xs[i] * ys[i];
+        }
+        dot = block_sum(dot, red);
+        if (threadIdx.x == 0) scr->dots[m] = dot;
+        __syncthreads();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = (atomicAdd(&scr->done, 1) == (int)gridDim.x - 1);
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        double t = 0.0;
+        for (int i = threadIdx.x; i < nmat; i += blockDim.x) t += __ldcg(&scr->dots[i]);
+        t = block_sum(t, red);
+        if (threadIdx.x == 0 && dot_out) *dot_out = t;
+    }
+}
+
+// device address of the scratch array, looked up once per device
+NoAllocScratch *g_noalloc_ptr[256];
+bool g_noalloc_ready[256];
+
+}  // namespace
+
+int tiled_symv_noalloc(const double *tiles, const long long *tile_offset, const int *order, const int *vector_offset,
+                       int nmatrices, int max_order, const double *x, double *y, double *dot, void *stream) {
+    FETI_CHECK(nmatrices >= 0 && nmatrices <= NOALLOC_MAX_MATRICES,
+               "FETI4ITiledSymvNoAlloc: nmatrices must be in [0, " + std::to_string(NOALLOC_MAX_MATRICES) +
+                   "] (size of the static scratch array)");
+    FETI_CHECK(max_order >= 0 && max_order <= NOALLOC_MAX_ORDER,
+               "FETI4ITiledSymvNoAlloc: max_order must be in [0, " + std::to_string(NOALLOC_MAX_ORDER) + "]");
+    FETI_CHECK(nmatrices == 0 || (tiles && tile_offset && order && vector_offset && x && y),
+               "FETI4ITiledSymvNoAlloc: null device pointer");
+    int dev = 0;
+    CUDA_CHECK(cudaGetDevice(&dev));
+    FETI_CHECK(dev >= 0 && dev < 256, "FETI4ITiledSymvNoAlloc: device index out of range");
+    if (!g_noalloc_ready[dev]) {
+        // first call on this device: resolve the device address of the scratch array
+        NoAllocScratch *p = nullptr;
+        cudaError_t rc = cudaGetSymbolAddress((void **)&p, g_noalloc_scratch);
+        FETI_CHECK(rc == cudaSuccess, std::string("FETI4ITiledSymvNoAlloc: cudaGetSymbolAddress failed: ") +
+                                          cudaGetErrorString(rc));
+        const int smem = (int)(2 * sizeof(double) * TILE * ((NOALLOC_MAX_ORDER + TILE - 1) / TILE));
+        CUDA_CHECK(cudaFuncSetAttribute(tile_symv_noalloc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        g_noalloc_ptr[dev] = p;
+        g_noalloc_ready[dev] = true;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    NoAllocScratch *scr = g_noalloc_ptr[dev];
+    CUDA_CHECK(cudaMemsetAsync(scr, 0, offsetof(NoAllocScratch, dots), s));  // counters start at zero
+    int nsm = 148;
+    CUDA_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const int grid = std::max(1, std::min(std::max(1, nmatrices), 2 * nsm));
+    const size_t smem = 2 * sizeof(double) * TILE * (size_t)((max_order + TILE - 1) / TILE);
+    tile_symv_noalloc_kernel<<<grid, 256, smem, s>>>(tiles, tile_offset, order, vector_offset, nmatrices, max_order, x,
+                                                     y, dot, scr);
+    CUDA_CHECK(cudaGetLastError());
+    return 0;
+}
+
+}  // namespace feti

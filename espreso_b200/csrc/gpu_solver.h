@@ -70,4 +70,8 @@ public:
 
 bool cuda_available(std::string &why);
 
+// Allocation-free batched tile SYMV on caller-owned device buffers (scratch in a static device array).
+int tiled_symv_noalloc(const double *tiles, const long long *tile_offset, const int *order, const int *vector_offset,
+                       int nmatrices, int max_order, const double *x, double *y, double *dot, void *stream);
+
 }  // namespace feti

@@ -36,6 +36,7 @@ EXPORTED = [
     "FETI4IGetStats", "FETI4IGetDualSolution", "FETI4IGetSubdomainInfo", "FETI4IGetSubdomainMultipliers",
     "FETI4IGetSubdomainNodes", "FETI4IGetSubdomainSchur", "FETI4IGetSubdomainKernel", "FETI4IGetDualRhs",
     "FETI4IApplySubdomainKplus", "FETI4IApplyDualOperator", "FETI4ITimeDualOperator", "FETI4ISolveResident", "FETI4ISetSolvePrecision",
+    "FETI4ITiledSymvNoAlloc",
 ]
 
 
@@ -85,6 +86,7 @@ def load(path: str = LIB_PATH):
         "FETI4ITimeDualOperator": ([vp, i32, i32], f64),
         "FETI4ISolveResident": ([vp], f64),
         "FETI4ISetSolvePrecision": ([vp, i32], None),
+        "FETI4ITiledSymvNoAlloc": ([vp, vp, vp, vp, i32, i32, vp, vp, vp, vp], i32),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -106,6 +108,40 @@ def _check(lib):
     msg = lib.FETI4IGetLastError()
     if msg:
         raise FETI4IError(msg.decode())
+
+
+def tiled_symv_noalloc(tiles, tile_offset, order, vector_offset, nmatrices, max_order, x, y, dot=0, stream=0):
+    """FETI4ITiledSymvNoAlloc on caller-owned device pointers (integers); returns the status code."""
+    lib = load()
+    rc = lib.FETI4ITiledSymvNoAlloc(C.c_void_p(tiles), C.c_void_p(tile_offset), C.c_void_p(order),
+                                    C.c_void_p(vector_offset), int(nmatrices), int(max_order), C.c_void_p(x),
+                                    C.c_void_p(y), C.c_void_p(dot) if dot else None,
+                                    C.c_void_p(stream) if stream else None)
+    if rc != 0:
+        _check(lib)
+        raise FETI4IError("FETI4ITiledSymvNoAlloc failed")
+    return rc
+
+
+def pack_symmetric_tiles(mats):
+    """Pack symmetric matrices into the 32x32 upper-tile layout of FETI4ITiledSymvNoAlloc.
+
+    Returns (tiles float64 array, tile_offset int64, order int32)."""
+    out, offs, orders = [], [], []
+    total = 0
+    for S in mats:
+        n = S.shape[0]
+        T = (n + 31) // 32
+        P = np.zeros((32 * T, 32 * T))
+        P[:n, :n] = S
+        offs.append(total)
+        orders.append(n)
+        for I in range(T):
+            for J in range(I, T):
+                out.append(P[32 * I:32 * I + 32, 32 * J:32 * J + 32].copy())
+        total += T * (T + 1) // 2
+    tiles = np.stack(out).ravel() if out else np.zeros(0)
+    return tiles, np.array(offs, dtype=np.int64), np.array(orders, dtype=np.int32)
 
 
 def default_options():

@@ -95,6 +95,27 @@ FETI4IReal FETI4ISolveResident(FETI4IInstance instance);
 /* Select the operator precision of the following solves (must have been prepared). */
 void FETI4ISetSolvePrecision(FETI4IInstance instance, FETI4IInt precision);
 
+/* Allocation-free batched SYMV: y_m = S_m x_m for m < nmatrices (no counterpart in
+ * the reference).  For callers that manage all device memory themselves and may
+ * not allocate while they run (for example a finite-element code that reserves
+ * its HBM pool at start-up): every pointer is caller-owned device memory and
+ * the call allocates nothing.  Layout: matrix m of order order[m] <= max_order
+ * is stored from tile tile_offset[m] of `tiles` as its T(T+1)/2 upper 32x32
+ * tiles, T = ceil(order/32), tile (I,J), I <= J, in row-major tile order, each
+ * tile row-major FP64, diagonal tiles holding the full symmetric block, zero
+ * padding beyond the order.  x and y use vector_offset[m].  If `dot` is not
+ * NULL the total x.y lands there (device memory).  Limits: nmatrices <= 16384
+ * and max_order <= 3200; larger values are rejected with an error (return -1,
+ * message in FETI4IGetLastError); matrices above max_order are skipped.  The
+ * scratch (work-queue counters, one dot partial per matrix) is a static array
+ * in device memory, held by every GPU that loads the library until exit; the
+ * first call on a device looks up its address, so that call should come before
+ * any stream capture.  Calls share the array: calls that overlap on the GPU
+ * race.  stream: a cudaStream_t, or NULL for the default stream. */
+int FETI4ITiledSymvNoAlloc(const FETI4IReal *tiles, const long long *tile_offset, const FETI4IInt *order,
+                           const FETI4IInt *vector_offset, FETI4IInt nmatrices, FETI4IInt max_order,
+                           const FETI4IReal *x, FETI4IReal *y, FETI4IReal *dot, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
