@@ -42,6 +42,8 @@ def parse():
     ap.add_argument("--schur", default="fp32", choices=sorted(SCHUR))
     ap.add_argument("--precond", type=int, default=1)
     ap.add_argument("--precision", type=float, default=1e-8)
+    ap.add_argument("--tile-kernel", type=int, default=1, help="0 register prefetch, 1 TMA bulk pipeline")
+    ap.add_argument("--delta", type=float, default=0.1, help="residual replacement threshold")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -199,7 +201,8 @@ def run_ours(args):
     inst = problems.make_instance(P, iopts={F.PRECONDITIONER: args.precond, F.VERBOSE_LEVEL: 0,
                                             F.MAX_ITERATIONS: 5000},
                                   ropts={F.PRECISION: args.precision},
-                                  ext={F.EXT_SCHUR_PRECISION: SCHUR[args.schur]})
+                                  ext={F.EXT_SCHUR_PRECISION: SCHUR[args.schur], F.EXT_TILE_KERNEL: args.tile_kernel,
+                                       F.EXT_RELIABLE_DELTA: args.delta})
     setup_s = time.time() - t0
     st0 = inst.stats()
     sol = np.zeros(P.ndofs)
@@ -265,7 +268,9 @@ def run_ours(args):
                    "pcg_iterations": int(st["iterations"]), "replacements": int(st["replacements"]),
                    "parallelism": f"replicas{world}", "l2": "working set > L2 (Schur tiles "
                    f"{alg / 1e9:.2f} GB per apply, 126 MB L2)", "wall_ms_per_step": wall,
-                   "setup_s": setup_s, "host_prep_s": st0["prep_seconds"]},
+                   "setup_s": setup_s, "host_prep_s": st0["prep_seconds"],
+                   "tile_kernel": "tma_bulk_pipeline" if args.tile_kernel == 1 else "ldg_prefetch",
+                   "reliable_delta": args.delta},
         "fp64_gpu": {"ms": fp64_ms, "pcg_iterations": int(st64["iterations"]), "speedup_mixed": fp64_ms / step_ms,
                      "fapply_ms": fp64_f},
         "solves_per_s": world * 1e3 / step_ms,

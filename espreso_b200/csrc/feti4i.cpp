@@ -55,7 +55,7 @@ namespace {
 std::mutex g_mutex;
 std::list<FETI4IStructMatrix *> g_matrices;
 std::list<FETI4IStructInstance *> g_instances;
-double g_ext[FETI4I_EXT_OPTIONS_SIZE] = {0, 1, 0, 48, 16, 0.1, 0};
+double g_ext[FETI4I_EXT_OPTIONS_SIZE] = {0, 1, 0, 48, 16, 0.1, 0, 1};
 
 template <typename F>
 void guarded(F &&f) {
@@ -126,6 +126,7 @@ void build(FETI4IStructInstance *I) {
     so.tiles_per_item = std::max(1, (int)I->ext[FETI4I_EXT_TILES_PER_ITEM]);
     so.chunk = std::max(1, (int)I->ext[FETI4I_EXT_GRAPH_CHUNK]);
     so.reliable_delta = I->ext[FETI4I_EXT_RELIABLE_DELTA];
+    so.tile_kernel = (int)I->ext[FETI4I_EXT_TILE_KERNEL];
     I->gpu.reset();
     I->rhs_on_device = false;
     if (I->ext[FETI4I_EXT_HOST_ONLY] == 0.0) {
@@ -385,6 +386,7 @@ void FETI4IGetStats(FETI4IInstance instance, FETI4IInt size, FETI4IReal *stats) 
         v[FETI4I_STAT_DEVICE_BYTES] = I->gpu ? (double)I->gpu->device_bytes() : 0.0;
         v[FETI4I_STAT_FINAL_NORM] = I->stats.final_norm;
         v[FETI4I_STAT_TOLERANCE] = I->stats.tol;
+        v[FETI4I_STAT_ELEMENTS] = (double)I->el.nelem();
         for (int i = 0; i < size && i < FETI4I_STAT_SIZE; ++i) stats[i] = v[i];
     });
 }
@@ -485,6 +487,16 @@ FETI4IReal FETI4ITimeDualOperator(FETI4IInstance instance, FETI4IInt precision, 
         ms = I->gpu->time_F(precision, std::max(1, reps));
     });
     return ms;
+}
+
+void FETI4IElementEnergies(FETI4IInstance instance, FETI4IInt size, const FETI4IReal *u, const FETI4IReal *v,
+                           FETI4IReal *out) {
+    guarded([&] {
+        auto *I = check_instance(instance);
+        FETI_CHECK(I->gpu, "FETI4I: no device solver");
+        FETI_CHECK(size > 0 && u && v && out, "FETI4I: invalid vectors");
+        I->gpu->element_energies(I->el, u, v, size, out);
+    });
 }
 
 int FETI4ITiledSymvNoAlloc(const FETI4IReal *tiles, const long long *tile_offset, const FETI4IInt *order,

@@ -47,7 +47,7 @@ struct DevState {
     int replacements;
     int max_it;
     int mixed;
-    int pad;
+    int error;          // set by a kernel whose bounded wait ran out (pipeline stalled)
     double tol;
     double precision;
     double rmax;        // largest projected residual norm since the last replacement
@@ -225,11 +225,19 @@ struct TileT<SCHUR_BF16> {
     static constexpr int EPC = 8;
 };
 
+// L2 policy for data streamed once per apply: evict first, so the vectors and
+// metadata of the small kernels stay resident in the 126 MB L2
+__device__ __forceinline__ unsigned long long policy_evict_first() {
+    unsigned long long pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
 __device__ __forceinline__ uint4 ld_stream(const uint4 *p) {
     uint4 v;
-    asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0,%1,%2,%3}, [%4];"
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
                  : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
-                 : "l"(p));
+                 : "l"(p), "l"(policy_evict_first()));
     return v;
 }
 
@@ -417,6 +425,237 @@ tile_symv_kernel(TileSetDev ts, DevProblem P, const double *src, const double *s
     // the last CTA to finish resets the work queue for the next launch and, in
     // the PCG loop, adds the item dot products p.Ap in item order
     __shared__ int s_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = (atomicAdd(&ts.queue[1], 1) == (int)gridDim.x - 1);
+    }
+    __syncthreads();
+    if (s_last) {
+        if (MODE == 1) {
+            __threadfence();
+            double t = 0.0;
+            for (int i = threadIdx.x; i < ts.nitems; i += blockDim.x) t += __ldcg(&ts.item_dot[i]);
+            t = block_sum(t, red);
+            if (threadIdx.x == 0) P.scal[SC_PAP] = t;
+        }
+        if (threadIdx.x == 0) {
+            ts.queue[0] = 0;
+            ts.queue[1] = 0;
+            __threadfence();
+        }
+    }
+}
+
+
+// ---------------------------------------------------------------------------------------------
+// TMA-staged tile SYMV.  One producer warp streams the tiles of the work queue
+// into a ring of shared-memory stages with 1D bulk copies
+// (cp.async.bulk ... mbarrier::complete_tx, L2 evict-first); eight consumer
+// warps reduce them (one tile per warp per stage) as in tile_symv_kernel.
+// Full/empty mbarriers hand the stages over; every wait is bounded: on time-out
+// the kernel records DevState::error, the producer drains its copies in flight
+// and the CTA returns.
+constexpr int TMA_CONSUMERS = 8;
+constexpr int TMA_MAX_STAGES = 16;
+constexpr long long WAIT_LIMIT = 1ll << 24;   // polls (with back-off) before a wait gives up
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, int count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(unsigned long long *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(unsigned long long *bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait for the phase of `parity`; false if the limit ran out
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity) {
+    for (long long i = 0; i < WAIT_LIMIT; ++i) {
+        if (mbar_try(bar, parity)) return true;
+        if (i > 64) __nanosleep(64);
+    }
+    return false;
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *bar,
+                                         unsigned long long pol) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(pol)
+        : "memory");
+}
+__device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, %0;" ::"n"(TMA_CONSUMERS * 32) : "memory"); }
+
+__device__ double consumer_sum(double v, double *sh) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    v = warp_sum(v);
+    consumer_sync();
+    if (lane == 0) sh[wid] = v;
+    consumer_sync();
+    double s = 0.0;
+    for (int i = 0; i < TMA_CONSUMERS; ++i) s += sh[i];
+    consumer_sync();
+    return s;
+}
+
+struct StageMeta {
+    int item, k, cnt, flags;  // flags: 1 first chunk of the item, 2 last chunk
+};
+
+template <int PREC, int MODE>
+__global__ void __launch_bounds__((TMA_CONSUMERS + 1) * 32, 1)
+tile_symv_tma_kernel(TileSetDev ts, DevProblem P, const double *src, const double *src2, double *out, int slot,
+                     int nstages, int xs_elems) {
+    using Acc = typename TileT<PREC>::Acc;
+    constexpr int EPC = TileT<PREC>::EPC;
+    constexpr int CPR = TILE / EPC;
+    constexpr unsigned TILE_BYTES = TILE * TILE * (PREC == SCHUR_FP64 ? 8 : PREC == SCHUR_FP32 ? 4 : 2);
+    constexpr unsigned STAGE_BYTES = TMA_CONSUMERS * TILE_BYTES;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) unsigned long long full_bar[TMA_MAX_STAGES], empty_bar[TMA_MAX_STAGES];
+    __shared__ StageMeta meta[TMA_MAX_STAGES];
+    __shared__ double red[32];
+    __shared__ double s_beta;
+    __shared__ int s_last;
+
+    if (MODE != 0) {
+        const int iter = P.st->iter_base + slot;
+        if (skip_iter(P.st, iter)) return;
+        if (MODE == 3 && P.st->replace_iter != iter) return;
+        if (MODE == 1) {
+            if (threadIdx.x == 0) s_beta = (iter == 0) ? 0.0 : P.scal[SC_RHO] / P.rho_hist[iter - 1];
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned char *ring = smem_raw;
+    Acc *xs = reinterpret_cast<Acc *>(smem_raw + (size_t)nstages * STAGE_BYTES);
+    Acc *ys = xs + xs_elems;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < nstages; ++i) {
+            mbar_init(&full_bar[i], 1);
+            mbar_init(&empty_bar[i], TMA_CONSUMERS);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const double beta = (MODE == 1) ? s_beta : 0.0;
+
+    if (warp == TMA_CONSUMERS) {
+        // ---------------- producer: one lane issues the bulk copies
+        if (lane == 0) {
+            const unsigned long long pol = policy_evict_first();
+            const unsigned char *tiles = reinterpret_cast<const unsigned char *>(ts.tiles);
+            long long c = 0;          // chunk counter
+            long long last_c[TMA_MAX_STAGES];
+            for (int i = 0; i < TMA_MAX_STAGES; ++i) last_c[i] = -1;
+            bool ok = true;
+            for (;;) {
+                int item = atomicAdd(&ts.queue[0], 1);
+                int4 it = make_int4(0, 0, 0, 0);
+                if (item < ts.nitems) it = ts.items[item];
+                const int k0 = it.y, k1 = it.z;
+                const long long tbase = item < ts.nitems ? ts.mat_tile0[it.x] : 0;
+                int k = k0;
+                do {
+                    const int st = (int)(c % nstages);
+                    const long long round = c / nstages;
+                    if (round > 0 && !mbar_wait(&empty_bar[st], (unsigned)((round - 1) & 1))) { ok = false; break; }
+                    if (item >= ts.nitems) {
+                        meta[st] = StageMeta{-1, 0, 0, 0};
+                        mbar_arrive(&full_bar[st]);
+                        ++c;
+                        break;
+                    }
+                    const int cnt = min(TMA_CONSUMERS, k1 - k);
+                    meta[st] = StageMeta{item, k, cnt, (k == k0 ? 1 : 0) | (k + cnt == k1 ? 2 : 0)};
+                    mbar_arrive_tx(&full_bar[st], (unsigned)cnt * TILE_BYTES);
+                    bulk_g2s(ring + (size_t)st * STAGE_BYTES, tiles + (size_t)(tbase + k) * TILE_BYTES,
+                             (unsigned)cnt * TILE_BYTES, &full_bar[st], pol);
+                    last_c[st] = c;
+                    ++c;
+                    k += cnt;
+                } while (k < k1);
+                if (!ok || item >= ts.nitems) break;
+            }
+            if (!ok) {
+                atomicExch(&P.st->error, 1);
+                // drain: wait (bounded) for the copies this thread issued
+                for (int st = 0; st < nstages; ++st)
+                    if (last_c[st] >= 0) mbar_wait(&full_bar[st], (unsigned)((last_c[st] / nstages) & 1));
+            }
+        }
+    } else {
+        // ---------------- consumers
+        const int idx = EPC * (lane % CPR) + lane / CPR;
+        long long c = 0;
+        int curI = -1, item = -1, n = 0, voff = 0, whole = 0;
+        Acc racc = 0;
+        for (;;) {
+            const int st = (int)(c % nstages);
+            if (!mbar_wait(&full_bar[st], (unsigned)((c / nstages) & 1))) {
+                atomicExch(&P.st->error, 1);
+                break;
+            }
+            const StageMeta m = meta[st];
+            if (m.item < 0) break;
+            if (m.flags & 1) {
+                // new item: stage x, clear y (the previous item's epilogue ended with a barrier)
+                item = m.item;
+                const int4 it = ts.items[item];
+                n = ts.mat_n[it.x];
+                voff = ts.mat_voff[it.x];
+                const int tn = ts.mat_tn[it.x];
+                whole = (it.y == 0) && (it.z == tn * (tn + 1) / 2);
+                for (int i = threadIdx.x; i < TILE * tn; i += TMA_CONSUMERS * 32) {
+                    double v = 0.0;
+                    if (i < n) v = (MODE == 1) ? src[voff + i] + beta * src2[voff + i] : src[voff + i];
+                    xs[i] = (Acc)v;
+                    ys[i] = (Acc)0;
+                }
+                consumer_sync();
+                curI = -1;
+                racc = 0;
+            }
+            if (warp < m.cnt) {
+                const uint4 *tp = reinterpret_cast<const uint4 *>(ring + (size_t)st * STAGE_BYTES + (size_t)warp * TILE_BYTES);
+                uint4 raw[CPR];
+#pragma unroll
+                for (int q = 0; q < CPR; ++q) raw[q] = tp[q * 32 + lane];
+                tile_fma<PREC>(raw, ts, ts.mat_tile0[ts.items[item].x] + m.k + warp, xs, ys, lane, curI, racc);
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty_bar[st]);
+            ++c;
+            if (m.flags & 2) {
+                if (curI >= 0) atomicAdd(&ys[TILE * curI + idx], racc);
+                curI = -1;
+                racc = 0;
+                consumer_sync();
+                double dot = 0.0;
+                for (int i = threadIdx.x; i < n; i += TMA_CONSUMERS * 32) {
+                    const double yv = (double)ys[i];
+                    dot += (double)xs[i] * yv;
+                    if (whole) out[voff + i] = yv;
+                    else atomicAdd(&out[voff + i], yv);
+                }
+                dot = consumer_sum(dot, red);
+                if (threadIdx.x == 0 && ts.item_dot) ts.item_dot[item] = dot;
+            }
+        }
+    }
+    // the last CTA resets the work queue and (PCG loop) adds the item dot products in order
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
@@ -893,6 +1132,11 @@ struct GpuSolver::Impl {
     double *d_f = nullptr, *d_kf = nullptr, *d_g = nullptr, *d_rhs = nullptr, *d_sol = nullptr;
     double *h_pinned = nullptr;
     size_t h_pinned_n = 0;
+    // element data for the adjoint sensitivities
+    int *el_dofs = nullptr;
+    double *el_K = nullptr, *el_out = nullptr, *el_u = nullptr, *el_v = nullptr;
+    size_t el_count = 0;
+    int el_nd = 0, el_n = 0;
     double *e_dev = nullptr;
     int rho_cap = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -1108,9 +1352,37 @@ static size_t tile_smem(int prec, int max_tn) {
 void GpuSolver::Impl::launch_tiles(const TileSetHost &T, int mode, const double *src, const double *src2, double *out,
                                    int slot) {
     int mtn = (&T == &Dir) ? max_tn_dir : max_tn;
+    TileSetDev td = T.dev();
+    FETI_CHECK(mode != 1 || src2 != nullptr, "internal: PCG direction update without a previous direction");
+    if (opt.tile_kernel == 1) {
+        const size_t acc = T.prec == SCHUR_FP64 ? 8 : 4;
+        const size_t tile_bytes = (size_t)TILE * TILE * (T.prec == SCHUR_FP64 ? 8 : T.prec == SCHUR_FP32 ? 4 : 2);
+        const size_t stage = (size_t)TMA_CONSUMERS * tile_bytes;
+        const int xs_elems = TILE * mtn;
+        const size_t xbytes = 2 * acc * (size_t)xs_elems;
+        const size_t budget = 220 * 1024;
+        int nst = (int)std::min<size_t>(TMA_MAX_STAGES, (budget - std::min(budget, xbytes)) / stage);
+        FETI_CHECK(nst >= 2, "FETI4I: subdomain too large for the TMA tile pipeline");
+        const size_t sm = (size_t)nst * stage + xbytes;
+        const int grid = std::max(1, std::min(T.nitems, nsm));
+#define LAUNCHT(PR, MD) tile_symv_tma_kernel<PR, MD><<<grid, (TMA_CONSUMERS + 1) * 32, sm, stream>>>(td, P, src, src2, out, slot, nst, xs_elems)
+#define LAUNCHT_MODES(PR)                                  \
+    switch (mode) {                                        \
+    case 0: LAUNCHT(PR, 0); break;                         \
+    case 1: LAUNCHT(PR, 1); break;                         \
+    case 2: LAUNCHT(PR, 2); break;                         \
+    default: LAUNCHT(PR, 3); break;                        \
+    }
+        if (T.prec == SCHUR_FP64) { LAUNCHT_MODES(SCHUR_FP64) }
+        else if (T.prec == SCHUR_FP32) { LAUNCHT_MODES(SCHUR_FP32) }
+        else { LAUNCHT_MODES(SCHUR_BF16) }
+#undef LAUNCHT_MODES
+#undef LAUNCHT
+        CUDA_CHECK(cudaGetLastError());
+        return;
+    }
     size_t sm = tile_smem(T.prec, mtn);
     int grid = std::max(1, std::min(T.nitems, nsm * 2));
-    TileSetDev td = T.dev();
 #define LAUNCH(PR, MD) tile_symv_kernel<PR, MD><<<grid, 256, sm, stream>>>(td, P, src, src2, out, slot)
 #define LAUNCH_MODES(PR)                                   \
     switch (mode) {                                        \
@@ -1119,7 +1391,6 @@ void GpuSolver::Impl::launch_tiles(const TileSetHost &T, int mode, const double 
     case 2: LAUNCH(PR, 2); break;                          \
     default: LAUNCH(PR, 3); break;                         \
     }
-    FETI_CHECK(mode != 1 || src2 != nullptr, "internal: PCG direction update without a previous direction");
     if (T.prec == SCHUR_FP64) { LAUNCH_MODES(SCHUR_FP64) }
     else if (T.prec == SCHUR_FP32) { LAUNCH_MODES(SCHUR_FP32) }
     else { LAUNCH_MODES(SCHUR_BF16) }
@@ -1134,6 +1405,11 @@ static void set_tile_limits(int v) {
     cudaFuncSetAttribute(tile_symv_kernel<PR, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
     cudaFuncSetAttribute(tile_symv_kernel<PR, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
     cudaFuncSetAttribute(tile_symv_kernel<PR, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+    const int t = 225 * 1024;
+    cudaFuncSetAttribute(tile_symv_tma_kernel<PR, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, t);
+    cudaFuncSetAttribute(tile_symv_tma_kernel<PR, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, t);
+    cudaFuncSetAttribute(tile_symv_tma_kernel<PR, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, t);
+    cudaFuncSetAttribute(tile_symv_tma_kernel<PR, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, t);
 }
 
 static void set_smem_limits() {
@@ -1459,6 +1735,7 @@ void GpuSolver::solve(SolveStats &stats) {
     h.replacements = 0;
     h.max_it = I.opt.max_iterations;
     h.mixed = mixed ? 1 : 0;
+    h.error = 0;
     h.precision = I.opt.precision;
     h.delta = I.opt.reliable_delta;
     const int nd = P.nd;
@@ -1498,6 +1775,7 @@ void GpuSolver::solve(SolveStats &stats) {
     CUDA_CHECK(cudaEventRecord(I.ev1, I.stream));
     CUDA_CHECK(cudaMemcpyAsync(&hs, I.st, sizeof(hs), cudaMemcpyDeviceToHost, I.stream));
     CUDA_CHECK(cudaStreamSynchronize(I.stream));
+    FETI_CHECK(hs.error == 0, "FETI4I: a device pipeline wait timed out (solve aborted)");
     float ms = 0.f;
     CUDA_CHECK(cudaEventElapsedTime(&ms, I.ev0, I.ev1));
     stats.t_solve_ms = ms;
@@ -1721,6 +1999,66 @@ int tiled_symv_noalloc(const double *tiles, const long long *tile_offset, const 
                                                      y, dot, scr);
     CUDA_CHECK(cudaGetLastError());
     return 0;
+}
+
+}  // namespace feti
+
+// =============================================================================================
+// Element energies v_e^T K_e u_e (adjoint sensitivities d/drho_e of v^T K u)
+namespace feti {
+namespace {
+
+__global__ void element_energy_kernel(int ne, int nd, const int *dofs, const double *K, const double *u,
+                                      const double *v, double *out) {
+    const int lane = threadIdx.x & 31;
+    const int e = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (e >= ne) return;
+    const int *de = dofs + (size_t)e * nd;
+    const double *Ke = K + (size_t)e * nd * nd;
+    double acc = 0.0;
+    for (int a = 0; a < nd; ++a) {
+        // row a: lanes stride over the columns (coalesced), v_a * sum_b K_ab u_b
+        double s = 0.0;
+        for (int b = lane; b < nd; b += 32) s += Ke[(size_t)a * nd + b] * u[de[b]];
+        acc += v[de[a]] * s;
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) out[e] = acc;
+}
+
+}  // namespace
+
+void GpuSolver::element_energies(const ElementData &el, const double *u, const double *v, int n, double *out) {
+    Impl &I = *impl;
+    const size_t ne = el.nelem();
+    FETI_CHECK(ne > 0, "FETI4I: no elements");
+    const int nd = (int)(el.dof_ptr[1] - el.dof_ptr[0]);
+    for (size_t e = 0; e < ne; ++e)
+        FETI_CHECK(el.dof_ptr[e + 1] - el.dof_ptr[e] == nd, "FETI4I: element energies need elements of one size");
+    if (I.el_dofs == nullptr || I.el_count != ne || I.el_nd != nd) {
+        I.el_dofs = I.upload(el.dofs);
+        I.el_K = I.upload(el.vals);
+        I.el_out = I.alloc<double>(ne);
+        I.el_count = ne;
+        I.el_nd = nd;
+        I.el_n = 0;
+    }
+    if (I.el_n < n) {
+        I.el_u = I.alloc<double>(n);
+        I.el_v = I.alloc<double>(n);
+        I.el_n = n;
+    }
+    CUDA_CHECK(cudaMemcpyAsync(I.el_u, u, sizeof(double) * n, cudaMemcpyHostToDevice, I.stream));
+    CUDA_CHECK(cudaMemcpyAsync(I.el_v, v, sizeof(double) * n, cudaMemcpyHostToDevice, I.stream));
+    int maxdof = 0;
+    for (int d : el.dofs) maxdof = std::max(maxdof, d);
+    FETI_CHECK(maxdof < n, "FETI4I: element DOF outside the given vectors");
+    const int wpb = 8;
+    element_energy_kernel<<<(unsigned)((ne + wpb - 1) / wpb), 32 * wpb, 0, I.stream>>>((int)ne, nd, I.el_dofs, I.el_K,
+                                                                                      I.el_u, I.el_v, I.el_out);
+    CUDA_CHECK(cudaGetLastError());
+    CUDA_CHECK(cudaMemcpyAsync(out, I.el_out, sizeof(double) * ne, cudaMemcpyDeviceToHost, I.stream));
+    CUDA_CHECK(cudaStreamSynchronize(I.stream));
 }
 
 }  // namespace feti

@@ -24,6 +24,7 @@ struct SolveOptions {
     int schur_precision = SCHUR_FP64;  // storage of the iteration operator
     int chunk = 16;                    // iterations per captured CUDA graph
     int tiles_per_item = 48;           // work-queue granularity of the tile SYMV
+    int tile_kernel = 1;               // 0: register-prefetch SYMV, 1: TMA bulk-copy pipeline
     double reliable_delta = 0.1;       // residual replacement threshold (mixed precision)
     bool use_graph = true;
 };
@@ -60,6 +61,8 @@ public:
     // average device time of `reps` F applies (inputs resident), returns ms
     double time_F(int precision, int reps);
     double fapply_bytes(int precision) const;
+    // out[e] = v_e^T K_e u_e over the stored elements (u, v: caller DOF vectors of size n)
+    void element_energies(const ElementData &el, const double *u, const double *v, int n, double *out);
     size_t device_bytes() const;
     int device_id() const;
     void set_options(const SolveOptions &opt);

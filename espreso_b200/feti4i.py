@@ -22,11 +22,11 @@ PRECISION, REAL_OPTIONS_SIZE = 0, 1
 PREC_NONE, PREC_LUMPED, PREC_WEIGHT, PREC_DIRICHLET = 0, 1, 2, 3
 # extended options (include/feti4i_ext.h)
 EXT_SCHUR_PRECISION, EXT_SCALING, EXT_HOST_ONLY, EXT_TILES_PER_ITEM, EXT_GRAPH_CHUNK, EXT_RELIABLE_DELTA, \
-    EXT_HOST_THREADS = range(7)
+    EXT_HOST_THREADS, EXT_TILE_KERNEL = range(8)
 FP64, FP32, BF16 = 0, 1, 2
 STAT_NAMES = ["iterations", "converged", "dual_size", "kernel_size", "subdomains", "prep_seconds",
               "upload_seconds", "solve_ms", "solve_wall_ms", "fapply_bytes", "replacements",
-              "kernel_launches", "device_bytes", "final_norm", "tolerance"]
+              "kernel_launches", "device_bytes", "final_norm", "tolerance", "elements"]
 
 EXPORTED = [
     "FETI4ISetDefaultIntegerOptions", "FETI4ISetDefaultRealOptions", "FETI4ICreateStiffnessMatrix",
@@ -36,7 +36,7 @@ EXPORTED = [
     "FETI4IGetStats", "FETI4IGetDualSolution", "FETI4IGetSubdomainInfo", "FETI4IGetSubdomainMultipliers",
     "FETI4IGetSubdomainNodes", "FETI4IGetSubdomainSchur", "FETI4IGetSubdomainKernel", "FETI4IGetDualRhs",
     "FETI4IApplySubdomainKplus", "FETI4IApplyDualOperator", "FETI4ITimeDualOperator", "FETI4ISolveResident", "FETI4ISetSolvePrecision",
-    "FETI4ITiledSymvNoAlloc",
+    "FETI4ITiledSymvNoAlloc", "FETI4IElementEnergies",
 ]
 
 
@@ -87,6 +87,7 @@ def load(path: str = LIB_PATH):
         "FETI4ISolveResident": ([vp], f64),
         "FETI4ISetSolvePrecision": ([vp, i32], None),
         "FETI4ITiledSymvNoAlloc": ([vp, vp, vp, vp, i32, i32, vp, vp, vp, vp], i32),
+        "FETI4IElementEnergies": ([vp, i32, pd, pd, pd], None),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -306,6 +307,14 @@ class Instance:
         ms = self.lib.FETI4ITimeDualOperator(self.h, int(precision), int(reps))
         _check(self.lib)
         return ms
+
+    def element_energies(self, u, v):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        out = np.zeros(int(self.stats()["elements"]))
+        self.lib.FETI4IElementEnergies(self.h, u.size, _dp(u), _dp(v), _dp(out))
+        _check(self.lib)
+        return out
 
     def update_rhs(self, rhs):
         r = np.ascontiguousarray(rhs, dtype=np.float64)

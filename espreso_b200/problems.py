@@ -148,6 +148,23 @@ def elasticity_cube(clusters=(1, 1, 1), domains=(4, 4, 4), elements=(8, 8, 8), l
     return Problem(name, 3, coords, nodes, dom, Ke, fe, dirichlet, (clusters, domains, elements))
 
 
+def adjoint_cube(clusters=(1, 1, 1), domains=(8, 8, 8), elements=(12, 12, 12), length=(1.0, 1.0, 1.0),
+                 nu=0.3, seed=0, name="adjoint"):
+    """Adjoint workload: x=0 face clamped, unit point load at the centre node of the x=1 face (-z),
+    rho_e ~ U[0.3, 1] seeded.  Returns (problem with unit-modulus element matrices, rho, load vector)."""
+    P = elasticity_cube(clusters, domains, elements, length, E=1.0, nu=nu, body=(0.0, 0.0, 0.0), name=name)
+    rng = np.random.default_rng(seed)
+    gid = _grid_element_index(P.elem_nodes, P.coords, [c * d * e for c, d, e in zip(clusters, domains, elements)],
+                              [l / (c * d * e) for l, c, d, e in zip(length, clusters, domains, elements)])
+    rho = rng.uniform(0.3, 1.0, size=P.elem_nodes.shape[0])[gid]
+    face = np.nonzero(np.abs(P.coords[:, 0] - length[0]) < 1e-12)[0]
+    c = np.array([length[0], 0.5 * length[1], 0.5 * length[2]])
+    node = face[np.argmin(np.sum((P.coords[face] - c) ** 2, axis=1))]
+    f = np.zeros(P.ndofs)
+    f[3 * node + 2] = -1.0
+    return P, rho, f
+
+
 def heat_cube(clusters=(1, 1, 1), domains=(8, 8, 8), elements=(10, 10, 10), length=(1.0, 1.0, 1.0),
               k_range=(1.0, 100.0), source=1.0, seed=0, name="heat"):
     """Heat conduction, per-element conductivity log-uniform on k_range, T=0 on z=0, uniform source."""
@@ -196,6 +213,8 @@ def make_instance(problem: Problem, iopts=None, ropts=None, ext=None, batched=Tr
             F.set_extended(F.EXT_SCHUR_PRECISION, 0)
             F.set_extended(F.EXT_HOST_ONLY, 0)
             F.set_extended(F.EXT_SCALING, 1)
+            F.set_extended(F.EXT_TILE_KERNEL, 1)
+            F.set_extended(F.EXT_RELIABLE_DELTA, 0.1)
     return inst
 
 

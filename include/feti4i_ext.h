@@ -40,6 +40,7 @@ typedef enum {
     FETI4I_EXT_GRAPH_CHUNK,      /* PCG iterations per captured CUDA graph (default 16) */
     FETI4I_EXT_RELIABLE_DELTA,   /* mixed precision: residual replacement threshold (default 0.1) */
     FETI4I_EXT_HOST_THREADS,     /* OpenMP threads of the preprocessing (0: all) */
+    FETI4I_EXT_TILE_KERNEL,      /* Schur SYMV: 0 register-prefetch loads, 1 TMA bulk-copy pipeline (default) */
     FETI4I_EXT_OPTIONS_SIZE
 } FETI4IExtOptions;
 void FETI4ISetExtendedOption(FETI4IInt key, FETI4IReal value);
@@ -61,6 +62,7 @@ typedef enum {
     FETI4I_STAT_DEVICE_BYTES,
     FETI4I_STAT_FINAL_NORM,
     FETI4I_STAT_TOLERANCE,
+    FETI4I_STAT_ELEMENTS,           /* stored elements */
     FETI4I_STAT_SIZE
 } FETI4IStatIndex;
 void FETI4IGetStats(FETI4IInstance instance, FETI4IInt size, FETI4IReal *stats);
@@ -94,6 +96,15 @@ FETI4IReal FETI4ITimeDualOperator(FETI4IInstance instance, FETI4IInt precision, 
 FETI4IReal FETI4ISolveResident(FETI4IInstance instance);
 /* Select the operator precision of the following solves (must have been prepared). */
 void FETI4ISetSolvePrecision(FETI4IInstance instance, FETI4IInt precision);
+
+/* Element energies out[e] = v_e^T K_e u_e for every stored element (in the order
+ * they were added; elements skipped by the zero-row rule are not stored), with u
+ * and v caller DOF vectors of length size.  For an adjoint solve v (K v = dL/du,
+ * zero Dirichlet values) this gives dL/drho_e = -(dK_e/drho_e : ...) when K_e
+ * scales with a material parameter: dL/dp_e = -(dE_e/dp_e / E_e) * out[e].
+ * Computed on the GPU (no counterpart in the reference). */
+void FETI4IElementEnergies(FETI4IInstance instance, FETI4IInt size, const FETI4IReal *u, const FETI4IReal *v,
+                           FETI4IReal *out);
 
 /* Allocation-free batched SYMV: y_m = S_m x_m for m < nmatrices (no counterpart in
  * the reference).  For callers that manage all device memory themselves and may

@@ -20,9 +20,13 @@ from helpers import direct_u, oracle_problem, with_library_operators
 pytestmark = pytest.mark.gpu
 
 
-def gpu_instance(P, prec=F.PREC_LUMPED, precision=1e-10, schur=F.FP64, max_it=1000):
-    return problems.make_instance(P, iopts={F.PRECONDITIONER: prec, F.VERBOSE_LEVEL: 0, F.MAX_ITERATIONS: max_it},
-                                  ropts={F.PRECISION: precision}, ext={F.EXT_SCHUR_PRECISION: schur})
+def gpu_instance(P, prec=F.PREC_LUMPED, precision=1e-10, schur=F.FP64, max_it=1000, tile_kernel=1):
+    F.set_extended(F.EXT_TILE_KERNEL, tile_kernel)
+    try:
+        return problems.make_instance(P, iopts={F.PRECONDITIONER: prec, F.VERBOSE_LEVEL: 0, F.MAX_ITERATIONS: max_it},
+                                      ropts={F.PRECISION: precision}, ext={F.EXT_SCHUR_PRECISION: schur})
+    finally:
+        F.set_extended(F.EXT_TILE_KERNEL, 1)
 
 
 @pytest.fixture(scope="module")
@@ -35,9 +39,10 @@ def heat():
     return problems.heat_cube(domains=(4, 3, 3), elements=(5, 5, 5), seed=1)
 
 
+@pytest.mark.parametrize("tile_kernel", [0, 1])
 @pytest.mark.parametrize("schur,tol", [(F.FP64, 1e-13), (F.FP32, 1e-6), (F.BF16, 2e-2)])
-def test_fapply_parity(elast, schur, tol):
-    inst = gpu_instance(elast, schur=schur)
+def test_fapply_parity(elast, schur, tol, tile_kernel):
+    inst = gpu_instance(elast, schur=schur, tile_kernel=tile_kernel)
     OP = with_library_operators(oracle_problem(elast), inst)
     rng = np.random.default_rng(1)
     for _ in range(3):
@@ -74,9 +79,10 @@ def test_fapply_edge_sizes():
     inst.destroy()
 
 
-@pytest.mark.parametrize("prec", [OF.PREC_NONE, OF.PREC_LUMPED, OF.PREC_WEIGHT, OF.PREC_DIRICHLET])
-def test_solve_elasticity(elast, prec):
-    inst = gpu_instance(elast, prec=prec)
+@pytest.mark.parametrize("prec,tile_kernel", [(OF.PREC_NONE, 1), (OF.PREC_LUMPED, 1), (OF.PREC_WEIGHT, 1),
+                                               (OF.PREC_DIRICHLET, 1), (OF.PREC_LUMPED, 0), (OF.PREC_DIRICHLET, 0)])
+def test_solve_elasticity(elast, prec, tile_kernel):
+    inst = gpu_instance(elast, prec=prec, tile_kernel=tile_kernel)
     sol = inst.solve()
     st = inst.stats()
     assert st["converged"] == 1.0
@@ -104,12 +110,12 @@ def test_solve_heat_dirichlet(heat):
     inst.destroy()
 
 
-@pytest.mark.parametrize("schur", [F.FP32])
-def test_mixed_precision_reaches_fp64_accuracy(heat, schur):
+@pytest.mark.parametrize("schur,tile_kernel", [(F.FP32, 1), (F.FP32, 0)])
+def test_mixed_precision_reaches_fp64_accuracy(heat, schur, tile_kernel):
     """FP32 Schur storage inside FP64 residual replacement reaches the FP64 answer.
     (BF16 storage is a measured F-apply variant: its 8-bit mantissa makes the
     projected operator lose definiteness and the PCG diverges.)"""
-    inst = gpu_instance(heat, prec=F.PREC_LUMPED, schur=schur, precision=1e-10, max_it=3000)
+    inst = gpu_instance(heat, prec=F.PREC_LUMPED, schur=schur, precision=1e-10, max_it=3000, tile_kernel=tile_kernel)
     u = inst.solve().reshape(-1, 1)
     st = inst.stats()
     assert st["converged"] == 1.0
