@@ -42,7 +42,8 @@ def parse():
     ap.add_argument("--schur", default="fp32", choices=sorted(SCHUR))
     ap.add_argument("--precond", type=int, default=1)
     ap.add_argument("--precision", type=float, default=1e-8)
-    ap.add_argument("--tile-kernel", type=int, default=1, help="0 register prefetch, 1 TMA bulk pipeline")
+    ap.add_argument("--tile-kernel", type=int, default=-1,
+                    help="-1 autotuned (default), 0 register prefetch, 1 TMA bulk pipeline")
     ap.add_argument("--delta", type=float, default=0.1, help="residual replacement threshold")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -201,7 +202,9 @@ def run_ours(args):
     inst = problems.make_instance(P, iopts={F.PRECONDITIONER: args.precond, F.VERBOSE_LEVEL: 0,
                                             F.MAX_ITERATIONS: 5000},
                                   ropts={F.PRECISION: args.precision},
-                                  ext={F.EXT_SCHUR_PRECISION: SCHUR[args.schur], F.EXT_TILE_KERNEL: args.tile_kernel,
+                                  ext={F.EXT_SCHUR_PRECISION: SCHUR[args.schur],
+                                       F.EXT_TILE_KERNEL: max(0, args.tile_kernel),
+                                       F.EXT_AUTOTUNE: 1 if args.tile_kernel < 0 else 0,
                                        F.EXT_RELIABLE_DELTA: args.delta})
     setup_s = time.time() - t0
     st0 = inst.stats()
@@ -244,12 +247,14 @@ def run_ours(args):
     achieved = alg / (t_f * 1e-3) / 1e9
     peak, peak_kind = peaks()
     traffic = None
+    traffic_src = None
     tp = os.path.join(ROOT, "profiles", "fapply_traffic.json")
     if os.path.exists(tp):
         tj = json.load(open(tp))
         key = f"{args.config}:{args.schur}"
         if key in tj:
             traffic = tj[key]["dram_bytes_per_launch"]
+            traffic_src = tj[key]["source"]
     fp64_f = inst.time_F(0, 10)
     # CPU baseline: oracle port on the host cores (rank 0, N=1 only)
     cpu = None
@@ -269,7 +274,7 @@ def run_ours(args):
                    "parallelism": f"replicas{world}", "l2": "working set > L2 (Schur tiles "
                    f"{alg / 1e9:.2f} GB per apply, 126 MB L2)", "wall_ms_per_step": wall,
                    "setup_s": setup_s, "host_prep_s": st0["prep_seconds"],
-                   "tile_kernel": "tma_bulk_pipeline" if args.tile_kernel == 1 else "ldg_prefetch",
+                   "tuning": inst.tuning(),
                    "reliable_delta": args.delta},
         "fp64_gpu": {"ms": fp64_ms, "pcg_iterations": int(st64["iterations"]), "speedup_mixed": fp64_ms / step_ms,
                      "fapply_ms": fp64_f},
@@ -277,7 +282,8 @@ def run_ours(args):
         "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": int(rhs.nbytes),
                 "d2h_bytes_per_step": int(sol.nbytes)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "kernel": "tile_symv_kernel", "launch_ms": t_f, "peak_kind": peak_kind,
+                     "traffic": traffic, "traffic_source": traffic_src, "kernel": "tile_symv_kernel",
+                     "launch_ms": t_f, "peak_kind": peak_kind,
                      "alg_bytes_per_launch": alg},
         "cpu_baseline": cpu,
         "gpu_launches": launches,

@@ -55,7 +55,7 @@ namespace {
 std::mutex g_mutex;
 std::list<FETI4IStructMatrix *> g_matrices;
 std::list<FETI4IStructInstance *> g_instances;
-double g_ext[FETI4I_EXT_OPTIONS_SIZE] = {0, 1, 0, 48, 16, 0.1, 0, 1};
+double g_ext[FETI4I_EXT_OPTIONS_SIZE] = {0, 1, 0, 48, 16, 0.1, 0, 0, 1};
 
 template <typename F>
 void guarded(F &&f) {
@@ -127,6 +127,7 @@ void build(FETI4IStructInstance *I) {
     so.chunk = std::max(1, (int)I->ext[FETI4I_EXT_GRAPH_CHUNK]);
     so.reliable_delta = I->ext[FETI4I_EXT_RELIABLE_DELTA];
     so.tile_kernel = (int)I->ext[FETI4I_EXT_TILE_KERNEL];
+    so.autotune = I->ext[FETI4I_EXT_AUTOTUNE] != 0.0;
     I->gpu.reset();
     I->rhs_on_device = false;
     if (I->ext[FETI4I_EXT_HOST_ONLY] == 0.0) {
@@ -389,6 +390,16 @@ void FETI4IGetStats(FETI4IInstance instance, FETI4IInt size, FETI4IReal *stats) 
         v[FETI4I_STAT_ELEMENTS] = (double)I->el.nelem();
         for (int i = 0; i < size && i < FETI4I_STAT_SIZE; ++i) stats[i] = v[i];
     });
+}
+
+const char *FETI4IGetTuning(FETI4IInstance instance) {
+    static thread_local std::string t;
+    t.clear();
+    guarded([&] {
+        auto *I = check_instance(instance);
+        if (I->gpu) t = I->gpu->tuning();
+    });
+    return t.c_str();
 }
 
 void FETI4IGetDualSolution(FETI4IInstance instance, FETI4IReal *lambda, FETI4IReal *amplitudes) {

@@ -1085,6 +1085,8 @@ __global__ void primal_merge_kernel(DevProblem P, const int *doff, const int *ro
 }  // namespace
 
 // =============================================================================================
+constexpr int kSizeClasses = 5;
+
 struct TileSetHost {
     int prec = -1;
     int nitems = 0;
@@ -1098,6 +1100,10 @@ struct TileSetHost {
     float *scale = nullptr;
     double *item_dot = nullptr;
     int *queue = nullptr;
+    int kernel = 0;                 // 0 register prefetch, 1 TMA pipeline (autotuned)
+    std::vector<int> h_tn;          // tile rows per matrix (host copy for re-itemising)
+    long long total_tiles = 0;
+    std::vector<int> class_tpi;     // chosen tiles per item of each size class
     TileSetDev dev() const {
         TileSetDev t;
         t.nitems = nitems; t.prec = prec; t.items = items; t.mat_n = mat_n; t.mat_voff = mat_voff; t.mat_tn = mat_tn;
@@ -1167,6 +1173,8 @@ struct GpuSolver::Impl {
 
     void build_tiles(TileSetHost &T, int prec, const std::vector<const double *> &mats, const std::vector<int> &ns,
                      const std::vector<int> &voffs, int tiles_per_item);
+    void itemize(TileSetHost &T, const std::vector<int> &tpi, int only_class);
+    void autotune(TileSetHost &T, double *x, double *y, int ny);
     void launch_tiles(const TileSetHost &T, int mode, const double *src, const double *src2, double *out, int slot);
     void capture_chunk(int chunk);
     void launch_iteration(int slot);
@@ -1314,24 +1322,9 @@ void GpuSolver::Impl::build_tiles(TileSetHost &T, int prec, const std::vector<co
                     }
             }
     }
-    // work items: up to tiles_per_item tiles of one matrix; largest matrices first
-    std::vector<int> order(nm);
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return mt[a] > mt[b]; });
-    std::vector<int4> items;
-    for (int m : order) {
-        int nt = mt[m] * (mt[m] + 1) / 2;
-        int pieces = std::max(1, (nt + tiles_per_item - 1) / tiles_per_item);
-        for (int k = 0; k < pieces; ++k) {
-            int a = (int)((long long)nt * k / pieces), b = (int)((long long)nt * (k + 1) / pieces);
-            items.push_back(make_int4(m, a, b, 0));
-        }
-    }
     T.prec = prec;
-    T.nitems = (int)items.size();
     T.bytes = data.size();
     T.alg_bytes = alg;
-    T.items = upload(items);
     T.mat_n = upload(mn);
     T.mat_voff = upload(mv);
     T.mat_tn = upload(mt);
@@ -1339,9 +1332,92 @@ void GpuSolver::Impl::build_tiles(TileSetHost &T, int prec, const std::vector<co
     T.tile_ij = upload(ij);
     T.tiles = upload(data);
     T.scale = prec == SCHUR_BF16 ? upload(sc) : nullptr;
-    T.item_dot = alloc<double>(items.size());
+    T.h_tn = mt;
+    T.total_tiles = total;
+    // item buffers sized for the finest granularity (one tile per item)
+    T.items = alloc<int4>((size_t)total);
+    T.item_dot = alloc<double>((size_t)total);
     T.queue = alloc<int>(2);
     CUDA_CHECK(cudaMemset(T.queue, 0, 2 * sizeof(int)));
+    T.kernel = opt.tile_kernel;
+    T.class_tpi.assign(kSizeClasses, tiles_per_item);
+    itemize(T, T.class_tpi, -1);
+}
+
+// Size class of a matrix with tn tile rows (autotuning granularity).
+static int size_class(int tn) { return tn <= 8 ? 0 : tn <= 16 ? 1 : tn <= 32 ? 2 : tn <= 64 ? 3 : 4; }
+
+// Work items: per matrix, pieces of about tpi[class] tiles; largest matrices first.
+// only_class >= 0 restricts the list to one size class (autotuning).
+void GpuSolver::Impl::itemize(TileSetHost &T, const std::vector<int> &tpi, int only_class) {
+    const int nm = (int)T.h_tn.size();
+    std::vector<int> order(nm);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return T.h_tn[a] > T.h_tn[b]; });
+    std::vector<int4> items;
+    for (int m : order) {
+        const int cls = size_class(T.h_tn[m]);
+        if (only_class >= 0 && cls != only_class) continue;
+        const int nt = T.h_tn[m] * (T.h_tn[m] + 1) / 2;
+        const int per = std::max(1, tpi[cls]);
+        const int pieces = std::max(1, (nt + per - 1) / per);
+        for (int k = 0; k < pieces; ++k) {
+            int a = (int)((long long)nt * k / pieces), b = (int)((long long)nt * (k + 1) / pieces);
+            items.push_back(make_int4(m, a, b, 0));
+        }
+    }
+    T.nitems = (int)items.size();
+    if (!items.empty())
+        CUDA_CHECK(cudaMemcpy(T.items, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));
+}
+
+// Autotuner: for each kernel variant and size class, time class-only applies over
+// candidate item granularities; keep the fastest (variant, per-class granularity).
+void GpuSolver::Impl::autotune(TileSetHost &T, double *x, double *y, int ny) {
+    const int cands[] = {16, 48, 128, 384, 1 << 20};
+    std::vector<int> present(kSizeClasses, 0);
+    for (int tn : T.h_tn) present[size_class(tn)] = 1;
+    cudaEvent_t a, b;
+    CUDA_CHECK(cudaEventCreate(&a));
+    CUDA_CHECK(cudaEventCreate(&b));
+    auto time_launch = [&](int reps) {
+        for (int i = 0; i < 2; ++i) launch_tiles(T, 0, x, nullptr, y, 0);
+        CUDA_CHECK(cudaEventRecord(a, stream));
+        for (int i = 0; i < reps; ++i) launch_tiles(T, 0, x, nullptr, y, 0);
+        CUDA_CHECK(cudaEventRecord(b, stream));
+        CUDA_CHECK(cudaEventSynchronize(b));
+        float ms = 0.f;
+        CUDA_CHECK(cudaEventElapsedTime(&ms, a, b));
+        return ms / reps;
+    };
+    double best_total = 1e30;
+    int best_kernel = T.kernel;
+    std::vector<int> best_tpi = T.class_tpi;
+    for (int kern = 0; kern < 2; ++kern) {
+        T.kernel = kern;
+        std::vector<int> tpi = T.class_tpi;
+        double total = 0.0;
+        for (int c = 0; c < kSizeClasses; ++c) {
+            if (!present[c]) continue;
+            double bt = 1e30;
+            for (int cand : cands) {
+                std::vector<int> t = tpi;
+                t[c] = cand;
+                itemize(T, t, c);
+                double ms = time_launch(5);
+                if (ms < bt) { bt = ms; tpi[c] = cand; }
+            }
+            total += bt;
+        }
+        if (total < best_total) { best_total = total; best_kernel = kern; best_tpi = tpi; }
+    }
+    T.kernel = best_kernel;
+    T.class_tpi = best_tpi;
+    itemize(T, T.class_tpi, -1);
+    CUDA_CHECK(cudaMemsetAsync(y, 0, sizeof(double) * ny, stream));
+    CUDA_CHECK(cudaStreamSynchronize(stream));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
 }
 
 static size_t tile_smem(int prec, int max_tn) {
@@ -1354,7 +1430,7 @@ void GpuSolver::Impl::launch_tiles(const TileSetHost &T, int mode, const double 
     int mtn = (&T == &Dir) ? max_tn_dir : max_tn;
     TileSetDev td = T.dev();
     FETI_CHECK(mode != 1 || src2 != nullptr, "internal: PCG direction update without a previous direction");
-    if (opt.tile_kernel == 1) {
+    if (T.kernel == 1) {
         const size_t acc = T.prec == SCHUR_FP64 ? 8 : 4;
         const size_t tile_bytes = (size_t)TILE * TILE * (T.prec == SCHUR_FP64 ? 8 : T.prec == SCHUR_FP32 ? 4 : 2);
         const size_t stage = (size_t)TMA_CONSUMERS * tile_bytes;
@@ -1671,8 +1747,29 @@ void GpuSolver::upload(const Decomposition &dec, const Prep &prep, const SolveOp
         FETI_CHECK(tile_smem(SCHUR_FP64, I.max_tn_dir) <= 200 * 1024, "FETI4I: a Dirichlet block is too large for the tile kernel");
         I.build_tiles(I.Dir, SCHUR_FP64, dm, dn, dv, opt.tiles_per_item);
     }
+    if (opt.autotune) {
+        CUDA_CHECK(cudaMemset(P.w, 0, sizeof(double) * NL));
+        I.autotune(I.F64, P.w, I.Ax64, NL);
+        if (opt.schur_precision != SCHUR_FP64) I.autotune(I.Flow, P.w, I.Ax64, NL);
+        if (opt.precond == PREC_DIRICHLET) {
+            CUDA_CHECK(cudaMemset(P.uT, 0, sizeof(double) * NT));
+            I.autotune(I.Dir, P.uT, P.vT, NT);
+        }
+    }
     I.upload_kplus(dec, prep, loff, toff);
     CUDA_CHECK(cudaDeviceSynchronize());
+}
+
+std::string GpuSolver::tuning() const {
+    auto one = [](const char *name, const TileSetHost &T) {
+        std::string s = std::string(name) + ":" + (T.kernel ? "tma" : "ldg") + "[";
+        for (size_t c = 0; c < T.class_tpi.size(); ++c) s += (c ? "," : "") + std::to_string(T.class_tpi[c]);
+        return s + "]";
+    };
+    std::string s = one("f64", impl->F64);
+    if (impl->Flow.prec >= 0) s += " " + one("low", impl->Flow);
+    if (impl->Dir.prec >= 0) s += " " + one("dir", impl->Dir);
+    return s;
 }
 
 void GpuSolver::solve_full(const double *rhs, int rhs_size, double *solution, int solution_size, SolveStats &stats,

@@ -24,7 +24,8 @@ struct SolveOptions {
     int schur_precision = SCHUR_FP64;  // storage of the iteration operator
     int chunk = 16;                    // iterations per captured CUDA graph
     int tiles_per_item = 48;           // work-queue granularity of the tile SYMV
-    int tile_kernel = 1;               // 0: register-prefetch SYMV, 1: TMA bulk-copy pipeline
+    int tile_kernel = 0;               // 0: register-prefetch SYMV, 1: TMA bulk-copy pipeline
+    bool autotune = true;              // time the variants and item granularities per size class at upload
     double reliable_delta = 0.1;       // residual replacement threshold (mixed precision)
     bool use_graph = true;
 };
@@ -66,6 +67,7 @@ public:
     size_t device_bytes() const;
     int device_id() const;
     void set_options(const SolveOptions &opt);
+    std::string tuning() const;        // chosen SYMV variant and granularities
 
     struct Impl;
     Impl *impl;

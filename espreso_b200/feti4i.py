@@ -22,7 +22,7 @@ PRECISION, REAL_OPTIONS_SIZE = 0, 1
 PREC_NONE, PREC_LUMPED, PREC_WEIGHT, PREC_DIRICHLET = 0, 1, 2, 3
 # extended options (include/feti4i_ext.h)
 EXT_SCHUR_PRECISION, EXT_SCALING, EXT_HOST_ONLY, EXT_TILES_PER_ITEM, EXT_GRAPH_CHUNK, EXT_RELIABLE_DELTA, \
-    EXT_HOST_THREADS, EXT_TILE_KERNEL = range(8)
+    EXT_HOST_THREADS, EXT_TILE_KERNEL, EXT_AUTOTUNE = range(9)
 FP64, FP32, BF16 = 0, 1, 2
 STAT_NAMES = ["iterations", "converged", "dual_size", "kernel_size", "subdomains", "prep_seconds",
               "upload_seconds", "solve_ms", "solve_wall_ms", "fapply_bytes", "replacements",
@@ -36,7 +36,7 @@ EXPORTED = [
     "FETI4IGetStats", "FETI4IGetDualSolution", "FETI4IGetSubdomainInfo", "FETI4IGetSubdomainMultipliers",
     "FETI4IGetSubdomainNodes", "FETI4IGetSubdomainSchur", "FETI4IGetSubdomainKernel", "FETI4IGetDualRhs",
     "FETI4IApplySubdomainKplus", "FETI4IApplyDualOperator", "FETI4ITimeDualOperator", "FETI4ISolveResident", "FETI4ISetSolvePrecision",
-    "FETI4ITiledSymvNoAlloc", "FETI4IElementEnergies",
+    "FETI4ITiledSymvNoAlloc", "FETI4IElementEnergies", "FETI4IGetTuning",
 ]
 
 
@@ -88,6 +88,7 @@ def load(path: str = LIB_PATH):
         "FETI4ISetSolvePrecision": ([vp, i32], None),
         "FETI4ITiledSymvNoAlloc": ([vp, vp, vp, vp, i32, i32, vp, vp, vp, vp], i32),
         "FETI4IElementEnergies": ([vp, i32, pd, pd, pd], None),
+        "FETI4IGetTuning": ([vp], C.c_char_p),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -307,6 +308,11 @@ class Instance:
         ms = self.lib.FETI4ITimeDualOperator(self.h, int(precision), int(reps))
         _check(self.lib)
         return ms
+
+    def tuning(self):
+        t = self.lib.FETI4IGetTuning(self.h)
+        _check(self.lib)
+        return t.decode()
 
     def element_energies(self, u, v):
         u = np.ascontiguousarray(u, dtype=np.float64)

@@ -213,7 +213,8 @@ def make_instance(problem: Problem, iopts=None, ropts=None, ext=None, batched=Tr
             F.set_extended(F.EXT_SCHUR_PRECISION, 0)
             F.set_extended(F.EXT_HOST_ONLY, 0)
             F.set_extended(F.EXT_SCALING, 1)
-            F.set_extended(F.EXT_TILE_KERNEL, 1)
+            F.set_extended(F.EXT_TILE_KERNEL, 0)
+            F.set_extended(F.EXT_AUTOTUNE, 1)
             F.set_extended(F.EXT_RELIABLE_DELTA, 0.1)
     return inst
 

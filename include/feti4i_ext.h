@@ -40,7 +40,8 @@ typedef enum {
     FETI4I_EXT_GRAPH_CHUNK,      /* PCG iterations per captured CUDA graph (default 16) */
     FETI4I_EXT_RELIABLE_DELTA,   /* mixed precision: residual replacement threshold (default 0.1) */
     FETI4I_EXT_HOST_THREADS,     /* OpenMP threads of the preprocessing (0: all) */
-    FETI4I_EXT_TILE_KERNEL,      /* Schur SYMV: 0 register-prefetch loads, 1 TMA bulk-copy pipeline (default) */
+    FETI4I_EXT_TILE_KERNEL,      /* Schur SYMV: 0 register-prefetch loads, 1 TMA bulk-copy pipeline */
+    FETI4I_EXT_AUTOTUNE,         /* 1 (default): time both SYMV variants and the work-item sizes per size class */
     FETI4I_EXT_OPTIONS_SIZE
 } FETI4IExtOptions;
 void FETI4ISetExtendedOption(FETI4IInt key, FETI4IReal value);
@@ -66,6 +67,10 @@ typedef enum {
     FETI4I_STAT_SIZE
 } FETI4IStatIndex;
 void FETI4IGetStats(FETI4IInstance instance, FETI4IInt size, FETI4IReal *stats);
+
+/* Result of the SYMV autotuner of an instance, e.g. "f64:ldg[48,48,128,..] low:tma[..]"
+ * (pointer valid until the next call on this thread). */
+const char *FETI4IGetTuning(FETI4IInstance instance);
 
 /* Dual solution lambda (dual size) and rigid-body amplitudes (kernel size) of the last solve. */
 void FETI4IGetDualSolution(FETI4IInstance instance, FETI4IReal *lambda, FETI4IReal *amplitudes);

@@ -20,13 +20,13 @@ from helpers import direct_u, oracle_problem, with_library_operators
 pytestmark = pytest.mark.gpu
 
 
-def gpu_instance(P, prec=F.PREC_LUMPED, precision=1e-10, schur=F.FP64, max_it=1000, tile_kernel=1):
-    F.set_extended(F.EXT_TILE_KERNEL, tile_kernel)
-    try:
-        return problems.make_instance(P, iopts={F.PRECONDITIONER: prec, F.VERBOSE_LEVEL: 0, F.MAX_ITERATIONS: max_it},
-                                      ropts={F.PRECISION: precision}, ext={F.EXT_SCHUR_PRECISION: schur})
-    finally:
-        F.set_extended(F.EXT_TILE_KERNEL, 1)
+def gpu_instance(P, prec=F.PREC_LUMPED, precision=1e-10, schur=F.FP64, max_it=1000, tile_kernel=None):
+    """tile_kernel None: autotuned; 0/1: that SYMV variant, autotuner off."""
+    ext = {F.EXT_SCHUR_PRECISION: schur}
+    if tile_kernel is not None:
+        ext.update({F.EXT_TILE_KERNEL: tile_kernel, F.EXT_AUTOTUNE: 0})
+    return problems.make_instance(P, iopts={F.PRECONDITIONER: prec, F.VERBOSE_LEVEL: 0, F.MAX_ITERATIONS: max_it},
+                                  ropts={F.PRECISION: precision}, ext=ext)
 
 
 @pytest.fixture(scope="module")
@@ -69,7 +69,7 @@ def test_fapply_edge_sizes():
     from espreso_b200.feti4i import EXT_TILES_PER_ITEM, set_extended
     set_extended(EXT_TILES_PER_ITEM, 7)
     try:
-        inst = gpu_instance(P)
+        inst = gpu_instance(P, tile_kernel=1)
     finally:
         set_extended(EXT_TILES_PER_ITEM, 48)
     OP = with_library_operators(oracle_problem(P), inst)
