@@ -48,6 +48,7 @@ struct FETI4IStructInstance {
     std::vector<double> b, e, lambda, alpha;
     double t_prep = 0.0, t_upload = 0.0, t_solve_wall = 0.0;
     bool rhs_on_device = false;
+    int multi_on_device = 0;
 };
 
 namespace {
@@ -272,6 +273,30 @@ void FETI4ISolve(FETI4IInstance instance, FETI4IInt solution_size, FETI4IReal *s
                  I->stats.converged ? "converged" : "stopped", I->stats.iterations, I->stats.final_norm, I->stats.tol,
                  I->stats.t_solve_ms);
     });
+}
+
+void FETI4ISolveMulti(FETI4IInstance instance, FETI4IInt nrhs, FETI4IInt size, const FETI4IReal *rhs,
+                      FETI4IReal *solutions) {
+    guarded([&] {
+        auto *I = check_instance(instance);
+        FETI_CHECK(I->gpu, "FETI4I: instance was created with FETI4I_EXT_HOST_ONLY; no device solver");
+        FETI_CHECK(rhs && solutions && size > 0, "FETI4ISolveMulti: invalid arrays");
+        double t0 = now_s();
+        I->gpu->solve_multi(rhs, nrhs, size, solutions, size, I->stats, true);
+        I->t_solve_wall = (now_s() - t0) * 1e3;
+        I->multi_on_device = nrhs;
+    });
+}
+
+FETI4IReal FETI4ISolveMultiResident(FETI4IInstance instance, FETI4IInt nrhs) {
+    double ms = -1.0;
+    guarded([&] {
+        auto *I = check_instance(instance);
+        FETI_CHECK(I->gpu && I->multi_on_device == nrhs, "FETI4ISolveMultiResident: call FETI4ISolveMulti first");
+        I->gpu->solve_multi(nullptr, nrhs, 0, nullptr, 0, I->stats, false);
+        ms = I->stats.t_solve_ms;
+    });
+    return ms;
 }
 
 FETI4IReal FETI4ISolveResident(FETI4IInstance instance) {

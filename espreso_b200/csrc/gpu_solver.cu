@@ -87,6 +87,22 @@ struct DevProblem {
 };
 
 enum { SC_RHO = 0, SC_PAP = 1, SC_WN2 = 2, SC_BN2 = 3, SC_PN2 = 4, SC_COUNT = 8 };
+
+// block (multi right-hand-side) solver vectors: [row][rhs]
+struct BlockDev {
+    int nr;              // right-hand sides (power of two <= 32)
+    double *x, *r, *w, *z, *y, *p, *Ap, *Ax, *bL, *uT, *vT, *d, *alpha, *e;
+    float *p32;          // FP32 copy of p (SYMM input in mixed precision)
+    double *part;        // nd * nr partials
+    double *unit_dot;    // SYMM work units * nr
+    double *scal;        // SC_COUNT * nr
+    double *rho_hist;    // (max_it + 64) * nr
+    double *tol, *rmax, *last_norm;  // nr
+    int *conv;           // nr: iteration whose stop test passed, -1
+    int *done;           // DONE_COUNT counters
+    int *queue;          // SYMM work queue [2]
+    int n_conv_target;
+};
 enum { DONE_W = 0, DONE_RHO = 1, DONE_B = 2, DONE_PN = 3, DONE_COUNT = 8 };
 
 struct TileSetDev {
@@ -1138,6 +1154,20 @@ struct GpuSolver::Impl {
     double *d_f = nullptr, *d_kf = nullptr, *d_g = nullptr, *d_rhs = nullptr, *d_sol = nullptr;
     double *h_pinned = nullptr;
     size_t h_pinned_n = 0;
+    // block (multi right-hand-side) solver
+    struct Block {
+        int nr = 0;
+        BlockDev B{};
+        int2 *units = nullptr;
+        int nunits = 0;
+        cudaGraphExec_t graph = nullptr;
+        int graph_chunk = 0, graph_prec = -1, graph_precond = -1;
+        double *rhs = nullptr, *sol = nullptr, *f = nullptr, *kf = nullptr, *g = nullptr;
+    } blk;
+    void ensure_block(int nr);
+    void launch_symm(const TileSetHost &T, bool src32, const double *x64, const float *x32, double *out, int slot,
+                     int mode);
+    void launch_block_iteration(int slot);
     // element data for the adjoint sensitivities
     int *el_dofs = nullptr;
     double *el_K = nullptr, *el_out = nullptr, *el_u = nullptr, *el_v = nullptr;
@@ -1163,6 +1193,7 @@ struct GpuSolver::Impl {
         return p;
     }
     ~Impl() {
+        if (blk.graph) cudaGraphExecDestroy(blk.graph);
         if (h_pinned) cudaFreeHost(h_pinned);
         if (graph) cudaGraphExecDestroy(graph);
         for (void *p : allocs) cudaFree(p);
@@ -2156,6 +2187,737 @@ void GpuSolver::element_energies(const ElementData &el, const double *u, const d
     CUDA_CHECK(cudaGetLastError());
     CUDA_CHECK(cudaMemcpyAsync(out, I.el_out, sizeof(double) * ne, cudaMemcpyDeviceToHost, I.stream));
     CUDA_CHECK(cudaStreamSynchronize(I.stream));
+}
+
+}  // namespace feti
+
+// =============================================================================================
+// Block (multi right-hand-side) dual PCG: nr load cases solved together.
+// Vectors are [row][rhs] (nr consecutive values per local row); scalars and
+// stop tests are per right-hand side; the F apply is a tile SYMM.
+namespace feti {
+namespace {
+
+
+
+// per-column sum over a CTA: threads with the same column (tid % nr) are combined
+__device__ void block_sum_cols(double v, int nr, double *sh /* >= 8*32 */, double *out_col /* nr */) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int o = 16; o >= nr; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    __syncthreads();
+    if (lane < nr) sh[wid * 32 + lane] = v;
+    __syncthreads();
+    if (threadIdx.x < nr) {
+        double s = 0.0;
+        for (int i = 0; i < nw; ++i) s += sh[i * 32 + threadIdx.x];
+        out_col[threadIdx.x] = s;
+    }
+    __syncthreads();
+}
+
+// last-CTA total of per-CTA column partials (partials[cta * nr + j]) into out[j]
+__device__ void grid_total_cols(const double *mine /* nr, shared */, double *partials, int nr, int *counter,
+                                double *out) {
+    __shared__ int s_last;
+    __syncthreads();
+    if (threadIdx.x < nr) partials[blockIdx.x * nr + threadIdx.x] = mine[threadIdx.x];
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = (atomicAdd(counter, 1) == (int)gridDim.x - 1);
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        if (threadIdx.x < nr) {
+            double t = 0.0;
+            for (int c = 0; c < (int)gridDim.x; ++c) t += __ldcg(&partials[c * nr + threadIdx.x]);
+            out[threadIdx.x] = t;
+        }
+        if (threadIdx.x == 0) *counter = 0;
+    }
+}
+
+// G_i v per column, v[(e - e0) * nr + j] (rows of the subdomain, written by this CTA)
+__device__ void g_dot_cols(const DevProblem &P, const BlockDev &B, int dsub, const double *v, double *sh) {
+    const int nr = B.nr;
+    const int e0 = P.loff[dsub], e1 = P.loff[dsub + 1];
+    const int nk = P.kof[dsub + 1] - P.kof[dsub];
+    for (int k = 0; k < nk; ++k) {
+        double s = 0.0;
+        for (int i = threadIdx.x; i < (e1 - e0) * nr; i += blockDim.x) s += P.Gl[(size_t)(e0 + i / nr) * P.KS + k] * v[i];
+        __shared__ double cols[32];
+        block_sum_cols(s, nr, sh, cols);
+        if (threadIdx.x < nr) B.d[(size_t)(P.kof[dsub] + k) * nr + threadIdx.x] = cols[threadIdx.x];
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ double gt_alpha_col(const DevProblem &P, int e, int j, int nr, const double *a) {
+    double s = 0.0;
+    const int nk = P.rnk[e], ko = P.rkof[e], pn = P.pnk[e], po = P.pkof[e];
+    const double *g = P.Gl + (size_t)e * P.KS, *gp = P.Gp + (size_t)e * P.KS;
+    for (int k = 0; k < nk; ++k) s += g[k] * a[(size_t)(ko + k) * nr + j];
+    for (int k = 0; k < pn; ++k) s += gp[k] * a[(size_t)(po + k) * nr + j];
+    return s;
+}
+
+// conv[j]: -1 running, -2 zero right-hand side (frozen from the start), >= 0 stop iteration
+__device__ __forceinline__ bool col_frozen(const BlockDev &B, int j, int iter) {
+    const int c = B.conv[j];
+    return c == -2 || (c >= 0 && iter > c);
+}
+
+__global__ void bcoarse_kernel(DevProblem P, BlockDev B, const double *in, double *out, int slot, int looped) {
+    if (looped && skip_iter(P.st, P.st->iter_base + slot)) return;
+    const int nr = B.nr;
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= P.nK) return;
+    const double *col = P.GGtinv + (size_t)row * P.nK;
+    double acc[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) acc[j] = 0.0;
+    for (int b = lane; b < P.nK; b += 32) {
+        const double m = col[b];
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+            if (j < nr) acc[j] += m * in[(size_t)b * nr + j];
+    }
+#pragma unroll
+    for (int j = 0; j < 32; ++j)
+        if (j < nr) {
+            double s = warp_sum(acc[j]);
+            if (lane == 0) out[(size_t)row * nr + j] = s;
+        }
+}
+
+__global__ void bgt_kernel(DevProblem P, BlockDev B, const double *a, double *xout) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < P.NL * B.nr) xout[i] = gt_alpha_col(P, i / B.nr, i % B.nr, B.nr, a);
+}
+
+// r = b - assemble(Ax), d = G r, |b_j|^2 totals (initial) / replacement
+__global__ void br0_kernel(DevProblem P, BlockDev B, int replace_mode, int slot) {
+    __shared__ double sh[8 * 32];
+    __shared__ double cols[32];
+    if (replace_mode) {
+        const int iter = P.st->iter_base + slot;
+        if (skip_iter(P.st, iter) || P.st->replace_iter != iter) return;
+    }
+    const int nr = B.nr, dsub = blockIdx.x;
+    const int e0 = P.loff[dsub], e1 = P.loff[dsub + 1];
+    double bb = 0.0;
+    for (int i = threadIdx.x; i < (e1 - e0) * nr; i += blockDim.x) {
+        const int e = e0 + i / nr, j = i % nr;
+        const int q = P.partner[e];
+        const size_t o = (size_t)e * nr + j;
+        const double a = B.Ax[o] + (q >= 0 ? B.Ax[(size_t)q * nr + j] : 0.0);
+        const double rv = B.bL[o] - a;
+        B.r[o] = rv;
+        bb += B.bL[o] * B.bL[o] * P.minv[e];
+    }
+    __syncthreads();
+    g_dot_cols(P, B, dsub, B.r + (size_t)e0 * nr, sh);
+    if (!replace_mode) {
+        block_sum_cols(bb, nr, sh, cols);
+        grid_total_cols(cols, B.part, nr, B.done + DONE_B, B.scal + SC_BN2 * nr);
+    }
+}
+
+__global__ void bpnorm_kernel(DevProblem P, BlockDev B) {
+    __shared__ double sh[8 * 32];
+    __shared__ double cols[32];
+    const int nr = B.nr, dsub = blockIdx.x;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < (P.loff[dsub + 1] - P.loff[dsub]) * nr; i += blockDim.x) {
+        const int e = P.loff[dsub] + i / nr, j = i % nr;
+        const double u = B.r[(size_t)e * nr + j] - gt_alpha_col(P, e, j, nr, B.alpha);
+        s += u * u * P.minv[e];
+    }
+    block_sum_cols(s, nr, sh, cols);
+    grid_total_cols(cols, B.part, nr, B.done + DONE_PN, B.scal + SC_PN2 * nr);
+}
+
+__global__ void btol_kernel(DevProblem P, BlockDev B) {
+    const int j = threadIdx.x;
+    if (j < B.nr) {
+        const double un = sqrt(B.scal[SC_PN2 * B.nr + j]), bn = sqrt(B.scal[SC_BN2 * B.nr + j]);
+        B.tol[j] = P.st->precision * fmin(un, bn);
+        B.rmax[j] = un;
+        B.conv[j] = (bn == 0.0 || un == 0.0) ? -2 : -1;
+    }
+}
+
+// w = r - G^T alpha, |w_j|^2; u_T = B^T W w; lumped v_T = K_TT u_T (columns)
+template <int PRECOND>
+__global__ void bw_prec_kernel(DevProblem P, BlockDev B, int slot) {
+    __shared__ double sh[8 * 32];
+    __shared__ double cols[32];
+    const int iter = P.st->iter_base + slot;
+    if (skip_iter(P.st, iter)) return;
+    const int nr = B.nr, dsub = blockIdx.x;
+    const int e0 = P.loff[dsub], e1 = P.loff[dsub + 1];
+    double ww = 0.0;
+    for (int i = threadIdx.x; i < (e1 - e0) * nr; i += blockDim.x) {
+        const int e = e0 + i / nr, j = i % nr;
+        const size_t o = (size_t)e * nr + j;
+        const double wv = B.r[o] - gt_alpha_col(P, e, j, nr, B.alpha);
+        B.w[o] = wv;
+        if (PRECOND == PREC_NONE) B.y[o] = wv;
+        ww += wv * wv * P.minv[e];
+    }
+    block_sum_cols(ww, nr, sh, cols);
+    grid_total_cols(cols, B.part, nr, B.done + DONE_W, B.scal + SC_WN2 * nr);
+    if (PRECOND == PREC_NONE) {
+        grid_total_cols(cols, B.part + (size_t)P.nd * nr, nr, B.done + DONE_RHO, B.scal + SC_RHO * nr);
+        return;
+    }
+    __syncthreads();
+    const int t0 = P.toff[dsub], nt = P.toff[dsub + 1] - t0;
+    for (int i = threadIdx.x; i < nt * nr; i += blockDim.x) {
+        const int t = i / nr, j = i % nr;
+        double s = 0.0;
+        for (int q = P.trow_ptr[t0 + t]; q < P.trow_ptr[t0 + t + 1]; ++q) {
+            const int e = P.trow_idx[q];
+            s += P.ws[e] * B.w[(size_t)e * nr + j];
+        }
+        B.uT[(size_t)(t0 + t) * nr + j] = s;
+        if (PRECOND == PREC_WEIGHT) B.vT[(size_t)(t0 + t) * nr + j] = s;
+    }
+    if (PRECOND != PREC_LUMPED) return;
+    __syncthreads();
+    const int sl0 = P.slice0[dsub];
+    for (int i = threadIdx.x; i < nt * nr; i += blockDim.x) {
+        const int t = i / nr, j = i % nr;
+        const int sl = sl0 + (t >> 5), ln = t & 31;
+        const int base = P.ell_ptr[sl], wd = P.ell_w[sl];
+        double s = 0.0;
+        for (int q = 0; q < wd; ++q) {
+            const int o = base + q * 32 + ln;
+            s += P.ell_val[o] * B.uT[(size_t)(t0 + P.ell_col[o]) * nr + j];
+        }
+        B.vT[(size_t)(t0 + t) * nr + j] = s;
+    }
+}
+
+__global__ void bz_kernel(DevProblem P, BlockDev B, int slot) {
+    __shared__ double sh[8 * 32];
+    const int iter = P.st->iter_base + slot;
+    if (skip_iter(P.st, iter)) return;
+    const int nr = B.nr, dsub = blockIdx.x;
+    const int e0 = P.loff[dsub], e1 = P.loff[dsub + 1];
+    for (int i = threadIdx.x; i < (e1 - e0) * nr; i += blockDim.x) {
+        const int e = e0 + i / nr, j = i % nr;
+        const int pt = P.ptidx[e];
+        double zv = P.ws[e] * B.vT[(size_t)P.tidx[e] * nr + j];
+        if (pt >= 0) zv += P.pws[e] * B.vT[(size_t)pt * nr + j];
+        B.z[(size_t)e * nr + j] = zv;
+    }
+    __syncthreads();
+    g_dot_cols(P, B, dsub, B.z + (size_t)e0 * nr, sh);
+}
+
+// y = z - G^T alpha, rho_j = y.w; clear the SYMM accumulators (not needed: rows written once)
+__global__ void by_kernel(DevProblem P, BlockDev B, int slot) {
+    __shared__ double sh[8 * 32];
+    __shared__ double cols[32];
+    const int iter = P.st->iter_base + slot;
+    if (skip_iter(P.st, iter)) return;
+    const int nr = B.nr, dsub = blockIdx.x;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < (P.loff[dsub + 1] - P.loff[dsub]) * nr; i += blockDim.x) {
+        const int e = P.loff[dsub] + i / nr, j = i % nr;
+        const size_t o = (size_t)e * nr + j;
+        const double yv = B.z[o] - gt_alpha_col(P, e, j, nr, B.alpha);
+        B.y[o] = yv;
+        s += yv * B.w[o] * P.minv[e];
+    }
+    block_sum_cols(s, nr, sh, cols);
+    grid_total_cols(cols, B.part + (size_t)P.nd * nr, nr, B.done + DONE_RHO, B.scal + SC_RHO * nr);
+}
+
+// p = y + beta_j p (and its FP32 copy)
+__global__ void bp_kernel(DevProblem P, BlockDev B, int slot) {
+    const int iter = P.st->iter_base + slot;
+    if (skip_iter(P.st, iter)) return;
+    const int nr = B.nr;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.NL * nr; i += gridDim.x * blockDim.x) {
+        const int j = i % nr;
+        const double beta = (iter == 0) ? 0.0 : B.scal[SC_RHO * nr + j] / B.rho_hist[(size_t)(iter - 1) * nr + j];
+        const double pv = col_frozen(B, j, iter) ? 0.0 : B.y[i] + beta * B.p[i];
+        B.p[i] = pv;
+        B.p32[i] = (float)pv;
+    }
+}
+
+__global__ void bupdate_kernel(DevProblem P, BlockDev B, int slot) {
+    __shared__ double sh[8 * 32];
+    const int iter = P.st->iter_base + slot;
+    if (skip_iter(P.st, iter)) return;
+    const int nr = B.nr, dsub = blockIdx.x;
+    const int e0 = P.loff[dsub], e1 = P.loff[dsub + 1];
+    for (int i = threadIdx.x; i < (e1 - e0) * nr; i += blockDim.x) {
+        const int e = e0 + i / nr, j = i % nr;
+        const size_t o = (size_t)e * nr + j;
+        double rv = B.r[o];
+        if (!col_frozen(B, j, iter)) {
+            const double alpha = B.scal[SC_RHO * nr + j] / B.scal[SC_PAP * nr + j];
+            B.x[o] += alpha * B.p[o];
+            const int q = P.partner[e];
+            const double a = B.Ap[o] + (q >= 0 ? B.Ap[(size_t)q * nr + j] : 0.0);
+            rv -= alpha * a;
+            B.r[o] = rv;
+        }
+    }
+    __syncthreads();
+    g_dot_cols(P, B, dsub, B.r + (size_t)e0 * nr, sh);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        DevState *st = P.st;
+        bool replace = false;
+        int nconv = 0;
+        double worst = 0.0;
+        const bool fresh = st->true_iter == iter;
+        for (int j = 0; j < nr; ++j) {
+            const double rho = B.scal[SC_RHO * nr + j];
+            B.rho_hist[(size_t)iter * nr + j] = rho;
+            if (B.conv[j] != -1) { ++nconv; continue; }
+            const double wn = sqrt(B.scal[SC_WN2 * nr + j]);
+            B.last_norm[j] = wn;
+            worst = fmax(worst, wn / fmax(B.tol[j], 1e-300));
+            if (!st->mixed) {
+                if (wn < B.tol[j]) { B.conv[j] = iter; ++nconv; }
+            } else {
+                B.rmax[j] = fresh ? wn : fmax(B.rmax[j], wn);
+                if (wn < B.tol[j]) {
+                    if (fresh) { B.conv[j] = iter; ++nconv; }
+                    else replace = true;
+                } else if (wn < st->delta * B.rmax[j]) {
+                    replace = true;
+                }
+            }
+        }
+        st->last_norm = worst;
+        if (nconv == nr && st->conv_iter < 0) st->conv_iter = iter;
+        if (replace && st->conv_iter < 0) {
+            st->replace_iter = iter + 1;
+            st->true_iter = iter + 1;
+            st->replacements += 1;
+        }
+    }
+}
+
+// Tile SYMM, full read: a warp owns one 32-row tile row of one subdomain and
+// accumulates Y_I = sum_J S_IJ X_J for all nr columns in registers, using the
+// stored upper tile (I,J) for J >= I and the stored tile (J,I) transposed for J < I.
+// Lane = (row group g, column j): NR columns, 32/NR row groups of NR rows each.
+template <int PREC, int NR, int SRC>  // SRC 0: FP64 x (replacement/initial/FP64 path), 1: FP32 p copy
+__global__ void __launch_bounds__(256)
+tile_symm_kernel(TileSetDev ts, DevProblem P, BlockDev B, const double *x64, const float *x32, double *out,
+                 const int2 *units, int nunits, int slot, int mode) {
+    using Acc = typename TileT<PREC>::Acc;
+    constexpr int EPC = TileT<PREC>::EPC;
+    constexpr int G = 32 / NR;          // row groups
+    constexpr unsigned TB = TILE * TILE * (PREC == SCHUR_FP64 ? 8 : 4);
+    extern __shared__ __align__(16) unsigned char symm_smem[];
+    __shared__ int s_last;
+    if (mode != 0) {
+        const int iter = P.st->iter_base + slot;
+        if (skip_iter(P.st, iter)) return;
+        if (mode == 3 && P.st->replace_iter != iter) return;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int j = lane % NR, g = lane / NR;
+    unsigned char *wbuf = symm_smem + (size_t)warp * TB;
+    Acc *tile = reinterpret_cast<Acc *>(wbuf);
+    for (;;) {
+        int u = 0;
+        if (lane == 0) u = atomicAdd(&B.queue[0], 1);
+        u = __shfl_sync(FULL, u, 0);
+        if (u >= nunits) break;
+        const int m = units[u].x, I = units[u].y;
+        const int n = ts.mat_n[m], voff = ts.mat_voff[m], tn = ts.mat_tn[m];
+        const long long t0 = ts.mat_tile0[m];
+        Acc acc[NR];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) acc[r] = 0;
+        for (int J = 0; J < tn; ++J) {
+            const bool upper = J >= I;
+            const int a = upper ? I : J, b = upper ? J : I;
+            const long long tid = t0 + (long long)a * tn - (long long)a * (a - 1) / 2 + (b - a);
+            // tile -> shared memory (each lane copies 16-byte chunks)
+            const uint4 *src = reinterpret_cast<const uint4 *>(ts.tiles) + (size_t)tid * (TB / 16);
+            uint4 *dst = reinterpret_cast<uint4 *>(wbuf);
+#pragma unroll
+            for (int q = 0; q < (int)(TB / 16 / 32); ++q) dst[q * 32 + lane] = ld_stream(src + q * 32 + lane);
+            __syncwarp();
+            // column j of X_J (32 values)
+            Acc xc[TILE];
+#pragma unroll
+            for (int c = 0; c < TILE; ++c) {
+                const int row = TILE * J + c;
+                Acc v = 0;
+                if (row < n) v = SRC ? (Acc)x32[(size_t)(voff + row) * NR + j] : (Acc)x64[(size_t)(voff + row) * NR + j];
+                xc[c] = v;
+            }
+            if (upper) {
+                // Y[r] += sum_c S[r][c] x[c], my rows r = g*NR + t
+#pragma unroll
+                for (int t = 0; t < NR; ++t) {
+                    const Acc *srow = tile + (g * NR + t) * TILE;
+                    Acc s = 0;
+#pragma unroll
+                    for (int c = 0; c < TILE; ++c) s += srow[c] * xc[c];
+                    acc[t] += s;
+                }
+            } else {
+                // Y[r] += sum_c S_JI[c][r] x[c]
+#pragma unroll
+                for (int c = 0; c < TILE; ++c) {
+                    const Acc *srow = tile + c * TILE + g * NR;
+                    const Acc xv = xc[c];
+#pragma unroll
+                    for (int t = 0; t < NR; ++t) acc[t] += srow[t] * xv;
+                }
+            }
+            __syncwarp();
+        }
+        // write the tile row and its dot with x (per column)
+        double dot = 0.0;
+#pragma unroll
+        for (int t = 0; t < NR; ++t) {
+            const int row = TILE * I + g * NR + t;
+            if (row < n) {
+                const size_t o = (size_t)(voff + row) * NR + j;
+                out[o] = (double)acc[t];
+                const double xv = SRC ? (double)x32[o] : x64[o];
+                dot += xv * (double)acc[t];
+            }
+        }
+#pragma unroll
+        for (int o = 16; o >= NR; o >>= 1) dot += __shfl_xor_sync(FULL, dot, o);
+        if (lane < NR) B.unit_dot[(size_t)u * NR + lane] = dot;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = (atomicAdd(&B.queue[1], 1) == (int)gridDim.x - 1);
+    }
+    __syncthreads();
+    if (s_last) {
+        if (mode == 1) {
+            __threadfence();
+            if (threadIdx.x < NR) {
+                double t = 0.0;
+                for (int q = 0; q < nunits; ++q) t += __ldcg(&B.unit_dot[(size_t)q * NR + threadIdx.x]);
+                B.scal[SC_PAP * NR + threadIdx.x] = t;
+            }
+        }
+        if (threadIdx.x == 0) {
+            B.queue[0] = 0;
+            B.queue[1] = 0;
+            __threadfence();
+        }
+    }
+}
+
+__global__ void bchunk_end_kernel(DevProblem P, int chunk) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) P.st->iter_base += chunk;
+}
+
+// ---- right-hand sides and primal recovery for nr columns (column-major local-DOF blocks)
+__global__ void bsplit_rhs_kernel(const double *rhs, int nc, const int *gdof, const double *invm, double *f, int ntot,
+                                  int nr) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)ntot * nr) return;
+    const int j = (int)(i / ntot), k = (int)(i % ntot);
+    const int gd = gdof[k];
+    f[i] = gd >= 0 ? rhs[(size_t)j * nc + gd] * invm[k] : 0.0;
+}
+
+__global__ void bbvec_kernel(DevProblem P, BlockDev B, const int *rdof, const double *rsign, const double *rc,
+                             const double *kf, int ntot) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nr = B.nr;
+    if (i >= P.NL * nr) return;
+    const int e = i / nr, j = i % nr;
+    const double *k = kf + (size_t)j * ntot;
+    double b = rsign[e] * k[rdof[e]] - rc[e];
+    const int q = P.partner[e];
+    if (q >= 0) b += rsign[q] * k[rdof[q]] - rc[q];
+    B.bL[i] = b;
+}
+
+__global__ void bevec_kernel(DevProblem P, BlockDev B, const int *doff, const int *rofs, const double *R,
+                             const double *f, int ntot) {
+    __shared__ double sh[32 * KMAX];
+    const int d = blockIdx.x % P.nd, j = blockIdx.x / P.nd;
+    const int n = doff[d + 1] - doff[d], nk = P.kof[d + 1] - P.kof[d];
+    const double *Rd = R + rofs[d];
+    const double *fj = f + (size_t)j * ntot;
+    double acc[KMAX];
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k) acc[k] = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double fi = fj[doff[d] + i];
+        for (int k = 0; k < nk; ++k) acc[k] += Rd[(size_t)k * n + i] * fi;
+    }
+    block_sum_k(acc, sh);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < nk; ++k) B.e[(size_t)(P.kof[d] + k) * B.nr + j] = -acc[k];
+}
+
+__global__ void bprimal_rhs_kernel(DevProblem P, BlockDev B, const int *tdof_g, const double *rsign, const double *f,
+                                   double *g, int ntot) {
+    const int nr = B.nr;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (long long)ntot * nr;
+         i += (long long)gridDim.x * blockDim.x)
+        g[i] = f[i];
+    __syncthreads();
+}
+
+__global__ void bprimal_bt_kernel(DevProblem P, BlockDev B, const int *tdof_g, const double *rsign, double *g,
+                                  int ntot) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nr = B.nr;
+    if (i >= P.NT * nr) return;
+    const int t = i / nr, j = i % nr;
+    double s = 0.0;
+    for (int q = P.trow_ptr[t]; q < P.trow_ptr[t + 1]; ++q) {
+        const int e = P.trow_idx[q];
+        s += rsign[e] * B.x[(size_t)e * nr + j];
+    }
+    g[(size_t)j * ntot + tdof_g[t]] -= s;
+}
+
+__global__ void bprimal_merge_kernel(DevProblem P, BlockDev B, const int *doff, const int *rofs, const double *R,
+                                     const double *u, const int *gdof, const double *invm, double *sol, int nc,
+                                     int ntot) {
+    const int d = blockIdx.x % P.nd, j = blockIdx.x / P.nd;
+    const int n = doff[d + 1] - doff[d], nk = P.kof[d + 1] - P.kof[d];
+    const double *Rd = R + rofs[d];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double val = u[(size_t)j * ntot + doff[d] + i];
+        for (int k = 0; k < nk; ++k) val += Rd[(size_t)k * n + i] * B.alpha[(size_t)(P.kof[d] + k) * B.nr + j];
+        const int gd = gdof[doff[d] + i];
+        if (gd >= 0) atomicAdd(&sol[(size_t)j * nc + gd], val * invm[doff[d] + i]);
+    }
+}
+
+}  // namespace
+}  // namespace feti
+
+// =============================================================================================
+// Block solver host side
+namespace feti {
+
+void GpuSolver::Impl::ensure_block(int nr) {
+    if (blk.nr == nr) return;
+    if (blk.graph) { cudaGraphExecDestroy(blk.graph); blk.graph = nullptr; }
+    const int NL = P.NL, NT = P.NT, nK = P.nK, nd = P.nd;
+    BlockDev &B = blk.B;
+    B.nr = nr;
+    B.x = alloc<double>((size_t)NL * nr); B.r = alloc<double>((size_t)NL * nr); B.w = alloc<double>((size_t)NL * nr);
+    B.z = alloc<double>((size_t)NL * nr); B.y = alloc<double>((size_t)NL * nr); B.p = alloc<double>((size_t)NL * nr);
+    B.Ap = alloc<double>((size_t)NL * nr); B.Ax = alloc<double>((size_t)NL * nr); B.bL = alloc<double>((size_t)NL * nr);
+    B.p32 = alloc<float>((size_t)NL * nr);
+    B.uT = alloc<double>((size_t)NT * nr); B.vT = alloc<double>((size_t)NT * nr);
+    B.d = alloc<double>((size_t)nK * nr); B.alpha = alloc<double>((size_t)nK * nr); B.e = alloc<double>((size_t)nK * nr);
+    B.part = alloc<double>((size_t)2 * nd * nr);
+    B.scal = alloc<double>((size_t)SC_COUNT * nr);
+    B.rho_hist = alloc<double>((size_t)(opt.max_iterations + 64) * nr);
+    B.tol = alloc<double>(nr); B.rmax = alloc<double>(nr); B.last_norm = alloc<double>(nr);
+    B.conv = alloc<int>(nr);
+    B.done = alloc<int>(DONE_COUNT);
+    B.queue = alloc<int>(2);
+    CUDA_CHECK(cudaMemset(B.done, 0, sizeof(int) * DONE_COUNT));
+    CUDA_CHECK(cudaMemset(B.queue, 0, sizeof(int) * 2));
+    CUDA_CHECK(cudaMemset(B.p, 0, sizeof(double) * NL * nr));
+    // SYMM work units (subdomain, tile row), longest rows first
+    std::vector<int2> units;
+    const std::vector<int> &tn = F64.h_tn;
+    std::vector<int> order(tn.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return tn[a] > tn[b]; });
+    for (int m : order)
+        for (int I = 0; I < tn[m]; ++I) units.push_back(make_int2(m, I));
+    blk.units = upload(units);
+    blk.nunits = (int)units.size();
+    B.unit_dot = alloc<double>((size_t)units.size() * nr);
+    blk.rhs = alloc<double>((size_t)std::max(1, n_caller) * nr);
+    blk.sol = alloc<double>((size_t)std::max(1, n_caller) * nr);
+    blk.f = alloc<double>((size_t)ntot * nr);
+    blk.kf = alloc<double>((size_t)ntot * nr);
+    blk.g = alloc<double>((size_t)ntot * nr);
+    blk.nr = nr;
+}
+
+template <int PR, int NR, int SRC>
+static void symm_launch(int grid, size_t sm, cudaStream_t st, TileSetDev td, DevProblem P, BlockDev B,
+                        const double *x64, const float *x32, double *out, const int2 *units, int nunits, int slot,
+                        int mode) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(tile_symm_kernel<PR, NR, SRC>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+        attr = true;
+    }
+    tile_symm_kernel<PR, NR, SRC><<<grid, 256, sm, st>>>(td, P, B, x64, x32, out, units, nunits, slot, mode);
+}
+
+void GpuSolver::Impl::launch_symm(const TileSetHost &T, bool src32, const double *x64, const float *x32, double *out,
+                                  int slot, int mode) {
+    const int nr = blk.nr;
+    const size_t TB = (size_t)TILE * TILE * (T.prec == SCHUR_FP64 ? 8 : 4);
+    const size_t sm = 8 * TB;
+    const int grid = std::max(1, std::min((blk.nunits + 7) / 8, nsm * 3));
+    TileSetDev td = T.dev();
+    FETI_CHECK(T.prec != SCHUR_BF16, "FETI4I: the multi right-hand-side solve supports FP64 and FP32 Schur storage");
+#define SYMM(PR, NR_, S) symm_launch<PR, NR_, S>(grid, sm, stream, td, P, blk.B, x64, x32, out, blk.units, blk.nunits, slot, mode)
+#define SYMM_NR(PR, S)                       \
+    switch (nr) {                            \
+    case 4: SYMM(PR, 4, S); break;           \
+    case 8: SYMM(PR, 8, S); break;           \
+    case 16: SYMM(PR, 16, S); break;         \
+    default: SYMM(PR, 32, S); break;         \
+    }
+    if (T.prec == SCHUR_FP64) { SYMM_NR(SCHUR_FP64, 0) }
+    else if (src32) { SYMM_NR(SCHUR_FP32, 1) }
+    else { SYMM_NR(SCHUR_FP32, 0) }
+#undef SYMM_NR
+#undef SYMM
+    CUDA_CHECK(cudaGetLastError());
+}
+
+void GpuSolver::Impl::launch_block_iteration(int slot) {
+    const int nd = P.nd;
+    const int cgrid = (P.nK + 7) / 8;
+    BlockDev &B = blk.B;
+    const bool mixed = opt.schur_precision != SCHUR_FP64;
+    if (mixed) {
+        launch_symm(F64, false, B.x, nullptr, B.Ax, slot, 3);
+        br0_kernel<<<nd, TPB, 0, stream>>>(P, B, 1, slot);
+    }
+    bcoarse_kernel<<<cgrid, 256, 0, stream>>>(P, B, B.d, B.alpha, slot, 1);
+    switch (opt.precond) {
+    case PREC_NONE: bw_prec_kernel<PREC_NONE><<<nd, TPB, 0, stream>>>(P, B, slot); break;
+    case PREC_LUMPED: bw_prec_kernel<PREC_LUMPED><<<nd, TPB, 0, stream>>>(P, B, slot); break;
+    default: bw_prec_kernel<PREC_WEIGHT><<<nd, TPB, 0, stream>>>(P, B, slot); break;
+    }
+    if (opt.precond != PREC_NONE) {
+        bz_kernel<<<nd, TPB, 0, stream>>>(P, B, slot);
+        bcoarse_kernel<<<cgrid, 256, 0, stream>>>(P, B, B.d, B.alpha, slot, 1);
+        by_kernel<<<nd, TPB, 0, stream>>>(P, B, slot);
+    }
+    bp_kernel<<<std::max(1, std::min(4096, (P.NL * blk.nr + 255) / 256)), 256, 0, stream>>>(P, B, slot);
+    if (mixed) launch_symm(Flow, true, nullptr, B.p32, B.Ap, slot, 1);
+    else launch_symm(F64, false, B.p, nullptr, B.Ap, slot, 1);
+    bupdate_kernel<<<nd, TPB, 0, stream>>>(P, B, slot);
+    CUDA_CHECK(cudaGetLastError());
+}
+
+void GpuSolver::solve_multi(const double *rhs, int nrhs, int rhs_size, double *solutions, int solution_size,
+                            SolveStats &stats, bool upload_rhs) {
+    Impl &I = *impl;
+    DevProblem &P = I.P;
+    FETI_CHECK(nrhs >= 1 && nrhs <= 32, "FETI4ISolveMulti: 1..32 right-hand sides per call");
+    FETI_CHECK(I.opt.precond != PREC_DIRICHLET,
+               "FETI4ISolveMulti: the Dirichlet preconditioner is not available for several right-hand sides");
+    int nr = 4;
+    while (nr < nrhs) nr *= 2;
+    I.ensure_block(nr);
+    BlockDev &B = I.blk.B;
+    const int nd = P.nd, nc = std::max(1, I.n_caller), ntot = I.ntot;
+    const int cgrid = (P.nK + 7) / 8;
+    if (upload_rhs) {
+        CUDA_CHECK(cudaMemsetAsync(I.blk.rhs, 0, sizeof(double) * (size_t)nc * nr, I.stream));
+        const int ncp = std::min(rhs_size, I.n_caller);
+        for (int j = 0; j < nrhs; ++j)
+            CUDA_CHECK(cudaMemcpyAsync(I.blk.rhs + (size_t)j * nc, rhs + (size_t)j * rhs_size, sizeof(double) * ncp,
+                                       cudaMemcpyHostToDevice, I.stream));
+        const long long tot = (long long)ntot * nr;
+        bsplit_rhs_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, I.stream>>>(I.blk.rhs, nc, I.d_gdof, I.d_invm, I.blk.f,
+                                                                              ntot, nr);
+        CUDA_CHECK(cudaMemsetAsync(I.blk.kf, 0, sizeof(double) * (size_t)ntot * nr, I.stream));
+        for (int j = 0; j < nrhs; ++j) I.launch_kplus(I.blk.f + (size_t)j * ntot, I.blk.kf + (size_t)j * ntot);
+        bevec_kernel<<<nd * nr, TPB, 0, I.stream>>>(P, B, I.d_doff, I.d_rofs, I.d_R, I.blk.f, ntot);
+        bbvec_kernel<<<(P.NL * nr + 255) / 256, 256, 0, I.stream>>>(P, B, I.d_rdof, I.d_rsign, I.d_rc, I.blk.kf, ntot);
+        CUDA_CHECK(cudaGetLastError());
+    }
+    // ---- block PCG
+    const bool mixed = I.opt.schur_precision != SCHUR_FP64;
+    DevState h{};
+    h.conv_iter = -1;
+    h.replace_iter = -1;
+    h.true_iter = 0;
+    h.max_it = I.opt.max_iterations;
+    h.mixed = mixed ? 1 : 0;
+    h.precision = I.opt.precision;
+    h.delta = I.opt.reliable_delta;
+    CUDA_CHECK(cudaEventRecord(I.ev0, I.stream));
+    CUDA_CHECK(cudaMemcpyAsync(I.st, &h, sizeof(h), cudaMemcpyHostToDevice, I.stream));
+    bcoarse_kernel<<<cgrid, 256, 0, I.stream>>>(P, B, B.e, B.alpha, 0, 0);
+    bgt_kernel<<<(P.NL * nr + 255) / 256, 256, 0, I.stream>>>(P, B, B.alpha, B.x);
+    CUDA_CHECK(cudaMemsetAsync(B.p, 0, sizeof(double) * (size_t)P.NL * nr, I.stream));
+    I.launch_symm(I.F64, false, B.x, nullptr, B.Ax, 0, 0);
+    br0_kernel<<<nd, TPB, 0, I.stream>>>(P, B, 0, 0);
+    bcoarse_kernel<<<cgrid, 256, 0, I.stream>>>(P, B, B.d, B.alpha, 0, 0);
+    bpnorm_kernel<<<nd, TPB, 0, I.stream>>>(P, B);
+    btol_kernel<<<1, 32, 0, I.stream>>>(P, B);
+    CUDA_CHECK(cudaGetLastError());
+    const int chunk = std::max(1, I.opt.chunk);
+    auto &G = I.blk;
+    if (!(G.graph && G.graph_chunk == chunk && G.graph_prec == I.opt.schur_precision &&
+          G.graph_precond == I.opt.precond)) {
+        if (G.graph) { cudaGraphExecDestroy(G.graph); G.graph = nullptr; }
+        cudaGraph_t g;
+        CUDA_CHECK(cudaStreamBeginCapture(I.stream, cudaStreamCaptureModeThreadLocal));
+        for (int j = 0; j < chunk; ++j) I.launch_block_iteration(j);
+        bchunk_end_kernel<<<1, 32, 0, I.stream>>>(P, chunk);
+        CUDA_CHECK(cudaStreamEndCapture(I.stream, &g));
+        CUDA_CHECK(cudaGraphInstantiate(&G.graph, g, 0));
+        cudaGraphDestroy(g);
+        G.graph_chunk = chunk;
+        G.graph_prec = I.opt.schur_precision;
+        G.graph_precond = I.opt.precond;
+    }
+    DevState hs{};
+    for (int done = 0; done < I.opt.max_iterations; done += chunk) {
+        CUDA_CHECK(cudaGraphLaunch(G.graph, I.stream));
+        CUDA_CHECK(cudaMemcpyAsync(&hs, I.st, sizeof(hs), cudaMemcpyDeviceToHost, I.stream));
+        CUDA_CHECK(cudaStreamSynchronize(I.stream));
+        if (hs.conv_iter >= 0) break;
+    }
+    bcoarse_kernel<<<cgrid, 256, 0, I.stream>>>(P, B, B.d, B.alpha, 0, 0);
+    CUDA_CHECK(cudaEventRecord(I.ev1, I.stream));
+    CUDA_CHECK(cudaMemcpyAsync(&hs, I.st, sizeof(hs), cudaMemcpyDeviceToHost, I.stream));
+    std::vector<int> conv(nr);
+    CUDA_CHECK(cudaMemcpyAsync(conv.data(), B.conv, sizeof(int) * nr, cudaMemcpyDeviceToHost, I.stream));
+    CUDA_CHECK(cudaStreamSynchronize(I.stream));
+    float ms = 0.f;
+    CUDA_CHECK(cudaEventElapsedTime(&ms, I.ev0, I.ev1));
+    stats.t_solve_ms = ms;
+    stats.converged = hs.conv_iter >= 0;
+    stats.iterations = stats.converged ? hs.conv_iter + 1 : std::min(hs.iter_base, I.opt.max_iterations);
+    stats.replacements = hs.replacements;
+    stats.final_norm = hs.last_norm;
+    stats.kernel_launches = 9 + (stats.iterations + chunk - 1) / chunk * chunk * 11;
+    stats.fapply_bytes = (mixed ? I.Flow : I.F64).alg_bytes;
+    // ---- primal recovery for every column
+    if (solutions) {
+        bprimal_rhs_kernel<<<4096, 256, 0, I.stream>>>(P, B, I.d_tdof_g, I.d_rsign, I.blk.f, I.blk.g, ntot);
+        bprimal_bt_kernel<<<(P.NT * nr + 255) / 256, 256, 0, I.stream>>>(P, B, I.d_tdof_g, I.d_rsign, I.blk.g, ntot);
+        for (int j = 0; j < nrhs; ++j) I.launch_kplus(I.blk.g + (size_t)j * ntot, I.blk.kf + (size_t)j * ntot);
+        CUDA_CHECK(cudaMemsetAsync(I.blk.sol, 0, sizeof(double) * (size_t)nc * nr, I.stream));
+        bprimal_merge_kernel<<<nd * nr, TPB, 0, I.stream>>>(P, B, I.d_doff, I.d_rofs, I.d_R, I.blk.kf, I.d_gdof, I.d_invm,
+                                                           I.blk.sol, nc, ntot);
+        CUDA_CHECK(cudaGetLastError());
+        const int ncp = std::min(solution_size, I.n_caller);
+        for (int j = 0; j < nrhs; ++j) {
+            CUDA_CHECK(cudaMemcpyAsync(solutions + (size_t)j * solution_size, I.blk.sol + (size_t)j * nc,
+                                       sizeof(double) * ncp, cudaMemcpyDeviceToHost, I.stream));
+        }
+        CUDA_CHECK(cudaStreamSynchronize(I.stream));
+        for (int j = 0; j < nrhs; ++j)
+            for (int i = std::max(0, ncp); i < solution_size; ++i) solutions[(size_t)j * solution_size + i] = 0.0;
+    }
 }
 
 }  // namespace feti

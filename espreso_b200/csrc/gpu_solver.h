@@ -57,6 +57,10 @@ public:
     // With upload_rhs == false the right-hand side of the previous call is reused.
     void solve_full(const double *rhs, int rhs_size, double *solution, int solution_size, SolveStats &st,
                     bool upload_rhs = true);
+    // Several right-hand sides (1..32, rhs[j * rhs_size + i]) solved together: block PCG with
+    // per-column scalars and stop tests, tile SYMM F apply; solutions[j * solution_size + i].
+    void solve_multi(const double *rhs, int nrhs, int rhs_size, double *solutions, int solution_size, SolveStats &st,
+                     bool upload_rhs = true);
     // y = F x in lambda space with the given operator precision (tests, benchmarks)
     void apply_F(const double *x_lambda, double *y_lambda, int precision);
     // average device time of `reps` F applies (inputs resident), returns ms

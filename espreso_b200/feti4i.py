@@ -36,7 +36,8 @@ EXPORTED = [
     "FETI4IGetStats", "FETI4IGetDualSolution", "FETI4IGetSubdomainInfo", "FETI4IGetSubdomainMultipliers",
     "FETI4IGetSubdomainNodes", "FETI4IGetSubdomainSchur", "FETI4IGetSubdomainKernel", "FETI4IGetDualRhs",
     "FETI4IApplySubdomainKplus", "FETI4IApplyDualOperator", "FETI4ITimeDualOperator", "FETI4ISolveResident", "FETI4ISetSolvePrecision",
-    "FETI4ITiledSymvNoAlloc", "FETI4IElementEnergies", "FETI4IGetTuning",
+    "FETI4ITiledSymvNoAlloc", "FETI4IElementEnergies", "FETI4IGetTuning", "FETI4ISolveMulti",
+    "FETI4ISolveMultiResident",
 ]
 
 
@@ -89,6 +90,8 @@ def load(path: str = LIB_PATH):
         "FETI4ITiledSymvNoAlloc": ([vp, vp, vp, vp, i32, i32, vp, vp, vp, vp], i32),
         "FETI4IElementEnergies": ([vp, i32, pd, pd, pd], None),
         "FETI4IGetTuning": ([vp], C.c_char_p),
+        "FETI4ISolveMulti": ([vp, i32, i32, pd, pd], None),
+        "FETI4ISolveMultiResident": ([vp, i32], f64),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -224,6 +227,19 @@ class Instance:
         self.lib.FETI4ISolve(self.h, sol.size, _dp(sol))
         _check(self.lib)
         return sol
+
+    def solve_multi(self, rhs):
+        """rhs (nrhs, size) -> solutions (nrhs, size), solved together."""
+        R = np.ascontiguousarray(np.atleast_2d(rhs), dtype=np.float64)
+        out = np.zeros_like(R)
+        self.lib.FETI4ISolveMulti(self.h, R.shape[0], R.shape[1], _dp(R), _dp(out))
+        _check(self.lib)
+        return out
+
+    def solve_multi_resident(self, nrhs):
+        ms = self.lib.FETI4ISolveMultiResident(self.h, int(nrhs))
+        _check(self.lib)
+        return ms
 
     def solve_resident(self):
         ms = self.lib.FETI4ISolveResident(self.h)

@@ -96,6 +96,14 @@ void FETI4IGetDualRhs(FETI4IInstance instance, FETI4IReal *b, FETI4IReal *e);
 void FETI4IApplyDualOperator(FETI4IInstance instance, FETI4IInt precision, FETI4IReal *x, FETI4IReal *y);
 /* Average device time in ms of one F apply over `reps` launches (inputs resident). */
 FETI4IReal FETI4ITimeDualOperator(FETI4IInstance instance, FETI4IInt precision, FETI4IInt reps);
+/* Several load cases at once (SURVEY of the reference: no multi-RHS path): nrhs right-hand
+ * sides (1..32) in rhs[j * size + i] are solved together by a block PCG whose F apply is a
+ * tile SYMM; solutions[j * size + i].  LUMPED, WEIGHT_FUNCTION or no preconditioner. */
+void FETI4ISolveMulti(FETI4IInstance instance, FETI4IInt nrhs, FETI4IInt size, const FETI4IReal *rhs,
+                      FETI4IReal *solutions);
+/* Re-solve the last FETI4ISolveMulti right-hand sides on the device; returns the device ms. */
+FETI4IReal FETI4ISolveMultiResident(FETI4IInstance instance, FETI4IInt nrhs);
+
 /* Solve on device-resident data only (right-hand side already uploaded by a
  * previous FETI4ISolve): returns the device time in ms of the dual PCG. */
 FETI4IReal FETI4ISolveResident(FETI4IInstance instance);

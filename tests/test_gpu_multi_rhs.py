@@ -1,0 +1,63 @@
+"""Several load cases solved together (FETI4ISolveMulti): block PCG + tile SYMM.
+
+Every column must equal the single right-hand-side solve and a direct solve to 1e-8,
+for FP64 Schur storage and for FP32 storage with FP64 residual replacement, and for
+right-hand-side counts that are padded to the SYMM width (5 -> 8) or fill it (32).
+"""
+import numpy as np
+import pytest
+
+from espreso_b200 import feti4i as F
+from espreso_b200 import problems
+from oracle import feti as OF
+
+pytestmark = pytest.mark.gpu
+
+
+def load_cases(P, nrhs, seed):
+    rng = np.random.default_rng(seed)
+    base = P.rhs()
+    out = []
+    for j in range(nrhs):
+        f = base * rng.uniform(0.5, 2.0) + rng.normal(0.0, np.abs(base).max(), size=base.size) * (j % 3 == 0)
+        out.append(f)
+    return np.array(out)
+
+
+def direct(P, f):
+    K, _ = OF.global_system(P.elem_nodes, P.Ke, np.zeros((P.Ke.shape[0], P.Ke.shape[1])), P.n_nodes, P.dpn)
+    dd, dv = P.dirichlet_dofs()
+    return OF.direct_solve(K, f, dd, dv)
+
+
+@pytest.mark.parametrize("kind,schur,nrhs,prec", [("elast", F.FP64, 5, F.PREC_LUMPED),
+                                                  ("elast", F.FP32, 8, F.PREC_LUMPED),
+                                                  ("heat", F.FP32, 32, F.PREC_LUMPED),
+                                                  ("heat", F.FP64, 3, F.PREC_NONE)])
+def test_multi_rhs_matches_single_and_direct(kind, schur, nrhs, prec):
+    P = (problems.elasticity_cube(domains=(3, 2, 2), elements=(3, 3, 3)) if kind == "elast"
+         else problems.heat_cube(domains=(3, 3, 2), elements=(4, 4, 4), seed=2))
+    inst = problems.make_instance(P, iopts={F.PRECONDITIONER: prec, F.VERBOSE_LEVEL: 0, F.MAX_ITERATIONS: 3000},
+                                  ropts={F.PRECISION: 1e-10}, ext={F.EXT_SCHUR_PRECISION: schur})
+    R = load_cases(P, nrhs, seed=nrhs)
+    U = inst.solve_multi(R)
+    st = inst.stats()
+    assert st["converged"] == 1.0
+    for j in range(nrhs):
+        ud = direct(P, R[j])
+        assert np.linalg.norm(U[j] - ud) <= 1e-8 * np.linalg.norm(ud), j
+    # the single right-hand-side path gives the same columns
+    for j in (0, nrhs - 1):
+        inst.update_rhs(R[j])
+        u1 = inst.solve()
+        assert np.linalg.norm(U[j] - u1) <= 1e-8 * np.linalg.norm(u1)
+    assert inst.solve_multi_resident(nrhs) > 0
+    inst.destroy()
+
+
+def test_multi_rhs_rejects_dirichlet_preconditioner():
+    P = problems.elasticity_cube(domains=(2, 1, 1), elements=(2, 2, 2))
+    inst = problems.make_instance(P, iopts={F.PRECONDITIONER: F.PREC_DIRICHLET, F.VERBOSE_LEVEL: 0})
+    with pytest.raises(F.FETI4IError, match="Dirichlet"):
+        inst.solve_multi(np.stack([P.rhs(), P.rhs()]))
+    inst.destroy()
