@@ -91,6 +91,7 @@ enum { SC_RHO = 0, SC_PAP = 1, SC_WN2 = 2, SC_BN2 = 3, SC_PN2 = 4, SC_COUNT = 8 
 // block (multi right-hand-side) solver vectors: [row][rhs]
 struct BlockDev {
     int nr;              // right-hand sides (power of two <= 32)
+    int lg;              // log2(nr)
     double *x, *r, *w, *z, *y, *p, *Ap, *Ax, *bL, *uT, *vT, *d, *alpha, *e;
     float *p32;          // FP32 copy of p (SYMM input in mixed precision)
     double *part;        // nd * nr partials
@@ -2200,6 +2201,8 @@ namespace {
 
 
 
+constexpr int UNR = 4;   // rows in flight per thread in the block vector kernels
+
 // per-column sum over a CTA: threads with the same column (tid % nr) are combined
 __device__ void block_sum_cols(double v, int nr, double *sh /* >= 8*32 */, double *out_col /* nr */) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -2226,11 +2229,19 @@ __device__ void grid_total_cols(const double *mine /* nr, shared */, double *par
     if (threadIdx.x == 0) s_last = (atomicAdd(counter, 1) == (int)gridDim.x - 1);
     __syncthreads();
     if (s_last) {
+        // every thread of the last CTA sums a fixed subset of the CTA partials of one column,
+        // then the subsets are combined in shared memory (fixed order: deterministic)
         __threadfence();
+        __shared__ double s_cols[1024];
+        const int j = threadIdx.x & (nr - 1), g = threadIdx.x / nr, ng = blockDim.x / nr;
+        double t = 0.0;
+        for (int c = g; c < (int)gridDim.x; c += ng) t += __ldcg(&partials[c * nr + j]);
+        s_cols[threadIdx.x] = t;
+        __syncthreads();
         if (threadIdx.x < nr) {
-            double t = 0.0;
-            for (int c = 0; c < (int)gridDim.x; ++c) t += __ldcg(&partials[c * nr + threadIdx.x]);
-            out[threadIdx.x] = t;
+            double u = 0.0;
+            for (int q = 0; q < ng; ++q) u += s_cols[q * nr + threadIdx.x];
+            out[threadIdx.x] = u;
         }
         if (threadIdx.x == 0) *counter = 0;
     }
@@ -2243,7 +2254,7 @@ __device__ void g_dot_cols(const DevProblem &P, const BlockDev &B, int dsub, con
     const int nk = P.kof[dsub + 1] - P.kof[dsub];
     for (int k = 0; k < nk; ++k) {
         double s = 0.0;
-        for (int i = threadIdx.x; i < (e1 - e0) * nr; i += blockDim.x) s += P.Gl[(size_t)(e0 + i / nr) * P.KS + k] * v[i];
+        for (int i = threadIdx.x; i < (e1 - e0) * nr; i += blockDim.x) s += P.Gl[(size_t)(e0 + (i >> B.lg)) * P.KS + k] * v[i];
         __shared__ double cols[32];
         block_sum_cols(s, nr, sh, cols);
         if (threadIdx.x < nr) B.d[(size_t)(P.kof[dsub] + k) * nr + threadIdx.x] = cols[threadIdx.x];
@@ -2266,33 +2277,50 @@ __device__ __forceinline__ bool col_frozen(const BlockDev &B, int j, int iter) {
     return c == -2 || (c >= 0 && iter > c);
 }
 
-__global__ void bcoarse_kernel(DevProblem P, BlockDev B, const double *in, double *out, int slot, int looped) {
+// out (nK x nr) = (GG^T)^-1 in: a CTA owns CR rows; 32-row blocks of `in` are staged in
+// shared memory and every thread keeps CR/8 rows of one column
+constexpr int CR = 16;
+__global__ void __launch_bounds__(256) bcoarse_kernel(DevProblem P, BlockDev B, const double *in, double *out, int slot,
+                                                      int looped) {
     if (looped && skip_iter(P.st, P.st->iter_base + slot)) return;
-    const int nr = B.nr;
-    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    if (row >= P.nK) return;
-    const double *col = P.GGtinv + (size_t)row * P.nK;
-    double acc[32];
+    __shared__ double xs[32][33];
+    __shared__ double ms[CR][33];
+    const int nr = B.nr, nK = P.nK;
+    const int r0 = blockIdx.x * CR;
+    const int j = threadIdx.x & 31, rg = threadIdx.x >> 5;   // column, row group (8 groups)
+    double acc[CR / 8];
 #pragma unroll
-    for (int j = 0; j < 32; ++j) acc[j] = 0.0;
-    for (int b = lane; b < P.nK; b += 32) {
-        const double m = col[b];
+    for (int q = 0; q < CR / 8; ++q) acc[q] = 0.0;
+    for (int b0 = 0; b0 < nK; b0 += 32) {
+        for (int t = threadIdx.x; t < 32 * 32; t += blockDim.x) {
+            const int b = t >> 5, c = t & 31;
+            xs[b][c] = (b0 + b < nK && c < nr) ? in[(size_t)(b0 + b) * nr + c] : 0.0;
+        }
+        for (int t = threadIdx.x; t < CR * 32; t += blockDim.x) {
+            const int r = t >> 5, c = t & 31;
+            ms[r][c] = (r0 + r < nK && b0 + c < nK) ? P.GGtinv[(size_t)(r0 + r) * nK + b0 + c] : 0.0;
+        }
+        __syncthreads();
 #pragma unroll
-        for (int j = 0; j < 32; ++j)
-            if (j < nr) acc[j] += m * in[(size_t)b * nr + j];
+        for (int q = 0; q < CR / 8; ++q) {
+            const int r = rg + 8 * q;
+            double sum = 0.0;
+#pragma unroll 8
+            for (int b = 0; b < 32; ++b) sum += ms[r][b] * xs[b][j];
+            acc[q] += sum;
+        }
+        __syncthreads();
     }
 #pragma unroll
-    for (int j = 0; j < 32; ++j)
-        if (j < nr) {
-            double s = warp_sum(acc[j]);
-            if (lane == 0) out[(size_t)row * nr + j] = s;
-        }
+    for (int q = 0; q < CR / 8; ++q) {
+        const int r = r0 + rg + 8 * q;
+        if (r < nK && j < nr) out[(size_t)r * nr + j] = acc[q];
+    }
 }
 
 __global__ void bgt_kernel(DevProblem P, BlockDev B, const double *a, double *xout) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < P.NL * B.nr) xout[i] = gt_alpha_col(P, i / B.nr, i % B.nr, B.nr, a);
+    if (i < P.NL * B.nr) xout[i] = gt_alpha_col(P, (i >> B.lg), (i & (B.nr - 1)), B.nr, a);
 }
 
 // r = b - assemble(Ax), d = G r, |b_j|^2 totals (initial) / replacement
@@ -2307,7 +2335,7 @@ __global__ void br0_kernel(DevProblem P, BlockDev B, int replace_mode, int slot)
     const int e0 = P.loff[dsub], e1 = P.loff[dsub + 1];
     double bb = 0.0;
     for (int i = threadIdx.x; i < (e1 - e0) * nr; i += blockDim.x) {
-        const int e = e0 + i / nr, j = i % nr;
+        const int e = e0 + (i >> B.lg), j = (i & (nr - 1));
         const int q = P.partner[e];
         const size_t o = (size_t)e * nr + j;
         const double a = B.Ax[o] + (q >= 0 ? B.Ax[(size_t)q * nr + j] : 0.0);
@@ -2329,7 +2357,7 @@ __global__ void bpnorm_kernel(DevProblem P, BlockDev B) {
     const int nr = B.nr, dsub = blockIdx.x;
     double s = 0.0;
     for (int i = threadIdx.x; i < (P.loff[dsub + 1] - P.loff[dsub]) * nr; i += blockDim.x) {
-        const int e = P.loff[dsub] + i / nr, j = i % nr;
+        const int e = P.loff[dsub] + (i >> B.lg), j = (i & (nr - 1));
         const double u = B.r[(size_t)e * nr + j] - gt_alpha_col(P, e, j, nr, B.alpha);
         s += u * u * P.minv[e];
     }
@@ -2357,13 +2385,31 @@ __global__ void bw_prec_kernel(DevProblem P, BlockDev B, int slot) {
     const int nr = B.nr, dsub = blockIdx.x;
     const int e0 = P.loff[dsub], e1 = P.loff[dsub + 1];
     double ww = 0.0;
-    for (int i = threadIdx.x; i < (e1 - e0) * nr; i += blockDim.x) {
-        const int e = e0 + i / nr, j = i % nr;
-        const size_t o = (size_t)e * nr + j;
-        const double wv = B.r[o] - gt_alpha_col(P, e, j, nr, B.alpha);
-        B.w[o] = wv;
-        if (PRECOND == PREC_NONE) B.y[o] = wv;
-        ww += wv * wv * P.minv[e];
+    const int cnt = (e1 - e0) * nr;
+    // UNR rows in flight per thread: all loads of a group are issued before its stores
+    for (int i0 = threadIdx.x; i0 < cnt; i0 += UNR * blockDim.x) {
+        double rv[UNR], ga[UNR], mv[UNR];
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            const int i = i0 + u * blockDim.x;
+            if (i < cnt) {
+                const int e = e0 + (i >> B.lg), j = i & (nr - 1);
+                rv[u] = B.r[(size_t)e * nr + j];
+                ga[u] = gt_alpha_col(P, e, j, nr, B.alpha);
+                mv[u] = P.minv[e];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            const int i = i0 + u * blockDim.x;
+            if (i < cnt) {
+                const size_t o = (size_t)e0 * nr + i;
+                const double wv = rv[u] - ga[u];
+                B.w[o] = wv;
+                if (PRECOND == PREC_NONE) B.y[o] = wv;
+                ww += wv * wv * mv[u];
+            }
+        }
     }
     block_sum_cols(ww, nr, sh, cols);
     grid_total_cols(cols, B.part, nr, B.done + DONE_W, B.scal + SC_WN2 * nr);
@@ -2374,7 +2420,7 @@ __global__ void bw_prec_kernel(DevProblem P, BlockDev B, int slot) {
     __syncthreads();
     const int t0 = P.toff[dsub], nt = P.toff[dsub + 1] - t0;
     for (int i = threadIdx.x; i < nt * nr; i += blockDim.x) {
-        const int t = i / nr, j = i % nr;
+        const int t = (i >> B.lg), j = (i & (nr - 1));
         double s = 0.0;
         for (int q = P.trow_ptr[t0 + t]; q < P.trow_ptr[t0 + t + 1]; ++q) {
             const int e = P.trow_idx[q];
@@ -2387,15 +2433,21 @@ __global__ void bw_prec_kernel(DevProblem P, BlockDev B, int slot) {
     __syncthreads();
     const int sl0 = P.slice0[dsub];
     for (int i = threadIdx.x; i < nt * nr; i += blockDim.x) {
-        const int t = i / nr, j = i % nr;
+        const int t = (i >> B.lg), j = (i & (nr - 1));
         const int sl = sl0 + (t >> 5), ln = t & 31;
         const int base = P.ell_ptr[sl], wd = P.ell_w[sl];
-        double s = 0.0;
-        for (int q = 0; q < wd; ++q) {
+        double s0 = 0.0, s1 = 0.0;
+        int q = 0;
+        for (; q + 1 < wd; q += 2) {
             const int o = base + q * 32 + ln;
-            s += P.ell_val[o] * B.uT[(size_t)(t0 + P.ell_col[o]) * nr + j];
+            s0 += P.ell_val[o] * B.uT[(size_t)(t0 + P.ell_col[o]) * nr + j];
+            s1 += P.ell_val[o + 32] * B.uT[(size_t)(t0 + P.ell_col[o + 32]) * nr + j];
         }
-        B.vT[(size_t)(t0 + t) * nr + j] = s;
+        if (q < wd) {
+            const int o = base + q * 32 + ln;
+            s0 += P.ell_val[o] * B.uT[(size_t)(t0 + P.ell_col[o]) * nr + j];
+        }
+        B.vT[(size_t)(t0 + t) * nr + j] = s0 + s1;
     }
 }
 
@@ -2405,12 +2457,24 @@ __global__ void bz_kernel(DevProblem P, BlockDev B, int slot) {
     if (skip_iter(P.st, iter)) return;
     const int nr = B.nr, dsub = blockIdx.x;
     const int e0 = P.loff[dsub], e1 = P.loff[dsub + 1];
-    for (int i = threadIdx.x; i < (e1 - e0) * nr; i += blockDim.x) {
-        const int e = e0 + i / nr, j = i % nr;
-        const int pt = P.ptidx[e];
-        double zv = P.ws[e] * B.vT[(size_t)P.tidx[e] * nr + j];
-        if (pt >= 0) zv += P.pws[e] * B.vT[(size_t)pt * nr + j];
-        B.z[(size_t)e * nr + j] = zv;
+    const int cnt = (e1 - e0) * nr;
+    for (int i0 = threadIdx.x; i0 < cnt; i0 += UNR * blockDim.x) {
+        double zv[UNR];
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            const int i = i0 + u * blockDim.x;
+            if (i < cnt) {
+                const int e = e0 + (i >> B.lg), j = i & (nr - 1);
+                const int pt = P.ptidx[e];
+                zv[u] = P.ws[e] * B.vT[(size_t)P.tidx[e] * nr + j];
+                if (pt >= 0) zv[u] += P.pws[e] * B.vT[(size_t)pt * nr + j];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            const int i = i0 + u * blockDim.x;
+            if (i < cnt) B.z[(size_t)e0 * nr + i] = zv[u];
+        }
     }
     __syncthreads();
     g_dot_cols(P, B, dsub, B.z + (size_t)e0 * nr, sh);
@@ -2424,12 +2488,30 @@ __global__ void by_kernel(DevProblem P, BlockDev B, int slot) {
     if (skip_iter(P.st, iter)) return;
     const int nr = B.nr, dsub = blockIdx.x;
     double s = 0.0;
-    for (int i = threadIdx.x; i < (P.loff[dsub + 1] - P.loff[dsub]) * nr; i += blockDim.x) {
-        const int e = P.loff[dsub] + i / nr, j = i % nr;
-        const size_t o = (size_t)e * nr + j;
-        const double yv = B.z[o] - gt_alpha_col(P, e, j, nr, B.alpha);
-        B.y[o] = yv;
-        s += yv * B.w[o] * P.minv[e];
+    const int e0 = P.loff[dsub], cnt = (P.loff[dsub + 1] - e0) * nr;
+    for (int i0 = threadIdx.x; i0 < cnt; i0 += UNR * blockDim.x) {
+        double zv[UNR], ga[UNR], wv[UNR], mv[UNR];
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            const int i = i0 + u * blockDim.x;
+            if (i < cnt) {
+                const int e = e0 + (i >> B.lg), j = i & (nr - 1);
+                const size_t o = (size_t)e0 * nr + i;
+                zv[u] = B.z[o];
+                wv[u] = B.w[o];
+                ga[u] = gt_alpha_col(P, e, j, nr, B.alpha);
+                mv[u] = P.minv[e];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            const int i = i0 + u * blockDim.x;
+            if (i < cnt) {
+                const double yv = zv[u] - ga[u];
+                B.y[(size_t)e0 * nr + i] = yv;
+                s += yv * wv[u] * mv[u];
+            }
+        }
     }
     block_sum_cols(s, nr, sh, cols);
     grid_total_cols(cols, B.part + (size_t)P.nd * nr, nr, B.done + DONE_RHO, B.scal + SC_RHO * nr);
@@ -2441,7 +2523,7 @@ __global__ void bp_kernel(DevProblem P, BlockDev B, int slot) {
     if (skip_iter(P.st, iter)) return;
     const int nr = B.nr;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.NL * nr; i += gridDim.x * blockDim.x) {
-        const int j = i % nr;
+        const int j = (i & (nr - 1));
         const double beta = (iter == 0) ? 0.0 : B.scal[SC_RHO * nr + j] / B.rho_hist[(size_t)(iter - 1) * nr + j];
         const double pv = col_frozen(B, j, iter) ? 0.0 : B.y[i] + beta * B.p[i];
         B.p[i] = pv;
@@ -2455,19 +2537,37 @@ __global__ void bupdate_kernel(DevProblem P, BlockDev B, int slot) {
     if (skip_iter(P.st, iter)) return;
     const int nr = B.nr, dsub = blockIdx.x;
     const int e0 = P.loff[dsub], e1 = P.loff[dsub + 1];
-    for (int i = threadIdx.x; i < (e1 - e0) * nr; i += blockDim.x) {
-        const int e = e0 + i / nr, j = i % nr;
-        const size_t o = (size_t)e * nr + j;
-        double rv = B.r[o];
-        if (!col_frozen(B, j, iter)) {
-            const double alpha = B.scal[SC_RHO * nr + j] / B.scal[SC_PAP * nr + j];
-            B.x[o] += alpha * B.p[o];
-            const int q = P.partner[e];
-            const double a = B.Ap[o] + (q >= 0 ? B.Ap[(size_t)q * nr + j] : 0.0);
-            rv -= alpha * a;
-            B.r[o] = rv;
+    // the stride keeps each thread on one column: alpha_j once per thread
+    const int jt = threadIdx.x & (nr - 1);
+    const bool frozen = col_frozen(B, jt, iter);
+    const double alpha = frozen ? 0.0 : B.scal[SC_RHO * nr + jt] / B.scal[SC_PAP * nr + jt];
+    const int cnt = (e1 - e0) * nr;
+    if (!frozen)
+        for (int i0 = threadIdx.x; i0 < cnt; i0 += UNR * blockDim.x) {
+            double xv[UNR], pv[UNR], rv[UNR], av[UNR];
+#pragma unroll
+            for (int u = 0; u < UNR; ++u) {
+                const int i = i0 + u * blockDim.x;
+                if (i < cnt) {
+                    const int e = e0 + (i >> B.lg);
+                    const size_t o = (size_t)e0 * nr + i;
+                    const int q = P.partner[e];
+                    xv[u] = B.x[o];
+                    pv[u] = B.p[o];
+                    rv[u] = B.r[o];
+                    av[u] = B.Ap[o] + (q >= 0 ? B.Ap[(size_t)q * nr + jt] : 0.0);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < UNR; ++u) {
+                const int i = i0 + u * blockDim.x;
+                if (i < cnt) {
+                    const size_t o = (size_t)e0 * nr + i;
+                    B.x[o] = xv[u] + alpha * pv[u];
+                    B.r[o] = rv[u] - alpha * av[u];
+                }
+            }
         }
-    }
     __syncthreads();
     g_dot_cols(P, B, dsub, B.r + (size_t)e0 * nr, sh);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -2510,7 +2610,7 @@ __global__ void bupdate_kernel(DevProblem P, BlockDev B, int slot) {
 // stored upper tile (I,J) for J >= I and the stored tile (J,I) transposed for J < I.
 // Lane = (row group g, column j): NR columns, 32/NR row groups of NR rows each.
 template <int PREC, int NR, int SRC>  // SRC 0: FP64 x (replacement/initial/FP64 path), 1: FP32 p copy
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, PREC == SCHUR_FP64 ? 2 : 3)
 tile_symm_kernel(TileSetDev ts, DevProblem P, BlockDev B, const double *x64, const float *x32, double *out,
                  const int2 *units, int nunits, int slot, int mode) {
     using Acc = typename TileT<PREC>::Acc;
@@ -2549,31 +2649,34 @@ tile_symm_kernel(TileSetDev ts, DevProblem P, BlockDev B, const double *x64, con
 #pragma unroll
             for (int q = 0; q < (int)(TB / 16 / 32); ++q) dst[q * 32 + lane] = ld_stream(src + q * 32 + lane);
             __syncwarp();
-            // column j of X_J (32 values)
-            Acc xc[TILE];
-#pragma unroll
-            for (int c = 0; c < TILE; ++c) {
-                const int row = TILE * J + c;
-                Acc v = 0;
-                if (row < n) v = SRC ? (Acc)x32[(size_t)(voff + row) * NR + j] : (Acc)x64[(size_t)(voff + row) * NR + j];
-                xc[c] = v;
-            }
+            // x column j of block J, row c (zero past the subdomain's rows)
+            const int rb = TILE * J;
+            auto xval = [&](int c) -> Acc {
+                const int row = rb + c;
+                if (row >= n) return (Acc)0;
+                return SRC ? (Acc)x32[(size_t)(voff + row) * NR + j] : (Acc)x64[(size_t)(voff + row) * NR + j];
+            };
             if (upper) {
-                // Y[r] += sum_c S[r][c] x[c], my rows r = g*NR + t
+                // Y[r] += sum_c S[r][c] x[c], my rows r = g*NR + t; eight columns per step keep the
+                // x values in few registers and NR independent accumulation chains in flight
 #pragma unroll
-                for (int t = 0; t < NR; ++t) {
-                    const Acc *srow = tile + (g * NR + t) * TILE;
-                    Acc s = 0;
+                for (int c0 = 0; c0 < TILE; c0 += 8) {
+                    Acc xc[8];
 #pragma unroll
-                    for (int c = 0; c < TILE; ++c) s += srow[c] * xc[c];
-                    acc[t] += s;
+                    for (int q = 0; q < 8; ++q) xc[q] = xval(c0 + q);
+#pragma unroll
+                    for (int t = 0; t < NR; ++t) {
+                        const Acc *srow = tile + (g * NR + t) * TILE + c0;
+                        acc[t] += ((srow[0] * xc[0] + srow[1] * xc[1]) + (srow[2] * xc[2] + srow[3] * xc[3])) +
+                                  ((srow[4] * xc[4] + srow[5] * xc[5]) + (srow[6] * xc[6] + srow[7] * xc[7]));
+                    }
                 }
             } else {
                 // Y[r] += sum_c S_JI[c][r] x[c]
-#pragma unroll
+#pragma unroll 4
                 for (int c = 0; c < TILE; ++c) {
                     const Acc *srow = tile + c * TILE + g * NR;
-                    const Acc xv = xc[c];
+                    const Acc xv = xval(c);
 #pragma unroll
                     for (int t = 0; t < NR; ++t) acc[t] += srow[t] * xv;
                 }
@@ -2638,7 +2741,7 @@ __global__ void bbvec_kernel(DevProblem P, BlockDev B, const int *rdof, const do
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int nr = B.nr;
     if (i >= P.NL * nr) return;
-    const int e = i / nr, j = i % nr;
+    const int e = (i >> B.lg), j = (i & (nr - 1));
     const double *k = kf + (size_t)j * ntot;
     double b = rsign[e] * k[rdof[e]] - rc[e];
     const int q = P.partner[e];
@@ -2679,7 +2782,7 @@ __global__ void bprimal_bt_kernel(DevProblem P, BlockDev B, const int *tdof_g, c
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int nr = B.nr;
     if (i >= P.NT * nr) return;
-    const int t = i / nr, j = i % nr;
+    const int t = (i >> B.lg), j = (i & (nr - 1));
     double s = 0.0;
     for (int q = P.trow_ptr[t]; q < P.trow_ptr[t + 1]; ++q) {
         const int e = P.trow_idx[q];
@@ -2715,6 +2818,7 @@ void GpuSolver::Impl::ensure_block(int nr) {
     const int NL = P.NL, NT = P.NT, nK = P.nK, nd = P.nd;
     BlockDev &B = blk.B;
     B.nr = nr;
+    B.lg = __builtin_ctz(nr);
     B.x = alloc<double>((size_t)NL * nr); B.r = alloc<double>((size_t)NL * nr); B.w = alloc<double>((size_t)NL * nr);
     B.z = alloc<double>((size_t)NL * nr); B.y = alloc<double>((size_t)NL * nr); B.p = alloc<double>((size_t)NL * nr);
     B.Ap = alloc<double>((size_t)NL * nr); B.Ax = alloc<double>((size_t)NL * nr); B.bL = alloc<double>((size_t)NL * nr);
@@ -2750,15 +2854,21 @@ void GpuSolver::Impl::ensure_block(int nr) {
     blk.nr = nr;
 }
 
+// persistent launch: as many CTAs as are resident at once (they drain the unit queue)
 template <int PR, int NR, int SRC>
-static void symm_launch(int grid, size_t sm, cudaStream_t st, TileSetDev td, DevProblem P, BlockDev B,
+static void symm_launch(int nsm, int ncta, size_t sm, cudaStream_t st, TileSetDev td, DevProblem P, BlockDev B,
                         const double *x64, const float *x32, double *out, const int2 *units, int nunits, int slot,
                         int mode) {
-    static bool attr = false;
-    if (!attr) {
+    static int per_sm = 0;
+    if (per_sm == 0) {
         cudaFuncSetAttribute(tile_symm_kernel<PR, NR, SRC>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-        attr = true;
+        int b = 1;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, tile_symm_kernel<PR, NR, SRC>, 256, sm) != cudaSuccess ||
+            b < 1)
+            b = 1;
+        per_sm = b;
     }
+    const int grid = std::max(1, std::min(ncta, nsm * per_sm));
     tile_symm_kernel<PR, NR, SRC><<<grid, 256, sm, st>>>(td, P, B, x64, x32, out, units, nunits, slot, mode);
 }
 
@@ -2767,10 +2877,10 @@ void GpuSolver::Impl::launch_symm(const TileSetHost &T, bool src32, const double
     const int nr = blk.nr;
     const size_t TB = (size_t)TILE * TILE * (T.prec == SCHUR_FP64 ? 8 : 4);
     const size_t sm = 8 * TB;
-    const int grid = std::max(1, std::min((blk.nunits + 7) / 8, nsm * 3));
+    const int ncta = (blk.nunits + 7) / 8;
     TileSetDev td = T.dev();
     FETI_CHECK(T.prec != SCHUR_BF16, "FETI4I: the multi right-hand-side solve supports FP64 and FP32 Schur storage");
-#define SYMM(PR, NR_, S) symm_launch<PR, NR_, S>(grid, sm, stream, td, P, blk.B, x64, x32, out, blk.units, blk.nunits, slot, mode)
+#define SYMM(PR, NR_, S) symm_launch<PR, NR_, S>(nsm, ncta, sm, stream, td, P, blk.B, x64, x32, out, blk.units, blk.nunits, slot, mode)
 #define SYMM_NR(PR, S)                       \
     switch (nr) {                            \
     case 4: SYMM(PR, 4, S); break;           \
@@ -2788,7 +2898,7 @@ void GpuSolver::Impl::launch_symm(const TileSetHost &T, bool src32, const double
 
 void GpuSolver::Impl::launch_block_iteration(int slot) {
     const int nd = P.nd;
-    const int cgrid = (P.nK + 7) / 8;
+    const int cgrid = (P.nK + CR - 1) / CR;
     BlockDev &B = blk.B;
     const bool mixed = opt.schur_precision != SCHUR_FP64;
     if (mixed) {
@@ -2825,7 +2935,7 @@ void GpuSolver::solve_multi(const double *rhs, int nrhs, int rhs_size, double *s
     I.ensure_block(nr);
     BlockDev &B = I.blk.B;
     const int nd = P.nd, nc = std::max(1, I.n_caller), ntot = I.ntot;
-    const int cgrid = (P.nK + 7) / 8;
+    const int cgrid = (P.nK + CR - 1) / CR;
     if (upload_rhs) {
         CUDA_CHECK(cudaMemsetAsync(I.blk.rhs, 0, sizeof(double) * (size_t)nc * nr, I.stream));
         const int ncp = std::min(rhs_size, I.n_caller);
