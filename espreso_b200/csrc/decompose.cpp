@@ -149,9 +149,11 @@ Decomposition decompose(const ElementData &el, int ndomains_hint, const std::vec
     dec.node_interval.assign(dec.n_nodes, -1);
     for (int p = 0; p < nint; ++p)
         for (int i = dec.interval_ptr[p]; i < dec.interval_ptr[p + 1]; ++i) dec.node_interval[used[i]] = p;
+    dec.interval_ext.assign(nint, 0);
     for (int p = 0; p < nint; ++p) {
         int n = used[dec.interval_ptr[p]];
         dec.interval_domains[p].assign(dlist.begin() + dptr[n], dlist.begin() + dptr[n + 1]);
+        dec.interval_ext[p] = ext[n];
     }
 
     // domain local node numbering (interval by interval)

@@ -21,6 +21,7 @@ struct ElementData {
     std::vector<int> nodes, dofs;     // already shifted by index_base
     std::vector<double> vals;         // row-major dofsSize^2 per element
     std::vector<int> partition;       // element -> subdomain (optional)
+    std::vector<int> sub_cluster;     // subdomain -> cluster for Hybrid Total FETI (optional)
     size_t nelem() const { return etype.size(); }
 };
 
@@ -45,6 +46,7 @@ struct Decomposition {
     std::vector<int> node_order;      // final node order (interval by interval)
     std::vector<int> interval_ptr;    // into node_order
     std::vector<std::vector<int>> interval_domains;
+    std::vector<char> interval_ext;   // 1 for intervals of the external-surface group
     std::vector<int> node_ndom;       // number of domains sharing each node
     std::vector<int> node_interval;   // node -> interval index
     std::vector<DomainRows> dom;

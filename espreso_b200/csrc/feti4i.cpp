@@ -100,8 +100,9 @@ void add_element(ElementData &el, int type, int nn, const int *nodes, int nd, co
 void build(FETI4IStructInstance *I) {
     const int *io = I->iopt;
     g_verbose = io[FETI4I_VERBOSE_LEVEL];
-    FETI_CHECK(io[FETI4I_FETI_METHOD] == 0,
-               "FETI4I: FETI_METHOD " + std::to_string(io[FETI4I_FETI_METHOD]) + " (HYBRID_FETI) is not supported by this build");
+    FETI_CHECK(io[FETI4I_FETI_METHOD] == 0 || io[FETI4I_FETI_METHOD] == 1,
+               "FETI4I: FETI_METHOD " + std::to_string(io[FETI4I_FETI_METHOD]) +
+                   " is not supported (0 TOTAL_FETI, 1 HYBRID_FETI)");
     FETI_CHECK(io[FETI4I_CGSOLVER] == 0, "FETI4I: only CGSOLVER 0 (PCG) is supported by this build");
     int prec = io[FETI4I_PRECONDITIONER];
     FETI_CHECK(prec >= 0 && prec <= 3, "FETI4I: PRECONDITIONER " + std::to_string(prec) + " is not supported (0..3)");
@@ -110,6 +111,13 @@ void build(FETI4IStructInstance *I) {
     double t0 = now_s();
     I->dec = decompose(I->el, io[FETI4I_SUBDOMAINS], I->dir_idx, I->dir_val);
     PrepOptions po;
+    po.method = io[FETI4I_FETI_METHOD];
+    if (po.method == 1 && !I->el.sub_cluster.empty()) {
+        FETI_CHECK((int)I->el.sub_cluster.size() == I->dec.ndom,
+                   "FETI4I: the cluster partition lists " + std::to_string(I->el.sub_cluster.size()) +
+                       " subdomains, the problem has " + std::to_string(I->dec.ndom));
+        po.sub_cluster = I->el.sub_cluster;
+    }
     po.precond = prec;
     po.scaling = I->ext[FETI4I_EXT_SCALING] != 0.0;
     po.threads = (int)I->ext[FETI4I_EXT_HOST_THREADS];
@@ -209,6 +217,14 @@ void FETI4ISetSubdomainPartition(FETI4IMatrix matrix, FETI4IInt size, FETI4IInt 
         auto *m = check_matrix(matrix);
         FETI_CHECK(size == (FETI4IInt)m->el.nelem(), "FETI4I: partition size differs from the number of added elements");
         m->el.partition.assign(elem2sub, elem2sub + size);
+    });
+}
+
+void FETI4ISetClusterPartition(FETI4IMatrix matrix, FETI4IInt nsubdomains, const FETI4IInt *sub2cluster) {
+    guarded([&] {
+        auto *m = check_matrix(matrix);
+        FETI_CHECK(nsubdomains >= 0 && (nsubdomains == 0 || sub2cluster), "FETI4I: invalid cluster partition");
+        m->el.sub_cluster.assign(sub2cluster, sub2cluster + nsubdomains);
     });
 }
 
@@ -486,6 +502,35 @@ void FETI4IGetSubdomainKernel(FETI4IInstance instance, FETI4IInt subdomain, FETI
         FETI_CHECK(subdomain >= 0 && subdomain < I->dec.ndom, "FETI4I: subdomain index out of range");
         const SubPrep &P = I->prep.sub[subdomain];
         std::copy(P.R.begin(), P.R.end(), R);
+    });
+}
+
+FETI4IInt FETI4IGetSubdomainCorners(FETI4IInstance instance, FETI4IInt subdomain, FETI4IInt *rows, FETI4IInt *dofs,
+                                    FETI4IReal *signs) {
+    FETI4IInt count = -1;
+    guarded([&] {
+        auto *I = check_instance(instance);
+        FETI_CHECK(subdomain >= 0 && subdomain < I->dec.ndom, "FETI4I: subdomain index out of range");
+        const SubPrep &S = I->prep.sub[subdomain];
+        count = (FETI4IInt)S.b0_row.size();
+        if (rows) std::copy(S.b0_row.begin(), S.b0_row.end(), rows);
+        if (dofs) std::copy(S.b0_dof.begin(), S.b0_dof.end(), dofs);
+        if (signs) std::copy(S.b0_sign.begin(), S.b0_sign.end(), signs);
+    });
+    return count;
+}
+
+void FETI4IGetClusterInfo(FETI4IInstance instance, FETI4IInt *info) {
+    guarded([&] {
+        auto *I = check_instance(instance);
+        FETI_CHECK(info, "FETI4I: null info array");
+        const Prep &P = I->prep;
+        info[0] = P.method;
+        info[1] = P.method == 1 ? (FETI4IInt)P.clusters.size() : I->dec.ndom;
+        int n0 = 0;
+        for (const auto &C : P.clusters) n0 += C.n0;
+        info[2] = n0;
+        info[3] = P.n_kern;
     });
 }
 

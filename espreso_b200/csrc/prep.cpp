@@ -14,6 +14,7 @@
 
 #include "common.h"
 #include "dense.h"
+#include "hybrid.h"
 
 namespace feti {
 
@@ -37,7 +38,10 @@ std::vector<int> bfs(const std::vector<std::vector<int>> &adj, int src) {
 // Three mutually distant nodes whose DOFs are all touched by B: the fix set
 // on which the kernel of K is detected (the algebraic regularisation of
 // src/solver/generic/SparseMatrix.cpp:3540-4495 works on a Schur complement
-// of K onto a small DOF set in the same way).
+// of K onto a small DOF set in the same way).  Distances are breadth-first over
+// the element edges, so on a structured mesh they are Manhattan distances: the
+// third node maximises da + db, which keeps it off the line through a and b
+// (three collinear nodes would leave a rotation free).
 std::vector<int> choose_fix_nodes(const std::vector<std::vector<int>> &adj, const std::vector<char> &cand) {
     int n = (int)adj.size();
     int a = -1;
@@ -55,7 +59,9 @@ std::vector<int> choose_fix_nodes(const std::vector<std::vector<int>> &adj, cons
     int c = -1;
     for (int i = 0; i < n; ++i) {
         if (!cand[i] || i == a || i == b) continue;
-        if (c < 0 || std::min(da[i], db[i]) > std::min(da[c], db[c])) c = i;
+        if (c < 0) { c = i; continue; }
+        const int si = da[i] + db[i], sc = da[c] + db[c];
+        if (si > sc || (si == sc && std::min(da[i], db[i]) > std::min(da[c], db[c]))) c = i;
     }
     if (c >= 0) fix.push_back(c);
     return fix;
@@ -110,8 +116,19 @@ static void prep_subdomain(const ElementData &el, const Decomposition &dec, int 
         for (int c = 0; c < dpn; ++c) all = all && touched[dpn * a + c];
         cand[a] = all;
     }
+    // node graph: the 12 edges of a HEXA8 element, all node pairs of other elements
+    static const int kHexEdges[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6},
+                                         {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
     for (int e : D.elems) {
         int64_t nb = el.node_ptr[e], ne_ = el.node_ptr[e + 1];
+        if (ne_ - nb == 8) {
+            for (const auto &ed : kHexEdges) {
+                const int u = g2l.at(el.nodes[nb + ed[0]]), v = g2l.at(el.nodes[nb + ed[1]]);
+                adj[u].push_back(v);
+                adj[v].push_back(u);
+            }
+            continue;
+        }
         for (int64_t i = nb; i < ne_; ++i)
             for (int64_t j = nb; j < ne_; ++j)
                 if (i != j) adj[g2l.at(el.nodes[i])].push_back(g2l.at(el.nodes[j]));
@@ -340,11 +357,29 @@ void preprocess(const ElementData &el, Decomposition &dec, const std::vector<dou
     }
     out.t_factor = now_s() - t0;
 
-    // coarse problem: kernel offsets, owners of every multiplier, GG^T and its inverse
+    // coarse problem: dual kernel space, owners of every multiplier, GG^T and its inverse
     double t1 = now_s();
-    out.kofs.assign(dec.ndom + 1, 0);
-    for (int d = 0; d < dec.ndom; ++d) out.kofs[d + 1] = out.kofs[d] + out.sub[d].nk;
-    out.n_kern = out.kofs[dec.ndom];
+    out.method = opt.method;
+    if (opt.method == 1) {
+        // Hybrid Total FETI: clusters glued at corners, cluster kernels in the dual problem
+        out.sub_cluster = opt.sub_cluster.empty() ? std::vector<int>(dec.ndom, 0) : opt.sub_cluster;
+        FETI_CHECK((int)out.sub_cluster.size() == dec.ndom,
+                   "FETI4I: the cluster partition must list one cluster per subdomain");
+        for (int c : out.sub_cluster) FETI_CHECK(c >= 0, "FETI4I: negative cluster index");
+        std::vector<int> n0;
+        hybrid_corners(dec, out.sub_cluster, out, n0);
+        hybrid_prepare(dec, out, n0, nthreads);
+    } else {
+        out.kofs.assign(dec.ndom + 1, 0);
+        for (int d = 0; d < dec.ndom; ++d) {
+            SubPrep &S = out.sub[d];
+            S.dnk = S.nk;
+            S.Rd = S.R;
+            S.Gd = S.G;
+            out.kofs[d + 1] = out.kofs[d] + S.nk;
+        }
+        out.n_kern = out.kofs[dec.ndom];
+    }
     out.own_dom.assign((size_t)2 * dec.n_lambda, -1);
     out.own_row.assign((size_t)2 * dec.n_lambda, -1);
     for (int d = 0; d < dec.ndom; ++d)
@@ -368,10 +403,10 @@ void preprocess(const ElementData &el, Decomposition &dec, const std::vector<dou
                 if (d2 < 0) continue;
                 int r2 = out.own_row[2 * (size_t)l + s2];
                 const SubPrep &A2 = out.sub[d2];
-                for (int a = 0; a < A1.nk; ++a)
-                    for (int b = 0; b < A2.nk; ++b)
+                for (int a = 0; a < A1.dnk; ++a)
+                    for (int b = 0; b < A2.dnk; ++b)
                         GG[(size_t)(out.kofs[d2] + b) * nK + out.kofs[d1] + a] +=
-                            A1.G[(size_t)a * A1.ni + r1] * A2.G[(size_t)b * A2.ni + r2];
+                            A1.Gd[(size_t)a * A1.ni + r1] * A2.Gd[(size_t)b * A2.ni + r2];
             }
         }
     }
@@ -386,20 +421,61 @@ void preprocess(const ElementData &el, Decomposition &dec, const std::vector<dou
     out.t_coarse = now_s() - t1;
 }
 
+void kplus_dual(const Prep &prep, std::vector<std::vector<double>> &x) {
+    const int nd = (int)prep.sub.size();
+    if (prep.method != 1) {
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int d = 0; d < nd; ++d) prep.sub[d].kplus(x[d].data());
+        return;
+    }
+    // cluster solve (cluster.cpp:796-916) with the cluster matrix M
+    const int ncl = (int)prep.clusters.size();
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int c = 0; c < ncl; ++c) {
+        const ClusterPrep &C = prep.clusters[c];
+        const int nc = C.n0 + C.ka;
+        std::vector<double> z(nc, 0.0), w(nc, 0.0), kx;
+        for (size_t mi = 0; mi < C.members.size(); ++mi) {
+            const int d = C.members[mi];
+            const SubPrep &S = prep.sub[d];
+            kx = x[d];
+            S.kplus(kx.data());
+            for (size_t j = 0; j < S.b0_row.size(); ++j) z[S.b0_row[j]] += S.b0_sign[j] * kx[S.b0_dof[j]];
+            for (int k = 0; k < S.nk; ++k) {
+                double s = 0.0;
+                for (int i = 0; i < S.n; ++i) s += S.R[(size_t)k * S.n + i] * x[d][i];
+                z[C.n0 + C.akofs[mi] + k] = -s;
+            }
+        }
+        for (int j = 0; j < nc; ++j)
+            for (int i = 0; i < nc; ++i) w[i] += C.M[(size_t)j * nc + i] * z[j];
+        for (size_t mi = 0; mi < C.members.size(); ++mi) {
+            const int d = C.members[mi];
+            const SubPrep &S = prep.sub[d];
+            std::vector<double> &v = x[d];
+            for (size_t j = 0; j < S.b0_row.size(); ++j) v[S.b0_dof[j]] -= S.b0_sign[j] * w[S.b0_row[j]];
+            S.kplus(v.data());
+            for (int k = 0; k < S.nk; ++k) {
+                const double a = w[C.n0 + C.akofs[mi] + k];
+                for (int i = 0; i < S.n; ++i) v[i] += S.R[(size_t)k * S.n + i] * a;
+            }
+        }
+    }
+}
+
 void make_rhs_vectors(const Decomposition &dec, const Prep &prep, std::vector<double> &b, std::vector<double> &e) {
     b.assign(dec.n_lambda, 0.0);
     e.assign(prep.n_kern, 0.0);
     const int nd = dec.ndom;
     std::vector<std::vector<double>> kf(nd);
-#pragma omp parallel for schedule(dynamic, 1)
+    for (int d = 0; d < nd; ++d) kf[d] = prep.sub[d].f;
+    kplus_dual(prep, kf);
     for (int d = 0; d < nd; ++d) {
         const SubPrep &S = prep.sub[d];
-        kf[d] = S.f;
-        S.kplus(kf[d].data());
-        for (int k = 0; k < S.nk; ++k) {
+        for (int k = 0; k < S.dnk; ++k) {
             double s = 0.0;
-            for (int i = 0; i < S.n; ++i) s += S.R[(size_t)k * S.n + i] * S.f[i];
-            e[prep.kofs[d] + k] = -s;
+            for (int i = 0; i < S.n; ++i) s += S.Rd[(size_t)k * S.n + i] * S.f[i];
+            e[prep.kofs[d] + k] -= s;
         }
     }
     for (int d = 0; d < nd; ++d) {
@@ -413,16 +489,18 @@ void primal_solution(const Decomposition &dec, const Prep &prep, const double *l
     const int dpn = dec.dpn;
     const int nd = dec.ndom;
     std::vector<std::vector<double>> u(nd);
+    for (int d = 0; d < nd; ++d) {
+        const DomainRows &D = dec.dom[d];
+        u[d] = prep.sub[d].f;
+        for (size_t r = 0; r < D.lam.size(); ++r) u[d][D.dof[r]] -= D.sign[r] * lambda[D.lam[r]];
+    }
+    kplus_dual(prep, u);
 #pragma omp parallel for schedule(dynamic, 1)
     for (int d = 0; d < nd; ++d) {
         const SubPrep &S = prep.sub[d];
-        const DomainRows &D = dec.dom[d];
-        u[d] = S.f;
-        for (size_t r = 0; r < D.lam.size(); ++r) u[d][D.dof[r]] -= D.sign[r] * lambda[D.lam[r]];
-        S.kplus(u[d].data());
-        for (int k = 0; k < S.nk; ++k) {
+        for (int k = 0; k < S.dnk; ++k) {
             double a = alpha[prep.kofs[d] + k];
-            for (int i = 0; i < S.n; ++i) u[d][i] += S.R[(size_t)k * S.n + i] * a;
+            for (int i = 0; i < S.n; ++i) u[d][i] += S.Rd[(size_t)k * S.n + i] * a;
         }
     }
     std::vector<double> cnt(solution_size, 0.0);

@@ -32,15 +32,42 @@ struct SubPrep {
     double kernel_residual = 0.0;  // ||K R||_F / (||K||_F) check of the detected kernel
     std::vector<double> ss_eigs;   // eigenvalues of the fix-DOF Schur block
 
+    // kernel space of the dual problem restricted to this subdomain: the subdomain's own kernel
+    // (Total FETI) or the cluster kernel R H_i (Hybrid Total FETI)
+    int dnk = 0;                   // columns
+    std::vector<double> Rd;        // n x dnk, local DOF order
+    std::vector<double> Gd;        // dnk x ni, row-major: -(B_i Rd)^T
+
+    // Hybrid Total FETI: corner rows of B0 touching this subdomain (one DOF per row)
+    std::vector<int> b0_row;       // cluster-local B0 row
+    std::vector<int> b0_dof;       // local DOF
+    std::vector<double> b0_sign;
+    std::vector<double> V;         // ni x (n0_i + nk), column-major: [B_i K^+ B0_i^T | G_i^T]
+
     // x := K_reg^{-1} x (local DOF order)
     void kplus(double *x) const;
+};
+
+// One cluster of Hybrid Total FETI: subdomains glued at corners by B0.
+struct ClusterPrep {
+    std::vector<int> members;       // subdomains, ascending
+    int n0 = 0;                     // B0 rows
+    int ka = 0;                     // sum of the members' kernel dimensions
+    std::vector<int> akofs;         // member -> offset in the ka block
+    int nkc = 0;                    // cluster kernel dimension
+    std::vector<double> H;          // ka x nkc, column-major: kernel of S_alpha
+    std::vector<double> M;          // (n0+ka)^2, column-major: [g0; e0] -> [lambda0; alpha]
+    double rho = 0.0;               // S_alpha regularisation weight
 };
 
 struct Prep {
     std::vector<SubPrep> sub;
     int n_lambda = 0;
-    int n_kern = 0;
-    std::vector<int> kofs;          // kernel offset per subdomain
+    int n_kern = 0;                 // dual kernel space (GG^T order)
+    std::vector<int> kofs;          // dual kernel offset per subdomain (its cluster's offset in HTFETI)
+    int method = 0;                 // 0 Total FETI, 1 Hybrid Total FETI
+    std::vector<int> sub_cluster;   // HTFETI: subdomain -> cluster
+    std::vector<ClusterPrep> clusters;
     std::vector<double> GGt_inv;    // n_kern x n_kern, dense symmetric inverse
     std::vector<int> lam_owner;     // 2 per multiplier: (domain, row) packed as domain*2^20+row? (see owners)
     std::vector<int> own_dom, own_row;  // 2 entries per multiplier, -1 if absent
@@ -48,6 +75,8 @@ struct Prep {
 };
 
 struct PrepOptions {
+    int method = 0;                 // FETI_METHOD: 0 Total FETI, 1 Hybrid Total FETI
+    std::vector<int> sub_cluster;   // HTFETI clusters (empty: one cluster)
     int precond = PREC_DIRICHLET;
     bool scaling = true;
     bool keep_dirichlet = false;
@@ -57,6 +86,10 @@ struct PrepOptions {
 // rhs: caller DOF vector (size >= max DOF + 1); split per subdomain by multiplicity.
 void preprocess(const ElementData &el, Decomposition &dec, const std::vector<double> &rhs, const PrepOptions &opt,
                 Prep &out);
+
+// x_i := K_c^+ x_i for the subdomains of every cluster (Hybrid Total FETI), x[d] in local DOF order;
+// with Total FETI x_i := K_i^+ x_i.
+void kplus_dual(const Prep &prep, std::vector<std::vector<double>> &x);
 
 // Right-hand-side dependent vectors: b = sum_i B_i K_i^+ f_i - c (lambda space), e = -R^T f.
 void make_rhs_vectors(const Decomposition &dec, const Prep &prep, std::vector<double> &b, std::vector<double> &e);

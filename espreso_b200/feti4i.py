@@ -37,7 +37,7 @@ EXPORTED = [
     "FETI4IGetSubdomainNodes", "FETI4IGetSubdomainSchur", "FETI4IGetSubdomainKernel", "FETI4IGetDualRhs",
     "FETI4IApplySubdomainKplus", "FETI4IApplyDualOperator", "FETI4ITimeDualOperator", "FETI4ISolveResident", "FETI4ISetSolvePrecision",
     "FETI4ITiledSymvNoAlloc", "FETI4IElementEnergies", "FETI4IGetTuning", "FETI4ISolveMulti",
-    "FETI4ISolveMultiResident",
+    "FETI4ISolveMultiResident", "FETI4ISetClusterPartition", "FETI4IGetSubdomainCorners", "FETI4IGetClusterInfo",
 ]
 
 
@@ -92,6 +92,9 @@ def load(path: str = LIB_PATH):
         "FETI4IGetTuning": ([vp], C.c_char_p),
         "FETI4ISolveMulti": ([vp, i32, i32, pd, pd], None),
         "FETI4ISolveMultiResident": ([vp, i32], f64),
+        "FETI4ISetClusterPartition": ([vp, i32, pi], None),
+        "FETI4IGetSubdomainCorners": ([vp, i32, pi, pi, pd], i32),
+        "FETI4IGetClusterInfo": ([vp, pi], None),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -193,6 +196,11 @@ class Matrix:
         self.lib.FETI4ISetSubdomainPartition(self.h, e.size, _ip(e))
         _check(self.lib)
 
+    def set_clusters(self, sub2cluster):
+        c = np.ascontiguousarray(sub2cluster, dtype=np.int32)
+        self.lib.FETI4ISetClusterPartition(self.h, c.size, _ip(c))
+        _check(self.lib)
+
     def destroy(self):
         if self.h:
             self.lib.FETI4IDestroy(self.h)
@@ -292,6 +300,21 @@ class Instance:
         self.lib.FETI4IGetSubdomainSchur(self.h, d, S.ctypes.data_as(C.POINTER(C.c_double)))
         _check(self.lib)
         return S
+
+    def corners(self, d):
+        """HYBRID_FETI corner rows of subdomain d: (cluster row, local DOF, sign) arrays."""
+        n = self.lib.FETI4IGetSubdomainCorners(self.h, d, None, None, None)
+        _check(self.lib)
+        rows = np.zeros(n, np.int32); dofs = np.zeros(n, np.int32); signs = np.zeros(n)
+        self.lib.FETI4IGetSubdomainCorners(self.h, d, _ip(rows), _ip(dofs), _dp(signs))
+        _check(self.lib)
+        return dict(row=rows.astype(np.int64), dof=dofs.astype(np.int64), sign=signs)
+
+    def cluster_info(self):
+        info = np.zeros(4, dtype=np.int32)
+        self.lib.FETI4IGetClusterInfo(self.h, _ip(info))
+        _check(self.lib)
+        return dict(method=int(info[0]), clusters=int(info[1]), corner_rows=int(info[2]), kernel_size=int(info[3]))
 
     def kernel(self, d):
         inf = self.subdomain_info(d)

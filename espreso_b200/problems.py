@@ -43,6 +43,11 @@ class Problem:
     def ndofs(self):
         return self.n_nodes * self.dpn
 
+    def sub_cluster(self):
+        """Cluster of every subdomain: the grid's clusters, subdomains numbered cluster by cluster."""
+        per = int(np.prod(self.grid[1]))
+        return np.arange(int(self.elem_domain.max()) + 1) // per
+
     def elem_dofs(self):
         d = self.dpn
         return (d * self.elem_nodes[:, :, None] + np.arange(d)[None, None, :]).reshape(self.elem_nodes.shape[0], -1)
@@ -183,14 +188,78 @@ def heat_cube(clusters=(1, 1, 1), domains=(8, 8, 8), elements=(10, 10, 10), leng
     return Problem(name, 1, coords, nodes, dom, Ke, fe, {0: (fixed, 0.0)}, (clusters, domains, elements))
 
 
+def bisection_boxes(side, levels, lo, hi, seed=0):
+    """Seeded recursive bisection of an element box into 2**levels boxes.
+
+    Level l splits every box along axis l % 3 at a position drawn uniformly from the
+    positions that still let both halves be split by the remaining levels on that axis
+    into pieces of lo..hi elements.  Returns a list of (origin, size) boxes."""
+    rng = np.random.default_rng(seed)
+    per_axis = [len([l for l in range(levels) if l % 3 == a]) for a in range(3)]
+    for a in range(3):
+        n = 2 ** per_axis[a]
+        if not (lo * n <= side[a] <= hi * n):
+            raise ValueError(f"side {side[a]} cannot be split into {n} pieces of {lo}..{hi} elements")
+    boxes = [((0, 0, 0), tuple(int(v) for v in side))]
+    done = [0, 0, 0]
+    for level in range(levels):
+        ax = level % 3
+        done[ax] += 1
+        pieces = 2 ** (per_axis[ax] - done[ax])          # pieces each half still becomes
+        out = []
+        for org, size in boxes:
+            n = size[ax]
+            amin = max(lo * pieces, n - hi * pieces)
+            amax = min(hi * pieces, n - lo * pieces)
+            a = int(rng.integers(amin, amax + 1))
+            s1, s2 = list(size), list(size)
+            s1[ax], s2[ax] = a, n - a
+            o2 = list(org)
+            o2[ax] += a
+            out += [(org, tuple(s1)), (tuple(o2), tuple(s2))]
+        boxes = out
+    return boxes
+
+
+def uneven_cube(physics="elasticity", side=(94, 94, 94), levels=9, lo=6, hi=14, seed=0, name=None, **kw):
+    """Unit cube whose subdomains come from seeded recursive bisection (2**levels subdomains of
+    lo..hi elements per side).  Elasticity: x=0 clamped, gravity; heat: the heat_cube setup."""
+    gen = elasticity_cube if physics == "elasticity" else heat_cube
+    P = gen(domains=(1, 1, 1), elements=tuple(side), name=name or f"{physics}_uneven", **kw)
+    boxes = bisection_boxes(side, levels, lo, hi, seed)
+    h = [1.0 / n for n in side]
+    ijk = np.rint(P.coords[P.elem_nodes[:, 0]] / np.asarray(h)[None, :]).astype(np.int64)
+    dom = np.full(P.elem_nodes.shape[0], -1, dtype=np.int64)
+    for d, (org, size) in enumerate(boxes):
+        m = np.all((ijk >= np.asarray(org)) & (ijk < np.asarray(org) + np.asarray(size)), axis=1)
+        dom[m] = d
+    assert (dom >= 0).all()
+    order = np.argsort(dom, kind="stable")
+    return Problem(P.name, P.dpn, P.coords, P.elem_nodes[order], dom[order], P.Ke[order], P.fe[order], P.dirichlet,
+                   ((1, 1, 1), (len(boxes), 1, 1), tuple(side)))
+
+
+def traction_loads(P: Problem, nrhs, seed=0, sigma=1e6, face_axis=0):
+    """Load cases of seeded random nodal tractions on the face x = 1: every DOF of every
+    node of the face draws N(0, sigma) (Pa per node; the cube is the unit cube)."""
+    rng = np.random.default_rng(seed)
+    face = np.nonzero(np.abs(P.coords[:, face_axis] - P.coords[:, face_axis].max()) < 1e-12)[0]
+    R = np.zeros((nrhs, P.ndofs))
+    dofs = (P.dpn * face[:, None] + np.arange(P.dpn)[None, :]).ravel()
+    R[:, dofs] = rng.normal(0.0, sigma, size=(nrhs, dofs.size))
+    return R
+
+
 def _grid_element_index(nodes, coords, ne, h):
     lo = coords[nodes[:, 0]]
     ijk = np.rint(lo / np.asarray(h)[None, :]).astype(np.int64)
     return ijk[:, 0] + ne[0] * (ijk[:, 1] + ne[1] * ijk[:, 2])
 
 
-def make_instance(problem: Problem, iopts=None, ropts=None, ext=None, batched=True):
-    """Push a problem through the FETI4I API exactly as a caller would."""
+def make_instance(problem: Problem, iopts=None, ropts=None, ext=None, batched=True, clusters=None):
+    """Push a problem through the FETI4I API exactly as a caller would.
+
+    ``clusters``: subdomain -> cluster map passed with FETI4ISetClusterPartition (HYBRID_FETI)."""
     from . import feti4i as F
     if ext:
         for k, v in ext.items():
@@ -203,6 +272,8 @@ def make_instance(problem: Problem, iopts=None, ropts=None, ext=None, batched=Tr
         for e in range(problem.elem_nodes.shape[0]):
             M.add_element(problem.elem_nodes[e], dofs[e], problem.Ke[e])
     M.set_partition(problem.elem_domain)
+    if clusters is not None:
+        M.set_clusters(clusters)
     dd, dv = problem.dirichlet_dofs()
     try:
         inst = F.Instance(M, problem.rhs(), dd, dv, iopts=iopts, ropts=ropts)
@@ -225,6 +296,14 @@ CONFIGS = {
     "c2_heat_512": dict(kind="heat", domains=(8, 8, 8), elements=(10, 10, 10)),
     # smaller variant of the heat workload (profiling captures; a few GB on the device)
     "c2_heat_216": dict(kind="heat", domains=(6, 6, 6), elements=(10, 10, 10)),
+    # 512 subdomains of 6..14 elements per side by seeded recursive bisection of a 94^3 grid
+    "c3_elasticity_uneven": dict(kind="uneven", physics="elasticity", side=(94, 94, 94), levels=9, lo=6, hi=14),
+    # the same construction at 64 subdomains
+    "c3_elasticity_uneven_64": dict(kind="uneven", physics="elasticity", side=(40, 40, 40), levels=6, lo=6, hi=14),
+    # Hybrid Total FETI: 4x4x4 clusters of 2x2x2 subdomains of 12^3 elements (run with --method 1)
+    "c4_htfeti": dict(kind="elasticity", clusters=(4, 4, 4), domains=(2, 2, 2), elements=(12, 12, 12)),
+    # the same cluster structure at 2x2x2 clusters of 2x2x2 subdomains of 6^3 elements
+    "c4_htfeti_small": dict(kind="elasticity", clusters=(2, 2, 2), domains=(2, 2, 2), elements=(6, 6, 6)),
 }
 
 
@@ -234,4 +313,6 @@ def build_config(name, **over):
     kind = cfg.pop("kind")
     if kind == "elasticity":
         return elasticity_cube(**cfg, name=name)
+    if kind == "uneven":
+        return uneven_cube(**cfg, name=name)
     return heat_cube(**cfg, name=name)

@@ -25,6 +25,13 @@ const char *FETI4IGetLastError(void);
  * elements are split into FETI4I_SUBDOMAINS contiguous blocks. */
 void FETI4ISetSubdomainPartition(FETI4IMatrix matrix, FETI4IInt size, FETI4IInt *elem2sub);
 
+/* Subdomain -> cluster map for FETI_METHOD = 1 (HYBRID_FETI).  The reference runs
+ * one cluster per MPI process (src/mesh/preprocessing/fetidata.cpp:146-188,
+ * src/assembler/constraints/equalityconstraints.cpp:504-555); here one process
+ * holds several clusters.  Without it HYBRID_FETI uses one cluster of all
+ * subdomains, as a single reference process does. */
+void FETI4ISetClusterPartition(FETI4IMatrix matrix, FETI4IInt nsubdomains, const FETI4IInt *sub2cluster);
+
 /* Batched FETI4IAddElement (src/app/apiwrapper/wrapper.cpp:140-165): nelems
  * elements with the same node/DOF counts, arrays laid out element after element. */
 void FETI4IAddElements(FETI4IMatrix matrix, FETI4IInt type, FETI4IInt nelems, FETI4IInt nodesSize, FETI4IInt *nodes,
@@ -89,6 +96,13 @@ void FETI4IGetSubdomainSchur(FETI4IInstance instance, FETI4IInt subdomain, FETI4
 void FETI4IGetSubdomainKernel(FETI4IInstance instance, FETI4IInt subdomain, FETI4IReal *R);
 /* x := K_reg^-1 x for one subdomain (host factor; local DOF order) */
 void FETI4IApplySubdomainKplus(FETI4IInstance instance, FETI4IInt subdomain, FETI4IReal *x);
+/* HYBRID_FETI corner rows B0 of one subdomain: cluster-local row, local DOF and sign per entry
+ * (one DOF per row).  Returns the entry count; null arrays only query it. */
+FETI4IInt FETI4IGetSubdomainCorners(FETI4IInstance instance, FETI4IInt subdomain, FETI4IInt *rows, FETI4IInt *dofs,
+                                    FETI4IReal *signs);
+/* info[0] FETI method, info[1] clusters (subdomains for TOTAL_FETI), info[2] corner rows over all
+ * clusters, info[3] dual kernel dimension */
+void FETI4IGetClusterInfo(FETI4IInstance instance, FETI4IInt *info);
 /* b (dual size) and e (kernel size) of the current right-hand side */
 void FETI4IGetDualRhs(FETI4IInstance instance, FETI4IReal *b, FETI4IReal *e);
 

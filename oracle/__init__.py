@@ -20,6 +20,10 @@ baseline leg.  It is a plain numpy/scipy restatement of ESPRESO's
                            (src/solver/specific/itersolver.cpp,
                            src/solver/specific/cpu/itersolvercpu.cpp,
                            src/solver/specific/cluster.cpp)
+* ``oracle.htfeti``     -- Hybrid Total FETI: corner nodes, B0 corner gluing,
+                           the cluster solve with F0 and S_alpha, cluster
+                           kernels (src/mesh/preprocessing/fetidata.cpp,
+                           src/solver/specific/cluster.cpp)
 
 Parity pins: the oracle's displacements are checked against the
 reference's own regression presets (benchmarks/**/HEXA8*.emr, stored as

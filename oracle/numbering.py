@@ -88,10 +88,12 @@ class Numbering:
         idx_of = {k: i for i, k in enumerate(ordered0)}
         ivals = sorted(((k[0], k[1], idx_of[k]) for k in keys), key=functools.cmp_to_key(_cmp_domains))
         self.intervals = []            # list of (domains tuple, node array sorted by ID)
+        self.interval_ext = []         # True for intervals of the external-surface group
         perm = []
         for doms, grp, _ in ivals:
             nodes = np.array(sorted(groups[(doms, grp)]), dtype=np.int64)
             self.intervals.append((doms, nodes))
+            self.interval_ext.append(grp == 0)
             perm.append(nodes)
         self.perm = np.concatenate(perm)                 # new index -> node ID
 

@@ -24,6 +24,14 @@ CASES = {
                          [3, 2, 1, 1, 2, 3, 4, 3, 4], "heat",
                          [("TOP", "MAX", "TEMPERATURE"), ("BOTTOM", "MIN", "TEMPERATURE"),
                           ("ALL_ELEMENTS", "AVG", "TEMPERATURE")]),
+    # HYBRID_FETI runs of the same cases: one cluster per process, clusters = args[0:3]
+    "pressure_hexa8_hybrid": ("benchmarks/linearElasticity3D/steadystate/pressure/HEXA8.HYBRID_FETI.emr",
+                              [2, 2, 1, 1, 2, 2, 5, 5, 5], "elasticity",
+                              [("Z1", "MIN", "DISPLACEMENT"), ("Z1", "MAX", "DISPLACEMENT")]),
+    "heat_hexa8_hybrid": ("benchmarks/diffusion3D/steadystate/simple/HEXA8.HYBRID_FETI.emr",
+                          [3, 2, 1, 1, 2, 3, 4, 3, 4], "heat",
+                          [("TOP", "MAX", "TEMPERATURE"), ("BOTTOM", "MIN", "TEMPERATURE"),
+                           ("ALL_ELEMENTS", "AVG", "TEMPERATURE")]),
 }
 
 

@@ -107,7 +107,7 @@ def test_host_operators_reproduce_solution(case, prec):
 def test_error_paths():
     P = CASES["elast_2x2x2"]()
     with pytest.raises(F.FETI4IError, match="HYBRID"):
-        problems.make_instance(P, iopts={F.FETI_METHOD: 1, F.VERBOSE_LEVEL: 0}, ext={F.EXT_HOST_ONLY: 1})
+        problems.make_instance(P, iopts={F.FETI_METHOD: 2, F.VERBOSE_LEVEL: 0}, ext={F.EXT_HOST_ONLY: 1})
     with pytest.raises(F.FETI4IError, match="PCG"):
         problems.make_instance(P, iopts={F.CGSOLVER: 3, F.VERBOSE_LEVEL: 0}, ext={F.EXT_HOST_ONLY: 1})
     with pytest.raises(F.FETI4IError, match="PRECONDITIONER"):
