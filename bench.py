@@ -46,6 +46,11 @@ def parse():
                     help="-1 autotuned (default), 0 register prefetch, 1 TMA bulk pipeline")
     ap.add_argument("--delta", type=float, default=0.1, help="residual replacement threshold")
     ap.add_argument("--nrhs", type=int, default=32, help="load cases of the batched (multi-RHS) leg, 0 to skip")
+    ap.add_argument("--method", type=int, default=0, choices=[0, 1],
+                    help="FETI_METHOD: 0 Total FETI, 1 Hybrid Total FETI on the config's clusters")
+    ap.add_argument("--loads", default="scaled", choices=["scaled", "traction"],
+                    help="batched leg load cases: scaled copies of the config load, or seeded N(0,1e6) "
+                         "nodal tractions on the x=1 face")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -201,12 +206,13 @@ def run_ours(args):
     P = problems.build_config(args.config)
     rhs = P.rhs()
     inst = problems.make_instance(P, iopts={F.PRECONDITIONER: args.precond, F.VERBOSE_LEVEL: 0,
-                                            F.MAX_ITERATIONS: 5000},
+                                            F.MAX_ITERATIONS: 5000, F.FETI_METHOD: args.method},
                                   ropts={F.PRECISION: args.precision},
                                   ext={F.EXT_SCHUR_PRECISION: SCHUR[args.schur],
                                        F.EXT_TILE_KERNEL: max(0, args.tile_kernel),
                                        F.EXT_AUTOTUNE: 1 if args.tile_kernel < 0 else 0,
-                                       F.EXT_RELIABLE_DELTA: args.delta})
+                                       F.EXT_RELIABLE_DELTA: args.delta},
+                                  clusters=P.sub_cluster() if args.method == 1 else None)
     setup_s = time.time() - t0
     st0 = inst.stats()
     sol = np.zeros(P.ndofs)
@@ -244,7 +250,10 @@ def run_ours(args):
     batched = None
     if args.nrhs > 0:
         rng = np.random.default_rng(1)
-        R = np.stack([rhs * rng.uniform(0.5, 2.0) for _ in range(args.nrhs)])
+        if args.loads == "traction":
+            R = problems.traction_loads(P, args.nrhs, seed=1)
+        else:
+            R = np.stack([rhs * rng.uniform(0.5, 2.0) for _ in range(args.nrhs)])
         inst.solve_multi(R)
         bms = [inst.solve_multi_resident(args.nrhs) for _ in range(max(1, args.steps))]
         stb = inst.stats()
@@ -292,8 +301,11 @@ def run_ours(args):
         "config": {"workload": args.config, "subdomains": int(st["subdomains"]), "dual_size": int(st["dual_size"]),
                    "kernel_size": nK, "precond": args.precond, "schur": args.schur, "precision": args.precision,
                    "pcg_iterations": int(st["iterations"]), "replacements": int(st["replacements"]),
-                   "parallelism": f"replicas{world}", "l2": "working set > L2 (Schur tiles "
-                   f"{alg / 1e9:.2f} GB per apply, 126 MB L2)", "wall_ms_per_step": wall,
+                   "method": ["TOTAL_FETI", "HYBRID_FETI"][args.method], "loads": args.loads,
+                   "parallelism": f"replicas{world}",
+                   "l2": (f"working set > L2 (Schur tiles {alg / 1e9:.2f} GB per apply, 126 MB L2)" if alg > 126e6
+                          else f"working set {alg / 1e6:.0f} MB fits in the 126 MB L2 (no flush)"),
+                   "wall_ms_per_step": wall,
                    "setup_s": setup_s, "host_prep_s": st0["prep_seconds"],
                    "tuning": inst.tuning(),
                    "reliable_delta": args.delta},

@@ -57,8 +57,10 @@ struct DevState {
 
 struct DevProblem {
     int nd, NL, nK, NT, KS;     // KS: row stride of the G coefficient arrays (max kernel dimension)
+    int nP;                 // partial G-products: one block per subdomain (nP = nK for Total FETI)
     const int *loff;        // nd+1
-    const int *kof;         // nd+1 kernel offsets
+    const int *kof;         // nd+1 offsets of the subdomains' partial G-product blocks
+    const int *akof;        // nd: offset of the subdomain's kernel block in the dual kernel space
     const int *toff;        // nd+1 T-space offsets
     const int *partner;     // NL: row of the other owner, -1
     const int *tidx;        // NL: global T index of the row's DOF
@@ -68,7 +70,7 @@ struct DevProblem {
     const double *minv;     // NL: 1 / multiplicity
     const double *Gl;       // NL*KS: G coefficients of the row
     const double *Gp;       // NL*KS: G coefficients of the partner row
-    const int *rkof, *rnk;  // NL: kernel offset / dimension of the row's subdomain
+    const int *rkof, *rnk;  // NL: dual kernel offset / dimension of the row's subdomain
     const int *pkof, *pnk;  // NL: same for the partner's subdomain (pnk = 0 without partner)
     const int *trow_ptr;    // NT+1
     const int *trow_idx;    // rows of each T index
@@ -77,7 +79,7 @@ struct DevProblem {
     const int *ell_w;       // per slice: width
     const unsigned short *ell_col;  // column (T index inside the subdomain)
     const double *ell_val;
-    const double *GGtinv;   // nK*nK
+    const double *GGtinv;   // nK x nP, row-major: (GG^T)^-1 times the sum over partial blocks
     const double *bL;       // NL replicated b
     double *x, *r, *w, *z, *y, *p, *Ap, *uT, *vT, *d, *alpha;
     double *part_w, *part_rho, *part_b, *rho_hist;
@@ -105,6 +107,30 @@ struct BlockDev {
     int n_conv_target;
 };
 enum { DONE_W = 0, DONE_RHO = 1, DONE_B = 2, DONE_PN = 3, DONE_COUNT = 8 };
+
+// Hybrid Total FETI cluster correction: F_c = sum_i B_i S_i B_i^T - V M V^T with, per subdomain,
+// V_i = [B_i K_i^+ B0_i^T | G_i^T] (n_i x m_i, column-major) and, per cluster, the dense
+// symmetric M mapping [g0; e0] to [lambda0; alpha].
+struct HybDev {
+    int ncl;
+    int max_nc;                   // largest cluster vector
+    const long long *voff;        // nd: offset of V_i
+    const int *zof;               // nd+1: offsets of the subdomains' slots (m_i = zof[i+1] - zof[i])
+    const int *m0;                // nd: B0 entries of the subdomain (first m0 columns of V_i)
+    const int *vmap;              // per slot: index into its cluster's vector
+    const int *sub_cl;            // nd: cluster of every subdomain
+    const int *cof;               // ncl+1: offsets of the cluster vectors
+    const long long *mof;         // ncl: offset of M_c (nc x nc)
+    const double *M;
+    const double *V;
+    const int *mem_ptr, *mem;     // ncl+1 / nd: members of every cluster, ascending
+    const int *b0dof;             // per slot of a B0 entry: local DOF (slots of e0 unused)
+    const double *b0sign;
+    double *z;                    // per slot: V_i^T x (or [B0 K^+ f; -R^T f])
+    double *w;                    // cluster vectors M z
+    double *part;                 // per CTA of the M kernel: z.w partial
+    int *done;                    // completion counter of the z.w reduction
+};
 
 struct TileSetDev {
     int nitems;
@@ -705,9 +731,9 @@ __global__ void coarse_kernel(DevProblem P, const double *in, double *out, int s
     int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     int lane = threadIdx.x & 31;
     if (row >= P.nK) return;
-    const double *col = P.GGtinv + (size_t)row * P.nK;
+    const double *col = P.GGtinv + (size_t)row * P.nP;
     double s = 0.0;
-    for (int b = lane; b < P.nK; b += 32) s += col[b] * in[b];
+    for (int b = lane; b < P.nP; b += 32) s += col[b] * in[b];
     s = warp_sum(s);
     if (lane == 0) out[row] = s;
 }
@@ -1085,7 +1111,8 @@ __global__ void primal_bt_kernel(DevProblem P, const int *tdof_g, const double *
     g[tdof_g[t]] -= s;
 }
 
-// u += R alpha, merged into the caller's DOF vector (average over subdomains)
+// u += R alpha (dual kernel basis and amplitudes), merged into the caller's DOF vector
+// (average over subdomains)
 __global__ void primal_merge_kernel(DevProblem P, const int *doff, const int *rofs, const double *R, const double *u,
                                     const int *gdof, const double *invm, double *sol) {
     const int d = blockIdx.x;
@@ -1093,9 +1120,165 @@ __global__ void primal_merge_kernel(DevProblem P, const int *doff, const int *ro
     const double *Rd = R + rofs[d];
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         double val = u[doff[d] + i];
-        for (int k = 0; k < nk; ++k) val += Rd[(size_t)k * n + i] * P.alpha[P.kof[d] + k];
+        for (int k = 0; k < nk; ++k) val += Rd[(size_t)k * n + i] * P.alpha[P.akof[d] + k];
         int g = gdof[doff[d] + i];
         if (g >= 0) atomicAdd(&sol[g], val * invm[doff[d] + i]);
+    }
+}
+
+
+// ---------------------------------------------------------------------------------------------
+// Hybrid Total FETI: the cluster correction of the dual operator and the cluster K^+.
+// cond: 0 always, 1 inside the PCG loop, 3 inside the loop on a residual-replacement iteration.
+__device__ __forceinline__ bool hyb_skip(const DevProblem &P, int slot, int cond) {
+    if (cond == 0) return false;
+    const int iter = P.st->iter_base + slot;
+    if (skip_iter(P.st, iter)) return true;
+    return cond == 3 && P.st->replace_iter != iter;
+}
+
+// z_i = V_i^T x_i: one warp per column of V_i.  With x == null the PCG direction
+// p = y + beta p is formed on the fly, as the tile SYMV does (update_kernel stores it later).
+__global__ void hyb_vt_kernel(DevProblem P, HybDev H, const double *x, int slot, int cond) {
+    if (hyb_skip(P, slot, cond)) return;
+    const int d = blockIdx.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int e0 = P.loff[d], ni = P.loff[d + 1] - e0;
+    const int z0 = H.zof[d], m = H.zof[d + 1] - z0;
+    const double *V = H.V + H.voff[d];
+    double beta = 0.0;
+    if (x == nullptr) {
+        const int iter = P.st->iter_base + slot;
+        beta = iter == 0 ? 0.0 : P.scal[SC_RHO] / P.rho_hist[iter - 1];
+    }
+    for (int c = wid; c < m; c += nw) {
+        const double *col = V + (size_t)c * ni;
+        double s = 0.0;
+        if (x == nullptr)
+            for (int r = lane; r < ni; r += 32) s += col[r] * (P.y[e0 + r] + beta * P.p[e0 + r]);
+        else
+            for (int r = lane; r < ni; r += 32) s += col[r] * x[e0 + r];
+        s = warp_sum(s);
+        if (lane == 0) H.z[z0 + c] = s;
+    }
+}
+
+// w_c = M_c z_c for every cluster; z_c is gathered from the member slots in member order.
+// grid (ncl, row blocks); with dot != null the last CTA subtracts sum_c z_c . w_c from *dot.
+constexpr int HM_ROWS = 64;
+__global__ void __launch_bounds__(256) hyb_m_kernel(DevProblem P, HybDev H, int slot, int cond, double *dot) {
+    if (hyb_skip(P, slot, cond)) return;
+    extern __shared__ double hz[];
+    __shared__ double sh[32];
+    __shared__ int s_last;
+    const int c = blockIdx.x;
+    const int nc = H.cof[c + 1] - H.cof[c];
+    for (int i = threadIdx.x; i < nc; i += blockDim.x) hz[i] = 0.0;
+    __syncthreads();
+    for (int q = H.mem_ptr[c]; q < H.mem_ptr[c + 1]; ++q) {
+        const int d = H.mem[q];
+        // the slots of one subdomain map to distinct entries of the cluster vector
+        for (int j = H.zof[d] + threadIdx.x; j < H.zof[d + 1]; j += blockDim.x) hz[H.vmap[j]] += H.z[j];
+        __syncthreads();
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int r0 = blockIdx.y * HM_ROWS, r1 = min(nc, r0 + HM_ROWS);
+    const double *M = H.M + H.mof[c];
+    double zw = 0.0;
+    for (int r = r0 + wid; r < r1; r += nw) {
+        const double *col = M + (size_t)r * nc;    // symmetric: column r = row r
+        double s = 0.0;
+        for (int j = lane; j < nc; j += 32) s += col[j] * hz[j];
+        s = warp_sum(s);
+        if (lane == 0) {
+            H.w[H.cof[c] + r] = s;
+            zw += s * hz[r];
+        }
+    }
+    if (dot == nullptr) return;
+    zw = block_sum(zw, sh);
+    const int cta = blockIdx.y * gridDim.x + blockIdx.x, ncta = gridDim.x * gridDim.y;
+    if (threadIdx.x == 0) {
+        H.part[cta] = zw;
+        __threadfence();
+        s_last = (atomicAdd(H.done, 1) == ncta - 1);
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        double t = 0.0;
+        for (int i = threadIdx.x; i < ncta; i += blockDim.x) t += __ldcg(&H.part[i]);
+        t = block_sum(t, sh);
+        if (threadIdx.x == 0) {
+            *dot -= t;
+            *H.done = 0;
+        }
+    }
+}
+
+// y_i -= V_i w_{c(i)}: one thread per row
+__global__ void hyb_v_kernel(DevProblem P, HybDev H, double *y, int slot, int cond) {
+    if (hyb_skip(P, slot, cond)) return;
+    extern __shared__ double wl[];
+    const int d = blockIdx.x;
+    const int e0 = P.loff[d], ni = P.loff[d + 1] - e0;
+    const int z0 = H.zof[d], m = H.zof[d + 1] - z0;
+    const double *wc = H.w + H.cof[H.sub_cl[d]];
+    for (int j = threadIdx.x; j < m; j += blockDim.x) wl[j] = wc[H.vmap[z0 + j]];
+    __syncthreads();
+    const double *V = H.V + H.voff[d];
+    for (int r = threadIdx.x; r < ni; r += blockDim.x) {
+        double s = 0.0;
+        for (int c = 0; c < m; ++c) s += V[(size_t)c * ni + r] * wl[c];
+        y[e0 + r] -= s;
+    }
+}
+
+// cluster K^+ on primal vectors, step 1: z_i = [B0_i (K_i^+ x_i); -R_i^T x_i]
+__global__ void hyb_kz_kernel(DevProblem P, HybDev H, const int *doff, const int *rofs, const double *R,
+                              const double *kx, const double *x) {
+    __shared__ double sh[32 * KMAX];
+    const int d = blockIdx.x;
+    const int n = doff[d + 1] - doff[d], z0 = H.zof[d], m0 = H.m0[d], nk = H.zof[d + 1] - z0 - m0;
+    for (int j = threadIdx.x; j < m0; j += blockDim.x) H.z[z0 + j] = H.b0sign[z0 + j] * kx[doff[d] + H.b0dof[z0 + j]];
+    const double *Rd = R + rofs[d];
+    double acc[KMAX];
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k) acc[k] = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double xi = x[doff[d] + i];
+        for (int k = 0; k < nk; ++k) acc[k] += Rd[(size_t)k * n + i] * xi;
+    }
+    block_sum_k(acc, sh);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < nk; ++k) H.z[z0 + m0 + k] = -acc[k];
+}
+
+// step 2: g_i = x_i - B0_i^T lambda0 (one thread walks a subdomain's corner entries: a corner DOF
+// can appear in several rows of one subdomain)
+__global__ void hyb_copy_kernel(const double *x, double *g, int ntot) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ntot; i += gridDim.x * blockDim.x) g[i] = x[i];
+}
+__global__ void hyb_kb0_kernel(DevProblem P, HybDev H, const int *doff, double *g) {
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= P.nd) return;
+    const int z0 = H.zof[d], m0 = H.m0[d];
+    const double *wc = H.w + H.cof[H.sub_cl[d]];
+    for (int j = 0; j < m0; ++j) g[doff[d] + H.b0dof[z0 + j]] -= H.b0sign[z0 + j] * wc[H.vmap[z0 + j]];
+}
+
+// step 3: out_i += R_i alpha_i
+__global__ void hyb_kr_kernel(DevProblem P, HybDev H, const int *doff, const int *rofs, const double *R, double *out) {
+    const int d = blockIdx.x;
+    const int n = doff[d + 1] - doff[d], z0 = H.zof[d], m0 = H.m0[d], nk = H.zof[d + 1] - z0 - m0;
+    const double *wc = H.w + H.cof[H.sub_cl[d]];
+    const double *Rd = R + rofs[d];
+    double a[KMAX];
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k) a[k] = k < nk ? wc[H.vmap[z0 + m0 + k]] : 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double s = 0.0;
+        for (int k = 0; k < nk; ++k) s += Rd[(size_t)k * n + i] * a[k];
+        out[doff[d] + i] += s;
     }
 }
 
@@ -1152,6 +1335,20 @@ struct GpuSolver::Impl {
     int max_T = 0, ntot = 0, n_caller = 0;
     int *d_doff = nullptr, *d_rofs = nullptr, *d_gdof = nullptr, *d_rdof = nullptr, *d_tdof_g = nullptr;
     double *d_invm = nullptr, *d_R = nullptr, *d_rsign = nullptr, *d_rc = nullptr;
+    // dual kernel basis per subdomain (the subdomain kernel, or the cluster kernel R_i H_i)
+    double *d_Rd = nullptr;
+    int *d_rdofs = nullptr;
+    std::vector<int> dual_to_partial;   // dual kernel index -> one partial slot holding it
+    // Hybrid Total FETI
+    bool hybrid = false;
+    HybDev H{};
+    int hyb_max_m = 0, hyb_rows = 1;
+    double *d_h = nullptr;              // primal scratch of the cluster K^+
+    void upload_hybrid(const Decomposition &dec, const Prep &prep);
+    // y -= V M V^T x (cond as hyb_skip; x null: the PCG direction y + beta p; dot: p.Ap to correct)
+    void launch_hybrid_F(const double *x, double *y, int slot, int cond, double *dot);
+    // out = K_c^+ in on the concatenated local primal vectors (Total FETI: K^+ in)
+    void launch_kplus_dual(const double *in, double *out);
     double *d_f = nullptr, *d_kf = nullptr, *d_g = nullptr, *d_rhs = nullptr, *d_sol = nullptr;
     double *h_pinned = nullptr;
     size_t h_pinned_n = 0;
@@ -1169,6 +1366,10 @@ struct GpuSolver::Impl {
     void launch_symm(const TileSetHost &T, bool src32, const double *x64, const float *x32, double *out, int slot,
                      int mode);
     void launch_block_iteration(int slot);
+    // block cluster correction y -= V M V^T x for nr columns
+    double *bh_z = nullptr, *bh_w = nullptr, *bh_part = nullptr;
+    int *bh_done = nullptr;
+    void launch_block_hybrid(const double *x, double *y, int slot, int cond, double *dot);
     // element data for the adjoint sensitivities
     int *el_dofs = nullptr;
     double *el_K = nullptr, *el_out = nullptr, *el_u = nullptr, *el_v = nullptr;
@@ -1226,7 +1427,7 @@ void GpuSolver::Impl::upload_kplus(const Decomposition &dec, const Prep &prep, c
                                    const std::vector<int> &toff) {
     const int nd = dec.ndom;
     const int dpn = dec.dpn;
-    std::vector<int> n(nd), tn(nd), doff(nd + 1, 0), rofs(nd + 1, 0);
+    std::vector<int> n(nd), tn(nd), doff(nd + 1, 0), rofs(nd + 1, 0), rdofs(nd + 1, 0);
     std::vector<long long> tile0(nd + 1, 0);
     max_T = 0;
     for (int d = 0; d < nd; ++d) {
@@ -1235,12 +1436,13 @@ void GpuSolver::Impl::upload_kplus(const Decomposition &dec, const Prep &prep, c
         max_T = std::max(max_T, tn[d]);
         doff[d + 1] = doff[d] + n[d];
         rofs[d + 1] = rofs[d] + n[d] * prep.sub[d].nk;
+        rdofs[d + 1] = rdofs[d] + n[d] * prep.sub[d].dnk;
         tile0[d + 1] = tile0[d] + (long long)tn[d] * (tn[d] + 1) / 2;
     }
     FETI_CHECK(sizeof(double) * TILE * (size_t)max_T <= 200 * 1024, "FETI4I: subdomain too large for the device K+ kernel");
     ntot = doff[nd];
     std::vector<int> pos(ntot), gdof(ntot), tdof_g(toff[nd]);
-    std::vector<double> invm(ntot), R(rofs[nd]);
+    std::vector<double> invm(ntot), R(rofs[nd]), Rd(prep.method == 1 ? rdofs[nd] : 0);
     std::vector<double> L((size_t)tile0[nd] * TILE * TILE, 0.0);
     n_caller = 0;
     for (int d = 0; d < nd; ++d) {
@@ -1255,6 +1457,7 @@ void GpuSolver::Impl::upload_kplus(const Decomposition &dec, const Prep &prep, c
                 n_caller = std::max(n_caller, g + 1);
             }
         std::copy(S.R.begin(), S.R.end(), R.begin() + rofs[d]);
+        if (prep.method == 1) std::copy(S.Rd.begin(), S.Rd.end(), Rd.begin() + rdofs[d]);
         for (int t = 0; t < S.t; ++t) tdof_g[toff[d] + t] = doff[d] + S.tdof[t];
         const int T = tn[d], nn = n[d];
         for (int J = 0; J < T; ++J)
@@ -1294,6 +1497,14 @@ void GpuSolver::Impl::upload_kplus(const Decomposition &dec, const Prep &prep, c
     d_gdof = upload(gdof);
     d_invm = upload(invm);
     d_R = upload(R);
+    if (prep.method == 1) {
+        d_Rd = upload(Rd);
+        d_rdofs = upload(rdofs);
+        d_h = alloc<double>(ntot);
+    } else {
+        d_Rd = d_R;
+        d_rdofs = d_rofs;
+    }
     d_rdof = upload(rdof);
     d_rsign = upload(rsign);
     d_rc = upload(rc);
@@ -1304,6 +1515,103 @@ void GpuSolver::Impl::upload_kplus(const Decomposition &dec, const Prep &prep, c
     d_rhs = alloc<double>(std::max(1, n_caller));
     d_sol = alloc<double>(std::max(1, n_caller));
     cudaFuncSetAttribute(kplus_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+}
+
+void GpuSolver::Impl::upload_hybrid(const Decomposition &dec, const Prep &prep) {
+    hybrid = prep.method == 1;
+    if (!hybrid) return;
+    const int nd = dec.ndom, ncl = (int)prep.clusters.size();
+    std::vector<long long> voff(nd), mof(ncl);
+    std::vector<int> zof(nd + 1, 0), m0(nd), sub_cl(nd), cof(ncl + 1, 0), mem_ptr(ncl + 1, 0), mem, member_idx(nd, -1);
+    long long mtot = 0;
+    int max_nc = 1;
+    for (int c = 0; c < ncl; ++c) {
+        const ClusterPrep &C = prep.clusters[c];
+        const int nc = C.n0 + C.ka;
+        cof[c + 1] = cof[c] + nc;
+        mof[c] = mtot;
+        mtot += (long long)nc * nc;
+        max_nc = std::max(max_nc, nc);
+        for (size_t i = 0; i < C.members.size(); ++i) {
+            mem.push_back(C.members[i]);
+            member_idx[C.members[i]] = (int)i;
+        }
+        mem_ptr[c + 1] = (int)mem.size();
+    }
+    size_t vtot = 0;
+    int max_m = 1;
+    for (int d = 0; d < nd; ++d) {
+        const SubPrep &S = prep.sub[d];
+        const int m = (int)S.b0_row.size() + S.nk;
+        zof[d + 1] = zof[d] + m;
+        m0[d] = (int)S.b0_row.size();
+        voff[d] = (long long)vtot;
+        vtot += (size_t)S.ni * m;
+        sub_cl[d] = prep.sub_cluster[d];
+        max_m = std::max(max_m, m);
+        FETI_CHECK(S.V.size() == (size_t)S.ni * m, "internal: cluster correction block of a subdomain has the wrong size");
+    }
+    FETI_CHECK(sizeof(double) * (size_t)max_nc <= 200 * 1024 && sizeof(double) * (size_t)max_m <= 200 * 1024,
+               "FETI4I: a cluster's corner problem is too large for the device; use more clusters");
+    std::vector<int> vmap(zof[nd]), b0dof(zof[nd], 0);
+    std::vector<double> b0sign(zof[nd], 0.0), V(vtot), M(mtot);
+    for (int d = 0; d < nd; ++d) {
+        const SubPrep &S = prep.sub[d];
+        const ClusterPrep &C = prep.clusters[sub_cl[d]];
+        const int z0 = zof[d];
+        for (int j = 0; j < m0[d]; ++j) {
+            vmap[z0 + j] = S.b0_row[j];
+            b0dof[z0 + j] = S.b0_dof[j];
+            b0sign[z0 + j] = S.b0_sign[j];
+        }
+        for (int k = 0; k < S.nk; ++k) vmap[z0 + m0[d] + k] = C.n0 + C.akofs[member_idx[d]] + k;
+        std::copy(S.V.begin(), S.V.end(), V.begin() + voff[d]);
+    }
+    for (int c = 0; c < ncl; ++c) std::copy(prep.clusters[c].M.begin(), prep.clusters[c].M.end(), M.begin() + mof[c]);
+    H.ncl = ncl;
+    H.max_nc = max_nc;
+    H.voff = upload(voff);
+    H.zof = upload(zof);
+    H.m0 = upload(m0);
+    H.vmap = upload(vmap);
+    H.sub_cl = upload(sub_cl);
+    H.cof = upload(cof);
+    H.mof = upload(mof);
+    H.M = upload(M);
+    H.V = upload(V);
+    H.mem_ptr = upload(mem_ptr);
+    H.mem = upload(mem);
+    H.b0dof = upload(b0dof);
+    H.b0sign = upload(b0sign);
+    H.z = alloc<double>(zof[nd]);
+    H.w = alloc<double>(cof[ncl]);
+    hyb_rows = (max_nc + HM_ROWS - 1) / HM_ROWS;
+    H.part = alloc<double>((size_t)ncl * hyb_rows);
+    H.done = alloc<int>(1);
+    CUDA_CHECK(cudaMemset(H.done, 0, sizeof(int)));
+    hyb_max_m = max_m;
+    cudaFuncSetAttribute(hyb_m_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(hyb_v_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+}
+
+void GpuSolver::Impl::launch_hybrid_F(const double *x, double *y, int slot, int cond, double *dot) {
+    if (!hybrid) return;
+    hyb_vt_kernel<<<P.nd, 256, 0, stream>>>(P, H, x, slot, cond);
+    hyb_m_kernel<<<dim3(H.ncl, hyb_rows), 256, sizeof(double) * H.max_nc, stream>>>(P, H, slot, cond, dot);
+    hyb_v_kernel<<<P.nd, 256, sizeof(double) * hyb_max_m, stream>>>(P, H, y, slot, cond);
+    CUDA_CHECK(cudaGetLastError());
+}
+
+void GpuSolver::Impl::launch_kplus_dual(const double *in, double *out) {
+    launch_kplus(in, out);
+    if (!hybrid) return;
+    hyb_kz_kernel<<<P.nd, 256, 0, stream>>>(P, H, d_doff, d_rofs, d_R, out, in);
+    hyb_m_kernel<<<dim3(H.ncl, hyb_rows), 256, sizeof(double) * H.max_nc, stream>>>(P, H, 0, 0, nullptr);
+    hyb_copy_kernel<<<std::max(1, std::min(4096, (ntot + 255) / 256)), 256, 0, stream>>>(in, d_h, ntot);
+    hyb_kb0_kernel<<<(P.nd + 127) / 128, 128, 0, stream>>>(P, H, d_doff, d_h);
+    launch_kplus(d_h, out);
+    hyb_kr_kernel<<<P.nd, 256, 0, stream>>>(P, H, d_doff, d_rofs, d_R, out);
+    CUDA_CHECK(cudaGetLastError());
 }
 
 void GpuSolver::Impl::build_tiles(TileSetHost &T, int prec, const std::vector<const double *> &mats,
@@ -1546,6 +1854,7 @@ void GpuSolver::Impl::launch_iteration(int slot) {
     if (mixed) {
         // residual replacement r = b - F64 x when the previous update asked for it
         launch_tiles(F64, 3, P.x, nullptr, Ax64, slot);
+        launch_hybrid_F(P.x, Ax64, slot, 3, nullptr);
         r0_kernel<<<nd, TPB, sizeof(double) * max_ni, stream>>>(P, Ax64, 1, slot);
     }
     coarse_kernel<<<cgrid, 256, 0, stream>>>(P, P.d, P.alpha, slot, 1);
@@ -1568,6 +1877,7 @@ void GpuSolver::Impl::launch_iteration(int slot) {
         zero2_kernel<<<(P.NL + 255) / 256, 256, 0, stream>>>(P.Ap, Ax64, P.NL);
     }
     launch_tiles(Fop, 1, P.y, P.p, P.Ap, slot);
+    launch_hybrid_F(nullptr, P.Ap, slot, 1, P.scal + SC_PAP);   // p = y + beta p formed on the fly
     update_kernel<<<nd, TPB, sizeof(double) * max_ni, stream>>>(P, slot);
     CUDA_CHECK(cudaGetLastError());
 }
@@ -1579,6 +1889,7 @@ int GpuSolver::Impl::kernels_per_iteration() const {
     if (mixed) k += 2;
     if (opt.precond != PREC_NONE) k += 3 + (opt.precond == PREC_DIRICHLET ? 2 : 0);
     else k += 1;
+    if (hybrid) k += mixed ? 6 : 3;
     return k;
 }
 
@@ -1637,19 +1948,21 @@ void GpuSolver::upload(const Decomposition &dec, const Prep &prep, const SolveOp
     set_smem_limits();
 
     const int nd = dec.ndom;
-    std::vector<int> loff(nd + 1, 0), kof(nd + 1, 0), toff(nd + 1, 0);
+    // kof: partial G-product blocks (one per subdomain, dual kernel columns of the subdomain)
+    std::vector<int> loff(nd + 1, 0), kof(nd + 1, 0), toff(nd + 1, 0), akof(nd, 0);
     for (int d = 0; d < nd; ++d) {
         loff[d + 1] = loff[d] + prep.sub[d].ni;
-        kof[d + 1] = kof[d] + prep.sub[d].nk;
+        kof[d + 1] = kof[d] + prep.sub[d].dnk;
+        akof[d] = prep.kofs[d];
         toff[d + 1] = toff[d] + prep.sub[d].t;
-        FETI_CHECK(prep.sub[d].nk <= KMAX, "FETI4I: kernel dimension above the supported bound");
+        FETI_CHECK(prep.sub[d].nk <= KMAX && prep.sub[d].dnk <= KMAX, "FETI4I: kernel dimension above the supported bound");
     }
     const int NL = loff[nd], NT = toff[nd];
     I.n_lambda = dec.n_lambda;
     I.h_loff = loff;
     I.h_lam.resize(NL);
     int KS = 1;
-    for (int d = 0; d < nd; ++d) KS = std::max(KS, prep.sub[d].nk);
+    for (int d = 0; d < nd; ++d) KS = std::max(KS, prep.sub[d].dnk);
     std::vector<int> partner(NL, -1), tidx(NL), rkof(NL), rnk(NL);
     std::vector<double> ws(NL), minv(NL), Gl((size_t)NL * KS, 0.0);
     I.max_ni = 0;
@@ -1667,9 +1980,9 @@ void GpuSolver::upload(const Decomposition &dec, const Prep &prep, const SolveOp
             tidx[e] = toff[d] + S.trow[r];
             ws[e] = D.w[r] * D.sign[r];
             minv[e] = d1 >= 0 ? 0.5 : 1.0;
-            rkof[e] = kof[d];
-            rnk[e] = S.nk;
-            for (int k = 0; k < S.nk; ++k) Gl[(size_t)e * KS + k] = S.G[(size_t)k * S.ni + r];
+            rkof[e] = akof[d];
+            rnk[e] = S.dnk;
+            for (int k = 0; k < S.dnk; ++k) Gl[(size_t)e * KS + k] = S.Gd[(size_t)k * S.ni + r];
         }
     }
     // partner data of every row (shortens the dependent-load chains of the assembly)
@@ -1724,8 +2037,8 @@ void GpuSolver::upload(const Decomposition &dec, const Prep &prep, const SolveOp
                "FETI4I: subdomain interface too large for the preconditioner kernel");
 
     DevProblem &P = I.P;
-    P.nd = nd; P.NL = NL; P.nK = prep.n_kern; P.NT = NT; P.KS = KS;
-    P.loff = I.upload(loff); P.kof = I.upload(kof); P.toff = I.upload(toff);
+    P.nd = nd; P.NL = NL; P.nK = prep.n_kern; P.NT = NT; P.KS = KS; P.nP = kof[nd];
+    P.loff = I.upload(loff); P.kof = I.upload(kof); P.toff = I.upload(toff); P.akof = I.upload(akof);
     P.partner = I.upload(partner); P.tidx = I.upload(tidx); P.ptidx = I.upload(ptidx);
     P.ws = I.upload(ws); P.pws = I.upload(pws); P.minv = I.upload(minv);
     P.Gl = I.upload(Gl); P.Gp = I.upload(Gp);
@@ -1736,14 +2049,27 @@ void GpuSolver::upload(const Decomposition &dec, const Prep &prep, const SolveOp
     P.scal = I.alloc<double>(SC_COUNT);
     P.done = I.alloc<int>(DONE_COUNT);
     CUDA_CHECK(cudaMemset(P.done, 0, sizeof(int) * DONE_COUNT));
-    P.GGtinv = I.upload(prep.GGt_inv);
+    {
+        // (GG^T)^-1 times the sum over the partial blocks: column b of partial block d, kernel k
+        // is column akof[d] + k of (GG^T)^-1
+        const int nK = prep.n_kern, nP = kof[nd];
+        std::vector<double> Gx((size_t)nK * nP);
+        I.dual_to_partial.assign(nK, -1);
+        for (int d = 0; d < nd; ++d)
+            for (int k = 0; k < prep.sub[d].dnk; ++k) {
+                const int b = kof[d] + k, col = akof[d] + k;
+                for (int r = 0; r < nK; ++r) Gx[(size_t)r * nP + b] = prep.GGt_inv[(size_t)col * nK + r];
+                if (I.dual_to_partial[col] < 0) I.dual_to_partial[col] = b;
+            }
+        P.GGtinv = I.upload(Gx);
+    }
     P.bL = I.alloc<double>(NL);
     P.x = I.alloc<double>(NL); P.r = I.alloc<double>(NL); P.w = I.alloc<double>(NL); P.z = I.alloc<double>(NL);
     P.y = I.alloc<double>(NL); P.p = I.alloc<double>(NL); P.Ap = I.alloc<double>(NL);
     I.Ax64 = I.alloc<double>(NL);
     P.uT = I.alloc<double>(NT); P.vT = I.alloc<double>(NT);
-    P.d = I.alloc<double>(prep.n_kern); P.alpha = I.alloc<double>(prep.n_kern);
-    I.e_dev = I.alloc<double>(prep.n_kern);
+    P.d = I.alloc<double>(P.nP); P.alpha = I.alloc<double>(prep.n_kern);
+    I.e_dev = I.alloc<double>(P.nP);
     P.part_w = I.alloc<double>(nd); P.part_rho = I.alloc<double>(nd); P.part_b = I.alloc<double>(nd);
     P.rho_hist = I.alloc<double>((size_t)opt.max_iterations + 64);
     I.st = I.alloc<DevState>(1);
@@ -1789,6 +2115,7 @@ void GpuSolver::upload(const Decomposition &dec, const Prep &prep, const SolveOp
         }
     }
     I.upload_kplus(dec, prep, loff, toff);
+    I.upload_hybrid(dec, prep);
     CUDA_CHECK(cudaDeviceSynchronize());
 }
 
@@ -1821,8 +2148,8 @@ void GpuSolver::solve_full(const double *rhs, int rhs_size, double *solution, in
         std::memcpy(I.h_pinned, rhs, sizeof(double) * ncp);
         CUDA_CHECK(cudaMemcpyAsync(I.d_rhs, I.h_pinned, sizeof(double) * ncp, cudaMemcpyHostToDevice, I.stream));
         split_rhs_kernel<<<(I.ntot + 255) / 256, 256, 0, I.stream>>>(I.d_rhs, I.d_gdof, I.d_invm, I.d_f, I.ntot);
-        I.launch_kplus(I.d_f, I.d_kf);
-        evec_kernel<<<nd, TPB, 0, I.stream>>>(P, I.d_doff, I.d_rofs, I.d_R, I.d_f, I.e_dev);
+        I.launch_kplus_dual(I.d_f, I.d_kf);
+        evec_kernel<<<nd, TPB, 0, I.stream>>>(P, I.d_doff, I.d_rdofs, I.d_Rd, I.d_f, I.e_dev);
         bvec_kernel<<<(P.NL + 255) / 256, 256, 0, I.stream>>>(P, I.d_rdof, I.d_rsign, I.d_rc, I.d_kf, (double *)P.bL);
         CUDA_CHECK(cudaGetLastError());
     }
@@ -1830,9 +2157,9 @@ void GpuSolver::solve_full(const double *rhs, int rhs_size, double *solution, in
     // primal: u = K^+ (f - B^T lambda) + R alpha, averaged into the caller's DOFs
     primal_rhs_kernel<<<std::max(1, std::min(4096, (I.ntot + 255) / 256)), 256, 0, I.stream>>>(P, I.d_tdof_g, I.d_rsign, I.d_f, I.d_g, I.ntot);
     primal_bt_kernel<<<(P.NT + 255) / 256, 256, 0, I.stream>>>(P, I.d_tdof_g, I.d_rsign, I.d_g);
-    I.launch_kplus(I.d_g, I.d_kf);
+    I.launch_kplus_dual(I.d_g, I.d_kf);
     CUDA_CHECK(cudaMemsetAsync(I.d_sol, 0, sizeof(double) * std::max(1, I.n_caller), I.stream));
-    primal_merge_kernel<<<nd, TPB, 0, I.stream>>>(P, I.d_doff, I.d_rofs, I.d_R, I.d_kf, I.d_gdof, I.d_invm, I.d_sol);
+    primal_merge_kernel<<<nd, TPB, 0, I.stream>>>(P, I.d_doff, I.d_rdofs, I.d_Rd, I.d_kf, I.d_gdof, I.d_invm, I.d_sol);
     CUDA_CHECK(cudaGetLastError());
     const int ncp = std::min(solution_size, I.n_caller);
     CUDA_CHECK(cudaMemcpyAsync(I.h_pinned, I.d_sol, sizeof(double) * std::max(0, ncp), cudaMemcpyDeviceToHost, I.stream));
@@ -1847,7 +2174,9 @@ void GpuSolver::set_rhs(const std::vector<double> &b, const std::vector<double> 
     std::vector<double> bL(I.h_lam.size());
     for (size_t i = 0; i < bL.size(); ++i) bL[i] = b[I.h_lam[i]];
     CUDA_CHECK(cudaMemcpyAsync((void *)I.P.bL, bL.data(), bL.size() * sizeof(double), cudaMemcpyHostToDevice, I.stream));
-    CUDA_CHECK(cudaMemcpyAsync(I.e_dev, e.data(), e.size() * sizeof(double), cudaMemcpyHostToDevice, I.stream));
+    std::vector<double> ep(I.P.nP, 0.0);
+    for (size_t k = 0; k < e.size() && k < I.dual_to_partial.size(); ++k) ep[I.dual_to_partial[k]] = e[k];
+    CUDA_CHECK(cudaMemcpyAsync(I.e_dev, ep.data(), ep.size() * sizeof(double), cudaMemcpyHostToDevice, I.stream));
     CUDA_CHECK(cudaStreamSynchronize(I.stream));
 }
 
@@ -1876,6 +2205,7 @@ void GpuSolver::solve(SolveStats &stats) {
     gt_kernel<<<(P.NL + 255) / 256, 256, 0, I.stream>>>(P, P.alpha, P.x);
     zero_kernel<<<(P.NL + 255) / 256, 256, 0, I.stream>>>(P.p, P.NL);
     I.launch_tiles(I.F64, 0, P.x, nullptr, I.Ax64, 0);
+    I.launch_hybrid_F(P.x, I.Ax64, 0, 0, nullptr);
     r0_kernel<<<nd, TPB, sizeof(double) * I.max_ni, I.stream>>>(P, I.Ax64, 0, 0);
     zero_kernel<<<(P.NL + 255) / 256, 256, 0, I.stream>>>(I.Ax64, P.NL);
     coarse_kernel<<<cgrid, 256, 0, I.stream>>>(P, P.d, P.alpha, 0, 0);
@@ -1938,6 +2268,7 @@ void GpuSolver::apply_F(const double *x_lambda, double *y_lambda, int precision)
     CUDA_CHECK(cudaMemcpyAsync(I.P.w, xL.data(), NL * sizeof(double), cudaMemcpyHostToDevice, I.stream));
     zero_kernel<<<(NL + 255) / 256, 256, 0, I.stream>>>(I.Ax64, NL);
     I.launch_tiles(T, 0, I.P.w, nullptr, I.Ax64, 0);
+    I.launch_hybrid_F(I.P.w, I.Ax64, 0, 0, nullptr);
     CUDA_CHECK(cudaMemcpyAsync(yL.data(), I.Ax64, NL * sizeof(double), cudaMemcpyDeviceToHost, I.stream));
     zero_kernel<<<(NL + 255) / 256, 256, 0, I.stream>>>(I.Ax64, NL);
     CUDA_CHECK(cudaStreamSynchronize(I.stream));
@@ -2285,20 +2616,20 @@ __global__ void __launch_bounds__(256) bcoarse_kernel(DevProblem P, BlockDev B, 
     if (looped && skip_iter(P.st, P.st->iter_base + slot)) return;
     __shared__ double xs[32][33];
     __shared__ double ms[CR][33];
-    const int nr = B.nr, nK = P.nK;
+    const int nr = B.nr, nK = P.nK, nP = P.nP;
     const int r0 = blockIdx.x * CR;
     const int j = threadIdx.x & 31, rg = threadIdx.x >> 5;   // column, row group (8 groups)
     double acc[CR / 8];
 #pragma unroll
     for (int q = 0; q < CR / 8; ++q) acc[q] = 0.0;
-    for (int b0 = 0; b0 < nK; b0 += 32) {
+    for (int b0 = 0; b0 < nP; b0 += 32) {
         for (int t = threadIdx.x; t < 32 * 32; t += blockDim.x) {
             const int b = t >> 5, c = t & 31;
-            xs[b][c] = (b0 + b < nK && c < nr) ? in[(size_t)(b0 + b) * nr + c] : 0.0;
+            xs[b][c] = (b0 + b < nP && c < nr) ? in[(size_t)(b0 + b) * nr + c] : 0.0;
         }
         for (int t = threadIdx.x; t < CR * 32; t += blockDim.x) {
             const int r = t >> 5, c = t & 31;
-            ms[r][c] = (r0 + r < nK && b0 + c < nK) ? P.GGtinv[(size_t)(r0 + r) * nK + b0 + c] : 0.0;
+            ms[r][c] = (r0 + r < nK && b0 + c < nP) ? P.GGtinv[(size_t)(r0 + r) * nP + b0 + c] : 0.0;
         }
         __syncthreads();
 #pragma unroll
@@ -2722,6 +3053,105 @@ tile_symm_kernel(TileSetDev ts, DevProblem P, BlockDev B, const double *x64, con
     }
 }
 
+// ---- Hybrid Total FETI cluster correction for nr columns ([row][rhs] layout)
+// z_i = V_i^T x_i: one warp per column of V_i, lane = (row group, rhs)
+__global__ void bhyb_vt_kernel(DevProblem P, HybDev H, BlockDev B, const double *x, double *z, int slot, int cond) {
+    if (hyb_skip(P, slot, cond)) return;
+    const int nr = B.nr, lg = B.lg;
+    const int d = blockIdx.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int j = lane & (nr - 1), g = lane >> lg, ng = 32 >> lg;
+    const int e0 = P.loff[d], ni = P.loff[d + 1] - e0;
+    const int z0 = H.zof[d], m = H.zof[d + 1] - z0;
+    const double *V = H.V + H.voff[d];
+    for (int c = wid; c < m; c += nw) {
+        const double *col = V + (size_t)c * ni;
+        double s = 0.0;
+        for (int r = g; r < ni; r += ng) s += col[r] * x[(size_t)(e0 + r) * nr + j];
+        for (int o = 16; o >= nr; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+        if (lane < nr) z[(size_t)(z0 + c) * nr + j] = s;
+    }
+}
+
+// w_c = M_c z_c for nr columns; grid (ncl, row blocks); dot: per column p.Ap totals to correct
+__global__ void __launch_bounds__(256) bhyb_m_kernel(DevProblem P, HybDev H, BlockDev B, const double *z, double *w,
+                                                     int slot, int cond, double *dot, double *part, int *done) {
+    if (hyb_skip(P, slot, cond)) return;
+    extern __shared__ double hz[];            // nc x nr
+    __shared__ double s_cols[256];
+    __shared__ int s_last;
+    const int nr = B.nr, lg = B.lg;
+    const int c = blockIdx.x;
+    const int nc = H.cof[c + 1] - H.cof[c];
+    for (int i = threadIdx.x; i < nc * nr; i += blockDim.x) hz[i] = 0.0;
+    __syncthreads();
+    for (int q = H.mem_ptr[c]; q < H.mem_ptr[c + 1]; ++q) {
+        const int d = H.mem[q];
+        const int z0 = H.zof[d], cnt = (H.zof[d + 1] - z0) * nr;
+        for (int t = threadIdx.x; t < cnt; t += blockDim.x)
+            hz[H.vmap[z0 + (t >> lg)] * nr + (t & (nr - 1))] += z[(size_t)z0 * nr + t];
+        __syncthreads();
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int j = lane & (nr - 1), g = lane >> lg, ng = 32 >> lg;
+    const int r0 = blockIdx.y * HM_ROWS, r1 = min(nc, r0 + HM_ROWS);
+    const double *M = H.M + H.mof[c];
+    double zw = 0.0;
+    for (int r = r0 + wid; r < r1; r += nw) {
+        const double *col = M + (size_t)r * nc;
+        double s = 0.0;
+        for (int k = g; k < nc; k += ng) s += col[k] * hz[k * nr + j];
+        for (int o = 16; o >= nr; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+        if (lane < nr) {
+            w[(size_t)(H.cof[c] + r) * nr + j] = s;
+            zw += s * hz[r * nr + j];
+        }
+    }
+    if (dot == nullptr) return;
+    // per-column partial of this CTA: lane j < nr of every warp holds column j
+    s_cols[threadIdx.x] = (lane < nr) ? zw : 0.0;
+    __syncthreads();
+    const int cta = blockIdx.y * gridDim.x + blockIdx.x, ncta = gridDim.x * gridDim.y;
+    if (threadIdx.x < nr) {
+        double t = 0.0;
+        for (int q = 0; q < nw; ++q) t += s_cols[q * 32 + threadIdx.x];
+        part[(size_t)cta * nr + threadIdx.x] = t;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = (atomicAdd(done, 1) == ncta - 1);
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        if (threadIdx.x < nr) {
+            double t = 0.0;
+            for (int q = 0; q < ncta; ++q) t += __ldcg(&part[(size_t)q * nr + threadIdx.x]);
+            dot[threadIdx.x] -= t;
+        }
+        if (threadIdx.x == 0) *done = 0;
+    }
+}
+
+// y_i -= V_i w_{c(i)} for nr columns: one thread per (row, rhs)
+__global__ void bhyb_v_kernel(DevProblem P, HybDev H, BlockDev B, const double *w, double *y, int slot, int cond) {
+    if (hyb_skip(P, slot, cond)) return;
+    extern __shared__ double wl[];            // m_i x nr
+    const int nr = B.nr, lg = B.lg;
+    const int d = blockIdx.x;
+    const int e0 = P.loff[d], ni = P.loff[d + 1] - e0;
+    const int z0 = H.zof[d], m = H.zof[d + 1] - z0;
+    const int cb = H.cof[H.sub_cl[d]];
+    for (int t = threadIdx.x; t < m * nr; t += blockDim.x)
+        wl[t] = w[(size_t)(cb + H.vmap[z0 + (t >> lg)]) * nr + (t & (nr - 1))];
+    __syncthreads();
+    const double *V = H.V + H.voff[d];
+    for (int t = threadIdx.x; t < ni * nr; t += blockDim.x) {
+        const int r = t >> lg, jj = t & (nr - 1);
+        double s = 0.0;
+        for (int c = 0; c < m; ++c) s += V[(size_t)c * ni + r] * wl[c * nr + jj];
+        y[(size_t)e0 * nr + t] -= s;
+    }
+}
+
 __global__ void bchunk_end_kernel(DevProblem P, int chunk) {
     if (threadIdx.x == 0 && blockIdx.x == 0) P.st->iter_base += chunk;
 }
@@ -2799,7 +3229,7 @@ __global__ void bprimal_merge_kernel(DevProblem P, BlockDev B, const int *doff, 
     const double *Rd = R + rofs[d];
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         double val = u[(size_t)j * ntot + doff[d] + i];
-        for (int k = 0; k < nk; ++k) val += Rd[(size_t)k * n + i] * B.alpha[(size_t)(P.kof[d] + k) * B.nr + j];
+        for (int k = 0; k < nk; ++k) val += Rd[(size_t)k * n + i] * B.alpha[(size_t)(P.akof[d] + k) * B.nr + j];
         const int gd = gdof[doff[d] + i];
         if (gd >= 0) atomicAdd(&sol[(size_t)j * nc + gd], val * invm[doff[d] + i]);
     }
@@ -2824,7 +3254,7 @@ void GpuSolver::Impl::ensure_block(int nr) {
     B.Ap = alloc<double>((size_t)NL * nr); B.Ax = alloc<double>((size_t)NL * nr); B.bL = alloc<double>((size_t)NL * nr);
     B.p32 = alloc<float>((size_t)NL * nr);
     B.uT = alloc<double>((size_t)NT * nr); B.vT = alloc<double>((size_t)NT * nr);
-    B.d = alloc<double>((size_t)nK * nr); B.alpha = alloc<double>((size_t)nK * nr); B.e = alloc<double>((size_t)nK * nr);
+    B.d = alloc<double>((size_t)P.nP * nr); B.alpha = alloc<double>((size_t)nK * nr); B.e = alloc<double>((size_t)P.nP * nr);
     B.part = alloc<double>((size_t)2 * nd * nr);
     B.scal = alloc<double>((size_t)SC_COUNT * nr);
     B.rho_hist = alloc<double>((size_t)(opt.max_iterations + 64) * nr);
@@ -2851,7 +3281,32 @@ void GpuSolver::Impl::ensure_block(int nr) {
     blk.f = alloc<double>((size_t)ntot * nr);
     blk.kf = alloc<double>((size_t)ntot * nr);
     blk.g = alloc<double>((size_t)ntot * nr);
+    if (hybrid) {
+        FETI_CHECK(sizeof(double) * (size_t)H.max_nc * nr <= 200 * 1024 &&
+                       sizeof(double) * (size_t)hyb_max_m * nr <= 200 * 1024,
+                   "FETI4ISolveMulti: a cluster's corner problem is too large for this many right-hand sides");
+        int nz = 0, ncv = 0;
+        CUDA_CHECK(cudaMemcpy(&nz, H.zof + P.nd, sizeof(int), cudaMemcpyDeviceToHost));
+        CUDA_CHECK(cudaMemcpy(&ncv, H.cof + H.ncl, sizeof(int), cudaMemcpyDeviceToHost));
+        bh_z = alloc<double>((size_t)nz * nr);
+        bh_w = alloc<double>((size_t)ncv * nr);
+        bh_part = alloc<double>((size_t)H.ncl * hyb_rows * nr);
+        bh_done = alloc<int>(1);
+        CUDA_CHECK(cudaMemset(bh_done, 0, sizeof(int)));
+        cudaFuncSetAttribute(bhyb_m_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        cudaFuncSetAttribute(bhyb_v_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    }
     blk.nr = nr;
+}
+
+void GpuSolver::Impl::launch_block_hybrid(const double *x, double *y, int slot, int cond, double *dot) {
+    if (!hybrid) return;
+    const int nr = blk.nr;
+    bhyb_vt_kernel<<<P.nd, 256, 0, stream>>>(P, H, blk.B, x, bh_z, slot, cond);
+    bhyb_m_kernel<<<dim3(H.ncl, hyb_rows), 256, sizeof(double) * (size_t)H.max_nc * nr, stream>>>(
+        P, H, blk.B, bh_z, bh_w, slot, cond, dot, bh_part, bh_done);
+    bhyb_v_kernel<<<P.nd, 256, sizeof(double) * (size_t)hyb_max_m * nr, stream>>>(P, H, blk.B, bh_w, y, slot, cond);
+    CUDA_CHECK(cudaGetLastError());
 }
 
 // persistent launch: as many CTAs as are resident at once (they drain the unit queue)
@@ -2903,6 +3358,7 @@ void GpuSolver::Impl::launch_block_iteration(int slot) {
     const bool mixed = opt.schur_precision != SCHUR_FP64;
     if (mixed) {
         launch_symm(F64, false, B.x, nullptr, B.Ax, slot, 3);
+        launch_block_hybrid(B.x, B.Ax, slot, 3, nullptr);
         br0_kernel<<<nd, TPB, 0, stream>>>(P, B, 1, slot);
     }
     bcoarse_kernel<<<cgrid, 256, 0, stream>>>(P, B, B.d, B.alpha, slot, 1);
@@ -2919,6 +3375,7 @@ void GpuSolver::Impl::launch_block_iteration(int slot) {
     bp_kernel<<<std::max(1, std::min(4096, (P.NL * blk.nr + 255) / 256)), 256, 0, stream>>>(P, B, slot);
     if (mixed) launch_symm(Flow, true, nullptr, B.p32, B.Ap, slot, 1);
     else launch_symm(F64, false, B.p, nullptr, B.Ap, slot, 1);
+    launch_block_hybrid(B.p, B.Ap, slot, 1, B.scal + SC_PAP * blk.nr);
     bupdate_kernel<<<nd, TPB, 0, stream>>>(P, B, slot);
     CUDA_CHECK(cudaGetLastError());
 }
@@ -2946,8 +3403,8 @@ void GpuSolver::solve_multi(const double *rhs, int nrhs, int rhs_size, double *s
         bsplit_rhs_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, I.stream>>>(I.blk.rhs, nc, I.d_gdof, I.d_invm, I.blk.f,
                                                                               ntot, nr);
         CUDA_CHECK(cudaMemsetAsync(I.blk.kf, 0, sizeof(double) * (size_t)ntot * nr, I.stream));
-        for (int j = 0; j < nrhs; ++j) I.launch_kplus(I.blk.f + (size_t)j * ntot, I.blk.kf + (size_t)j * ntot);
-        bevec_kernel<<<nd * nr, TPB, 0, I.stream>>>(P, B, I.d_doff, I.d_rofs, I.d_R, I.blk.f, ntot);
+        for (int j = 0; j < nrhs; ++j) I.launch_kplus_dual(I.blk.f + (size_t)j * ntot, I.blk.kf + (size_t)j * ntot);
+        bevec_kernel<<<nd * nr, TPB, 0, I.stream>>>(P, B, I.d_doff, I.d_rdofs, I.d_Rd, I.blk.f, ntot);
         bbvec_kernel<<<(P.NL * nr + 255) / 256, 256, 0, I.stream>>>(P, B, I.d_rdof, I.d_rsign, I.d_rc, I.blk.kf, ntot);
         CUDA_CHECK(cudaGetLastError());
     }
@@ -2967,6 +3424,7 @@ void GpuSolver::solve_multi(const double *rhs, int nrhs, int rhs_size, double *s
     bgt_kernel<<<(P.NL * nr + 255) / 256, 256, 0, I.stream>>>(P, B, B.alpha, B.x);
     CUDA_CHECK(cudaMemsetAsync(B.p, 0, sizeof(double) * (size_t)P.NL * nr, I.stream));
     I.launch_symm(I.F64, false, B.x, nullptr, B.Ax, 0, 0);
+    I.launch_block_hybrid(B.x, B.Ax, 0, 0, nullptr);
     br0_kernel<<<nd, TPB, 0, I.stream>>>(P, B, 0, 0);
     bcoarse_kernel<<<cgrid, 256, 0, I.stream>>>(P, B, B.d, B.alpha, 0, 0);
     bpnorm_kernel<<<nd, TPB, 0, I.stream>>>(P, B);
@@ -3014,9 +3472,9 @@ void GpuSolver::solve_multi(const double *rhs, int nrhs, int rhs_size, double *s
     if (solutions) {
         bprimal_rhs_kernel<<<4096, 256, 0, I.stream>>>(P, B, I.d_tdof_g, I.d_rsign, I.blk.f, I.blk.g, ntot);
         bprimal_bt_kernel<<<(P.NT * nr + 255) / 256, 256, 0, I.stream>>>(P, B, I.d_tdof_g, I.d_rsign, I.blk.g, ntot);
-        for (int j = 0; j < nrhs; ++j) I.launch_kplus(I.blk.g + (size_t)j * ntot, I.blk.kf + (size_t)j * ntot);
+        for (int j = 0; j < nrhs; ++j) I.launch_kplus_dual(I.blk.g + (size_t)j * ntot, I.blk.kf + (size_t)j * ntot);
         CUDA_CHECK(cudaMemsetAsync(I.blk.sol, 0, sizeof(double) * (size_t)nc * nr, I.stream));
-        bprimal_merge_kernel<<<nd * nr, TPB, 0, I.stream>>>(P, B, I.d_doff, I.d_rofs, I.d_R, I.blk.kf, I.d_gdof, I.d_invm,
+        bprimal_merge_kernel<<<nd * nr, TPB, 0, I.stream>>>(P, B, I.d_doff, I.d_rdofs, I.d_Rd, I.blk.kf, I.d_gdof, I.d_invm,
                                                            I.blk.sol, nc, ntot);
         CUDA_CHECK(cudaGetLastError());
         const int ncp = std::min(solution_size, I.n_caller);
