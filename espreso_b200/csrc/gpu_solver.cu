@@ -2602,6 +2602,20 @@ __device__ __forceinline__ double gt_alpha_col(const DevProblem &P, int e, int j
     return s;
 }
 
+// Same with a compile-time kernel width KC (every row's coefficients padded to KC with zeros,
+// the amplitudes padded by KC zero rows): the loads of all k are independent, so the rows a
+// thread keeps in flight overlap their latencies.  KC = 0 falls back to the per-row counts.
+template <int KC>
+__device__ __forceinline__ double gt_alpha_colk(const DevProblem &P, int e, int j, int nr, const double *a) {
+    if (KC == 0) return gt_alpha_col(P, e, j, nr, a);
+    const int ko = P.rkof[e], po = P.pkof[e];
+    const double *g = P.Gl + (size_t)e * KC, *gp = P.Gp + (size_t)e * KC;
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < KC; ++k) s += g[k] * a[(size_t)(ko + k) * nr + j] + gp[k] * a[(size_t)(po + k) * nr + j];
+    return s;
+}
+
 // conv[j]: -1 running, -2 zero right-hand side (frozen from the start), >= 0 stop iteration
 __device__ __forceinline__ bool col_frozen(const BlockDev &B, int j, int iter) {
     const int c = B.conv[j];
@@ -2707,7 +2721,7 @@ __global__ void btol_kernel(DevProblem P, BlockDev B) {
 }
 
 // w = r - G^T alpha, |w_j|^2; u_T = B^T W w; lumped v_T = K_TT u_T (columns)
-template <int PRECOND>
+template <int PRECOND, int KC>
 __global__ void bw_prec_kernel(DevProblem P, BlockDev B, int slot) {
     __shared__ double sh[8 * 32];
     __shared__ double cols[32];
@@ -2726,7 +2740,7 @@ __global__ void bw_prec_kernel(DevProblem P, BlockDev B, int slot) {
             if (i < cnt) {
                 const int e = e0 + (i >> B.lg), j = i & (nr - 1);
                 rv[u] = B.r[(size_t)e * nr + j];
-                ga[u] = gt_alpha_col(P, e, j, nr, B.alpha);
+                ga[u] = gt_alpha_colk<KC>(P, e, j, nr, B.alpha);
                 mv[u] = P.minv[e];
             }
         }
@@ -2811,7 +2825,8 @@ __global__ void bz_kernel(DevProblem P, BlockDev B, int slot) {
     g_dot_cols(P, B, dsub, B.z + (size_t)e0 * nr, sh);
 }
 
-// y = z - G^T alpha, rho_j = y.w; clear the SYMM accumulators (not needed: rows written once)
+// y = z - G^T alpha, rho_j = y.w
+template <int KC>
 __global__ void by_kernel(DevProblem P, BlockDev B, int slot) {
     __shared__ double sh[8 * 32];
     __shared__ double cols[32];
@@ -2830,7 +2845,7 @@ __global__ void by_kernel(DevProblem P, BlockDev B, int slot) {
                 const size_t o = (size_t)e0 * nr + i;
                 zv[u] = B.z[o];
                 wv[u] = B.w[o];
-                ga[u] = gt_alpha_col(P, e, j, nr, B.alpha);
+                ga[u] = gt_alpha_colk<KC>(P, e, j, nr, B.alpha);
                 mv[u] = P.minv[e];
             }
         }
@@ -3254,7 +3269,10 @@ void GpuSolver::Impl::ensure_block(int nr) {
     B.Ap = alloc<double>((size_t)NL * nr); B.Ax = alloc<double>((size_t)NL * nr); B.bL = alloc<double>((size_t)NL * nr);
     B.p32 = alloc<float>((size_t)NL * nr);
     B.uT = alloc<double>((size_t)NT * nr); B.vT = alloc<double>((size_t)NT * nr);
-    B.d = alloc<double>((size_t)P.nP * nr); B.alpha = alloc<double>((size_t)nK * nr); B.e = alloc<double>((size_t)P.nP * nr);
+    // alpha carries KS zero rows past nK for the fixed-width G^T alpha loads
+    B.d = alloc<double>((size_t)P.nP * nr); B.alpha = alloc<double>((size_t)(nK + P.KS) * nr);
+    B.e = alloc<double>((size_t)P.nP * nr);
+    CUDA_CHECK(cudaMemset(B.alpha, 0, sizeof(double) * (size_t)(nK + P.KS) * nr));
     B.part = alloc<double>((size_t)2 * nd * nr);
     B.scal = alloc<double>((size_t)SC_COUNT * nr);
     B.rho_hist = alloc<double>((size_t)(opt.max_iterations + 64) * nr);
@@ -3363,14 +3381,25 @@ void GpuSolver::Impl::launch_block_iteration(int slot) {
     }
     bcoarse_kernel<<<cgrid, 256, 0, stream>>>(P, B, B.d, B.alpha, slot, 1);
     switch (opt.precond) {
-    case PREC_NONE: bw_prec_kernel<PREC_NONE><<<nd, TPB, 0, stream>>>(P, B, slot); break;
-    case PREC_LUMPED: bw_prec_kernel<PREC_LUMPED><<<nd, TPB, 0, stream>>>(P, B, slot); break;
-    default: bw_prec_kernel<PREC_WEIGHT><<<nd, TPB, 0, stream>>>(P, B, slot); break;
+#define BW(PC)                                                                         \
+    switch (P.KS) {                                                                    \
+    case 1: bw_prec_kernel<PC, 1><<<nd, TPB, 0, stream>>>(P, B, slot); break;          \
+    case 6: bw_prec_kernel<PC, 6><<<nd, TPB, 0, stream>>>(P, B, slot); break;          \
+    default: bw_prec_kernel<PC, 0><<<nd, TPB, 0, stream>>>(P, B, slot); break;         \
     }
+    case PREC_NONE: BW(PREC_NONE) break;
+    case PREC_LUMPED: BW(PREC_LUMPED) break;
+    default: BW(PREC_WEIGHT) break;
+    }
+#undef BW
     if (opt.precond != PREC_NONE) {
         bz_kernel<<<nd, TPB, 0, stream>>>(P, B, slot);
         bcoarse_kernel<<<cgrid, 256, 0, stream>>>(P, B, B.d, B.alpha, slot, 1);
-        by_kernel<<<nd, TPB, 0, stream>>>(P, B, slot);
+        switch (P.KS) {
+        case 1: by_kernel<1><<<nd, TPB, 0, stream>>>(P, B, slot); break;
+        case 6: by_kernel<6><<<nd, TPB, 0, stream>>>(P, B, slot); break;
+        default: by_kernel<0><<<nd, TPB, 0, stream>>>(P, B, slot); break;
+        }
     }
     bp_kernel<<<std::max(1, std::min(4096, (P.NL * blk.nr + 255) / 256)), 256, 0, stream>>>(P, B, slot);
     if (mixed) launch_symm(Flow, true, nullptr, B.p32, B.Ap, slot, 1);
