@@ -79,6 +79,8 @@ struct DevProblem {
     const int *ell_w;       // per slice: width
     const unsigned short *ell_col;  // column (T index inside the subdomain)
     const double *ell_val;
+    const int *tbase;       // NT: first T index of the subdomain owning each T index
+    const int *tslot;       // NT: (ELL slice << 5) | row within the slice
     const double *GGtinv;   // nK x nP, row-major: (GG^T)^-1 times the sum over partial blocks
     const double *bL;       // NL replicated b
     double *x, *r, *w, *z, *y, *p, *Ap, *uT, *vT, *d, *alpha;
@@ -959,8 +961,10 @@ __global__ void chunk_end_kernel(DevProblem P, int chunk) {
 // ---------------------------------------------------------------------------------------------
 // K^+ on the device: forward/backward substitution with the Cholesky factor of
 // K_reg (factor order), stored as 32x32 lower tiles (I >= J), block column by
-// block column.  One CTA per subdomain; diagonal blocks are solved by warp 0
-// with shuffles, off-diagonal blocks are applied by all warps.
+// block column; the diagonal tiles hold the inverse of their 32x32 triangular block,
+// so a diagonal step is a 32-term product per lane instead of a chain of 32 dependent
+// divisions.  One CTA per subdomain; diagonal blocks are applied by warp 0 with
+// shuffles, off-diagonal blocks by all warps.
 struct KplusDev {
     int nd;
     const int *n;            // DOFs per subdomain
@@ -992,18 +996,16 @@ __global__ void __launch_bounds__(256) kplus_kernel(KplusDev K, const double *in
     // forward: L y = f
     for (int J = 0; J < T; ++J) {
         if (warp == 0) {
+            // y_J = inv(L_JJ) v_J: lane r forms row r (zero above the diagonal)
             const double *row = dtiles + (size_t)ltile(T, J, J) * TILE * TILE + lane * TILE;
-            double Lr[TILE];
+            const double vr = v[TILE * J + lane];
+            double s0 = 0.0, s1 = 0.0;
 #pragma unroll
-            for (int k = 0; k < TILE; ++k) Lr[k] = row[k];
-            double vr = v[TILE * J + lane];
-#pragma unroll
-            for (int k = 0; k < TILE; ++k) {
-                double xk = __shfl_sync(FULL, vr / Lr[k], k);
-                if (lane == k) vr = xk;
-                else if (lane > k) vr -= Lr[k] * xk;
+            for (int k = 0; k < TILE; k += 2) {
+                s0 += row[k] * __shfl_sync(FULL, vr, k);
+                s1 += row[k + 1] * __shfl_sync(FULL, vr, k + 1);
             }
-            v[TILE * J + lane] = vr;
+            v[TILE * J + lane] = s0 + s1;
         }
         __syncthreads();
         for (int I = J + 1 + warp; I < T; I += nw) {
@@ -1040,17 +1042,15 @@ __global__ void __launch_bounds__(256) kplus_kernel(KplusDev K, const double *in
         if (warp == 0) {
             double vc = v[TILE * J + lane];
             for (int w = 0; w < nw; ++w) vc -= part[w][lane];
+            // x_J = inv(L_JJ)^T v_J: lane c forms column c of inv(L_JJ)
             const double *tile = dtiles + (size_t)ltile(T, J, J) * TILE * TILE;
-            double Lc[TILE];
+            double s0 = 0.0, s1 = 0.0;
 #pragma unroll
-            for (int k = 0; k < TILE; ++k) Lc[k] = tile[k * TILE + lane];
-#pragma unroll
-            for (int k = TILE - 1; k >= 0; --k) {
-                double xk = __shfl_sync(FULL, vc / Lc[k], k);
-                if (lane == k) vc = xk;
-                else if (lane < k) vc -= Lc[k] * xk;
+            for (int k = 0; k < TILE; k += 2) {
+                s0 += tile[k * TILE + lane] * __shfl_sync(FULL, vc, k);
+                s1 += tile[(k + 1) * TILE + lane] * __shfl_sync(FULL, vc, k + 1);
             }
-            v[TILE * J + lane] = vc;
+            v[TILE * J + lane] = s0 + s1;
         }
         __syncthreads();
     }
@@ -1361,6 +1361,7 @@ struct GpuSolver::Impl {
         cudaGraphExec_t graph = nullptr;
         int graph_chunk = 0, graph_prec = -1, graph_precond = -1;
         double *rhs = nullptr, *sol = nullptr, *f = nullptr, *kf = nullptr, *g = nullptr;
+        int flat_grid = 1;
     } blk;
     void ensure_block(int nr);
     void launch_symm(const TileSetHost &T, bool src32, const double *x64, const float *x32, double *out, int slot,
@@ -1471,6 +1472,18 @@ void GpuSolver::Impl::upload_kplus(const Decomposition &dec, const Prep &prep, c
                         else if (gr == gc) v = 1.0;
                         tile[r * TILE + c] = v;
                     }
+                if (I == J) {
+                    // diagonal tile: inverse of its lower-triangular block, column by column
+                    double inv[TILE * TILE] = {};
+                    for (int c = 0; c < TILE; ++c) {
+                        for (int r = c; r < TILE; ++r) {
+                            double sum = (r == c) ? 1.0 : 0.0;
+                            for (int k = c; k < r; ++k) sum -= tile[r * TILE + k] * inv[k * TILE + c];
+                            inv[r * TILE + c] = sum / tile[r * TILE + r];
+                        }
+                    }
+                    std::copy(inv, inv + TILE * TILE, tile);
+                }
             }
     }
     // per local multiplier row: DOF in the concatenated local space, sign, Dirichlet value
@@ -2033,6 +2046,12 @@ void GpuSolver::upload(const Decomposition &dec, const Prep &prep, const SolveOp
             slice0[d + 1]++;
         }
     }
+    std::vector<int> tbase(NT), tslot(NT);
+    for (int d = 0; d < nd; ++d)
+        for (int t = toff[d]; t < toff[d + 1]; ++t) {
+            tbase[t] = toff[d];
+            tslot[t] = ((slice0[d] + ((t - toff[d]) >> 5)) << 5) | ((t - toff[d]) & 31);
+        }
     FETI_CHECK(sizeof(double) * (size_t)(I.max_nt + I.max_ni) <= 200 * 1024,
                "FETI4I: subdomain interface too large for the preconditioner kernel");
 
@@ -2046,6 +2065,7 @@ void GpuSolver::upload(const Decomposition &dec, const Prep &prep, const SolveOp
     P.trow_ptr = I.upload(trow_ptr); P.trow_idx = I.upload(trow_idx);
     P.slice0 = I.upload(slice0); P.ell_ptr = I.upload(ell_ptr); P.ell_w = I.upload(ell_w);
     P.ell_col = I.upload(ell_col); P.ell_val = I.upload(ell_val);
+    P.tbase = I.upload(tbase); P.tslot = I.upload(tslot);
     P.scal = I.alloc<double>(SC_COUNT);
     P.done = I.alloc<int>(DONE_COUNT);
     CUDA_CHECK(cudaMemset(P.done, 0, sizeof(int) * DONE_COUNT));
@@ -2720,82 +2740,6 @@ __global__ void btol_kernel(DevProblem P, BlockDev B) {
     }
 }
 
-// w = r - G^T alpha, |w_j|^2; u_T = B^T W w; lumped v_T = K_TT u_T (columns)
-template <int PRECOND, int KC>
-__global__ void bw_prec_kernel(DevProblem P, BlockDev B, int slot) {
-    __shared__ double sh[8 * 32];
-    __shared__ double cols[32];
-    const int iter = P.st->iter_base + slot;
-    if (skip_iter(P.st, iter)) return;
-    const int nr = B.nr, dsub = blockIdx.x;
-    const int e0 = P.loff[dsub], e1 = P.loff[dsub + 1];
-    double ww = 0.0;
-    const int cnt = (e1 - e0) * nr;
-    // UNR rows in flight per thread: all loads of a group are issued before its stores
-    for (int i0 = threadIdx.x; i0 < cnt; i0 += UNR * blockDim.x) {
-        double rv[UNR], ga[UNR], mv[UNR];
-#pragma unroll
-        for (int u = 0; u < UNR; ++u) {
-            const int i = i0 + u * blockDim.x;
-            if (i < cnt) {
-                const int e = e0 + (i >> B.lg), j = i & (nr - 1);
-                rv[u] = B.r[(size_t)e * nr + j];
-                ga[u] = gt_alpha_colk<KC>(P, e, j, nr, B.alpha);
-                mv[u] = P.minv[e];
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < UNR; ++u) {
-            const int i = i0 + u * blockDim.x;
-            if (i < cnt) {
-                const size_t o = (size_t)e0 * nr + i;
-                const double wv = rv[u] - ga[u];
-                B.w[o] = wv;
-                if (PRECOND == PREC_NONE) B.y[o] = wv;
-                ww += wv * wv * mv[u];
-            }
-        }
-    }
-    block_sum_cols(ww, nr, sh, cols);
-    grid_total_cols(cols, B.part, nr, B.done + DONE_W, B.scal + SC_WN2 * nr);
-    if (PRECOND == PREC_NONE) {
-        grid_total_cols(cols, B.part + (size_t)P.nd * nr, nr, B.done + DONE_RHO, B.scal + SC_RHO * nr);
-        return;
-    }
-    __syncthreads();
-    const int t0 = P.toff[dsub], nt = P.toff[dsub + 1] - t0;
-    for (int i = threadIdx.x; i < nt * nr; i += blockDim.x) {
-        const int t = (i >> B.lg), j = (i & (nr - 1));
-        double s = 0.0;
-        for (int q = P.trow_ptr[t0 + t]; q < P.trow_ptr[t0 + t + 1]; ++q) {
-            const int e = P.trow_idx[q];
-            s += P.ws[e] * B.w[(size_t)e * nr + j];
-        }
-        B.uT[(size_t)(t0 + t) * nr + j] = s;
-        if (PRECOND == PREC_WEIGHT) B.vT[(size_t)(t0 + t) * nr + j] = s;
-    }
-    if (PRECOND != PREC_LUMPED) return;
-    __syncthreads();
-    const int sl0 = P.slice0[dsub];
-    for (int i = threadIdx.x; i < nt * nr; i += blockDim.x) {
-        const int t = (i >> B.lg), j = (i & (nr - 1));
-        const int sl = sl0 + (t >> 5), ln = t & 31;
-        const int base = P.ell_ptr[sl], wd = P.ell_w[sl];
-        double s0 = 0.0, s1 = 0.0;
-        int q = 0;
-        for (; q + 1 < wd; q += 2) {
-            const int o = base + q * 32 + ln;
-            s0 += P.ell_val[o] * B.uT[(size_t)(t0 + P.ell_col[o]) * nr + j];
-            s1 += P.ell_val[o + 32] * B.uT[(size_t)(t0 + P.ell_col[o + 32]) * nr + j];
-        }
-        if (q < wd) {
-            const int o = base + q * 32 + ln;
-            s0 += P.ell_val[o] * B.uT[(size_t)(t0 + P.ell_col[o]) * nr + j];
-        }
-        B.vT[(size_t)(t0 + t) * nr + j] = s0 + s1;
-    }
-}
-
 __global__ void bz_kernel(DevProblem P, BlockDev B, int slot) {
     __shared__ double sh[8 * 32];
     const int iter = P.st->iter_base + slot;
@@ -2825,42 +2769,130 @@ __global__ void bz_kernel(DevProblem P, BlockDev B, int slot) {
     g_dot_cols(P, B, dsub, B.z + (size_t)e0 * nr, sh);
 }
 
-// y = z - G^T alpha, rho_j = y.w
-template <int KC>
-__global__ void by_kernel(DevProblem P, BlockDev B, int slot) {
+// ---- flat block kernels: a persistent grid over all rows (no per-subdomain reduction needed)
+// thread column: the grid stride is a multiple of 32 >= nr, so every thread stays on column
+// threadIdx.x & (nr - 1) and block_sum_cols combines the right partial sums
+
+// w = r - G^T alpha, |w_j|^2 (and y = w, rho_j = |w_j|^2 without a preconditioner)
+template <int PRECOND, int KC>
+__global__ void __launch_bounds__(256) bw_flat_kernel(DevProblem P, BlockDev B, int slot) {
     __shared__ double sh[8 * 32];
     __shared__ double cols[32];
     const int iter = P.st->iter_base + slot;
     if (skip_iter(P.st, iter)) return;
-    const int nr = B.nr, dsub = blockIdx.x;
-    double s = 0.0;
-    const int e0 = P.loff[dsub], cnt = (P.loff[dsub + 1] - e0) * nr;
-    for (int i0 = threadIdx.x; i0 < cnt; i0 += UNR * blockDim.x) {
-        double zv[UNR], ga[UNR], wv[UNR], mv[UNR];
+    const int nr = B.nr;
+    const long long cnt = (long long)P.NL * nr, stride = (long long)gridDim.x * blockDim.x;
+    double ww = 0.0;
+    for (long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; i0 < cnt; i0 += UNR * stride) {
+        double rv[UNR], ga[UNR], mv[UNR];
 #pragma unroll
         for (int u = 0; u < UNR; ++u) {
-            const int i = i0 + u * blockDim.x;
+            const long long i = i0 + u * stride;
             if (i < cnt) {
-                const int e = e0 + (i >> B.lg), j = i & (nr - 1);
-                const size_t o = (size_t)e0 * nr + i;
-                zv[u] = B.z[o];
-                wv[u] = B.w[o];
+                const int e = (int)(i >> B.lg), j = (int)(i & (nr - 1));
+                rv[u] = B.r[i];
                 ga[u] = gt_alpha_colk<KC>(P, e, j, nr, B.alpha);
                 mv[u] = P.minv[e];
             }
         }
 #pragma unroll
         for (int u = 0; u < UNR; ++u) {
-            const int i = i0 + u * blockDim.x;
+            const long long i = i0 + u * stride;
+            if (i < cnt) {
+                const double wv = rv[u] - ga[u];
+                B.w[i] = wv;
+                if (PRECOND == PREC_NONE) B.y[i] = wv;
+                ww += wv * wv * mv[u];
+            }
+        }
+    }
+    block_sum_cols(ww, nr, sh, cols);
+    grid_total_cols(cols, B.part, nr, B.done + DONE_W, B.scal + SC_WN2 * nr);
+    if (PRECOND == PREC_NONE)
+        grid_total_cols(cols, B.part + (size_t)gridDim.x * nr, nr, B.done + DONE_RHO, B.scal + SC_RHO * nr);
+}
+
+// u_T = B^T W w over all touched DOFs (v_T = u_T for the weight-function preconditioner)
+template <int PRECOND>
+__global__ void __launch_bounds__(256) bu_flat_kernel(DevProblem P, BlockDev B, int slot) {
+    const int iter = P.st->iter_base + slot;
+    if (skip_iter(P.st, iter)) return;
+    const int nr = B.nr;
+    const long long cnt = (long long)P.NT * nr, stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += stride) {
+        const int t = (int)(i >> B.lg), j = (int)(i & (nr - 1));
+        const int q0 = P.trow_ptr[t], q1 = P.trow_ptr[t + 1];
+        double s = 0.0;
+        for (int q = q0; q < q1; ++q) {
+            const int e = P.trow_idx[q];
+            s += P.ws[e] * B.w[(size_t)e * nr + j];
+        }
+        B.uT[i] = s;
+        if (PRECOND == PREC_WEIGHT) B.vT[i] = s;
+    }
+}
+
+// lumped v_T = K_TT u_T (sliced ELL of every subdomain)
+__global__ void __launch_bounds__(256) bell_flat_kernel(DevProblem P, BlockDev B, int slot) {
+    const int iter = P.st->iter_base + slot;
+    if (skip_iter(P.st, iter)) return;
+    const int nr = B.nr;
+    const long long cnt = (long long)P.NT * nr, stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += stride) {
+        const int t = (int)(i >> B.lg), j = (int)(i & (nr - 1));
+        const int t0 = P.tbase[t], ts = P.tslot[t];
+        const int sl = ts >> 5, ln = ts & 31;
+        const int base = P.ell_ptr[sl], wd = P.ell_w[sl];
+        double s0 = 0.0, s1 = 0.0;
+        int q = 0;
+        for (; q + 1 < wd; q += 2) {
+            const int o = base + q * 32 + ln;
+            s0 += P.ell_val[o] * B.uT[(size_t)(t0 + P.ell_col[o]) * nr + j];
+            s1 += P.ell_val[o + 32] * B.uT[(size_t)(t0 + P.ell_col[o + 32]) * nr + j];
+        }
+        if (q < wd) {
+            const int o = base + q * 32 + ln;
+            s0 += P.ell_val[o] * B.uT[(size_t)(t0 + P.ell_col[o]) * nr + j];
+        }
+        B.vT[i] = s0 + s1;
+    }
+}
+
+// y = z - G^T alpha, rho_j = y.w
+template <int KC>
+__global__ void __launch_bounds__(256) by_flat_kernel(DevProblem P, BlockDev B, int slot) {
+    __shared__ double sh[8 * 32];
+    __shared__ double cols[32];
+    const int iter = P.st->iter_base + slot;
+    if (skip_iter(P.st, iter)) return;
+    const int nr = B.nr;
+    const long long cnt = (long long)P.NL * nr, stride = (long long)gridDim.x * blockDim.x;
+    double s = 0.0;
+    for (long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; i0 < cnt; i0 += UNR * stride) {
+        double zv[UNR], ga[UNR], wv[UNR], mv[UNR];
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            const long long i = i0 + u * stride;
+            if (i < cnt) {
+                const int e = (int)(i >> B.lg), j = (int)(i & (nr - 1));
+                zv[u] = B.z[i];
+                wv[u] = B.w[i];
+                ga[u] = gt_alpha_colk<KC>(P, e, j, nr, B.alpha);
+                mv[u] = P.minv[e];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            const long long i = i0 + u * stride;
             if (i < cnt) {
                 const double yv = zv[u] - ga[u];
-                B.y[(size_t)e0 * nr + i] = yv;
+                B.y[i] = yv;
                 s += yv * wv[u] * mv[u];
             }
         }
     }
     block_sum_cols(s, nr, sh, cols);
-    grid_total_cols(cols, B.part + (size_t)P.nd * nr, nr, B.done + DONE_RHO, B.scal + SC_RHO * nr);
+    grid_total_cols(cols, B.part + (size_t)gridDim.x * nr, nr, B.done + DONE_RHO, B.scal + SC_RHO * nr);
 }
 
 // p = y + beta_j p (and its FP32 copy)
@@ -3273,7 +3305,9 @@ void GpuSolver::Impl::ensure_block(int nr) {
     B.d = alloc<double>((size_t)P.nP * nr); B.alpha = alloc<double>((size_t)(nK + P.KS) * nr);
     B.e = alloc<double>((size_t)P.nP * nr);
     CUDA_CHECK(cudaMemset(B.alpha, 0, sizeof(double) * (size_t)(nK + P.KS) * nr));
-    B.part = alloc<double>((size_t)2 * nd * nr);
+    // persistent grid of the flat block kernels: rows of all subdomains, UNR per thread in flight
+    blk.flat_grid = std::max(1, std::min(nsm * 8, (int)(((long long)NL * nr + 256LL * UNR - 1) / (256LL * UNR))));
+    B.part = alloc<double>((size_t)2 * std::max(nd, blk.flat_grid) * nr);
     B.scal = alloc<double>((size_t)SC_COUNT * nr);
     B.rho_hist = alloc<double>((size_t)(opt.max_iterations + 64) * nr);
     B.tol = alloc<double>(nr); B.rmax = alloc<double>(nr); B.last_norm = alloc<double>(nr);
@@ -3380,25 +3414,33 @@ void GpuSolver::Impl::launch_block_iteration(int slot) {
         br0_kernel<<<nd, TPB, 0, stream>>>(P, B, 1, slot);
     }
     bcoarse_kernel<<<cgrid, 256, 0, stream>>>(P, B, B.d, B.alpha, slot, 1);
-    switch (opt.precond) {
-#define BW(PC)                                                                         \
-    switch (P.KS) {                                                                    \
-    case 1: bw_prec_kernel<PC, 1><<<nd, TPB, 0, stream>>>(P, B, slot); break;          \
-    case 6: bw_prec_kernel<PC, 6><<<nd, TPB, 0, stream>>>(P, B, slot); break;          \
-    default: bw_prec_kernel<PC, 0><<<nd, TPB, 0, stream>>>(P, B, slot); break;         \
+    const int fgrid = blk.flat_grid;
+#define BW(PC)                                                                              \
+    switch (P.KS) {                                                                         \
+    case 1: bw_flat_kernel<PC, 1><<<fgrid, 256, 0, stream>>>(P, B, slot); break;            \
+    case 6: bw_flat_kernel<PC, 6><<<fgrid, 256, 0, stream>>>(P, B, slot); break;            \
+    default: bw_flat_kernel<PC, 0><<<fgrid, 256, 0, stream>>>(P, B, slot); break;           \
     }
+    switch (opt.precond) {
     case PREC_NONE: BW(PREC_NONE) break;
-    case PREC_LUMPED: BW(PREC_LUMPED) break;
-    default: BW(PREC_WEIGHT) break;
+    case PREC_LUMPED:
+        BW(PREC_LUMPED)
+        bu_flat_kernel<PREC_LUMPED><<<fgrid, 256, 0, stream>>>(P, B, slot);
+        bell_flat_kernel<<<fgrid, 256, 0, stream>>>(P, B, slot);
+        break;
+    default:
+        BW(PREC_WEIGHT)
+        bu_flat_kernel<PREC_WEIGHT><<<fgrid, 256, 0, stream>>>(P, B, slot);
+        break;
     }
 #undef BW
     if (opt.precond != PREC_NONE) {
         bz_kernel<<<nd, TPB, 0, stream>>>(P, B, slot);
         bcoarse_kernel<<<cgrid, 256, 0, stream>>>(P, B, B.d, B.alpha, slot, 1);
         switch (P.KS) {
-        case 1: by_kernel<1><<<nd, TPB, 0, stream>>>(P, B, slot); break;
-        case 6: by_kernel<6><<<nd, TPB, 0, stream>>>(P, B, slot); break;
-        default: by_kernel<0><<<nd, TPB, 0, stream>>>(P, B, slot); break;
+        case 1: by_flat_kernel<1><<<fgrid, 256, 0, stream>>>(P, B, slot); break;
+        case 6: by_flat_kernel<6><<<fgrid, 256, 0, stream>>>(P, B, slot); break;
+        default: by_flat_kernel<0><<<fgrid, 256, 0, stream>>>(P, B, slot); break;
         }
     }
     bp_kernel<<<std::max(1, std::min(4096, (P.NL * blk.nr + 255) / 256)), 256, 0, stream>>>(P, B, slot);
