@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--loads", default="scaled", choices=["scaled", "traction"],
                     help="batched leg load cases: scaled copies of the config load, or seeded N(0,1e6) "
                          "nodal tractions on the x=1 face")
+    ap.add_argument("--symm-tensor", type=int, default=0, choices=[0, 1],
+                    help="batched leg: FP32 SYMM on the tensor cores (tcgen05, 3xTF32) instead of CUDA cores")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -211,7 +213,8 @@ def run_ours(args):
                                   ext={F.EXT_SCHUR_PRECISION: SCHUR[args.schur],
                                        F.EXT_TILE_KERNEL: max(0, args.tile_kernel),
                                        F.EXT_AUTOTUNE: 1 if args.tile_kernel < 0 else 0,
-                                       F.EXT_RELIABLE_DELTA: args.delta},
+                                       F.EXT_RELIABLE_DELTA: args.delta,
+                                       F.EXT_SYMM_TENSOR: args.symm_tensor},
                                   clusters=P.sub_cluster() if args.method == 1 else None)
     setup_s = time.time() - t0
     st0 = inst.stats()
@@ -268,7 +271,8 @@ def run_ours(args):
         batched = {"nrhs": args.nrhs, "ms_per_batch": bmed, "ms_per_solve": bmed / args.nrhs,
                    "pcg_iterations": int(stb["iterations"]), "replacements": int(stb["replacements"]),
                    "fp64_ms_per_batch": b64, "fp64_single_ms_per_solve": fp64_ms,
-                   "speedup_vs_fp64_single": fp64_ms / (bmed / args.nrhs), "e2e_ms_per_batch": e2e_b}
+                   "speedup_vs_fp64_single": fp64_ms / (bmed / args.nrhs), "e2e_ms_per_batch": e2e_b,
+                   "symm": "tcgen05 3xTF32" if args.symm_tensor else "CUDA cores FP32"}
     NL = int(sum(inst.subdomain_info(d)["rows"] for d in range(int(st["subdomains"]))))
     nK = int(st["kernel_size"])
     # roofline of the F apply kernel (events on the library stream)

@@ -1362,6 +1362,8 @@ struct GpuSolver::Impl {
         int graph_chunk = 0, graph_prec = -1, graph_precond = -1;
         double *rhs = nullptr, *sol = nullptr, *f = nullptr, *kf = nullptr, *g = nullptr;
         int flat_grid = 1;
+        int2 *units4 = nullptr;
+        int nunits4 = 0;
     } blk;
     void ensure_block(int nr);
     void launch_symm(const TileSetHost &T, bool src32, const double *x64, const float *x32, double *out, int slot,
@@ -3100,6 +3102,276 @@ tile_symm_kernel(TileSetDev ts, DevProblem P, BlockDev B, const double *x64, con
     }
 }
 
+// ---- Tile SYMM on the 5th-generation tensor cores (FP32 tiles, 3xTF32 split)
+// A unit is four consecutive 32-row tile rows of one subdomain (M = 128 rows of S).  For
+// every 32-column block J the CTA stages A = S[128 rows, 32 columns] (upper tiles as stored,
+// lower tiles transposed) and B = X_J^T (NR x 32) in shared memory, in the 128-byte swizzled
+// K-major layout of the UMMA descriptors, each split into TF32 parts x = hi + lo.  One thread
+// issues hi*hi + hi*lo + lo*hi as tcgen05.mma kind::tf32 (M=128, N=NR, K=8, four K steps)
+// into an FP32 accumulator in tensor memory; the dropped lo*lo term and the TF32 rounding of
+// lo leave about 2^-21 relative error per product, the order of FP32 accumulation.
+// Two stages: staging block J+1 overlaps the MMAs of block J; tcgen05.commit arrives on the
+// stage's mbarrier when its MMAs are done.  Every wait is bounded: on time-out the kernel
+// records an error, waits (bounded) for its MMAs, frees its tensor memory and returns.
+namespace tc {
+constexpr int M = 128;
+constexpr unsigned A_BYTES = M * 128;   // 128 rows x 32 FP32
+constexpr int THREADS = 256;
+// K-major operand, 128-byte swizzle: 8-row atoms of 1024 bytes (SBO), version 1
+__device__ __forceinline__ uint64_t sdesc(unsigned addr) {
+    return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)1 << 16) | ((uint64_t)64 << 32) | ((uint64_t)1 << 46) |
+           ((uint64_t)2 << 61);
+}
+// kind::tf32: D FP32, A and B TF32, both K-major, N = NR, M = 128
+template <int N>
+__host__ __device__ constexpr uint32_t idesc() {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+// byte offset of FP32 element (row, k) inside a swizzled K-major operand (32 k per row)
+__device__ __forceinline__ unsigned swz(int row, int chunk) {
+    return (unsigned)((row >> 3) * 1024 + (row & 7) * 128 + ((chunk ^ (row & 7)) << 4));
+}
+__device__ __forceinline__ float tf32_hi(float x) {
+    unsigned r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+__device__ __forceinline__ void split_store(unsigned char *hi, unsigned char *lo, unsigned off, float4 v) {
+    float4 h, l;
+    h.x = tf32_hi(v.x); l.x = v.x - h.x;
+    h.y = tf32_hi(v.y); l.y = v.y - h.y;
+    h.z = tf32_hi(v.z); l.z = v.z - h.z;
+    h.w = tf32_hi(v.w); l.w = v.w - h.w;
+    *reinterpret_cast<float4 *>(hi + off) = h;
+    *reinterpret_cast<float4 *>(lo + off) = l;
+}
+__device__ __forceinline__ void mma(unsigned tmem, uint64_t a, uint64_t b, uint32_t id, unsigned acc) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(tmem),
+        "l"(a), "l"(b), "r"(id), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+__device__ __forceinline__ void commit(unsigned long long *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// 16 columns of 32 lanes: lane i of warp w (w % 4 = q) gets TMEM lane 32q + i
+__device__ __forceinline__ void ld16(unsigned taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void ld4(unsigned taddr, uint32_t (&r)[16]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void ld8(unsigned taddr, uint32_t (&r)[16]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+}  // namespace tc
+
+template <int NR>
+__global__ void __launch_bounds__(tc::THREADS, 1)
+tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, double *out, const int2 *units,
+                    int nunits, int slot, int mode) {
+    static_assert(NR == 8 || NR == 16 || NR == 32, "tensor-core SYMM: 8, 16 or 32 right-hand sides");
+    constexpr unsigned B_BYTES = NR * 128;
+    constexpr unsigned STAGE = 2 * tc::A_BYTES + 2 * B_BYTES;
+    constexpr int HALF = NR / 2;                 // columns read back by each warp half
+    extern __shared__ unsigned char tc_smem[];
+    __shared__ unsigned long long bar[2];
+    __shared__ unsigned s_tmem;
+    __shared__ int s_unit, s_last, s_err;
+    __shared__ double s_dot[tc::THREADS / 32][NR];
+    if (mode != 0) {
+        const int iter = P.st->iter_base + slot;
+        if (skip_iter(P.st, iter)) return;
+    }
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const unsigned base = smem_u32(tc_smem);
+    unsigned char *buf = tc_smem + ((1024u - (base & 1023u)) & 1023u);   // 1024-byte aligned stages
+    const unsigned ncols = 32;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(ncols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_err = 0;
+    }
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const unsigned tmem = s_tmem;
+    constexpr uint32_t ID = tc::idesc<NR>();
+    unsigned phase[2] = {0u, 0u};
+    bool pending[2] = {false, false};
+    unsigned seq = 0;
+    bool ok = true;
+    for (;;) {
+        if (tid == 0) s_unit = atomicAdd(&B.queue[0], 1);
+        const bool all_ok = __syncthreads_and(ok);   // a timed-out wait stops every thread together
+        const int u = s_unit;
+        if (u >= nunits || !all_ok) break;
+        ok = true;
+        const int m = units[u].x, I0 = 4 * units[u].y;
+        const int n = ts.mat_n[m], voff = ts.mat_voff[m], tn = ts.mat_tn[m];
+        const long long t0 = ts.mat_tile0[m];
+        const float *tiles = reinterpret_cast<const float *>(ts.tiles);
+        for (int J = 0; J < tn; ++J) {
+            const int st = seq & 1;
+            if (pending[st]) {
+                if (!mbar_wait(&bar[st], phase[st])) ok = false;
+                phase[st] ^= 1u;
+                pending[st] = false;
+            }
+            unsigned char *ahi = buf + st * STAGE, *alo = ahi + tc::A_BYTES, *bhi = alo + tc::A_BYTES,
+                          *blo = bhi + B_BYTES;
+            // A: 128 rows x 8 chunks of 4 FP32; a warp handles 32 chunks of one 32-row tile row
+#pragma unroll
+            for (int it = 0; it < (tc::M * 8) / tc::THREADS; ++it) {
+                const int q = tid + it * tc::THREADS;
+                const int qq = q >> 8, I = I0 + qq;       // warp-uniform
+                int rr, c;
+                float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (I < tn && J >= I) {
+                    rr = (q >> 3) & 31;
+                    c = q & 7;
+                    const long long tid_ = t0 + (long long)I * tn - (long long)I * (I - 1) / 2 + (J - I);
+                    v = *reinterpret_cast<const float4 *>(tiles + (size_t)tid_ * (TILE * TILE) + rr * TILE + 4 * c);
+                } else {
+                    rr = q & 31;
+                    c = (q >> 5) & 7;
+                    if (I < tn) {
+                        const long long tid_ = t0 + (long long)J * tn - (long long)J * (J - 1) / 2 + (I - J);
+                        const float *tp = tiles + (size_t)tid_ * (TILE * TILE) + rr;
+                        v.x = tp[(4 * c + 0) * TILE];
+                        v.y = tp[(4 * c + 1) * TILE];
+                        v.z = tp[(4 * c + 2) * TILE];
+                        v.w = tp[(4 * c + 3) * TILE];
+                    }
+                }
+                tc::split_store(ahi, alo, tc::swz(qq * 32 + rr, c), v);
+            }
+            // B: NR rows (right-hand sides) x 8 chunks; lanes along the right-hand sides
+            for (int q = tid; q < NR * 8; q += tc::THREADS) {
+                const int nn = q % NR, c = q / NR;
+                float4 v;
+                const int r0 = TILE * J + 4 * c;
+                v.x = (r0 + 0 < n) ? x32[(size_t)(voff + r0 + 0) * NR + nn] : 0.f;
+                v.y = (r0 + 1 < n) ? x32[(size_t)(voff + r0 + 1) * NR + nn] : 0.f;
+                v.z = (r0 + 2 < n) ? x32[(size_t)(voff + r0 + 2) * NR + nn] : 0.f;
+                v.w = (r0 + 3 < n) ? x32[(size_t)(voff + r0 + 3) * NR + nn] : 0.f;
+                tc::split_store(bhi, blo, tc::swz(nn, c), v);
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncthreads();
+            if (tid == 0) {
+                tc::fence_after();
+                const unsigned a_hi = smem_u32(ahi), a_lo = smem_u32(alo), b_hi = smem_u32(bhi), b_lo = smem_u32(blo);
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk) {
+                    const unsigned off = 32u * kk;
+                    tc::mma(tmem, tc::sdesc(a_hi + off), tc::sdesc(b_hi + off), ID, (J > 0 || kk > 0) ? 1u : 0u);
+                    tc::mma(tmem, tc::sdesc(a_hi + off), tc::sdesc(b_lo + off), ID, 1u);
+                    tc::mma(tmem, tc::sdesc(a_lo + off), tc::sdesc(b_hi + off), ID, 1u);
+                }
+                tc::commit(&bar[st]);
+            }
+            pending[st] = true;
+            ++seq;
+        }
+        // the last commit tracks every MMA issued before it: the accumulator is complete
+        {
+            const int lst = (seq - 1) & 1;
+            if (!mbar_wait(&bar[lst], phase[lst])) ok = false;
+            phase[lst] ^= 1u;
+            pending[lst] = false;
+        }
+        tc::fence_after();
+        // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31, columns (w / 4) * HALF .. +HALF-1
+        uint32_t r[16];
+        const unsigned taddr = tmem + ((unsigned)(32 * (warp & 3)) << 16) + (unsigned)((warp >> 2) * HALF);
+        if (HALF == 16) tc::ld16(taddr, r);
+        else if (HALF == 8) tc::ld8(taddr, r);
+        else tc::ld4(taddr, r);
+        const int row = TILE * I0 + 32 * (warp & 3) + lane;
+        const int c0 = (warp >> 2) * HALF;
+        double dl[HALF];
+#pragma unroll
+        for (int c = 0; c < HALF; ++c) {
+            dl[c] = 0.0;
+            if (row < n && ok) {
+                const size_t o = (size_t)(voff + row) * NR + c0 + c;
+                const double y = (double)__uint_as_float(r[c]);
+                out[o] = y;
+                dl[c] = (double)x32[o] * y;
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < HALF; ++c) {
+            double v = dl[c];
+#pragma unroll
+            for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+            if (lane == 0) s_dot[warp][c] = v;
+        }
+        tc::fence_before();
+        __syncthreads();
+        if (tid < NR) {
+            const int h = tid / HALF, c = tid % HALF;
+            double t = 0.0;
+            for (int w = 0; w < 4; ++w) t += s_dot[4 * h + w][c];
+            B.unit_dot[(size_t)u * NR + tid] = t;
+        }
+    }
+    // drain: both stages idle before the tensor memory is released
+    for (int stg = 0; stg < 2; ++stg)
+        if (pending[stg]) {
+            if (!mbar_wait(&bar[stg], phase[stg])) ok = false;
+            pending[stg] = false;
+        }
+    if (!ok && lane == 0) s_err = 1;
+    tc::fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+    if (tid == 0 && s_err) atomicExch(&P.st->error, 1);
+    if (tid == 0) {
+        __threadfence();
+        s_last = (atomicAdd(&B.queue[1], 1) == (int)gridDim.x - 1);
+    }
+    __syncthreads();
+    if (s_last) {
+        if (mode == 1) {
+            __threadfence();
+            if (tid < NR) {
+                double t = 0.0;
+                for (int q = 0; q < nunits; ++q) t += __ldcg(&B.unit_dot[(size_t)q * NR + tid]);
+                B.scal[SC_PAP * NR + tid] = t;
+            }
+        }
+        if (tid == 0) {
+            B.queue[0] = 0;
+            B.queue[1] = 0;
+            __threadfence();
+        }
+    }
+}
+
 // ---- Hybrid Total FETI cluster correction for nr columns ([row][rhs] layout)
 // z_i = V_i^T x_i: one warp per column of V_i, lane = (row group, rhs)
 __global__ void bhyb_vt_kernel(DevProblem P, HybDev H, BlockDev B, const double *x, double *z, int slot, int cond) {
@@ -3327,7 +3599,13 @@ void GpuSolver::Impl::ensure_block(int nr) {
         for (int I = 0; I < tn[m]; ++I) units.push_back(make_int2(m, I));
     blk.units = upload(units);
     blk.nunits = (int)units.size();
-    B.unit_dot = alloc<double>((size_t)units.size() * nr);
+    // tensor-core SYMM units: four tile rows each (M = 128)
+    std::vector<int2> units4;
+    for (int m : order)
+        for (int I4 = 0; 4 * I4 < tn[m]; ++I4) units4.push_back(make_int2(m, I4));
+    blk.units4 = upload(units4);
+    blk.nunits4 = (int)units4.size();
+    B.unit_dot = alloc<double>(std::max(units.size(), units4.size()) * nr);
     blk.rhs = alloc<double>((size_t)std::max(1, n_caller) * nr);
     blk.sol = alloc<double>((size_t)std::max(1, n_caller) * nr);
     blk.f = alloc<double>((size_t)ntot * nr);
@@ -3379,9 +3657,36 @@ static void symm_launch(int nsm, int ncta, size_t sm, cudaStream_t st, TileSetDe
     tile_symm_kernel<PR, NR, SRC><<<grid, 256, sm, st>>>(td, P, B, x64, x32, out, units, nunits, slot, mode);
 }
 
+template <int NR>
+static void symm_tc_launch(int nsm, int nunits, cudaStream_t st, TileSetDev td, DevProblem P, BlockDev B,
+                           const float *x32, double *out, const int2 *units, int slot, int mode) {
+    constexpr size_t sm = 2 * (2 * 128 * 128 + 2 * NR * 128) + 1024;
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        cudaFuncSetAttribute(tile_symm_tc_kernel<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        int b = 1;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, tile_symm_tc_kernel<NR>, tc::THREADS, sm) != cudaSuccess ||
+            b < 1)
+            b = 1;
+        per_sm = b;
+    }
+    const int grid = std::max(1, std::min(nunits, nsm * per_sm));
+    tile_symm_tc_kernel<NR><<<grid, tc::THREADS, sm, st>>>(td, P, B, x32, out, units, nunits, slot, mode);
+}
+
 void GpuSolver::Impl::launch_symm(const TileSetHost &T, bool src32, const double *x64, const float *x32, double *out,
                                   int slot, int mode) {
     const int nr = blk.nr;
+    if (opt.symm_tensor && T.prec == SCHUR_FP32 && src32 && nr >= 8) {
+        TileSetDev td = T.dev();
+        switch (nr) {
+        case 8: symm_tc_launch<8>(nsm, blk.nunits4, stream, td, P, blk.B, x32, out, blk.units4, slot, mode); break;
+        case 16: symm_tc_launch<16>(nsm, blk.nunits4, stream, td, P, blk.B, x32, out, blk.units4, slot, mode); break;
+        default: symm_tc_launch<32>(nsm, blk.nunits4, stream, td, P, blk.B, x32, out, blk.units4, slot, mode); break;
+        }
+        CUDA_CHECK(cudaGetLastError());
+        return;
+    }
     const size_t TB = (size_t)TILE * TILE * (T.prec == SCHUR_FP64 ? 8 : 4);
     const size_t sm = 8 * TB;
     const int ncta = (blk.nunits + 7) / 8;
