@@ -3233,6 +3233,42 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
         const int n = ts.mat_n[m], voff = ts.mat_voff[m], tn = ts.mat_tn[m];
         const long long t0 = ts.mat_tile0[m];
         const float *tiles = reinterpret_cast<const float *>(ts.tiles);
+        // block J of the unit into registers: four 16-byte A chunks and one B chunk per thread
+        constexpr int AIT = (tc::M * 8) / tc::THREADS;
+        float4 ra[AIT], rb = make_float4(0.f, 0.f, 0.f, 0.f);
+        auto load_block = [&](int J) {
+#pragma unroll
+            for (int it = 0; it < AIT; ++it) {
+                const int q = tid + it * tc::THREADS;
+                const int qq = q >> 8, I = I0 + qq;       // warp-uniform
+                ra[it] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (I < tn && J >= I) {
+                    const int rr = (q >> 3) & 31, c = q & 7;
+                    const long long tid_ = t0 + (long long)I * tn - (long long)I * (I - 1) / 2 + (J - I);
+                    const uint4 u4 =
+                        ld_stream(reinterpret_cast<const uint4 *>(tiles + (size_t)tid_ * (TILE * TILE) + rr * TILE + 4 * c));
+                    ra[it] = make_float4(__uint_as_float(u4.x), __uint_as_float(u4.y), __uint_as_float(u4.z),
+                                         __uint_as_float(u4.w));
+                } else if (I < tn) {
+                    const int rr = q & 31, c = (q >> 5) & 7;
+                    const long long tid_ = t0 + (long long)J * tn - (long long)J * (J - 1) / 2 + (I - J);
+                    const float *tp = tiles + (size_t)tid_ * (TILE * TILE) + rr;
+                    ra[it].x = tp[(4 * c + 0) * TILE];
+                    ra[it].y = tp[(4 * c + 1) * TILE];
+                    ra[it].z = tp[(4 * c + 2) * TILE];
+                    ra[it].w = tp[(4 * c + 3) * TILE];
+                }
+            }
+            if (tid < NR * 8) {
+                const int nn = tid % NR, c = tid / NR;
+                const int r0 = TILE * J + 4 * c;
+                rb.x = (r0 + 0 < n) ? x32[(size_t)(voff + r0 + 0) * NR + nn] : 0.f;
+                rb.y = (r0 + 1 < n) ? x32[(size_t)(voff + r0 + 1) * NR + nn] : 0.f;
+                rb.z = (r0 + 2 < n) ? x32[(size_t)(voff + r0 + 2) * NR + nn] : 0.f;
+                rb.w = (r0 + 3 < n) ? x32[(size_t)(voff + r0 + 3) * NR + nn] : 0.f;
+            }
+        };
+        load_block(0);
         for (int J = 0; J < tn; ++J) {
             const int st = seq & 1;
             if (pending[st]) {
@@ -3242,43 +3278,15 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
             }
             unsigned char *ahi = buf + st * STAGE, *alo = ahi + tc::A_BYTES, *bhi = alo + tc::A_BYTES,
                           *blo = bhi + B_BYTES;
-            // A: 128 rows x 8 chunks of 4 FP32; a warp handles 32 chunks of one 32-row tile row
 #pragma unroll
-            for (int it = 0; it < (tc::M * 8) / tc::THREADS; ++it) {
+            for (int it = 0; it < AIT; ++it) {
                 const int q = tid + it * tc::THREADS;
-                const int qq = q >> 8, I = I0 + qq;       // warp-uniform
-                int rr, c;
-                float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (I < tn && J >= I) {
-                    rr = (q >> 3) & 31;
-                    c = q & 7;
-                    const long long tid_ = t0 + (long long)I * tn - (long long)I * (I - 1) / 2 + (J - I);
-                    v = *reinterpret_cast<const float4 *>(tiles + (size_t)tid_ * (TILE * TILE) + rr * TILE + 4 * c);
-                } else {
-                    rr = q & 31;
-                    c = (q >> 5) & 7;
-                    if (I < tn) {
-                        const long long tid_ = t0 + (long long)J * tn - (long long)J * (J - 1) / 2 + (I - J);
-                        const float *tp = tiles + (size_t)tid_ * (TILE * TILE) + rr;
-                        v.x = tp[(4 * c + 0) * TILE];
-                        v.y = tp[(4 * c + 1) * TILE];
-                        v.z = tp[(4 * c + 2) * TILE];
-                        v.w = tp[(4 * c + 3) * TILE];
-                    }
-                }
-                tc::split_store(ahi, alo, tc::swz(qq * 32 + rr, c), v);
+                const int qq = q >> 8, I = I0 + qq;
+                const bool up = (I < tn && J >= I);
+                const int rr = up ? ((q >> 3) & 31) : (q & 31), c = up ? (q & 7) : ((q >> 5) & 7);
+                tc::split_store(ahi, alo, tc::swz(qq * 32 + rr, c), ra[it]);
             }
-            // B: NR rows (right-hand sides) x 8 chunks; lanes along the right-hand sides
-            for (int q = tid; q < NR * 8; q += tc::THREADS) {
-                const int nn = q % NR, c = q / NR;
-                float4 v;
-                const int r0 = TILE * J + 4 * c;
-                v.x = (r0 + 0 < n) ? x32[(size_t)(voff + r0 + 0) * NR + nn] : 0.f;
-                v.y = (r0 + 1 < n) ? x32[(size_t)(voff + r0 + 1) * NR + nn] : 0.f;
-                v.z = (r0 + 2 < n) ? x32[(size_t)(voff + r0 + 2) * NR + nn] : 0.f;
-                v.w = (r0 + 3 < n) ? x32[(size_t)(voff + r0 + 3) * NR + nn] : 0.f;
-                tc::split_store(bhi, blo, tc::swz(nn, c), v);
-            }
+            if (tid < NR * 8) tc::split_store(bhi, blo, tc::swz(tid % NR, tid / NR), rb);
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncthreads();
             if (tid == 0) {
@@ -3295,6 +3303,7 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
             }
             pending[st] = true;
             ++seq;
+            if (J + 1 < tn) load_block(J + 1);   // in flight while the MMAs of block J run
         }
         // the last commit tracks every MMA issued before it: the accumulator is complete
         {
