@@ -3182,7 +3182,7 @@ __device__ __forceinline__ void ld8(unsigned taddr, uint32_t (&r)[16]) {
 }  // namespace tc
 
 template <int NR>
-__global__ void __launch_bounds__(tc::THREADS, 1)
+__global__ void __launch_bounds__(tc::THREADS, 2)
 tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, double *out, const int2 *units,
                     int nunits, int slot, int mode) {
     static_assert(NR == 8 || NR == 16 || NR == 32, "tensor-core SYMM: 8, 16 or 32 right-hand sides");
@@ -3233,10 +3233,11 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
         const int n = ts.mat_n[m], voff = ts.mat_voff[m], tn = ts.mat_tn[m];
         const long long t0 = ts.mat_tile0[m];
         const float *tiles = reinterpret_cast<const float *>(ts.tiles);
-        // block J of the unit into registers: four 16-byte A chunks and one B chunk per thread
+        // block J of the unit into registers: four 16-byte A chunks and one B chunk per thread;
+        // two register sets keep blocks J+1 and J+2 in flight while block J is staged
         constexpr int AIT = (tc::M * 8) / tc::THREADS;
-        float4 ra[AIT], rb = make_float4(0.f, 0.f, 0.f, 0.f);
-        auto load_block = [&](int J) {
+        float4 ra0[AIT], ra1[AIT], rb0 = make_float4(0.f, 0.f, 0.f, 0.f), rb1 = rb0;
+        auto load_block = [&](int J, float4 (&ra)[AIT], float4 &rb) {
 #pragma unroll
             for (int it = 0; it < AIT; ++it) {
                 const int q = tid + it * tc::THREADS;
@@ -3268,8 +3269,7 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
                 rb.w = (r0 + 3 < n) ? x32[(size_t)(voff + r0 + 3) * NR + nn] : 0.f;
             }
         };
-        load_block(0);
-        for (int J = 0; J < tn; ++J) {
+        auto step = [&](int J, float4 (&ra)[AIT], float4 &rb) {
             const int st = seq & 1;
             if (pending[st]) {
                 if (!mbar_wait(&bar[st], phase[st])) ok = false;
@@ -3303,7 +3303,13 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
             }
             pending[st] = true;
             ++seq;
-            if (J + 1 < tn) load_block(J + 1);   // in flight while the MMAs of block J run
+            if (J + 2 < tn) load_block(J + 2, ra, rb);   // in flight while blocks J and J+1 are processed
+        };
+        load_block(0, ra0, rb0);
+        if (tn > 1) load_block(1, ra1, rb1);
+        for (int J = 0; J < tn; J += 2) {
+            step(J, ra0, rb0);
+            if (J + 1 < tn) step(J + 1, ra1, rb1);
         }
         // the last commit tracks every MMA issued before it: the accumulator is complete
         {
