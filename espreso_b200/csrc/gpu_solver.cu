@@ -3662,6 +3662,8 @@ static void symm_launch(int nsm, int ncta, size_t sm, cudaStream_t st, TileSetDe
     static int per_sm = 0;
     if (per_sm == 0) {
         cudaFuncSetAttribute(tile_symm_kernel<PR, NR, SRC>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+        cudaFuncSetAttribute(tile_symm_kernel<PR, NR, SRC>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
         int b = 1;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, tile_symm_kernel<PR, NR, SRC>, 256, sm) != cudaSuccess ||
             b < 1)
@@ -3676,16 +3678,16 @@ template <int NR>
 static void symm_tc_launch(int nsm, int nunits, cudaStream_t st, TileSetDev td, DevProblem P, BlockDev B,
                            const float *x32, double *out, const int2 *units, int slot, int mode) {
     constexpr size_t sm = 2 * (2 * 128 * 128 + 2 * NR * 128) + 1024;
-    static int per_sm = 0;
-    if (per_sm == 0) {
+    static bool attr = false;
+    if (!attr) {
         cudaFuncSetAttribute(tile_symm_tc_kernel<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        int b = 1;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, tile_symm_tc_kernel<NR>, tc::THREADS, sm) != cudaSuccess ||
-            b < 1)
-            b = 1;
-        per_sm = b;
+        cudaFuncSetAttribute(tile_symm_tc_kernel<NR>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
+        attr = true;
     }
-    const int grid = std::max(1, std::min(nunits, nsm * per_sm));
+    // two CTAs per SM fit (registers and shared memory); CTAs never wait for one another, so a
+    // CTA that is not co-resident only starts later
+    const int grid = std::max(1, std::min(nunits, nsm * 2));
     tile_symm_tc_kernel<NR><<<grid, tc::THREADS, sm, st>>>(td, P, B, x32, out, units, nunits, slot, mode);
 }
 
