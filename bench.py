@@ -51,8 +51,12 @@ def parse():
     ap.add_argument("--loads", default="scaled", choices=["scaled", "traction"],
                     help="batched leg load cases: scaled copies of the config load, or seeded N(0,1e6) "
                          "nodal tractions on the x=1 face")
-    ap.add_argument("--symm-tensor", type=int, default=0, choices=[0, 1],
+    ap.add_argument("--symm-tensor", type=int, default=1, choices=[0, 1],
                     help="batched leg: FP32 SYMM on the tensor cores (tcgen05, 3xTF32) instead of CUDA cores")
+    ap.add_argument("--leg", default="solve", choices=["solve", "adjoint"],
+                    help="adjoint: one forward + backward of the density-to-displacement map (torch.autograd)")
+    ap.add_argument("--adjoint-grid", type=int, nargs=2, default=[4, 6], metavar=("DOMAINS", "ELEMENTS"),
+                    help="adjoint leg: DOMAINS^3 subdomains of ELEMENTS^3 HEXA8")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -372,9 +376,45 @@ def cpu_baseline_from_library(inst, P, args):
                       f"{iters} PCG iterations; projector and preconditioner not counted (lower bound)"}
 
 
+def run_adjoint(args):
+    """Forward + backward of the adjoint workload (seeded densities, point load, compliance plus a
+    seeded quadratic), timed on the host clock around the autograd calls; the two dual solves are
+    reported with their device times."""
+    import torch
+    from espreso_b200 import adjoint, problems
+    nd, ne = args.adjoint_grid
+    P, rho, f = problems.adjoint_cube(domains=(nd, nd, nd), elements=(ne, ne, ne), seed=0)
+    model = adjoint.SIMPModel(P, P.Ke, rhs=f, precision=args.precision, max_it=5000)
+    q = np.random.default_rng(9).uniform(0.0, 1e10, size=P.ndofs)
+    times = []
+    for _ in range(args.warmup + args.steps):
+        r = torch.tensor(rho, dtype=torch.float64, requires_grad=True)
+        t = time.perf_counter()
+        u = adjoint.solve(r, model)
+        t_fwd = time.perf_counter() - t
+        L = torch.dot(torch.from_numpy(f), u) + 0.5 * torch.sum(torch.from_numpy(q) * u * u)
+        t = time.perf_counter()
+        L.backward()
+        t_bwd = time.perf_counter() - t
+        times.append((t_fwd, t_bwd))
+    fwd = float(np.median([a for a, _ in times[args.warmup:]])) * 1e3
+    bwd = float(np.median([b for _, b in times[args.warmup:]])) * 1e3
+    line = {"metric": "adjoint forward + backward wall time", "value": fwd + bwd, "unit": "ms", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"adjoint_elasticity_{nd}^3x{ne}^3", "subdomains": nd ** 3,
+                       "elements": int(P.elem_nodes.shape[0]), "dofs": int(P.ndofs)},
+            "forward_ms": fwd, "backward_ms": bwd,
+            "note": "forward includes the host factorisation and Schur assembly of the new densities; "
+                    "backward reuses them (second dual solve + element sensitivity kernel)"}
+    print(json.dumps(line))
+
+
 if __name__ == "__main__":
     a = parse()
-    if a.impl == "reference":
+    if a.leg == "adjoint":
+        run_adjoint(a)
+    elif a.impl == "reference":
         run_reference(a)
     else:
         run_ours(a)

@@ -49,8 +49,8 @@ typedef enum {
     FETI4I_EXT_HOST_THREADS,     /* OpenMP threads of the preprocessing (0: all) */
     FETI4I_EXT_TILE_KERNEL,      /* Schur SYMV: 0 register-prefetch loads, 1 TMA bulk-copy pipeline */
     FETI4I_EXT_AUTOTUNE,         /* 1 (default): time both SYMV variants and the work-item sizes per size class */
-    FETI4I_EXT_SYMM_TENSOR,      /* multi-RHS solves with FP32 Schur storage: 1 tcgen05 tensor-core SYMM (3xTF32,
-                                    8 or more right-hand sides), 0 CUDA-core SYMM */
+    FETI4I_EXT_SYMM_TENSOR,      /* multi-RHS solves with FP32 Schur storage: 1 (default) tcgen05 tensor-core SYMM
+                                    (3xTF32, 8 or more right-hand sides), 0 CUDA-core SYMM */
     FETI4I_EXT_OPTIONS_SIZE
 } FETI4IExtOptions;
 void FETI4ISetExtendedOption(FETI4IInt key, FETI4IReal value);
