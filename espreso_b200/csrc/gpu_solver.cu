@@ -3181,18 +3181,29 @@ __device__ __forceinline__ void ld8(unsigned taddr, uint32_t (&r)[16]) {
 }
 }  // namespace tc
 
+// Raw tiles and x blocks arrive by cp.async.bulk into a ring of RAW slots, issued by thread 0
+// RAW-1 column blocks ahead (across unit boundaries); all threads convert a raw slot into the
+// swizzled TF32 hi/lo stage of the MMAs.  Slot metadata (unit, block) travels with the slot.
+namespace tc {
+constexpr int RAW = 4;
+}
+
 template <int NR>
-__global__ void __launch_bounds__(tc::THREADS, 2)
+__global__ void __launch_bounds__(tc::THREADS, 1)
 tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, double *out, const int2 *units,
                     int nunits, int slot, int mode) {
     static_assert(NR == 8 || NR == 16 || NR == 32, "tensor-core SYMM: 8, 16 or 32 right-hand sides");
     constexpr unsigned B_BYTES = NR * 128;
     constexpr unsigned STAGE = 2 * tc::A_BYTES + 2 * B_BYTES;
-    constexpr int HALF = NR / 2;                 // columns read back by each warp half
+    constexpr unsigned XB = TILE * NR * 4;                 // x block: 32 rows x NR FP32
+    constexpr unsigned RSLOT = 4 * TILE * TILE * 4 + XB;   // four raw tiles + x block
+    constexpr int HALF = NR / 2;
     extern __shared__ unsigned char tc_smem[];
-    __shared__ unsigned long long bar[2];
+    __shared__ unsigned long long bar[2];                  // MMA stages: commit arrivals
+    __shared__ unsigned long long full[tc::RAW];           // raw slots: bulk-copy completion
+    __shared__ int meta_unit[tc::RAW], meta_j[tc::RAW];
     __shared__ unsigned s_tmem;
-    __shared__ int s_unit, s_last, s_err;
+    __shared__ int s_err;
     __shared__ double s_dot[tc::THREADS / 32][NR];
     if (mode != 0) {
         const int iter = P.st->iter_base + slot;
@@ -3201,6 +3212,7 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned base = smem_u32(tc_smem);
     unsigned char *buf = tc_smem + ((1024u - (base & 1023u)) & 1023u);   // 1024-byte aligned stages
+    unsigned char *raw = buf + 2 * STAGE;                                  // raw ring after the stages
     const unsigned ncols = 32;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
@@ -3211,6 +3223,7 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
     if (tid == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
+        for (int r = 0; r < tc::RAW; ++r) mbar_init(&full[r], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_err = 0;
     }
@@ -3219,112 +3232,149 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
     tc::fence_after();
     const unsigned tmem = s_tmem;
     constexpr uint32_t ID = tc::idesc<NR>();
+    const float *tiles = reinterpret_cast<const float *>(ts.tiles);
+    const unsigned long long pol = policy_evict_first();
+    // producer state (thread 0 only): the next block to issue
+    int p_unit = -1, p_j = 0, p_tn = 0;
+    bool p_done = false;
+    long long issued = 0;          // steps issued (thread 0)
+    // issue the next step into its raw slot; an end marker (unit -1) once the queue is empty
+    auto produce = [&]() {
+        if (p_done) return;
+        if (p_unit < 0 || p_j >= p_tn) {
+            const int u = atomicAdd(&B.queue[0], 1);
+            if (u >= nunits) {
+                const int r = (int)(issued % tc::RAW);
+                meta_unit[r] = -1;
+                meta_j[r] = 0;
+                mbar_arrive(&full[r]);
+                ++issued;
+                p_done = true;
+                return;
+            }
+            p_unit = u;
+            p_j = 0;
+            p_tn = ts.mat_tn[units[u].x];
+        }
+        const int r = (int)(issued % tc::RAW);
+        const int m = units[p_unit].x, I0 = 4 * units[p_unit].y, J = p_j;
+        const int tn = p_tn, voff = ts.mat_voff[m];
+        const long long t0 = ts.mat_tile0[m];
+        unsigned char *dst = raw + (size_t)r * RSLOT;
+        int nval = 0;
+        for (int q = 0; q < 4; ++q)
+            if (I0 + q < tn) ++nval;
+        meta_unit[r] = p_unit;
+        meta_j[r] = J;
+        // the slot was read by generic loads before the last barrier; order them before the async writes
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_arrive_tx(&full[r], (unsigned)nval * (TILE * TILE * 4) + XB);
+        for (int q = 0; q < 4; ++q) {
+            const int I = I0 + q;
+            if (I >= tn) continue;
+            const int a = J >= I ? I : J, b = J >= I ? J : I;
+            const long long tid_ = t0 + (long long)a * tn - (long long)a * (a - 1) / 2 + (b - a);
+            bulk_g2s(dst + q * (TILE * TILE * 4), tiles + (size_t)tid_ * (TILE * TILE), TILE * TILE * 4, &full[r], pol);
+        }
+        // x rows 32J..32J+31 (rows past the subdomain are zeroed at conversion; the vector is padded)
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                smem_u32(dst + 4 * TILE * TILE * 4)),
+            "l"(x32 + (size_t)(voff + TILE * J) * NR), "r"(XB), "r"(smem_u32(&full[r]))
+            : "memory");
+        ++issued;
+        ++p_j;
+    };
+    if (tid == 0)
+        for (int k = 0; k < tc::RAW - 1; ++k) produce();
     unsigned phase[2] = {0u, 0u};
     bool pending[2] = {false, false};
     unsigned seq = 0;
+    long long step = 0;            // steps consumed
     bool ok = true;
     for (;;) {
-        if (tid == 0) s_unit = atomicAdd(&B.queue[0], 1);
-        const bool all_ok = __syncthreads_and(ok);   // a timed-out wait stops every thread together
-        const int u = s_unit;
-        if (u >= nunits || !all_ok) break;
-        ok = true;
+        if (tid == 0) produce();   // keeps RAW - 1 blocks in flight beyond the one converted now
+        const int r = (int)(step % tc::RAW);
+        if (!mbar_wait(&full[r], (unsigned)((step / tc::RAW) & 1))) ok = false;
+        const bool all_ok = __syncthreads_and(ok);
+        const int u = meta_unit[r], J = meta_j[r];
+        if (u < 0 || !all_ok) break;
+        ++step;
         const int m = units[u].x, I0 = 4 * units[u].y;
         const int n = ts.mat_n[m], voff = ts.mat_voff[m], tn = ts.mat_tn[m];
-        const long long t0 = ts.mat_tile0[m];
-        const float *tiles = reinterpret_cast<const float *>(ts.tiles);
-        // block J of the unit into registers: four 16-byte A chunks and one B chunk per thread;
-        // two register sets keep blocks J+1 and J+2 in flight while block J is staged
-        constexpr int AIT = (tc::M * 8) / tc::THREADS;
-        float4 ra0[AIT], ra1[AIT], rb0 = make_float4(0.f, 0.f, 0.f, 0.f), rb1 = rb0;
-        auto load_block = [&](int J, float4 (&ra)[AIT], float4 &rb) {
+        const unsigned char *src = raw + (size_t)r * RSLOT;
+        const int st = seq & 1;
+        if (pending[st]) {
+            if (!mbar_wait(&bar[st], phase[st])) ok = false;
+            phase[st] ^= 1u;
+            pending[st] = false;
+        }
+        unsigned char *ahi = buf + st * STAGE, *alo = ahi + tc::A_BYTES, *bhi = alo + tc::A_BYTES,
+                      *blo = bhi + B_BYTES;
+        // A: 128 rows x 8 chunks; upper tiles as stored, lower tiles transposed, missing rows zero
 #pragma unroll
-            for (int it = 0; it < AIT; ++it) {
-                const int q = tid + it * tc::THREADS;
-                const int qq = q >> 8, I = I0 + qq;       // warp-uniform
-                ra[it] = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (I < tn && J >= I) {
-                    const int rr = (q >> 3) & 31, c = q & 7;
-                    const long long tid_ = t0 + (long long)I * tn - (long long)I * (I - 1) / 2 + (J - I);
-                    const uint4 u4 =
-                        ld_stream(reinterpret_cast<const uint4 *>(tiles + (size_t)tid_ * (TILE * TILE) + rr * TILE + 4 * c));
-                    ra[it] = make_float4(__uint_as_float(u4.x), __uint_as_float(u4.y), __uint_as_float(u4.z),
-                                         __uint_as_float(u4.w));
-                } else if (I < tn) {
-                    const int rr = q & 31, c = (q >> 5) & 7;
-                    const long long tid_ = t0 + (long long)J * tn - (long long)J * (J - 1) / 2 + (I - J);
-                    const float *tp = tiles + (size_t)tid_ * (TILE * TILE) + rr;
-                    ra[it].x = tp[(4 * c + 0) * TILE];
-                    ra[it].y = tp[(4 * c + 1) * TILE];
-                    ra[it].z = tp[(4 * c + 2) * TILE];
-                    ra[it].w = tp[(4 * c + 3) * TILE];
+        for (int it = 0; it < (tc::M * 8) / tc::THREADS; ++it) {
+            const int q = tid + it * tc::THREADS;
+            const int qq = q >> 8, I = I0 + qq;       // warp-uniform
+            const float *tsrc = reinterpret_cast<const float *>(src + qq * (TILE * TILE * 4));
+            int rr, c;
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (I < tn && J >= I) {
+                rr = (q >> 3) & 31;
+                c = q & 7;
+                v = *reinterpret_cast<const float4 *>(tsrc + rr * TILE + 4 * c);
+            } else {
+                rr = q & 31;
+                c = (q >> 5) & 7;
+                if (I < tn) {
+                    v.x = tsrc[(4 * c + 0) * TILE + rr];
+                    v.y = tsrc[(4 * c + 1) * TILE + rr];
+                    v.z = tsrc[(4 * c + 2) * TILE + rr];
+                    v.w = tsrc[(4 * c + 3) * TILE + rr];
                 }
             }
-            if (tid < NR * 8) {
-                const int nn = tid % NR, c = tid / NR;
-                const int r0 = TILE * J + 4 * c;
-                rb.x = (r0 + 0 < n) ? x32[(size_t)(voff + r0 + 0) * NR + nn] : 0.f;
-                rb.y = (r0 + 1 < n) ? x32[(size_t)(voff + r0 + 1) * NR + nn] : 0.f;
-                rb.z = (r0 + 2 < n) ? x32[(size_t)(voff + r0 + 2) * NR + nn] : 0.f;
-                rb.w = (r0 + 3 < n) ? x32[(size_t)(voff + r0 + 3) * NR + nn] : 0.f;
-            }
-        };
-        auto step = [&](int J, float4 (&ra)[AIT], float4 &rb) {
-            const int st = seq & 1;
-            if (pending[st]) {
-                if (!mbar_wait(&bar[st], phase[st])) ok = false;
-                phase[st] ^= 1u;
-                pending[st] = false;
-            }
-            unsigned char *ahi = buf + st * STAGE, *alo = ahi + tc::A_BYTES, *bhi = alo + tc::A_BYTES,
-                          *blo = bhi + B_BYTES;
-#pragma unroll
-            for (int it = 0; it < AIT; ++it) {
-                const int q = tid + it * tc::THREADS;
-                const int qq = q >> 8, I = I0 + qq;
-                const bool up = (I < tn && J >= I);
-                const int rr = up ? ((q >> 3) & 31) : (q & 31), c = up ? (q & 7) : ((q >> 5) & 7);
-                tc::split_store(ahi, alo, tc::swz(qq * 32 + rr, c), ra[it]);
-            }
-            if (tid < NR * 8) tc::split_store(bhi, blo, tc::swz(tid % NR, tid / NR), rb);
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            __syncthreads();
-            if (tid == 0) {
-                tc::fence_after();
-                const unsigned a_hi = smem_u32(ahi), a_lo = smem_u32(alo), b_hi = smem_u32(bhi), b_lo = smem_u32(blo);
-#pragma unroll
-                for (int kk = 0; kk < 4; ++kk) {
-                    const unsigned off = 32u * kk;
-                    tc::mma(tmem, tc::sdesc(a_hi + off), tc::sdesc(b_hi + off), ID, (J > 0 || kk > 0) ? 1u : 0u);
-                    tc::mma(tmem, tc::sdesc(a_hi + off), tc::sdesc(b_lo + off), ID, 1u);
-                    tc::mma(tmem, tc::sdesc(a_lo + off), tc::sdesc(b_hi + off), ID, 1u);
-                }
-                tc::commit(&bar[st]);
-            }
-            pending[st] = true;
-            ++seq;
-            if (J + 2 < tn) load_block(J + 2, ra, rb);   // in flight while blocks J and J+1 are processed
-        };
-        load_block(0, ra0, rb0);
-        if (tn > 1) load_block(1, ra1, rb1);
-        for (int J = 0; J < tn; J += 2) {
-            step(J, ra0, rb0);
-            if (J + 1 < tn) step(J + 1, ra1, rb1);
+            tc::split_store(ahi, alo, tc::swz(qq * 32 + rr, c), v);
         }
-        // the last commit tracks every MMA issued before it: the accumulator is complete
-        {
-            const int lst = (seq - 1) & 1;
-            if (!mbar_wait(&bar[lst], phase[lst])) ok = false;
-            phase[lst] ^= 1u;
-            pending[lst] = false;
+        // B: NR rows (right-hand sides) x 8 chunks; x rows past the subdomain are zero
+        if (tid < NR * 8) {
+            const int nn = tid % NR, c = tid / NR;
+            const float *xs = reinterpret_cast<const float *>(src + 4 * TILE * TILE * 4);
+            const int r0 = TILE * J + 4 * c;
+            float4 v;
+            v.x = (r0 + 0 < n) ? xs[(4 * c + 0) * NR + nn] : 0.f;
+            v.y = (r0 + 1 < n) ? xs[(4 * c + 1) * NR + nn] : 0.f;
+            v.z = (r0 + 2 < n) ? xs[(4 * c + 2) * NR + nn] : 0.f;
+            v.w = (r0 + 3 < n) ? xs[(4 * c + 3) * NR + nn] : 0.f;
+            tc::split_store(bhi, blo, tc::swz(nn, c), v);
         }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            tc::fence_after();
+            const unsigned a_hi = smem_u32(ahi), a_lo = smem_u32(alo), b_hi = smem_u32(bhi), b_lo = smem_u32(blo);
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) {
+                const unsigned off = 32u * kk;
+                tc::mma(tmem, tc::sdesc(a_hi + off), tc::sdesc(b_hi + off), ID, (J > 0 || kk > 0) ? 1u : 0u);
+                tc::mma(tmem, tc::sdesc(a_hi + off), tc::sdesc(b_lo + off), ID, 1u);
+                tc::mma(tmem, tc::sdesc(a_lo + off), tc::sdesc(b_hi + off), ID, 1u);
+            }
+            tc::commit(&bar[st]);
+        }
+        pending[st] = true;
+        ++seq;
+        if (J + 1 < tn) continue;
+        // last block of the unit: the commit tracks every MMA issued before it
+        if (!mbar_wait(&bar[st], phase[st])) ok = false;
+        phase[st] ^= 1u;
+        pending[st] = false;
         tc::fence_after();
         // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31, columns (w / 4) * HALF .. +HALF-1
-        uint32_t r[16];
+        uint32_t rv[16];
         const unsigned taddr = tmem + ((unsigned)(32 * (warp & 3)) << 16) + (unsigned)((warp >> 2) * HALF);
-        if (HALF == 16) tc::ld16(taddr, r);
-        else if (HALF == 8) tc::ld8(taddr, r);
-        else tc::ld4(taddr, r);
+        if (HALF == 16) tc::ld16(taddr, rv);
+        else if (HALF == 8) tc::ld8(taddr, rv);
+        else tc::ld4(taddr, rv);
         const int row = TILE * I0 + 32 * (warp & 3) + lane;
         const int c0 = (warp >> 2) * HALF;
         double dl[HALF];
@@ -3333,7 +3383,7 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
             dl[c] = 0.0;
             if (row < n && ok) {
                 const size_t o = (size_t)(voff + row) * NR + c0 + c;
-                const double y = (double)__uint_as_float(r[c]);
+                const double y = (double)__uint_as_float(rv[c]);
                 out[o] = y;
                 dl[c] = (double)x32[o] * y;
             }
@@ -3354,18 +3404,22 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
             B.unit_dot[(size_t)u * NR + tid] = t;
         }
     }
-    // drain: both stages idle before the tensor memory is released
+    // drain: every issued copy and every MMA has landed before the CTA leaves
+    if (tid == 0)
+        for (long long k = step; k < issued; ++k)
+            if (!mbar_wait(&full[k % tc::RAW], (unsigned)((k / tc::RAW) & 1))) ok = false;
     for (int stg = 0; stg < 2; ++stg)
         if (pending[stg]) {
             if (!mbar_wait(&bar[stg], phase[stg])) ok = false;
             pending[stg] = false;
         }
-    if (!ok && lane == 0) s_err = 1;
+    if (!ok) s_err = 1;
     tc::fence_before();
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
-    if (tid == 0 && s_err) atomicExch(&P.st->error, 1);
+    __shared__ int s_last;
     if (tid == 0) {
+        if (s_err) atomicExch(&P.st->error, 1);
         __threadfence();
         s_last = (atomicAdd(&B.queue[1], 1) == (int)gridDim.x - 1);
     }
@@ -3586,7 +3640,9 @@ void GpuSolver::Impl::ensure_block(int nr) {
     B.x = alloc<double>((size_t)NL * nr); B.r = alloc<double>((size_t)NL * nr); B.w = alloc<double>((size_t)NL * nr);
     B.z = alloc<double>((size_t)NL * nr); B.y = alloc<double>((size_t)NL * nr); B.p = alloc<double>((size_t)NL * nr);
     B.Ap = alloc<double>((size_t)NL * nr); B.Ax = alloc<double>((size_t)NL * nr); B.bL = alloc<double>((size_t)NL * nr);
-    B.p32 = alloc<float>((size_t)NL * nr);
+    // 32 rows of padding: the tensor-core SYMM copies whole 32-row x blocks
+    B.p32 = alloc<float>((size_t)(NL + TILE) * nr);
+    CUDA_CHECK(cudaMemset(B.p32, 0, sizeof(float) * (size_t)(NL + TILE) * nr));
     B.uT = alloc<double>((size_t)NT * nr); B.vT = alloc<double>((size_t)NT * nr);
     // alpha carries KS zero rows past nK for the fixed-width G^T alpha loads
     B.d = alloc<double>((size_t)P.nP * nr); B.alpha = alloc<double>((size_t)(nK + P.KS) * nr);
@@ -3677,7 +3733,7 @@ static void symm_launch(int nsm, int ncta, size_t sm, cudaStream_t st, TileSetDe
 template <int NR>
 static void symm_tc_launch(int nsm, int nunits, cudaStream_t st, TileSetDev td, DevProblem P, BlockDev B,
                            const float *x32, double *out, const int2 *units, int slot, int mode) {
-    constexpr size_t sm = 2 * (2 * 128 * 128 + 2 * NR * 128) + 1024;
+    constexpr size_t sm = 2 * (2 * 128 * 128 + 2 * NR * 128) + tc::RAW * (4 * 32 * 32 * 4 + 32 * NR * 4) + 1024;
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(tile_symm_tc_kernel<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -3685,9 +3741,8 @@ static void symm_tc_launch(int nsm, int nunits, cudaStream_t st, TileSetDev td, 
                              cudaSharedmemCarveoutMaxShared);
         attr = true;
     }
-    // two CTAs per SM fit (registers and shared memory); CTAs never wait for one another, so a
-    // CTA that is not co-resident only starts later
-    const int grid = std::max(1, std::min(nunits, nsm * 2));
+    // one CTA per SM (the raw ring and the stages fill its shared memory)
+    const int grid = std::max(1, std::min(nunits, nsm));
     tile_symm_tc_kernel<NR><<<grid, tc::THREADS, sm, st>>>(td, P, B, x32, out, units, nunits, slot, mode);
 }
 
