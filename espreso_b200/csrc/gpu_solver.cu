@@ -3185,7 +3185,9 @@ __device__ __forceinline__ void ld8(unsigned taddr, uint32_t (&r)[16]) {
 // RAW-1 column blocks ahead (across unit boundaries); all threads convert a raw slot into the
 // swizzled TF32 hi/lo stage of the MMAs.  Slot metadata (unit, block) travels with the slot.
 namespace tc {
-constexpr int RAW = 4;
+constexpr int RAW = 4;      // raw slots (three column blocks in flight beyond the one converted)
+constexpr int NST = 3;      // MMA operand stages
+constexpr int PRODUCER = 32;  // thread that issues the bulk copies (warp 1): thread 0 issues the MMAs
 }
 
 template <int NR>
@@ -3199,9 +3201,10 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
     constexpr unsigned RSLOT = 4 * TILE * TILE * 4 + XB;   // four raw tiles + x block
     constexpr int HALF = NR / 2;
     extern __shared__ unsigned char tc_smem[];
-    __shared__ unsigned long long bar[2];                  // MMA stages: commit arrivals
+    __shared__ unsigned long long bar[tc::NST];            // MMA stages: commit arrivals
     __shared__ unsigned long long full[tc::RAW];           // raw slots: bulk-copy completion
-    __shared__ int meta_unit[tc::RAW], meta_j[tc::RAW];
+    // per raw slot: unit, block J, subdomain rows n, first row voff, tile rows tn, first tile row I0
+    __shared__ int meta[tc::RAW][6];
     __shared__ unsigned s_tmem;
     __shared__ int s_err;
     __shared__ double s_dot[tc::THREADS / 32][NR];
@@ -3212,7 +3215,7 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned base = smem_u32(tc_smem);
     unsigned char *buf = tc_smem + ((1024u - (base & 1023u)) & 1023u);   // 1024-byte aligned stages
-    unsigned char *raw = buf + 2 * STAGE;                                  // raw ring after the stages
+    unsigned char *raw = buf + tc::NST * STAGE;                             // raw ring after the stages
     const unsigned ncols = 32;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
@@ -3221,8 +3224,7 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        for (int b = 0; b < tc::NST; ++b) mbar_init(&bar[b], 1);
         for (int r = 0; r < tc::RAW; ++r) mbar_init(&full[r], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_err = 0;
@@ -3234,38 +3236,48 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
     constexpr uint32_t ID = tc::idesc<NR>();
     const float *tiles = reinterpret_cast<const float *>(ts.tiles);
     const unsigned long long pol = policy_evict_first();
-    // producer state (thread 0 only): the next block to issue
-    int p_unit = -1, p_j = 0, p_tn = 0;
+    // producer state (thread PRODUCER only): the unit being issued, cached, and the next unit
+    // already taken from the queue so that its atomic overlaps the current unit
+    int p_unit = -1, p_j = 0, p_tn = 0, p_m = 0, p_I0 = 0, p_n = 0, p_voff = 0, p_next = -1;
+    long long p_t0 = 0;
     bool p_done = false;
-    long long issued = 0;          // steps issued (thread 0)
+    long long issued = 0;          // steps issued (thread PRODUCER)
+    if (tid == tc::PRODUCER) p_next = atomicAdd(&B.queue[0], 1);
     // issue the next step into its raw slot; an end marker (unit -1) once the queue is empty
     auto produce = [&]() {
         if (p_done) return;
         if (p_unit < 0 || p_j >= p_tn) {
-            const int u = atomicAdd(&B.queue[0], 1);
+            const int u = p_next;
             if (u >= nunits) {
                 const int r = (int)(issued % tc::RAW);
-                meta_unit[r] = -1;
-                meta_j[r] = 0;
+                meta[r][0] = -1;
                 mbar_arrive(&full[r]);
                 ++issued;
                 p_done = true;
                 return;
             }
+            p_next = atomicAdd(&B.queue[0], 1);
             p_unit = u;
             p_j = 0;
-            p_tn = ts.mat_tn[units[u].x];
+            p_m = units[u].x;
+            p_I0 = 4 * units[u].y;
+            p_tn = ts.mat_tn[p_m];
+            p_n = ts.mat_n[p_m];
+            p_voff = ts.mat_voff[p_m];
+            p_t0 = ts.mat_tile0[p_m];
         }
         const int r = (int)(issued % tc::RAW);
-        const int m = units[p_unit].x, I0 = 4 * units[p_unit].y, J = p_j;
-        const int tn = p_tn, voff = ts.mat_voff[m];
-        const long long t0 = ts.mat_tile0[m];
+        const int I0 = p_I0, J = p_j, tn = p_tn;
         unsigned char *dst = raw + (size_t)r * RSLOT;
         int nval = 0;
         for (int q = 0; q < 4; ++q)
             if (I0 + q < tn) ++nval;
-        meta_unit[r] = p_unit;
-        meta_j[r] = J;
+        meta[r][0] = p_unit;
+        meta[r][1] = J;
+        meta[r][2] = p_n;
+        meta[r][3] = p_voff;
+        meta[r][4] = tn;
+        meta[r][5] = I0;
         // the slot was read by generic loads before the last barrier; order them before the async writes
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         mbar_arrive_tx(&full[r], (unsigned)nval * (TILE * TILE * 4) + XB);
@@ -3273,37 +3285,36 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
             const int I = I0 + q;
             if (I >= tn) continue;
             const int a = J >= I ? I : J, b = J >= I ? J : I;
-            const long long tid_ = t0 + (long long)a * tn - (long long)a * (a - 1) / 2 + (b - a);
+            const long long tid_ = p_t0 + (long long)a * tn - (long long)a * (a - 1) / 2 + (b - a);
             bulk_g2s(dst + q * (TILE * TILE * 4), tiles + (size_t)tid_ * (TILE * TILE), TILE * TILE * 4, &full[r], pol);
         }
         // x rows 32J..32J+31 (rows past the subdomain are zeroed at conversion; the vector is padded)
         asm volatile(
             "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                 smem_u32(dst + 4 * TILE * TILE * 4)),
-            "l"(x32 + (size_t)(voff + TILE * J) * NR), "r"(XB), "r"(smem_u32(&full[r]))
+            "l"(x32 + (size_t)(p_voff + TILE * J) * NR), "r"(XB), "r"(smem_u32(&full[r]))
             : "memory");
         ++issued;
         ++p_j;
     };
-    if (tid == 0)
+    if (tid == tc::PRODUCER)
         for (int k = 0; k < tc::RAW - 1; ++k) produce();
-    unsigned phase[2] = {0u, 0u};
-    bool pending[2] = {false, false};
+    unsigned phase[tc::NST] = {};
+    bool pending[tc::NST] = {};
     unsigned seq = 0;
     long long step = 0;            // steps consumed
     bool ok = true;
     for (;;) {
-        if (tid == 0) produce();   // keeps RAW - 1 blocks in flight beyond the one converted now
+        if (tid == tc::PRODUCER) produce();   // keeps RAW - 1 blocks in flight beyond the one converted now
         const int r = (int)(step % tc::RAW);
         if (!mbar_wait(&full[r], (unsigned)((step / tc::RAW) & 1))) ok = false;
         const bool all_ok = __syncthreads_and(ok);
-        const int u = meta_unit[r], J = meta_j[r];
+        const int u = meta[r][0];
         if (u < 0 || !all_ok) break;
+        const int J = meta[r][1], n = meta[r][2], voff = meta[r][3], tn = meta[r][4], I0 = meta[r][5];
         ++step;
-        const int m = units[u].x, I0 = 4 * units[u].y;
-        const int n = ts.mat_n[m], voff = ts.mat_voff[m], tn = ts.mat_tn[m];
         const unsigned char *src = raw + (size_t)r * RSLOT;
-        const int st = seq & 1;
+        const int st = seq % tc::NST;
         if (pending[st]) {
             if (!mbar_wait(&bar[st], phase[st])) ok = false;
             phase[st] ^= 1u;
@@ -3405,10 +3416,10 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
         }
     }
     // drain: every issued copy and every MMA has landed before the CTA leaves
-    if (tid == 0)
+    if (tid == tc::PRODUCER)
         for (long long k = step; k < issued; ++k)
             if (!mbar_wait(&full[k % tc::RAW], (unsigned)((k / tc::RAW) & 1))) ok = false;
-    for (int stg = 0; stg < 2; ++stg)
+    for (int stg = 0; stg < tc::NST; ++stg)
         if (pending[stg]) {
             if (!mbar_wait(&bar[stg], phase[stg])) ok = false;
             pending[stg] = false;
@@ -3733,7 +3744,7 @@ static void symm_launch(int nsm, int ncta, size_t sm, cudaStream_t st, TileSetDe
 template <int NR>
 static void symm_tc_launch(int nsm, int nunits, cudaStream_t st, TileSetDev td, DevProblem P, BlockDev B,
                            const float *x32, double *out, const int2 *units, int slot, int mode) {
-    constexpr size_t sm = 2 * (2 * 128 * 128 + 2 * NR * 128) + tc::RAW * (4 * 32 * 32 * 4 + 32 * NR * 4) + 1024;
+    constexpr size_t sm = tc::NST * (2 * 128 * 128 + 2 * NR * 128) + tc::RAW * (4 * 32 * 32 * 4 + 32 * NR * 4) + 1024;
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(tile_symm_tc_kernel<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
