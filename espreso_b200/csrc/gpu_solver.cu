@@ -3181,17 +3181,36 @@ __device__ __forceinline__ void ld8(unsigned taddr, uint32_t (&r)[16]) {
 }
 }  // namespace tc
 
-// Raw tiles and x blocks arrive by cp.async.bulk into a ring of RAW slots, issued by thread 0
-// RAW-1 column blocks ahead (across unit boundaries); all threads convert a raw slot into the
-// swizzled TF32 hi/lo stage of the MMAs.  Slot metadata (unit, block) travels with the slot.
+// Warp-specialised pipeline (no CTA-wide barrier inside the loop):
+//   warp 0      issues the MMAs (one lane) and owns the tensor memory;
+//   warp 1      issues the cp.async.bulk copies of raw tiles and x blocks into a RAW-slot ring;
+//   warps 2..9  convert a raw slot into a swizzled TF32 hi/lo MMA stage, and run the epilogue
+//               of a finished unit (tcgen05.ld by lane quadrant, two accumulators alternate).
+// Hand-overs are mbarriers: full/empty (raw ring), staged/done (MMA stages), acc_full/acc_empty
+// (accumulators).  Every wait is bounded and gives up at once after any other wait timed out;
+// the copies and MMAs in flight are drained (bounded) before the tensor memory is released.
 namespace tc {
-constexpr int RAW = 4;      // raw slots (three column blocks in flight beyond the one converted)
-constexpr int NST = 3;      // MMA operand stages
-constexpr int PRODUCER = 32;  // thread that issues the bulk copies (warp 1): thread 0 issues the MMAs
+constexpr int RAW = 4;        // raw slots
+constexpr int NST = 3;        // MMA operand stages
+constexpr int CONV = 8;       // converter warps
+constexpr int WS_THREADS = 32 * (2 + CONV);
 }
 
+struct TcAbort {
+    int *flag;
+    __device__ bool wait(unsigned long long *bar, unsigned parity) const {
+        for (long long i = 0; i < WAIT_LIMIT; ++i) {
+            if (mbar_try(bar, parity)) return true;
+            if (*(volatile int *)flag) return false;
+            if (i > 64) __nanosleep(64);
+        }
+        atomicExch(flag, 1);
+        return false;
+    }
+};
+
 template <int NR>
-__global__ void __launch_bounds__(tc::THREADS, 1)
+__global__ void __launch_bounds__(tc::WS_THREADS, 1)
 tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, double *out, const int2 *units,
                     int nunits, int slot, int mode) {
     static_assert(NR == 8 || NR == 16 || NR == 32, "tensor-core SYMM: 8, 16 or 32 right-hand sides");
@@ -3200,14 +3219,15 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
     constexpr unsigned XB = TILE * NR * 4;                 // x block: 32 rows x NR FP32
     constexpr unsigned RSLOT = 4 * TILE * TILE * 4 + XB;   // four raw tiles + x block
     constexpr int HALF = NR / 2;
+    constexpr int CT = 32 * tc::CONV;                      // converter threads
     extern __shared__ unsigned char tc_smem[];
-    __shared__ unsigned long long bar[tc::NST];            // MMA stages: commit arrivals
-    __shared__ unsigned long long full[tc::RAW];           // raw slots: bulk-copy completion
-    // per raw slot: unit, block J, subdomain rows n, first row voff, tile rows tn, first tile row I0
-    __shared__ int meta[tc::RAW][6];
+    __shared__ unsigned long long full[tc::RAW], empty[tc::RAW];
+    __shared__ unsigned long long staged[tc::NST], done[tc::NST];
+    __shared__ unsigned long long acc_full[2], acc_empty[2];
+    __shared__ int meta[tc::RAW][6];                      // unit, J, n, voff, tn, I0 (unit -1: end)
+    __shared__ int smeta[tc::NST][3];                     // unit, J, tn of a staged block (unit -1: end)
     __shared__ unsigned s_tmem;
-    __shared__ int s_err;
-    __shared__ double s_dot[tc::THREADS / 32][NR];
+    __shared__ int s_abort;
     if (mode != 0) {
         const int iter = P.st->iter_base + slot;
         if (skip_iter(P.st, iter)) return;
@@ -3215,8 +3235,8 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned base = smem_u32(tc_smem);
     unsigned char *buf = tc_smem + ((1024u - (base & 1023u)) & 1023u);   // 1024-byte aligned stages
-    unsigned char *raw = buf + tc::NST * STAGE;                             // raw ring after the stages
-    const unsigned ncols = 32;
+    unsigned char *raw = buf + tc::NST * STAGE;
+    const unsigned ncols = 64;                                            // two accumulators of 32 columns
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
                      "r"(ncols)
@@ -3224,213 +3244,223 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        for (int b = 0; b < tc::NST; ++b) mbar_init(&bar[b], 1);
-        for (int r = 0; r < tc::RAW; ++r) mbar_init(&full[r], 1);
+        for (int r = 0; r < tc::RAW; ++r) { mbar_init(&full[r], 1); mbar_init(&empty[r], tc::CONV); }
+        for (int s = 0; s < tc::NST; ++s) { mbar_init(&staged[s], tc::CONV); mbar_init(&done[s], 1); }
+        for (int a = 0; a < 2; ++a) { mbar_init(&acc_full[a], 1); mbar_init(&acc_empty[a], tc::CONV); }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        s_err = 0;
+        s_abort = 0;
     }
     tc::fence_before();
     __syncthreads();
     tc::fence_after();
     const unsigned tmem = s_tmem;
-    constexpr uint32_t ID = tc::idesc<NR>();
+    const TcAbort W{&s_abort};
     const float *tiles = reinterpret_cast<const float *>(ts.tiles);
-    const unsigned long long pol = policy_evict_first();
-    // producer state (thread PRODUCER only): the unit being issued, cached, and the next unit
-    // already taken from the queue so that its atomic overlaps the current unit
-    int p_unit = -1, p_j = 0, p_tn = 0, p_m = 0, p_I0 = 0, p_n = 0, p_voff = 0, p_next = -1;
-    long long p_t0 = 0;
-    bool p_done = false;
-    long long issued = 0;          // steps issued (thread PRODUCER)
-    if (tid == tc::PRODUCER) p_next = atomicAdd(&B.queue[0], 1);
-    // issue the next step into its raw slot; an end marker (unit -1) once the queue is empty
-    auto produce = [&]() {
-        if (p_done) return;
-        if (p_unit < 0 || p_j >= p_tn) {
-            const int u = p_next;
-            if (u >= nunits) {
-                const int r = (int)(issued % tc::RAW);
-                meta[r][0] = -1;
-                mbar_arrive(&full[r]);
-                ++issued;
-                p_done = true;
-                return;
-            }
-            p_next = atomicAdd(&B.queue[0], 1);
-            p_unit = u;
-            p_j = 0;
-            p_m = units[u].x;
-            p_I0 = 4 * units[u].y;
-            p_tn = ts.mat_tn[p_m];
-            p_n = ts.mat_n[p_m];
-            p_voff = ts.mat_voff[p_m];
-            p_t0 = ts.mat_tile0[p_m];
-        }
-        const int r = (int)(issued % tc::RAW);
-        const int I0 = p_I0, J = p_j, tn = p_tn;
-        unsigned char *dst = raw + (size_t)r * RSLOT;
-        int nval = 0;
-        for (int q = 0; q < 4; ++q)
-            if (I0 + q < tn) ++nval;
-        meta[r][0] = p_unit;
-        meta[r][1] = J;
-        meta[r][2] = p_n;
-        meta[r][3] = p_voff;
-        meta[r][4] = tn;
-        meta[r][5] = I0;
-        // the slot was read by generic loads before the last barrier; order them before the async writes
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_arrive_tx(&full[r], (unsigned)nval * (TILE * TILE * 4) + XB);
-        for (int q = 0; q < 4; ++q) {
-            const int I = I0 + q;
-            if (I >= tn) continue;
-            const int a = J >= I ? I : J, b = J >= I ? J : I;
-            const long long tid_ = p_t0 + (long long)a * tn - (long long)a * (a - 1) / 2 + (b - a);
-            bulk_g2s(dst + q * (TILE * TILE * 4), tiles + (size_t)tid_ * (TILE * TILE), TILE * TILE * 4, &full[r], pol);
-        }
-        // x rows 32J..32J+31 (rows past the subdomain are zeroed at conversion; the vector is padded)
-        asm volatile(
-            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                smem_u32(dst + 4 * TILE * TILE * 4)),
-            "l"(x32 + (size_t)(p_voff + TILE * J) * NR), "r"(XB), "r"(smem_u32(&full[r]))
-            : "memory");
-        ++issued;
-        ++p_j;
-    };
-    if (tid == tc::PRODUCER)
-        for (int k = 0; k < tc::RAW - 1; ++k) produce();
-    unsigned phase[tc::NST] = {};
-    bool pending[tc::NST] = {};
-    unsigned seq = 0;
-    long long step = 0;            // steps consumed
-    bool ok = true;
-    for (;;) {
-        if (tid == tc::PRODUCER) produce();   // keeps RAW - 1 blocks in flight beyond the one converted now
-        const int r = (int)(step % tc::RAW);
-        if (!mbar_wait(&full[r], (unsigned)((step / tc::RAW) & 1))) ok = false;
-        const bool all_ok = __syncthreads_and(ok);
-        const int u = meta[r][0];
-        if (u < 0 || !all_ok) break;
-        const int J = meta[r][1], n = meta[r][2], voff = meta[r][3], tn = meta[r][4], I0 = meta[r][5];
-        ++step;
-        const unsigned char *src = raw + (size_t)r * RSLOT;
-        const int st = seq % tc::NST;
-        if (pending[st]) {
-            if (!mbar_wait(&bar[st], phase[st])) ok = false;
-            phase[st] ^= 1u;
-            pending[st] = false;
-        }
-        unsigned char *ahi = buf + st * STAGE, *alo = ahi + tc::A_BYTES, *bhi = alo + tc::A_BYTES,
-                      *blo = bhi + B_BYTES;
-        // A: 128 rows x 8 chunks; upper tiles as stored, lower tiles transposed, missing rows zero
-#pragma unroll
-        for (int it = 0; it < (tc::M * 8) / tc::THREADS; ++it) {
-            const int q = tid + it * tc::THREADS;
-            const int qq = q >> 8, I = I0 + qq;       // warp-uniform
-            const float *tsrc = reinterpret_cast<const float *>(src + qq * (TILE * TILE * 4));
-            int rr, c;
-            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (I < tn && J >= I) {
-                rr = (q >> 3) & 31;
-                c = q & 7;
-                v = *reinterpret_cast<const float4 *>(tsrc + rr * TILE + 4 * c);
-            } else {
-                rr = q & 31;
-                c = (q >> 5) & 7;
-                if (I < tn) {
-                    v.x = tsrc[(4 * c + 0) * TILE + rr];
-                    v.y = tsrc[(4 * c + 1) * TILE + rr];
-                    v.z = tsrc[(4 * c + 2) * TILE + rr];
-                    v.w = tsrc[(4 * c + 3) * TILE + rr];
+
+    if (warp == 1) {
+        // ---------------- producer ----------------
+        if (lane == 0) {
+            const unsigned long long pol = policy_evict_first();
+            int next = atomicAdd(&B.queue[0], 1);
+            long long k = 0;            // steps issued
+            for (;;) {
+                const int u = next;
+                const bool end = u >= nunits;
+                int m = 0, I0 = 0, tn = 1, n = 0, voff = 0;
+                long long t0 = 0;
+                if (!end) {
+                    next = atomicAdd(&B.queue[0], 1);
+                    m = units[u].x;
+                    I0 = 4 * units[u].y;
+                    tn = ts.mat_tn[m];
+                    n = ts.mat_n[m];
+                    voff = ts.mat_voff[m];
+                    t0 = ts.mat_tile0[m];
                 }
+                for (int J = 0; J < (end ? 1 : tn); ++J, ++k) {
+                    const int r = (int)(k % tc::RAW);
+                    if (k >= tc::RAW && !W.wait(&empty[r], (unsigned)(((k / tc::RAW) - 1) & 1))) break;
+                    meta[r][0] = end ? -1 : u;
+                    meta[r][1] = J;
+                    meta[r][2] = n;
+                    meta[r][3] = voff;
+                    meta[r][4] = tn;
+                    meta[r][5] = I0;
+                    if (end) {
+                        mbar_arrive(&full[r]);
+                        continue;
+                    }
+                    unsigned char *dst = raw + (size_t)r * RSLOT;
+                    int nval = 0;
+                    for (int q = 0; q < 4; ++q)
+                        if (I0 + q < tn) ++nval;
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    mbar_arrive_tx(&full[r], (unsigned)nval * (TILE * TILE * 4) + XB);
+                    for (int q = 0; q < 4; ++q) {
+                        const int I = I0 + q;
+                        if (I >= tn) continue;
+                        const int a = J >= I ? I : J, b = J >= I ? J : I;
+                        const long long tid_ = t0 + (long long)a * tn - (long long)a * (a - 1) / 2 + (b - a);
+                        bulk_g2s(dst + q * (TILE * TILE * 4), tiles + (size_t)tid_ * (TILE * TILE), TILE * TILE * 4,
+                                 &full[r], pol);
+                    }
+                    asm volatile(
+                        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                            smem_u32(dst + 4 * TILE * TILE * 4)),
+                        "l"(x32 + (size_t)(voff + TILE * J) * NR), "r"(XB), "r"(smem_u32(&full[r]))
+                        : "memory");
+                }
+                if (end || s_abort) break;
             }
-            tc::split_store(ahi, alo, tc::swz(qq * 32 + rr, c), v);
+            // drain: the copies of the last RAW steps have landed (bounded, also after an abort)
+            for (long long q = (k > tc::RAW ? k - tc::RAW : 0); q < k; ++q)
+                mbar_wait(&full[q % tc::RAW], (unsigned)((q / tc::RAW) & 1));
         }
-        // B: NR rows (right-hand sides) x 8 chunks; x rows past the subdomain are zero
-        if (tid < NR * 8) {
-            const int nn = tid % NR, c = tid / NR;
-            const float *xs = reinterpret_cast<const float *>(src + 4 * TILE * TILE * 4);
-            const int r0 = TILE * J + 4 * c;
-            float4 v;
-            v.x = (r0 + 0 < n) ? xs[(4 * c + 0) * NR + nn] : 0.f;
-            v.y = (r0 + 1 < n) ? xs[(4 * c + 1) * NR + nn] : 0.f;
-            v.z = (r0 + 2 < n) ? xs[(4 * c + 2) * NR + nn] : 0.f;
-            v.w = (r0 + 3 < n) ? xs[(4 * c + 3) * NR + nn] : 0.f;
-            tc::split_store(bhi, blo, tc::swz(nn, c), v);
+        __syncwarp();
+    } else if (warp == 0) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0) {
+            constexpr uint32_t ID = tc::idesc<NR>();
+            long long k = 0;          // staged blocks consumed
+            int units_done = 0;
+            for (;;) {
+                const int st = (int)(k % tc::NST);
+                if (!W.wait(&staged[st], (unsigned)((k / tc::NST) & 1))) break;
+                const int u = smeta[st][0], J = smeta[st][1], tn = smeta[st][2];
+                if (u < 0) break;
+                const int acc = units_done & 1;
+                // the epilogue of the unit two back has read this accumulator
+                if (J == 0 && units_done >= 2 && !W.wait(&acc_empty[acc], (unsigned)(((units_done >> 1) - 1) & 1)))
+                    break;
+                tc::fence_after();
+                unsigned char *ahi = buf + st * STAGE, *alo = ahi + tc::A_BYTES, *bhi = alo + tc::A_BYTES,
+                              *blo = bhi + B_BYTES;
+                const unsigned a_hi = smem_u32(ahi), a_lo = smem_u32(alo), b_hi = smem_u32(bhi), b_lo = smem_u32(blo);
+                const unsigned d = tmem + 32u * acc;
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk) {
+                    const unsigned off = 32u * kk;
+                    tc::mma(d, tc::sdesc(a_hi + off), tc::sdesc(b_hi + off), ID, (J > 0 || kk > 0) ? 1u : 0u);
+                    tc::mma(d, tc::sdesc(a_hi + off), tc::sdesc(b_lo + off), ID, 1u);
+                    tc::mma(d, tc::sdesc(a_lo + off), tc::sdesc(b_hi + off), ID, 1u);
+                }
+                tc::commit(&done[st]);                 // the stage is free once these MMAs are done
+                if (J + 1 == tn) {
+                    tc::commit(&acc_full[acc]);        // the unit's accumulator is complete
+                    ++units_done;
+                }
+                ++k;
+            }
+            // drain: the last commit tracks every MMA issued before it
+            if (k > 0) mbar_wait(&done[(k - 1) % tc::NST], (unsigned)(((k - 1) / tc::NST) & 1));
         }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (tid == 0) {
+        __syncwarp();
+    } else {
+        // ---------------- converters and epilogue ----------------
+        const int cw = warp - 2, ct = tid - 64;
+        long long k = 0;
+        int units_done = 0;
+        for (;;) {
+            const int r = (int)(k % tc::RAW), st = (int)(k % tc::NST);
+            if (!W.wait(&full[r], (unsigned)((k / tc::RAW) & 1))) break;
+            // the MMAs of this stage's previous use are done (and have read its metadata)
+            if (k >= tc::NST && !W.wait(&done[st], (unsigned)(((k / tc::NST) - 1) & 1))) break;
+            const int u = meta[r][0];
+            if (u < 0) {
+                if (cw == 0 && lane == 0) smeta[st][0] = -1;
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&staged[st]);
+                break;
+            }
+            const int J = meta[r][1], n = meta[r][2], voff = meta[r][3], tn = meta[r][4], I0 = meta[r][5];
+            const unsigned char *src = raw + (size_t)r * RSLOT;
+            unsigned char *ahi = buf + st * STAGE, *alo = ahi + tc::A_BYTES, *bhi = alo + tc::A_BYTES,
+                          *blo = bhi + B_BYTES;
+#pragma unroll
+            for (int it = 0; it < (tc::M * 8) / CT; ++it) {
+                const int q = ct + it * CT;
+                const int qq = q >> 8, I = I0 + qq;       // warp-uniform
+                const float *tsrc = reinterpret_cast<const float *>(src + qq * (TILE * TILE * 4));
+                int rr, c;
+                float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (I < tn && J >= I) {
+                    rr = (q >> 3) & 31;
+                    c = q & 7;
+                    v = *reinterpret_cast<const float4 *>(tsrc + rr * TILE + 4 * c);
+                } else {
+                    rr = q & 31;
+                    c = (q >> 5) & 7;
+                    if (I < tn) {
+                        v.x = tsrc[(4 * c + 0) * TILE + rr];
+                        v.y = tsrc[(4 * c + 1) * TILE + rr];
+                        v.z = tsrc[(4 * c + 2) * TILE + rr];
+                        v.w = tsrc[(4 * c + 3) * TILE + rr];
+                    }
+                }
+                tc::split_store(ahi, alo, tc::swz(qq * 32 + rr, c), v);
+            }
+            if (ct < NR * 8) {
+                const int nn = ct % NR, c = ct / NR;
+                const float *xs = reinterpret_cast<const float *>(src + 4 * TILE * TILE * 4);
+                const int r0 = TILE * J + 4 * c;
+                float4 v;
+                v.x = (r0 + 0 < n) ? xs[(4 * c + 0) * NR + nn] : 0.f;
+                v.y = (r0 + 1 < n) ? xs[(4 * c + 1) * NR + nn] : 0.f;
+                v.z = (r0 + 2 < n) ? xs[(4 * c + 2) * NR + nn] : 0.f;
+                v.w = (r0 + 3 < n) ? xs[(4 * c + 3) * NR + nn] : 0.f;
+                tc::split_store(bhi, blo, tc::swz(nn, c), v);
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) {
+                if (cw == 0) {
+                    smeta[st][0] = u;
+                    smeta[st][1] = J;
+                    smeta[st][2] = tn;
+                }
+                mbar_arrive(&staged[st]);
+                mbar_arrive(&empty[r]);
+            }
+            ++k;
+            if (J + 1 < tn) continue;
+            // epilogue: lane quadrant (warp % 4), column half (converter warp / 4)
+            const int acc = units_done & 1;
+            ++units_done;
+            if (!W.wait(&acc_full[acc], (unsigned)(((units_done - 1) >> 1) & 1))) break;
             tc::fence_after();
-            const unsigned a_hi = smem_u32(ahi), a_lo = smem_u32(alo), b_hi = smem_u32(bhi), b_lo = smem_u32(blo);
+            const int qd = warp & 3, h = cw >> 2;
+            uint32_t rv[16];
+            const unsigned taddr = tmem + 32u * acc + ((unsigned)(32 * qd) << 16) + (unsigned)(h * HALF);
+            if (HALF == 16) tc::ld16(taddr, rv);
+            else if (HALF == 8) tc::ld8(taddr, rv);
+            else tc::ld4(taddr, rv);
+            tc::fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acc_empty[acc]);
+            const int row = TILE * I0 + 32 * qd + lane;
+            const int c0 = h * HALF;
 #pragma unroll
-            for (int kk = 0; kk < 4; ++kk) {
-                const unsigned off = 32u * kk;
-                tc::mma(tmem, tc::sdesc(a_hi + off), tc::sdesc(b_hi + off), ID, (J > 0 || kk > 0) ? 1u : 0u);
-                tc::mma(tmem, tc::sdesc(a_hi + off), tc::sdesc(b_lo + off), ID, 1u);
-                tc::mma(tmem, tc::sdesc(a_lo + off), tc::sdesc(b_hi + off), ID, 1u);
+            for (int c = 0; c < HALF; ++c) {
+                double dl = 0.0;
+                if (row < n) {
+                    const size_t o = (size_t)(voff + row) * NR + c0 + c;
+                    const double y = (double)__uint_as_float(rv[c]);
+                    out[o] = y;
+                    dl = (double)x32[o] * y;
+                }
+#pragma unroll
+                for (int o = 16; o >= 1; o >>= 1) dl += __shfl_xor_sync(FULL, dl, o);
+                // four quadrant partials per unit and column, summed by the last CTA
+                if (lane == 0) B.unit_dot[((size_t)u * 4 + qd) * NR + c0 + c] = dl;
             }
-            tc::commit(&bar[st]);
-        }
-        pending[st] = true;
-        ++seq;
-        if (J + 1 < tn) continue;
-        // last block of the unit: the commit tracks every MMA issued before it
-        if (!mbar_wait(&bar[st], phase[st])) ok = false;
-        phase[st] ^= 1u;
-        pending[st] = false;
-        tc::fence_after();
-        // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31, columns (w / 4) * HALF .. +HALF-1
-        uint32_t rv[16];
-        const unsigned taddr = tmem + ((unsigned)(32 * (warp & 3)) << 16) + (unsigned)((warp >> 2) * HALF);
-        if (HALF == 16) tc::ld16(taddr, rv);
-        else if (HALF == 8) tc::ld8(taddr, rv);
-        else tc::ld4(taddr, rv);
-        const int row = TILE * I0 + 32 * (warp & 3) + lane;
-        const int c0 = (warp >> 2) * HALF;
-        double dl[HALF];
-#pragma unroll
-        for (int c = 0; c < HALF; ++c) {
-            dl[c] = 0.0;
-            if (row < n && ok) {
-                const size_t o = (size_t)(voff + row) * NR + c0 + c;
-                const double y = (double)__uint_as_float(rv[c]);
-                out[o] = y;
-                dl[c] = (double)x32[o] * y;
-            }
-        }
-#pragma unroll
-        for (int c = 0; c < HALF; ++c) {
-            double v = dl[c];
-#pragma unroll
-            for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
-            if (lane == 0) s_dot[warp][c] = v;
-        }
-        tc::fence_before();
-        __syncthreads();
-        if (tid < NR) {
-            const int h = tid / HALF, c = tid % HALF;
-            double t = 0.0;
-            for (int w = 0; w < 4; ++w) t += s_dot[4 * h + w][c];
-            B.unit_dot[(size_t)u * NR + tid] = t;
         }
     }
-    // drain: every issued copy and every MMA has landed before the CTA leaves
-    if (tid == tc::PRODUCER)
-        for (long long k = step; k < issued; ++k)
-            if (!mbar_wait(&full[k % tc::RAW], (unsigned)((k / tc::RAW) & 1))) ok = false;
-    for (int stg = 0; stg < tc::NST; ++stg)
-        if (pending[stg]) {
-            if (!mbar_wait(&bar[stg], phase[stg])) ok = false;
-            pending[stg] = false;
-        }
-    if (!ok) s_err = 1;
     tc::fence_before();
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
     __shared__ int s_last;
     if (tid == 0) {
-        if (s_err) atomicExch(&P.st->error, 1);
+        if (s_abort) atomicExch(&P.st->error, 1);
         __threadfence();
         s_last = (atomicAdd(&B.queue[1], 1) == (int)gridDim.x - 1);
     }
@@ -3440,7 +3470,7 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
             __threadfence();
             if (tid < NR) {
                 double t = 0.0;
-                for (int q = 0; q < nunits; ++q) t += __ldcg(&B.unit_dot[(size_t)q * NR + tid]);
+                for (int q = 0; q < 4 * nunits; ++q) t += __ldcg(&B.unit_dot[(size_t)q * NR + tid]);
                 B.scal[SC_PAP * NR + tid] = t;
             }
         }
@@ -3687,7 +3717,8 @@ void GpuSolver::Impl::ensure_block(int nr) {
         for (int I4 = 0; 4 * I4 < tn[m]; ++I4) units4.push_back(make_int2(m, I4));
     blk.units4 = upload(units4);
     blk.nunits4 = (int)units4.size();
-    B.unit_dot = alloc<double>(std::max(units.size(), units4.size()) * nr);
+    // CUDA-core SYMM: one dot per unit and column; tensor-core SYMM: four lane-quadrant partials
+    B.unit_dot = alloc<double>(std::max(units.size(), 4 * units4.size()) * nr);
     blk.rhs = alloc<double>((size_t)std::max(1, n_caller) * nr);
     blk.sol = alloc<double>((size_t)std::max(1, n_caller) * nr);
     blk.f = alloc<double>((size_t)ntot * nr);
@@ -3754,7 +3785,7 @@ static void symm_tc_launch(int nsm, int nunits, cudaStream_t st, TileSetDev td, 
     }
     // one CTA per SM (the raw ring and the stages fill its shared memory)
     const int grid = std::max(1, std::min(nunits, nsm));
-    tile_symm_tc_kernel<NR><<<grid, tc::THREADS, sm, st>>>(td, P, B, x32, out, units, nunits, slot, mode);
+    tile_symm_tc_kernel<NR><<<grid, tc::WS_THREADS, sm, st>>>(td, P, B, x32, out, units, nunits, slot, mode);
 }
 
 void GpuSolver::Impl::launch_symm(const TileSetHost &T, bool src32, const double *x64, const float *x32, double *out,
