@@ -3194,6 +3194,9 @@ constexpr int RAW = 4;        // raw slots
 constexpr int NST = 3;        // MMA operand stages
 constexpr int CONV = 8;       // converter warps
 constexpr int WS_THREADS = 32 * (2 + CONV);
+// independent accumulation chains per unit: the three products hi*hi, hi*lo, lo*hi, each split
+// over even and odd K steps; dependent MMAs on one accumulator serialise, independent ones overlap
+constexpr int NCH = 6;
 }
 
 struct TcAbort {
@@ -3236,7 +3239,7 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
     const unsigned base = smem_u32(tc_smem);
     unsigned char *buf = tc_smem + ((1024u - (base & 1023u)) & 1023u);   // 1024-byte aligned stages
     unsigned char *raw = buf + tc::NST * STAGE;
-    const unsigned ncols = 64;                                            // two accumulators of 32 columns
+    const unsigned ncols = 512;                    // two units x NCH accumulators of 32 columns (384 used)
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
                      "r"(ncols)
@@ -3336,13 +3339,15 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
                 unsigned char *ahi = buf + st * STAGE, *alo = ahi + tc::A_BYTES, *bhi = alo + tc::A_BYTES,
                               *blo = bhi + B_BYTES;
                 const unsigned a_hi = smem_u32(ahi), a_lo = smem_u32(alo), b_hi = smem_u32(bhi), b_lo = smem_u32(blo);
-                const unsigned d = tmem + 32u * acc;
+                const unsigned d = tmem + 32u * tc::NCH * acc;
 #pragma unroll
                 for (int kk = 0; kk < 4; ++kk) {
                     const unsigned off = 32u * kk;
-                    tc::mma(d, tc::sdesc(a_hi + off), tc::sdesc(b_hi + off), ID, (J > 0 || kk > 0) ? 1u : 0u);
-                    tc::mma(d, tc::sdesc(a_hi + off), tc::sdesc(b_lo + off), ID, 1u);
-                    tc::mma(d, tc::sdesc(a_lo + off), tc::sdesc(b_hi + off), ID, 1u);
+                    const unsigned first = (J > 0 || kk > 1) ? 1u : 0u;   // first MMA of each chain overwrites
+                    const unsigned dc = d + 32u * (kk & 1);
+                    tc::mma(dc, tc::sdesc(a_hi + off), tc::sdesc(b_hi + off), ID, first);
+                    tc::mma(dc + 64u, tc::sdesc(a_hi + off), tc::sdesc(b_lo + off), ID, first);
+                    tc::mma(dc + 128u, tc::sdesc(a_lo + off), tc::sdesc(b_hi + off), ID, first);
                 }
                 tc::commit(&done[st]);                 // the stage is free once these MMAs are done
                 if (J + 1 == tn) {
@@ -3429,11 +3434,20 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
             if (!W.wait(&acc_full[acc], (unsigned)(((units_done - 1) >> 1) & 1))) break;
             tc::fence_after();
             const int qd = warp & 3, h = cw >> 2;
-            uint32_t rv[16];
-            const unsigned taddr = tmem + 32u * acc + ((unsigned)(32 * qd) << 16) + (unsigned)(h * HALF);
-            if (HALF == 16) tc::ld16(taddr, rv);
-            else if (HALF == 8) tc::ld8(taddr, rv);
-            else tc::ld4(taddr, rv);
+            float ysum[16];
+#pragma unroll
+            for (int c = 0; c < 16; ++c) ysum[c] = 0.f;
+            // chains in the order hi*hi (even, odd K), hi*lo, lo*hi: the small terms are added last
+#pragma unroll
+            for (int ch = 0; ch < tc::NCH; ++ch) {
+                uint32_t rv[16];
+                const unsigned taddr = tmem + 32u * (tc::NCH * acc + ch) + ((unsigned)(32 * qd) << 16) + (unsigned)(h * HALF);
+                if (HALF == 16) tc::ld16(taddr, rv);
+                else if (HALF == 8) tc::ld8(taddr, rv);
+                else tc::ld4(taddr, rv);
+#pragma unroll
+                for (int c = 0; c < HALF; ++c) ysum[c] += __uint_as_float(rv[c]);
+            }
             tc::fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&acc_empty[acc]);
@@ -3444,7 +3458,7 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
                 double dl = 0.0;
                 if (row < n) {
                     const size_t o = (size_t)(voff + row) * NR + c0 + c;
-                    const double y = (double)__uint_as_float(rv[c]);
+                    const double y = (double)ysum[c];
                     out[o] = y;
                     dl = (double)x32[o] * y;
                 }
