@@ -3181,56 +3181,19 @@ __device__ __forceinline__ void ld8(unsigned taddr, uint32_t (&r)[16]) {
 }
 }  // namespace tc
 
-// Warp-specialised pipeline (no CTA-wide barrier inside the loop):
-//   warp 0      issues the MMAs (one lane) and owns the tensor memory;
-//   warp 1      issues the cp.async.bulk copies of raw tiles and x blocks into a RAW-slot ring;
-//   warps 2..9  convert a raw slot into a swizzled TF32 hi/lo MMA stage, and run the epilogue
-//               of a finished unit (tcgen05.ld by lane quadrant, two accumulators alternate).
-// Hand-overs are mbarriers: full/empty (raw ring), staged/done (MMA stages), acc_full/acc_empty
-// (accumulators).  Every wait is bounded and gives up at once after any other wait timed out;
-// the copies and MMAs in flight are drained (bounded) before the tensor memory is released.
-namespace tc {
-constexpr int RAW = 4;        // raw slots
-constexpr int NST = 3;        // MMA operand stages
-constexpr int CONV = 8;       // converter warps
-constexpr int WS_THREADS = 32 * (2 + CONV);
-// independent accumulation chains per unit: the three products hi*hi, hi*lo, lo*hi, each split
-// over even and odd K steps; dependent MMAs on one accumulator serialise, independent ones overlap
-constexpr int NCH = 6;
-}
-
-struct TcAbort {
-    int *flag;
-    __device__ bool wait(unsigned long long *bar, unsigned parity) const {
-        for (long long i = 0; i < WAIT_LIMIT; ++i) {
-            if (mbar_try(bar, parity)) return true;
-            if (*(volatile int *)flag) return false;
-            if (i > 64) __nanosleep(64);
-        }
-        atomicExch(flag, 1);
-        return false;
-    }
-};
-
 template <int NR>
-__global__ void __launch_bounds__(tc::WS_THREADS, 1)
+__global__ void __launch_bounds__(tc::THREADS, 2)
 tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, double *out, const int2 *units,
                     int nunits, int slot, int mode) {
     static_assert(NR == 8 || NR == 16 || NR == 32, "tensor-core SYMM: 8, 16 or 32 right-hand sides");
     constexpr unsigned B_BYTES = NR * 128;
     constexpr unsigned STAGE = 2 * tc::A_BYTES + 2 * B_BYTES;
-    constexpr unsigned XB = TILE * NR * 4;                 // x block: 32 rows x NR FP32
-    constexpr unsigned RSLOT = 4 * TILE * TILE * 4 + XB;   // four raw tiles + x block
-    constexpr int HALF = NR / 2;
-    constexpr int CT = 32 * tc::CONV;                      // converter threads
+    constexpr int HALF = NR / 2;                 // columns read back by each warp half
     extern __shared__ unsigned char tc_smem[];
-    __shared__ unsigned long long full[tc::RAW], empty[tc::RAW];
-    __shared__ unsigned long long staged[tc::NST], done[tc::NST];
-    __shared__ unsigned long long acc_full[2], acc_empty[2];
-    __shared__ int meta[tc::RAW][6];                      // unit, J, n, voff, tn, I0 (unit -1: end)
-    __shared__ int smeta[tc::NST][3];                     // unit, J, tn of a staged block (unit -1: end)
+    __shared__ unsigned long long bar[2];
     __shared__ unsigned s_tmem;
-    __shared__ int s_abort;
+    __shared__ int s_unit, s_last, s_err;
+    __shared__ double s_dot[tc::THREADS / 32][NR];
     if (mode != 0) {
         const int iter = P.st->iter_base + slot;
         if (skip_iter(P.st, iter)) return;
@@ -3238,8 +3201,7 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned base = smem_u32(tc_smem);
     unsigned char *buf = tc_smem + ((1024u - (base & 1023u)) & 1023u);   // 1024-byte aligned stages
-    unsigned char *raw = buf + tc::NST * STAGE;
-    const unsigned ncols = 512;                    // two units x NCH accumulators of 32 columns (384 used)
+    const unsigned ncols = 32;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
                      "r"(ncols)
@@ -3247,234 +3209,163 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        for (int r = 0; r < tc::RAW; ++r) { mbar_init(&full[r], 1); mbar_init(&empty[r], tc::CONV); }
-        for (int s = 0; s < tc::NST; ++s) { mbar_init(&staged[s], tc::CONV); mbar_init(&done[s], 1); }
-        for (int a = 0; a < 2; ++a) { mbar_init(&acc_full[a], 1); mbar_init(&acc_empty[a], tc::CONV); }
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        s_abort = 0;
+        s_err = 0;
     }
     tc::fence_before();
     __syncthreads();
     tc::fence_after();
     const unsigned tmem = s_tmem;
-    const TcAbort W{&s_abort};
-    const float *tiles = reinterpret_cast<const float *>(ts.tiles);
-
-    if (warp == 1) {
-        // ---------------- producer ----------------
-        if (lane == 0) {
-            const unsigned long long pol = policy_evict_first();
-            int next = atomicAdd(&B.queue[0], 1);
-            long long k = 0;            // steps issued
-            for (;;) {
-                const int u = next;
-                const bool end = u >= nunits;
-                int m = 0, I0 = 0, tn = 1, n = 0, voff = 0;
-                long long t0 = 0;
-                if (!end) {
-                    next = atomicAdd(&B.queue[0], 1);
-                    m = units[u].x;
-                    I0 = 4 * units[u].y;
-                    tn = ts.mat_tn[m];
-                    n = ts.mat_n[m];
-                    voff = ts.mat_voff[m];
-                    t0 = ts.mat_tile0[m];
-                }
-                for (int J = 0; J < (end ? 1 : tn); ++J, ++k) {
-                    const int r = (int)(k % tc::RAW);
-                    if (k >= tc::RAW && !W.wait(&empty[r], (unsigned)(((k / tc::RAW) - 1) & 1))) break;
-                    meta[r][0] = end ? -1 : u;
-                    meta[r][1] = J;
-                    meta[r][2] = n;
-                    meta[r][3] = voff;
-                    meta[r][4] = tn;
-                    meta[r][5] = I0;
-                    if (end) {
-                        mbar_arrive(&full[r]);
-                        continue;
-                    }
-                    unsigned char *dst = raw + (size_t)r * RSLOT;
-                    int nval = 0;
-                    for (int q = 0; q < 4; ++q)
-                        if (I0 + q < tn) ++nval;
-                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                    mbar_arrive_tx(&full[r], (unsigned)nval * (TILE * TILE * 4) + XB);
-                    for (int q = 0; q < 4; ++q) {
-                        const int I = I0 + q;
-                        if (I >= tn) continue;
-                        const int a = J >= I ? I : J, b = J >= I ? J : I;
-                        const long long tid_ = t0 + (long long)a * tn - (long long)a * (a - 1) / 2 + (b - a);
-                        bulk_g2s(dst + q * (TILE * TILE * 4), tiles + (size_t)tid_ * (TILE * TILE), TILE * TILE * 4,
-                                 &full[r], pol);
-                    }
-                    asm volatile(
-                        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                            smem_u32(dst + 4 * TILE * TILE * 4)),
-                        "l"(x32 + (size_t)(voff + TILE * J) * NR), "r"(XB), "r"(smem_u32(&full[r]))
-                        : "memory");
-                }
-                if (end || s_abort) break;
-            }
-            // drain: the copies of the last RAW steps have landed (bounded, also after an abort)
-            for (long long q = (k > tc::RAW ? k - tc::RAW : 0); q < k; ++q)
-                mbar_wait(&full[q % tc::RAW], (unsigned)((q / tc::RAW) & 1));
-        }
-        __syncwarp();
-    } else if (warp == 0) {
-        // ---------------- MMA issuer ----------------
-        if (lane == 0) {
-            constexpr uint32_t ID = tc::idesc<NR>();
-            long long k = 0;          // staged blocks consumed
-            int units_done = 0;
-            for (;;) {
-                const int st = (int)(k % tc::NST);
-                if (!W.wait(&staged[st], (unsigned)((k / tc::NST) & 1))) break;
-                const int u = smeta[st][0], J = smeta[st][1], tn = smeta[st][2];
-                if (u < 0) break;
-                const int acc = units_done & 1;
-                // the epilogue of the unit two back has read this accumulator
-                if (J == 0 && units_done >= 2 && !W.wait(&acc_empty[acc], (unsigned)(((units_done >> 1) - 1) & 1)))
-                    break;
-                tc::fence_after();
-                unsigned char *ahi = buf + st * STAGE, *alo = ahi + tc::A_BYTES, *bhi = alo + tc::A_BYTES,
-                              *blo = bhi + B_BYTES;
-                const unsigned a_hi = smem_u32(ahi), a_lo = smem_u32(alo), b_hi = smem_u32(bhi), b_lo = smem_u32(blo);
-                const unsigned d = tmem + 32u * tc::NCH * acc;
+    constexpr uint32_t ID = tc::idesc<NR>();
+    unsigned phase[2] = {0u, 0u};
+    bool pending[2] = {false, false};
+    unsigned seq = 0;
+    bool ok = true;
+    for (;;) {
+        if (tid == 0) s_unit = atomicAdd(&B.queue[0], 1);
+        const bool all_ok = __syncthreads_and(ok);   // a timed-out wait stops every thread together
+        const int u = s_unit;
+        if (u >= nunits || !all_ok) break;
+        ok = true;
+        const int m = units[u].x, I0 = 4 * units[u].y;
+        const int n = ts.mat_n[m], voff = ts.mat_voff[m], tn = ts.mat_tn[m];
+        const long long t0 = ts.mat_tile0[m];
+        const float *tiles = reinterpret_cast<const float *>(ts.tiles);
+        // block J of the unit into registers: four 16-byte A chunks and one B chunk per thread;
+        // two register sets keep blocks J+1 and J+2 in flight while block J is staged
+        constexpr int AIT = (tc::M * 8) / tc::THREADS;
+        float4 ra0[AIT], ra1[AIT], rb0 = make_float4(0.f, 0.f, 0.f, 0.f), rb1 = rb0;
+        auto load_block = [&](int J, float4 (&ra)[AIT], float4 &rb) {
 #pragma unroll
-                for (int kk = 0; kk < 4; ++kk) {
-                    const unsigned off = 32u * kk;
-                    const unsigned first = (J > 0 || kk > 1) ? 1u : 0u;   // first MMA of each chain overwrites
-                    const unsigned dc = d + 32u * (kk & 1);
-                    tc::mma(dc, tc::sdesc(a_hi + off), tc::sdesc(b_hi + off), ID, first);
-                    tc::mma(dc + 64u, tc::sdesc(a_hi + off), tc::sdesc(b_lo + off), ID, first);
-                    tc::mma(dc + 128u, tc::sdesc(a_lo + off), tc::sdesc(b_hi + off), ID, first);
+            for (int it = 0; it < AIT; ++it) {
+                const int q = tid + it * tc::THREADS;
+                const int qq = q >> 8, I = I0 + qq;       // warp-uniform
+                ra[it] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (I < tn && J >= I) {
+                    const int rr = (q >> 3) & 31, c = q & 7;
+                    const long long tid_ = t0 + (long long)I * tn - (long long)I * (I - 1) / 2 + (J - I);
+                    const uint4 u4 =
+                        ld_stream(reinterpret_cast<const uint4 *>(tiles + (size_t)tid_ * (TILE * TILE) + rr * TILE + 4 * c));
+                    ra[it] = make_float4(__uint_as_float(u4.x), __uint_as_float(u4.y), __uint_as_float(u4.z),
+                                         __uint_as_float(u4.w));
+                } else if (I < tn) {
+                    const int rr = q & 31, c = (q >> 5) & 7;
+                    const long long tid_ = t0 + (long long)J * tn - (long long)J * (J - 1) / 2 + (I - J);
+                    const float *tp = tiles + (size_t)tid_ * (TILE * TILE) + rr;
+                    ra[it].x = tp[(4 * c + 0) * TILE];
+                    ra[it].y = tp[(4 * c + 1) * TILE];
+                    ra[it].z = tp[(4 * c + 2) * TILE];
+                    ra[it].w = tp[(4 * c + 3) * TILE];
                 }
-                tc::commit(&done[st]);                 // the stage is free once these MMAs are done
-                if (J + 1 == tn) {
-                    tc::commit(&acc_full[acc]);        // the unit's accumulator is complete
-                    ++units_done;
-                }
-                ++k;
             }
-            // drain: the last commit tracks every MMA issued before it
-            if (k > 0) mbar_wait(&done[(k - 1) % tc::NST], (unsigned)(((k - 1) / tc::NST) & 1));
-        }
-        __syncwarp();
-    } else {
-        // ---------------- converters and epilogue ----------------
-        const int cw = warp - 2, ct = tid - 64;
-        long long k = 0;
-        int units_done = 0;
-        for (;;) {
-            const int r = (int)(k % tc::RAW), st = (int)(k % tc::NST);
-            if (!W.wait(&full[r], (unsigned)((k / tc::RAW) & 1))) break;
-            // the MMAs of this stage's previous use are done (and have read its metadata)
-            if (k >= tc::NST && !W.wait(&done[st], (unsigned)(((k / tc::NST) - 1) & 1))) break;
-            const int u = meta[r][0];
-            if (u < 0) {
-                if (cw == 0 && lane == 0) smeta[st][0] = -1;
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&staged[st]);
-                break;
+            if (tid < NR * 8) {
+                const int nn = tid % NR, c = tid / NR;
+                const int r0 = TILE * J + 4 * c;
+                rb.x = (r0 + 0 < n) ? x32[(size_t)(voff + r0 + 0) * NR + nn] : 0.f;
+                rb.y = (r0 + 1 < n) ? x32[(size_t)(voff + r0 + 1) * NR + nn] : 0.f;
+                rb.z = (r0 + 2 < n) ? x32[(size_t)(voff + r0 + 2) * NR + nn] : 0.f;
+                rb.w = (r0 + 3 < n) ? x32[(size_t)(voff + r0 + 3) * NR + nn] : 0.f;
             }
-            const int J = meta[r][1], n = meta[r][2], voff = meta[r][3], tn = meta[r][4], I0 = meta[r][5];
-            const unsigned char *src = raw + (size_t)r * RSLOT;
+        };
+        auto step = [&](int J, float4 (&ra)[AIT], float4 &rb) {
+            const int st = seq & 1;
+            if (pending[st]) {
+                if (!mbar_wait(&bar[st], phase[st])) ok = false;
+                phase[st] ^= 1u;
+                pending[st] = false;
+            }
             unsigned char *ahi = buf + st * STAGE, *alo = ahi + tc::A_BYTES, *bhi = alo + tc::A_BYTES,
                           *blo = bhi + B_BYTES;
 #pragma unroll
-            for (int it = 0; it < (tc::M * 8) / CT; ++it) {
-                const int q = ct + it * CT;
-                const int qq = q >> 8, I = I0 + qq;       // warp-uniform
-                const float *tsrc = reinterpret_cast<const float *>(src + qq * (TILE * TILE * 4));
-                int rr, c;
-                float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (I < tn && J >= I) {
-                    rr = (q >> 3) & 31;
-                    c = q & 7;
-                    v = *reinterpret_cast<const float4 *>(tsrc + rr * TILE + 4 * c);
-                } else {
-                    rr = q & 31;
-                    c = (q >> 5) & 7;
-                    if (I < tn) {
-                        v.x = tsrc[(4 * c + 0) * TILE + rr];
-                        v.y = tsrc[(4 * c + 1) * TILE + rr];
-                        v.z = tsrc[(4 * c + 2) * TILE + rr];
-                        v.w = tsrc[(4 * c + 3) * TILE + rr];
-                    }
-                }
-                tc::split_store(ahi, alo, tc::swz(qq * 32 + rr, c), v);
+            for (int it = 0; it < AIT; ++it) {
+                const int q = tid + it * tc::THREADS;
+                const int qq = q >> 8, I = I0 + qq;
+                const bool up = (I < tn && J >= I);
+                const int rr = up ? ((q >> 3) & 31) : (q & 31), c = up ? (q & 7) : ((q >> 5) & 7);
+                tc::split_store(ahi, alo, tc::swz(qq * 32 + rr, c), ra[it]);
             }
-            if (ct < NR * 8) {
-                const int nn = ct % NR, c = ct / NR;
-                const float *xs = reinterpret_cast<const float *>(src + 4 * TILE * TILE * 4);
-                const int r0 = TILE * J + 4 * c;
-                float4 v;
-                v.x = (r0 + 0 < n) ? xs[(4 * c + 0) * NR + nn] : 0.f;
-                v.y = (r0 + 1 < n) ? xs[(4 * c + 1) * NR + nn] : 0.f;
-                v.z = (r0 + 2 < n) ? xs[(4 * c + 2) * NR + nn] : 0.f;
-                v.w = (r0 + 3 < n) ? xs[(4 * c + 3) * NR + nn] : 0.f;
-                tc::split_store(bhi, blo, tc::swz(nn, c), v);
-            }
+            if (tid < NR * 8) tc::split_store(bhi, blo, tc::swz(tid % NR, tid / NR), rb);
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            __syncwarp();
-            if (lane == 0) {
-                if (cw == 0) {
-                    smeta[st][0] = u;
-                    smeta[st][1] = J;
-                    smeta[st][2] = tn;
+            __syncthreads();
+            if (tid == 0) {
+                tc::fence_after();
+                const unsigned a_hi = smem_u32(ahi), a_lo = smem_u32(alo), b_hi = smem_u32(bhi), b_lo = smem_u32(blo);
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk) {
+                    const unsigned off = 32u * kk;
+                    tc::mma(tmem, tc::sdesc(a_hi + off), tc::sdesc(b_hi + off), ID, (J > 0 || kk > 0) ? 1u : 0u);
+                    tc::mma(tmem, tc::sdesc(a_hi + off), tc::sdesc(b_lo + off), ID, 1u);
+                    tc::mma(tmem, tc::sdesc(a_lo + off), tc::sdesc(b_hi + off), ID, 1u);
                 }
-                mbar_arrive(&staged[st]);
-                mbar_arrive(&empty[r]);
+                tc::commit(&bar[st]);
             }
-            ++k;
-            if (J + 1 < tn) continue;
-            // epilogue: lane quadrant (warp % 4), column half (converter warp / 4)
-            const int acc = units_done & 1;
-            ++units_done;
-            if (!W.wait(&acc_full[acc], (unsigned)(((units_done - 1) >> 1) & 1))) break;
-            tc::fence_after();
-            const int qd = warp & 3, h = cw >> 2;
-            float ysum[16];
+            pending[st] = true;
+            ++seq;
+            if (J + 2 < tn) load_block(J + 2, ra, rb);   // in flight while blocks J and J+1 are processed
+        };
+        load_block(0, ra0, rb0);
+        if (tn > 1) load_block(1, ra1, rb1);
+        for (int J = 0; J < tn; J += 2) {
+            step(J, ra0, rb0);
+            if (J + 1 < tn) step(J + 1, ra1, rb1);
+        }
+        // the last commit tracks every MMA issued before it: the accumulator is complete
+        {
+            const int lst = (seq - 1) & 1;
+            if (!mbar_wait(&bar[lst], phase[lst])) ok = false;
+            phase[lst] ^= 1u;
+            pending[lst] = false;
+        }
+        tc::fence_after();
+        // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31, columns (w / 4) * HALF .. +HALF-1
+        uint32_t r[16];
+        const unsigned taddr = tmem + ((unsigned)(32 * (warp & 3)) << 16) + (unsigned)((warp >> 2) * HALF);
+        if (HALF == 16) tc::ld16(taddr, r);
+        else if (HALF == 8) tc::ld8(taddr, r);
+        else tc::ld4(taddr, r);
+        const int row = TILE * I0 + 32 * (warp & 3) + lane;
+        const int c0 = (warp >> 2) * HALF;
+        double dl[HALF];
 #pragma unroll
-            for (int c = 0; c < 16; ++c) ysum[c] = 0.f;
-            // chains in the order hi*hi (even, odd K), hi*lo, lo*hi: the small terms are added last
-#pragma unroll
-            for (int ch = 0; ch < tc::NCH; ++ch) {
-                uint32_t rv[16];
-                const unsigned taddr = tmem + 32u * (tc::NCH * acc + ch) + ((unsigned)(32 * qd) << 16) + (unsigned)(h * HALF);
-                if (HALF == 16) tc::ld16(taddr, rv);
-                else if (HALF == 8) tc::ld8(taddr, rv);
-                else tc::ld4(taddr, rv);
-#pragma unroll
-                for (int c = 0; c < HALF; ++c) ysum[c] += __uint_as_float(rv[c]);
-            }
-            tc::fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&acc_empty[acc]);
-            const int row = TILE * I0 + 32 * qd + lane;
-            const int c0 = h * HALF;
-#pragma unroll
-            for (int c = 0; c < HALF; ++c) {
-                double dl = 0.0;
-                if (row < n) {
-                    const size_t o = (size_t)(voff + row) * NR + c0 + c;
-                    const double y = (double)ysum[c];
-                    out[o] = y;
-                    dl = (double)x32[o] * y;
-                }
-#pragma unroll
-                for (int o = 16; o >= 1; o >>= 1) dl += __shfl_xor_sync(FULL, dl, o);
-                // four quadrant partials per unit and column, summed by the last CTA
-                if (lane == 0) B.unit_dot[((size_t)u * 4 + qd) * NR + c0 + c] = dl;
+        for (int c = 0; c < HALF; ++c) {
+            dl[c] = 0.0;
+            if (row < n && ok) {
+                const size_t o = (size_t)(voff + row) * NR + c0 + c;
+                const double y = (double)__uint_as_float(r[c]);
+                out[o] = y;
+                dl[c] = (double)x32[o] * y;
             }
         }
+#pragma unroll
+        for (int c = 0; c < HALF; ++c) {
+            double v = dl[c];
+#pragma unroll
+            for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+            if (lane == 0) s_dot[warp][c] = v;
+        }
+        tc::fence_before();
+        __syncthreads();
+        if (tid < NR) {
+            const int h = tid / HALF, c = tid % HALF;
+            double t = 0.0;
+            for (int w = 0; w < 4; ++w) t += s_dot[4 * h + w][c];
+            B.unit_dot[(size_t)u * NR + tid] = t;
+        }
     }
+    // drain: both stages idle before the tensor memory is released
+    for (int stg = 0; stg < 2; ++stg)
+        if (pending[stg]) {
+            if (!mbar_wait(&bar[stg], phase[stg])) ok = false;
+            pending[stg] = false;
+        }
+    if (!ok && lane == 0) s_err = 1;
     tc::fence_before();
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
-    __shared__ int s_last;
+    if (tid == 0 && s_err) atomicExch(&P.st->error, 1);
     if (tid == 0) {
-        if (s_abort) atomicExch(&P.st->error, 1);
         __threadfence();
         s_last = (atomicAdd(&B.queue[1], 1) == (int)gridDim.x - 1);
     }
@@ -3484,7 +3375,7 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
             __threadfence();
             if (tid < NR) {
                 double t = 0.0;
-                for (int q = 0; q < 4 * nunits; ++q) t += __ldcg(&B.unit_dot[(size_t)q * NR + tid]);
+                for (int q = 0; q < nunits; ++q) t += __ldcg(&B.unit_dot[(size_t)q * NR + tid]);
                 B.scal[SC_PAP * NR + tid] = t;
             }
         }
@@ -3695,9 +3586,7 @@ void GpuSolver::Impl::ensure_block(int nr) {
     B.x = alloc<double>((size_t)NL * nr); B.r = alloc<double>((size_t)NL * nr); B.w = alloc<double>((size_t)NL * nr);
     B.z = alloc<double>((size_t)NL * nr); B.y = alloc<double>((size_t)NL * nr); B.p = alloc<double>((size_t)NL * nr);
     B.Ap = alloc<double>((size_t)NL * nr); B.Ax = alloc<double>((size_t)NL * nr); B.bL = alloc<double>((size_t)NL * nr);
-    // 32 rows of padding: the tensor-core SYMM copies whole 32-row x blocks
-    B.p32 = alloc<float>((size_t)(NL + TILE) * nr);
-    CUDA_CHECK(cudaMemset(B.p32, 0, sizeof(float) * (size_t)(NL + TILE) * nr));
+    B.p32 = alloc<float>((size_t)NL * nr);
     B.uT = alloc<double>((size_t)NT * nr); B.vT = alloc<double>((size_t)NT * nr);
     // alpha carries KS zero rows past nK for the fixed-width G^T alpha loads
     B.d = alloc<double>((size_t)P.nP * nr); B.alpha = alloc<double>((size_t)(nK + P.KS) * nr);
@@ -3731,8 +3620,7 @@ void GpuSolver::Impl::ensure_block(int nr) {
         for (int I4 = 0; 4 * I4 < tn[m]; ++I4) units4.push_back(make_int2(m, I4));
     blk.units4 = upload(units4);
     blk.nunits4 = (int)units4.size();
-    // CUDA-core SYMM: one dot per unit and column; tensor-core SYMM: four lane-quadrant partials
-    B.unit_dot = alloc<double>(std::max(units.size(), 4 * units4.size()) * nr);
+    B.unit_dot = alloc<double>(std::max(units.size(), units4.size()) * nr);
     blk.rhs = alloc<double>((size_t)std::max(1, n_caller) * nr);
     blk.sol = alloc<double>((size_t)std::max(1, n_caller) * nr);
     blk.f = alloc<double>((size_t)ntot * nr);
@@ -3789,7 +3677,7 @@ static void symm_launch(int nsm, int ncta, size_t sm, cudaStream_t st, TileSetDe
 template <int NR>
 static void symm_tc_launch(int nsm, int nunits, cudaStream_t st, TileSetDev td, DevProblem P, BlockDev B,
                            const float *x32, double *out, const int2 *units, int slot, int mode) {
-    constexpr size_t sm = tc::NST * (2 * 128 * 128 + 2 * NR * 128) + tc::RAW * (4 * 32 * 32 * 4 + 32 * NR * 4) + 1024;
+    constexpr size_t sm = 2 * (2 * 128 * 128 + 2 * NR * 128) + 1024;
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(tile_symm_tc_kernel<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -3797,9 +3685,10 @@ static void symm_tc_launch(int nsm, int nunits, cudaStream_t st, TileSetDev td, 
                              cudaSharedmemCarveoutMaxShared);
         attr = true;
     }
-    // one CTA per SM (the raw ring and the stages fill its shared memory)
-    const int grid = std::max(1, std::min(nunits, nsm));
-    tile_symm_tc_kernel<NR><<<grid, tc::WS_THREADS, sm, st>>>(td, P, B, x32, out, units, nunits, slot, mode);
+    // two CTAs per SM fit (registers and shared memory); CTAs never wait for one another, so a
+    // CTA that is not co-resident only starts later
+    const int grid = std::max(1, std::min(nunits, nsm * 2));
+    tile_symm_tc_kernel<NR><<<grid, tc::THREADS, sm, st>>>(td, P, B, x32, out, units, nunits, slot, mode);
 }
 
 void GpuSolver::Impl::launch_symm(const TileSetHost &T, bool src32, const double *x64, const float *x32, double *out,
