@@ -194,7 +194,21 @@ __device__ __forceinline__ bool skip_iter(const DevState *st, int iter) {
 }
 
 // (G^T a) at local row e: own coefficients plus the partner's
+template <int KC>
+__device__ __forceinline__ double gt_alpha_fixed(const DevProblem &P, int e, const double *a) {
+    const int ko = P.rkof[e], po = P.pkof[e];
+    const double *g = P.Gl + (size_t)e * KC, *gp = P.Gp + (size_t)e * KC;
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < KC; ++k) s += g[k] * a[ko + k] + gp[k] * a[po + k];
+    return s;
+}
+// The common kernel widths 1 (heat) and 6 (elasticity) take fixed-width loads: coefficients
+// zero-padded to KS and the amplitudes padded by KS zero entries, so the loads do not depend
+// on the per-row counts and overlap.
 __device__ __forceinline__ double gt_alpha(const DevProblem &P, int e, const double *a) {
+    if (P.KS == 1) return gt_alpha_fixed<1>(P, e, a);
+    if (P.KS == 6) return gt_alpha_fixed<6>(P, e, a);
     double s = 0.0;
     const int nk = P.rnk[e], ko = P.rkof[e], pn = P.pnk[e], po = P.pkof[e];
     const double *g = P.Gl + (size_t)e * P.KS, *gp = P.Gp + (size_t)e * P.KS;
@@ -2090,7 +2104,9 @@ void GpuSolver::upload(const Decomposition &dec, const Prep &prep, const SolveOp
     P.y = I.alloc<double>(NL); P.p = I.alloc<double>(NL); P.Ap = I.alloc<double>(NL);
     I.Ax64 = I.alloc<double>(NL);
     P.uT = I.alloc<double>(NT); P.vT = I.alloc<double>(NT);
-    P.d = I.alloc<double>(P.nP); P.alpha = I.alloc<double>(prep.n_kern);
+    P.d = I.alloc<double>(P.nP);
+    P.alpha = I.alloc<double>(prep.n_kern + KS);
+    CUDA_CHECK(cudaMemset(P.alpha, 0, sizeof(double) * (prep.n_kern + KS)));
     I.e_dev = I.alloc<double>(P.nP);
     P.part_w = I.alloc<double>(nd); P.part_rho = I.alloc<double>(nd); P.part_b = I.alloc<double>(nd);
     P.rho_hist = I.alloc<double>((size_t)opt.max_iterations + 64);
