@@ -34,7 +34,7 @@ namespace {
 
 constexpr int KMAX = 8;        // kernel dimension bound per subdomain (elasticity: 6)
 constexpr int TPB = 256;       // threads of the per-subdomain kernels
-constexpr int TPB1 = 1024;     // threads of the single right-hand-side per-subdomain PCG kernels
+constexpr int TPB1 = 512;      // threads of the single right-hand-side w/preconditioner kernel
 constexpr int TILE = 32;       // Schur tile edge
 constexpr unsigned FULL = 0xffffffffu;
 
@@ -772,7 +772,7 @@ __global__ void zero2_kernel(double *a, double *b, int n) {
 }
 
 // r = b - assemble(Ax); d = G r per subdomain; ||b||^2 total (initial call).  One CTA per subdomain.
-__global__ void __launch_bounds__(TPB1) r0_kernel(DevProblem P, double *Ax, int replace_mode, int slot) {
+__global__ void r0_kernel(DevProblem P, double *Ax, int replace_mode, int slot) {
     extern __shared__ double rv_s[];
     __shared__ double sh[32 * KMAX];
     if (replace_mode) {
@@ -796,7 +796,7 @@ __global__ void __launch_bounds__(TPB1) r0_kernel(DevProblem P, double *Ax, int 
 }
 
 // ||P r||^2 with alpha = (GG^T)^-1 G r (initial stop tolerance)
-__global__ void __launch_bounds__(TPB1) pnorm_kernel(DevProblem P) {
+__global__ void pnorm_kernel(DevProblem P) {
     __shared__ double sh[32];
     const int dsub = blockIdx.x;
     double s = 0.0;
@@ -869,7 +869,7 @@ __global__ void __launch_bounds__(TPB1) w_prec_kernel(DevProblem P, int slot) {
 }
 
 // z = assemble(W B v_T); d = G z.  One CTA per subdomain.
-__global__ void __launch_bounds__(TPB1) z_kernel(DevProblem P, int slot) {
+__global__ void z_kernel(DevProblem P, int slot) {
     extern __shared__ double zs[];
     __shared__ double sh[32 * KMAX];
     const int iter = P.st->iter_base + slot;
@@ -888,7 +888,7 @@ __global__ void __launch_bounds__(TPB1) z_kernel(DevProblem P, int slot) {
 }
 
 // y = z - G^T alpha, rho = y.w total; clear the F apply accumulators.
-__global__ void __launch_bounds__(TPB1) y_kernel(DevProblem P, double *Ax64, int slot) {
+__global__ void y_kernel(DevProblem P, double *Ax64, int slot) {
     __shared__ double sh[32];
     const int iter = P.st->iter_base + slot;
     if (skip_iter(P.st, iter)) return;
@@ -911,7 +911,7 @@ __global__ void zero_vT_kernel(DevProblem P, int slot) {
 }
 
 // p = y + beta p, x += alpha p, r -= alpha assemble(Ap), d = G r, convergence check.
-__global__ void __launch_bounds__(TPB1) update_kernel(DevProblem P, int slot) {
+__global__ void update_kernel(DevProblem P, int slot) {
     extern __shared__ double rs_s[];
     __shared__ double sh[32 * KMAX];
     const int iter = P.st->iter_base + slot;
@@ -1885,7 +1885,7 @@ void GpuSolver::Impl::launch_iteration(int slot) {
         // residual replacement r = b - F64 x when the previous update asked for it
         launch_tiles(F64, 3, P.x, nullptr, Ax64, slot);
         launch_hybrid_F(P.x, Ax64, slot, 3, nullptr);
-        r0_kernel<<<nd, TPB1, sizeof(double) * max_ni, stream>>>(P, Ax64, 1, slot);
+        r0_kernel<<<nd, TPB, sizeof(double) * max_ni, stream>>>(P, Ax64, 1, slot);
     }
     coarse_kernel<<<cgrid, 256, 0, stream>>>(P, P.d, P.alpha, slot, 1);
     const size_t tsm = sizeof(double) * (size_t)(max_ni + max_nt);
@@ -1900,15 +1900,15 @@ void GpuSolver::Impl::launch_iteration(int slot) {
             zero_vT_kernel<<<std::max(1, std::min(1024, (P.NT + 255) / 256)), 256, 0, stream>>>(P, slot);
             launch_tiles(Dir, 2, P.uT, nullptr, P.vT, slot);
         }
-        z_kernel<<<nd, TPB1, sizeof(double) * max_ni, stream>>>(P, slot);
+        z_kernel<<<nd, TPB, sizeof(double) * max_ni, stream>>>(P, slot);
         coarse_kernel<<<cgrid, 256, 0, stream>>>(P, P.d, P.alpha, slot, 1);
-        y_kernel<<<nd, TPB1, 0, stream>>>(P, Ax64, slot);
+        y_kernel<<<nd, TPB, 0, stream>>>(P, Ax64, slot);
     } else {
         zero2_kernel<<<(P.NL + 255) / 256, 256, 0, stream>>>(P.Ap, Ax64, P.NL);
     }
     launch_tiles(Fop, 1, P.y, P.p, P.Ap, slot);
     launch_hybrid_F(nullptr, P.Ap, slot, 1, P.scal + SC_PAP);   // p = y + beta p formed on the fly
-    update_kernel<<<nd, TPB1, sizeof(double) * max_ni, stream>>>(P, slot);
+    update_kernel<<<nd, TPB, sizeof(double) * max_ni, stream>>>(P, slot);
     CUDA_CHECK(cudaGetLastError());
 }
 
@@ -2245,10 +2245,10 @@ void GpuSolver::solve(SolveStats &stats) {
     zero_kernel<<<(P.NL + 255) / 256, 256, 0, I.stream>>>(P.p, P.NL);
     I.launch_tiles(I.F64, 0, P.x, nullptr, I.Ax64, 0);
     I.launch_hybrid_F(P.x, I.Ax64, 0, 0, nullptr);
-    r0_kernel<<<nd, TPB1, sizeof(double) * I.max_ni, I.stream>>>(P, I.Ax64, 0, 0);
+    r0_kernel<<<nd, TPB, sizeof(double) * I.max_ni, I.stream>>>(P, I.Ax64, 0, 0);
     zero_kernel<<<(P.NL + 255) / 256, 256, 0, I.stream>>>(I.Ax64, P.NL);
     coarse_kernel<<<cgrid, 256, 0, I.stream>>>(P, P.d, P.alpha, 0, 0);
-    pnorm_kernel<<<nd, TPB1, 0, I.stream>>>(P);
+    pnorm_kernel<<<nd, TPB, 0, I.stream>>>(P);
     tol_kernel<<<1, 256, 0, I.stream>>>(P);
     CUDA_CHECK(cudaGetLastError());
     int launches = 9;
