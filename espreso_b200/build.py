@@ -20,8 +20,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 HOST_FLAGS = "-fPIC,-fopenmp,-march=x86-64-v3,-O3,-Wall,-Wno-unused-function"
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", HOST_FLAGS, "-I", os.path.join(ROOT, "include")]
 
-SOURCES = ["dense.cpp", "decompose.cpp", "prep.cpp", "hybrid.cpp", "feti4i.cpp", "gpu_solver.cu"]
-HEADERS = ["common.h", "dense.h", "decompose.h", "prep.h", "gpu_solver.h"]
+SOURCES = ["dense.cpp", "decompose.cpp", "prep.cpp", "hybrid.cpp", "feti4i.cpp", "gpu_solver.cu", "gpu_prep.cu"]
+HEADERS = ["common.h", "dense.h", "decompose.h", "prep.h", "gpu_solver.h", "gpu_prep.h", "hybrid.h"]
 
 
 def _newer(target, deps):

@@ -1,0 +1,726 @@
+// Batched FP64 partial Cholesky of the augmented subdomain matrices [K_reg B~^T; B~ 0] on sm_100a.
+//
+// One batch holds the dense matrices of many subdomains (column-major, lower triangle used,
+// leading dimension padded to 32 rows).  Per elimination step every subdomain of the batch that
+// still has columns in the current phase contributes one "item" (panel columns [k0, k0+w), rows
+// [k0, rend)), and three launches process all items of the step together:
+//   diag_kernel    one CTA per item: Cholesky of the w x w diagonal block in shared memory;
+//   trsm_kernel    one CTA per 64-row block below it: L_ik = A_ik L_kk^-T;
+//   update_kernel  one CTA per 64 x 64 lower tile of the trailing block: A_IJ -= L_Ik L_Jk^T.
+// Phases: untouched columns (rows of K only: the B~ rows are zero there and stay zero), touched
+// columns (B~ rows included), fix columns after the host's regularisation of the fix-DOF block.
+#include "gpu_prep.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+
+#include "common.h"
+
+#define PCHECK(x)                                                                                  \
+    do {                                                                                           \
+        cudaError_t e_ = (x);                                                                      \
+        if (e_ != cudaSuccess)                                                                     \
+            throw ::feti::Error(std::string("CUDA error ") + cudaGetErrorString(e_) + " in " #x); \
+    } while (0)
+
+namespace feti {
+
+namespace {
+
+constexpr int NB = 64;    // panel width and tile edge
+constexpr int PT = 256;   // threads per CTA
+
+struct SubD {
+    long long a;          // offset of the dense matrix in the arena (doubles)
+    int ld;               // leading dimension
+    int n, N;             // columns eliminated (DOFs of K), rows (n + ni)
+};
+
+struct Item {
+    int sub, k0, w, rend; // panel [k0, k0+w), rows [k0, rend)
+    int trs0, upd0;       // first CTA of this item in the trsm / update grid
+};
+
+struct ElemD {
+    long long val;        // offset of K_e in the batch value buffer
+    int nd;               // element DOFs
+    int pos;              // offset of its factor positions in the batch position buffer
+    int sub;              // batch-local subdomain
+};
+
+struct JobD {
+    int sub, n, n1, nc, ni, ns;
+    long long boff;       // offset of its B~ rows in bpos / bsign
+    long long lp, s, sd;  // offsets of its outputs in the staging buffer (doubles)
+    long long fx;         // offset of its fix-DOF block in the fix buffer
+};
+
+// item whose first CTA is the largest one <= b (items with no CTAs share the next item's start)
+template <int WHICH>
+__device__ __forceinline__ int find_item(const Item *it, int n, int b) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        const int v = WHICH == 0 ? it[mid].trs0 : it[mid].upd0;
+        if (v <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// ---------------------------------------------------------------------------------------------
+// assembly and set-up
+
+// Scatter-add of the element matrices of one colour into the lower triangles (elements of one
+// colour share no DOF, so no two CTAs add into the same entry and the sums are deterministic).
+__global__ void assemble_kernel(const ElemD *els, const int *list, int count, const double *vals, const int *epos,
+                                const SubD *subs, double *arena) {
+    for (int e = blockIdx.x; e < count; e += gridDim.x) {
+        const ElemD E = els[list[e]];
+        const SubD sd = subs[E.sub];
+        double *A = arena + sd.a;
+        const int nd = E.nd;
+        for (int q = threadIdx.x; q < nd * nd; q += blockDim.x) {
+            const int a = q / nd, c = q - a * nd;
+            const int pa = epos[E.pos + a], pc = epos[E.pos + c];
+            if (pa >= pc) A[(size_t)pc * sd.ld + pa] += vals[E.val + q];
+        }
+    }
+}
+
+// B~ rows below K: row n + r holds sign_r at the factor column of the row's DOF.
+__global__ void brows_kernel(const JobD *jobs, const SubD *subs, const int *bpos, const double *bsign, double *arena) {
+    const JobD J = jobs[blockIdx.y];
+    const SubD sd = subs[J.sub];
+    double *A = arena + sd.a;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < J.ni; r += gridDim.x * blockDim.x)
+        A[(size_t)bpos[J.boff + r] * sd.ld + J.n + r] = bsign[J.boff + r];
+}
+
+// Partial sums of ||K||_F^2 from the lower triangle (off-diagonal entries counted twice).
+__global__ void knorm_kernel(const JobD *jobs, const SubD *subs, const double *arena, double *part) {
+    const JobD J = jobs[blockIdx.y];
+    const SubD sd = subs[J.sub];
+    const double *A = arena + sd.a;
+    const long long tot = (long long)J.n * J.n;
+    double s = 0.0;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(q / J.n), i = (int)(q - (long long)j * J.n);
+        if (i >= j) {
+            const double v = A[(size_t)j * sd.ld + i];
+            s += (i > j ? 2.0 : 1.0) * v * v;
+        }
+    }
+    __shared__ double red[PT / 32];
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < PT / 32; ++w) t += red[w];
+        part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = t;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// elimination step
+
+// Cholesky of the w x w diagonal block of every item; a non-positive pivot is recorded (first
+// column per subdomain) and replaced by 1 so that the elimination stays finite.
+__global__ void __launch_bounds__(PT) diag_kernel(const Item *items, const SubD *subs, double *arena, int *fail) {
+    __shared__ double D[NB][NB + 1];
+    __shared__ int s_bad;
+    const Item it = items[blockIdx.x];
+    const SubD sd = subs[it.sub];
+    double *A = arena + sd.a;
+    const size_t ld = sd.ld;
+    const int k0 = it.k0, w = it.w, tid = threadIdx.x;
+    for (int q = tid; q < w * w; q += PT) {
+        const int i = q % w, j = q / w;
+        if (i >= j) D[i][j] = A[(size_t)(k0 + j) * ld + k0 + i];
+    }
+    if (tid == 0) s_bad = -1;
+    __syncthreads();
+    for (int j = 0; j < w; ++j) {
+        if (tid == 0) {
+            double d = D[j][j];
+            if (!(d > 0.0)) {
+                if (s_bad < 0) s_bad = j;
+                d = 1.0;
+            }
+            D[j][j] = sqrt(d);
+        }
+        __syncthreads();
+        const double piv = D[j][j];
+        for (int i = j + 1 + tid; i < w; i += PT) D[i][j] /= piv;
+        __syncthreads();
+        const int m = w - j - 1;
+        for (int q = tid; q < m * m; q += PT) {
+            const int i = j + 1 + q % m, c = j + 1 + q / m;
+            if (i >= c) D[i][c] -= D[i][j] * D[c][j];
+        }
+        __syncthreads();
+    }
+    if (tid == 0 && s_bad >= 0) atomicMin(&fail[it.sub], k0 + s_bad);
+    for (int q = tid; q < w * w; q += PT) {
+        const int i = q % w, j = q / w;
+        if (i >= j) A[(size_t)(k0 + j) * ld + k0 + i] = D[i][j];
+    }
+}
+
+// Row blocks below the diagonal block: P := P L_kk^-T, column by column.
+__global__ void __launch_bounds__(PT) trsm_kernel(const Item *items, int nitems, const SubD *subs, double *arena) {
+    extern __shared__ double tsm[];
+    double(*D)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(tsm);
+    double(*P)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(tsm + NB * (NB + 1));
+    const int b = blockIdx.x, tid = threadIdx.x;
+    const Item it = items[find_item<0>(items, nitems, b)];
+    const SubD sd = subs[it.sub];
+    double *A = arena + sd.a;
+    const size_t ld = sd.ld;
+    const int k0 = it.k0, w = it.w;
+    const int row0 = k0 + w + NB * (b - it.trs0);
+    const int rows = min(NB, it.rend - row0);
+    for (int q = tid; q < w * w; q += PT) {
+        const int i = q % w, j = q / w;
+        if (i >= j) D[i][j] = A[(size_t)(k0 + j) * ld + k0 + i];
+    }
+    for (int q = tid; q < NB * w; q += PT) {
+        const int r = q % NB, j = q / NB;
+        if (r < rows) P[r][j] = A[(size_t)(k0 + j) * ld + row0 + r];
+    }
+    __syncthreads();
+    for (int j = 0; j < w; ++j) {
+        if (tid < rows) P[tid][j] /= D[j][j];
+        __syncthreads();
+        const int m = w - j - 1;
+        for (int q = tid; q < NB * m; q += PT) {
+            const int r = q % NB, c = j + 1 + q / NB;
+            if (r < rows) P[r][c] -= P[r][j] * D[c][j];
+        }
+        __syncthreads();
+    }
+    for (int q = tid; q < NB * w; q += PT) {
+        const int r = q % NB, j = q / NB;
+        if (r < rows) A[(size_t)(k0 + j) * ld + row0 + r] = P[r][j];
+    }
+}
+
+// Trailing update of the lower tiles: A_IJ -= L_I L_J^T (w-deep), 4 x 4 outputs per thread.
+__global__ void __launch_bounds__(PT) update_kernel(const Item *items, int nitems, const SubD *subs, double *arena) {
+    extern __shared__ double usm[];
+    double *LI = usm, *LJ = usm + NB * NB;
+    const int b = blockIdx.x, tid = threadIdx.x;
+    const Item it = items[find_item<1>(items, nitems, b)];
+    const SubD sd = subs[it.sub];
+    double *A = arena + sd.a;
+    const size_t ld = sd.ld;
+    const int t = b - it.upd0;
+    int I = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while ((I + 1) * (I + 2) / 2 <= t) ++I;
+    while (I * (I + 1) / 2 > t) --I;
+    const int J = t - I * (I + 1) / 2;
+    const int k0 = it.k0, w = it.w;
+    const int r0 = k0 + w;
+    const int rI = r0 + NB * I, rJ = r0 + NB * J;
+    const int nI = min(NB, it.rend - rI), nJ = min(NB, it.rend - rJ);
+    for (int q = tid; q < NB * w; q += PT) {
+        const int i = q % NB, k = q / NB;
+        const double *col = A + (size_t)(k0 + k) * ld;
+        LI[k * NB + i] = i < nI ? col[rI + i] : 0.0;
+        LJ[k * NB + i] = i < nJ ? col[rJ + i] : 0.0;
+    }
+    __syncthreads();
+    const int tx = tid & 15, ty = tid >> 4;
+    double acc[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = 0.0;
+    for (int k = 0; k < w; ++k) {
+        double a[4], c[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            a[u] = LI[k * NB + tx + 16 * u];
+            c[u] = LJ[k * NB + ty + 16 * u];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) acc[u][v] = fma(a[u], c[v], acc[u][v]);
+    }
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        const int j = ty + 16 * v;
+        if (j >= nJ) continue;
+        double *col = A + (size_t)(rJ + j) * ld + rI;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int i = tx + 16 * u;
+            if (i < nI && (I != J || i >= j)) col[i] -= acc[u][v];
+        }
+    }
+}
+
+// The same update on the FP64 tensor-core path (mma.m8n8k4.f64): eight warps, each a 32 x 16
+// block of the tile as 4 x 2 fragments of 8 x 8.  Panels are staged k-major with a stride of 72
+// doubles (8 mod 16), so the 8 x 4 fragment loads take the minimum of two shared-memory wavefronts.
+constexpr int LDS = 72;
+
+__device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(c[0]), "+d"(c[1])
+                 : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(PT) update_mma_kernel(const Item *items, int nitems, const SubD *subs,
+                                                        double *arena) {
+    extern __shared__ double msm[];
+    double *LI = msm, *LJ = msm + NB * LDS;
+    const int b = blockIdx.x, tid = threadIdx.x;
+    const Item it = items[find_item<1>(items, nitems, b)];
+    const SubD sd = subs[it.sub];
+    double *A = arena + sd.a;
+    const size_t ld = sd.ld;
+    const int t = b - it.upd0;
+    int I = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while ((I + 1) * (I + 2) / 2 <= t) ++I;
+    while (I * (I + 1) / 2 > t) --I;
+    const int J = t - I * (I + 1) / 2;
+    const int k0 = it.k0, w = it.w, w4 = (it.w + 3) & ~3;
+    const int r0 = k0 + w;
+    const int rI = r0 + NB * I, rJ = r0 + NB * J;
+    const int nI = min(NB, it.rend - rI), nJ = min(NB, it.rend - rJ);
+    for (int q = tid; q < NB * w4; q += PT) {
+        const int i = q % NB, k = q / NB;
+        const double *col = A + (size_t)(k0 + k) * ld;
+        const bool kin = k < w;
+        LI[k * LDS + i] = (kin && i < nI) ? col[rI + i] : 0.0;
+        LJ[k * LDS + i] = (kin && i < nJ) ? col[rJ + i] : 0.0;
+    }
+    __syncthreads();
+    const int lane = tid & 31, warp = tid >> 5;
+    const int wm = warp & 1, wn = warp >> 1;
+    const int g = lane >> 2, q4 = lane & 3;
+    double acc[4][2][2];
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+#pragma unroll
+        for (int n = 0; n < 2; ++n) acc[m][n][0] = acc[m][n][1] = 0.0;
+    for (int k = 0; k < w4; k += 4) {
+        const double *la = LI + (k + q4) * LDS + wm * 32 + g;
+        const double *lb = LJ + (k + q4) * LDS + wn * 16 + g;
+        double a[4], c[2];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) a[m] = la[m * 8];
+#pragma unroll
+        for (int n = 0; n < 2; ++n) c[n] = lb[n * 8];
+#pragma unroll
+        for (int m = 0; m < 4; ++m)
+#pragma unroll
+            for (int n = 0; n < 2; ++n) dmma(acc[m][n], a[m], c[n]);
+    }
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        const int r = wm * 32 + m * 8 + g;
+#pragma unroll
+        for (int n = 0; n < 2; ++n)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int c = wn * 16 + n * 8 + 2 * q4 + h;
+                if (r < nI && c < nJ && (I != J || r >= c)) A[(size_t)(rJ + c) * ld + rI + r] -= acc[m][n][h];
+            }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// extraction
+
+// dst (m x m, column-major, full) = scale * symmetric block at (r0, r0) read from the lower triangle
+__global__ void copy_sym_kernel(const JobD *jobs, const SubD *subs, const double *arena, double *dst, int which,
+                                double scale) {
+    const JobD J = jobs[blockIdx.y];
+    const SubD sd = subs[J.sub];
+    const double *A = arena + sd.a;
+    int r0, m;
+    long long off;
+    if (which == 0) { r0 = J.n; m = J.ni; off = J.s; }                  // -S
+    else if (which == 1) { r0 = J.n1; m = J.n - J.n1; off = J.sd; }     // Dirichlet Schur complement
+    else { r0 = J.nc; m = J.ns; off = J.fx; }                           // fix-DOF block
+    if (off < 0) return;
+    const long long tot = (long long)m * m;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(q / m), i = (int)(q - (long long)j * m);
+        const double v = i >= j ? A[(size_t)(r0 + j) * sd.ld + r0 + i] : A[(size_t)(r0 + i) * sd.ld + r0 + j];
+        dst[off + q] = scale * v;
+    }
+}
+
+// packed lower factor of the leading n x n block: column j holds rows j..n-1
+__global__ void pack_kernel(const JobD *jobs, const SubD *subs, const double *arena, double *stage) {
+    const JobD J = jobs[blockIdx.y];
+    const SubD sd = subs[J.sub];
+    const double *A = arena + sd.a;
+    for (int j = blockIdx.x; j < J.n; j += gridDim.x) {
+        const size_t p0 = (size_t)j * J.n - (size_t)j * (j - 1) / 2;
+        const double *col = A + (size_t)j * sd.ld;
+        for (int i = j + threadIdx.x; i < J.n; i += blockDim.x) stage[J.lp + p0 + (i - j)] = col[i];
+    }
+}
+
+// A(nc + i, nc + j) += reg(i, j), i >= j
+__global__ void add_reg_kernel(const JobD *jobs, const SubD *subs, double *arena, const double *reg) {   // reg at J.fx
+    const JobD J = jobs[blockIdx.x];
+    const SubD sd = subs[J.sub];
+    double *A = arena + sd.a;
+    for (int q = threadIdx.x; q < J.ns * J.ns; q += blockDim.x) {
+        const int j = q / J.ns, i = q - j * J.ns;
+        if (i >= j) A[(size_t)(J.nc + j) * sd.ld + J.nc + i] += reg[J.fx + q];
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// host side
+
+template <typename T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    void reserve(size_t m) {
+        if (m <= n) return;
+        if (p) PCHECK(cudaFree(p));
+        p = nullptr;
+        n = 0;
+        PCHECK(cudaMalloc(&p, std::max<size_t>(m, 1) * sizeof(T)));
+        n = m;
+    }
+    void put(const std::vector<T> &v) {
+        reserve(v.size());
+        if (!v.empty()) PCHECK(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    }
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+};
+
+struct Step {
+    std::vector<Item> items;
+    int ntrs = 0, nupd = 0;
+};
+
+// Steps of one phase: columns [lo(job), hi(job)) in NB panels, rows below up to rend(job).
+template <typename Lo, typename Hi, typename Rend>
+std::vector<Step> make_steps(int njobs, Lo lo, Hi hi, Rend rend, double &flops) {
+    std::vector<Step> steps;
+    for (int s = 0;; ++s) {
+        Step st;
+        for (int j = 0; j < njobs; ++j) {
+            const int k0 = lo(j) + s * NB;
+            if (k0 >= hi(j)) continue;
+            Item it;
+            it.sub = j;
+            it.k0 = k0;
+            it.w = std::min(NB, hi(j) - k0);
+            it.rend = rend(j);
+            it.trs0 = st.ntrs;
+            it.upd0 = st.nupd;
+            const int below = it.rend - k0 - it.w;
+            const int nb = below > 0 ? (below + NB - 1) / NB : 0;
+            st.ntrs += nb;
+            st.nupd += nb * (nb + 1) / 2;
+            st.items.push_back(it);
+            const double w = it.w, r = below;
+            flops += w * w * w / 3.0 + r * w * w + r * r * w;
+        }
+        if (st.items.empty()) break;
+        steps.push_back(std::move(st));
+    }
+    return steps;
+}
+
+}  // namespace
+
+void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const RegulariseFn &regularise,
+                   size_t mem_budget, DevFactorTimes *times) {
+    const double t_start = now_s();
+    DevFactorTimes tm;
+    const int nj = (int)jobs.size();
+    if (nj == 0) {
+        if (times) *times = tm;
+        return;
+    }
+    if (mem_budget == 0) {
+        size_t fr = 0, tot = 0;
+        PCHECK(cudaMemGetInfo(&fr, &tot));
+        mem_budget = fr / 2;
+    }
+    PCHECK(cudaFuncSetAttribute(trsm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(2 * NB * (NB + 1) * sizeof(double))));
+    PCHECK(cudaFuncSetAttribute(update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(2 * NB * NB * sizeof(double))));
+    PCHECK(cudaFuncSetAttribute(update_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(2 * NB * LDS * sizeof(double))));
+    const char *simt_env = std::getenv("FETI4I_DEVICE_PREP_SIMT");
+    const bool simt = simt_env && simt_env[0] == '1';
+
+    // per-job sizes and batches
+    struct Sz {
+        int ld, N;
+        size_t a, lp, s, sd, fx, vals, pos;
+    };
+    std::vector<Sz> sz(nj);
+    for (int j = 0; j < nj; ++j) {
+        const DevFactorJob &J = jobs[j];
+        FETI_CHECK(J.n > 0 && J.ns >= 0 && J.n1 >= 0 && J.n1 + J.ns <= J.n, "FETI4I: invalid device factorisation job");
+        Sz &z = sz[j];
+        z.N = J.n + J.ni;
+        z.ld = (z.N + 31) / 32 * 32;
+        z.a = (size_t)z.ld * z.N;
+        z.lp = (size_t)J.n * (J.n + 1) / 2;
+        z.s = (size_t)J.ni * J.ni;
+        z.sd = J.want_sdir ? (size_t)(J.n - J.n1) * (J.n - J.n1) : 0;
+        z.fx = (size_t)J.ns * J.ns;
+        z.vals = 0;
+        for (int k = 0; k < J.nelem; ++k) {
+            const int e = J.elems[k];
+            const size_t nd = (size_t)(el.dof_ptr[e + 1] - el.dof_ptr[e]);
+            z.vals += nd * nd;
+        }
+        z.pos = J.elpos.size();
+    }
+    std::vector<int> bstart{0};
+    {
+        size_t cur = 0;
+        for (int j = 0; j < nj; ++j) {
+            const size_t bytes = 8 * (sz[j].a + sz[j].lp + sz[j].s + sz[j].sd + sz[j].fx + sz[j].vals) + 4 * sz[j].pos;
+            if (j > bstart.back() && cur + bytes > mem_budget) {
+                bstart.push_back(j);
+                cur = 0;
+            }
+            cur += bytes;
+        }
+        bstart.push_back(nj);
+    }
+
+    DevBuf<double> arena, stage, fxb, vals, bsign, reg, part;
+    DevBuf<int> epos, bpos, fail, list;
+    DevBuf<SubD> dsubs;
+    DevBuf<JobD> djobs;
+    DevBuf<ElemD> dels;
+    DevBuf<Item> ditems;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    PCHECK(cudaEventCreate(&ev0));
+    PCHECK(cudaEventCreate(&ev1));
+    struct EvGuard {
+        cudaEvent_t a, b;
+        ~EvGuard() {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+    } evg{ev0, ev1};
+    constexpr int KN_BLOCKS = 64;
+
+    for (size_t bi = 0; bi + 1 < bstart.size(); ++bi) {
+        const int j0 = bstart[bi], j1 = bstart[bi + 1], nb = j1 - j0;
+        // layout of the batch
+        std::vector<SubD> subs(nb);
+        std::vector<JobD> jd(nb);
+        size_t a_tot = 0, st_tot = 0, fx_tot = 0, v_tot = 0, p_tot = 0, b_tot = 0;
+        for (int q = 0; q < nb; ++q) {
+            const DevFactorJob &J = jobs[j0 + q];
+            const Sz &z = sz[j0 + q];
+            subs[q] = SubD{(long long)a_tot, z.ld, J.n, z.N};
+            a_tot += z.a;
+            JobD &d = jd[q];
+            d.sub = q;
+            d.n = J.n;
+            d.n1 = J.n1;
+            d.nc = J.n - J.ns;
+            d.ni = J.ni;
+            d.ns = J.ns;
+            d.boff = (long long)b_tot;
+            b_tot += J.ni;
+            d.lp = (long long)st_tot;
+            st_tot += z.lp;
+            d.s = (long long)st_tot;
+            st_tot += z.s;
+            d.sd = J.want_sdir ? (long long)st_tot : -1;
+            st_tot += z.sd;
+            d.fx = (long long)fx_tot;
+            fx_tot += z.fx;
+            v_tot += z.vals;
+            p_tot += z.pos;
+        }
+        // element data, colour lists, B~ rows
+        std::vector<double> hv;
+        hv.reserve(v_tot);
+        std::vector<int> hp;
+        hp.reserve(p_tot);
+        std::vector<ElemD> he;
+        std::vector<std::vector<int>> colors;
+        std::vector<int> hbp;
+        std::vector<double> hbs;
+        hbp.reserve(b_tot);
+        hbs.reserve(b_tot);
+        for (int q = 0; q < nb; ++q) {
+            const DevFactorJob &J = jobs[j0 + q];
+            FETI_CHECK((int)J.elcolor.size() == J.nelem, "FETI4I: element colours missing");
+            if ((int)colors.size() < J.ncolors) colors.resize(J.ncolors);
+            size_t po = 0;
+            for (int k = 0; k < J.nelem; ++k) {
+                const int e = J.elems[k];
+                const int nd = (int)(el.dof_ptr[e + 1] - el.dof_ptr[e]);
+                ElemD E;
+                E.val = (long long)hv.size();
+                E.nd = nd;
+                E.pos = (int)(hp.size());
+                E.sub = q;
+                const double *Ke = el.vals.data() + el.val_ptr[e];
+                hv.insert(hv.end(), Ke, Ke + (size_t)nd * nd);
+                hp.insert(hp.end(), J.elpos.begin() + po, J.elpos.begin() + po + nd);
+                po += nd;
+                colors[J.elcolor[k]].push_back((int)he.size());
+                he.push_back(E);
+            }
+            FETI_CHECK(po == J.elpos.size(), "FETI4I: element DOF positions do not match the elements");
+            FETI_CHECK((int)J.bpos.size() == J.ni && (int)J.bsign.size() == J.ni, "FETI4I: B rows missing");
+            hbp.insert(hbp.end(), J.bpos.begin(), J.bpos.end());
+            hbs.insert(hbs.end(), J.bsign.begin(), J.bsign.end());
+        }
+        std::vector<int> hl;
+        std::vector<std::pair<int, int>> cl;   // (offset, count) per colour
+        for (auto &c : colors) {
+            cl.emplace_back((int)hl.size(), (int)c.size());
+            hl.insert(hl.end(), c.begin(), c.end());
+        }
+        arena.reserve(a_tot);
+        stage.reserve(st_tot);
+        fxb.reserve(fx_tot);
+        vals.put(hv);
+        epos.put(hp);
+        dels.put(he);
+        list.put(hl);
+        bpos.put(hbp);
+        bsign.put(hbs);
+        dsubs.put(subs);
+        djobs.put(jd);
+        std::vector<int> hf(nb, INT_MAX);
+        fail.put(hf);
+        part.reserve((size_t)nb * KN_BLOCKS);
+
+        // elimination schedule
+        double flops = 0.0;
+        auto jn = [&](int q) { return jobs[j0 + q].n; };
+        auto jn1 = [&](int q) { return jobs[j0 + q].n1; };
+        auto jnc = [&](int q) { return jobs[j0 + q].n - jobs[j0 + q].ns; };
+        auto jN = [&](int q) { return sz[j0 + q].N; };
+        auto zero = [](int) { return 0; };
+        std::vector<Step> ph1 = make_steps(nb, zero, jn1, jn, flops);
+        std::vector<Step> ph2 = make_steps(nb, jn1, jnc, jN, flops);
+        std::vector<Step> ph3 = make_steps(nb, jnc, jn, jN, flops);
+        std::vector<Item> all;
+        auto offsets = [&](std::vector<Step> &ph) {
+            std::vector<size_t> o;
+            for (auto &s : ph) {
+                o.push_back(all.size());
+                all.insert(all.end(), s.items.begin(), s.items.end());
+            }
+            return o;
+        };
+        std::vector<size_t> o1 = offsets(ph1), o2 = offsets(ph2), o3 = offsets(ph3);
+        ditems.put(all);
+        tm.flops += flops;
+
+        PCHECK(cudaEventRecord(ev0));
+        PCHECK(cudaMemset(arena.p, 0, a_tot * sizeof(double)));
+        for (auto &c : cl) {
+            if (c.second == 0) continue;
+            assemble_kernel<<<std::min(c.second, 65535), 128>>>(dels.p, list.p + c.first, c.second, vals.p, epos.p,
+                                                               dsubs.p, arena.p);
+            ++tm.launches;
+        }
+        brows_kernel<<<dim3(8, nb), PT>>>(djobs.p, dsubs.p, bpos.p, bsign.p, arena.p);
+        knorm_kernel<<<dim3(KN_BLOCKS, nb), PT>>>(djobs.p, dsubs.p, arena.p, part.p);
+        tm.launches += 2;
+        PCHECK(cudaGetLastError());
+        auto run = [&](std::vector<Step> &ph, std::vector<size_t> &off) {
+            for (size_t s = 0; s < ph.size(); ++s) {
+                const Item *it = ditems.p + off[s];
+                const int ni = (int)ph[s].items.size();
+                diag_kernel<<<ni, PT>>>(it, dsubs.p, arena.p, fail.p);
+                ++tm.launches;
+                if (ph[s].ntrs > 0) {
+                    trsm_kernel<<<ph[s].ntrs, PT, 2 * NB * (NB + 1) * sizeof(double)>>>(it, ni, dsubs.p, arena.p);
+                    ++tm.launches;
+                }
+                if (ph[s].nupd > 0) {
+                    if (simt)
+                        update_kernel<<<ph[s].nupd, PT, 2 * NB * NB * sizeof(double)>>>(it, ni, dsubs.p, arena.p);
+                    else
+                        update_mma_kernel<<<ph[s].nupd, PT, 2 * NB * LDS * sizeof(double)>>>(it, ni, dsubs.p,
+                                                                                              arena.p);
+                    ++tm.launches;
+                }
+            }
+            PCHECK(cudaGetLastError());
+        };
+        run(ph1, o1);
+        copy_sym_kernel<<<dim3(64, nb), PT>>>(djobs.p, dsubs.p, arena.p, stage.p, 1, 1.0);   // Dirichlet
+        ++tm.launches;
+        run(ph2, o2);
+        copy_sym_kernel<<<dim3(1, nb), PT>>>(djobs.p, dsubs.p, arena.p, fxb.p, 2, 1.0);       // fix block
+        ++tm.launches;
+        PCHECK(cudaGetLastError());
+        PCHECK(cudaEventRecord(ev1));
+        PCHECK(cudaEventSynchronize(ev1));
+        float ms = 0.f;
+        PCHECK(cudaEventElapsedTime(&ms, ev0, ev1));
+        tm.device_ms += ms;
+
+        // host: fix-block regularisation (skipped for subdomains whose elimination already failed)
+        PCHECK(cudaMemcpy(hf.data(), fail.p, nb * sizeof(int), cudaMemcpyDeviceToHost));
+        std::vector<double> hfx(fx_tot), hreg(fx_tot, 0.0);
+        if (fx_tot) PCHECK(cudaMemcpy(hfx.data(), fxb.p, fx_tot * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int q = 0; q < nb; ++q)
+            if (jobs[j0 + q].ns > 0 && hf[q] == INT_MAX) regularise(j0 + q, hfx.data() + jd[q].fx, hreg.data() + jd[q].fx);
+        reg.put(hreg);
+        PCHECK(cudaEventRecord(ev0));
+        add_reg_kernel<<<nb, 64>>>(djobs.p, dsubs.p, arena.p, reg.p);
+        ++tm.launches;
+        run(ph3, o3);
+        copy_sym_kernel<<<dim3(256, nb), PT>>>(djobs.p, dsubs.p, arena.p, stage.p, 0, -1.0);
+        pack_kernel<<<dim3(256, nb), PT>>>(djobs.p, dsubs.p, arena.p, stage.p);
+        tm.launches += 2;
+        PCHECK(cudaGetLastError());
+        PCHECK(cudaEventRecord(ev1));
+        PCHECK(cudaEventSynchronize(ev1));
+        PCHECK(cudaEventElapsedTime(&ms, ev0, ev1));
+        tm.device_ms += ms;
+
+        // results
+        PCHECK(cudaMemcpy(hf.data(), fail.p, nb * sizeof(int), cudaMemcpyDeviceToHost));
+        std::vector<double> hpart((size_t)nb * KN_BLOCKS);
+        PCHECK(cudaMemcpy(hpart.data(), part.p, hpart.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int q = 0; q < nb; ++q) {
+            DevFactorJob &J = jobs[j0 + q];
+            J.fail_col = hf[q] == INT_MAX ? -1 : hf[q];
+            double s = 0.0;
+            for (int k = 0; k < KN_BLOCKS; ++k) s += hpart[(size_t)q * KN_BLOCKS + k];
+            J.knorm = std::sqrt(s);
+            if (J.Lp) PCHECK(cudaMemcpy(J.Lp, stage.p + jd[q].lp, sz[j0 + q].lp * sizeof(double), cudaMemcpyDeviceToHost));
+            if (J.S) PCHECK(cudaMemcpy(J.S, stage.p + jd[q].s, sz[j0 + q].s * sizeof(double), cudaMemcpyDeviceToHost));
+            if (J.want_sdir && J.Sdir)
+                PCHECK(cudaMemcpy(J.Sdir, stage.p + jd[q].sd, sz[j0 + q].sd * sizeof(double), cudaMemcpyDeviceToHost));
+        }
+        ++tm.batches;
+    }
+    tm.total_s = now_s() - t_start;
+    if (times) *times = tm;
+}
+
+}  // namespace feti

@@ -14,6 +14,7 @@
 
 #include "common.h"
 #include "dense.h"
+#include "gpu_prep.h"
 #include "hybrid.h"
 
 namespace feti {
@@ -95,7 +96,40 @@ void SubPrep::kplus(double *x) const {
     for (int i = 0; i < n; ++i) x[i] = y[pos[i]];
 }
 
-static void prep_subdomain(const ElementData &el, const Decomposition &dec, int d, const PrepOptions &opt, SubPrep &S) {
+// Per-subdomain state between the symbolic phase, the numeric factorisation (host or device) and
+// the kernel / G phase.
+struct SubWork {
+    int n1 = 0;                     // untouched DOFs (factor positions 0..n1-1)
+    int ns = 0;                     // fix DOFs (the last ns factor positions)
+    double rho = 0.0;               // largest diagonal entry of K: weight of the regularisation
+    std::vector<int> fixdofs;
+    std::vector<int> eldof;         // device path: factor position of every element DOF
+    std::vector<int> elcolor;       // device path: element colours (one colour shares no node)
+    int ncolors = 0;
+    std::vector<double> Kfix;       // n x ns: columns of K at the fix DOFs, factor-order rows
+    double knorm = 0.0;             // ||K||_F
+    std::vector<double> V;          // ns x ns: eigenvectors of the fix-DOF Schur block
+    int defect = 0;
+};
+
+// Element DOFs of element e as local DOF indices of subdomain d.
+static void element_local_dofs(const ElementData &el, const Decomposition &dec, int d, int e, std::vector<int> &eldof) {
+    const int dpn = dec.dpn;
+    const auto &g2l = dec.g2l[d];
+    const int nd = (int)(el.dof_ptr[e + 1] - el.dof_ptr[e]);
+    eldof.resize(nd);
+    for (int k = 0; k < nd; ++k) {
+        const int dof = el.dofs[el.dof_ptr[e] + k];
+        eldof[k] = dpn * g2l.at(dec.dof_node[dof]) + dec.dof_comp[dof];
+    }
+}
+
+// Symbolic phase: fix nodes, factor order [untouched | touched, not fix | fix], T numbering,
+// K restricted to T (lumped preconditioner), the largest diagonal entry of K.  With `device`
+// also the element DOF positions, element colours and the fix columns of K for the device
+// factorisation.
+static void prep_symbolic(const ElementData &el, const Decomposition &dec, int d, const PrepOptions &opt, SubPrep &S,
+                          SubWork &W, bool device) {
     const DomainRows &D = dec.dom[d];
     const int dpn = dec.dpn;
     const int n = D.ndofs;
@@ -104,7 +138,6 @@ static void prep_subdomain(const ElementData &el, const Decomposition &dec, int 
     S.n = n;
     S.ni = (int)D.lam.size();
 
-    // element local DOFs
     std::vector<std::vector<int>> adj(nn);
     std::vector<int> eldof;
     // touched DOFs and candidate fix nodes
@@ -136,43 +169,40 @@ static void prep_subdomain(const ElementData &el, const Decomposition &dec, int 
     for (auto &v : adj) { std::sort(v.begin(), v.end()); v.erase(std::unique(v.begin(), v.end()), v.end()); }
     S.fix_nodes = choose_fix_nodes(adj, cand);
     std::vector<char> isfix(n, 0);
-    std::vector<int> fixdofs;
+    W.fixdofs.clear();
     for (int a : S.fix_nodes)
-        for (int c = 0; c < dpn; ++c) { isfix[dpn * a + c] = 1; fixdofs.push_back(dpn * a + c); }
-    const int ns = (int)fixdofs.size();
+        for (int c = 0; c < dpn; ++c) { isfix[dpn * a + c] = 1; W.fixdofs.push_back(dpn * a + c); }
+    const int ns = (int)W.fixdofs.size();
+    W.ns = ns;
 
     // factor order: [untouched | touched, not fix | fix]
     S.pos.assign(n, -1);
     int p = 0;
     for (int i = 0; i < n; ++i) if (!touched[i]) S.pos[i] = p++;
     const int n1 = p;
+    W.n1 = n1;
     for (int i = 0; i < n; ++i) if (touched[i] && !isfix[i]) S.pos[i] = p++;
-    for (int i : fixdofs) S.pos[i] = p++;
+    for (int i : W.fixdofs) S.pos[i] = p++;
     S.t = n - n1;
     S.tdof.resize(S.t);
     for (int i = 0; i < n; ++i) if (S.pos[i] >= n1) S.tdof[S.pos[i] - n1] = i;
     S.trow.resize(S.ni);
     for (int r = 0; r < S.ni; ++r) S.trow[r] = S.pos[D.dof[r]] - n1;
 
-    // dense K in factor order and sparse K in T order
-    std::vector<double> A((size_t)n * n, 0.0);
+    // K diagonal, K restricted to T (lumped), device-path element data
     std::vector<double> diag(n, 0.0);
     S.f.assign(n, 0.0);
     std::vector<std::vector<std::pair<int, double>>> KT(S.t);
+    if (device) {
+        W.eldof.clear();
+        W.Kfix.assign((size_t)n * ns, 0.0);
+    }
     for (int e : D.elems) {
-        int nd = (int)(el.dof_ptr[e + 1] - el.dof_ptr[e]);
-        eldof.resize(nd);
-        for (int k = 0; k < nd; ++k) {
-            int dof = el.dofs[el.dof_ptr[e] + k];
-            eldof[k] = dpn * g2l.at(dec.dof_node[dof]) + dec.dof_comp[dof];
-        }
+        element_local_dofs(el, dec, d, e, eldof);
+        const int nd = (int)eldof.size();
         const double *Ke = el.vals.data() + el.val_ptr[e];
         for (int a = 0; a < nd; ++a) {
-            int pa = S.pos[eldof[a]];
-            for (int b = 0; b < nd; ++b) {
-                double v = Ke[(size_t)a * nd + b];
-                A[(size_t)S.pos[eldof[b]] * n + pa] += v;
-            }
+            const int pa = S.pos[eldof[a]];
             diag[eldof[a]] += Ke[(size_t)a * nd + a];
             if (pa >= n1)
                 for (int b = 0; b < nd; ++b) {
@@ -180,7 +210,17 @@ static void prep_subdomain(const ElementData &el, const Decomposition &dec, int 
                     if (pb >= n1) KT[pa - n1].emplace_back(pb - n1, Ke[(size_t)a * nd + b]);
                 }
         }
+        if (device) {
+            for (int a = 0; a < nd; ++a) W.eldof.push_back(S.pos[eldof[a]]);
+            // column pb of K at a fix DOF, row pa (the host path's dense assembly order)
+            for (int a = 0; a < nd; ++a)
+                for (int b = 0; b < nd; ++b) {
+                    const int pb = S.pos[eldof[b]];
+                    if (pb >= n - ns) W.Kfix[(size_t)(pb - (n - ns)) * n + S.pos[eldof[a]]] += Ke[(size_t)a * nd + b];
+                }
+        }
     }
+    W.rho = *std::max_element(diag.begin(), diag.end());
     if (opt.precond == PREC_LUMPED) {
         S.KT_ptr.assign(S.t + 1, 0);
         for (int i = 0; i < S.t; ++i) {
@@ -196,15 +236,76 @@ static void prep_subdomain(const ElementData &el, const Decomposition &dec, int 
             S.KT_ptr[i + 1] = (int)S.KT_col.size();
         }
     }
-    KT.clear();
-    KT.shrink_to_fit();
-    // Frobenius norm of K for the kernel check
+    if (device) {
+        // greedy element colouring: elements of one colour share no node
+        const int ne = (int)D.elems.size();
+        W.elcolor.assign(ne, 0);
+        std::vector<uint64_t> used(nn, 0);
+        W.ncolors = 0;
+        for (int k = 0; k < ne; ++k) {
+            const int e = D.elems[k];
+            uint64_t mask = 0;
+            for (int64_t i = el.node_ptr[e]; i < el.node_ptr[e + 1]; ++i) mask |= used[g2l.at(el.nodes[i])];
+            int c = 0;
+            while (c < 64 && ((mask >> c) & 1u)) ++c;
+            FETI_CHECK(c < 64, "FETI4I: more than 64 element colours in a subdomain");
+            W.elcolor[k] = c;
+            W.ncolors = std::max(W.ncolors, c + 1);
+            for (int64_t i = el.node_ptr[e]; i < el.node_ptr[e + 1]; ++i) used[g2l.at(el.nodes[i])] |= (uint64_t)1 << c;
+        }
+    }
+}
+
+// Kernel detection on the fix-DOF Schur block Sss (ns x ns, full, column-major): defect, the
+// regularisation reg = rho V_k V_k^T over the kernel eigenvectors (ns x ns, column-major).
+static void fix_block(SubPrep &S, SubWork &W, const double *Sss, double *reg) {
+    const int ns = W.ns;
+    std::vector<double> A(Sss, Sss + (size_t)ns * ns), ev(ns);
+    W.V.assign((size_t)ns * ns, 0.0);
+    dense::jacobi_eigen(A.data(), ns, ev.data(), W.V.data());
+    S.ss_eigs = ev;
+    // defect: the last eigenvalue before a jump of more than 1e5 (SparseMatrix.cpp:3657-3661)
+    int defect = 0;
+    double scale = std::fabs(ev[ns - 1]);
+    for (int k = ns - 2; k >= 0; --k)
+        if (std::fabs(ev[k]) < 1e-5 * std::fabs(ev[k + 1])) { defect = k + 1; break; }
+    if (defect == 0 && scale > 0 && std::fabs(ev[0]) < 1e-10 * scale) defect = 1;
+    FETI_CHECK(defect > 0, "FETI4I: subdomain stiffness matrix is not singular (Total FETI expects floating subdomains)");
+    S.nk = defect;
+    W.defect = defect;
+    const std::vector<double> &V = W.V;
+    for (int j = 0; j < ns; ++j)
+        for (int i = 0; i < ns; ++i) {
+            double r = 0.0;
+            for (int k = 0; k < defect; ++k) r += V[(size_t)k * ns + i] * V[(size_t)k * ns + j];
+            reg[(size_t)j * ns + i] = W.rho * r;
+        }
+}
+
+// Host numeric phase: dense K in factor order, partial Cholesky with the fix-block
+// regularisation in between, S_i = B (K_reg^-1)_TT B^T, the packed factor.
+static void prep_numeric_host(const ElementData &el, const Decomposition &dec, int d, const PrepOptions &opt,
+                              SubPrep &S, SubWork &W) {
+    const DomainRows &D = dec.dom[d];
+    const int n = S.n, n1 = W.n1, ns = W.ns;
+    std::vector<int> eldof;
+    std::vector<double> A((size_t)n * n, 0.0);
+    for (int e : D.elems) {
+        element_local_dofs(el, dec, d, e, eldof);
+        const int nd = (int)eldof.size();
+        const double *Ke = el.vals.data() + el.val_ptr[e];
+        for (int a = 0; a < nd; ++a) {
+            const int pa = S.pos[eldof[a]];
+            for (int b = 0; b < nd; ++b) A[(size_t)S.pos[eldof[b]] * n + pa] += Ke[(size_t)a * nd + b];
+        }
+    }
+    // Frobenius norm of K and its columns at the fix DOFs for the kernel check
     double knorm = 0.0;
     for (size_t i = 0; i < A.size(); ++i) knorm += A[i] * A[i];
-    knorm = std::sqrt(knorm);
-    std::vector<double> Kfix((size_t)n * ns);  // original columns of K at the fix DOFs (factor order rows)
+    W.knorm = std::sqrt(knorm);
+    W.Kfix.assign((size_t)n * ns, 0.0);
     for (int j = 0; j < ns; ++j)
-        std::memcpy(&Kfix[(size_t)j * n], &A[(size_t)(n - ns + j) * n], sizeof(double) * n);
+        std::memcpy(&W.Kfix[(size_t)j * n], &A[(size_t)(n - ns + j) * n], sizeof(double) * n);
 
     // 1) eliminate the untouched DOFs: trailing block = Schur complement onto T
     int info = dense::potrf_lower(A.data(), n, n, n1);
@@ -222,44 +323,50 @@ static void prep_subdomain(const ElementData &el, const Decomposition &dec, int 
     double *At = A.data() + (size_t)n1 * n + n1;
     info = dense::potrf_lower(At, S.t, n, S.t - ns);
     FETI_CHECK(info == 0, "FETI4I: fix-node choice does not remove the rigid-body modes of a subdomain");
-    // 3) kernel of the fix-DOF Schur block
+    // 3) kernel of the fix-DOF Schur block, regularisation, last columns
     double *Ass = A.data() + (size_t)(n - ns) * n + (n - ns);
-    std::vector<double> Sss((size_t)ns * ns), ev(ns), V((size_t)ns * ns);
+    std::vector<double> Sss((size_t)ns * ns), reg((size_t)ns * ns);
     for (int j = 0; j < ns; ++j)
         for (int i = 0; i < ns; ++i) Sss[(size_t)j * ns + i] = (i >= j) ? Ass[(size_t)j * n + i] : Ass[(size_t)i * n + j];
-    dense::jacobi_eigen(Sss.data(), ns, ev.data(), V.data());
-    S.ss_eigs = ev;
-    // defect: the last eigenvalue before a jump of more than 1e5 (SparseMatrix.cpp:3657-3661)
-    int defect = 0;
-    double scale = std::fabs(ev[ns - 1]);
-    for (int k = ns - 2; k >= 0; --k)
-        if (std::fabs(ev[k]) < 1e-5 * std::fabs(ev[k + 1])) { defect = k + 1; break; }
-    if (defect == 0 && scale > 0 && std::fabs(ev[0]) < 1e-10 * scale) defect = 1;
-    FETI_CHECK(defect > 0, "FETI4I: subdomain stiffness matrix is not singular (Total FETI expects floating subdomains)");
-    S.nk = defect;
-    double rho = *std::max_element(diag.begin(), diag.end());
+    fix_block(S, W, Sss.data(), reg.data());
     for (int j = 0; j < ns; ++j)
-        for (int i = j; i < ns; ++i) {
-            double r = 0.0;
-            for (int k = 0; k < defect; ++k) r += V[(size_t)k * ns + i] * V[(size_t)k * ns + j];
-            Ass[(size_t)j * n + i] += rho * r;
-        }
+        for (int i = j; i < ns; ++i) Ass[(size_t)j * n + i] += reg[(size_t)j * ns + i];
     info = dense::potrf_lower(Ass, ns, n, ns);
     FETI_CHECK(info == 0, "FETI4I: regularised fix block is not positive definite");
 
-    // 4) kernel R = [-K_rr^-1 K_rs N; N] via the factor: R_r = -L_rr^-T (L_sr^T N)
+    // 4) S_i = B (K_reg^-1)_TT B^T with (K_reg^-1)_TT = W^T W, W = L_TT^-1
+    std::vector<double> Wt((size_t)S.t * S.t, 0.0), KiTT((size_t)S.t * S.t);
+    for (int j = 0; j < S.t; ++j)
+        for (int i = j; i < S.t; ++i) Wt[(size_t)j * S.t + i] = A[(size_t)(n1 + j) * n + n1 + i];
+    dense::trtri_lower(Wt.data(), S.t, S.t);
+    dense::lauum_lower(Wt.data(), S.t, S.t, KiTT.data(), S.t);
+    S.S.assign((size_t)S.ni * S.ni, 0.0);
+    for (int k = 0; k < S.ni; ++k)
+        for (int j = 0; j < S.ni; ++j)
+            S.S[(size_t)k * S.ni + j] = D.sign[j] * D.sign[k] * KiTT[(size_t)S.trow[k] * S.t + S.trow[j]];
+
+    // packed factor (host K^+ solves, device K^+ tiles, kernel below)
+    S.Lp.resize((size_t)n * (n + 1) / 2);
+    dense::pack_lower(A.data(), n, n, S.Lp.data());
+}
+
+// Kernel R = [-K_rr^-1 K_rs N; N] from the packed factor: R_r = -L_rr^-T (L_sr^T N); its check
+// against the fix columns of K; orthonormal columns; G_i = -(B_i R_i)^T.
+static void prep_finish(const Decomposition &dec, int d, SubPrep &S, SubWork &W) {
+    const DomainRows &D = dec.dom[d];
+    const int n = S.n, ns = W.ns, defect = W.defect;
     const int nr = n - ns;
+    const double *Lp = S.Lp.data();
     std::vector<double> Rp((size_t)n * defect, 0.0);
     for (int k = 0; k < defect; ++k) {
         double *x = &Rp[(size_t)k * n];
         for (int s = 0; s < ns; ++s) {
-            double v = V[(size_t)k * ns + s];
+            double v = W.V[(size_t)k * ns + s];
             x[nr + s] = v;
-            const double *Lrow = A.data() + (n - ns + s);  // row (nr+s), column j at Lrow[j*n]
-            for (int j = 0; j < nr; ++j) x[j] += Lrow[(size_t)j * n] * v;
+            for (int j = 0; j < nr; ++j) x[j] += Lp[dense::packed_index(n, nr + s, j)] * v;
         }
         for (int j = nr - 1; j >= 0; --j) {
-            const double *cj = A.data() + (size_t)j * n;
+            const double *cj = Lp + dense::packed_index(n, j, j) - j;   // cj[i] = L(i, j), i >= j
             double s = x[j];
             for (int i = j + 1; i < nr; ++i) s -= cj[i] * x[i];
             x[j] = s / cj[j];
@@ -275,34 +382,110 @@ static void prep_subdomain(const ElementData &el, const Decomposition &dec, int 
         for (int k = 0; k < defect; ++k)
             for (int j = 0; j < ns; ++j) {
                 double s = 0.0;
-                for (int i = 0; i < n; ++i) s += Kfix[(size_t)j * n + i] * Rp[(size_t)k * n + i];
+                for (int i = 0; i < n; ++i) s += W.Kfix[(size_t)j * n + i] * Rp[(size_t)k * n + i];
                 res += s * s;
             }
         double rn = 0.0;
         for (double v : Rp) rn += v * v;
-        S.kernel_residual = std::sqrt(res) / (knorm * std::sqrt(rn));
+        S.kernel_residual = std::sqrt(res) / (W.knorm * std::sqrt(rn));
     }
     orthonormalize(S.R, n, defect);
-
-    // 5) S_i = B (K_reg^-1)_TT B^T with (K_reg^-1)_TT = W^T W, W = L_TT^-1
-    std::vector<double> W((size_t)S.t * S.t, 0.0), KiTT((size_t)S.t * S.t);
-    for (int j = 0; j < S.t; ++j)
-        for (int i = j; i < S.t; ++i) W[(size_t)j * S.t + i] = A[(size_t)(n1 + j) * n + n1 + i];
-    dense::trtri_lower(W.data(), S.t, S.t);
-    dense::lauum_lower(W.data(), S.t, S.t, KiTT.data(), S.t);
-    S.S.assign((size_t)S.ni * S.ni, 0.0);
-    for (int k = 0; k < S.ni; ++k)
-        for (int j = 0; j < S.ni; ++j)
-            S.S[(size_t)k * S.ni + j] = D.sign[j] * D.sign[k] * KiTT[(size_t)S.trow[k] * S.t + S.trow[j]];
 
     // G_i = -(B_i R_i)^T (row-major nk x ni)
     S.G.assign((size_t)defect * S.ni, 0.0);
     for (int k = 0; k < defect; ++k)
         for (int j = 0; j < S.ni; ++j) S.G[(size_t)k * S.ni + j] = -D.sign[j] * S.R[(size_t)k * n + D.dof[j]];
+    W.Kfix.clear();
+    W.Kfix.shrink_to_fit();
+}
 
-    // packed factor for host K^+ solves
-    S.Lp.resize((size_t)n * (n + 1) / 2);
-    dense::pack_lower(A.data(), n, n, S.Lp.data());
+static void prep_subdomain(const ElementData &el, const Decomposition &dec, int d, const PrepOptions &opt, SubPrep &S) {
+    SubWork W;
+    prep_symbolic(el, dec, d, opt, S, W, false);
+    prep_numeric_host(el, dec, d, opt, S, W);
+    prep_finish(dec, d, S, W);
+}
+
+// Device path: symbolic phase on the host threads, every subdomain's elimination and Schur
+// complement on the GPU (gpu_prep.cu), kernels and G on the host threads.
+static void prep_all_device(const ElementData &el, const Decomposition &dec, const PrepOptions &opt,
+                            std::vector<SubPrep> &sub, const std::vector<int> &order, int nthreads,
+                            std::vector<std::string> &errors, DevFactorTimes &dt) {
+    const int nd = dec.ndom;
+    std::vector<SubWork> work(nd);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+    for (int k = 0; k < nd; ++k) {
+        const int d = order[k];
+        try {
+            prep_symbolic(el, dec, d, opt, sub[d], work[d], true);
+        } catch (const std::exception &ex) {
+            errors[d] = ex.what();
+        }
+    }
+    std::vector<int> ids;   // subdomains of the device jobs, largest first
+    for (int k = 0; k < nd; ++k)
+        if (errors[order[k]].empty()) ids.push_back(order[k]);
+    std::vector<DevFactorJob> jobs(ids.size());
+    for (size_t q = 0; q < ids.size(); ++q) {
+        const int d = ids[q];
+        SubPrep &S = sub[d];
+        SubWork &W = work[d];
+        const DomainRows &D = dec.dom[d];
+        DevFactorJob &J = jobs[q];
+        J.n = S.n;
+        J.n1 = W.n1;
+        J.ns = W.ns;
+        J.ni = S.ni;
+        J.elems = D.elems.data();
+        J.nelem = (int)D.elems.size();
+        J.elpos = std::move(W.eldof);
+        J.elcolor = std::move(W.elcolor);
+        J.ncolors = W.ncolors;
+        J.bpos.resize(S.ni);
+        for (int r = 0; r < S.ni; ++r) J.bpos[r] = S.pos[D.dof[r]];
+        J.bsign = D.sign;
+        J.want_sdir = opt.precond == PREC_DIRICHLET;
+        S.Lp.assign((size_t)S.n * (S.n + 1) / 2, 0.0);
+        S.S.assign((size_t)S.ni * S.ni, 0.0);
+        if (J.want_sdir) S.Sdir.assign((size_t)S.t * S.t, 0.0);
+        J.Lp = S.Lp.data();
+        J.S = S.S.data();
+        J.Sdir = J.want_sdir ? S.Sdir.data() : nullptr;
+    }
+    auto reg = [&](int q, const double *Sss, double *r) {
+        const int d = ids[q];
+        try {
+            fix_block(sub[d], work[d], Sss, r);
+        } catch (const std::exception &ex) {
+            errors[d] = ex.what();
+            std::fill(r, r + (size_t)work[d].ns * work[d].ns, 0.0);
+        }
+    };
+    device_factor(el, jobs, reg, opt.device_mem, &dt);
+    for (size_t q = 0; q < ids.size(); ++q) {
+        const int d = ids[q];
+        const DevFactorJob &J = jobs[q];
+        if (J.fail_col >= 0 && errors[d].empty()) {
+            if (J.fail_col < J.n1)
+                errors[d] = "FETI4I: interior block of a subdomain stiffness matrix is not positive definite";
+            else if (J.fail_col < J.n - J.ns)
+                errors[d] = "FETI4I: fix-node choice does not remove the rigid-body modes of a subdomain";
+            else
+                errors[d] = "FETI4I: regularised fix block is not positive definite";
+        }
+        work[d].knorm = J.knorm;
+    }
+    jobs.clear();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+    for (int k = 0; k < (int)ids.size(); ++k) {
+        const int d = ids[k];
+        if (!errors[d].empty()) continue;
+        try {
+            prep_finish(dec, d, sub[d], work[d]);
+        } catch (const std::exception &ex) {
+            errors[d] = ex.what();
+        }
+    }
 }
 
 void preprocess(const ElementData &el, Decomposition &dec, const std::vector<double> &rhs, const PrepOptions &opt,
@@ -332,13 +515,22 @@ void preprocess(const ElementData &el, Decomposition &dec, const std::vector<dou
     std::sort(order.begin(), order.end(), [&](int a, int b) { return dec.dom[a].ndofs > dec.dom[b].ndofs; });
     int nthreads = opt.threads > 0 ? opt.threads : omp_get_max_threads();
     std::vector<std::string> errors(dec.ndom);
+    out.device_prep = opt.device;
+    if (opt.device) {
+        DevFactorTimes dt;
+        prep_all_device(el, dec, opt, out.sub, order, nthreads, errors, dt);
+        out.t_device_factor_ms = dt.device_ms;
+        out.device_factor_flops = dt.flops;
+        out.device_factor_launches = dt.launches;
+    } else {
 #pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
-    for (int k = 0; k < dec.ndom; ++k) {
-        int d = order[k];
-        try {
-            prep_subdomain(el, dec, d, opt, out.sub[d]);
-        } catch (const std::exception &ex) {
-            errors[d] = ex.what();
+        for (int k = 0; k < dec.ndom; ++k) {
+            int d = order[k];
+            try {
+                prep_subdomain(el, dec, d, opt, out.sub[d]);
+            } catch (const std::exception &ex) {
+                errors[d] = ex.what();
+            }
         }
     }
     for (int d = 0; d < dec.ndom; ++d)

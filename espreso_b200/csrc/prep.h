@@ -72,6 +72,10 @@ struct Prep {
     std::vector<int> lam_owner;     // 2 per multiplier: (domain, row) packed as domain*2^20+row? (see owners)
     std::vector<int> own_dom, own_row;  // 2 entries per multiplier, -1 if absent
     double t_factor = 0.0, t_coarse = 0.0;
+    bool device_prep = false;          // eliminations and Schur complements ran on the GPU
+    double t_device_factor_ms = 0.0;   // device time of those eliminations (events)
+    double device_factor_flops = 0.0;
+    int device_factor_launches = 0;
 };
 
 struct PrepOptions {
@@ -81,6 +85,8 @@ struct PrepOptions {
     bool scaling = true;
     bool keep_dirichlet = false;
     int threads = 0;
+    bool device = false;            // subdomain eliminations and S_i on the current CUDA device
+    size_t device_mem = 0;          // bytes for one batch of dense subdomain matrices (0: half the free memory)
 };
 
 // rhs: caller DOF vector (size >= max DOF + 1); split per subdomain by multiplicity.

@@ -22,11 +22,12 @@ PRECISION, REAL_OPTIONS_SIZE = 0, 1
 PREC_NONE, PREC_LUMPED, PREC_WEIGHT, PREC_DIRICHLET = 0, 1, 2, 3
 # extended options (include/feti4i_ext.h)
 EXT_SCHUR_PRECISION, EXT_SCALING, EXT_HOST_ONLY, EXT_TILES_PER_ITEM, EXT_GRAPH_CHUNK, EXT_RELIABLE_DELTA, \
-    EXT_HOST_THREADS, EXT_TILE_KERNEL, EXT_AUTOTUNE, EXT_SYMM_TENSOR = range(10)
+    EXT_HOST_THREADS, EXT_TILE_KERNEL, EXT_AUTOTUNE, EXT_SYMM_TENSOR, EXT_DEVICE_PREP = range(11)
 FP64, FP32, BF16 = 0, 1, 2
 STAT_NAMES = ["iterations", "converged", "dual_size", "kernel_size", "subdomains", "prep_seconds",
               "upload_seconds", "solve_ms", "solve_wall_ms", "fapply_bytes", "replacements",
-              "kernel_launches", "device_bytes", "final_norm", "tolerance", "elements"]
+              "kernel_launches", "device_bytes", "final_norm", "tolerance", "elements", "prep_device_ms",
+              "prep_device_flops"]
 
 EXPORTED = [
     "FETI4ISetDefaultIntegerOptions", "FETI4ISetDefaultRealOptions", "FETI4ICreateStiffnessMatrix",
