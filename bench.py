@@ -57,6 +57,8 @@ def parse():
                     help="adjoint: one forward + backward of the density-to-displacement map (torch.autograd)")
     ap.add_argument("--adjoint-grid", type=int, nargs=2, default=[4, 6], metavar=("DOMAINS", "ELEMENTS"),
                     help="adjoint leg: DOMAINS^3 subdomains of ELEMENTS^3 HEXA8")
+    ap.add_argument("--device-prep", type=int, default=1, choices=[0, 1],
+                    help="subdomain eliminations and Schur complements on the GPU (1) or on the host (0)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -218,7 +220,8 @@ def run_ours(args):
                                        F.EXT_TILE_KERNEL: max(0, args.tile_kernel),
                                        F.EXT_AUTOTUNE: 1 if args.tile_kernel < 0 else 0,
                                        F.EXT_RELIABLE_DELTA: args.delta,
-                                       F.EXT_SYMM_TENSOR: args.symm_tensor},
+                                       F.EXT_SYMM_TENSOR: args.symm_tensor,
+                                       F.EXT_DEVICE_PREP: args.device_prep},
                                   clusters=P.sub_cluster() if args.method == 1 else None)
     setup_s = time.time() - t0
     st0 = inst.stats()
@@ -314,7 +317,11 @@ def run_ours(args):
                    "l2": (f"working set > L2 (Schur tiles {alg / 1e9:.2f} GB per apply, 126 MB L2)" if alg > 126e6
                           else f"working set {alg / 1e6:.0f} MB fits in the 126 MB L2 (no flush)"),
                    "wall_ms_per_step": wall,
-                   "setup_s": setup_s, "host_prep_s": st0["prep_seconds"],
+                   "setup_s": setup_s, "prep_s": st0["prep_seconds"],
+                   "prep": ("device" if args.device_prep else "host"),
+                   "prep_device_ms": st0["prep_device_ms"],
+                   "prep_device_tflops": (st0["prep_device_flops"] / st0["prep_device_ms"] * 1e-9
+                                          if st0["prep_device_ms"] > 0 else None),
                    "tuning": inst.tuning(),
                    "reliable_delta": args.delta},
         "fp64_gpu": {"ms": fp64_ms, "pcg_iterations": int(st64["iterations"]), "speedup_mixed": fp64_ms / step_ms,
@@ -384,7 +391,8 @@ def run_adjoint(args):
     from espreso_b200 import adjoint, problems
     nd, ne = args.adjoint_grid
     P, rho, f = problems.adjoint_cube(domains=(nd, nd, nd), elements=(ne, ne, ne), seed=0)
-    model = adjoint.SIMPModel(P, P.Ke, rhs=f, precision=args.precision, max_it=5000)
+    model = adjoint.SIMPModel(P, P.Ke, rhs=f, precision=args.precision, max_it=5000,
+                              device_prep=bool(args.device_prep))
     q = np.random.default_rng(9).uniform(0.0, 1e10, size=P.ndofs)
     times = []
     for _ in range(args.warmup + args.steps):
@@ -405,8 +413,10 @@ def run_adjoint(args):
             "config": {"workload": f"adjoint_elasticity_{nd}^3x{ne}^3", "subdomains": nd ** 3,
                        "elements": int(P.elem_nodes.shape[0]), "dofs": int(P.ndofs)},
             "forward_ms": fwd, "backward_ms": bwd,
-            "note": "forward includes the host factorisation and Schur assembly of the new densities; "
-                    "backward reuses them (second dual solve + element sensitivity kernel)"}
+            "prep": "device" if args.device_prep else "host",
+            "note": "forward includes the factorisation and Schur assembly of the new densities ("
+                    + ("GPU" if args.device_prep else "host") + "); backward reuses them (second dual solve + "
+                    "element sensitivity kernel)"}
     print(json.dumps(line))
 
 

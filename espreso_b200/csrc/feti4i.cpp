@@ -111,6 +111,7 @@ void build(FETI4IStructInstance *I) {
     FETI_CHECK(io[FETI4I_MAX_ITERATIONS] > 0, "FETI4I: MAX_ITERATIONS must be positive");
     double t0 = now_s();
     I->dec = decompose(I->el, io[FETI4I_SUBDOMAINS], I->dir_idx, I->dir_val);
+    FETI_LOG(2, "FETI4I: decomposition %.3f s\n", now_s() - t0);
     PrepOptions po;
     po.method = io[FETI4I_FETI_METHOD];
     if (po.method == 1 && !I->el.sub_cluster.empty()) {
@@ -501,7 +502,8 @@ void FETI4IGetSubdomainSchur(FETI4IInstance instance, FETI4IInt subdomain, FETI4
         auto *I = check_instance(instance);
         FETI_CHECK(subdomain >= 0 && subdomain < I->dec.ndom, "FETI4I: subdomain index out of range");
         const SubPrep &P = I->prep.sub[subdomain];
-        std::copy(P.S.begin(), P.S.end(), S);
+        if (P.S.empty() && I->gpu) I->gpu->subdomain_schur(subdomain, S);   // device preprocessing
+        else std::copy(P.S.begin(), P.S.end(), S);
     });
 }
 
@@ -547,7 +549,8 @@ void FETI4IApplySubdomainKplus(FETI4IInstance instance, FETI4IInt subdomain, FET
     guarded([&] {
         auto *I = check_instance(instance);
         FETI_CHECK(subdomain >= 0 && subdomain < I->dec.ndom, "FETI4I: subdomain index out of range");
-        I->prep.sub[subdomain].kplus(x);
+        if (I->prep.sub[subdomain].Lp.empty() && I->gpu) I->gpu->subdomain_kplus(subdomain, x);   // device factor
+        else I->prep.sub[subdomain].kplus(x);
     });
 }
 
@@ -555,7 +558,14 @@ void FETI4IGetDualRhs(FETI4IInstance instance, FETI4IReal *b, FETI4IReal *e) {
     guarded([&] {
         auto *I = check_instance(instance);
         std::vector<double> bb, ee;
-        make_rhs_vectors(I->dec, I->prep, bb, ee);
+        if (I->prep.dstore && I->gpu) {   // device preprocessing: K^+ only on the device
+            bb.assign(I->dec.n_lambda, 0.0);
+            ee.assign(I->prep.n_kern, 0.0);
+            I->gpu->dual_rhs(I->rhs.data(), (int)I->rhs.size(), bb.data(), ee.data(), I->dec.n_lambda,
+                             I->prep.n_kern);
+        } else {
+            make_rhs_vectors(I->dec, I->prep, bb, ee);
+        }
         if (b) std::copy(bb.begin(), bb.end(), b);
         if (e) std::copy(ee.begin(), ee.end(), e);
     });

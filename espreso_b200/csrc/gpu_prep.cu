@@ -385,6 +385,183 @@ __global__ void add_reg_kernel(const JobD *jobs, const SubD *subs, double *arena
 }
 
 // ---------------------------------------------------------------------------------------------
+// device-resident outputs
+
+constexpr int TL = 32;    // tile edge of the dual iteration's Schur and K^+ stores
+
+struct TJob {
+    int sub;              // batch-local subdomain
+    int r0, m;            // symmetric block at (r0, r0) of size m (sym), or the leading m x m factor (kp)
+    int tn;               // tiles per side
+    long long tile0;      // first tile in the store
+    int cta0;             // first CTA of this job
+    double scale;
+};
+
+__device__ __forceinline__ int find_tjob(const TJob *tj, int n, int b) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (tj[mid].cta0 <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Upper tiles of a symmetric block kept in the lower triangle: one CTA per tile (I <= J, row of
+// tiles after row of tiles), tile[r][c] = scale * M(32 I + r, 32 J + c), zero beyond m.
+__global__ void __launch_bounds__(PT) sym_tiles_kernel(const TJob *tj, int ntj, const SubD *subs,
+                                                       const double *arena, double *out) {
+    const TJob J_ = tj[find_tjob(tj, ntj, blockIdx.x)];
+    const SubD sd = subs[J_.sub];
+    const double *A = arena + sd.a;
+    const int t = blockIdx.x - J_.cta0, tn = J_.tn;
+    // row of tiles I: first tile I * tn - I (I - 1) / 2
+    int lo = 0, hi = tn - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if ((long long)mid * tn - (long long)mid * (mid - 1) / 2 <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    const int I = lo, J = I + (t - (int)((long long)I * tn - (long long)I * (I - 1) / 2));
+    double *tile = out + (size_t)(J_.tile0 + t) * TL * TL;
+    for (int q = threadIdx.x; q < TL * TL; q += PT) {
+        const int r = q / TL, c = q % TL;
+        const int i = TL * I + r, j = TL * J + c;
+        double v = 0.0;
+        if (i < J_.m && j < J_.m)
+            v = i >= j ? A[(size_t)(J_.r0 + j) * sd.ld + J_.r0 + i] : A[(size_t)(J_.r0 + i) * sd.ld + J_.r0 + j];
+        tile[q] = J_.scale * v;
+    }
+}
+
+// Lower tiles of the leading factor (I >= J, column of tiles after column of tiles): tile[r][c] =
+// L(32 I + r, 32 J + c); beyond m the diagonal is 1 and the rest 0.  A diagonal tile is replaced by
+// the inverse of its lower triangle (forward substitution, one lane per column).
+__global__ void __launch_bounds__(PT) kp_tiles_kernel(const TJob *tj, int ntj, const SubD *subs,
+                                                      const double *arena, double *out) {
+    __shared__ double T[TL][TL + 1];
+    __shared__ double V[TL][TL + 1];
+    const TJob J_ = tj[find_tjob(tj, ntj, blockIdx.x)];
+    const SubD sd = subs[J_.sub];
+    const double *A = arena + sd.a;
+    const int t = blockIdx.x - J_.cta0, tn = J_.tn;
+    // column of tiles J: first tile J * tn - J (J - 1) / 2
+    int lo = 0, hi = tn - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if ((long long)mid * tn - (long long)mid * (mid - 1) / 2 <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    const int J = lo, I = J + (t - (int)((long long)J * tn - (long long)J * (J - 1) / 2));
+    const int m = J_.m;
+    for (int q = threadIdx.x; q < TL * TL; q += PT) {
+        const int c = q / TL, r = q % TL;     // rows contiguous in the arena's column
+        const int i = TL * I + r, j = TL * J + c;
+        double v;
+        if (i < m && j < m) v = i >= j ? A[(size_t)j * sd.ld + i] : 0.0;
+        else v = i == j ? 1.0 : 0.0;
+        T[r][c] = v;
+    }
+    __syncthreads();
+    double *tile = out + (size_t)(J_.tile0 + t) * TL * TL;
+    if (I != J) {
+        for (int q = threadIdx.x; q < TL * TL; q += PT) tile[q] = T[q / TL][q % TL];
+        return;
+    }
+    if (threadIdx.x < TL) {
+        const int c = threadIdx.x;
+        for (int r = 0; r < c; ++r) V[r][c] = 0.0;
+        for (int r = c; r < TL; ++r) {
+            double sum = r == c ? 1.0 : 0.0;
+            for (int k = c; k < r; ++k) sum -= T[r][k] * V[k][c];
+            V[r][c] = sum / T[r][r];
+        }
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < TL * TL; q += PT) tile[q] = V[q / TL][q % TL];
+}
+
+// Kernel vectors: backward solve L_rr^T x_r = -L_sr^T N over 64-column blocks, descending.  One step
+// per block J (the first step is the fix block itself, whose x = N is given): CTA `below` solves
+// x_J = L_JJ^-T y_J and stores it; CTAs 0..below-1 subtract L_{J,i}^T x_J from y_i.  X and Y hold
+// n x nk per subdomain, column after column.
+struct BItem {
+    int sub, c0, w;       // block rows [c0, c0 + w)
+    int given;            // 1: x_J is known (the fix block), no solve and no store
+    int nk;
+    long long xo;         // offset of the subdomain's X / Y
+    int n;                // rows of X / Y
+    int cta0;
+};
+
+__global__ void __launch_bounds__(PT) bsolve_kernel(const BItem *items, int nitems, const SubD *subs,
+                                                    const double *arena, double *X, double *Y) {
+    __shared__ double D[NB][NB + 1];    // L_JJ (lower), or the tile L(J rows, i columns)
+    __shared__ double x[NB][8];
+    __shared__ double y[NB][8];
+    int lo = 0, hi = nitems - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (items[mid].cta0 <= (int)blockIdx.x) lo = mid;
+        else hi = mid - 1;
+    }
+    const BItem it = items[lo];
+    const SubD sd = subs[it.sub];
+    const double *A = arena + sd.a;
+    const int tid = threadIdx.x, w = it.w, nk = it.nk, c0 = it.c0;
+    const int l = blockIdx.x - it.cta0;
+    const int below = (c0 + NB - 1) / NB;
+    double *Xs = X + it.xo, *Ys = Y + it.xo;
+    if (it.given) {
+        for (int q = tid; q < NB * nk; q += PT) {
+            const int r = q % NB, k = q / NB;
+            x[r][k] = r < w ? Xs[(size_t)k * it.n + c0 + r] : 0.0;
+        }
+    } else {
+        for (int q = tid; q < w * w; q += PT) {
+            const int i = q % w, j = q / w;
+            if (i >= j) D[i][j] = A[(size_t)(c0 + j) * sd.ld + c0 + i];
+        }
+        for (int q = tid; q < NB * nk; q += PT) {
+            const int r = q % NB, k = q / NB;
+            y[r][k] = r < w ? Ys[(size_t)k * it.n + c0 + r] : 0.0;
+        }
+        __syncthreads();
+        for (int r = w - 1; r >= 0; --r) {
+            if (tid < nk) x[r][tid] = y[r][tid] / D[r][r];
+            __syncthreads();
+            for (int q = tid; q < r * nk; q += PT) {
+                const int i = q % r, k = q / r;
+                y[i][k] -= D[r][i] * x[r][k];
+            }
+            __syncthreads();
+        }
+        if (l == below) {
+            for (int q = tid; q < w * nk; q += PT) {
+                const int r = q % w, k = q / w;
+                Xs[(size_t)k * it.n + c0 + r] = x[r][k];
+            }
+            return;
+        }
+    }
+    __syncthreads();
+    // y_i -= L(J rows, i columns)^T x_J, i = block l: columns 64 l .. min(64 l + 64, c0) - 1
+    const int cm = min(NB, c0 - NB * l);
+    for (int q = tid; q < cm * w; q += PT) {
+        const int r = q % w, c = q / w;
+        D[r][c] = A[(size_t)(NB * l + c) * sd.ld + c0 + r];
+    }
+    __syncthreads();
+    for (int q = tid; q < cm * nk; q += PT) {
+        const int c = q % cm, k = q / cm;
+        double sum = 0.0;
+        for (int r = 0; r < w; ++r) sum += D[r][c] * x[r][k];
+        Ys[(size_t)k * it.n + NB * l + c] -= sum;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // host side
 
 template <typename T>
@@ -445,14 +622,54 @@ std::vector<Step> make_steps(int njobs, Lo lo, Hi hi, Rend rend, double &flops) 
 
 }  // namespace
 
+DevPrepStore::~DevPrepStore() {
+    if (s_tiles) cudaFree(s_tiles);
+    if (dir_tiles) cudaFree(dir_tiles);
+    if (kp_tiles) cudaFree(kp_tiles);
+}
+
 void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const RegulariseFn &regularise,
-                   size_t mem_budget, DevFactorTimes *times) {
+                   size_t mem_budget, DevFactorTimes *times, DevPrepStore *store, int ndom) {
     const double t_start = now_s();
     DevFactorTimes tm;
     const int nj = (int)jobs.size();
     if (nj == 0) {
         if (times) *times = tm;
         return;
+    }
+    const bool resident = store != nullptr;
+    if (resident) {
+        // tile stores for every subdomain (slots without a job get no tiles)
+        std::vector<int> sn(ndom, 0), st(ndom, 0), kn(ndom, 0);
+        bool dir = false;
+        for (const DevFactorJob &J : jobs) {
+            FETI_CHECK(J.slot >= 0 && J.slot < ndom, "FETI4I: device factorisation job outside the store");
+            sn[J.slot] = J.ni;
+            kn[J.slot] = J.n;
+            if (J.want_sdir) {
+                st[J.slot] = J.n - J.n1;
+                dir = true;
+            }
+        }
+        auto offsets = [&](const std::vector<int> &m, bool lower) {
+            std::vector<long long> o(ndom + 1, 0);
+            for (int d = 0; d < ndom; ++d) {
+                const long long t = (m[d] + TL - 1) / TL;
+                o[d + 1] = o[d] + t * (t + 1) / 2;
+            }
+            (void)lower;
+            return o;
+        };
+        store->nd = ndom;
+        store->s_tile0 = offsets(sn, false);
+        store->kp_tile0 = offsets(kn, true);
+        const size_t tb = (size_t)TL * TL * sizeof(double);
+        PCHECK(cudaMalloc(&store->s_tiles, std::max<long long>(store->s_tile0[ndom], 1) * tb));
+        PCHECK(cudaMalloc(&store->kp_tiles, std::max<long long>(store->kp_tile0[ndom], 1) * tb));
+        if (dir) {
+            store->dir_tile0 = offsets(st, false);
+            PCHECK(cudaMalloc(&store->dir_tiles, std::max<long long>(store->dir_tile0[ndom], 1) * tb));
+        }
     }
     if (mem_budget == 0) {
         size_t fr = 0, tot = 0;
@@ -481,9 +698,9 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
         z.N = J.n + J.ni;
         z.ld = (z.N + 31) / 32 * 32;
         z.a = (size_t)z.ld * z.N;
-        z.lp = (size_t)J.n * (J.n + 1) / 2;
-        z.s = (size_t)J.ni * J.ni;
-        z.sd = J.want_sdir ? (size_t)(J.n - J.n1) * (J.n - J.n1) : 0;
+        z.lp = resident ? 0 : (size_t)J.n * (J.n + 1) / 2;
+        z.s = resident ? 0 : (size_t)J.ni * J.ni;
+        z.sd = (J.want_sdir && !resident) ? (size_t)(J.n - J.n1) * (J.n - J.n1) : 0;
         z.fx = (size_t)J.ns * J.ns;
         z.vals = 0;
         for (int k = 0; k < J.nelem; ++k) {
@@ -497,7 +714,9 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
     {
         size_t cur = 0;
         for (int j = 0; j < nj; ++j) {
-            const size_t bytes = 8 * (sz[j].a + sz[j].lp + sz[j].s + sz[j].sd + sz[j].fx + sz[j].vals) + 4 * sz[j].pos;
+            const size_t bytes = 8 * (sz[j].a + sz[j].lp + sz[j].s + sz[j].sd + sz[j].fx + sz[j].vals +
+                                      (resident ? 16 * (size_t)jobs[j].n : 0)) +
+                                 4 * sz[j].pos;
             if (j > bstart.back() && cur + bytes > mem_budget) {
                 bstart.push_back(j);
                 cur = 0;
@@ -507,7 +726,9 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
         bstart.push_back(nj);
     }
 
-    DevBuf<double> arena, stage, fxb, vals, bsign, reg, part;
+    DevBuf<double> arena, stage, fxb, vals, bsign, reg, part, dX, dY;
+    DevBuf<TJob> dtj;
+    DevBuf<BItem> dbi;
     DevBuf<int> epos, bpos, fail, list;
     DevBuf<SubD> dsubs;
     DevBuf<JobD> djobs;
@@ -669,9 +890,40 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
             }
             PCHECK(cudaGetLastError());
         };
+        // symmetric-block or factor tiles of this batch into a store
+        auto tiles = [&](int which, double *out, const std::vector<long long> &t0, double scale) {
+            std::vector<TJob> tj;
+            int ctas = 0;
+            for (int q = 0; q < nb; ++q) {
+                const DevFactorJob &J = jobs[j0 + q];
+                TJob t;
+                t.sub = q;
+                if (which == 0) { t.r0 = J.n; t.m = J.ni; }
+                else if (which == 1) { if (!J.want_sdir) continue; t.r0 = J.n1; t.m = J.n - J.n1; }
+                else { t.r0 = 0; t.m = J.n; }
+                t.tn = (t.m + TL - 1) / TL;
+                t.tile0 = t0[J.slot];
+                t.cta0 = ctas;
+                t.scale = scale;
+                const int cnt = t.tn * (t.tn + 1) / 2;
+                if (cnt == 0) continue;
+                ctas += cnt;
+                tj.push_back(t);
+            }
+            if (ctas == 0) return;
+            dtj.put(tj);
+            if (which == 2) kp_tiles_kernel<<<ctas, PT>>>(dtj.p, (int)tj.size(), dsubs.p, arena.p, out);
+            else sym_tiles_kernel<<<ctas, PT>>>(dtj.p, (int)tj.size(), dsubs.p, arena.p, out);
+            ++tm.launches;
+            PCHECK(cudaGetLastError());
+        };
         run(ph1, o1);
-        copy_sym_kernel<<<dim3(64, nb), PT>>>(djobs.p, dsubs.p, arena.p, stage.p, 1, 1.0);   // Dirichlet
-        ++tm.launches;
+        if (resident) {
+            if (store->dir_tiles) tiles(1, store->dir_tiles, store->dir_tile0, 1.0);   // Dirichlet
+        } else {
+            copy_sym_kernel<<<dim3(64, nb), PT>>>(djobs.p, dsubs.p, arena.p, stage.p, 1, 1.0);   // Dirichlet
+            ++tm.launches;
+        }
         run(ph2, o2);
         copy_sym_kernel<<<dim3(1, nb), PT>>>(djobs.p, dsubs.p, arena.p, fxb.p, 2, 1.0);       // fix block
         ++tm.launches;
@@ -693,10 +945,81 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
         add_reg_kernel<<<nb, 64>>>(djobs.p, dsubs.p, arena.p, reg.p);
         ++tm.launches;
         run(ph3, o3);
-        copy_sym_kernel<<<dim3(256, nb), PT>>>(djobs.p, dsubs.p, arena.p, stage.p, 0, -1.0);
-        pack_kernel<<<dim3(256, nb), PT>>>(djobs.p, dsubs.p, arena.p, stage.p);
-        tm.launches += 2;
-        PCHECK(cudaGetLastError());
+        std::vector<BItem> bitems;
+        std::vector<std::vector<size_t>> bsteps;   // item ranges per backward-solve step
+        size_t x_tot = 0;
+        if (resident) {
+            tiles(0, store->s_tiles, store->s_tile0, -1.0);
+            tiles(2, store->kp_tiles, store->kp_tile0, 1.0);
+            // kernel vectors: X = [x_r; N], Y = 0
+            std::vector<long long> xo(nb);
+            int maxb = 0;
+            for (int q = 0; q < nb; ++q) {
+                const DevFactorJob &J = jobs[j0 + q];
+                FETI_CHECK(J.nk >= 0 && J.nk <= 8, "FETI4I: kernel dimension above 8");
+                xo[q] = (long long)x_tot;
+                x_tot += (size_t)J.n * J.nk;
+                maxb = std::max(maxb, (J.n - J.ns + NB - 1) / NB);
+            }
+            std::vector<double> hx(std::max<size_t>(x_tot, 1), 0.0);
+            for (int q = 0; q < nb; ++q) {
+                const DevFactorJob &J = jobs[j0 + q];
+                FETI_CHECK((int)J.N.size() >= J.ns * J.nk, "FETI4I: kernel eigenvectors missing");
+                for (int k = 0; k < J.nk; ++k)
+                    for (int r = 0; r < J.ns; ++r) hx[xo[q] + (size_t)k * J.n + (J.n - J.ns) + r] = J.N[(size_t)k * J.ns + r];
+            }
+            dX.put(hx);
+            dY.reserve(hx.size());
+            PCHECK(cudaMemset(dY.p, 0, hx.size() * sizeof(double)));
+            for (int step = 0; step <= maxb; ++step) {
+                std::vector<size_t> rng{bitems.size()};
+                int ctas = 0;
+                for (int q = 0; q < nb; ++q) {
+                    const DevFactorJob &J = jobs[j0 + q];
+                    if (J.nk == 0) continue;
+                    const int nr = J.n - J.ns, nbr = (nr + NB - 1) / NB;
+                    BItem b;
+                    b.sub = q;
+                    b.nk = J.nk;
+                    b.xo = xo[q];
+                    b.n = J.n;
+                    b.cta0 = ctas;
+                    int cnt;
+                    if (step == 0) {
+                        b.c0 = nr;
+                        b.w = J.ns;
+                        b.given = 1;
+                        cnt = nbr;
+                    } else {
+                        const int blk = nbr - step;
+                        if (blk < 0) continue;
+                        b.c0 = NB * blk;
+                        b.w = std::min(NB, nr - b.c0);
+                        b.given = 0;
+                        cnt = blk + 1;
+                    }
+                    if (cnt == 0) continue;
+                    ctas += cnt;
+                    bitems.push_back(b);
+                }
+                rng.push_back(bitems.size());
+                rng.push_back((size_t)ctas);
+                bsteps.push_back(rng);
+            }
+            dbi.put(bitems);
+            for (auto &r : bsteps) {
+                const int cnt = (int)(r[1] - r[0]), ctas = (int)r[2];
+                if (ctas == 0) continue;
+                bsolve_kernel<<<ctas, PT>>>(dbi.p + r[0], cnt, dsubs.p, arena.p, dX.p, dY.p);
+                ++tm.launches;
+            }
+            PCHECK(cudaGetLastError());
+        } else {
+            copy_sym_kernel<<<dim3(256, nb), PT>>>(djobs.p, dsubs.p, arena.p, stage.p, 0, -1.0);
+            pack_kernel<<<dim3(256, nb), PT>>>(djobs.p, dsubs.p, arena.p, stage.p);
+            tm.launches += 2;
+            PCHECK(cudaGetLastError());
+        }
         PCHECK(cudaEventRecord(ev1));
         PCHECK(cudaEventSynchronize(ev1));
         PCHECK(cudaEventElapsedTime(&ms, ev0, ev1));
@@ -712,6 +1035,14 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
             double s = 0.0;
             for (int k = 0; k < KN_BLOCKS; ++k) s += hpart[(size_t)q * KN_BLOCKS + k];
             J.knorm = std::sqrt(s);
+            if (resident) {
+                if (J.Rp && J.nk > 0) {
+                    size_t o = 0;
+                    for (int p = 0; p < q; ++p) o += (size_t)jobs[j0 + p].n * jobs[j0 + p].nk;
+                    PCHECK(cudaMemcpy(J.Rp, dX.p + o, (size_t)J.n * J.nk * sizeof(double), cudaMemcpyDeviceToHost));
+                }
+                continue;
+            }
             if (J.Lp) PCHECK(cudaMemcpy(J.Lp, stage.p + jd[q].lp, sz[j0 + q].lp * sizeof(double), cudaMemcpyDeviceToHost));
             if (J.S) PCHECK(cudaMemcpy(J.S, stage.p + jd[q].s, sz[j0 + q].s * sizeof(double), cudaMemcpyDeviceToHost));
             if (J.want_sdir && J.Sdir)

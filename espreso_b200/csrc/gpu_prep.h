@@ -23,8 +23,23 @@
 
 namespace feti {
 
+// Device-resident results of device_factor for Total FETI: the tile stores the dual iteration
+// reads, handed to the GPU solver without a host copy.  Subdomain d's tiles start at tile0[d]
+// (tile0 has ndom + 1 entries); a tile is 32 x 32 doubles, row-major.
+struct DevPrepStore {
+    int nd = 0;
+    double *s_tiles = nullptr;       // S_i: upper tiles (I <= J), row of tiles after row of tiles
+    std::vector<long long> s_tile0;
+    double *dir_tiles = nullptr;     // Dirichlet Schur complements, same layout (null without them)
+    std::vector<long long> dir_tile0;
+    double *kp_tiles = nullptr;      // K_reg factor: lower tiles (I >= J), column of tiles after column,
+    std::vector<long long> kp_tile0; // diagonal tiles replaced by the inverse of their triangle
+    ~DevPrepStore();
+};
+
 struct DevFactorJob {
     // inputs
+    int slot = 0;                // subdomain index (tile offsets in a DevPrepStore)
     int n = 0;                   // DOFs
     int n1 = 0;                  // untouched DOFs (eliminated first)
     int ns = 0;                  // fix DOFs (eliminated last)
@@ -37,7 +52,11 @@ struct DevFactorJob {
     std::vector<int> bpos;       // per B row: factor position of its DOF (>= n1)
     std::vector<double> bsign;   // per B row: sign
     bool want_sdir = false;      // snapshot the Schur complement onto the touched DOFs
-    // outputs (host buffers sized by the caller)
+    // set by the regularisation callback: kernel dimension and the kernel eigenvectors N (ns x nk)
+    int nk = 0;
+    std::vector<double> N;
+    // outputs (host buffers sized by the caller; with a DevPrepStore only Rp is written)
+    double *Rp = nullptr;        // n x nk: kernel [-L_rr^-T L_sr^T N; N] in factor order (store mode)
     double *Lp = nullptr;        // n(n+1)/2: packed lower factor of K_reg (factor order)
     double *S = nullptr;         // ni x ni, column-major, full symmetric
     double *Sdir = nullptr;      // t x t (t = n - n1), column-major, full symmetric
@@ -55,12 +74,16 @@ struct DevFactorTimes {
 
 // regularise(job, Sss, reg): Sss is the ns x ns fix-DOF Schur block (column-major, full); the
 // callback writes reg (ns x ns, column-major), which is added to the block before its columns are
-// eliminated.  It runs on the host between the elimination phases of each batch.
+// eliminated, and sets the job's nk and N.  It runs on the host between the elimination phases of
+// each batch.
 using RegulariseFn = std::function<void(int job, const double *Sss, double *reg)>;
 
 // Factorises every job on the current CUDA device, in batches whose dense matrices fit
-// `mem_budget` bytes (0: half of the free device memory).  Throws feti::Error on CUDA errors.
+// `mem_budget` bytes (0: half of the free device memory).  With `store` (sized by this call for
+// `ndom` subdomains; jobs' slots index it) S_i, the Dirichlet blocks and the K^+ factor stay on the
+// device as tiles and only the kernels Rp come back; without it Lp, S and Sdir are copied to the
+// host.  Throws feti::Error on CUDA errors.
 void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const RegulariseFn &regularise,
-                   size_t mem_budget, DevFactorTimes *times);
+                   size_t mem_budget, DevFactorTimes *times, DevPrepStore *store = nullptr, int ndom = 0);
 
 }  // namespace feti

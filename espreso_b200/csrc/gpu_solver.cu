@@ -19,6 +19,7 @@
 
 #include "common.h"
 #include "dense.h"
+#include "gpu_prep.h"
 #include "gpu_solver.h"
 
 #define CUDA_CHECK(x)                                                                              \
@@ -1341,6 +1342,7 @@ struct GpuSolver::Impl {
     int max_tn = 0, max_tn_dir = 0, max_nt = 0, max_ni = 0;
     std::vector<int> h_lam;       // L row -> lambda
     std::vector<int> h_loff;
+    std::vector<int> h_doff;      // local-DOF offsets of the subdomains (K^+ vectors)
     int n_lambda = 0;
     cudaGraphExec_t graph = nullptr;
     int graph_chunk = 0, graph_prec = -1, graph_precond = -1;
@@ -1423,7 +1425,16 @@ struct GpuSolver::Impl {
     }
 
     void build_tiles(TileSetHost &T, int prec, const std::vector<const double *> &mats, const std::vector<int> &ns,
-                     const std::vector<int> &voffs, int tiles_per_item);
+                     const std::vector<int> &voffs, int tiles_per_item, double *dev64 = nullptr);
+    // takes over a device buffer allocated elsewhere (freed with the solver)
+    template <typename T>
+    T *adopt(T *&p, size_t n) {
+        T *q = p;
+        p = nullptr;
+        allocs.push_back(q);
+        bytes += n * sizeof(T);
+        return q;
+    }
     void itemize(TileSetHost &T, const std::vector<int> &tpi, int only_class);
     void autotune(TileSetHost &T, double *x, double *y, int ny);
     void launch_tiles(const TileSetHost &T, int mode, const double *src, const double *src2, double *out, int slot);
@@ -1461,7 +1472,9 @@ void GpuSolver::Impl::upload_kplus(const Decomposition &dec, const Prep &prep, c
     ntot = doff[nd];
     std::vector<int> pos(ntot), gdof(ntot), tdof_g(toff[nd]);
     std::vector<double> invm(ntot), R(rofs[nd]), Rd(prep.method == 1 ? rdofs[nd] : 0);
-    std::vector<double> L((size_t)tile0[nd] * TILE * TILE, 0.0);
+    DevPrepStore *ds = prep.dstore.get();
+    if (ds) FETI_CHECK(ds->kp_tiles && ds->kp_tile0 == tile0, "FETI4I: device K+ tiles do not match the subdomains");
+    std::vector<double> L(ds ? 0 : (size_t)tile0[nd] * TILE * TILE, 0.0);
     n_caller = 0;
     for (int d = 0; d < nd; ++d) {
         const SubPrep &S = prep.sub[d];
@@ -1477,6 +1490,7 @@ void GpuSolver::Impl::upload_kplus(const Decomposition &dec, const Prep &prep, c
         std::copy(S.R.begin(), S.R.end(), R.begin() + rofs[d]);
         if (prep.method == 1) std::copy(S.Rd.begin(), S.Rd.end(), Rd.begin() + rdofs[d]);
         for (int t = 0; t < S.t; ++t) tdof_g[toff[d] + t] = doff[d] + S.tdof[t];
+        if (ds) continue;   // factor tiles written by the device preprocessing
         const int T = tn[d], nn = n[d];
         for (int J = 0; J < T; ++J)
             for (int I = J; I < T; ++I) {
@@ -1519,10 +1533,11 @@ void GpuSolver::Impl::upload_kplus(const Decomposition &dec, const Prep &prep, c
     KP.n = upload(n);
     KP.tn = upload(tn);
     d_doff = upload(doff);
+    h_doff = doff;
     KP.doff = d_doff;
     KP.tile0 = upload(tile0);
     KP.pos = upload(pos);
-    KP.L = upload(L);
+    KP.L = ds ? adopt(ds->kp_tiles, (size_t)tile0[nd] * TILE * TILE) : upload(L);
     d_rofs = upload(rofs);
     d_gdof = upload(gdof);
     d_invm = upload(invm);
@@ -1644,8 +1659,37 @@ void GpuSolver::Impl::launch_kplus_dual(const double *in, double *out) {
     CUDA_CHECK(cudaGetLastError());
 }
 
+// FP64 Schur tiles already on the device -> FP32 or BF16 (per-tile scale) tiles.
+__global__ void __launch_bounds__(256) convert_tiles_kernel(const double *src, void *dst, float *scale, int prec,
+                                                            long long ntiles) {
+    __shared__ float s_red[8];
+    for (long long g = blockIdx.x; g < ntiles; g += gridDim.x) {
+        const double *t = src + (size_t)g * TILE * TILE;
+        float s = 1.0f;
+        if (prec == SCHUR_BF16) {
+            double amax = 0.0;
+            for (int q = threadIdx.x; q < TILE * TILE; q += 256) amax = fmax(amax, fabs(t[q]));
+            float a = (float)amax;
+            for (int o = 16; o; o >>= 1) a = fmaxf(a, __shfl_xor_sync(0xffffffffu, a, o));
+            if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = a;
+            __syncthreads();
+            a = 0.0f;
+            for (int w = 0; w < 8; ++w) a = fmaxf(a, s_red[w]);
+            s = a > 0.0f ? a : 1.0f;
+            if (threadIdx.x == 0) scale[g] = s;
+            __syncthreads();
+        }
+        for (int q = threadIdx.x; q < TILE * TILE; q += 256) {
+            const size_t o = (size_t)g * TILE * TILE + q;
+            if (prec == SCHUR_FP32) ((float *)dst)[o] = (float)t[q];
+            else ((__nv_bfloat16 *)dst)[o] = __float2bfloat16_rn((float)(t[q] / s));
+        }
+    }
+}
+
 void GpuSolver::Impl::build_tiles(TileSetHost &T, int prec, const std::vector<const double *> &mats,
-                                  const std::vector<int> &ns, const std::vector<int> &voffs, int tiles_per_item) {
+                                  const std::vector<int> &ns, const std::vector<int> &voffs, int tiles_per_item,
+                                  double *dev64) {
     const int nm = (int)mats.size();
     const size_t esz = prec == SCHUR_FP64 ? 8 : prec == SCHUR_FP32 ? 4 : 2;
     const size_t tbytes = (size_t)TILE * TILE * esz;
@@ -1662,6 +1706,43 @@ void GpuSolver::Impl::build_tiles(TileSetHost &T, int prec, const std::vector<co
         alg += (double)ns[m] * (ns[m] + 1) / 2 * (double)esz + (double)ns[m] * (4 + 8 + 8);
     }
     std::vector<unsigned> ij(total);
+    if (dev64) {
+        // tiles already on the device (device preprocessing): FP64 taken over, others converted
+        for (int m = 0; m < nm; ++m) {
+            long long g = m0[m];
+            for (int I = 0; I < mt[m]; ++I)
+                for (int J = I; J < mt[m]; ++J, ++g) ij[g] = ((unsigned)I << 16) | (unsigned)J;
+        }
+        T.prec = prec;
+        T.bytes = (size_t)total * tbytes;
+        T.alg_bytes = alg;
+        T.mat_n = upload(mn);
+        T.mat_voff = upload(mv);
+        T.mat_tn = upload(mt);
+        T.mat_tile0 = upload(m0);
+        T.tile_ij = upload(ij);
+        T.scale = nullptr;
+        if (prec == SCHUR_FP64) {
+            T.tiles = dev64;
+        } else {
+            T.tiles = alloc<unsigned char>((size_t)std::max<long long>(total, 1) * tbytes);
+            if (prec == SCHUR_BF16) T.scale = alloc<float>((size_t)std::max<long long>(total, 1));
+            if (total > 0)
+                convert_tiles_kernel<<<(unsigned)std::min<long long>(total, 65535), 256>>>(dev64, T.tiles, T.scale,
+                                                                                          prec, total);
+            CUDA_CHECK(cudaGetLastError());
+        }
+        T.h_tn = mt;
+        T.total_tiles = total;
+        T.items = alloc<int4>((size_t)total);
+        T.item_dot = alloc<double>((size_t)total);
+        T.queue = alloc<int>(2);
+        CUDA_CHECK(cudaMemset(T.queue, 0, 2 * sizeof(int)));
+        T.kernel = opt.tile_kernel;
+        T.class_tpi.assign(kSizeClasses, tiles_per_item);
+        itemize(T, T.class_tpi, -1);
+        return;
+    }
     std::vector<unsigned char> data((size_t)total * tbytes);
     std::vector<float> sc(prec == SCHUR_BF16 ? total : 0);
     for (int m = 0; m < nm; ++m) {
@@ -2129,8 +2210,12 @@ void GpuSolver::upload(const Decomposition &dec, const Prep &prep, const SolveOp
         I.max_tn = std::max(I.max_tn, (ns[d] + TILE - 1) / TILE);
     }
     FETI_CHECK(tile_smem(SCHUR_FP64, I.max_tn) <= 200 * 1024, "FETI4I: a Schur complement is too large for the tile kernel");
-    I.build_tiles(I.F64, SCHUR_FP64, mats, ns, voffs, opt.tiles_per_item);
-    if (opt.schur_precision != SCHUR_FP64) I.build_tiles(I.Flow, opt.schur_precision, mats, ns, voffs, opt.tiles_per_item);
+    DevPrepStore *ds = prep.dstore.get();
+    FETI_CHECK(!ds || (ds->nd == nd && ds->s_tiles && ds->kp_tiles), "FETI4I: device preprocessing store missing");
+    double *s64 = ds ? I.adopt(ds->s_tiles, (size_t)ds->s_tile0[nd] * TILE * TILE) : nullptr;
+    I.build_tiles(I.F64, SCHUR_FP64, mats, ns, voffs, opt.tiles_per_item, s64);
+    if (opt.schur_precision != SCHUR_FP64)
+        I.build_tiles(I.Flow, opt.schur_precision, mats, ns, voffs, opt.tiles_per_item, s64);
     if (opt.precond == PREC_DIRICHLET) {
         std::vector<const double *> dm(nd);
         std::vector<int> dn(nd), dv(nd);
@@ -2142,7 +2227,9 @@ void GpuSolver::upload(const Decomposition &dec, const Prep &prep, const SolveOp
             I.max_tn_dir = std::max(I.max_tn_dir, (dn[d] + TILE - 1) / TILE);
         }
         FETI_CHECK(tile_smem(SCHUR_FP64, I.max_tn_dir) <= 200 * 1024, "FETI4I: a Dirichlet block is too large for the tile kernel");
-        I.build_tiles(I.Dir, SCHUR_FP64, dm, dn, dv, opt.tiles_per_item);
+        FETI_CHECK(!ds || ds->dir_tiles, "FETI4I: device preprocessing store has no Dirichlet blocks");
+        double *d64 = ds ? I.adopt(ds->dir_tiles, (size_t)ds->dir_tile0[nd] * TILE * TILE) : nullptr;
+        I.build_tiles(I.Dir, SCHUR_FP64, dm, dn, dv, opt.tiles_per_item, d64);
     }
     if (opt.autotune) {
         CUDA_CHECK(cudaMemset(P.w, 0, sizeof(double) * NL));
@@ -2295,6 +2382,61 @@ void GpuSolver::get_solution(std::vector<double> &lambda, std::vector<double> &a
     for (size_t e = 0; e < xL.size(); ++e) lambda[I.h_lam[e]] = xL[e];
     alpha.resize(I.P.nK);
     CUDA_CHECK(cudaMemcpy(alpha.data(), I.P.alpha, alpha.size() * sizeof(double), cudaMemcpyDeviceToHost));
+}
+
+void GpuSolver::subdomain_schur(int d, double *S) {
+    Impl &I = *impl;
+    const TileSetHost &T = I.F64;
+    FETI_CHECK(d >= 0 && d < (int)T.h_tn.size(), "FETI4I: subdomain index out of range");
+    long long t0 = 0;
+    for (int m = 0; m < d; ++m) t0 += (long long)T.h_tn[m] * (T.h_tn[m] + 1) / 2;
+    const int tn = T.h_tn[d], n = I.h_loff[d + 1] - I.h_loff[d];
+    std::vector<double> tiles((size_t)tn * (tn + 1) / 2 * TILE * TILE);
+    CUDA_CHECK(cudaMemcpy(tiles.data(), (const double *)T.tiles + (size_t)t0 * TILE * TILE,
+                          tiles.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    long long g = 0;
+    for (int Ib = 0; Ib < tn; ++Ib)
+        for (int Jb = Ib; Jb < tn; ++Jb, ++g)
+            for (int r = 0; r < TILE; ++r)
+                for (int c = 0; c < TILE; ++c) {
+                    const int i = TILE * Ib + r, j = TILE * Jb + c;
+                    if (i >= n || j >= n) continue;
+                    const double v = tiles[(size_t)g * TILE * TILE + r * TILE + c];
+                    S[(size_t)j * n + i] = v;
+                    S[(size_t)i * n + j] = v;
+                }
+}
+
+void GpuSolver::subdomain_kplus(int d, double *x) {
+    Impl &I = *impl;
+    FETI_CHECK(!I.hybrid, "FETI4I: device subdomain K+ is available for Total FETI");
+    FETI_CHECK(d >= 0 && d + 1 < (int)I.h_doff.size(), "FETI4I: subdomain index out of range");
+    const int o = I.h_doff[d], n = I.h_doff[d + 1] - I.h_doff[d];
+    CUDA_CHECK(cudaMemsetAsync(I.d_f, 0, sizeof(double) * I.ntot, I.stream));
+    CUDA_CHECK(cudaMemcpyAsync(I.d_f + o, x, sizeof(double) * n, cudaMemcpyHostToDevice, I.stream));
+    I.launch_kplus(I.d_f, I.d_kf);
+    CUDA_CHECK(cudaMemcpyAsync(x, I.d_kf + o, sizeof(double) * n, cudaMemcpyDeviceToHost, I.stream));
+    CUDA_CHECK(cudaStreamSynchronize(I.stream));
+}
+
+void GpuSolver::dual_rhs(const double *rhs, int rhs_size, double *b, double *e, int n_lambda, int n_kern) {
+    Impl &I = *impl;
+    DevProblem &P = I.P;
+    CUDA_CHECK(cudaMemsetAsync(I.d_rhs, 0, sizeof(double) * std::max(1, I.n_caller), I.stream));
+    const int ncp = std::min(rhs_size, I.n_caller);
+    CUDA_CHECK(cudaMemcpyAsync(I.d_rhs, rhs, sizeof(double) * std::max(0, ncp), cudaMemcpyHostToDevice, I.stream));
+    split_rhs_kernel<<<(I.ntot + 255) / 256, 256, 0, I.stream>>>(I.d_rhs, I.d_gdof, I.d_invm, I.d_f, I.ntot);
+    I.launch_kplus_dual(I.d_f, I.d_kf);
+    evec_kernel<<<P.nd, TPB, 0, I.stream>>>(P, I.d_doff, I.d_rdofs, I.d_Rd, I.d_f, I.e_dev);
+    bvec_kernel<<<(P.NL + 255) / 256, 256, 0, I.stream>>>(P, I.d_rdof, I.d_rsign, I.d_rc, I.d_kf, (double *)P.bL);
+    CUDA_CHECK(cudaGetLastError());
+    std::vector<double> bL(P.NL), ep(P.nP);
+    CUDA_CHECK(cudaMemcpyAsync(bL.data(), P.bL, sizeof(double) * P.NL, cudaMemcpyDeviceToHost, I.stream));
+    CUDA_CHECK(cudaMemcpyAsync(ep.data(), I.e_dev, sizeof(double) * P.nP, cudaMemcpyDeviceToHost, I.stream));
+    CUDA_CHECK(cudaStreamSynchronize(I.stream));
+    for (int i = 0; i < n_lambda; ++i) b[i] = 0.0;
+    for (size_t r = 0; r < bL.size(); ++r) b[I.h_lam[r]] = bL[r];
+    for (int k = 0; k < n_kern && k < (int)I.dual_to_partial.size(); ++k) e[k] = ep[I.dual_to_partial[k]];
 }
 
 void GpuSolver::apply_F(const double *x_lambda, double *y_lambda, int precision) {

@@ -62,6 +62,12 @@ public:
     // per-column scalars and stop tests, tile SYMM F apply; solutions[j * solution_size + i].
     void solve_multi(const double *rhs, int nrhs, int rhs_size, double *solutions, int solution_size, SolveStats &st,
                      bool upload_rhs = true);
+    // Introspection through the device data (device preprocessing keeps S_i and K^+ only there):
+    // S_i as a full ni x ni column-major matrix; x := K_i^+ x (local DOF order); b and e of the
+    // caller right-hand side (multiplier order, dual kernel order).
+    void subdomain_schur(int d, double *S);
+    void subdomain_kplus(int d, double *x);
+    void dual_rhs(const double *rhs, int rhs_size, double *b, double *e, int n_lambda, int n_kern);
     // y = F x in lambda space with the given operator precision (tests, benchmarks)
     void apply_F(const double *x_lambda, double *y_lambda, int precision);
     // average device time of `reps` F applies (inputs resident), returns ms

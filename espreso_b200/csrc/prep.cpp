@@ -352,8 +352,9 @@ static void prep_numeric_host(const ElementData &el, const Decomposition &dec, i
 
 // Kernel R = [-K_rr^-1 K_rs N; N] from the packed factor: R_r = -L_rr^-T (L_sr^T N); its check
 // against the fix columns of K; orthonormal columns; G_i = -(B_i R_i)^T.
+static void finish_kernel(const Decomposition &dec, int d, SubPrep &S, SubWork &W, const std::vector<double> &Rp);
+
 static void prep_finish(const Decomposition &dec, int d, SubPrep &S, SubWork &W) {
-    const DomainRows &D = dec.dom[d];
     const int n = S.n, ns = W.ns, defect = W.defect;
     const int nr = n - ns;
     const double *Lp = S.Lp.data();
@@ -373,6 +374,13 @@ static void prep_finish(const Decomposition &dec, int d, SubPrep &S, SubWork &W)
         }
         for (int j = 0; j < nr; ++j) x[j] = -x[j];
     }
+    finish_kernel(dec, d, S, W, Rp);
+}
+
+// Rp (n x defect, factor order) -> R in local DOF order, the kernel check, orthonormal columns, G.
+static void finish_kernel(const Decomposition &dec, int d, SubPrep &S, SubWork &W, const std::vector<double> &Rp) {
+    const DomainRows &D = dec.dom[d];
+    const int n = S.n, ns = W.ns, defect = W.defect;
     S.R.assign((size_t)n * defect, 0.0);
     for (int k = 0; k < defect; ++k)
         for (int i = 0; i < n; ++i) S.R[(size_t)k * n + i] = Rp[(size_t)k * n + S.pos[i]];
@@ -410,8 +418,10 @@ static void prep_subdomain(const ElementData &el, const Decomposition &dec, int 
 // complement on the GPU (gpu_prep.cu), kernels and G on the host threads.
 static void prep_all_device(const ElementData &el, const Decomposition &dec, const PrepOptions &opt,
                             std::vector<SubPrep> &sub, const std::vector<int> &order, int nthreads,
-                            std::vector<std::string> &errors, DevFactorTimes &dt) {
+                            std::vector<std::string> &errors, DevFactorTimes &dt,
+                            std::shared_ptr<DevPrepStore> &dstore) {
     const int nd = dec.ndom;
+    const double t0 = now_s();
     std::vector<SubWork> work(nd);
 #pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
     for (int k = 0; k < nd; ++k) {
@@ -425,6 +435,11 @@ static void prep_all_device(const ElementData &el, const Decomposition &dec, con
     std::vector<int> ids;   // subdomains of the device jobs, largest first
     for (int k = 0; k < nd; ++k)
         if (errors[order[k]].empty()) ids.push_back(order[k]);
+    // Total FETI keeps S_i, the Dirichlet blocks and K^+ on the device (the tile stores of the dual
+    // iteration); Hybrid Total FETI needs the host K^+ for its cluster problems and copies them back.
+    const bool resident = opt.method == 0;
+    std::shared_ptr<DevPrepStore> store = resident ? std::make_shared<DevPrepStore>() : nullptr;
+    std::vector<std::vector<double>> Rps(resident ? nd : 0);
     std::vector<DevFactorJob> jobs(ids.size());
     for (size_t q = 0; q < ids.size(); ++q) {
         const int d = ids[q];
@@ -445,6 +460,8 @@ static void prep_all_device(const ElementData &el, const Decomposition &dec, con
         for (int r = 0; r < S.ni; ++r) J.bpos[r] = S.pos[D.dof[r]];
         J.bsign = D.sign;
         J.want_sdir = opt.precond == PREC_DIRICHLET;
+        J.slot = d;
+        if (resident) continue;
         S.Lp.assign((size_t)S.n * (S.n + 1) / 2, 0.0);
         S.S.assign((size_t)S.ni * S.ni, 0.0);
         if (J.want_sdir) S.Sdir.assign((size_t)S.t * S.t, 0.0);
@@ -456,12 +473,22 @@ static void prep_all_device(const ElementData &el, const Decomposition &dec, con
         const int d = ids[q];
         try {
             fix_block(sub[d], work[d], Sss, r);
+            DevFactorJob &J = jobs[q];
+            J.nk = work[d].defect;
+            J.N.assign(work[d].V.begin(), work[d].V.begin() + (size_t)J.nk * J.ns);
+            if (resident) {
+                Rps[d].assign((size_t)J.n * J.nk, 0.0);
+                J.Rp = Rps[d].data();
+            }
         } catch (const std::exception &ex) {
             errors[d] = ex.what();
             std::fill(r, r + (size_t)work[d].ns * work[d].ns, 0.0);
         }
     };
-    device_factor(el, jobs, reg, opt.device_mem, &dt);
+    const double t1 = now_s();
+    device_factor(el, jobs, reg, opt.device_mem, &dt, store.get(), nd);
+    const double t2 = now_s();
+    dstore = store;
     for (size_t q = 0; q < ids.size(); ++q) {
         const int d = ids[q];
         const DevFactorJob &J = jobs[q];
@@ -481,11 +508,14 @@ static void prep_all_device(const ElementData &el, const Decomposition &dec, con
         const int d = ids[k];
         if (!errors[d].empty()) continue;
         try {
-            prep_finish(dec, d, sub[d], work[d]);
+            if (resident) finish_kernel(dec, d, sub[d], work[d], Rps[d]);
+            else prep_finish(dec, d, sub[d], work[d]);
         } catch (const std::exception &ex) {
             errors[d] = ex.what();
         }
     }
+    FETI_LOG(2, "FETI4I: device preprocessing: symbolic %.3f s, device %.3f s (kernels %.1f ms, %.1f GFLOP, %d batches), kernels/G %.3f s\n",
+             t1 - t0, t2 - t1, dt.device_ms, dt.flops * 1e-9, dt.batches, now_s() - t2);
 }
 
 void preprocess(const ElementData &el, Decomposition &dec, const std::vector<double> &rhs, const PrepOptions &opt,
@@ -518,7 +548,7 @@ void preprocess(const ElementData &el, Decomposition &dec, const std::vector<dou
     out.device_prep = opt.device;
     if (opt.device) {
         DevFactorTimes dt;
-        prep_all_device(el, dec, opt, out.sub, order, nthreads, errors, dt);
+        prep_all_device(el, dec, opt, out.sub, order, nthreads, errors, dt, out.dstore);
         out.t_device_factor_ms = dt.device_ms;
         out.device_factor_flops = dt.flops;
         out.device_factor_launches = dt.launches;
@@ -548,6 +578,7 @@ void preprocess(const ElementData &el, Decomposition &dec, const std::vector<dou
             }
     }
     out.t_factor = now_s() - t0;
+    FETI_LOG(2, "FETI4I: subdomain preprocessing %.3f s\n", out.t_factor);
 
     // coarse problem: dual kernel space, owners of every multiplier, GG^T and its inverse
     double t1 = now_s();
@@ -611,6 +642,7 @@ void preprocess(const ElementData &el, Decomposition &dec, const std::vector<dou
     out.GGt_inv.assign((size_t)nK * nK, 0.0);
     dense::lauum_lower(Wc.data(), nK, nK, out.GGt_inv.data(), nK);
     out.t_coarse = now_s() - t1;
+    FETI_LOG(2, "FETI4I: coarse problem %.3f s\n", out.t_coarse);
 }
 
 void kplus_dual(const Prep &prep, std::vector<std::vector<double>> &x) {

@@ -4,11 +4,14 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
 #include <vector>
 
 #include "decompose.h"
 
 namespace feti {
+
+struct DevPrepStore;
 
 enum Precond { PREC_NONE = 0, PREC_LUMPED = 1, PREC_WEIGHT = 2, PREC_DIRICHLET = 3 };
 
@@ -73,6 +76,9 @@ struct Prep {
     std::vector<int> own_dom, own_row;  // 2 entries per multiplier, -1 if absent
     double t_factor = 0.0, t_coarse = 0.0;
     bool device_prep = false;          // eliminations and Schur complements ran on the GPU
+    // Total FETI with device preprocessing: S_i, Dirichlet blocks and K^+ as device tiles (the host
+    // SubPrep::S, Sdir and Lp stay empty)
+    std::shared_ptr<DevPrepStore> dstore;
     double t_device_factor_ms = 0.0;   // device time of those eliminations (events)
     double device_factor_flops = 0.0;
     int device_factor_launches = 0;
