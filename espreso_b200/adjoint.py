@@ -25,7 +25,7 @@ class SIMPModel:
     """E(rho) = E_min + rho^p (E0 - E_min) on a fixed mesh with unit-modulus element matrices."""
 
     def __init__(self, problem: problems.Problem, K_unit, E0=2.1e11, E_min=1e-9, p=3.0, rhs=None,
-                 precond=F.PREC_LUMPED, precision=1e-10, max_it=2000, device_prep=False):
+                 precond=F.PREC_LUMPED, precision=1e-10, max_it=2000, device_prep=True):
         self.P = problem
         self.device_prep = device_prep   # subdomain factorisations and S_i on the GPU (FETI4I_EXT_DEVICE_PREP)
         self.K_unit = np.ascontiguousarray(K_unit, dtype=np.float64)   # (E, nd, nd)
@@ -50,7 +50,7 @@ class SIMPModel:
         try:
             inst = F.Instance(M, self.f, self.dd, self.dv, iopts=self.iopts, ropts=self.ropts)
         finally:
-            F.set_extended(F.EXT_DEVICE_PREP, 0)
+            F.set_extended(F.EXT_DEVICE_PREP, 1)
             M.destroy()
         return inst
 

@@ -57,7 +57,7 @@ namespace {
 std::mutex g_mutex;
 std::list<FETI4IStructMatrix *> g_matrices;
 std::list<FETI4IStructInstance *> g_instances;
-double g_ext[FETI4I_EXT_OPTIONS_SIZE] = {0, 1, 0, 48, 16, 0.1, 0, 0, 1, 1, 0};
+double g_ext[FETI4I_EXT_OPTIONS_SIZE] = {0, 1, 0, 48, 16, 0.1, 0, 0, 1, 1, 1};
 
 template <typename F>
 void guarded(F &&f) {
@@ -123,11 +123,10 @@ void build(FETI4IStructInstance *I) {
     po.precond = prec;
     po.scaling = I->ext[FETI4I_EXT_SCALING] != 0.0;
     po.threads = (int)I->ext[FETI4I_EXT_HOST_THREADS];
-    po.device = I->ext[FETI4I_EXT_DEVICE_PREP] != 0.0;
+    // the device preprocessing runs with the GPU path; HOST_ONLY instances preprocess on the host
+    po.device = I->ext[FETI4I_EXT_DEVICE_PREP] != 0.0 && I->ext[FETI4I_EXT_HOST_ONLY] == 0.0;
     // batch size of the device eliminations in bytes (tests force one subdomain per batch)
     if (const char *b = std::getenv("FETI4I_DEVICE_PREP_BATCH_BYTES")) po.device_mem = std::strtoull(b, nullptr, 10);
-    FETI_CHECK(!po.device || I->ext[FETI4I_EXT_HOST_ONLY] == 0.0,
-               "FETI4I: DEVICE_PREP needs the GPU path (HOST_ONLY is set)");
     I->prep = Prep();
     preprocess(I->el, I->dec, I->rhs, po, I->prep);
     I->t_prep = now_s() - t0;

@@ -51,9 +51,10 @@ typedef enum {
     FETI4I_EXT_AUTOTUNE,         /* 1 (default): time both SYMV variants and the work-item sizes per size class */
     FETI4I_EXT_SYMM_TENSOR,      /* multi-RHS solves with FP32 Schur storage: 1 (default) tcgen05 tensor-core SYMM
                                     (3xTF32, 8 or more right-hand sides), 0 CUDA-core SYMM */
-    FETI4I_EXT_DEVICE_PREP,      /* 1: subdomain eliminations and Schur complements S_i on the GPU (batched FP64
-                                    partial Cholesky of [K_reg B^T; B 0]), 0 (default): host dense path.  The
-                                    reference assembles S_i on the host (SparseSolverMKL.cpp:1207) */
+    FETI4I_EXT_DEVICE_PREP,      /* 1 (default): subdomain eliminations and Schur complements S_i on the GPU
+                                    (batched FP64 partial Cholesky of [K_reg B^T; B 0]); 0, or HOST_ONLY: host
+                                    dense path.  The reference assembles S_i on the host
+                                    (SparseSolverMKL.cpp:1207) */
     FETI4I_EXT_OPTIONS_SIZE
 } FETI4IExtOptions;
 void FETI4ISetExtendedOption(FETI4IInt key, FETI4IReal value);

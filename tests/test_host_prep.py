@@ -112,9 +112,6 @@ def test_error_paths():
         problems.make_instance(P, iopts={F.CGSOLVER: 3, F.VERBOSE_LEVEL: 0}, ext={F.EXT_HOST_ONLY: 1})
     with pytest.raises(F.FETI4IError, match="PRECONDITIONER"):
         problems.make_instance(P, iopts={F.PRECONDITIONER: 5, F.VERBOSE_LEVEL: 0}, ext={F.EXT_HOST_ONLY: 1})
-    # the device Schur assembly needs the GPU path
-    with pytest.raises(F.FETI4IError, match="DEVICE_PREP"):
-        problems.make_instance(P, iopts={F.VERBOSE_LEVEL: 0}, ext={F.EXT_HOST_ONLY: 1, F.EXT_DEVICE_PREP: 1})
     inst = host_instance(P)
     with pytest.raises(F.FETI4IError, match="HOST_ONLY"):
         inst.solve()
