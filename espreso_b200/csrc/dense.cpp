@@ -2,6 +2,8 @@
 // extensions) and the blocked Cholesky / triangular routines built on it.
 #include "dense.h"
 
+#include <omp.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -135,18 +137,28 @@ int potf2(double *A, int n, int lda) {
 }
 }  // namespace
 
+// Large problems outside a parallel region (the coarse problem) split their independent work over
+// the host threads; every element sees the same operations in the same order either way.
+static bool parallel_worth(double work) { return work > 4e6 && !omp_in_parallel() && omp_get_max_threads() > 1; }
+
 void trsm_rlt(int m, int k, const double *L, int ldl, double *B, int ldb) {
-    // column j of X: X_j = (B_j - sum_{p<j} X_p L(j,p)) / L(j,j)
-    for (int j = 0; j < k; ++j) {
-        double *bj = B + (size_t)j * ldb;
-        for (int p = 0; p < j; ++p) {
-            double l = L[(size_t)p * ldl + j];
-            if (l == 0.0) continue;
-            const double *bp = B + (size_t)p * ldb;
-            for (int i = 0; i < m; ++i) bj[i] -= bp[i] * l;
+    // column j of X: X_j = (B_j - sum_{p<j} X_p L(j,p)) / L(j,j); rows are independent
+    const int RB = 256;
+    const int nb = (m + RB - 1) / RB;
+#pragma omp parallel for schedule(dynamic, 1) if (parallel_worth((double)m * k * k))
+    for (int b = 0; b < nb; ++b) {
+        const int i0 = b * RB, i1 = std::min(m, i0 + RB);
+        for (int j = 0; j < k; ++j) {
+            double *bj = B + (size_t)j * ldb;
+            for (int p = 0; p < j; ++p) {
+                double l = L[(size_t)p * ldl + j];
+                if (l == 0.0) continue;
+                const double *bp = B + (size_t)p * ldb;
+                for (int i = i0; i < i1; ++i) bj[i] -= bp[i] * l;
+            }
+            double inv = 1.0 / L[(size_t)j * ldl + j];
+            for (int i = i0; i < i1; ++i) bj[i] *= inv;
         }
-        double inv = 1.0 / L[(size_t)j * ldl + j];
-        for (int i = 0; i < m; ++i) bj[i] *= inv;
     }
 }
 
@@ -162,8 +174,10 @@ int potrf_lower(double *A, int n, int lda, int ncols) {
         double *P = Akk + kb;  // rows k+kb..n-1 of the panel
         trsm_rlt(m, kb, Akk, lda, P, lda);
         // trailing lower update A22 -= P P^T, by column blocks
-        for (int j0 = 0; j0 < m; j0 += NB) {
-            int jb = std::min(NB, m - j0);
+        const int nblk = (m + NB - 1) / NB;
+#pragma omp parallel for schedule(dynamic, 1) if (parallel_worth((double)m * m * kb))
+        for (int b = 0; b < nblk; ++b) {
+            const int j0 = b * NB, jb = std::min(NB, m - j0);
             gemm_nt_sub(m - j0, jb, kb, P + j0, lda, P + j0, lda,
                         A + (size_t)(k + kb + j0) * lda + k + kb + j0, lda);
         }
@@ -178,16 +192,24 @@ void trtri_lower(double *L, int n, int ld) {
     // in place), x_jj = 1/l_jj and x_21 = -X22 (l_21 x_jj); X22 * v is formed
     // as a sum of contiguous column axpys.
     std::vector<double> y(n);
+    const bool par = parallel_worth((double)n * n * n / 3.0);
     for (int j = n - 1; j >= 0; --j) {
         double xjj = 1.0 / L[(size_t)j * ld + j];
         int m = n - j - 1;
         double *l21 = L + (size_t)j * ld + j + 1;
-        std::fill(y.begin(), y.begin() + m, 0.0);
-        for (int p = 0; p < m; ++p) {
-            double v = l21[p] * xjj;
-            if (v == 0.0) continue;
-            const double *xc = L + (size_t)(j + 1 + p) * ld + j + 1;  // column p of X22, rows p..m-1
-            for (int i = p; i < m; ++i) y[i] += xc[i] * v;
+        // y = X22 (l21 xjj): rows i in independent chunks, the sum over p in ascending order
+        const int RB = 128;
+        const int nb = (m + RB - 1) / RB;
+#pragma omp parallel for schedule(static) if (par && m > 512)
+        for (int b = 0; b < nb; ++b) {
+            const int i0 = b * RB, i1 = std::min(m, i0 + RB);
+            std::fill(y.begin() + i0, y.begin() + i1, 0.0);
+            for (int p = 0; p < i1; ++p) {
+                double v = l21[p] * xjj;
+                if (v == 0.0) continue;
+                const double *xc = L + (size_t)(j + 1 + p) * ld + j + 1;  // column p of X22, rows p..m-1
+                for (int i = std::max(p, i0); i < i1; ++i) y[i] += xc[i] * v;
+            }
         }
         L[(size_t)j * ld + j] = xjj;
         for (int i = 0; i < m; ++i) l21[i] = -y[i];
@@ -195,7 +217,8 @@ void trtri_lower(double *L, int n, int ld) {
 }
 
 void lauum_lower(const double *W, int n, int ldw, double *C, int ldc) {
-    // C(i,j) = sum_{p >= max(i,j)} W(p,i) W(p,j)
+    // C(i,j) = sum_{p >= max(i,j)} W(p,i) W(p,j); columns are independent
+#pragma omp parallel for schedule(dynamic, 8) if (parallel_worth((double)n * n * n / 3.0))
     for (int j = 0; j < n; ++j) {
         const double *wj = W + (size_t)j * ldw;
         for (int i = j; i < n; ++i) {

@@ -32,7 +32,9 @@ namespace feti {
 
 namespace {
 
-constexpr int NB = 64;    // panel width and tile edge
+constexpr int PW = 128;   // panel width (k-depth of every trailing update)
+constexpr int TE = 64;    // row block of the panel solve and tile edge of the trailing update
+constexpr int BS = 64;    // column block of the kernel backward solve
 constexpr int PT = 256;   // threads per CTA
 
 struct SubD {
@@ -130,39 +132,86 @@ __global__ void knorm_kernel(const JobD *jobs, const SubD *subs, const double *a
 // ---------------------------------------------------------------------------------------------
 // elimination step
 
-// Cholesky of the w x w diagonal block of every item; a non-positive pivot is recorded (first
-// column per subdomain) and replaced by 1 so that the elimination stays finite.
-__global__ void __launch_bounds__(PT) diag_kernel(const Item *items, const SubD *subs, double *arena, int *fail) {
-    __shared__ double D[NB][NB + 1];
+// Cholesky of the w x w diagonal block of every item, blocked by 32 columns: warp 0 factors a 32 x 32
+// block (one lane per row) and inverts it (one lane per column); all warps multiply the rows below
+// by the inverse and update the rest of the panel block.  A non-positive pivot is recorded (first
+// column per subdomain) and replaced by 1 so that the elimination stays finite.  The inverses of the
+// 32 x 32 diagonal blocks go to `dinv` (four per item) for the panel solve.
+constexpr int DB = 32;
+constexpr int DSM = (PW * (PW + 1) + DB * (DB + 1) + (PW - DB) * (DB + 1)) * (int)sizeof(double);
+
+__global__ void __launch_bounds__(PT) diag_kernel(const Item *items, const SubD *subs, double *arena, int *fail,
+                                                  double *dinv) {
+    extern __shared__ double dsm[];
+    double(*D)[PW + 1] = reinterpret_cast<double(*)[PW + 1]>(dsm);
+    double(*V)[DB + 1] = reinterpret_cast<double(*)[DB + 1]>(dsm + PW * (PW + 1));
+    double(*T)[DB + 1] = reinterpret_cast<double(*)[DB + 1]>(dsm + PW * (PW + 1) + DB * (DB + 1));
     __shared__ int s_bad;
     const Item it = items[blockIdx.x];
     const SubD sd = subs[it.sub];
     double *A = arena + sd.a;
     const size_t ld = sd.ld;
-    const int k0 = it.k0, w = it.w, tid = threadIdx.x;
+    const int k0 = it.k0, w = it.w, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int q = tid; q < w * w; q += PT) {
         const int i = q % w, j = q / w;
         if (i >= j) D[i][j] = A[(size_t)(k0 + j) * ld + k0 + i];
     }
     if (tid == 0) s_bad = -1;
     __syncthreads();
-    for (int j = 0; j < w; ++j) {
-        if (tid == 0) {
-            double d = D[j][j];
-            if (!(d > 0.0)) {
-                if (s_bad < 0) s_bad = j;
-                d = 1.0;
+    double *dout = dinv + (size_t)blockIdx.x * (PW / DB) * DB * DB;
+    for (int c0 = 0; c0 < w; c0 += DB) {
+        const int bw = min(DB, w - c0);
+        if (warp == 0) {
+            // factor the bw x bw block, lane = row
+            for (int j = 0; j < bw; ++j) {
+                if (lane == j) {
+                    double d = D[c0 + j][c0 + j];
+                    if (!(d > 0.0)) {
+                        if (s_bad < 0) s_bad = c0 + j;
+                        d = 1.0;
+                    }
+                    D[c0 + j][c0 + j] = sqrt(d);
+                }
+                __syncwarp();
+                if (lane > j && lane < bw) D[c0 + lane][c0 + j] /= D[c0 + j][c0 + j];
+                __syncwarp();
+                if (lane > j && lane < bw)
+                    for (int c = j + 1; c <= lane; ++c) D[c0 + lane][c0 + c] -= D[c0 + lane][c0 + j] * D[c0 + c][c0 + j];
+                __syncwarp();
             }
-            D[j][j] = sqrt(d);
+            // inverse of the block, lane = column (zero above the diagonal and outside bw)
+            for (int r = 0; r < DB; ++r) V[r][lane] = 0.0;
+            if (lane < bw)
+                for (int r = lane; r < bw; ++r) {
+                    double sum = r == lane ? 1.0 : 0.0;
+                    for (int k = lane; k < r; ++k) sum -= D[c0 + r][c0 + k] * V[k][lane];
+                    V[r][lane] = sum / D[c0 + r][c0 + r];
+                }
+            __syncwarp();
+            for (int r = 0; r < DB; ++r) dout[(size_t)(c0 / DB) * DB * DB + r * DB + lane] = V[r][lane];
         }
         __syncthreads();
-        const double piv = D[j][j];
-        for (int i = j + 1 + tid; i < w; i += PT) D[i][j] /= piv;
+        // rows below the block within the panel: X = P V^T, X[r][j] = sum_{m <= j} P[r][m] V[j][m]
+        const int rb = c0 + bw, nr = w - rb;
+        for (int q = tid; q < nr * bw; q += PT) {
+            const int r = q % nr, j = q / nr;
+            double sum = 0.0;
+            for (int m = 0; m <= j; ++m) sum += D[rb + r][c0 + m] * V[j][m];
+            T[r][j] = sum;
+        }
         __syncthreads();
-        const int m = w - j - 1;
-        for (int q = tid; q < m * m; q += PT) {
-            const int i = j + 1 + q % m, c = j + 1 + q / m;
-            if (i >= c) D[i][c] -= D[i][j] * D[c][j];
+        for (int q = tid; q < nr * bw; q += PT) {
+            const int r = q % nr, j = q / nr;
+            D[rb + r][c0 + j] = T[r][j];
+        }
+        __syncthreads();
+        // rest of the panel block: D[i][j] -= sum_m X[i][m] X[j][m], i >= j >= rb
+        for (int q = tid; q < nr * nr; q += PT) {
+            const int i = rb + q % nr, j = rb + q / nr;
+            if (i < j) continue;
+            double sum = 0.0;
+            for (int m = 0; m < bw; ++m) sum += D[i][c0 + m] * D[j][c0 + m];
+            D[i][j] -= sum;
         }
         __syncthreads();
     }
@@ -173,103 +222,65 @@ __global__ void __launch_bounds__(PT) diag_kernel(const Item *items, const SubD 
     }
 }
 
-// Row blocks below the diagonal block: P := P L_kk^-T, column by column.
-__global__ void __launch_bounds__(PT) trsm_kernel(const Item *items, int nitems, const SubD *subs, double *arena) {
+// Row blocks below the diagonal block: X = P L_kk^-T by 32-column blocks,
+// X_b = (P_b - sum_{c < b} X_c L_bc^T) V_b^T with the inverted diagonal blocks V_b of diag_kernel.
+constexpr int TSM = (TE * (PW + 1) + DB * (PW + 1) + DB * (DB + 1) + TE * (DB + 1)) * (int)sizeof(double);
+
+__global__ void __launch_bounds__(PT) trsm_kernel(const Item *items, int nitems, const SubD *subs, double *arena,
+                                                  const double *dinv) {
     extern __shared__ double tsm[];
-    double(*D)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(tsm);
-    double(*P)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(tsm + NB * (NB + 1));
+    double(*P)[PW + 1] = reinterpret_cast<double(*)[PW + 1]>(tsm);
+    double(*Lb)[PW + 1] = reinterpret_cast<double(*)[PW + 1]>(tsm + TE * (PW + 1));
+    double(*V)[DB + 1] = reinterpret_cast<double(*)[DB + 1]>(tsm + (TE + DB) * (PW + 1));
+    double(*T)[DB + 1] = reinterpret_cast<double(*)[DB + 1]>(tsm + (TE + DB) * (PW + 1) + DB * (DB + 1));
     const int b = blockIdx.x, tid = threadIdx.x;
-    const Item it = items[find_item<0>(items, nitems, b)];
+    const int ii = find_item<0>(items, nitems, b);
+    const Item it = items[ii];
     const SubD sd = subs[it.sub];
     double *A = arena + sd.a;
     const size_t ld = sd.ld;
     const int k0 = it.k0, w = it.w;
-    const int row0 = k0 + w + NB * (b - it.trs0);
-    const int rows = min(NB, it.rend - row0);
-    for (int q = tid; q < w * w; q += PT) {
-        const int i = q % w, j = q / w;
-        if (i >= j) D[i][j] = A[(size_t)(k0 + j) * ld + k0 + i];
+    const int row0 = k0 + w + TE * (b - it.trs0);
+    const int rows = min(TE, it.rend - row0);
+    const double *vin = dinv + (size_t)ii * (PW / DB) * DB * DB;
+    for (int q = tid; q < TE * w; q += PT) {
+        const int r = q % TE, j = q / TE;
+        P[r][j] = r < rows ? A[(size_t)(k0 + j) * ld + row0 + r] : 0.0;
     }
-    for (int q = tid; q < NB * w; q += PT) {
-        const int r = q % NB, j = q / NB;
-        if (r < rows) P[r][j] = A[(size_t)(k0 + j) * ld + row0 + r];
-    }
-    __syncthreads();
-    for (int j = 0; j < w; ++j) {
-        if (tid < rows) P[tid][j] /= D[j][j];
+    for (int c0 = 0; c0 < w; c0 += DB) {
+        const int bw = min(DB, w - c0);
+        // rows c0.. of the factor block (columns < c0 + bw) and the inverse of its diagonal block
+        for (int q = tid; q < bw * (c0 + bw); q += PT) {
+            const int r = q % bw, c = q / bw;
+            Lb[r][c] = A[(size_t)(k0 + c) * ld + k0 + c0 + r];
+        }
+        for (int q = tid; q < DB * DB; q += PT) V[q / DB][q % DB] = vin[(size_t)(c0 / DB) * DB * DB + q];
         __syncthreads();
-        const int m = w - j - 1;
-        for (int q = tid; q < NB * m; q += PT) {
-            const int r = q % NB, c = j + 1 + q / NB;
-            if (r < rows) P[r][c] -= P[r][j] * D[c][j];
+        for (int q = tid; q < TE * bw; q += PT) {
+            const int r = q % TE, m = q / TE;
+            double sum = P[r][c0 + m];
+            for (int c = 0; c < c0; ++c) sum -= P[r][c] * Lb[m][c];
+            T[r][m] = sum;
+        }
+        __syncthreads();
+        for (int q = tid; q < TE * bw; q += PT) {
+            const int r = q % TE, j = q / TE;
+            double sum = 0.0;
+            for (int m = 0; m <= j; ++m) sum += T[r][m] * V[j][m];
+            P[r][c0 + j] = sum;
         }
         __syncthreads();
     }
-    for (int q = tid; q < NB * w; q += PT) {
-        const int r = q % NB, j = q / NB;
+    for (int q = tid; q < TE * w; q += PT) {
+        const int r = q % TE, j = q / TE;
         if (r < rows) A[(size_t)(k0 + j) * ld + row0 + r] = P[r][j];
     }
 }
 
-// Trailing update of the lower tiles: A_IJ -= L_I L_J^T (w-deep), 4 x 4 outputs per thread.
-__global__ void __launch_bounds__(PT) update_kernel(const Item *items, int nitems, const SubD *subs, double *arena) {
-    extern __shared__ double usm[];
-    double *LI = usm, *LJ = usm + NB * NB;
-    const int b = blockIdx.x, tid = threadIdx.x;
-    const Item it = items[find_item<1>(items, nitems, b)];
-    const SubD sd = subs[it.sub];
-    double *A = arena + sd.a;
-    const size_t ld = sd.ld;
-    const int t = b - it.upd0;
-    int I = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
-    while ((I + 1) * (I + 2) / 2 <= t) ++I;
-    while (I * (I + 1) / 2 > t) --I;
-    const int J = t - I * (I + 1) / 2;
-    const int k0 = it.k0, w = it.w;
-    const int r0 = k0 + w;
-    const int rI = r0 + NB * I, rJ = r0 + NB * J;
-    const int nI = min(NB, it.rend - rI), nJ = min(NB, it.rend - rJ);
-    for (int q = tid; q < NB * w; q += PT) {
-        const int i = q % NB, k = q / NB;
-        const double *col = A + (size_t)(k0 + k) * ld;
-        LI[k * NB + i] = i < nI ? col[rI + i] : 0.0;
-        LJ[k * NB + i] = i < nJ ? col[rJ + i] : 0.0;
-    }
-    __syncthreads();
-    const int tx = tid & 15, ty = tid >> 4;
-    double acc[4][4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) acc[u][v] = 0.0;
-    for (int k = 0; k < w; ++k) {
-        double a[4], c[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            a[u] = LI[k * NB + tx + 16 * u];
-            c[u] = LJ[k * NB + ty + 16 * u];
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-#pragma unroll
-            for (int v = 0; v < 4; ++v) acc[u][v] = fma(a[u], c[v], acc[u][v]);
-    }
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-        const int j = ty + 16 * v;
-        if (j >= nJ) continue;
-        double *col = A + (size_t)(rJ + j) * ld + rI;
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int i = tx + 16 * u;
-            if (i < nI && (I != J || i >= j)) col[i] -= acc[u][v];
-        }
-    }
-}
-
-// The same update on the FP64 tensor-core path (mma.m8n8k4.f64): eight warps, each a 32 x 16
-// block of the tile as 4 x 2 fragments of 8 x 8.  Panels are staged k-major with a stride of 72
-// doubles (8 mod 16), so the 8 x 4 fragment loads take the minimum of two shared-memory wavefronts.
+// Trailing update A_IJ -= L_Ik L_Jk^T of one 64 x 64 lower tile on the FP64 tensor-core path
+// (mma.m8n8k4.f64): eight warps, each a 32 x 16 block of the tile as 4 x 2 fragments of 8 x 8.
+// Panels are staged k-major with a stride of 72 doubles (8 mod 16), so the 8 x 4 fragment loads take
+// the minimum of two shared-memory wavefronts.
 constexpr int LDS = 72;
 
 __device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
@@ -278,10 +289,21 @@ __device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
                  : "d"(a), "d"(b));
 }
 
-__global__ void __launch_bounds__(PT) update_mma_kernel(const Item *items, int nitems, const SubD *subs,
-                                                        double *arena) {
-    extern __shared__ double msm[];
-    double *LI = msm, *LJ = msm + NB * LDS;
+// The panels stream through shared memory in k-chunks of 16 with cp.async
+// (two buffers, the next chunk in flight while the current one feeds the MMAs; rows beyond the
+// block and k beyond w are zero-filled by the copy), and the C tile is loaded into registers before
+// the first chunk so that its latency overlaps the staging.
+constexpr int KCH = 16;
+
+__device__ __forceinline__ void cp_async8(double *dst, const double *src, bool valid) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    const int n = valid ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
+
+__global__ void __launch_bounds__(PT, 2) update_pipe_kernel(const Item *items, int nitems, const SubD *subs,
+                                                         double *arena) {
+    __shared__ double buf[2][2][KCH][LDS];   // [stage][panel I / J][k][row]
     const int b = blockIdx.x, tid = threadIdx.x;
     const Item it = items[find_item<1>(items, nitems, b)];
     const SubD sd = subs[it.sub];
@@ -292,38 +314,73 @@ __global__ void __launch_bounds__(PT) update_mma_kernel(const Item *items, int n
     while ((I + 1) * (I + 2) / 2 <= t) ++I;
     while (I * (I + 1) / 2 > t) --I;
     const int J = t - I * (I + 1) / 2;
-    const int k0 = it.k0, w = it.w, w4 = (it.w + 3) & ~3;
+    const int k0 = it.k0, w = it.w;
     const int r0 = k0 + w;
-    const int rI = r0 + NB * I, rJ = r0 + NB * J;
-    const int nI = min(NB, it.rend - rI), nJ = min(NB, it.rend - rJ);
-    for (int q = tid; q < NB * w4; q += PT) {
-        const int i = q % NB, k = q / NB;
-        const double *col = A + (size_t)(k0 + k) * ld;
-        const bool kin = k < w;
-        LI[k * LDS + i] = (kin && i < nI) ? col[rI + i] : 0.0;
-        LJ[k * LDS + i] = (kin && i < nJ) ? col[rJ + i] : 0.0;
-    }
-    __syncthreads();
+    const int rI = r0 + TE * I, rJ = r0 + TE * J;
+    const int nI = min(TE, it.rend - rI), nJ = min(TE, it.rend - rJ);
+    const int nch = (w + KCH - 1) / KCH;
+    // chunk c: 2 panels x 16 k x 64 rows = 2048 doubles, 8 per thread
+    // thread tid copies row i = tid % 64 of both panels at k = tid / 64 + 4 u, u = 0..3
+    const int ci = tid & (TE - 1), ck = tid >> 6;
+    const bool okI = ci < nI, okJ = ci < nJ;
+    const double *srcI = A + (size_t)k0 * ld + rI + ci, *srcJ = A + (size_t)k0 * ld + rJ + ci;
+    auto issue = [&](int c) {
+        const int st = c & 1;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int kk = ck + 4 * u, k = c * KCH + kk;
+            const bool kin = k < w;
+            const size_t o = kin ? (size_t)k * ld : 0;
+            // a copy that is switched off reads nothing; its address is the matrix start regardless
+            cp_async8(&buf[st][0][kk][ci], (kin && okI) ? srcI + o : A, kin && okI);
+            cp_async8(&buf[st][1][kk][ci], (kin && okJ) ? srcJ + o : A, kin && okJ);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    issue(0);
+    if (nch > 1) issue(1);
     const int lane = tid & 31, warp = tid >> 5;
     const int wm = warp & 1, wn = warp >> 1;
     const int g = lane >> 2, q4 = lane & 3;
+    // the C tile in the accumulator layout, loaded while the first chunks are in flight
+    double cv[4][2][2];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        const int r = wm * 32 + m * 8 + g;
+#pragma unroll
+        for (int n = 0; n < 2; ++n)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int c = wn * 16 + n * 8 + 2 * q4 + h;
+                cv[m][n][h] = (r < nI && c < nJ) ? A[(size_t)(rJ + c) * ld + rI + r] : 0.0;
+            }
+    }
     double acc[4][2][2];
 #pragma unroll
     for (int m = 0; m < 4; ++m)
 #pragma unroll
         for (int n = 0; n < 2; ++n) acc[m][n][0] = acc[m][n][1] = 0.0;
-    for (int k = 0; k < w4; k += 4) {
-        const double *la = LI + (k + q4) * LDS + wm * 32 + g;
-        const double *lb = LJ + (k + q4) * LDS + wn * 16 + g;
-        double a[4], c[2];
+    for (int c = 0; c < nch; ++c) {
+        if (c + 1 < nch) asm volatile("cp.async.wait_group 1;" ::: "memory");
+        else asm volatile("cp.async.wait_group 0;" ::: "memory");
+        __syncthreads();
+        const int st = c & 1;
 #pragma unroll
-        for (int m = 0; m < 4; ++m) a[m] = la[m * 8];
+        for (int kk = 0; kk < KCH; kk += 4) {
+            const double *la = &buf[st][0][kk + q4][wm * 32 + g];
+            const double *lb = &buf[st][1][kk + q4][wn * 16 + g];
+            double a[4], bb[2];
 #pragma unroll
-        for (int n = 0; n < 2; ++n) c[n] = lb[n * 8];
+            for (int m = 0; m < 4; ++m) a[m] = la[m * 8];
 #pragma unroll
-        for (int m = 0; m < 4; ++m)
+            for (int n = 0; n < 2; ++n) bb[n] = lb[n * 8];
 #pragma unroll
-            for (int n = 0; n < 2; ++n) dmma(acc[m][n], a[m], c[n]);
+            for (int m = 0; m < 4; ++m)
+#pragma unroll
+                for (int n = 0; n < 2; ++n) dmma(acc[m][n], a[m], bb[n]);
+        }
+        __syncthreads();
+        if (c + 2 < nch) issue(c + 2);
     }
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
@@ -333,7 +390,8 @@ __global__ void __launch_bounds__(PT) update_mma_kernel(const Item *items, int n
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int c = wn * 16 + n * 8 + 2 * q4 + h;
-                if (r < nI && c < nJ && (I != J || r >= c)) A[(size_t)(rJ + c) * ld + rI + r] -= acc[m][n][h];
+                if (r < nI && c < nJ && (I != J || r >= c))
+                    A[(size_t)(rJ + c) * ld + rI + r] = cv[m][n][h] - acc[m][n][h];
             }
     }
 }
@@ -364,6 +422,7 @@ __global__ void copy_sym_kernel(const JobD *jobs, const SubD *subs, const double
 // packed lower factor of the leading n x n block: column j holds rows j..n-1
 __global__ void pack_kernel(const JobD *jobs, const SubD *subs, const double *arena, double *stage) {
     const JobD J = jobs[blockIdx.y];
+    if (J.lp < 0) return;
     const SubD sd = subs[J.sub];
     const double *A = arena + sd.a;
     for (int j = blockIdx.x; j < J.n; j += gridDim.x) {
@@ -497,9 +556,9 @@ struct BItem {
 
 __global__ void __launch_bounds__(PT) bsolve_kernel(const BItem *items, int nitems, const SubD *subs,
                                                     const double *arena, double *X, double *Y) {
-    __shared__ double D[NB][NB + 1];    // L_JJ (lower), or the tile L(J rows, i columns)
-    __shared__ double x[NB][8];
-    __shared__ double y[NB][8];
+    __shared__ double D[BS][BS + 1];    // L_JJ (lower), or the tile L(J rows, i columns)
+    __shared__ double x[BS][8];
+    __shared__ double y[BS][8];
     int lo = 0, hi = nitems - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
@@ -511,11 +570,11 @@ __global__ void __launch_bounds__(PT) bsolve_kernel(const BItem *items, int nite
     const double *A = arena + sd.a;
     const int tid = threadIdx.x, w = it.w, nk = it.nk, c0 = it.c0;
     const int l = blockIdx.x - it.cta0;
-    const int below = (c0 + NB - 1) / NB;
+    const int below = (c0 + BS - 1) / BS;
     double *Xs = X + it.xo, *Ys = Y + it.xo;
     if (it.given) {
-        for (int q = tid; q < NB * nk; q += PT) {
-            const int r = q % NB, k = q / NB;
+        for (int q = tid; q < BS * nk; q += PT) {
+            const int r = q % BS, k = q / BS;
             x[r][k] = r < w ? Xs[(size_t)k * it.n + c0 + r] : 0.0;
         }
     } else {
@@ -523,8 +582,8 @@ __global__ void __launch_bounds__(PT) bsolve_kernel(const BItem *items, int nite
             const int i = q % w, j = q / w;
             if (i >= j) D[i][j] = A[(size_t)(c0 + j) * sd.ld + c0 + i];
         }
-        for (int q = tid; q < NB * nk; q += PT) {
-            const int r = q % NB, k = q / NB;
+        for (int q = tid; q < BS * nk; q += PT) {
+            const int r = q % BS, k = q / BS;
             y[r][k] = r < w ? Ys[(size_t)k * it.n + c0 + r] : 0.0;
         }
         __syncthreads();
@@ -547,17 +606,17 @@ __global__ void __launch_bounds__(PT) bsolve_kernel(const BItem *items, int nite
     }
     __syncthreads();
     // y_i -= L(J rows, i columns)^T x_J, i = block l: columns 64 l .. min(64 l + 64, c0) - 1
-    const int cm = min(NB, c0 - NB * l);
+    const int cm = min(BS, c0 - BS * l);
     for (int q = tid; q < cm * w; q += PT) {
         const int r = q % w, c = q / w;
-        D[r][c] = A[(size_t)(NB * l + c) * sd.ld + c0 + r];
+        D[r][c] = A[(size_t)(BS * l + c) * sd.ld + c0 + r];
     }
     __syncthreads();
     for (int q = tid; q < cm * nk; q += PT) {
         const int c = q % cm, k = q / cm;
         double sum = 0.0;
         for (int r = 0; r < w; ++r) sum += D[r][c] * x[r][k];
-        Ys[(size_t)k * it.n + NB * l + c] -= sum;
+        Ys[(size_t)k * it.n + BS * l + c] -= sum;
     }
 }
 
@@ -590,24 +649,24 @@ struct Step {
     int ntrs = 0, nupd = 0;
 };
 
-// Steps of one phase: columns [lo(job), hi(job)) in NB panels, rows below up to rend(job).
+// Steps of one phase: columns [lo(job), hi(job)) in PW panels, rows below up to rend(job).
 template <typename Lo, typename Hi, typename Rend>
 std::vector<Step> make_steps(int njobs, Lo lo, Hi hi, Rend rend, double &flops) {
     std::vector<Step> steps;
     for (int s = 0;; ++s) {
         Step st;
         for (int j = 0; j < njobs; ++j) {
-            const int k0 = lo(j) + s * NB;
+            const int k0 = lo(j) + s * PW;
             if (k0 >= hi(j)) continue;
             Item it;
             it.sub = j;
             it.k0 = k0;
-            it.w = std::min(NB, hi(j) - k0);
+            it.w = std::min(PW, hi(j) - k0);
             it.rend = rend(j);
             it.trs0 = st.ntrs;
             it.upd0 = st.nupd;
             const int below = it.rend - k0 - it.w;
-            const int nb = below > 0 ? (below + NB - 1) / NB : 0;
+            const int nb = below > 0 ? (below + TE - 1) / TE : 0;
             st.ntrs += nb;
             st.nupd += nb * (nb + 1) / 2;
             st.items.push_back(it);
@@ -676,14 +735,8 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
         PCHECK(cudaMemGetInfo(&fr, &tot));
         mem_budget = fr / 2;
     }
-    PCHECK(cudaFuncSetAttribute(trsm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(2 * NB * (NB + 1) * sizeof(double))));
-    PCHECK(cudaFuncSetAttribute(update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(2 * NB * NB * sizeof(double))));
-    PCHECK(cudaFuncSetAttribute(update_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(2 * NB * LDS * sizeof(double))));
-    const char *simt_env = std::getenv("FETI4I_DEVICE_PREP_SIMT");
-    const bool simt = simt_env && simt_env[0] == '1';
+    PCHECK(cudaFuncSetAttribute(diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, DSM));
+    PCHECK(cudaFuncSetAttribute(trsm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TSM));
 
     // per-job sizes and batches
     struct Sz {
@@ -698,8 +751,8 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
         z.N = J.n + J.ni;
         z.ld = (z.N + 31) / 32 * 32;
         z.a = (size_t)z.ld * z.N;
-        z.lp = resident ? 0 : (size_t)J.n * (J.n + 1) / 2;
-        z.s = resident ? 0 : (size_t)J.ni * J.ni;
+        z.lp = (resident || !J.Lp) ? 0 : (size_t)J.n * (J.n + 1) / 2;
+        z.s = (resident || !J.S) ? 0 : (size_t)J.ni * J.ni;
         z.sd = (J.want_sdir && !resident) ? (size_t)(J.n - J.n1) * (J.n - J.n1) : 0;
         z.fx = (size_t)J.ns * J.ns;
         z.vals = 0;
@@ -726,7 +779,7 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
         bstart.push_back(nj);
     }
 
-    DevBuf<double> arena, stage, fxb, vals, bsign, reg, part, dX, dY;
+    DevBuf<double> arena, stage, fxb, vals, bsign, reg, part, dX, dY, dinvb;
     DevBuf<TJob> dtj;
     DevBuf<BItem> dbi;
     DevBuf<int> epos, bpos, fail, list;
@@ -745,8 +798,19 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
         }
     } evg{ev0, ev1};
     constexpr int KN_BLOCKS = 64;
+    double *pinned = nullptr;   // staging of the element values
+    size_t pinned_n = 0;
+    struct PinGuard {
+        double *&p;
+        ~PinGuard() {
+            if (p) cudaFreeHost(p);
+        }
+    } ping{pinned};
 
+    double th_setup = now_s() - t_start, th_stage = 0.0, th_wait = 0.0, th_reg = 0.0, th_out = 0.0;
+    double th_gather = 0.0, th_h2d = 0.0;
     for (size_t bi = 0; bi + 1 < bstart.size(); ++bi) {
+        double tq = now_s();
         const int j0 = bstart[bi], j1 = bstart[bi + 1], nb = j1 - j0;
         // layout of the batch
         std::vector<SubD> subs(nb);
@@ -766,9 +830,9 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
             d.ns = J.ns;
             d.boff = (long long)b_tot;
             b_tot += J.ni;
-            d.lp = (long long)st_tot;
+            d.lp = z.lp ? (long long)st_tot : -1;
             st_tot += z.lp;
-            d.s = (long long)st_tot;
+            d.s = z.s ? (long long)st_tot : -1;
             st_tot += z.s;
             d.sd = J.want_sdir ? (long long)st_tot : -1;
             st_tot += z.sd;
@@ -778,8 +842,8 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
             p_tot += z.pos;
         }
         // element data, colour lists, B~ rows
-        std::vector<double> hv;
-        hv.reserve(v_tot);
+        size_t hv_n = 0;
+        std::vector<const double *> src;   // K_e of every batch element (gathered in parallel below)
         std::vector<int> hp;
         hp.reserve(p_tot);
         std::vector<ElemD> he;
@@ -797,12 +861,12 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
                 const int e = J.elems[k];
                 const int nd = (int)(el.dof_ptr[e + 1] - el.dof_ptr[e]);
                 ElemD E;
-                E.val = (long long)hv.size();
+                E.val = (long long)hv_n;
                 E.nd = nd;
                 E.pos = (int)(hp.size());
                 E.sub = q;
-                const double *Ke = el.vals.data() + el.val_ptr[e];
-                hv.insert(hv.end(), Ke, Ke + (size_t)nd * nd);
+                src.push_back(el.vals.data() + el.val_ptr[e]);
+                hv_n += (size_t)nd * nd;
                 hp.insert(hp.end(), J.elpos.begin() + po, J.elpos.begin() + po + nd);
                 po += nd;
                 colors[J.elcolor[k]].push_back((int)he.size());
@@ -822,7 +886,26 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
         arena.reserve(a_tot);
         stage.reserve(st_tot);
         fxb.reserve(fx_tot);
-        vals.put(hv);
+        // element values: parallel gather into pinned memory, one copy to the device
+        const double tg0 = now_s();
+        if (hv_n > pinned_n) {
+            if (pinned) PCHECK(cudaFreeHost(pinned));
+            pinned = nullptr;
+            pinned_n = 0;
+            PCHECK(cudaMallocHost(&pinned, hv_n * sizeof(double)));
+            pinned_n = hv_n;
+        }
+        {
+            const long long ne_ = (long long)he.size();
+#pragma omp parallel for schedule(static)
+            for (long long k = 0; k < ne_; ++k)
+                std::memcpy(pinned + he[k].val, src[k], sizeof(double) * (size_t)he[k].nd * he[k].nd);
+        }
+        const double tg1 = now_s();
+        vals.reserve(hv_n);
+        if (hv_n) PCHECK(cudaMemcpy(vals.p, pinned, hv_n * sizeof(double), cudaMemcpyHostToDevice));
+        th_gather += tg1 - tg0;
+        th_h2d += now_s() - tg1;
         epos.put(hp);
         dels.put(he);
         list.put(hl);
@@ -855,10 +938,23 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
         };
         std::vector<size_t> o1 = offsets(ph1), o2 = offsets(ph2), o3 = offsets(ph3);
         ditems.put(all);
+        size_t maxitems = 0;   // inverted 32 x 32 diagonal blocks of the largest step
+        for (auto *ph : {&ph1, &ph2, &ph3})
+            for (auto &st : *ph) maxitems = std::max(maxitems, st.items.size());
+        dinvb.reserve(std::max<size_t>(maxitems, 1) * (PW / DB) * DB * DB);
         tm.flops += flops;
 
+        th_stage += now_s() - tq;
+        tq = now_s();
         PCHECK(cudaEventRecord(ev0));
         PCHECK(cudaMemset(arena.p, 0, a_tot * sizeof(double)));
+        for (int q = 0; q < nb; ++q) {
+            const DevFactorJob &J = jobs[j0 + q];
+            if (!J.dense) continue;
+            PCHECK(cudaMemcpy2D(arena.p + subs[q].a, (size_t)subs[q].ld * sizeof(double), J.dense,
+                                (size_t)J.n * sizeof(double), (size_t)J.n * sizeof(double), J.n,
+                                cudaMemcpyHostToDevice));
+        }
         for (auto &c : cl) {
             if (c.second == 0) continue;
             assemble_kernel<<<std::min(c.second, 65535), 128>>>(dels.p, list.p + c.first, c.second, vals.p, epos.p,
@@ -873,18 +969,14 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
             for (size_t s = 0; s < ph.size(); ++s) {
                 const Item *it = ditems.p + off[s];
                 const int ni = (int)ph[s].items.size();
-                diag_kernel<<<ni, PT>>>(it, dsubs.p, arena.p, fail.p);
+                diag_kernel<<<ni, PT, DSM>>>(it, dsubs.p, arena.p, fail.p, dinvb.p);
                 ++tm.launches;
                 if (ph[s].ntrs > 0) {
-                    trsm_kernel<<<ph[s].ntrs, PT, 2 * NB * (NB + 1) * sizeof(double)>>>(it, ni, dsubs.p, arena.p);
+                    trsm_kernel<<<ph[s].ntrs, PT, TSM>>>(it, ni, dsubs.p, arena.p, dinvb.p);
                     ++tm.launches;
                 }
                 if (ph[s].nupd > 0) {
-                    if (simt)
-                        update_kernel<<<ph[s].nupd, PT, 2 * NB * NB * sizeof(double)>>>(it, ni, dsubs.p, arena.p);
-                    else
-                        update_mma_kernel<<<ph[s].nupd, PT, 2 * NB * LDS * sizeof(double)>>>(it, ni, dsubs.p,
-                                                                                              arena.p);
+                    update_pipe_kernel<<<ph[s].nupd, PT>>>(it, ni, dsubs.p, arena.p);
                     ++tm.launches;
                 }
             }
@@ -930,6 +1022,8 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
         PCHECK(cudaGetLastError());
         PCHECK(cudaEventRecord(ev1));
         PCHECK(cudaEventSynchronize(ev1));
+        th_wait += now_s() - tq;
+        tq = now_s();
         float ms = 0.f;
         PCHECK(cudaEventElapsedTime(&ms, ev0, ev1));
         tm.device_ms += ms;
@@ -941,6 +1035,8 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
         for (int q = 0; q < nb; ++q)
             if (jobs[j0 + q].ns > 0 && hf[q] == INT_MAX) regularise(j0 + q, hfx.data() + jd[q].fx, hreg.data() + jd[q].fx);
         reg.put(hreg);
+        th_reg += now_s() - tq;
+        tq = now_s();
         PCHECK(cudaEventRecord(ev0));
         add_reg_kernel<<<nb, 64>>>(djobs.p, dsubs.p, arena.p, reg.p);
         ++tm.launches;
@@ -959,7 +1055,7 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
                 FETI_CHECK(J.nk >= 0 && J.nk <= 8, "FETI4I: kernel dimension above 8");
                 xo[q] = (long long)x_tot;
                 x_tot += (size_t)J.n * J.nk;
-                maxb = std::max(maxb, (J.n - J.ns + NB - 1) / NB);
+                maxb = std::max(maxb, (J.n - J.ns + BS - 1) / BS);
             }
             std::vector<double> hx(std::max<size_t>(x_tot, 1), 0.0);
             for (int q = 0; q < nb; ++q) {
@@ -977,7 +1073,7 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
                 for (int q = 0; q < nb; ++q) {
                     const DevFactorJob &J = jobs[j0 + q];
                     if (J.nk == 0) continue;
-                    const int nr = J.n - J.ns, nbr = (nr + NB - 1) / NB;
+                    const int nr = J.n - J.ns, nbr = (nr + BS - 1) / BS;
                     BItem b;
                     b.sub = q;
                     b.nk = J.nk;
@@ -993,8 +1089,8 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
                     } else {
                         const int blk = nbr - step;
                         if (blk < 0) continue;
-                        b.c0 = NB * blk;
-                        b.w = std::min(NB, nr - b.c0);
+                        b.c0 = BS * blk;
+                        b.w = std::min(BS, nr - b.c0);
                         b.given = 0;
                         cnt = blk + 1;
                     }
@@ -1022,6 +1118,8 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
         }
         PCHECK(cudaEventRecord(ev1));
         PCHECK(cudaEventSynchronize(ev1));
+        th_wait += now_s() - tq;
+        tq = now_s();
         PCHECK(cudaEventElapsedTime(&ms, ev0, ev1));
         tm.device_ms += ms;
 
@@ -1048,9 +1146,13 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
             if (J.want_sdir && J.Sdir)
                 PCHECK(cudaMemcpy(J.Sdir, stage.p + jd[q].sd, sz[j0 + q].sd * sizeof(double), cudaMemcpyDeviceToHost));
         }
+        th_out += now_s() - tq;
         ++tm.batches;
     }
     tm.total_s = now_s() - t_start;
+    FETI_LOG(2, "FETI4I: device factorisation: setup %.3f s, staging %.3f s (element gather %.3f s, copy %.3f s), "
+                "device waits %.3f s, fix blocks %.3f s, results %.3f s\n", th_setup, th_stage, th_gather, th_h2d,
+             th_wait, th_reg, th_out);
     if (times) *times = tm;
 }
 

@@ -44,6 +44,7 @@ struct DevFactorJob {
     int n1 = 0;                  // untouched DOFs (eliminated first)
     int ns = 0;                  // fix DOFs (eliminated last)
     int ni = 0;                  // rows of B_i
+    const double *dense = nullptr;  // instead of elements: the n x n matrix itself (column-major)
     const int *elems = nullptr;  // element ids of the subdomain (into ElementData)
     int nelem = 0;
     std::vector<int> elpos;      // factor position of every element DOF, element after element

@@ -633,14 +633,33 @@ void preprocess(const ElementData &el, Decomposition &dec, const std::vector<dou
             }
         }
     }
-    int info = dense::potrf_lower(GG.data(), nK, nK, nK);
-    FETI_CHECK(info == 0, "FETI4I: the coarse problem G G^T is singular");
-    std::vector<double> Wc((size_t)nK * nK, 0.0);
-    for (int j = 0; j < nK; ++j)
-        for (int i = j; i < nK; ++i) Wc[(size_t)j * nK + i] = GG[(size_t)j * nK + i];
-    dense::trtri_lower(Wc.data(), nK, nK);
     out.GGt_inv.assign((size_t)nK * nK, 0.0);
-    dense::lauum_lower(Wc.data(), nK, nK, out.GGt_inv.data(), nK);
+    if (opt.device && nK > 0) {
+        // (G G^T)^-1 as the trailing block of the eliminated [G G^T I; I 0] on the device
+        std::vector<DevFactorJob> cj(1);
+        DevFactorJob &J = cj[0];
+        J.n = nK;
+        J.ni = nK;
+        J.dense = GG.data();
+        J.bpos.resize(nK);
+        std::iota(J.bpos.begin(), J.bpos.end(), 0);
+        J.bsign.assign(nK, 1.0);
+        J.S = out.GGt_inv.data();
+        DevFactorTimes ct;
+        device_factor(el, cj, [](int, const double *, double *) {}, 0, &ct);
+        FETI_CHECK(J.fail_col < 0, "FETI4I: the coarse problem G G^T is singular");
+        out.t_device_factor_ms += ct.device_ms;
+        out.device_factor_flops += ct.flops;
+        out.device_factor_launches += ct.launches;
+    } else {
+        int info = dense::potrf_lower(GG.data(), nK, nK, nK);
+        FETI_CHECK(info == 0, "FETI4I: the coarse problem G G^T is singular");
+        std::vector<double> Wc((size_t)nK * nK, 0.0);
+        for (int j = 0; j < nK; ++j)
+            for (int i = j; i < nK; ++i) Wc[(size_t)j * nK + i] = GG[(size_t)j * nK + i];
+        dense::trtri_lower(Wc.data(), nK, nK);
+        dense::lauum_lower(Wc.data(), nK, nK, out.GGt_inv.data(), nK);
+    }
     out.t_coarse = now_s() - t1;
     FETI_LOG(2, "FETI4I: coarse problem %.3f s\n", out.t_coarse);
 }
