@@ -57,6 +57,9 @@ struct ElemD {
 
 struct JobD {
     int sub, n, n1, nc, ni, ns;
+    int nrow;             // appended rows (B and B0)
+    int m0;               // B0 rows
+    long long vo;         // offset of the [B; B0] K^+ B0^T block in the staging buffer, -1 without B0
     long long boff;       // offset of its B~ rows in bpos / bsign
     long long lp, s, sd;  // offsets of its outputs in the staging buffer (doubles)
     long long fx;         // offset of its fix-DOF block in the fix buffer
@@ -100,7 +103,7 @@ __global__ void brows_kernel(const JobD *jobs, const SubD *subs, const int *bpos
     const JobD J = jobs[blockIdx.y];
     const SubD sd = subs[J.sub];
     double *A = arena + sd.a;
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < J.ni; r += gridDim.x * blockDim.x)
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < J.nrow; r += gridDim.x * blockDim.x)
         A[(size_t)bpos[J.boff + r] * sd.ld + J.n + r] = bsign[J.boff + r];
 }
 
@@ -416,6 +419,22 @@ __global__ void copy_sym_kernel(const JobD *jobs, const SubD *subs, const double
         const int j = (int)(q / m), i = (int)(q - (long long)j * m);
         const double v = i >= j ? A[(size_t)(r0 + j) * sd.ld + r0 + i] : A[(size_t)(r0 + i) * sd.ld + r0 + j];
         dst[off + q] = scale * v;
+    }
+}
+
+// -[B; B0] K^+ B0^T: rows n .. n + ni + m0 - 1, columns n + ni .. n + ni + m0 - 1 of the symmetric
+// trailing block, (ni + m0) x m0 column-major
+__global__ void copy_b0_kernel(const JobD *jobs, const SubD *subs, const double *arena, double *stage) {
+    const JobD J = jobs[blockIdx.y];
+    if (J.vo < 0) return;
+    const SubD sd = subs[J.sub];
+    const double *A = arena + sd.a;
+    const int rows = J.ni + J.m0;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < rows * J.m0; q += gridDim.x * blockDim.x) {
+        const int j = q / rows, r = q - j * rows;
+        const int gi = J.n + r, gj = J.n + J.ni + j;
+        const double v = gi >= gj ? A[(size_t)gj * sd.ld + gi] : A[(size_t)gi * sd.ld + gj];
+        stage[J.vo + q] = -v;
     }
 }
 
@@ -741,20 +760,22 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
     // per-job sizes and batches
     struct Sz {
         int ld, N;
-        size_t a, lp, s, sd, fx, vals, pos;
+        size_t a, lp, s, sd, fx, vals, pos, v;
     };
     std::vector<Sz> sz(nj);
     for (int j = 0; j < nj; ++j) {
         const DevFactorJob &J = jobs[j];
         FETI_CHECK(J.n > 0 && J.ns >= 0 && J.n1 >= 0 && J.n1 + J.ns <= J.n, "FETI4I: invalid device factorisation job");
         Sz &z = sz[j];
-        z.N = J.n + J.ni;
+        FETI_CHECK(J.b0pos.size() == J.b0sign.size(), "FETI4I: corner rows incomplete");
+        z.N = J.n + J.ni + (int)J.b0pos.size();
         z.ld = (z.N + 31) / 32 * 32;
         z.a = (size_t)z.ld * z.N;
         z.lp = (resident || !J.Lp) ? 0 : (size_t)J.n * (J.n + 1) / 2;
         z.s = (resident || !J.S) ? 0 : (size_t)J.ni * J.ni;
         z.sd = (J.want_sdir && !resident) ? (size_t)(J.n - J.n1) * (J.n - J.n1) : 0;
         z.fx = (size_t)J.ns * J.ns;
+        z.v = J.b0pos.empty() ? 0 : (size_t)(J.ni + J.b0pos.size()) * J.b0pos.size();
         z.vals = 0;
         for (int k = 0; k < J.nelem; ++k) {
             const int e = J.elems[k];
@@ -767,7 +788,7 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
     {
         size_t cur = 0;
         for (int j = 0; j < nj; ++j) {
-            const size_t bytes = 8 * (sz[j].a + sz[j].lp + sz[j].s + sz[j].sd + sz[j].fx + sz[j].vals +
+            const size_t bytes = 8 * (sz[j].a + sz[j].lp + sz[j].s + sz[j].sd + sz[j].fx + sz[j].vals + sz[j].v +
                                       (resident ? 16 * (size_t)jobs[j].n : 0)) +
                                  4 * sz[j].pos;
             if (j > bstart.back() && cur + bytes > mem_budget) {
@@ -807,6 +828,21 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
         }
     } ping{pinned};
 
+    // Element values: when the jobs use most of the element array and it takes a small share of the
+    // device memory, it goes to the device once and the assembly reads it in place.
+    bool all_vals = false;
+    {
+        size_t used = 0;
+        for (const Sz &z : sz) used += z.vals;
+        size_t fr = 0, tot = 0;
+        PCHECK(cudaMemGetInfo(&fr, &tot));
+        const size_t bytes = el.vals.size() * sizeof(double);
+        if (used > 0 && used * 2 >= el.vals.size() && bytes < fr / 8) {
+            vals.reserve(el.vals.size());
+            PCHECK(cudaMemcpy(vals.p, el.vals.data(), bytes, cudaMemcpyHostToDevice));
+            all_vals = true;
+        }
+    }
     double th_setup = now_s() - t_start, th_stage = 0.0, th_wait = 0.0, th_reg = 0.0, th_out = 0.0;
     double th_gather = 0.0, th_h2d = 0.0;
     for (size_t bi = 0; bi + 1 < bstart.size(); ++bi) {
@@ -828,14 +864,18 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
             d.nc = J.n - J.ns;
             d.ni = J.ni;
             d.ns = J.ns;
+            d.m0 = (int)J.b0pos.size();
+            d.nrow = J.ni + d.m0;
             d.boff = (long long)b_tot;
-            b_tot += J.ni;
+            b_tot += d.nrow;
             d.lp = z.lp ? (long long)st_tot : -1;
             st_tot += z.lp;
             d.s = z.s ? (long long)st_tot : -1;
             st_tot += z.s;
             d.sd = J.want_sdir ? (long long)st_tot : -1;
             st_tot += z.sd;
+            d.vo = z.v ? (long long)st_tot : -1;
+            st_tot += z.v;
             d.fx = (long long)fx_tot;
             fx_tot += z.fx;
             v_tot += z.vals;
@@ -861,7 +901,7 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
                 const int e = J.elems[k];
                 const int nd = (int)(el.dof_ptr[e + 1] - el.dof_ptr[e]);
                 ElemD E;
-                E.val = (long long)hv_n;
+                E.val = all_vals ? (long long)el.val_ptr[e] : (long long)hv_n;
                 E.nd = nd;
                 E.pos = (int)(hp.size());
                 E.sub = q;
@@ -876,6 +916,9 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
             FETI_CHECK((int)J.bpos.size() == J.ni && (int)J.bsign.size() == J.ni, "FETI4I: B rows missing");
             hbp.insert(hbp.end(), J.bpos.begin(), J.bpos.end());
             hbs.insert(hbs.end(), J.bsign.begin(), J.bsign.end());
+            for (int p : J.b0pos) FETI_CHECK(p >= J.n1 && p < J.n, "FETI4I: a corner DOF is not on the subdomain interface");
+            hbp.insert(hbp.end(), J.b0pos.begin(), J.b0pos.end());
+            hbs.insert(hbs.end(), J.b0sign.begin(), J.b0sign.end());
         }
         std::vector<int> hl;
         std::vector<std::pair<int, int>> cl;   // (offset, count) per colour
@@ -886,8 +929,10 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
         arena.reserve(a_tot);
         stage.reserve(st_tot);
         fxb.reserve(fx_tot);
-        // element values: parallel gather into pinned memory, one copy to the device
+        // element values: parallel gather into pinned memory, one copy to the device (unless the
+        // whole element array is already there)
         const double tg0 = now_s();
+        if (all_vals) hv_n = 0;
         if (hv_n > pinned_n) {
             if (pinned) PCHECK(cudaFreeHost(pinned));
             pinned = nullptr;
@@ -895,15 +940,17 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
             PCHECK(cudaMallocHost(&pinned, hv_n * sizeof(double)));
             pinned_n = hv_n;
         }
-        {
+        if (!all_vals) {
             const long long ne_ = (long long)he.size();
 #pragma omp parallel for schedule(static)
             for (long long k = 0; k < ne_; ++k)
                 std::memcpy(pinned + he[k].val, src[k], sizeof(double) * (size_t)he[k].nd * he[k].nd);
         }
         const double tg1 = now_s();
-        vals.reserve(hv_n);
-        if (hv_n) PCHECK(cudaMemcpy(vals.p, pinned, hv_n * sizeof(double), cudaMemcpyHostToDevice));
+        if (!all_vals) {
+            vals.reserve(hv_n);
+            if (hv_n) PCHECK(cudaMemcpy(vals.p, pinned, hv_n * sizeof(double), cudaMemcpyHostToDevice));
+        }
         th_gather += tg1 - tg0;
         th_h2d += now_s() - tg1;
         epos.put(hp);
@@ -1041,6 +1088,8 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
         add_reg_kernel<<<nb, 64>>>(djobs.p, dsubs.p, arena.p, reg.p);
         ++tm.launches;
         run(ph3, o3);
+        copy_b0_kernel<<<dim3(16, nb), PT>>>(djobs.p, dsubs.p, arena.p, stage.p);
+        ++tm.launches;
         std::vector<BItem> bitems;
         std::vector<std::vector<size_t>> bsteps;   // item ranges per backward-solve step
         size_t x_tot = 0;
@@ -1133,6 +1182,17 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
             double s = 0.0;
             for (int k = 0; k < KN_BLOCKS; ++k) s += hpart[(size_t)q * KN_BLOCKS + k];
             J.knorm = std::sqrt(s);
+            if (jd[q].vo >= 0 && (J.V || J.F0)) {
+                const int m0 = jd[q].m0, rows = J.ni + m0;
+                std::vector<double> blk((size_t)rows * m0);
+                PCHECK(cudaMemcpy(blk.data(), stage.p + jd[q].vo, blk.size() * sizeof(double), cudaMemcpyDeviceToHost));
+                for (int c = 0; c < m0; ++c) {
+                    if (J.V)
+                        for (int r = 0; r < J.ni; ++r) J.V[(size_t)c * J.ni + r] = blk[(size_t)c * rows + r];
+                    if (J.F0)
+                        for (int r = 0; r < m0; ++r) J.F0[(size_t)c * m0 + r] = blk[(size_t)c * rows + J.ni + r];
+                }
+            }
             if (resident) {
                 if (J.Rp && J.nk > 0) {
                     size_t o = 0;

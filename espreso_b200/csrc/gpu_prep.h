@@ -52,6 +52,12 @@ struct DevFactorJob {
     int ncolors = 0;
     std::vector<int> bpos;       // per B row: factor position of its DOF (>= n1)
     std::vector<double> bsign;   // per B row: sign
+    // Hybrid Total FETI: the corner rows B0 of the subdomain (one DOF each, factor position >= n1),
+    // appended after the B rows; the trailing block then also holds B K^+ B0^T and B0 K^+ B0^T
+    std::vector<int> b0pos;
+    std::vector<double> b0sign;
+    double *V = nullptr;         // ni x m0: B K_reg^-1 B0^T (column-major), copied back
+    double *F0 = nullptr;        // m0 x m0: B0 K_reg^-1 B0^T, copied back
     bool want_sdir = false;      // snapshot the Schur complement onto the touched DOFs
     // set by the regularisation callback: kernel dimension and the kernel eigenvectors N (ns x nk)
     int nk = 0;

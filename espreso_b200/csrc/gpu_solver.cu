@@ -2409,7 +2409,6 @@ void GpuSolver::subdomain_schur(int d, double *S) {
 
 void GpuSolver::subdomain_kplus(int d, double *x) {
     Impl &I = *impl;
-    FETI_CHECK(!I.hybrid, "FETI4I: device subdomain K+ is available for Total FETI");
     FETI_CHECK(d >= 0 && d + 1 < (int)I.h_doff.size(), "FETI4I: subdomain index out of range");
     const int o = I.h_doff[d], n = I.h_doff[d + 1] - I.h_doff[d];
     CUDA_CHECK(cudaMemsetAsync(I.d_f, 0, sizeof(double) * I.ntot, I.stream));

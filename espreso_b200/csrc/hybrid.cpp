@@ -123,13 +123,21 @@ void hybrid_prepare(const Decomposition &dec, Prep &prep, const std::vector<int>
         S.V.assign((size_t)ni * (m0 + nk), 0.0);
         F0loc[d].assign((size_t)m0 * m0, 0.0);
         B0R[d].assign((size_t)m0 * nk, 0.0);
-        std::vector<double> x(n);
-        for (int j = 0; j < m0; ++j) {
-            std::fill(x.begin(), x.end(), 0.0);
-            x[S.b0_dof[j]] = S.b0_sign[j];
-            S.kplus(x.data());
-            for (int r = 0; r < ni; ++r) S.V[(size_t)j * ni + r] = D.sign[r] * x[D.dof[r]];
-            for (int l = 0; l < m0; ++l) F0loc[d][(size_t)j * m0 + l] = S.b0_sign[l] * x[S.b0_dof[l]];
+        if (!S.BKB0.empty() || (m0 > 0 && S.Lp.empty())) {
+            // device preprocessing: both blocks come from the eliminated [K B^T B0^T; B; B0]
+            FETI_CHECK(S.BKB0.size() == (size_t)ni * m0 && S.B0KB0.size() == (size_t)m0 * m0,
+                       "FETI4I: corner blocks of the device preprocessing missing");
+            std::copy(S.BKB0.begin(), S.BKB0.end(), S.V.begin());
+            F0loc[d] = S.B0KB0;
+        } else {
+            std::vector<double> x(n);
+            for (int j = 0; j < m0; ++j) {
+                std::fill(x.begin(), x.end(), 0.0);
+                x[S.b0_dof[j]] = S.b0_sign[j];
+                S.kplus(x.data());
+                for (int r = 0; r < ni; ++r) S.V[(size_t)j * ni + r] = D.sign[r] * x[D.dof[r]];
+                for (int l = 0; l < m0; ++l) F0loc[d][(size_t)j * m0 + l] = S.b0_sign[l] * x[S.b0_dof[l]];
+            }
         }
         for (int k = 0; k < nk; ++k) {
             for (int r = 0; r < ni; ++r) S.V[(size_t)(m0 + k) * ni + r] = S.G[(size_t)k * ni + r];

@@ -435,9 +435,10 @@ static void prep_all_device(const ElementData &el, const Decomposition &dec, con
     std::vector<int> ids;   // subdomains of the device jobs, largest first
     for (int k = 0; k < nd; ++k)
         if (errors[order[k]].empty()) ids.push_back(order[k]);
-    // Total FETI keeps S_i, the Dirichlet blocks and K^+ on the device (the tile stores of the dual
-    // iteration); Hybrid Total FETI needs the host K^+ for its cluster problems and copies them back.
-    const bool resident = opt.method == 0;
+    // S_i, the Dirichlet blocks and K^+ stay on the device (the tile stores of the dual iteration);
+    // Hybrid Total FETI appends its corner rows B0, and B K^+ B0^T, B0 K^+ B0^T come back for the
+    // cluster problems.
+    const bool resident = true;
     std::shared_ptr<DevPrepStore> store = resident ? std::make_shared<DevPrepStore>() : nullptr;
     std::vector<std::vector<double>> Rps(resident ? nd : 0);
     std::vector<DevFactorJob> jobs(ids.size());
@@ -461,6 +462,16 @@ static void prep_all_device(const ElementData &el, const Decomposition &dec, con
         J.bsign = D.sign;
         J.want_sdir = opt.precond == PREC_DIRICHLET;
         J.slot = d;
+        if (!S.b0_dof.empty()) {
+            const int m0 = (int)S.b0_dof.size();
+            J.b0pos.resize(m0);
+            for (int j = 0; j < m0; ++j) J.b0pos[j] = S.pos[S.b0_dof[j]];
+            J.b0sign = S.b0_sign;
+            S.BKB0.assign((size_t)S.ni * m0, 0.0);
+            S.B0KB0.assign((size_t)m0 * m0, 0.0);
+            J.V = S.BKB0.data();
+            J.F0 = S.B0KB0.data();
+        }
         if (resident) continue;
         S.Lp.assign((size_t)S.n * (S.n + 1) / 2, 0.0);
         S.S.assign((size_t)S.ni * S.ni, 0.0);
@@ -546,6 +557,15 @@ void preprocess(const ElementData &el, Decomposition &dec, const std::vector<dou
     int nthreads = opt.threads > 0 ? opt.threads : omp_get_max_threads();
     std::vector<std::string> errors(dec.ndom);
     out.device_prep = opt.device;
+    std::vector<int> n0;
+    if (opt.method == 1) {
+        // Hybrid Total FETI: clusters glued at corners (the corner rows depend on the numbering only)
+        out.sub_cluster = opt.sub_cluster.empty() ? std::vector<int>(dec.ndom, 0) : opt.sub_cluster;
+        FETI_CHECK((int)out.sub_cluster.size() == dec.ndom,
+                   "FETI4I: the cluster partition must list one cluster per subdomain");
+        for (int c : out.sub_cluster) FETI_CHECK(c >= 0, "FETI4I: negative cluster index");
+        hybrid_corners(dec, out.sub_cluster, out, n0);
+    }
     if (opt.device) {
         DevFactorTimes dt;
         prep_all_device(el, dec, opt, out.sub, order, nthreads, errors, dt, out.dstore);
@@ -584,13 +604,7 @@ void preprocess(const ElementData &el, Decomposition &dec, const std::vector<dou
     double t1 = now_s();
     out.method = opt.method;
     if (opt.method == 1) {
-        // Hybrid Total FETI: clusters glued at corners, cluster kernels in the dual problem
-        out.sub_cluster = opt.sub_cluster.empty() ? std::vector<int>(dec.ndom, 0) : opt.sub_cluster;
-        FETI_CHECK((int)out.sub_cluster.size() == dec.ndom,
-                   "FETI4I: the cluster partition must list one cluster per subdomain");
-        for (int c : out.sub_cluster) FETI_CHECK(c >= 0, "FETI4I: negative cluster index");
-        std::vector<int> n0;
-        hybrid_corners(dec, out.sub_cluster, out, n0);
+        // Hybrid Total FETI: cluster problems and cluster kernels in the dual problem
         hybrid_prepare(dec, out, n0, nthreads);
     } else {
         out.kofs.assign(dec.ndom + 1, 0);

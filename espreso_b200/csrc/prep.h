@@ -46,6 +46,8 @@ struct SubPrep {
     std::vector<int> b0_dof;       // local DOF
     std::vector<double> b0_sign;
     std::vector<double> V;         // ni x (n0_i + nk), column-major: [B_i K^+ B0_i^T | G_i^T]
+    // device preprocessing: B_i K^+ B0_i^T (ni x n0_i) and B0_i K^+ B0_i^T (n0_i x n0_i), column-major
+    std::vector<double> BKB0, B0KB0;
 
     // x := K_reg^{-1} x (local DOF order)
     void kplus(double *x) const;

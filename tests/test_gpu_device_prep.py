@@ -149,3 +149,20 @@ def test_low_precision_tiles(cases, schur, tol):
     ylo = inst.apply_F(x, schur)
     assert np.linalg.norm(ylo - y64) <= tol * np.linalg.norm(y64)
     inst.destroy()
+
+
+def test_hybrid_matches_host():
+    """Hybrid Total FETI: the corner rows B0 ride along in the device elimination; the dual operator
+    and the solution match the host path."""
+    P = problems.elasticity_cube(clusters=(2, 2, 1), domains=(1, 2, 2), elements=(3, 3, 3))
+    cl = P.sub_cluster()
+    host = instance(P, False, method=1, clusters=cl)
+    dev = instance(P, True, method=1, clusters=cl)
+    rng = np.random.default_rng(13)
+    x = rng.standard_normal(int(dev.stats()["dual_size"]))
+    yh, yd = host.apply_F(x, F.FP64), dev.apply_F(x, F.FP64)
+    assert np.linalg.norm(yd - yh) <= 1e-9 * np.linalg.norm(yh)
+    uh, ud = host.solve(), dev.solve()
+    assert np.linalg.norm(ud - uh) <= 1e-8 * np.linalg.norm(uh)
+    host.destroy()
+    dev.destroy()
