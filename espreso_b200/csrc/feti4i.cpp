@@ -98,7 +98,14 @@ void add_element(ElementData &el, int type, int nn, const int *nodes, int nd, co
     el.val_ptr.push_back((int64_t)el.vals.size());
 }
 
-void build(FETI4IStructInstance *I) {
+// The decomposition depends on the element structure, the partition and the Dirichlet DOFs only;
+// a matrix update with the same structure keeps it.
+bool same_structure(const ElementData &a, const ElementData &b) {
+    return a.etype == b.etype && a.node_ptr == b.node_ptr && a.dof_ptr == b.dof_ptr && a.nodes == b.nodes &&
+           a.dofs == b.dofs && a.partition == b.partition && a.index_base == b.index_base;
+}
+
+void build(FETI4IStructInstance *I, bool keep_decomposition = false) {
     const int *io = I->iopt;
     g_verbose = io[FETI4I_VERBOSE_LEVEL];
     FETI_CHECK(io[FETI4I_FETI_METHOD] == 0 || io[FETI4I_FETI_METHOD] == 1,
@@ -110,8 +117,10 @@ void build(FETI4IStructInstance *I) {
     FETI_CHECK(I->ropt[FETI4I_PRECISION] > 0, "FETI4I: PRECISION must be positive");
     FETI_CHECK(io[FETI4I_MAX_ITERATIONS] > 0, "FETI4I: MAX_ITERATIONS must be positive");
     double t0 = now_s();
-    I->dec = decompose(I->el, io[FETI4I_SUBDOMAINS], I->dir_idx, I->dir_val);
-    FETI_LOG(2, "FETI4I: decomposition %.3f s\n", now_s() - t0);
+    if (!keep_decomposition) {
+        I->dec = decompose(I->el, io[FETI4I_SUBDOMAINS], I->dir_idx, I->dir_val);
+        FETI_LOG(2, "FETI4I: decomposition %.3f s\n", now_s() - t0);
+    }
     PrepOptions po;
     po.method = io[FETI4I_FETI_METHOD];
     if (po.method == 1 && !I->el.sub_cluster.empty()) {
@@ -350,9 +359,46 @@ void FETI4IUpdateStiffnessMatrix(FETI4IInstance instance, FETI4IMatrix stiffness
         auto *I = check_instance(instance);
         auto *m = check_matrix(stiffnessMatrix);
         std::vector<int> part = I->el.partition;
-        I->el = m->el;
-        if (I->el.partition.empty() && part.size() == I->el.nelem()) I->el.partition = part;
-        build(I);
+        ElementData el = m->el;
+        if (el.partition.empty() && part.size() == el.nelem()) el.partition = part;
+        const bool keep = same_structure(el, I->el);
+        I->el = std::move(el);
+        build(I, keep);
+    });
+}
+
+void FETI4IUpdateStiffnessMatrixScaled(FETI4IInstance instance, FETI4IMatrix stiffnessMatrix, FETI4IInt size,
+                                       const FETI4IReal *scale) {
+    guarded([&] {
+        auto *I = check_instance(instance);
+        auto *m = check_matrix(stiffnessMatrix);
+        const ElementData &src = m->el;
+        FETI_CHECK(size == (FETI4IInt)src.nelem() && (size == 0 || scale),
+                   "FETI4I: one scale per stored element of the matrix is required");
+        std::vector<int> part = I->el.partition;
+        const bool keep = same_structure(src, I->el) ||
+                          (src.partition.empty() && part.size() == src.nelem() && [&] {
+                              ElementData probe;
+                              probe.etype = src.etype; probe.node_ptr = src.node_ptr; probe.dof_ptr = src.dof_ptr;
+                              probe.nodes = src.nodes; probe.dofs = src.dofs; probe.partition = part;
+                              probe.index_base = src.index_base;
+                              return same_structure(probe, I->el);
+                          }());
+        // K_e := scale_e * K_e of the matrix object (element after element, in parallel)
+        I->el.vals.resize(src.vals.size());
+        const long long ne = (long long)src.nelem();
+#pragma omp parallel for schedule(static)
+        for (long long e = 0; e < ne; ++e) {
+            const double s_ = scale[e];
+            for (int64_t k = src.val_ptr[e]; k < src.val_ptr[e + 1]; ++k) I->el.vals[k] = s_ * src.vals[k];
+        }
+        if (!keep) {
+            std::vector<double> v = std::move(I->el.vals);
+            I->el = src;
+            I->el.vals = std::move(v);
+            if (I->el.partition.empty() && part.size() == I->el.nelem()) I->el.partition = part;
+        }
+        build(I, keep);
     });
 }
 

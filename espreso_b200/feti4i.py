@@ -32,6 +32,7 @@ STAT_NAMES = ["iterations", "converged", "dual_size", "kernel_size", "subdomains
 EXPORTED = [
     "FETI4ISetDefaultIntegerOptions", "FETI4ISetDefaultRealOptions", "FETI4ICreateStiffnessMatrix",
     "FETI4IAddElement", "FETI4ICreateInstance", "FETI4ISolve", "FETI4IUpdateStiffnessMatrix",
+    "FETI4IUpdateStiffnessMatrixScaled",
     "FETI4IUpdateRhs", "FETI4IUpdateDirichlet", "FETI4IDestroy",
     "FETI4IGetLastError", "FETI4ISetSubdomainPartition", "FETI4IAddElements", "FETI4ISetExtendedOption",
     "FETI4IGetStats", "FETI4IGetDualSolution", "FETI4IGetSubdomainInfo", "FETI4IGetSubdomainMultipliers",
@@ -68,6 +69,7 @@ def load(path: str = LIB_PATH):
         "FETI4ICreateInstance": ([P(vp), vp, i32, pd, pi, i32, pi, i32, pi, pd, pi, pd], None),
         "FETI4ISolve": ([vp, i32, pd], None),
         "FETI4IUpdateStiffnessMatrix": ([vp, vp], None),
+        "FETI4IUpdateStiffnessMatrixScaled": ([vp, vp, i32, pd], None),
         "FETI4IUpdateRhs": ([vp, i32, pd], None),
         "FETI4IUpdateDirichlet": ([vp, i32, pi, pd], None),
         "FETI4IDestroy": ([vp], None),
@@ -375,6 +377,12 @@ class Instance:
 
     def update_matrix(self, matrix: Matrix):
         self.lib.FETI4IUpdateStiffnessMatrix(self.h, matrix.h)
+        _check(self.lib)
+
+    def update_matrix_scaled(self, matrix: Matrix, scale):
+        """K_e := scale[e] * K_e of ``matrix`` (FETI4IUpdateStiffnessMatrixScaled)."""
+        sc = np.ascontiguousarray(scale, dtype=np.float64)
+        self.lib.FETI4IUpdateStiffnessMatrixScaled(self.h, matrix.h, int(sc.size), _dp(sc))
         _check(self.lib)
 
     def destroy(self):

@@ -37,6 +37,15 @@ void FETI4ISetClusterPartition(FETI4IMatrix matrix, FETI4IInt nsubdomains, const
 void FETI4IAddElements(FETI4IMatrix matrix, FETI4IInt type, FETI4IInt nelems, FETI4IInt nodesSize, FETI4IInt *nodes,
                        FETI4IInt dofsSize, FETI4IInt *dofs, FETI4IReal *values);
 
+/* FETI4IUpdateStiffnessMatrix with K_e := scale[e] * K_e of `matrix` (one scale per stored element),
+ * e.g. the densities of a topology-optimisation step applied to unit-modulus element matrices.
+ * Like FETI4IUpdateStiffnessMatrix (which here also keeps the decomposition when the element
+ * structure and partition are unchanged), it repeats the subdomain factorisations and the Schur
+ * complements.  No counterpart in the reference; it saves the caller building and passing scaled
+ * copies of every element matrix. */
+void FETI4IUpdateStiffnessMatrixScaled(FETI4IInstance instance, FETI4IMatrix matrix, FETI4IInt size,
+                                       const FETI4IReal *scale);
+
 /* Extended options, read by FETI4ICreateInstance (process-wide, like the
  * reference's global ECF configuration). */
 typedef enum {

@@ -153,3 +153,27 @@ def test_update_rhs_and_dirichlet():
         dir_rows = m["c"] != 0
         assert np.all(m["c"][dir_rows] == 1e-3)
     inst.destroy()
+
+
+def test_update_matrix_scaled():
+    """FETI4IUpdateStiffnessMatrixScaled: K_e := s_e K_e of a matrix object, decomposition kept;
+    the result equals an instance built from the scaled element matrices."""
+    P = CASES["elast_2x2x2"]()
+    rng = np.random.default_rng(4)
+    scale = rng.uniform(0.5, 2.0, P.elem_nodes.shape[0])
+    unit = F.Matrix(0)
+    unit.add_elements(P.elem_nodes, P.elem_dofs(), P.Ke)
+    unit.set_partition(P.elem_domain)
+    inst = host_instance(P)
+    inst.update_matrix_scaled(unit, scale)
+    scaled = problems.elasticity_cube(domains=(2, 2, 2), elements=(3, 3, 3))
+    scaled.Ke = P.Ke * scale[:, None, None]
+    ref = host_instance(scaled)
+    for d in range(int(ref.stats()["subdomains"])):
+        np.testing.assert_allclose(inst.schur(d), ref.schur(d), rtol=1e-12, atol=1e-12 * np.abs(ref.schur(d)).max())
+        np.testing.assert_array_equal(inst.multipliers(d)["lam"], ref.multipliers(d)["lam"])
+    with pytest.raises(F.FETI4IError, match="one scale per stored element"):
+        inst.update_matrix_scaled(unit, scale[:-1])
+    unit.destroy()
+    inst.destroy()
+    ref.destroy()
