@@ -2043,6 +2043,7 @@ bool cuda_available(std::string &why) {
 }
 
 void GpuSolver::upload(const Decomposition &dec, const Prep &prep, const SolveOptions &opt) {
+    const double tu0 = now_s();
     Impl &I = *impl;
     I.opt = opt;
     std::string why;
@@ -2199,6 +2200,7 @@ void GpuSolver::upload(const Decomposition &dec, const Prep &prep, const SolveOp
     CUDA_CHECK(cudaMemset(P.p, 0, sizeof(double) * NL));
     I.rho_cap = opt.max_iterations + 64;
 
+    const double tu1 = now_s();
     // Schur tiles: FP64 always (true residuals, FP64 path), low precision on request
     std::vector<const double *> mats(nd);
     std::vector<int> ns(nd), voffs(nd);
@@ -2240,9 +2242,12 @@ void GpuSolver::upload(const Decomposition &dec, const Prep &prep, const SolveOp
             I.autotune(I.Dir, P.uT, P.vT, NT);
         }
     }
+    const double tu2 = now_s();
     I.upload_kplus(dec, prep, loff, toff);
     I.upload_hybrid(dec, prep);
     CUDA_CHECK(cudaDeviceSynchronize());
+    FETI_LOG(2, "FETI4I: upload: dual layout %.3f s, tiles and autotuning %.3f s, K+ and clusters %.3f s\n",
+             tu1 - tu0, tu2 - tu1, now_s() - tu2);
 }
 
 std::string GpuSolver::tuning() const {
