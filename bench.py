@@ -53,8 +53,9 @@ def parse():
                          "nodal tractions on the x=1 face")
     ap.add_argument("--symm-tensor", type=int, default=1, choices=[0, 1],
                     help="batched leg: FP32 SYMM on the tensor cores (tcgen05, 3xTF32) instead of CUDA cores")
-    ap.add_argument("--leg", default="solve", choices=["solve", "adjoint"],
-                    help="adjoint: one forward + backward of the density-to-displacement map (torch.autograd)")
+    ap.add_argument("--leg", default="solve", choices=["solve", "adjoint", "prep"],
+                    help="adjoint: one forward + backward of the density-to-displacement map (torch.autograd); "
+                         "prep: instance creation only (preprocessing times)")
     ap.add_argument("--adjoint-grid", type=int, nargs=2, default=[4, 6], metavar=("DOMAINS", "ELEMENTS"),
                     help="adjoint leg: DOMAINS^3 subdomains of ELEMENTS^3 HEXA8")
     ap.add_argument("--device-prep", type=int, default=1, choices=[0, 1],
@@ -420,10 +421,43 @@ def run_adjoint(args):
     print(json.dumps(line))
 
 
+def run_prep(args):
+    """Instance creation of --config: decomposition, preprocessing (device or host) and upload; one
+    JSON line with the times and the device eliminations' flops and rate."""
+    from espreso_b200 import feti4i as F
+    from espreso_b200 import problems
+    P = problems.build_config(args.config)
+    times = []
+    st = {}
+    for _ in range(args.warmup + args.steps):
+        t = time.perf_counter()
+        inst = problems.make_instance(P, iopts={F.PRECONDITIONER: args.precond, F.VERBOSE_LEVEL: 0,
+                                                F.FETI_METHOD: args.method},
+                                      ropts={F.PRECISION: args.precision},
+                                      ext={F.EXT_SCHUR_PRECISION: SCHUR[args.schur], F.EXT_AUTOTUNE: 0,
+                                           F.EXT_DEVICE_PREP: args.device_prep},
+                                      clusters=P.sub_cluster() if args.method == 1 else None)
+        times.append(time.perf_counter() - t)
+        st = inst.stats()
+        inst.destroy()
+    wall = float(np.median(times[args.warmup:])) * 1e3
+    line = {"metric": "instance creation wall time", "value": wall, "unit": "ms", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": args.config, "subdomains": int(st["subdomains"]),
+                                            "prep": "device" if args.device_prep else "host"},
+            "prep_s": st["prep_seconds"], "upload_s": st["upload_seconds"],
+            "prep_device_ms": st["prep_device_ms"], "prep_device_gflop": st["prep_device_flops"] * 1e-9,
+            "prep_device_tflops": (st["prep_device_flops"] / st["prep_device_ms"] * 1e-9
+                                   if st["prep_device_ms"] > 0 else None)}
+    print(json.dumps(line))
+
+
 if __name__ == "__main__":
     a = parse()
     if a.leg == "adjoint":
         run_adjoint(a)
+    elif a.leg == "prep":
+        run_prep(a)
     elif a.impl == "reference":
         run_reference(a)
     else:

@@ -136,6 +136,9 @@ void build(FETI4IStructInstance *I, bool keep_decomposition = false) {
     po.device = I->ext[FETI4I_EXT_DEVICE_PREP] != 0.0 && I->ext[FETI4I_EXT_HOST_ONLY] == 0.0;
     // batch size of the device eliminations in bytes (tests force one subdomain per batch)
     if (const char *b = std::getenv("FETI4I_DEVICE_PREP_BATCH_BYTES")) po.device_mem = std::strtoull(b, nullptr, 10);
+    // the previous device solver (and its tile stores) goes first: a rebuild must not hold two
+    // copies of the device data at once
+    I->gpu.reset();
     I->prep = Prep();
     preprocess(I->el, I->dec, I->rhs, po, I->prep);
     I->t_prep = now_s() - t0;

@@ -298,6 +298,8 @@ CONFIGS = {
     "c2_heat_512": dict(kind="heat", domains=(8, 8, 8), elements=(10, 10, 10)),
     # smaller variant of the heat workload (profiling captures; a few GB on the device)
     "c2_heat_216": dict(kind="heat", domains=(6, 6, 6), elements=(10, 10, 10)),
+    # four subdomains of the c4/c5 subdomain size (device preprocessing captures; about 3 GB)
+    "prep_elasticity_4x12": dict(kind="elasticity", domains=(2, 2, 1), elements=(12, 12, 12)),
     # 512 subdomains of 6..14 elements per side by seeded recursive bisection of a 94^3 grid
     "c3_elasticity_uneven": dict(kind="uneven", physics="elasticity", side=(94, 94, 94), levels=9, lo=6, hi=14),
     # the same construction at 64 subdomains
