@@ -989,13 +989,23 @@ struct KplusDev {
     const long long *tile0;  // first tile of each subdomain
     const int *pos;          // local DOF -> factor position (concatenated)
     const double *L;         // tiles
+    const int *jt;           // first 32-block holding a touched DOF (factor order: untouched DOFs first)
+    double *z;               // forward results L^-1 f kept by mode 1 (factor order, concatenated)
 };
+
+// K^+ modes of kplus_kernel:
+//   0  out = K^+ in;
+//   1  (b = B K^+ f needs K^+ f at the touched DOFs only) forward pass over every block, kept in z;
+//      backward pass over the blocks from jt on: out is K^+ in at the touched DOFs, not elsewhere;
+//   2  (primal, in = -B^T lambda is zero at the untouched DOFs) forward pass from block jt on, plus
+//      the kept z = L^-1 f, then the whole backward pass: out = K^+ (f - B^T lambda).
+enum { KPLUS_FULL = 0, KPLUS_TOUCHED = 1, KPLUS_PRIMAL = 2 };
 
 __device__ __forceinline__ long long ltile(int T, int I, int J) {
     return (long long)J * T - (long long)J * (J - 1) / 2 + (I - J);
 }
 
-__global__ void __launch_bounds__(256) kplus_kernel(KplusDev K, const double *in, double *out) {
+__global__ void __launch_bounds__(256) kplus_kernel(KplusDev K, const double *in, double *out, int mode) {
     extern __shared__ double v[];
     __shared__ double part[8][32];
     const int d = blockIdx.x;
@@ -1009,8 +1019,10 @@ __global__ void __launch_bounds__(256) kplus_kernel(KplusDev K, const double *in
     for (int i = threadIdx.x; i < n; i += blockDim.x) v[pos[i]] = in[o + i];
     __syncthreads();
     const int cq = lane % 16, h = lane / 16, idx = 2 * cq + h;
-    // forward: L y = f
-    for (int J = 0; J < T; ++J) {
+    const int jt = mode == KPLUS_FULL ? 0 : K.jt[d];
+    double *zs = K.z + o;
+    // forward: L y = f (rows before block jt are zero in mode 2, so their steps are skipped)
+    for (int J = (mode == KPLUS_PRIMAL ? jt : 0); J < T; ++J) {
         if (warp == 0) {
             // y_J = inv(L_JJ) v_J: lane r forms row r (zero above the diagonal)
             const double *row = dtiles + (size_t)ltile(T, J, J) * TILE * TILE + lane * TILE;
@@ -1038,8 +1050,15 @@ __global__ void __launch_bounds__(256) kplus_kernel(KplusDev K, const double *in
         }
         __syncthreads();
     }
-    // backward: L^T x = y
-    for (int J = T - 1; J >= 0; --J) {
+    if (mode == KPLUS_TOUCHED) {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) zs[i] = v[i];
+        __syncthreads();
+    } else if (mode == KPLUS_PRIMAL) {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) v[i] += zs[i];
+        __syncthreads();
+    }
+    // backward: L^T x = y (in mode 1 only down to block jt)
+    for (int J = T - 1; J >= (mode == KPLUS_TOUCHED ? jt : 0); --J) {
         double cp = 0.0;
         for (int I = J + 1 + warp; I < T; I += nw) {
             const uint4 *tp = tiles + (size_t)ltile(T, I, J) * (TILE * 16);
@@ -1071,6 +1090,119 @@ __global__ void __launch_bounds__(256) kplus_kernel(KplusDev K, const double *in
         __syncthreads();
     }
     for (int i = threadIdx.x; i < n; i += blockDim.x) out[o + i] = v[pos[i]];
+}
+
+// K^+ on NC right-hand sides at once (columns j0 .. j0+NC-1 of in/out, `stride` doubles apart):
+// every factor tile is loaded once per pass and applied to all NC columns, so the factor is read
+// once for NC load cases.  Same tile walk and modes as kplus_kernel; z (mode 1/2) holds the
+// forward results of every column at the same stride.  Warps take off-diagonal tiles; warp w
+// handles the diagonal blocks of columns w, w + 8, ...
+template <int NC>
+__global__ void __launch_bounds__(256) kplus_multi_kernel(KplusDev K, const double *in, double *out, int mode,
+                                                          int j0, long long stride, double *z) {
+    extern __shared__ double vm[];              // [NC][TILE * T]
+    __shared__ double part[8][NC][TILE];
+    const int d = blockIdx.x;
+    const int n = K.n[d], T = K.tn[d], o = K.doff[d];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int NP = TILE * T;
+    const int *pos = K.pos + o;
+    const uint4 *tiles = reinterpret_cast<const uint4 *>(K.L) + (size_t)K.tile0[d] * (TILE * 16);
+    const double *dtiles = K.L + (size_t)K.tile0[d] * TILE * TILE;
+    const int jt = mode == KPLUS_FULL ? 0 : K.jt[d];
+    for (int i = threadIdx.x; i < NC * NP; i += blockDim.x) vm[i] = 0.0;
+    __syncthreads();
+    for (int c = 0; c < NC; ++c)
+        for (int i = threadIdx.x; i < n; i += blockDim.x) vm[c * NP + pos[i]] = in[(size_t)(j0 + c) * stride + o + i];
+    __syncthreads();
+    const int cq = lane % 16, h = lane / 16, idx = 2 * cq + h;
+    for (int J = (mode == KPLUS_PRIMAL ? jt : 0); J < T; ++J) {
+        {
+            const double *row = dtiles + (size_t)ltile(T, J, J) * TILE * TILE + lane * TILE;
+            for (int c = warp; c < NC; c += nw) {
+                double *vc = vm + c * NP;
+                const double vr = vc[TILE * J + lane];
+                double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+                for (int k = 0; k < TILE; k += 2) {
+                    s0 += row[k] * __shfl_sync(FULL, vr, k);
+                    s1 += row[k + 1] * __shfl_sync(FULL, vr, k + 1);
+                }
+                vc[TILE * J + lane] = s0 + s1;
+            }
+        }
+        __syncthreads();
+        for (int I = J + 1 + warp; I < T; I += nw) {
+            const uint4 *tp = tiles + (size_t)ltile(T, I, J) * (TILE * 16);
+            uint4 t[16];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) t[q] = ld_stream(tp + q * 32 + lane);
+            for (int c = 0; c < NC; ++c) {
+                double *vc = vm + c * NP;
+                const double x0 = vc[TILE * J + 2 * cq], x1 = vc[TILE * J + 2 * cq + 1];
+                double rs[16];
+#pragma unroll
+                for (int q = 0; q < 16; ++q)
+                    rs[q] = __hiloint2double(t[q].y, t[q].x) * x0 + __hiloint2double(t[q].w, t[q].z) * x1;
+                const double r = reduce_scatter<16, 0>(rs, lane);
+                vc[TILE * I + idx] -= r;
+            }
+        }
+        __syncthreads();
+    }
+    if (mode == KPLUS_TOUCHED) {
+        for (int c = 0; c < NC; ++c)
+            for (int i = threadIdx.x; i < n; i += blockDim.x) z[(size_t)(j0 + c) * stride + o + i] = vm[c * NP + i];
+        __syncthreads();
+    } else if (mode == KPLUS_PRIMAL) {
+        for (int c = 0; c < NC; ++c)
+            for (int i = threadIdx.x; i < n; i += blockDim.x) vm[c * NP + i] += z[(size_t)(j0 + c) * stride + o + i];
+        __syncthreads();
+    }
+    for (int J = T - 1; J >= (mode == KPLUS_TOUCHED ? jt : 0); --J) {
+        double cp[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) cp[c] = 0.0;
+        for (int I = J + 1 + warp; I < T; I += nw) {
+            const uint4 *tp = tiles + (size_t)ltile(T, I, J) * (TILE * 16);
+            uint4 t[16];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) t[q] = ld_stream(tp + q * 32 + lane);
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                const double *vc = vm + c * NP;
+                double cs[2] = {0.0, 0.0};
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    const double xr = vc[TILE * I + 2 * q + h];
+                    cs[0] += __hiloint2double(t[q].y, t[q].x) * xr;
+                    cs[1] += __hiloint2double(t[q].w, t[q].z) * xr;
+                }
+                cp[c] += reduce_scatter<2, 4>(cs, lane);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < NC; ++c) part[warp][c][idx] = cp[c];
+        __syncthreads();
+        {
+            const double *tile = dtiles + (size_t)ltile(T, J, J) * TILE * TILE;
+            for (int c = warp; c < NC; c += nw) {
+                double *vc = vm + c * NP;
+                double v0 = vc[TILE * J + lane];
+                for (int w = 0; w < nw; ++w) v0 -= part[w][c][lane];
+                double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+                for (int k = 0; k < TILE; k += 2) {
+                    s0 += tile[k * TILE + lane] * __shfl_sync(FULL, v0, k);
+                    s1 += tile[(k + 1) * TILE + lane] * __shfl_sync(FULL, v0, k + 1);
+                }
+                vc[TILE * J + lane] = s0 + s1;
+            }
+        }
+        __syncthreads();
+    }
+    for (int c = 0; c < NC; ++c)
+        for (int i = threadIdx.x; i < n; i += blockDim.x) out[(size_t)(j0 + c) * stride + o + i] = vm[c * NP + pos[i]];
 }
 
 // subdomain loads f_i = rhs(caller DOF) / multiplicity
@@ -1114,7 +1246,7 @@ __global__ void bvec_kernel(DevProblem P, const int *rdof, const double *rsign, 
 // g = f - B^T lambda (local DOF space), gathered through the touched-DOF rows
 __global__ void primal_rhs_kernel(DevProblem P, const int *tdof_g, const double *rsign, const double *f, double *g,
                                   int ntot) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ntot; i += gridDim.x * blockDim.x) g[i] = f[i];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ntot; i += gridDim.x * blockDim.x) g[i] = f ? f[i] : 0.0;
 }
 __global__ void primal_bt_kernel(DevProblem P, const int *tdof_g, const double *rsign, double *g) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1378,6 +1510,7 @@ struct GpuSolver::Impl {
         cudaGraphExec_t graph = nullptr;
         int graph_chunk = 0, graph_prec = -1, graph_precond = -1;
         double *rhs = nullptr, *sol = nullptr, *f = nullptr, *kf = nullptr, *g = nullptr;
+        double *zk = nullptr;   // forward results L^-1 f of every column (K^+ modes 1 and 2)
         int flat_grid = 1;
         int2 *units4 = nullptr;
         int nunits4 = 0;
@@ -1443,12 +1576,37 @@ struct GpuSolver::Impl {
     int kernels_per_iteration() const;
     void upload_kplus(const Decomposition &dec, const Prep &prep, const std::vector<int> &loff,
                       const std::vector<int> &toff);
-    void launch_kplus(const double *in, double *out);
+    void launch_kplus(const double *in, double *out, int mode = KPLUS_FULL);
+    void launch_kplus_multi(const double *in, double *out, int ncol, int mode, double *z);
 };
 
-void GpuSolver::Impl::launch_kplus(const double *in, double *out) {
+// dynamic shared memory available to kplus_multi_kernel<NC> next to its static partial sums
+static size_t kplus_multi_smem(int nc) { return (size_t)220 * 1024 - (size_t)nc * 8 * TILE * sizeof(double); }
+
+// K^+ on ncol columns (stride ntot): groups of NC columns per pass, NC as large as shared memory allows.
+void GpuSolver::Impl::launch_kplus_multi(const double *in, double *out, int ncol, int mode, double *z) {
+    const size_t per_col = sizeof(double) * TILE * (size_t)max_T;
+    int j0 = 0;
+    while (j0 < ncol) {
+        const int left = ncol - j0;
+        int nc = 16;
+        while (nc > 1 && (nc > left || (size_t)nc * per_col > kplus_multi_smem(nc))) nc /= 2;
+        const size_t sm = (size_t)nc * per_col;
+        switch (nc) {
+        case 16: kplus_multi_kernel<16><<<P.nd, 256, sm, stream>>>(KP, in, out, mode, j0, ntot, z); break;
+        case 8: kplus_multi_kernel<8><<<P.nd, 256, sm, stream>>>(KP, in, out, mode, j0, ntot, z); break;
+        case 4: kplus_multi_kernel<4><<<P.nd, 256, sm, stream>>>(KP, in, out, mode, j0, ntot, z); break;
+        case 2: kplus_multi_kernel<2><<<P.nd, 256, sm, stream>>>(KP, in, out, mode, j0, ntot, z); break;
+        default: kplus_multi_kernel<1><<<P.nd, 256, sm, stream>>>(KP, in, out, mode, j0, ntot, z); break;
+        }
+        CUDA_CHECK(cudaGetLastError());
+        j0 += nc;
+    }
+}
+
+void GpuSolver::Impl::launch_kplus(const double *in, double *out, int mode) {
     size_t sm = sizeof(double) * TILE * (size_t)max_T;
-    kplus_kernel<<<P.nd, 256, sm, stream>>>(KP, in, out);
+    kplus_kernel<<<P.nd, 256, sm, stream>>>(KP, in, out, mode);
     CUDA_CHECK(cudaGetLastError());
 }
 
@@ -1537,6 +1695,12 @@ void GpuSolver::Impl::upload_kplus(const Decomposition &dec, const Prep &prep, c
     KP.doff = d_doff;
     KP.tile0 = upload(tile0);
     KP.pos = upload(pos);
+    {
+        std::vector<int> jt(nd);
+        for (int d = 0; d < nd; ++d) jt[d] = (prep.sub[d].n - prep.sub[d].t) / TILE;
+        KP.jt = upload(jt);
+        KP.z = alloc<double>(std::max(1, ntot));
+    }
     KP.L = ds ? adopt(ds->kp_tiles, (size_t)tile0[nd] * TILE * TILE) : upload(L);
     d_rofs = upload(rofs);
     d_gdof = upload(gdof);
@@ -1560,6 +1724,11 @@ void GpuSolver::Impl::upload_kplus(const Decomposition &dec, const Prep &prep, c
     d_rhs = alloc<double>(std::max(1, n_caller));
     d_sol = alloc<double>(std::max(1, n_caller));
     cudaFuncSetAttribute(kplus_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    CUDA_CHECK(cudaFuncSetAttribute(kplus_multi_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kplus_multi_smem(16)));
+    CUDA_CHECK(cudaFuncSetAttribute(kplus_multi_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kplus_multi_smem(8)));
+    CUDA_CHECK(cudaFuncSetAttribute(kplus_multi_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kplus_multi_smem(4)));
+    CUDA_CHECK(cudaFuncSetAttribute(kplus_multi_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kplus_multi_smem(2)));
+    CUDA_CHECK(cudaFuncSetAttribute(kplus_multi_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kplus_multi_smem(1)));
 }
 
 void GpuSolver::Impl::upload_hybrid(const Decomposition &dec, const Prep &prep) {
@@ -2279,16 +2448,22 @@ void GpuSolver::solve_full(const double *rhs, int rhs_size, double *solution, in
         std::memcpy(I.h_pinned, rhs, sizeof(double) * ncp);
         CUDA_CHECK(cudaMemcpyAsync(I.d_rhs, I.h_pinned, sizeof(double) * ncp, cudaMemcpyHostToDevice, I.stream));
         split_rhs_kernel<<<(I.ntot + 255) / 256, 256, 0, I.stream>>>(I.d_rhs, I.d_gdof, I.d_invm, I.d_f, I.ntot);
-        I.launch_kplus_dual(I.d_f, I.d_kf);
+        // Total FETI: b needs K^+ f at the touched DOFs only; the forward pass L^-1 f is kept for
+        // the primal recovery
+        if (I.hybrid) I.launch_kplus_dual(I.d_f, I.d_kf);
+        else I.launch_kplus(I.d_f, I.d_kf, KPLUS_TOUCHED);
         evec_kernel<<<nd, TPB, 0, I.stream>>>(P, I.d_doff, I.d_rdofs, I.d_Rd, I.d_f, I.e_dev);
         bvec_kernel<<<(P.NL + 255) / 256, 256, 0, I.stream>>>(P, I.d_rdof, I.d_rsign, I.d_rc, I.d_kf, (double *)P.bL);
         CUDA_CHECK(cudaGetLastError());
     }
     solve(stats);
-    // primal: u = K^+ (f - B^T lambda) + R alpha, averaged into the caller's DOFs
-    primal_rhs_kernel<<<std::max(1, std::min(4096, (I.ntot + 255) / 256)), 256, 0, I.stream>>>(P, I.d_tdof_g, I.d_rsign, I.d_f, I.d_g, I.ntot);
+    // primal: u = K^+ (f - B^T lambda) + R alpha, averaged into the caller's DOFs; Total FETI
+    // forms L^-1 (f - B^T lambda) from the kept L^-1 f and a forward pass over the touched blocks
+    primal_rhs_kernel<<<std::max(1, std::min(4096, (I.ntot + 255) / 256)), 256, 0, I.stream>>>(
+        P, I.d_tdof_g, I.d_rsign, I.hybrid ? I.d_f : nullptr, I.d_g, I.ntot);
     primal_bt_kernel<<<(P.NT + 255) / 256, 256, 0, I.stream>>>(P, I.d_tdof_g, I.d_rsign, I.d_g);
-    I.launch_kplus_dual(I.d_g, I.d_kf);
+    if (I.hybrid) I.launch_kplus_dual(I.d_g, I.d_kf);
+    else I.launch_kplus(I.d_g, I.d_kf, KPLUS_PRIMAL);
     CUDA_CHECK(cudaMemsetAsync(I.d_sol, 0, sizeof(double) * std::max(1, I.n_caller), I.stream));
     primal_merge_kernel<<<nd, TPB, 0, I.stream>>>(P, I.d_doff, I.d_rdofs, I.d_Rd, I.d_kf, I.d_gdof, I.d_invm, I.d_sol);
     CUDA_CHECK(cudaGetLastError());
@@ -2430,7 +2605,8 @@ void GpuSolver::dual_rhs(const double *rhs, int rhs_size, double *b, double *e, 
     const int ncp = std::min(rhs_size, I.n_caller);
     CUDA_CHECK(cudaMemcpyAsync(I.d_rhs, rhs, sizeof(double) * std::max(0, ncp), cudaMemcpyHostToDevice, I.stream));
     split_rhs_kernel<<<(I.ntot + 255) / 256, 256, 0, I.stream>>>(I.d_rhs, I.d_gdof, I.d_invm, I.d_f, I.ntot);
-    I.launch_kplus_dual(I.d_f, I.d_kf);
+    if (I.hybrid) I.launch_kplus_dual(I.d_f, I.d_kf);
+    else I.launch_kplus(I.d_f, I.d_kf, KPLUS_TOUCHED);
     evec_kernel<<<P.nd, TPB, 0, I.stream>>>(P, I.d_doff, I.d_rdofs, I.d_Rd, I.d_f, I.e_dev);
     bvec_kernel<<<(P.NL + 255) / 256, 256, 0, I.stream>>>(P, I.d_rdof, I.d_rsign, I.d_rc, I.d_kf, (double *)P.bL);
     CUDA_CHECK(cudaGetLastError());
@@ -3700,8 +3876,7 @@ __global__ void bprimal_rhs_kernel(DevProblem P, BlockDev B, const int *tdof_g, 
     const int nr = B.nr;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (long long)ntot * nr;
          i += (long long)gridDim.x * blockDim.x)
-        g[i] = f[i];
-    __syncthreads();
+        g[i] = f ? f[i] : 0.0;
 }
 
 __global__ void bprimal_bt_kernel(DevProblem P, BlockDev B, const int *tdof_g, const double *rsign, double *g,
@@ -3789,6 +3964,7 @@ void GpuSolver::Impl::ensure_block(int nr) {
     blk.f = alloc<double>((size_t)ntot * nr);
     blk.kf = alloc<double>((size_t)ntot * nr);
     blk.g = alloc<double>((size_t)ntot * nr);
+    blk.zk = alloc<double>((size_t)ntot * nr);
     if (hybrid) {
         FETI_CHECK(sizeof(double) * (size_t)H.max_nc * nr <= 200 * 1024 &&
                        sizeof(double) * (size_t)hyb_max_m * nr <= 200 * 1024,
@@ -3959,7 +4135,10 @@ void GpuSolver::solve_multi(const double *rhs, int nrhs, int rhs_size, double *s
         bsplit_rhs_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, I.stream>>>(I.blk.rhs, nc, I.d_gdof, I.d_invm, I.blk.f,
                                                                               ntot, nr);
         CUDA_CHECK(cudaMemsetAsync(I.blk.kf, 0, sizeof(double) * (size_t)ntot * nr, I.stream));
-        for (int j = 0; j < nrhs; ++j) I.launch_kplus_dual(I.blk.f + (size_t)j * ntot, I.blk.kf + (size_t)j * ntot);
+        if (I.hybrid)
+            for (int j = 0; j < nrhs; ++j) I.launch_kplus_dual(I.blk.f + (size_t)j * ntot, I.blk.kf + (size_t)j * ntot);
+        else
+            I.launch_kplus_multi(I.blk.f, I.blk.kf, nrhs, KPLUS_TOUCHED, I.blk.zk);
         bevec_kernel<<<nd * nr, TPB, 0, I.stream>>>(P, B, I.d_doff, I.d_rdofs, I.d_Rd, I.blk.f, ntot);
         bbvec_kernel<<<(P.NL * nr + 255) / 256, 256, 0, I.stream>>>(P, B, I.d_rdof, I.d_rsign, I.d_rc, I.blk.kf, ntot);
         CUDA_CHECK(cudaGetLastError());
@@ -4026,9 +4205,13 @@ void GpuSolver::solve_multi(const double *rhs, int nrhs, int rhs_size, double *s
     stats.fapply_bytes = (mixed ? I.Flow : I.F64).alg_bytes;
     // ---- primal recovery for every column
     if (solutions) {
-        bprimal_rhs_kernel<<<4096, 256, 0, I.stream>>>(P, B, I.d_tdof_g, I.d_rsign, I.blk.f, I.blk.g, ntot);
+        bprimal_rhs_kernel<<<4096, 256, 0, I.stream>>>(P, B, I.d_tdof_g, I.d_rsign, I.hybrid ? I.blk.f : nullptr,
+                                                      I.blk.g, ntot);
         bprimal_bt_kernel<<<(P.NT * nr + 255) / 256, 256, 0, I.stream>>>(P, B, I.d_tdof_g, I.d_rsign, I.blk.g, ntot);
-        for (int j = 0; j < nrhs; ++j) I.launch_kplus_dual(I.blk.g + (size_t)j * ntot, I.blk.kf + (size_t)j * ntot);
+        if (I.hybrid)
+            for (int j = 0; j < nrhs; ++j) I.launch_kplus_dual(I.blk.g + (size_t)j * ntot, I.blk.kf + (size_t)j * ntot);
+        else
+            I.launch_kplus_multi(I.blk.g, I.blk.kf, nrhs, KPLUS_PRIMAL, I.blk.zk);
         CUDA_CHECK(cudaMemsetAsync(I.blk.sol, 0, sizeof(double) * (size_t)nc * nr, I.stream));
         bprimal_merge_kernel<<<nd * nr, TPB, 0, I.stream>>>(P, B, I.d_doff, I.d_rdofs, I.d_Rd, I.blk.kf, I.d_gdof, I.d_invm,
                                                            I.blk.sol, nc, ntot);
