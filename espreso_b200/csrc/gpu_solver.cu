@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 
@@ -36,6 +37,7 @@ namespace {
 constexpr int KMAX = 8;        // kernel dimension bound per subdomain (elasticity: 6)
 constexpr int TPB = 256;       // threads of the per-subdomain kernels
 constexpr int TPB1 = 512;      // threads of the single right-hand-side w/preconditioner kernel
+constexpr int TPBB = 1024;     // threads of the per-subdomain block (multi right-hand-side) kernels
 constexpr int TILE = 32;       // Schur tile edge
 constexpr unsigned FULL = 0xffffffffu;
 
@@ -3081,8 +3083,8 @@ __global__ void btol_kernel(DevProblem P, BlockDev B) {
     }
 }
 
-__global__ void bz_kernel(DevProblem P, BlockDev B, int slot) {
-    __shared__ double sh[8 * 32];
+__global__ void __launch_bounds__(TPBB) bz_kernel(DevProblem P, BlockDev B, int slot) {
+    __shared__ double sh[32 * 32];
     const int iter = P.st->iter_base + slot;
     if (skip_iter(P.st, iter)) return;
     const int nr = B.nr, dsub = blockIdx.x;
@@ -3250,8 +3252,8 @@ __global__ void bp_kernel(DevProblem P, BlockDev B, int slot) {
     }
 }
 
-__global__ void bupdate_kernel(DevProblem P, BlockDev B, int slot) {
-    __shared__ double sh[8 * 32];
+__global__ void __launch_bounds__(TPBB) bupdate_kernel(DevProblem P, BlockDev B, int slot) {
+    __shared__ double sh[32 * 32];
     const int iter = P.st->iter_base + slot;
     if (skip_iter(P.st, iter)) return;
     const int nr = B.nr, dsub = blockIdx.x;
@@ -4096,7 +4098,7 @@ void GpuSolver::Impl::launch_block_iteration(int slot) {
     }
 #undef BW
     if (opt.precond != PREC_NONE) {
-        bz_kernel<<<nd, TPB, 0, stream>>>(P, B, slot);
+        bz_kernel<<<nd, TPBB, 0, stream>>>(P, B, slot);
         bcoarse_kernel<<<cgrid, 256, 0, stream>>>(P, B, B.d, B.alpha, slot, 1);
         switch (P.KS) {
         case 1: by_flat_kernel<1><<<fgrid, 256, 0, stream>>>(P, B, slot); break;
@@ -4108,7 +4110,7 @@ void GpuSolver::Impl::launch_block_iteration(int slot) {
     if (mixed) launch_symm(Flow, true, nullptr, B.p32, B.Ap, slot, 1);
     else launch_symm(F64, false, B.p, nullptr, B.Ap, slot, 1);
     launch_block_hybrid(B.p, B.Ap, slot, 1, B.scal + SC_PAP * blk.nr);
-    bupdate_kernel<<<nd, TPB, 0, stream>>>(P, B, slot);
+    bupdate_kernel<<<nd, TPBB, 0, stream>>>(P, B, slot);
     CUDA_CHECK(cudaGetLastError());
 }
 
