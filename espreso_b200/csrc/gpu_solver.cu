@@ -2342,15 +2342,23 @@ void GpuSolver::upload(const Decomposition &dec, const Prep &prep, const SolveOp
     {
         // (GG^T)^-1 times the sum over the partial blocks: column b of partial block d, kernel k
         // is column akof[d] + k of (GG^T)^-1
+        // ((GG^T)^-1 is symmetric: row r of it is read contiguously)
         const int nK = prep.n_kern, nP = kof[nd];
         std::vector<double> Gx((size_t)nK * nP);
+        std::vector<int> bcol(nP);
         I.dual_to_partial.assign(nK, -1);
         for (int d = 0; d < nd; ++d)
             for (int k = 0; k < prep.sub[d].dnk; ++k) {
                 const int b = kof[d] + k, col = akof[d] + k;
-                for (int r = 0; r < nK; ++r) Gx[(size_t)r * nP + b] = prep.GGt_inv[(size_t)col * nK + r];
+                bcol[b] = col;
                 if (I.dual_to_partial[col] < 0) I.dual_to_partial[col] = b;
             }
+#pragma omp parallel for schedule(static)
+        for (int r = 0; r < nK; ++r) {
+            const double *src = prep.GGt_inv.data() + (size_t)r * nK;
+            double *dst = Gx.data() + (size_t)r * nP;
+            for (int b = 0; b < nP; ++b) dst[b] = src[bcol[b]];
+        }
         P.GGtinv = I.upload(Gx);
     }
     P.bL = I.alloc<double>(NL);
@@ -3176,51 +3184,102 @@ __global__ void __launch_bounds__(256) bu_flat_kernel(DevProblem P, BlockDev B, 
 }
 
 // lumped v_T = K_TT u_T (sliced ELL of every subdomain)
-__global__ void __launch_bounds__(256) bell_flat_kernel(DevProblem P, BlockDev B, int slot) {
+// Two columns per thread (16-byte loads and stores; the per-row index loads serve both).
+// Per-column block sums when every thread holds columns 2 (lane % (nr/2)) and 2 (lane % (nr/2)) + 1.
+__device__ void block_sum_cols2(double s0, double s1, int nr, double *sh /* >= 8*32 */, double *out_col) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5, hnr = nr >> 1;
+    for (int o = 16; o >= hnr; o >>= 1) {
+        s0 += __shfl_xor_sync(FULL, s0, o);
+        s1 += __shfl_xor_sync(FULL, s1, o);
+    }
+    __syncthreads();
+    if (lane < hnr) {
+        sh[wid * 32 + 2 * lane] = s0;
+        sh[wid * 32 + 2 * lane + 1] = s1;
+    }
+    __syncthreads();
+    if (threadIdx.x < nr) {
+        double t = 0.0;
+        for (int i = 0; i < nw; ++i) t += sh[i * 32 + threadIdx.x];
+        out_col[threadIdx.x] = t;
+    }
+    __syncthreads();
+}
+
+template <int KC>
+__device__ __forceinline__ double2 gt_alpha_colk2(const DevProblem &P, int e, int j, int nr, const double *a) {
+    double2 r = make_double2(0.0, 0.0);
+    if (KC == 0) {
+        r.x = gt_alpha_col(P, e, j, nr, a);
+        r.y = gt_alpha_col(P, e, j + 1, nr, a);
+        return r;
+    }
+    const int ko = P.rkof[e], po = P.pkof[e];
+    const double *g = P.Gl + (size_t)e * KC, *gp = P.Gp + (size_t)e * KC;
+#pragma unroll
+    for (int k = 0; k < KC; ++k) {
+        const double2 x = *reinterpret_cast<const double2 *>(a + (size_t)(ko + k) * nr + j);
+        const double2 y = *reinterpret_cast<const double2 *>(a + (size_t)(po + k) * nr + j);
+        r.x += g[k] * x.x + gp[k] * y.x;
+        r.y += g[k] * x.y + gp[k] * y.y;
+    }
+    return r;
+}
+
+__global__ void __launch_bounds__(256) bell_flat2_kernel(DevProblem P, BlockDev B, int slot) {
     const int iter = P.st->iter_base + slot;
     if (skip_iter(P.st, iter)) return;
-    const int nr = B.nr;
-    const long long cnt = (long long)P.NT * nr, stride = (long long)gridDim.x * blockDim.x;
+    const int nr = B.nr, lh = B.lg - 1;
+    const long long cnt = (long long)P.NT * (nr >> 1), stride = (long long)gridDim.x * blockDim.x;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += stride) {
-        const int t = (int)(i >> B.lg), j = (int)(i & (nr - 1));
+        const int t = (int)(i >> lh), j = 2 * (int)(i & ((nr >> 1) - 1));
         const int t0 = P.tbase[t], ts = P.tslot[t];
         const int sl = ts >> 5, ln = ts & 31;
         const int base = P.ell_ptr[sl], wd = P.ell_w[sl];
-        double s0 = 0.0, s1 = 0.0;
+        double2 s0 = make_double2(0.0, 0.0), s1 = make_double2(0.0, 0.0);
         int q = 0;
         for (; q + 1 < wd; q += 2) {
             const int o = base + q * 32 + ln;
-            s0 += P.ell_val[o] * B.uT[(size_t)(t0 + P.ell_col[o]) * nr + j];
-            s1 += P.ell_val[o + 32] * B.uT[(size_t)(t0 + P.ell_col[o + 32]) * nr + j];
+            const double v0 = P.ell_val[o], v1 = P.ell_val[o + 32];
+            const double2 u0 = *reinterpret_cast<const double2 *>(B.uT + (size_t)(t0 + P.ell_col[o]) * nr + j);
+            const double2 u1 = *reinterpret_cast<const double2 *>(B.uT + (size_t)(t0 + P.ell_col[o + 32]) * nr + j);
+            s0.x += v0 * u0.x;
+            s0.y += v0 * u0.y;
+            s1.x += v1 * u1.x;
+            s1.y += v1 * u1.y;
         }
         if (q < wd) {
             const int o = base + q * 32 + ln;
-            s0 += P.ell_val[o] * B.uT[(size_t)(t0 + P.ell_col[o]) * nr + j];
+            const double v0 = P.ell_val[o];
+            const double2 u0 = *reinterpret_cast<const double2 *>(B.uT + (size_t)(t0 + P.ell_col[o]) * nr + j);
+            s0.x += v0 * u0.x;
+            s0.y += v0 * u0.y;
         }
-        B.vT[i] = s0 + s1;
+        *reinterpret_cast<double2 *>(B.vT + (size_t)t * nr + j) = make_double2(s0.x + s1.x, s0.y + s1.y);
     }
 }
 
-// y = z - G^T alpha, rho_j = y.w
 template <int KC>
-__global__ void __launch_bounds__(256) by_flat_kernel(DevProblem P, BlockDev B, int slot) {
+__global__ void __launch_bounds__(256) by_flat2_kernel(DevProblem P, BlockDev B, int slot) {
     __shared__ double sh[8 * 32];
     __shared__ double cols[32];
     const int iter = P.st->iter_base + slot;
     if (skip_iter(P.st, iter)) return;
-    const int nr = B.nr;
-    const long long cnt = (long long)P.NL * nr, stride = (long long)gridDim.x * blockDim.x;
-    double s = 0.0;
+    const int nr = B.nr, lh = B.lg - 1;
+    const long long cnt = (long long)P.NL * (nr >> 1), stride = (long long)gridDim.x * blockDim.x;
+    double s0 = 0.0, s1 = 0.0;
     for (long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; i0 < cnt; i0 += UNR * stride) {
-        double zv[UNR], ga[UNR], wv[UNR], mv[UNR];
+        double2 zv[UNR], ga[UNR], wv[UNR];
+        double mv[UNR];
 #pragma unroll
         for (int u = 0; u < UNR; ++u) {
             const long long i = i0 + u * stride;
             if (i < cnt) {
-                const int e = (int)(i >> B.lg), j = (int)(i & (nr - 1));
-                zv[u] = B.z[i];
-                wv[u] = B.w[i];
-                ga[u] = gt_alpha_colk<KC>(P, e, j, nr, B.alpha);
+                const int e = (int)(i >> lh), j = 2 * (int)(i & ((nr >> 1) - 1));
+                const size_t o = (size_t)e * nr + j;
+                zv[u] = *reinterpret_cast<const double2 *>(B.z + o);
+                wv[u] = *reinterpret_cast<const double2 *>(B.w + o);
+                ga[u] = gt_alpha_colk2<KC>(P, e, j, nr, B.alpha);
                 mv[u] = P.minv[e];
             }
         }
@@ -3228,15 +3287,20 @@ __global__ void __launch_bounds__(256) by_flat_kernel(DevProblem P, BlockDev B, 
         for (int u = 0; u < UNR; ++u) {
             const long long i = i0 + u * stride;
             if (i < cnt) {
-                const double yv = zv[u] - ga[u];
-                B.y[i] = yv;
-                s += yv * wv[u] * mv[u];
+                const int e = (int)(i >> lh), j = 2 * (int)(i & ((nr >> 1) - 1));
+                const double2 yv = make_double2(zv[u].x - ga[u].x, zv[u].y - ga[u].y);
+                *reinterpret_cast<double2 *>(B.y + (size_t)e * nr + j) = yv;
+                s0 += yv.x * wv[u].x * mv[u];
+                s1 += yv.y * wv[u].y * mv[u];
             }
         }
     }
-    block_sum_cols(s, nr, sh, cols);
+    block_sum_cols2(s0, s1, nr, sh, cols);
     grid_total_cols(cols, B.part + (size_t)gridDim.x * nr, nr, B.done + DONE_RHO, B.scal + SC_RHO * nr);
 }
+
+
+// y = z - G^T alpha, rho_j = y.w
 
 // p = y + beta_j p (and its FP32 copy)
 __global__ void bp_kernel(DevProblem P, BlockDev B, int slot) {
@@ -4089,7 +4153,7 @@ void GpuSolver::Impl::launch_block_iteration(int slot) {
     case PREC_LUMPED:
         BW(PREC_LUMPED)
         bu_flat_kernel<PREC_LUMPED><<<fgrid, 256, 0, stream>>>(P, B, slot);
-        bell_flat_kernel<<<fgrid, 256, 0, stream>>>(P, B, slot);
+        bell_flat2_kernel<<<fgrid, 256, 0, stream>>>(P, B, slot);
         break;
     default:
         BW(PREC_WEIGHT)
@@ -4101,9 +4165,9 @@ void GpuSolver::Impl::launch_block_iteration(int slot) {
         bz_kernel<<<nd, TPBB, 0, stream>>>(P, B, slot);
         bcoarse_kernel<<<cgrid, 256, 0, stream>>>(P, B, B.d, B.alpha, slot, 1);
         switch (P.KS) {
-        case 1: by_flat_kernel<1><<<fgrid, 256, 0, stream>>>(P, B, slot); break;
-        case 6: by_flat_kernel<6><<<fgrid, 256, 0, stream>>>(P, B, slot); break;
-        default: by_flat_kernel<0><<<fgrid, 256, 0, stream>>>(P, B, slot); break;
+        case 1: by_flat2_kernel<1><<<fgrid, 256, 0, stream>>>(P, B, slot); break;
+        case 6: by_flat2_kernel<6><<<fgrid, 256, 0, stream>>>(P, B, slot); break;
+        default: by_flat2_kernel<0><<<fgrid, 256, 0, stream>>>(P, B, slot); break;
         }
     }
     bp_kernel<<<std::max(1, std::min(4096, (P.NL * blk.nr + 255) / 256)), 256, 0, stream>>>(P, B, slot);
