@@ -2,6 +2,7 @@
 #include "decompose.h"
 
 #include <algorithm>
+#include <array>
 #include <numeric>
 #include <unordered_map>
 
@@ -14,23 +15,12 @@ namespace {
 // HEXA8 faces (node positions inside the element), reference hexahedron8.cpp:12-19
 const int kHexFaces[6][4] = {{0, 1, 5, 4}, {3, 2, 1, 0}, {4, 5, 6, 7}, {7, 6, 2, 3}, {1, 2, 6, 5}, {3, 0, 4, 7}};
 
-struct FaceKey {
-    int v[4];
-    bool operator==(const FaceKey &o) const { return v[0] == o.v[0] && v[1] == o.v[1] && v[2] == o.v[2] && v[3] == o.v[3]; }
-};
-struct FaceHash {
-    size_t operator()(const FaceKey &k) const {
-        uint64_t h = 1469598103934665603ull;
-        for (int i = 0; i < 4; ++i) { h ^= (uint64_t)(uint32_t)k.v[i]; h *= 1099511628211ull; }
-        return (size_t)h;
-    }
-};
-
 }  // namespace
 
 Decomposition decompose(const ElementData &el, int ndomains_hint, const std::vector<int> &dir_dofs,
                         const std::vector<double> &dir_vals) {
     Decomposition dec;
+    const double tdec = now_s();
     const size_t ne = el.nelem();
     FETI_CHECK(ne > 0, "FETI4I: the stiffness matrix has no elements");
 
@@ -67,6 +57,7 @@ Decomposition decompose(const ElementData &el, int ndomains_hint, const std::vec
         }
     }
 
+    FETI_LOG(3, "FETI4I: decompose t_maps %.3f s\n", now_s() - tdec);
     // element -> domain
     dec.elem_domain.resize(ne);
     if (!el.partition.empty()) {
@@ -87,39 +78,88 @@ Decomposition decompose(const ElementData &el, int ndomains_hint, const std::vec
     for (size_t e = 0; e < ne; ++e) dec.dom[dec.elem_domain[e]].elems.push_back((int)e);
     for (int d = 0; d < dec.ndom; ++d) FETI_CHECK(!dec.dom[d].elems.empty(), "FETI4I: empty subdomain in partition");
 
-    // node -> sorted domain list (CSR)
-    std::vector<std::pair<int, int>> nd_pairs;
-    nd_pairs.reserve(el.nodes.size());
-    for (size_t e = 0; e < ne; ++e)
-        for (int64_t i = el.node_ptr[e]; i < el.node_ptr[e + 1]; ++i) nd_pairs.emplace_back(el.nodes[i], dec.elem_domain[e]);
-    std::sort(nd_pairs.begin(), nd_pairs.end());
-    nd_pairs.erase(std::unique(nd_pairs.begin(), nd_pairs.end()), nd_pairs.end());
-    std::vector<int> dptr(dec.n_nodes + 1, 0), dlist(nd_pairs.size());
-    for (auto &p : nd_pairs) dptr[p.first + 1]++;
-    for (int n = 0; n < dec.n_nodes; ++n) dptr[n + 1] += dptr[n];
-    for (size_t i = 0; i < nd_pairs.size(); ++i) dlist[i] = nd_pairs[i].second;
+    FETI_LOG(3, "FETI4I: decompose t_elemdom %.3f s\n", now_s() - tdec);
+    // node -> sorted domain list (CSR): the domains of each node's elements, bucketed by node
+    std::vector<int> dptr(dec.n_nodes + 1, 0), dlist;
+    {
+        std::vector<int> cnt(dec.n_nodes + 1, 0);
+        for (size_t e = 0; e < ne; ++e)
+            for (int64_t i = el.node_ptr[e]; i < el.node_ptr[e + 1]; ++i) cnt[el.nodes[i] + 1]++;
+        for (int n = 0; n < dec.n_nodes; ++n) cnt[n + 1] += cnt[n];
+        std::vector<int> bucket(cnt[dec.n_nodes]);
+        {
+            std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+            for (size_t e = 0; e < ne; ++e)
+                for (int64_t i = el.node_ptr[e]; i < el.node_ptr[e + 1]; ++i) bucket[fill[el.nodes[i]]++] = dec.elem_domain[e];
+        }
+        std::vector<int> len(dec.n_nodes, 0);
+#pragma omp parallel for schedule(static)
+        for (int n = 0; n < dec.n_nodes; ++n) {
+            int *b = bucket.data() + cnt[n], *e = bucket.data() + cnt[n + 1];
+            std::sort(b, e);
+            len[n] = (int)(std::unique(b, e) - b);
+        }
+        for (int n = 0; n < dec.n_nodes; ++n) dptr[n + 1] = dptr[n] + len[n];
+        dlist.resize(dptr[dec.n_nodes]);
+#pragma omp parallel for schedule(static)
+        for (int n = 0; n < dec.n_nodes; ++n)
+            std::copy(bucket.begin() + cnt[n], bucket.begin() + cnt[n] + len[n], dlist.begin() + dptr[n]);
+    }
     dec.node_ndom.resize(dec.n_nodes);
     for (int n = 0; n < dec.n_nodes; ++n) dec.node_ndom[n] = dptr[n + 1] - dptr[n];
 
-    // nodes on the external surface (faces owned by one element); HEXA8 only
+    FETI_LOG(3, "FETI4I: decompose t_nodedom %.3f s\n", now_s() - tdec);
+    // nodes on the external surface: faces owned by one element (HEXA8 only).  Faces are bucketed
+    // by their smallest node; a face appearing once in its bucket is external.
     std::vector<char> ext(dec.n_nodes, 0);
     {
-        std::unordered_map<FaceKey, int, FaceHash> faces;
-        faces.reserve(ne * 6);
+        std::vector<int> cnt(dec.n_nodes + 1, 0);
+        auto face_key = [&](size_t e, int f, int (&k)[4]) {
+            const int *en = &el.nodes[el.node_ptr[e]];
+            for (int i = 0; i < 4; ++i) k[i] = en[kHexFaces[f][i]];
+            std::sort(k, k + 4);
+        };
+        int k[4];
         for (size_t e = 0; e < ne; ++e) {
             if (el.node_ptr[e + 1] - el.node_ptr[e] != 8) continue;
-            const int *en = &el.nodes[el.node_ptr[e]];
             for (int f = 0; f < 6; ++f) {
-                FaceKey k{{en[kHexFaces[f][0]], en[kHexFaces[f][1]], en[kHexFaces[f][2]], en[kHexFaces[f][3]]}};
-                std::sort(k.v, k.v + 4);
-                faces[k]++;
+                face_key(e, f, k);
+                cnt[k[0] + 1]++;
             }
         }
-        for (auto &kv : faces)
-            if (kv.second == 1)
-                for (int i = 0; i < 4; ++i) ext[kv.first.v[i]] = 1;
+        for (int n = 0; n < dec.n_nodes; ++n) cnt[n + 1] += cnt[n];
+        std::vector<std::array<int, 3>> rest(cnt[dec.n_nodes]);   // the other three nodes of each face
+        {
+            std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+            for (size_t e = 0; e < ne; ++e) {
+                if (el.node_ptr[e + 1] - el.node_ptr[e] != 8) continue;
+                for (int f = 0; f < 6; ++f) {
+                    face_key(e, f, k);
+                    rest[fill[k[0]]++] = {k[1], k[2], k[3]};
+                }
+            }
+        }
+        std::vector<char> extf(rest.size(), 0);
+#pragma omp parallel for schedule(dynamic, 1024)
+        for (int n = 0; n < dec.n_nodes; ++n) {
+            auto *b = rest.data() + cnt[n], *e = rest.data() + cnt[n + 1];
+            std::sort(b, e);
+            for (auto *q = b; q < e;) {
+                auto *r = q + 1;
+                while (r < e && *r == *q) ++r;
+                if (r - q == 1) extf[q - rest.data()] = 1;
+                q = r;
+            }
+        }
+        for (int n = 0; n < dec.n_nodes; ++n)
+            for (int i = cnt[n]; i < cnt[n + 1]; ++i)
+                if (extf[i]) {
+                    ext[n] = 1;
+                    for (int v : rest[i]) ext[v] = 1;
+                }
     }
 
+    FETI_LOG(3, "FETI4I: decompose t_faces %.3f s\n", now_s() - tdec);
     // final node order: by (domain list with "longer first on a common prefix", surface group, node ID)
     std::vector<int> used;
     for (int n = 0; n < dec.n_nodes; ++n)
@@ -156,6 +196,7 @@ Decomposition decompose(const ElementData &el, int ndomains_hint, const std::vec
         dec.interval_ext[p] = ext[n];
     }
 
+    FETI_LOG(3, "FETI4I: decompose t_order %.3f s\n", now_s() - tdec);
     // domain local node numbering (interval by interval)
     dec.g2l.assign(dec.ndom, std::unordered_map<int, int>());
     for (int p = 0; p < nint; ++p)
@@ -167,6 +208,7 @@ Decomposition decompose(const ElementData &el, int ndomains_hint, const std::vec
             }
     for (int d = 0; d < dec.ndom; ++d) dec.dom[d].ndofs = dpn * (int)dec.dom[d].nodes.size();
 
+    FETI_LOG(3, "FETI4I: decompose t_g2l %.3f s\n", now_s() - tdec);
     // Dirichlet nodes per (component, interval); values by (node, comp)
     std::vector<char> dmask((size_t)dec.n_nodes * dpn, 0);
     std::vector<double> dval((size_t)dec.n_nodes * dpn, 0.0);
@@ -256,6 +298,7 @@ Decomposition decompose(const ElementData &el, int ndomains_hint, const std::vec
             }
         }
     }
+    FETI_LOG(3, "FETI4I: decompose t_rows %.3f s\n", now_s() - tdec);
     // rows in ascending multiplier order
     for (auto &D : dec.dom) {
         size_t n = D.lam.size();
@@ -268,6 +311,7 @@ Decomposition decompose(const ElementData &el, int ndomains_hint, const std::vec
         permute_d(D.sign); permute_d(D.c);
         D.w.assign(n, 1.0);
     }
+    FETI_LOG(3, "FETI4I: decompose done %.3f s\n", now_s() - tdec);
     return dec;
 }
 
