@@ -1591,6 +1591,7 @@ void GpuSolver::Impl::launch_kplus_multi(const double *in, double *out, int ncol
     int j0 = 0;
     while (j0 < ncol) {
         const int left = ncol - j0;
+        // (groups of 16, 8, 4 and 2 gave 120, 128, 120 and 133 ms of batched e2e on c2)
         int nc = 16;
         while (nc > 1 && (nc > left || (size_t)nc * per_col > kplus_multi_smem(nc))) nc /= 2;
         const size_t sm = (size_t)nc * per_col;
