@@ -1500,6 +1500,10 @@ struct GpuSolver::Impl {
     void launch_hybrid_F(const double *x, double *y, int slot, int cond, double *dot);
     // out = K_c^+ in on the concatenated local primal vectors (Total FETI: K^+ in)
     void launch_kplus_dual(const double *in, double *out);
+    void launch_kplus_dual_multi(const double *in, double *out, int ncol);
+    int hyb_w_size = 0;                       // cluster vector length (sum over clusters)
+    double *hyb_wsave = nullptr, *hyb_hm = nullptr;   // per-column cluster vectors / second K^+ inputs
+    size_t hyb_wsave_n = 0, hyb_hm_n = 0;
     double *d_f = nullptr, *d_kf = nullptr, *d_g = nullptr, *d_rhs = nullptr, *d_sol = nullptr;
     double *h_pinned = nullptr;
     size_t h_pinned_n = 0;
@@ -1516,6 +1520,8 @@ struct GpuSolver::Impl {
         int flat_grid = 1;
         int2 *units4 = nullptr;
         int nunits4 = 0;
+        int2 *dunits = nullptr;   // SYMM units of the Dirichlet blocks (Dirichlet preconditioner)
+        int ndunits = 0;
     } blk;
     void ensure_block(int nr);
     void launch_symm(const TileSetHost &T, bool src32, const double *x64, const float *x32, double *out, int slot,
@@ -1802,6 +1808,7 @@ void GpuSolver::Impl::upload_hybrid(const Decomposition &dec, const Prep &prep) 
     H.b0sign = upload(b0sign);
     H.z = alloc<double>(zof[nd]);
     H.w = alloc<double>(cof[ncl]);
+    hyb_w_size = cof[ncl];
     hyb_rows = (max_nc + HM_ROWS - 1) / HM_ROWS;
     H.part = alloc<double>((size_t)ncl * hyb_rows);
     H.done = alloc<int>(1);
@@ -1816,6 +1823,40 @@ void GpuSolver::Impl::launch_hybrid_F(const double *x, double *y, int slot, int 
     hyb_vt_kernel<<<P.nd, 256, 0, stream>>>(P, H, x, slot, cond);
     hyb_m_kernel<<<dim3(H.ncl, hyb_rows), 256, sizeof(double) * H.max_nc, stream>>>(P, H, slot, cond, dot);
     hyb_v_kernel<<<P.nd, 256, sizeof(double) * hyb_max_m, stream>>>(P, H, y, slot, cond);
+    CUDA_CHECK(cudaGetLastError());
+}
+
+// K_c^+ (or K^+) on ncol columns (stride ntot): both K^+ passes of the cluster solve on all columns
+// at once (kplus_multi_kernel); the small cluster steps run column by column, with each column's
+// cluster vector kept for its final R alpha step.
+void GpuSolver::Impl::launch_kplus_dual_multi(const double *in, double *out, int ncol) {
+    launch_kplus_multi(in, out, ncol, KPLUS_FULL, nullptr);
+    if (!hybrid) return;
+    const int wn = hyb_w_size;
+    if (hyb_wsave_n < (size_t)ncol * wn) {
+        hyb_wsave = alloc<double>((size_t)ncol * wn);
+        hyb_wsave_n = (size_t)ncol * wn;
+    }
+    if (hyb_hm_n < (size_t)ncol * ntot) {
+        hyb_hm = alloc<double>((size_t)ncol * ntot);
+        hyb_hm_n = (size_t)ncol * ntot;
+    }
+    for (int j = 0; j < ncol; ++j) {
+        const double *inj = in + (size_t)j * ntot;
+        double *outj = out + (size_t)j * ntot, *hj = hyb_hm + (size_t)j * ntot;
+        hyb_kz_kernel<<<P.nd, 256, 0, stream>>>(P, H, d_doff, d_rofs, d_R, outj, inj);
+        hyb_m_kernel<<<dim3(H.ncl, hyb_rows), 256, sizeof(double) * H.max_nc, stream>>>(P, H, 0, 0, nullptr);
+        hyb_copy_kernel<<<std::max(1, std::min(4096, (ntot + 255) / 256)), 256, 0, stream>>>(inj, hj, ntot);
+        hyb_kb0_kernel<<<(P.nd + 127) / 128, 128, 0, stream>>>(P, H, d_doff, hj);
+        CUDA_CHECK(cudaMemcpyAsync(hyb_wsave + (size_t)j * wn, H.w, sizeof(double) * wn, cudaMemcpyDeviceToDevice,
+                                   stream));
+    }
+    launch_kplus_multi(hyb_hm, out, ncol, KPLUS_FULL, nullptr);
+    for (int j = 0; j < ncol; ++j) {
+        HybDev Hj = H;
+        Hj.w = hyb_wsave + (size_t)j * wn;
+        hyb_kr_kernel<<<P.nd, 256, 0, stream>>>(P, Hj, d_doff, d_rofs, d_R, out + (size_t)j * ntot);
+    }
     CUDA_CHECK(cudaGetLastError());
 }
 
@@ -4025,7 +4066,21 @@ void GpuSolver::Impl::ensure_block(int nr) {
         for (int I4 = 0; 4 * I4 < tn[m]; ++I4) units4.push_back(make_int2(m, I4));
     blk.units4 = upload(units4);
     blk.nunits4 = (int)units4.size();
-    B.unit_dot = alloc<double>(std::max(units.size(), units4.size()) * nr);
+    size_t max_units = std::max(units.size(), units4.size());
+    if (opt.precond == PREC_DIRICHLET) {
+        // SYMM units of the Dirichlet blocks S_dir (T space)
+        std::vector<int2> du;
+        const std::vector<int> &dtn = Dir.h_tn;
+        std::vector<int> dorder(dtn.size());
+        std::iota(dorder.begin(), dorder.end(), 0);
+        std::stable_sort(dorder.begin(), dorder.end(), [&](int a, int b) { return dtn[a] > dtn[b]; });
+        for (int m : dorder)
+            for (int I = 0; I < dtn[m]; ++I) du.push_back(make_int2(m, I));
+        blk.dunits = upload(du);
+        blk.ndunits = (int)du.size();
+        max_units = std::max(max_units, du.size());
+    }
+    B.unit_dot = alloc<double>(max_units * nr);
     blk.rhs = alloc<double>((size_t)std::max(1, n_caller) * nr);
     blk.sol = alloc<double>((size_t)std::max(1, n_caller) * nr);
     blk.f = alloc<double>((size_t)ntot * nr);
@@ -4100,7 +4155,10 @@ static void symm_tc_launch(int nsm, int nunits, cudaStream_t st, TileSetDev td, 
 void GpuSolver::Impl::launch_symm(const TileSetHost &T, bool src32, const double *x64, const float *x32, double *out,
                                   int slot, int mode) {
     const int nr = blk.nr;
-    if (opt.symm_tensor && T.prec == SCHUR_FP32 && src32 && nr >= 8) {
+    const bool dir = &T == &Dir;
+    const int2 *units = dir ? blk.dunits : blk.units;
+    const int nunits = dir ? blk.ndunits : blk.nunits;
+    if (!dir && opt.symm_tensor && T.prec == SCHUR_FP32 && src32 && nr >= 8) {
         TileSetDev td = T.dev();
         switch (nr) {
         case 8: symm_tc_launch<8>(nsm, blk.nunits4, stream, td, P, blk.B, x32, out, blk.units4, slot, mode); break;
@@ -4112,10 +4170,10 @@ void GpuSolver::Impl::launch_symm(const TileSetHost &T, bool src32, const double
     }
     const size_t TB = (size_t)TILE * TILE * (T.prec == SCHUR_FP64 ? 8 : 4);
     const size_t sm = 8 * TB;
-    const int ncta = (blk.nunits + 7) / 8;
+    const int ncta = (nunits + 7) / 8;
     TileSetDev td = T.dev();
     FETI_CHECK(T.prec != SCHUR_BF16, "FETI4I: the multi right-hand-side solve supports FP64 and FP32 Schur storage");
-#define SYMM(PR, NR_, S) symm_launch<PR, NR_, S>(nsm, ncta, sm, stream, td, P, blk.B, x64, x32, out, blk.units, blk.nunits, slot, mode)
+#define SYMM(PR, NR_, S) symm_launch<PR, NR_, S>(nsm, ncta, sm, stream, td, P, blk.B, x64, x32, out, units, nunits, slot, mode)
 #define SYMM_NR(PR, S)                       \
     switch (nr) {                            \
     case 4: SYMM(PR, 4, S); break;           \
@@ -4156,6 +4214,12 @@ void GpuSolver::Impl::launch_block_iteration(int slot) {
         bu_flat_kernel<PREC_LUMPED><<<fgrid, 256, 0, stream>>>(P, B, slot);
         bell_flat2_kernel<<<fgrid, 256, 0, stream>>>(P, B, slot);
         break;
+    case PREC_DIRICHLET:
+        // u_T = B^T W w, then v_T = S_dir u_T (FP64 SYMM over the Dirichlet blocks)
+        BW(PREC_WEIGHT)
+        bu_flat_kernel<PREC_LUMPED><<<fgrid, 256, 0, stream>>>(P, B, slot);
+        launch_symm(Dir, false, B.uT, nullptr, B.vT, slot, 2);
+        break;
     default:
         BW(PREC_WEIGHT)
         bu_flat_kernel<PREC_WEIGHT><<<fgrid, 256, 0, stream>>>(P, B, slot);
@@ -4184,8 +4248,6 @@ void GpuSolver::solve_multi(const double *rhs, int nrhs, int rhs_size, double *s
     Impl &I = *impl;
     DevProblem &P = I.P;
     FETI_CHECK(nrhs >= 1 && nrhs <= 32, "FETI4ISolveMulti: 1..32 right-hand sides per call");
-    FETI_CHECK(I.opt.precond != PREC_DIRICHLET,
-               "FETI4ISolveMulti: the Dirichlet preconditioner is not available for several right-hand sides");
     int nr = 4;
     while (nr < nrhs) nr *= 2;
     I.ensure_block(nr);
@@ -4203,7 +4265,7 @@ void GpuSolver::solve_multi(const double *rhs, int nrhs, int rhs_size, double *s
                                                                               ntot, nr);
         CUDA_CHECK(cudaMemsetAsync(I.blk.kf, 0, sizeof(double) * (size_t)ntot * nr, I.stream));
         if (I.hybrid)
-            for (int j = 0; j < nrhs; ++j) I.launch_kplus_dual(I.blk.f + (size_t)j * ntot, I.blk.kf + (size_t)j * ntot);
+            I.launch_kplus_dual_multi(I.blk.f, I.blk.kf, nrhs);
         else
             I.launch_kplus_multi(I.blk.f, I.blk.kf, nrhs, KPLUS_TOUCHED, I.blk.zk);
         bevec_kernel<<<nd * nr, TPB, 0, I.stream>>>(P, B, I.d_doff, I.d_rdofs, I.d_Rd, I.blk.f, ntot);
@@ -4276,7 +4338,7 @@ void GpuSolver::solve_multi(const double *rhs, int nrhs, int rhs_size, double *s
                                                       I.blk.g, ntot);
         bprimal_bt_kernel<<<(P.NT * nr + 255) / 256, 256, 0, I.stream>>>(P, B, I.d_tdof_g, I.d_rsign, I.blk.g, ntot);
         if (I.hybrid)
-            for (int j = 0; j < nrhs; ++j) I.launch_kplus_dual(I.blk.g + (size_t)j * ntot, I.blk.kf + (size_t)j * ntot);
+            I.launch_kplus_dual_multi(I.blk.g, I.blk.kf, nrhs);
         else
             I.launch_kplus_multi(I.blk.g, I.blk.kf, nrhs, KPLUS_PRIMAL, I.blk.zk);
         CUDA_CHECK(cudaMemsetAsync(I.blk.sol, 0, sizeof(double) * (size_t)nc * nr, I.stream));

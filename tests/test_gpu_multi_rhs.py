@@ -36,7 +36,9 @@ def direct(P, f):
                                                          ("heat", F.FP32, 32, F.PREC_LUMPED, 0),
                                                          ("heat", F.FP32, 32, F.PREC_LUMPED, 1),
                                                          ("heat", F.FP32, 13, F.PREC_WEIGHT, 1),
-                                                         ("heat", F.FP64, 3, F.PREC_NONE, 0)])
+                                                         ("heat", F.FP64, 3, F.PREC_NONE, 0),
+                                                         ("elast", F.FP32, 8, F.PREC_DIRICHLET, 1),
+                                                         ("heat", F.FP64, 6, F.PREC_DIRICHLET, 0)])
 def test_multi_rhs_matches_single_and_direct(kind, schur, nrhs, prec, tensor):
     """tensor=1: FP32 SYMM on the tensor cores (tcgen05, 3xTF32) inside FP64 residual replacement."""
     P = (problems.elasticity_cube(domains=(3, 2, 2), elements=(3, 3, 3)) if kind == "elast"
@@ -60,9 +62,15 @@ def test_multi_rhs_matches_single_and_direct(kind, schur, nrhs, prec, tensor):
     inst.destroy()
 
 
-def test_multi_rhs_rejects_dirichlet_preconditioner():
-    P = problems.elasticity_cube(domains=(2, 1, 1), elements=(2, 2, 2))
-    inst = problems.make_instance(P, iopts={F.PRECONDITIONER: F.PREC_DIRICHLET, F.VERBOSE_LEVEL: 0})
-    with pytest.raises(F.FETI4IError, match="Dirichlet"):
-        inst.solve_multi(np.stack([P.rhs(), P.rhs()]))
+def test_multi_rhs_dirichlet_hybrid():
+    """Dirichlet preconditioner in the block PCG (S_dir SYMM) with Hybrid Total FETI."""
+    P = problems.elasticity_cube(clusters=(2, 2, 1), domains=(1, 2, 2), elements=(3, 3, 3))
+    inst = problems.make_instance(P, iopts={F.PRECONDITIONER: F.PREC_DIRICHLET, F.VERBOSE_LEVEL: 0,
+                                            F.FETI_METHOD: 1, F.MAX_ITERATIONS: 3000},
+                                  ropts={F.PRECISION: 1e-10}, clusters=P.sub_cluster())
+    R = load_cases(P, 4, 3)
+    U = inst.solve_multi(R)
+    for j in range(R.shape[0]):
+        ud = direct(P, R[j])
+        assert np.linalg.norm(U[j] - ud) <= 1e-8 * np.linalg.norm(ud)
     inst.destroy()
