@@ -6,7 +6,8 @@
 // [k0, rend)), and three launches process all items of the step together:
 //   diag_kernel    one CTA per item: Cholesky of the w x w diagonal block in shared memory;
 //   trsm_kernel    one CTA per 64-row block below it: L_ik = A_ik L_kk^-T;
-//   update_kernel  one CTA per 64 x 64 lower tile of the trailing block: A_IJ -= L_Ik L_Jk^T.
+//   update_pipe_kernel  one CTA per 64 x 64 lower tile of the trailing block: A_IJ -= L_Ik L_Jk^T
+//                  (FP64 MMA, 128-deep panels streamed by cp.async).
 // Phases: untouched columns (rows of K only: the B~ rows are zero there and stay zero), touched
 // columns (B~ rows included), fix columns after the host's regularisation of the fix-DOF block.
 #include "gpu_prep.h"
@@ -61,7 +62,7 @@ struct JobD {
     int m0;               // B0 rows
     long long vo;         // offset of the [B; B0] K^+ B0^T block in the staging buffer, -1 without B0
     long long boff;       // offset of its B~ rows in bpos / bsign
-    long long lp, s, sd;  // offsets of its outputs in the staging buffer (doubles)
+    long long s;          // offset of its S output in the staging buffer (doubles), -1 without
     long long fx;         // offset of its fix-DOF block in the fix buffer
 };
 
@@ -412,7 +413,6 @@ __global__ void copy_sym_kernel(const JobD *jobs, const SubD *subs, const double
     int r0, m;
     long long off;
     if (which == 0) { r0 = J.n; m = J.ni; off = J.s; }                  // -S
-    else if (which == 1) { r0 = J.n1; m = J.n - J.n1; off = J.sd; }     // Dirichlet Schur complement
     else { r0 = J.nc; m = J.ns; off = J.fx; }                           // fix-DOF block
     if (off < 0) return;
     const long long tot = (long long)m * m;
@@ -439,18 +439,6 @@ __global__ void copy_b0_kernel(const JobD *jobs, const SubD *subs, const double 
     }
 }
 
-// packed lower factor of the leading n x n block: column j holds rows j..n-1
-__global__ void pack_kernel(const JobD *jobs, const SubD *subs, const double *arena, double *stage) {
-    const JobD J = jobs[blockIdx.y];
-    if (J.lp < 0) return;
-    const SubD sd = subs[J.sub];
-    const double *A = arena + sd.a;
-    for (int j = blockIdx.x; j < J.n; j += gridDim.x) {
-        const size_t p0 = (size_t)j * J.n - (size_t)j * (j - 1) / 2;
-        const double *col = A + (size_t)j * sd.ld;
-        for (int i = j + threadIdx.x; i < J.n; i += blockDim.x) stage[J.lp + p0 + (i - j)] = col[i];
-    }
-}
 
 // A(nc + i, nc + j) += reg(i, j), i >= j
 __global__ void add_reg_kernel(const JobD *jobs, const SubD *subs, double *arena, const double *reg) {   // reg at J.fx
@@ -764,7 +752,7 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
     // per-job sizes and batches
     struct Sz {
         int ld, N;
-        size_t a, lp, s, sd, fx, vals, pos, v;
+        size_t a, s, fx, vals, pos, v;
     };
     std::vector<Sz> sz(nj);
     for (int j = 0; j < nj; ++j) {
@@ -775,9 +763,7 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
         z.N = J.n + J.ni + (int)J.b0pos.size();
         z.ld = (z.N + 31) / 32 * 32;
         z.a = (size_t)z.ld * z.N;
-        z.lp = (resident || !J.Lp) ? 0 : (size_t)J.n * (J.n + 1) / 2;
         z.s = (resident || !J.S) ? 0 : (size_t)J.ni * J.ni;
-        z.sd = (J.want_sdir && !resident) ? (size_t)(J.n - J.n1) * (J.n - J.n1) : 0;
         z.fx = (size_t)J.ns * J.ns;
         z.v = J.b0pos.empty() ? 0 : (size_t)(J.ni + J.b0pos.size()) * J.b0pos.size();
         z.vals = 0;
@@ -792,7 +778,7 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
     {
         size_t cur = 0;
         for (int j = 0; j < nj; ++j) {
-            const size_t bytes = 8 * (sz[j].a + sz[j].lp + sz[j].s + sz[j].sd + sz[j].fx + sz[j].vals + sz[j].v +
+            const size_t bytes = 8 * (sz[j].a + sz[j].s + sz[j].fx + sz[j].vals + sz[j].v +
                                       (resident ? 16 * (size_t)jobs[j].n : 0)) +
                                  4 * sz[j].pos;
             if (j > bstart.back() && cur + bytes > mem_budget) {
@@ -872,12 +858,8 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
             d.nrow = J.ni + d.m0;
             d.boff = (long long)b_tot;
             b_tot += d.nrow;
-            d.lp = z.lp ? (long long)st_tot : -1;
-            st_tot += z.lp;
             d.s = z.s ? (long long)st_tot : -1;
             st_tot += z.s;
-            d.sd = J.want_sdir ? (long long)st_tot : -1;
-            st_tot += z.sd;
             d.vo = z.v ? (long long)st_tot : -1;
             st_tot += z.v;
             d.fx = (long long)fx_tot;
@@ -1061,12 +1043,7 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
             PCHECK(cudaGetLastError());
         };
         run(ph1, o1);
-        if (resident) {
-            if (store->dir_tiles) tiles(1, store->dir_tiles, store->dir_tile0, 1.0);   // Dirichlet
-        } else {
-            copy_sym_kernel<<<dim3(64, nb), PT>>>(djobs.p, dsubs.p, arena.p, stage.p, 1, 1.0);   // Dirichlet
-            ++tm.launches;
-        }
+        if (resident && store->dir_tiles) tiles(1, store->dir_tiles, store->dir_tile0, 1.0);   // Dirichlet
         run(ph2, o2);
         copy_sym_kernel<<<dim3(1, nb), PT>>>(djobs.p, dsubs.p, arena.p, fxb.p, 2, 1.0);       // fix block
         ++tm.launches;
@@ -1165,8 +1142,7 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
             PCHECK(cudaGetLastError());
         } else {
             copy_sym_kernel<<<dim3(256, nb), PT>>>(djobs.p, dsubs.p, arena.p, stage.p, 0, -1.0);
-            pack_kernel<<<dim3(256, nb), PT>>>(djobs.p, dsubs.p, arena.p, stage.p);
-            tm.launches += 2;
+            tm.launches += 1;
             PCHECK(cudaGetLastError());
         }
         PCHECK(cudaEventRecord(ev1));
@@ -1205,10 +1181,7 @@ void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const
                 }
                 continue;
             }
-            if (J.Lp) PCHECK(cudaMemcpy(J.Lp, stage.p + jd[q].lp, sz[j0 + q].lp * sizeof(double), cudaMemcpyDeviceToHost));
             if (J.S) PCHECK(cudaMemcpy(J.S, stage.p + jd[q].s, sz[j0 + q].s * sizeof(double), cudaMemcpyDeviceToHost));
-            if (J.want_sdir && J.Sdir)
-                PCHECK(cudaMemcpy(J.Sdir, stage.p + jd[q].sd, sz[j0 + q].sd * sizeof(double), cudaMemcpyDeviceToHost));
         }
         th_out += now_s() - tq;
         ++tm.batches;

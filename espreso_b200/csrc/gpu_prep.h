@@ -62,11 +62,10 @@ struct DevFactorJob {
     // set by the regularisation callback: kernel dimension and the kernel eigenvectors N (ns x nk)
     int nk = 0;
     std::vector<double> N;
-    // outputs (host buffers sized by the caller; with a DevPrepStore only Rp is written)
+    // outputs (host buffers sized by the caller)
     double *Rp = nullptr;        // n x nk: kernel [-L_rr^-T L_sr^T N; N] in factor order (store mode)
-    double *Lp = nullptr;        // n(n+1)/2: packed lower factor of K_reg (factor order)
-    double *S = nullptr;         // ni x ni, column-major, full symmetric
-    double *Sdir = nullptr;      // t x t (t = n - n1), column-major, full symmetric
+    double *S = nullptr;         // ni x ni, column-major, full symmetric (without a store: the
+                                 // coarse problem's dense inverse)
     double knorm = 0.0;          // Frobenius norm of the assembled K
     int fail_col = -1;           // first column with a non-positive pivot, -1 if none
 };
@@ -88,8 +87,8 @@ using RegulariseFn = std::function<void(int job, const double *Sss, double *reg)
 // Factorises every job on the current CUDA device, in batches whose dense matrices fit
 // `mem_budget` bytes (0: half of the free device memory).  With `store` (sized by this call for
 // `ndom` subdomains; jobs' slots index it) S_i, the Dirichlet blocks and the K^+ factor stay on the
-// device as tiles and only the kernels Rp come back; without it Lp, S and Sdir are copied to the
-// host.  Throws feti::Error on CUDA errors.
+// device as tiles and only the kernels Rp come back; without it S is copied to the host (the dense
+// inverse of the coarse problem).  Throws feti::Error on CUDA errors.
 void device_factor(const ElementData &el, std::vector<DevFactorJob> &jobs, const RegulariseFn &regularise,
                    size_t mem_budget, DevFactorTimes *times, DevPrepStore *store = nullptr, int ndom = 0);
 

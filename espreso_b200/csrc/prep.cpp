@@ -438,9 +438,8 @@ static void prep_all_device(const ElementData &el, const Decomposition &dec, con
     // S_i, the Dirichlet blocks and K^+ stay on the device (the tile stores of the dual iteration);
     // Hybrid Total FETI appends its corner rows B0, and B K^+ B0^T, B0 K^+ B0^T come back for the
     // cluster problems.
-    const bool resident = true;
-    std::shared_ptr<DevPrepStore> store = resident ? std::make_shared<DevPrepStore>() : nullptr;
-    std::vector<std::vector<double>> Rps(resident ? nd : 0);
+    std::shared_ptr<DevPrepStore> store = std::make_shared<DevPrepStore>();
+    std::vector<std::vector<double>> Rps(nd);
     std::vector<DevFactorJob> jobs(ids.size());
     for (size_t q = 0; q < ids.size(); ++q) {
         const int d = ids[q];
@@ -472,13 +471,6 @@ static void prep_all_device(const ElementData &el, const Decomposition &dec, con
             J.V = S.BKB0.data();
             J.F0 = S.B0KB0.data();
         }
-        if (resident) continue;
-        S.Lp.assign((size_t)S.n * (S.n + 1) / 2, 0.0);
-        S.S.assign((size_t)S.ni * S.ni, 0.0);
-        if (J.want_sdir) S.Sdir.assign((size_t)S.t * S.t, 0.0);
-        J.Lp = S.Lp.data();
-        J.S = S.S.data();
-        J.Sdir = J.want_sdir ? S.Sdir.data() : nullptr;
     }
     auto reg = [&](int q, const double *Sss, double *r) {
         const int d = ids[q];
@@ -487,10 +479,8 @@ static void prep_all_device(const ElementData &el, const Decomposition &dec, con
             DevFactorJob &J = jobs[q];
             J.nk = work[d].defect;
             J.N.assign(work[d].V.begin(), work[d].V.begin() + (size_t)J.nk * J.ns);
-            if (resident) {
-                Rps[d].assign((size_t)J.n * J.nk, 0.0);
-                J.Rp = Rps[d].data();
-            }
+            Rps[d].assign((size_t)J.n * J.nk, 0.0);
+            J.Rp = Rps[d].data();
         } catch (const std::exception &ex) {
             errors[d] = ex.what();
             std::fill(r, r + (size_t)work[d].ns * work[d].ns, 0.0);
@@ -519,8 +509,7 @@ static void prep_all_device(const ElementData &el, const Decomposition &dec, con
         const int d = ids[k];
         if (!errors[d].empty()) continue;
         try {
-            if (resident) finish_kernel(dec, d, sub[d], work[d], Rps[d]);
-            else prep_finish(dec, d, sub[d], work[d]);
+            finish_kernel(dec, d, sub[d], work[d], Rps[d]);
         } catch (const std::exception &ex) {
             errors[d] = ex.what();
         }
