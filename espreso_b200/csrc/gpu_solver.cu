@@ -3166,45 +3166,6 @@ __global__ void __launch_bounds__(TPBB) bz_kernel(DevProblem P, BlockDev B, int 
 // thread column: the grid stride is a multiple of 32 >= nr, so every thread stays on column
 // threadIdx.x & (nr - 1) and block_sum_cols combines the right partial sums
 
-// w = r - G^T alpha, |w_j|^2 (and y = w, rho_j = |w_j|^2 without a preconditioner)
-template <int PRECOND, int KC>
-__global__ void __launch_bounds__(256) bw_flat_kernel(DevProblem P, BlockDev B, int slot) {
-    __shared__ double sh[8 * 32];
-    __shared__ double cols[32];
-    const int iter = P.st->iter_base + slot;
-    if (skip_iter(P.st, iter)) return;
-    const int nr = B.nr;
-    const long long cnt = (long long)P.NL * nr, stride = (long long)gridDim.x * blockDim.x;
-    double ww = 0.0;
-    for (long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; i0 < cnt; i0 += UNR * stride) {
-        double rv[UNR], ga[UNR], mv[UNR];
-#pragma unroll
-        for (int u = 0; u < UNR; ++u) {
-            const long long i = i0 + u * stride;
-            if (i < cnt) {
-                const int e = (int)(i >> B.lg), j = (int)(i & (nr - 1));
-                rv[u] = B.r[i];
-                ga[u] = gt_alpha_colk<KC>(P, e, j, nr, B.alpha);
-                mv[u] = P.minv[e];
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < UNR; ++u) {
-            const long long i = i0 + u * stride;
-            if (i < cnt) {
-                const double wv = rv[u] - ga[u];
-                B.w[i] = wv;
-                if (PRECOND == PREC_NONE) B.y[i] = wv;
-                ww += wv * wv * mv[u];
-            }
-        }
-    }
-    block_sum_cols(ww, nr, sh, cols);
-    grid_total_cols(cols, B.part, nr, B.done + DONE_W, B.scal + SC_WN2 * nr);
-    if (PRECOND == PREC_NONE)
-        grid_total_cols(cols, B.part + (size_t)gridDim.x * nr, nr, B.done + DONE_RHO, B.scal + SC_RHO * nr);
-}
-
 // u_T = B^T W w over all touched DOFs (v_T = u_T for the weight-function preconditioner)
 template <int PRECOND>
 __global__ void __launch_bounds__(256) bu_flat_kernel(DevProblem P, BlockDev B, int slot) {
@@ -3299,6 +3260,49 @@ __global__ void __launch_bounds__(256) bell_flat2_kernel(DevProblem P, BlockDev 
         }
         *reinterpret_cast<double2 *>(B.vT + (size_t)t * nr + j) = make_double2(s0.x + s1.x, s0.y + s1.y);
     }
+}
+
+// w = r - G^T alpha, |w_j|^2 (and y = w, rho_j = |w_j|^2 without a preconditioner); two columns
+// per thread, as in bell_flat2_kernel
+template <int PRECOND, int KC>
+__global__ void __launch_bounds__(256) bw_flat2_kernel(DevProblem P, BlockDev B, int slot) {
+    __shared__ double sh[8 * 32];
+    __shared__ double cols[32];
+    const int iter = P.st->iter_base + slot;
+    if (skip_iter(P.st, iter)) return;
+    const int nr = B.nr, lh = B.lg - 1;
+    const long long cnt = (long long)P.NL * (nr >> 1), stride = (long long)gridDim.x * blockDim.x;
+    double s0 = 0.0, s1 = 0.0;
+    for (long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; i0 < cnt; i0 += UNR * stride) {
+        double2 rv[UNR], ga[UNR];
+        double mv[UNR];
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            const long long i = i0 + u * stride;
+            if (i < cnt) {
+                const int e = (int)(i >> lh), j = 2 * (int)(i & ((nr >> 1) - 1));
+                rv[u] = *reinterpret_cast<const double2 *>(B.r + (size_t)e * nr + j);
+                ga[u] = gt_alpha_colk2<KC>(P, e, j, nr, B.alpha);
+                mv[u] = P.minv[e];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            const long long i = i0 + u * stride;
+            if (i < cnt) {
+                const int e = (int)(i >> lh), j = 2 * (int)(i & ((nr >> 1) - 1));
+                const double2 wv = make_double2(rv[u].x - ga[u].x, rv[u].y - ga[u].y);
+                *reinterpret_cast<double2 *>(B.w + (size_t)e * nr + j) = wv;
+                if (PRECOND == PREC_NONE) *reinterpret_cast<double2 *>(B.y + (size_t)e * nr + j) = wv;
+                s0 += wv.x * wv.x * mv[u];
+                s1 += wv.y * wv.y * mv[u];
+            }
+        }
+    }
+    block_sum_cols2(s0, s1, nr, sh, cols);
+    grid_total_cols(cols, B.part, nr, B.done + DONE_W, B.scal + SC_WN2 * nr);
+    if (PRECOND == PREC_NONE)
+        grid_total_cols(cols, B.part + (size_t)gridDim.x * nr, nr, B.done + DONE_RHO, B.scal + SC_RHO * nr);
 }
 
 template <int KC>
@@ -4203,9 +4207,9 @@ void GpuSolver::Impl::launch_block_iteration(int slot) {
     const int fgrid = blk.flat_grid;
 #define BW(PC)                                                                              \
     switch (P.KS) {                                                                         \
-    case 1: bw_flat_kernel<PC, 1><<<fgrid, 256, 0, stream>>>(P, B, slot); break;            \
-    case 6: bw_flat_kernel<PC, 6><<<fgrid, 256, 0, stream>>>(P, B, slot); break;            \
-    default: bw_flat_kernel<PC, 0><<<fgrid, 256, 0, stream>>>(P, B, slot); break;           \
+    case 1: bw_flat2_kernel<PC, 1><<<fgrid, 256, 0, stream>>>(P, B, slot); break;           \
+    case 6: bw_flat2_kernel<PC, 6><<<fgrid, 256, 0, stream>>>(P, B, slot); break;           \
+    default: bw_flat2_kernel<PC, 0><<<fgrid, 256, 0, stream>>>(P, B, slot); break;          \
     }
     switch (opt.precond) {
     case PREC_NONE: BW(PREC_NONE) break;
