@@ -338,6 +338,7 @@ def run_ours(args):
                    "prep_device_tflops": (st0["prep_device_flops"] / st0["prep_device_ms"] * 1e-9
                                           if st0["prep_device_ms"] > 0 else None),
                    "tuning": inst.tuning(),
+                   "kplus_tiles_applied": st0["kplus_tiles"],
                    "reliable_delta": args.delta},
         "fp64_gpu": {"ms": fp64_ms, "pcg_iterations": int(st64["iterations"]), "speedup_mixed": fp64_ms / step_ms,
                      "fapply_ms": fp64_f},

@@ -487,6 +487,7 @@ void FETI4IGetStats(FETI4IInstance instance, FETI4IInt size, FETI4IReal *stats) 
         v[FETI4I_STAT_ELEMENTS] = (double)I->el.nelem();
         v[FETI4I_STAT_PREP_DEVICE_MS] = I->prep.t_device_factor_ms;
         v[FETI4I_STAT_PREP_DEVICE_FLOPS] = I->prep.device_factor_flops;
+        v[FETI4I_STAT_KPLUS_TILES] = I->gpu ? I->gpu->kplus_tile_fraction() : 0.0;
         for (int i = 0; i < size && i < FETI4I_STAT_SIZE; ++i) stats[i] = v[i];
     });
 }

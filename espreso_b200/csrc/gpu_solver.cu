@@ -152,6 +152,39 @@ struct TileSetDev {
 };
 
 // ---------------------------------------------------------------------------------------------
+// Programmatic dependent launch (opt-in, FETI4I_PDL=1).  With it a kernel launched by launch_pdl
+// may be scheduled while its predecessor in the stream still drains, and pdl_enter() returns once
+// the predecessor has completed and its writes are visible, so it is the first
+// statement of every kernel launched that way.  For an ordinary launch it is a no-op.  Measured on
+// the heat workload of 512 subdomains: 6.57 ms per solve with it against 6.55 ms without, and
+// 6.9 ms when the successor was also released early (griddepcontrol.launch_dependents), so it is
+// off by default.
+__device__ __forceinline__ void pdl_enter() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+bool pdl_enabled() {
+    static const bool on = [] {
+        const char *e = getenv("FETI4I_PDL");
+        return e && e[0] == '1';
+    }();
+    return on;
+}
+
+// kernel<<<grid, block, smem, stream>>>(args...) with the programmatic-serialization attribute
+template <typename... KA, typename... A>
+void launch_pdl(void (*kernel)(KA...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream, A... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    CUDA_CHECK(cudaLaunchKernelEx(&cfg, kernel, static_cast<KA>(args)...));
+}
+
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll
@@ -402,6 +435,7 @@ __device__ __forceinline__ void tile_fma(const uint4 (&raw)[TILE / TileT<PREC>::
 template <int PREC, int MODE>
 __global__ void __launch_bounds__(256, 2)
 tile_symv_kernel(TileSetDev ts, DevProblem P, const double *src, const double *src2, double *out, int slot) {
+    pdl_enter();
     using Acc = typename TileT<PREC>::Acc;
     constexpr int EPC = TileT<PREC>::EPC;
     constexpr int CPR = TILE / EPC;          // 16-byte chunks per tile row (= loads per lane)
@@ -581,6 +615,7 @@ template <int PREC, int MODE>
 __global__ void __launch_bounds__((TMA_CONSUMERS + 1) * 32, 1)
 tile_symv_tma_kernel(TileSetDev ts, DevProblem P, const double *src, const double *src2, double *out, int slot,
                      int nstages, int xs_elems) {
+    pdl_enter();
     using Acc = typename TileT<PREC>::Acc;
     constexpr int EPC = TileT<PREC>::EPC;
     constexpr int CPR = TILE / EPC;
@@ -744,6 +779,7 @@ tile_symv_tma_kernel(TileSetDev ts, DevProblem P, const double *src, const doubl
 // ---------------------------------------------------------------------------------------------
 // coarse problem: out = (GG^T)^-1 in   (dense symmetric, one warp per row)
 __global__ void coarse_kernel(DevProblem P, const double *in, double *out, int slot, int looped) {
+    pdl_enter();
     if (looped) {
         int iter = P.st->iter_base + slot;
         if (skip_iter(P.st, iter)) return;
@@ -770,12 +806,14 @@ __global__ void zero_kernel(double *v, int n) {
 }
 
 __global__ void zero2_kernel(double *a, double *b, int n) {
+    pdl_enter();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) { a[i] = 0.0; b[i] = 0.0; }
 }
 
 // r = b - assemble(Ax); d = G r per subdomain; ||b||^2 total (initial call).  One CTA per subdomain.
 __global__ void r0_kernel(DevProblem P, double *Ax, int replace_mode, int slot) {
+    pdl_enter();
     extern __shared__ double rv_s[];
     __shared__ double sh[32 * KMAX];
     if (replace_mode) {
@@ -823,6 +861,7 @@ __global__ void tol_kernel(DevProblem P) {
 // and rho = y.w is taken here.  One CTA per subdomain.
 template <int PRECOND>
 __global__ void __launch_bounds__(TPB1) w_prec_kernel(DevProblem P, int slot) {
+    pdl_enter();
     extern __shared__ double sm[];
     __shared__ double sh[32];
     const int iter = P.st->iter_base + slot;
@@ -873,6 +912,7 @@ __global__ void __launch_bounds__(TPB1) w_prec_kernel(DevProblem P, int slot) {
 
 // z = assemble(W B v_T); d = G z.  One CTA per subdomain.
 __global__ void z_kernel(DevProblem P, int slot) {
+    pdl_enter();
     extern __shared__ double zs[];
     __shared__ double sh[32 * KMAX];
     const int iter = P.st->iter_base + slot;
@@ -892,6 +932,7 @@ __global__ void z_kernel(DevProblem P, int slot) {
 
 // y = z - G^T alpha, rho = y.w total; clear the F apply accumulators.
 __global__ void y_kernel(DevProblem P, double *Ax64, int slot) {
+    pdl_enter();
     __shared__ double sh[32];
     const int iter = P.st->iter_base + slot;
     if (skip_iter(P.st, iter)) return;
@@ -908,6 +949,7 @@ __global__ void y_kernel(DevProblem P, double *Ax64, int slot) {
 }
 
 __global__ void zero_vT_kernel(DevProblem P, int slot) {
+    pdl_enter();
     const int iter = P.st->iter_base + slot;
     if (skip_iter(P.st, iter)) return;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < P.NT; t += gridDim.x * blockDim.x) P.vT[t] = 0.0;
@@ -915,6 +957,7 @@ __global__ void zero_vT_kernel(DevProblem P, int slot) {
 
 // p = y + beta p, x += alpha p, r -= alpha assemble(Ap), d = G r, convergence check.
 __global__ void update_kernel(DevProblem P, int slot) {
+    pdl_enter();
     extern __shared__ double rs_s[];
     __shared__ double sh[32 * KMAX];
     const int iter = P.st->iter_base + slot;
@@ -971,6 +1014,7 @@ __global__ void update_kernel(DevProblem P, int slot) {
 }
 
 __global__ void chunk_end_kernel(DevProblem P, int chunk) {
+    pdl_enter();
     if (threadIdx.x == 0 && blockIdx.x == 0) P.st->iter_base += chunk;
 }
 
@@ -993,7 +1037,27 @@ struct KplusDev {
     const double *L;         // tiles
     const int *jt;           // first 32-block holding a touched DOF (factor order: untouched DOFs first)
     double *z;               // forward results L^-1 f kept by mode 1 (factor order, concatenated)
+    // tiles of block column J that are not all zero (the factor keeps the envelope of K_reg, so
+    // whole tiles left of a row's first coupling are exactly zero): rows[cptr[cbase[d] + J] ..
+    // cptr[cbase[d] + J + 1]) in ascending order, the diagonal tile first
+    const int *cbase;
+    const int *cptr;
+    const int *rows;
 };
+
+// nz[t] = 1 when tile t holds a nonzero (one warp per tile)
+__global__ void tile_nz_kernel(const double *L, long long ntiles, unsigned char *nz) {
+    const int lane = threadIdx.x & 31;
+    const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long t = w0; t < ntiles; t += nw) {
+        const double *tp = L + (size_t)t * TILE * TILE;
+        bool any = false;
+        for (int k = lane; k < TILE * TILE; k += 32) any |= tp[k] != 0.0;
+        any = __any_sync(FULL, any);
+        if (lane == 0) nz[t] = any ? 1 : 0;
+    }
+}
 
 // K^+ modes of kplus_kernel:
 //   0  out = K^+ in;
@@ -1016,6 +1080,7 @@ __global__ void __launch_bounds__(256) kplus_kernel(KplusDev K, const double *in
     const int *pos = K.pos + o;
     const uint4 *tiles = reinterpret_cast<const uint4 *>(K.L) + (size_t)K.tile0[d] * (TILE * 16);
     const double *dtiles = K.L + (size_t)K.tile0[d] * TILE * TILE;
+    const int *cp = K.cptr + K.cbase[d];
     for (int i = threadIdx.x; i < TILE * T; i += blockDim.x) v[i] = 0.0;
     __syncthreads();
     for (int i = threadIdx.x; i < n; i += blockDim.x) v[pos[i]] = in[o + i];
@@ -1038,7 +1103,8 @@ __global__ void __launch_bounds__(256) kplus_kernel(KplusDev K, const double *in
             v[TILE * J + lane] = s0 + s1;
         }
         __syncthreads();
-        for (int I = J + 1 + warp; I < T; I += nw) {
+        for (int q = cp[J] + 1 + warp; q < cp[J + 1]; q += nw) {
+            const int I = K.rows[q];
             const uint4 *tp = tiles + (size_t)ltile(T, I, J) * (TILE * 16);
             double rs[16];
             const double x0 = v[TILE * J + 2 * cq], x1 = v[TILE * J + 2 * cq + 1];
@@ -1061,8 +1127,9 @@ __global__ void __launch_bounds__(256) kplus_kernel(KplusDev K, const double *in
     }
     // backward: L^T x = y (in mode 1 only down to block jt)
     for (int J = T - 1; J >= (mode == KPLUS_TOUCHED ? jt : 0); --J) {
-        double cp = 0.0;
-        for (int I = J + 1 + warp; I < T; I += nw) {
+        double cpart = 0.0;
+        for (int q = cp[J] + 1 + warp; q < cp[J + 1]; q += nw) {
+            const int I = K.rows[q];
             const uint4 *tp = tiles + (size_t)ltile(T, I, J) * (TILE * 16);
             double cs[2] = {0.0, 0.0};
 #pragma unroll
@@ -1072,9 +1139,9 @@ __global__ void __launch_bounds__(256) kplus_kernel(KplusDev K, const double *in
                 cs[0] += __hiloint2double(u.y, u.x) * xr;
                 cs[1] += __hiloint2double(u.w, u.z) * xr;
             }
-            cp += reduce_scatter<2, 4>(cs, lane);
+            cpart += reduce_scatter<2, 4>(cs, lane);
         }
-        part[warp][idx] = cp;
+        part[warp][idx] = cpart;
         __syncthreads();
         if (warp == 0) {
             double vc = v[TILE * J + lane];
@@ -1111,6 +1178,7 @@ __global__ void __launch_bounds__(256) kplus_multi_kernel(KplusDev K, const doub
     const int *pos = K.pos + o;
     const uint4 *tiles = reinterpret_cast<const uint4 *>(K.L) + (size_t)K.tile0[d] * (TILE * 16);
     const double *dtiles = K.L + (size_t)K.tile0[d] * TILE * TILE;
+    const int *cp = K.cptr + K.cbase[d];
     const int jt = mode == KPLUS_FULL ? 0 : K.jt[d];
     for (int i = threadIdx.x; i < NC * NP; i += blockDim.x) vm[i] = 0.0;
     __syncthreads();
@@ -1134,7 +1202,8 @@ __global__ void __launch_bounds__(256) kplus_multi_kernel(KplusDev K, const doub
             }
         }
         __syncthreads();
-        for (int I = J + 1 + warp; I < T; I += nw) {
+        for (int qi = cp[J] + 1 + warp; qi < cp[J + 1]; qi += nw) {
+            const int I = K.rows[qi];
             const uint4 *tp = tiles + (size_t)ltile(T, I, J) * (TILE * 16);
             uint4 t[16];
 #pragma unroll
@@ -1162,10 +1231,11 @@ __global__ void __launch_bounds__(256) kplus_multi_kernel(KplusDev K, const doub
         __syncthreads();
     }
     for (int J = T - 1; J >= (mode == KPLUS_TOUCHED ? jt : 0); --J) {
-        double cp[NC];
+        double cpart[NC];
 #pragma unroll
-        for (int c = 0; c < NC; ++c) cp[c] = 0.0;
-        for (int I = J + 1 + warp; I < T; I += nw) {
+        for (int c = 0; c < NC; ++c) cpart[c] = 0.0;
+        for (int qi = cp[J] + 1 + warp; qi < cp[J + 1]; qi += nw) {
+            const int I = K.rows[qi];
             const uint4 *tp = tiles + (size_t)ltile(T, I, J) * (TILE * 16);
             uint4 t[16];
 #pragma unroll
@@ -1180,11 +1250,11 @@ __global__ void __launch_bounds__(256) kplus_multi_kernel(KplusDev K, const doub
                     cs[0] += __hiloint2double(t[q].y, t[q].x) * xr;
                     cs[1] += __hiloint2double(t[q].w, t[q].z) * xr;
                 }
-                cp[c] += reduce_scatter<2, 4>(cs, lane);
+                cpart[c] += reduce_scatter<2, 4>(cs, lane);
             }
         }
 #pragma unroll
-        for (int c = 0; c < NC; ++c) part[warp][c][idx] = cp[c];
+        for (int c = 0; c < NC; ++c) part[warp][c][idx] = cpart[c];
         __syncthreads();
         {
             const double *tile = dtiles + (size_t)ltile(T, J, J) * TILE * TILE;
@@ -1205,6 +1275,164 @@ __global__ void __launch_bounds__(256) kplus_multi_kernel(KplusDev K, const doub
     }
     for (int c = 0; c < NC; ++c)
         for (int i = threadIdx.x; i < n; i += blockDim.x) out[(size_t)(j0 + c) * stride + o + i] = vm[c * NP + pos[i]];
+}
+
+// K^+ on NC = 8 or 16 right-hand sides with FP64 tensor-core MMAs (mma.m8n8k4.f64).  Same tile
+// walk, nonzero-tile lists and modes as kplus_multi_kernel.  Every 32 x 32 step is
+// C(32 x NC) += A(32 x 32) B(32 x NC) as 4 x NC/8 blocks of 8 x 8 over 8 k-steps of 4: A is the
+// factor tile read straight from global memory in fragment order (the tile in the forward pass, its
+// transpose in the backward pass; every 32-byte sector is read once), B the column block of the
+// vectors in shared memory.  The vectors are kept in factor order, NP + KPM_PAD doubles apart, so
+// that the fragment loads and stores take the minimum two wavefronts.  Warps take the off-diagonal
+// tiles of a block column in turn; the diagonal step (inverse diagonal tile) is split over 4 x NC/8
+// warps.  The backward partial sums of the warps meet in shared memory.
+constexpr int KPM_PAD = 4;
+
+__device__ __forceinline__ void dmma84(double (&c)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(c[0]), "+d"(c[1])
+                 : "d"(a), "d"(b));
+}
+
+template <int NC>
+__global__ void __launch_bounds__(256, 1) kplus_mma_kernel(KplusDev K, const double *in, double *out, int mode,
+                                                           int j0, long long stride, double *z) {
+    static_assert(NC == 8 || NC == 16, "K+ MMA kernel: 8 or 16 columns");
+    constexpr int NB = NC / 8;
+    extern __shared__ double vm[];                 // [NC][NP + KPM_PAD]
+    __shared__ double part[8][4 * NB * 2 * 32];    // backward partials per warp, fragment order
+    const int d = blockIdx.x;
+    const int n = K.n[d], T = K.tn[d], o = K.doff[d];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int gr = lane >> 2, gc = lane & 3;       // fragment row (group) and column in the group
+    const int NP = TILE * T, NPp = NP + KPM_PAD;
+    const int *pos = K.pos + o;
+    const double *L = K.L + (size_t)K.tile0[d] * TILE * TILE;
+    const int *cp = K.cptr + K.cbase[d];
+    const int jt = mode == KPLUS_FULL ? 0 : K.jt[d];
+    for (int i = threadIdx.x; i < NC * NPp; i += blockDim.x) vm[i] = 0.0;
+    __syncthreads();
+    for (int c = 0; c < NC; ++c)
+        for (int i = threadIdx.x; i < n; i += blockDim.x) vm[c * NPp + pos[i]] = in[(size_t)(j0 + c) * stride + o + i];
+    __syncthreads();
+
+    // block J := inv(L_JJ) block J (trans: inv(L_JJ)^T), warps 0 .. 4 NB - 1, one 8 x 8 block each
+    auto diag = [&](int J, bool trans) {
+        const bool act = warp < 4 * NB;
+        const int mb = warp & 3, nb = warp >> 2;
+        double acc[2] = {0.0, 0.0};
+        if (act) {
+            const double *tile = L + (size_t)ltile(T, J, J) * TILE * TILE;
+            const double *bcol = vm + (size_t)(8 * nb + gr) * NPp + TILE * J;
+#pragma unroll
+            for (int ks = 0; ks < 8; ++ks) {
+                const int k = 4 * ks + gc;
+                const double a = trans ? __ldg(tile + k * TILE + 8 * mb + gr) : __ldg(tile + (8 * mb + gr) * TILE + k);
+                dmma84(acc, a, bcol[k]);
+            }
+        }
+        __syncthreads();   // block J read by every active warp before it is overwritten
+        if (act) {
+            double *cc = vm + (size_t)(8 * nb + 2 * gc) * NPp + TILE * J + 8 * mb + gr;
+            cc[0] = acc[0];
+            cc[NPp] = acc[1];
+        }
+        __syncthreads();
+    };
+
+    // forward: L y = f
+    for (int J = (mode == KPLUS_PRIMAL ? jt : 0); J < T; ++J) {
+        diag(J, false);
+        double bf[8][NB];
+#pragma unroll
+        for (int ks = 0; ks < 8; ++ks)
+#pragma unroll
+            for (int nb = 0; nb < NB; ++nb) bf[ks][nb] = vm[(size_t)(8 * nb + gr) * NPp + TILE * J + 4 * ks + gc];
+        for (int qi = cp[J] + 1 + warp; qi < cp[J + 1]; qi += 8) {
+            const int I = K.rows[qi];
+            const double *tile = L + (size_t)ltile(T, I, J) * TILE * TILE + gr * TILE + gc;
+            double af[4][8];
+#pragma unroll
+            for (int mb = 0; mb < 4; ++mb)
+#pragma unroll
+                for (int ks = 0; ks < 8; ++ks) af[mb][ks] = __ldg(tile + 8 * mb * TILE + 4 * ks);
+            double acc[4][NB][2];
+#pragma unroll
+            for (int mb = 0; mb < 4; ++mb)
+#pragma unroll
+                for (int nb = 0; nb < NB; ++nb) {
+                    acc[mb][nb][0] = 0.0;
+                    acc[mb][nb][1] = 0.0;
+#pragma unroll
+                    for (int ks = 0; ks < 8; ++ks) dmma84(acc[mb][nb], af[mb][ks], bf[ks][nb]);
+                }
+#pragma unroll
+            for (int mb = 0; mb < 4; ++mb)
+#pragma unroll
+                for (int nb = 0; nb < NB; ++nb) {
+                    double *cc = vm + (size_t)(8 * nb + 2 * gc) * NPp + TILE * I + 8 * mb + gr;
+                    cc[0] -= acc[mb][nb][0];
+                    cc[NPp] -= acc[mb][nb][1];
+                }
+        }
+        __syncthreads();
+    }
+    if (mode == KPLUS_TOUCHED) {
+        for (int c = 0; c < NC; ++c)
+            for (int i = threadIdx.x; i < n; i += blockDim.x) z[(size_t)(j0 + c) * stride + o + i] = vm[c * NPp + i];
+        __syncthreads();
+    } else if (mode == KPLUS_PRIMAL) {
+        for (int c = 0; c < NC; ++c)
+            for (int i = threadIdx.x; i < n; i += blockDim.x) vm[c * NPp + i] += z[(size_t)(j0 + c) * stride + o + i];
+        __syncthreads();
+    }
+    // backward: L^T x = y (mode 1: down to block jt)
+    for (int J = T - 1; J >= (mode == KPLUS_TOUCHED ? jt : 0); --J) {
+        double acc[4][NB][2];
+#pragma unroll
+        for (int mb = 0; mb < 4; ++mb)
+#pragma unroll
+            for (int nb = 0; nb < NB; ++nb) acc[mb][nb][0] = acc[mb][nb][1] = 0.0;
+        for (int qi = cp[J] + 1 + warp; qi < cp[J + 1]; qi += 8) {
+            const int I = K.rows[qi];
+            // A = L_IJ^T: A[m][k] = L_IJ[k][m]
+            const double *tile = L + (size_t)ltile(T, I, J) * TILE * TILE + gc * TILE + gr;
+            double af[4][8], bf[8][NB];
+#pragma unroll
+            for (int mb = 0; mb < 4; ++mb)
+#pragma unroll
+                for (int ks = 0; ks < 8; ++ks) af[mb][ks] = __ldg(tile + 4 * ks * TILE + 8 * mb);
+#pragma unroll
+            for (int ks = 0; ks < 8; ++ks)
+#pragma unroll
+                for (int nb = 0; nb < NB; ++nb) bf[ks][nb] = vm[(size_t)(8 * nb + gr) * NPp + TILE * I + 4 * ks + gc];
+#pragma unroll
+            for (int mb = 0; mb < 4; ++mb)
+#pragma unroll
+                for (int nb = 0; nb < NB; ++nb)
+#pragma unroll
+                    for (int ks = 0; ks < 8; ++ks) dmma84(acc[mb][nb], af[mb][ks], bf[ks][nb]);
+        }
+#pragma unroll
+        for (int mb = 0; mb < 4; ++mb)
+#pragma unroll
+            for (int nb = 0; nb < NB; ++nb) {
+                part[warp][((mb * NB + nb) * 2 + 0) * 32 + lane] = acc[mb][nb][0];
+                part[warp][((mb * NB + nb) * 2 + 1) * 32 + lane] = acc[mb][nb][1];
+            }
+        __syncthreads();
+        for (int q = threadIdx.x; q < 32 * NC; q += blockDim.x) {
+            const int ln = q & 31, e = (q >> 5) & 1, blk = q >> 6, mb = blk / NB, nb = blk % NB;
+            double sum = 0.0;
+#pragma unroll
+            for (int w = 0; w < 8; ++w) sum += part[w][q];
+            vm[(size_t)(8 * nb + 2 * (ln & 3) + e) * NPp + TILE * J + 8 * mb + (ln >> 2)] -= sum;
+        }
+        __syncthreads();
+        diag(J, true);
+    }
+    for (int c = 0; c < NC; ++c)
+        for (int i = threadIdx.x; i < n; i += blockDim.x) out[(size_t)(j0 + c) * stride + o + i] = vm[c * NPp + pos[i]];
 }
 
 // subdomain loads f_i = rhs(caller DOF) / multiplicity
@@ -1290,6 +1518,7 @@ __device__ __forceinline__ bool hyb_skip(const DevProblem &P, int slot, int cond
 // z_i = V_i^T x_i: one warp per column of V_i.  With x == null the PCG direction
 // p = y + beta p is formed on the fly, as the tile SYMV does (update_kernel stores it later).
 __global__ void hyb_vt_kernel(DevProblem P, HybDev H, const double *x, int slot, int cond) {
+    pdl_enter();
     if (hyb_skip(P, slot, cond)) return;
     const int d = blockIdx.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int e0 = P.loff[d], ni = P.loff[d + 1] - e0;
@@ -1316,6 +1545,7 @@ __global__ void hyb_vt_kernel(DevProblem P, HybDev H, const double *x, int slot,
 // grid (ncl, row blocks); with dot != null the last CTA subtracts sum_c z_c . w_c from *dot.
 constexpr int HM_ROWS = 64;
 __global__ void __launch_bounds__(256) hyb_m_kernel(DevProblem P, HybDev H, int slot, int cond, double *dot) {
+    pdl_enter();
     if (hyb_skip(P, slot, cond)) return;
     extern __shared__ double hz[];
     __shared__ double sh[32];
@@ -1367,6 +1597,7 @@ __global__ void __launch_bounds__(256) hyb_m_kernel(DevProblem P, HybDev H, int 
 
 // y_i -= V_i w_{c(i)}: one thread per row
 __global__ void hyb_v_kernel(DevProblem P, HybDev H, double *y, int slot, int cond) {
+    pdl_enter();
     if (hyb_skip(P, slot, cond)) return;
     extern __shared__ double wl[];
     const int d = blockIdx.x;
@@ -1483,6 +1714,7 @@ struct GpuSolver::Impl {
     double *Ax64 = nullptr;   // F apply output outside the iteration operator (initial, replacement, tests)
     // device K^+ and the right-hand-side / primal vectors
     KplusDev KP{};
+    long long kplus_tiles_kept = 0, kplus_tiles_total = 0;   // factor tiles applied / stored
     int max_T = 0, ntot = 0, n_caller = 0;
     int *d_doff = nullptr, *d_rofs = nullptr, *d_gdof = nullptr, *d_rdof = nullptr, *d_tdof_g = nullptr;
     double *d_invm = nullptr, *d_R = nullptr, *d_rsign = nullptr, *d_rc = nullptr;
@@ -1590,6 +1822,15 @@ struct GpuSolver::Impl {
 
 // dynamic shared memory available to kplus_multi_kernel<NC> next to its static partial sums
 static size_t kplus_multi_smem(int nc) { return (size_t)220 * 1024 - (size_t)nc * 8 * TILE * sizeof(double); }
+// dynamic shared memory available to kplus_mma_kernel<NC> next to its 16 KB per 8 columns of partials
+static size_t kplus_mma_smem(int nc) { return (size_t)226 * 1024 - (size_t)(nc / 8) * 16 * 1024; }
+static bool kplus_mma_enabled() {
+    static const bool on = [] {
+        const char *e = getenv("FETI4I_KPLUS_MMA");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
 
 // K^+ on ncol columns (stride ntot): groups of NC columns per pass, NC as large as shared memory allows.
 void GpuSolver::Impl::launch_kplus_multi(const double *in, double *out, int ncol, int mode, double *z) {
@@ -1601,6 +1842,16 @@ void GpuSolver::Impl::launch_kplus_multi(const double *in, double *out, int ncol
         int nc = 16;
         while (nc > 1 && (nc > left || (size_t)nc * per_col > kplus_multi_smem(nc))) nc /= 2;
         const size_t sm = (size_t)nc * per_col;
+        // FP64 tensor-core variant for 8 or 16 columns when the padded vectors fit next to its
+        // partial sums
+        const size_t sm_mma = sizeof(double) * (size_t)nc * ((size_t)TILE * max_T + KPM_PAD);
+        if (kplus_mma_enabled() && (nc == 16 || nc == 8) && sm_mma <= kplus_mma_smem(nc)) {
+            if (nc == 16) kplus_mma_kernel<16><<<P.nd, 256, sm_mma, stream>>>(KP, in, out, mode, j0, ntot, z);
+            else kplus_mma_kernel<8><<<P.nd, 256, sm_mma, stream>>>(KP, in, out, mode, j0, ntot, z);
+            CUDA_CHECK(cudaGetLastError());
+            j0 += nc;
+            continue;
+        }
         switch (nc) {
         case 16: kplus_multi_kernel<16><<<P.nd, 256, sm, stream>>>(KP, in, out, mode, j0, ntot, z); break;
         case 8: kplus_multi_kernel<8><<<P.nd, 256, sm, stream>>>(KP, in, out, mode, j0, ntot, z); break;
@@ -1711,6 +1962,40 @@ void GpuSolver::Impl::upload_kplus(const Decomposition &dec, const Prep &prep, c
         KP.z = alloc<double>(std::max(1, ntot));
     }
     KP.L = ds ? adopt(ds->kp_tiles, (size_t)tile0[nd] * TILE * TILE) : upload(L);
+    {
+        // nonzero tiles per block column, found on the device factor
+        const long long ntiles = tile0[nd];
+        unsigned char *d_nz = nullptr;
+        CUDA_CHECK(cudaMalloc(&d_nz, (size_t)std::max<long long>(1, ntiles)));
+        tile_nz_kernel<<<nsm * 8, 256, 0, stream>>>(KP.L, ntiles, d_nz);
+        CUDA_CHECK(cudaGetLastError());
+        std::vector<unsigned char> nz((size_t)ntiles);
+        CUDA_CHECK(cudaMemcpyAsync(nz.data(), d_nz, (size_t)ntiles, cudaMemcpyDeviceToHost, stream));
+        CUDA_CHECK(cudaStreamSynchronize(stream));
+        CUDA_CHECK(cudaFree(d_nz));
+        std::vector<int> cbase(nd + 1, 0), cptr, rows;
+        long long kept = 0;
+        for (int d = 0; d < nd; ++d) {
+            const int T = tn[d];
+            cbase[d] = (int)cptr.size();
+            for (int J = 0; J < T; ++J) {
+                cptr.push_back((int)rows.size());
+                const long long c0 = tile0[d] + (long long)J * T - (long long)J * (J - 1) / 2;
+                rows.push_back(J);   // the diagonal tile (its inverse) is always applied
+                for (int I = J + 1; I < T; ++I)
+                    if (nz[(size_t)(c0 + I - J)]) rows.push_back(I);
+            }
+            cptr.push_back((int)rows.size());
+        }
+        kept = (long long)rows.size();
+        cbase[nd] = (int)cptr.size();
+        FETI_CHECK(kept < (1LL << 31), "FETI4I: too many factor tiles");
+        KP.cbase = upload(cbase);
+        KP.cptr = upload(cptr);
+        KP.rows = upload(rows);
+        kplus_tiles_kept = kept;
+        kplus_tiles_total = ntiles;
+    }
     d_rofs = upload(rofs);
     d_gdof = upload(gdof);
     d_invm = upload(invm);
@@ -1738,6 +2023,8 @@ void GpuSolver::Impl::upload_kplus(const Decomposition &dec, const Prep &prep, c
     CUDA_CHECK(cudaFuncSetAttribute(kplus_multi_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kplus_multi_smem(4)));
     CUDA_CHECK(cudaFuncSetAttribute(kplus_multi_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kplus_multi_smem(2)));
     CUDA_CHECK(cudaFuncSetAttribute(kplus_multi_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kplus_multi_smem(1)));
+    CUDA_CHECK(cudaFuncSetAttribute(kplus_mma_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kplus_mma_smem(16)));
+    CUDA_CHECK(cudaFuncSetAttribute(kplus_mma_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kplus_mma_smem(8)));
 }
 
 void GpuSolver::Impl::upload_hybrid(const Decomposition &dec, const Prep &prep) {
@@ -1820,10 +2107,9 @@ void GpuSolver::Impl::upload_hybrid(const Decomposition &dec, const Prep &prep) 
 
 void GpuSolver::Impl::launch_hybrid_F(const double *x, double *y, int slot, int cond, double *dot) {
     if (!hybrid) return;
-    hyb_vt_kernel<<<P.nd, 256, 0, stream>>>(P, H, x, slot, cond);
-    hyb_m_kernel<<<dim3(H.ncl, hyb_rows), 256, sizeof(double) * H.max_nc, stream>>>(P, H, slot, cond, dot);
-    hyb_v_kernel<<<P.nd, 256, sizeof(double) * hyb_max_m, stream>>>(P, H, y, slot, cond);
-    CUDA_CHECK(cudaGetLastError());
+    launch_pdl(hyb_vt_kernel, dim3(P.nd), dim3(256), 0, stream, P, H, x, slot, cond);
+    launch_pdl(hyb_m_kernel, dim3(H.ncl, hyb_rows), dim3(256), sizeof(double) * H.max_nc, stream, P, H, slot, cond, dot);
+    launch_pdl(hyb_v_kernel, dim3(P.nd), dim3(256), sizeof(double) * hyb_max_m, stream, P, H, y, slot, cond);
 }
 
 // K_c^+ (or K^+) on ncol columns (stride ntot): both K^+ passes of the cluster solve on all columns
@@ -2105,7 +2391,9 @@ void GpuSolver::Impl::launch_tiles(const TileSetHost &T, int mode, const double 
         FETI_CHECK(nst >= 2, "FETI4I: subdomain too large for the TMA tile pipeline");
         const size_t sm = (size_t)nst * stage + xbytes;
         const int grid = std::max(1, std::min(T.nitems, nsm));
-#define LAUNCHT(PR, MD) tile_symv_tma_kernel<PR, MD><<<grid, (TMA_CONSUMERS + 1) * 32, sm, stream>>>(td, P, src, src2, out, slot, nst, xs_elems)
+#define LAUNCHT(PR, MD)                                                                                 \
+    launch_pdl(tile_symv_tma_kernel<PR, MD>, dim3(grid), dim3((TMA_CONSUMERS + 1) * 32), sm, stream, td, P, src, src2, \
+               out, slot, nst, xs_elems)
 #define LAUNCHT_MODES(PR)                                  \
     switch (mode) {                                        \
     case 0: LAUNCHT(PR, 0); break;                         \
@@ -2123,7 +2411,7 @@ void GpuSolver::Impl::launch_tiles(const TileSetHost &T, int mode, const double 
     }
     size_t sm = tile_smem(T.prec, mtn);
     int grid = std::max(1, std::min(T.nitems, nsm * 2));
-#define LAUNCH(PR, MD) tile_symv_kernel<PR, MD><<<grid, 256, sm, stream>>>(td, P, src, src2, out, slot)
+#define LAUNCH(PR, MD) launch_pdl(tile_symv_kernel<PR, MD>, dim3(grid), dim3(256), sm, stream, td, P, src, src2, out, slot)
 #define LAUNCH_MODES(PR)                                   \
     switch (mode) {                                        \
     case 0: LAUNCH(PR, 0); break;                          \
@@ -2179,31 +2467,31 @@ void GpuSolver::Impl::launch_iteration(int slot) {
         // residual replacement r = b - F64 x when the previous update asked for it
         launch_tiles(F64, 3, P.x, nullptr, Ax64, slot);
         launch_hybrid_F(P.x, Ax64, slot, 3, nullptr);
-        r0_kernel<<<nd, TPB, sizeof(double) * max_ni, stream>>>(P, Ax64, 1, slot);
+        launch_pdl(r0_kernel, dim3(nd), dim3(TPB), sizeof(double) * max_ni, stream, P, Ax64, 1, slot);
     }
-    coarse_kernel<<<cgrid, 256, 0, stream>>>(P, P.d, P.alpha, slot, 1);
+    launch_pdl(coarse_kernel, dim3(cgrid), dim3(256), 0, stream, P, P.d, P.alpha, slot, 1);
     const size_t tsm = sizeof(double) * (size_t)(max_ni + max_nt);
     switch (opt.precond) {
-    case PREC_NONE: w_prec_kernel<PREC_NONE><<<nd, TPB1, tsm, stream>>>(P, slot); break;
-    case PREC_LUMPED: w_prec_kernel<PREC_LUMPED><<<nd, TPB1, tsm, stream>>>(P, slot); break;
-    case PREC_WEIGHT: w_prec_kernel<PREC_WEIGHT><<<nd, TPB1, tsm, stream>>>(P, slot); break;
-    default: w_prec_kernel<PREC_DIRICHLET><<<nd, TPB1, tsm, stream>>>(P, slot); break;
+    case PREC_NONE: launch_pdl(w_prec_kernel<PREC_NONE>, dim3(nd), dim3(TPB1), tsm, stream, P, slot); break;
+    case PREC_LUMPED: launch_pdl(w_prec_kernel<PREC_LUMPED>, dim3(nd), dim3(TPB1), tsm, stream, P, slot); break;
+    case PREC_WEIGHT: launch_pdl(w_prec_kernel<PREC_WEIGHT>, dim3(nd), dim3(TPB1), tsm, stream, P, slot); break;
+    default: launch_pdl(w_prec_kernel<PREC_DIRICHLET>, dim3(nd), dim3(TPB1), tsm, stream, P, slot); break;
     }
     if (opt.precond != PREC_NONE) {
         if (opt.precond == PREC_DIRICHLET) {
-            zero_vT_kernel<<<std::max(1, std::min(1024, (P.NT + 255) / 256)), 256, 0, stream>>>(P, slot);
+            launch_pdl(zero_vT_kernel, dim3(std::max(1, std::min(1024, (P.NT + 255) / 256))), dim3(256), 0, stream, P,
+                       slot);
             launch_tiles(Dir, 2, P.uT, nullptr, P.vT, slot);
         }
-        z_kernel<<<nd, TPB, sizeof(double) * max_ni, stream>>>(P, slot);
-        coarse_kernel<<<cgrid, 256, 0, stream>>>(P, P.d, P.alpha, slot, 1);
-        y_kernel<<<nd, TPB, 0, stream>>>(P, Ax64, slot);
+        launch_pdl(z_kernel, dim3(nd), dim3(TPB), sizeof(double) * max_ni, stream, P, slot);
+        launch_pdl(coarse_kernel, dim3(cgrid), dim3(256), 0, stream, P, P.d, P.alpha, slot, 1);
+        launch_pdl(y_kernel, dim3(nd), dim3(TPB), 0, stream, P, Ax64, slot);
     } else {
-        zero2_kernel<<<(P.NL + 255) / 256, 256, 0, stream>>>(P.Ap, Ax64, P.NL);
+        launch_pdl(zero2_kernel, dim3((P.NL + 255) / 256), dim3(256), 0, stream, P.Ap, Ax64, P.NL);
     }
     launch_tiles(Fop, 1, P.y, P.p, P.Ap, slot);
     launch_hybrid_F(nullptr, P.Ap, slot, 1, P.scal + SC_PAP);   // p = y + beta p formed on the fly
-    update_kernel<<<nd, TPB, sizeof(double) * max_ni, stream>>>(P, slot);
-    CUDA_CHECK(cudaGetLastError());
+    launch_pdl(update_kernel, dim3(nd), dim3(TPB), sizeof(double) * max_ni, stream, P, slot);
 }
 
 int GpuSolver::Impl::kernels_per_iteration() const {
@@ -2223,7 +2511,7 @@ void GpuSolver::Impl::capture_chunk(int chunk) {
     cudaGraph_t g;
     CUDA_CHECK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     for (int j = 0; j < chunk; ++j) launch_iteration(j);
-    chunk_end_kernel<<<1, 32, 0, stream>>>(P, chunk);
+    launch_pdl(chunk_end_kernel, dim3(1), dim3(32), 0, stream, P, chunk);
     CUDA_CHECK(cudaStreamEndCapture(stream, &g));
     CUDA_CHECK(cudaGraphInstantiate(&graph, g, 0));
     cudaGraphDestroy(g);
@@ -2235,6 +2523,9 @@ void GpuSolver::Impl::capture_chunk(int chunk) {
 GpuSolver::GpuSolver() : impl(new Impl) {}
 GpuSolver::~GpuSolver() { delete impl; }
 size_t GpuSolver::device_bytes() const { return impl->bytes; }
+double GpuSolver::kplus_tile_fraction() const {
+    return impl->kplus_tiles_total ? (double)impl->kplus_tiles_kept / (double)impl->kplus_tiles_total : 0.0;
+}
 int GpuSolver::device_id() const { return impl->device; }
 void GpuSolver::set_options(const SolveOptions &opt) {
     FETI_CHECK(opt.schur_precision == SCHUR_FP64 || impl->Flow.prec == opt.schur_precision,
@@ -3040,6 +3331,7 @@ __device__ __forceinline__ bool col_frozen(const BlockDev &B, int j, int iter) {
 constexpr int CR = 16;
 __global__ void __launch_bounds__(256) bcoarse_kernel(DevProblem P, BlockDev B, const double *in, double *out, int slot,
                                                       int looped) {
+    pdl_enter();
     if (looped && skip_iter(P.st, P.st->iter_base + slot)) return;
     __shared__ double xs[32][33];
     __shared__ double ms[CR][33];
@@ -3083,6 +3375,7 @@ __global__ void bgt_kernel(DevProblem P, BlockDev B, const double *a, double *xo
 
 // r = b - assemble(Ax), d = G r, |b_j|^2 totals (initial) / replacement
 __global__ void br0_kernel(DevProblem P, BlockDev B, int replace_mode, int slot) {
+    pdl_enter();
     __shared__ double sh[8 * 32];
     __shared__ double cols[32];
     if (replace_mode) {
@@ -3134,6 +3427,7 @@ __global__ void btol_kernel(DevProblem P, BlockDev B) {
 }
 
 __global__ void __launch_bounds__(TPBB) bz_kernel(DevProblem P, BlockDev B, int slot) {
+    pdl_enter();
     __shared__ double sh[32 * 32];
     const int iter = P.st->iter_base + slot;
     if (skip_iter(P.st, iter)) return;
@@ -3169,6 +3463,7 @@ __global__ void __launch_bounds__(TPBB) bz_kernel(DevProblem P, BlockDev B, int 
 // u_T = B^T W w over all touched DOFs (v_T = u_T for the weight-function preconditioner)
 template <int PRECOND>
 __global__ void __launch_bounds__(256) bu_flat_kernel(DevProblem P, BlockDev B, int slot) {
+    pdl_enter();
     const int iter = P.st->iter_base + slot;
     if (skip_iter(P.st, iter)) return;
     const int nr = B.nr;
@@ -3230,6 +3525,7 @@ __device__ __forceinline__ double2 gt_alpha_colk2(const DevProblem &P, int e, in
 }
 
 __global__ void __launch_bounds__(256) bell_flat2_kernel(DevProblem P, BlockDev B, int slot) {
+    pdl_enter();
     const int iter = P.st->iter_base + slot;
     if (skip_iter(P.st, iter)) return;
     const int nr = B.nr, lh = B.lg - 1;
@@ -3266,6 +3562,7 @@ __global__ void __launch_bounds__(256) bell_flat2_kernel(DevProblem P, BlockDev 
 // per thread, as in bell_flat2_kernel
 template <int PRECOND, int KC>
 __global__ void __launch_bounds__(256) bw_flat2_kernel(DevProblem P, BlockDev B, int slot) {
+    pdl_enter();
     __shared__ double sh[8 * 32];
     __shared__ double cols[32];
     const int iter = P.st->iter_base + slot;
@@ -3307,6 +3604,7 @@ __global__ void __launch_bounds__(256) bw_flat2_kernel(DevProblem P, BlockDev B,
 
 template <int KC>
 __global__ void __launch_bounds__(256) by_flat2_kernel(DevProblem P, BlockDev B, int slot) {
+    pdl_enter();
     __shared__ double sh[8 * 32];
     __shared__ double cols[32];
     const int iter = P.st->iter_base + slot;
@@ -3350,6 +3648,7 @@ __global__ void __launch_bounds__(256) by_flat2_kernel(DevProblem P, BlockDev B,
 
 // p = y + beta_j p (and its FP32 copy)
 __global__ void bp_kernel(DevProblem P, BlockDev B, int slot) {
+    pdl_enter();
     const int iter = P.st->iter_base + slot;
     if (skip_iter(P.st, iter)) return;
     const int nr = B.nr;
@@ -3363,6 +3662,7 @@ __global__ void bp_kernel(DevProblem P, BlockDev B, int slot) {
 }
 
 __global__ void __launch_bounds__(TPBB) bupdate_kernel(DevProblem P, BlockDev B, int slot) {
+    pdl_enter();
     __shared__ double sh[32 * 32];
     const int iter = P.st->iter_base + slot;
     if (skip_iter(P.st, iter)) return;
@@ -3444,6 +3744,7 @@ template <int PREC, int NR, int SRC>  // SRC 0: FP64 x (replacement/initial/FP64
 __global__ void __launch_bounds__(256, PREC == SCHUR_FP64 ? 2 : 3)
 tile_symm_kernel(TileSetDev ts, DevProblem P, BlockDev B, const double *x64, const float *x32, double *out,
                  const int2 *units, int nunits, int slot, int mode) {
+    pdl_enter();
     using Acc = typename TileT<PREC>::Acc;
     constexpr int EPC = TileT<PREC>::EPC;
     constexpr int G = 32 / NR;          // row groups
@@ -3553,6 +3854,119 @@ tile_symm_kernel(TileSetDev ts, DevProblem P, BlockDev B, const double *x64, con
     }
 }
 
+// Tile SYMM of FP64 tiles on the FP64 tensor cores (mma.m8n8k4.f64), with the units and results of
+// tile_symm_kernel<SCHUR_FP64, NR, 0>.  A warp owns one 32-row tile row I of one subdomain and
+// forms, for every block column J, C(32 x NR) += A(32 x 32) X_J(32 x NR): A is the stored tile
+// (I, J) for J >= I and the transpose of the stored tile (J, I) for J < I, read straight from
+// global memory in fragment order (every 32-byte sector once), as 4 x NR/8 blocks of 8 x 8 over
+// 8 k-steps of 4.  x rows past the subdomain read as zero.
+template <int NR>
+__global__ void __launch_bounds__(256, 1)
+tile_symm_mma_kernel(TileSetDev ts, DevProblem P, BlockDev B, const double *x64, double *out, const int2 *units,
+                     int nunits, int slot, int mode) {
+    pdl_enter();
+    static_assert(NR == 8 || NR == 16 || NR == 32, "FP64 MMA SYMM: 8, 16 or 32 right-hand sides");
+    constexpr int NB = NR / 8;
+    __shared__ int s_last;
+    if (mode != 0) {
+        const int iter = P.st->iter_base + slot;
+        if (skip_iter(P.st, iter)) return;
+        if (mode == 3 && P.st->replace_iter != iter) return;
+    }
+    const int lane = threadIdx.x & 31;
+    const int gr = lane >> 2, gc = lane & 3;
+    const double *tiles = reinterpret_cast<const double *>(ts.tiles);
+    for (;;) {
+        int u = 0;
+        if (lane == 0) u = atomicAdd(&B.queue[0], 1);
+        u = __shfl_sync(FULL, u, 0);
+        if (u >= nunits) break;
+        const int m = units[u].x, I = units[u].y;
+        const int n = ts.mat_n[m], voff = ts.mat_voff[m], tn = ts.mat_tn[m];
+        const long long t0 = ts.mat_tile0[m];
+        double acc[4][NB][2];
+#pragma unroll
+        for (int mb = 0; mb < 4; ++mb)
+#pragma unroll
+            for (int nb = 0; nb < NB; ++nb) acc[mb][nb][0] = acc[mb][nb][1] = 0.0;
+        for (int J = 0; J < tn; ++J) {
+            const bool upper = J >= I;
+            const int a = upper ? I : J, b = upper ? J : I;
+            const double *tile = tiles + (size_t)(t0 + (long long)a * tn - (long long)a * (a - 1) / 2 + (b - a)) * (TILE * TILE);
+            // A[r][k] = tile[r][k] (upper) or tile[k][r] (lower)
+            const double *ab = upper ? tile + gr * TILE + gc : tile + gc * TILE + gr;
+            const int s_m = upper ? 8 * TILE : 8, s_k = upper ? 4 : 4 * TILE;
+            double bf[8][NB];
+#pragma unroll
+            for (int ks = 0; ks < 8; ++ks) {
+                const int row = TILE * J + 4 * ks + gc;
+#pragma unroll
+                for (int nb = 0; nb < NB; ++nb)
+                    bf[ks][nb] = row < n ? __ldg(x64 + (size_t)(voff + row) * NR + 8 * nb + gr) : 0.0;
+            }
+#pragma unroll
+            for (int mb = 0; mb < 4; ++mb) {
+                double af[8];
+#pragma unroll
+                for (int ks = 0; ks < 8; ++ks) af[ks] = __ldg(ab + mb * s_m + ks * s_k);
+#pragma unroll
+                for (int nb = 0; nb < NB; ++nb)
+#pragma unroll
+                    for (int ks = 0; ks < 8; ++ks) dmma84(acc[mb][nb], af[ks], bf[ks][nb]);
+            }
+        }
+        // rows of the tile row and their dot with x, per column
+        double dot[NB][2];
+#pragma unroll
+        for (int nb = 0; nb < NB; ++nb) dot[nb][0] = dot[nb][1] = 0.0;
+#pragma unroll
+        for (int mb = 0; mb < 4; ++mb) {
+            const int row = TILE * I + 8 * mb + gr;
+            if (row < n) {
+#pragma unroll
+                for (int nb = 0; nb < NB; ++nb)
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        const size_t o = (size_t)(voff + row) * NR + 8 * nb + 2 * gc + e;
+                        out[o] = acc[mb][nb][e];
+                        dot[nb][e] += x64[o] * acc[mb][nb][e];
+                    }
+            }
+        }
+#pragma unroll
+        for (int nb = 0; nb < NB; ++nb)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                double v = dot[nb][e];
+                v += __shfl_xor_sync(FULL, v, 4);
+                v += __shfl_xor_sync(FULL, v, 8);
+                v += __shfl_xor_sync(FULL, v, 16);
+                if (gr == 0) B.unit_dot[(size_t)u * NR + 8 * nb + 2 * gc + e] = v;
+            }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = (atomicAdd(&B.queue[1], 1) == (int)gridDim.x - 1);
+    }
+    __syncthreads();
+    if (s_last) {
+        if (mode == 1) {
+            __threadfence();
+            if (threadIdx.x < NR) {
+                double t = 0.0;
+                for (int q = 0; q < nunits; ++q) t += __ldcg(&B.unit_dot[(size_t)q * NR + threadIdx.x]);
+                B.scal[SC_PAP * NR + threadIdx.x] = t;
+            }
+        }
+        if (threadIdx.x == 0) {
+            B.queue[0] = 0;
+            B.queue[1] = 0;
+            __threadfence();
+        }
+    }
+}
+
 // ---- Tile SYMM on the 5th-generation tensor cores (FP32 tiles, 3xTF32 split)
 // A unit is four consecutive 32-row tile rows of one subdomain (M = 128 rows of S).  For
 // every 32-column block J the CTA stages A = S[128 rows, 32 columns] (upper tiles as stored,
@@ -3636,6 +4050,7 @@ template <int NR>
 __global__ void __launch_bounds__(tc::THREADS, 2)
 tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, double *out, const int2 *units,
                     int nunits, int slot, int mode) {
+    pdl_enter();
     static_assert(NR == 8 || NR == 16 || NR == 32, "tensor-core SYMM: 8, 16 or 32 right-hand sides");
     constexpr unsigned B_BYTES = NR * 128;
     constexpr unsigned STAGE = 2 * tc::A_BYTES + 2 * B_BYTES;
@@ -3841,6 +4256,7 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
 // ---- Hybrid Total FETI cluster correction for nr columns ([row][rhs] layout)
 // z_i = V_i^T x_i: one warp per column of V_i, lane = (row group, rhs)
 __global__ void bhyb_vt_kernel(DevProblem P, HybDev H, BlockDev B, const double *x, double *z, int slot, int cond) {
+    pdl_enter();
     if (hyb_skip(P, slot, cond)) return;
     const int nr = B.nr, lg = B.lg;
     const int d = blockIdx.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -3860,6 +4276,7 @@ __global__ void bhyb_vt_kernel(DevProblem P, HybDev H, BlockDev B, const double 
 // w_c = M_c z_c for nr columns; grid (ncl, row blocks); dot: per column p.Ap totals to correct
 __global__ void __launch_bounds__(256) bhyb_m_kernel(DevProblem P, HybDev H, BlockDev B, const double *z, double *w,
                                                      int slot, int cond, double *dot, double *part, int *done) {
+    pdl_enter();
     if (hyb_skip(P, slot, cond)) return;
     extern __shared__ double hz[];            // nc x nr
     __shared__ double s_cols[256];
@@ -3918,6 +4335,7 @@ __global__ void __launch_bounds__(256) bhyb_m_kernel(DevProblem P, HybDev H, Blo
 
 // y_i -= V_i w_{c(i)} for nr columns: one thread per (row, rhs)
 __global__ void bhyb_v_kernel(DevProblem P, HybDev H, BlockDev B, const double *w, double *y, int slot, int cond) {
+    pdl_enter();
     if (hyb_skip(P, slot, cond)) return;
     extern __shared__ double wl[];            // m_i x nr
     const int nr = B.nr, lg = B.lg;
@@ -3938,6 +4356,7 @@ __global__ void bhyb_v_kernel(DevProblem P, HybDev H, BlockDev B, const double *
 }
 
 __global__ void bchunk_end_kernel(DevProblem P, int chunk) {
+    pdl_enter();
     if (threadIdx.x == 0 && blockIdx.x == 0) P.st->iter_base += chunk;
 }
 
@@ -4112,11 +4531,11 @@ void GpuSolver::Impl::ensure_block(int nr) {
 void GpuSolver::Impl::launch_block_hybrid(const double *x, double *y, int slot, int cond, double *dot) {
     if (!hybrid) return;
     const int nr = blk.nr;
-    bhyb_vt_kernel<<<P.nd, 256, 0, stream>>>(P, H, blk.B, x, bh_z, slot, cond);
-    bhyb_m_kernel<<<dim3(H.ncl, hyb_rows), 256, sizeof(double) * (size_t)H.max_nc * nr, stream>>>(
-        P, H, blk.B, bh_z, bh_w, slot, cond, dot, bh_part, bh_done);
-    bhyb_v_kernel<<<P.nd, 256, sizeof(double) * (size_t)hyb_max_m * nr, stream>>>(P, H, blk.B, bh_w, y, slot, cond);
-    CUDA_CHECK(cudaGetLastError());
+    launch_pdl(bhyb_vt_kernel, dim3(P.nd), dim3(256), 0, stream, P, H, blk.B, x, bh_z, slot, cond);
+    launch_pdl(bhyb_m_kernel, dim3(H.ncl, hyb_rows), dim3(256), sizeof(double) * (size_t)H.max_nc * nr, stream, P, H,
+               blk.B, bh_z, bh_w, slot, cond, dot, bh_part, bh_done);
+    launch_pdl(bhyb_v_kernel, dim3(P.nd), dim3(256), sizeof(double) * (size_t)hyb_max_m * nr, stream, P, H, blk.B, bh_w,
+               y, slot, cond);
 }
 
 // persistent launch: as many CTAs as are resident at once (they drain the unit queue)
@@ -4136,7 +4555,30 @@ static void symm_launch(int nsm, int ncta, size_t sm, cudaStream_t st, TileSetDe
         per_sm = b;
     }
     const int grid = std::max(1, std::min(ncta, nsm * per_sm));
-    tile_symm_kernel<PR, NR, SRC><<<grid, 256, sm, st>>>(td, P, B, x64, x32, out, units, nunits, slot, mode);
+    launch_pdl(tile_symm_kernel<PR, NR, SRC>, dim3(grid), dim3(256), sm, st, td, P, B, x64, x32, out, units, nunits, slot,
+               mode);
+}
+
+static bool symm_mma_enabled() {
+    static const bool on = [] {
+        const char *e = getenv("FETI4I_SYMM_MMA");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+template <int NR>
+static void symm_mma_launch(int nsm, int ncta, cudaStream_t st, TileSetDev td, DevProblem P, BlockDev B,
+                            const double *x64, double *out, const int2 *units, int nunits, int slot, int mode) {
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        int b = 1;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, tile_symm_mma_kernel<NR>, 256, 0) != cudaSuccess || b < 1)
+            b = 1;
+        per_sm = b;
+    }
+    const int grid = std::max(1, std::min(ncta, nsm * per_sm));
+    launch_pdl(tile_symm_mma_kernel<NR>, dim3(grid), dim3(256), 0, st, td, P, B, x64, out, units, nunits, slot, mode);
 }
 
 template <int NR>
@@ -4153,7 +4595,7 @@ static void symm_tc_launch(int nsm, int nunits, cudaStream_t st, TileSetDev td, 
     // two CTAs per SM fit (registers and shared memory); CTAs never wait for one another, so a
     // CTA that is not co-resident only starts later
     const int grid = std::max(1, std::min(nunits, nsm * 2));
-    tile_symm_tc_kernel<NR><<<grid, tc::THREADS, sm, st>>>(td, P, B, x32, out, units, nunits, slot, mode);
+    launch_pdl(tile_symm_tc_kernel<NR>, dim3(grid), dim3(tc::THREADS), sm, st, td, P, B, x32, out, units, nunits, slot, mode);
 }
 
 void GpuSolver::Impl::launch_symm(const TileSetHost &T, bool src32, const double *x64, const float *x32, double *out,
@@ -4176,6 +4618,15 @@ void GpuSolver::Impl::launch_symm(const TileSetHost &T, bool src32, const double
     const size_t sm = 8 * TB;
     const int ncta = (nunits + 7) / 8;
     TileSetDev td = T.dev();
+    if (T.prec == SCHUR_FP64 && nr >= 8 && symm_mma_enabled()) {
+        switch (nr) {
+        case 8: symm_mma_launch<8>(nsm, ncta, stream, td, P, blk.B, x64, out, units, nunits, slot, mode); break;
+        case 16: symm_mma_launch<16>(nsm, ncta, stream, td, P, blk.B, x64, out, units, nunits, slot, mode); break;
+        default: symm_mma_launch<32>(nsm, ncta, stream, td, P, blk.B, x64, out, units, nunits, slot, mode); break;
+        }
+        CUDA_CHECK(cudaGetLastError());
+        return;
+    }
     FETI_CHECK(T.prec != SCHUR_BF16, "FETI4I: the multi right-hand-side solve supports FP64 and FP32 Schur storage");
 #define SYMM(PR, NR_, S) symm_launch<PR, NR_, S>(nsm, ncta, sm, stream, td, P, blk.B, x64, x32, out, units, nunits, slot, mode)
 #define SYMM_NR(PR, S)                       \
@@ -4201,50 +4652,50 @@ void GpuSolver::Impl::launch_block_iteration(int slot) {
     if (mixed) {
         launch_symm(F64, false, B.x, nullptr, B.Ax, slot, 3);
         launch_block_hybrid(B.x, B.Ax, slot, 3, nullptr);
-        br0_kernel<<<nd, TPB, 0, stream>>>(P, B, 1, slot);
+        launch_pdl(br0_kernel, dim3(nd), dim3(TPB), 0, stream, P, B, 1, slot);
     }
-    bcoarse_kernel<<<cgrid, 256, 0, stream>>>(P, B, B.d, B.alpha, slot, 1);
+    launch_pdl(bcoarse_kernel, dim3(cgrid), dim3(256), 0, stream, P, B, B.d, B.alpha, slot, 1);
     const int fgrid = blk.flat_grid;
 #define BW(PC)                                                                              \
     switch (P.KS) {                                                                         \
-    case 1: bw_flat2_kernel<PC, 1><<<fgrid, 256, 0, stream>>>(P, B, slot); break;           \
-    case 6: bw_flat2_kernel<PC, 6><<<fgrid, 256, 0, stream>>>(P, B, slot); break;           \
-    default: bw_flat2_kernel<PC, 0><<<fgrid, 256, 0, stream>>>(P, B, slot); break;          \
+    case 1: launch_pdl(bw_flat2_kernel<PC, 1>, dim3(fgrid), dim3(256), 0, stream, P, B, slot); break;  \
+    case 6: launch_pdl(bw_flat2_kernel<PC, 6>, dim3(fgrid), dim3(256), 0, stream, P, B, slot); break;  \
+    default: launch_pdl(bw_flat2_kernel<PC, 0>, dim3(fgrid), dim3(256), 0, stream, P, B, slot); break; \
     }
     switch (opt.precond) {
     case PREC_NONE: BW(PREC_NONE) break;
     case PREC_LUMPED:
         BW(PREC_LUMPED)
-        bu_flat_kernel<PREC_LUMPED><<<fgrid, 256, 0, stream>>>(P, B, slot);
-        bell_flat2_kernel<<<fgrid, 256, 0, stream>>>(P, B, slot);
+        launch_pdl(bu_flat_kernel<PREC_LUMPED>, dim3(fgrid), dim3(256), 0, stream, P, B, slot);
+        launch_pdl(bell_flat2_kernel, dim3(fgrid), dim3(256), 0, stream, P, B, slot);
         break;
     case PREC_DIRICHLET:
         // u_T = B^T W w, then v_T = S_dir u_T (FP64 SYMM over the Dirichlet blocks)
         BW(PREC_WEIGHT)
-        bu_flat_kernel<PREC_LUMPED><<<fgrid, 256, 0, stream>>>(P, B, slot);
+        launch_pdl(bu_flat_kernel<PREC_LUMPED>, dim3(fgrid), dim3(256), 0, stream, P, B, slot);
         launch_symm(Dir, false, B.uT, nullptr, B.vT, slot, 2);
         break;
     default:
         BW(PREC_WEIGHT)
-        bu_flat_kernel<PREC_WEIGHT><<<fgrid, 256, 0, stream>>>(P, B, slot);
+        launch_pdl(bu_flat_kernel<PREC_WEIGHT>, dim3(fgrid), dim3(256), 0, stream, P, B, slot);
         break;
     }
 #undef BW
     if (opt.precond != PREC_NONE) {
-        bz_kernel<<<nd, TPBB, 0, stream>>>(P, B, slot);
-        bcoarse_kernel<<<cgrid, 256, 0, stream>>>(P, B, B.d, B.alpha, slot, 1);
+        launch_pdl(bz_kernel, dim3(nd), dim3(TPBB), 0, stream, P, B, slot);
+        launch_pdl(bcoarse_kernel, dim3(cgrid), dim3(256), 0, stream, P, B, B.d, B.alpha, slot, 1);
         switch (P.KS) {
-        case 1: by_flat2_kernel<1><<<fgrid, 256, 0, stream>>>(P, B, slot); break;
-        case 6: by_flat2_kernel<6><<<fgrid, 256, 0, stream>>>(P, B, slot); break;
-        default: by_flat2_kernel<0><<<fgrid, 256, 0, stream>>>(P, B, slot); break;
+        case 1: launch_pdl(by_flat2_kernel<1>, dim3(fgrid), dim3(256), 0, stream, P, B, slot); break;
+        case 6: launch_pdl(by_flat2_kernel<6>, dim3(fgrid), dim3(256), 0, stream, P, B, slot); break;
+        default: launch_pdl(by_flat2_kernel<0>, dim3(fgrid), dim3(256), 0, stream, P, B, slot); break;
         }
     }
-    bp_kernel<<<std::max(1, std::min(4096, (P.NL * blk.nr + 255) / 256)), 256, 0, stream>>>(P, B, slot);
+    launch_pdl(bp_kernel, dim3(std::max(1, std::min(4096, (P.NL * blk.nr + 255) / 256))), dim3(256), 0, stream, P, B,
+               slot);
     if (mixed) launch_symm(Flow, true, nullptr, B.p32, B.Ap, slot, 1);
     else launch_symm(F64, false, B.p, nullptr, B.Ap, slot, 1);
     launch_block_hybrid(B.p, B.Ap, slot, 1, B.scal + SC_PAP * blk.nr);
-    bupdate_kernel<<<nd, TPBB, 0, stream>>>(P, B, slot);
-    CUDA_CHECK(cudaGetLastError());
+    launch_pdl(bupdate_kernel, dim3(nd), dim3(TPBB), 0, stream, P, B, slot);
 }
 
 void GpuSolver::solve_multi(const double *rhs, int nrhs, int rhs_size, double *solutions, int solution_size,
@@ -4306,7 +4757,7 @@ void GpuSolver::solve_multi(const double *rhs, int nrhs, int rhs_size, double *s
         cudaGraph_t g;
         CUDA_CHECK(cudaStreamBeginCapture(I.stream, cudaStreamCaptureModeThreadLocal));
         for (int j = 0; j < chunk; ++j) I.launch_block_iteration(j);
-        bchunk_end_kernel<<<1, 32, 0, I.stream>>>(P, chunk);
+        launch_pdl(bchunk_end_kernel, dim3(1), dim3(32), 0, I.stream, P, chunk);
         CUDA_CHECK(cudaStreamEndCapture(I.stream, &g));
         CUDA_CHECK(cudaGraphInstantiate(&G.graph, g, 0));
         cudaGraphDestroy(g);

@@ -76,6 +76,7 @@ public:
     // out[e] = v_e^T K_e u_e over the stored elements (u, v: caller DOF vectors of size n)
     void element_energies(const ElementData &el, const double *u, const double *v, int n, double *out);
     size_t device_bytes() const;
+    double kplus_tile_fraction() const;   // applied / stored K+ factor tiles
     int device_id() const;
     void set_options(const SolveOptions &opt);
     std::string tuning() const;        // chosen SYMV variant and granularities

@@ -27,7 +27,7 @@ FP64, FP32, BF16 = 0, 1, 2
 STAT_NAMES = ["iterations", "converged", "dual_size", "kernel_size", "subdomains", "prep_seconds",
               "upload_seconds", "solve_ms", "solve_wall_ms", "fapply_bytes", "replacements",
               "kernel_launches", "device_bytes", "final_norm", "tolerance", "elements", "prep_device_ms",
-              "prep_device_flops"]
+              "prep_device_flops", "kplus_tiles"]
 
 EXPORTED = [
     "FETI4ISetDefaultIntegerOptions", "FETI4ISetDefaultRealOptions", "FETI4ICreateStiffnessMatrix",

@@ -88,6 +88,7 @@ typedef enum {
     FETI4I_STAT_ELEMENTS,           /* stored elements */
     FETI4I_STAT_PREP_DEVICE_MS,     /* device time of the GPU eliminations (FETI4I_EXT_DEVICE_PREP), else 0 */
     FETI4I_STAT_PREP_DEVICE_FLOPS,  /* their algorithmic FP64 flops */
+    FETI4I_STAT_KPLUS_TILES,        /* fraction of the stored K+ factor tiles that are not all zero (applied) */
     FETI4I_STAT_SIZE
 } FETI4IStatIndex;
 void FETI4IGetStats(FETI4IInstance instance, FETI4IInt size, FETI4IReal *stats);

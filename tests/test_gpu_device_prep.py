@@ -55,6 +55,12 @@ def test_schur_kernel_kplus(cases, name):
     st = dev.stats()
     assert st["prep_device_ms"] > 0 and st["prep_device_flops"] > 0
     assert host.stats()["prep_device_ms"] == 0
+    # the K^+ kernels apply only the factor tiles that are not all zero; both factors have the
+    # same envelope, so the same tiles
+    assert 0.0 < st["kplus_tiles"] <= 1.0
+    assert abs(st["kplus_tiles"] - host.stats()["kplus_tiles"]) <= 0.02
+    if name == "elast_big":
+        assert st["kplus_tiles"] < 0.95
     rng = np.random.default_rng(5)
     for d in range(int(P.elem_domain.max()) + 1):
         ih, idv = host.subdomain_info(d), dev.subdomain_info(d)
