@@ -11,6 +11,7 @@
 //                                       src/solver/generic/SparseMatrix.cpp:1093-1160
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <omp.h>
 
 #include <algorithm>
 #include <cmath>
@@ -1739,6 +1740,10 @@ struct GpuSolver::Impl {
     double *d_f = nullptr, *d_kf = nullptr, *d_g = nullptr, *d_rhs = nullptr, *d_sol = nullptr;
     double *h_pinned = nullptr;
     size_t h_pinned_n = 0;
+    std::vector<cudaEvent_t> stage_ev;
+    void ensure_pinned(size_t n);
+    void h2d_columns(double *dev, size_t dev_pitch, const double *host, size_t host_pitch, size_t count, int ncols);
+    void d2h_columns(double *host, size_t host_pitch, const double *dev, size_t dev_pitch, size_t count, int ncols);
     // block (multi right-hand-side) solver
     struct Block {
         int nr = 0;
@@ -1790,6 +1795,7 @@ struct GpuSolver::Impl {
     ~Impl() {
         if (blk.graph) cudaGraphExecDestroy(blk.graph);
         if (h_pinned) cudaFreeHost(h_pinned);
+        for (cudaEvent_t e : stage_ev) cudaEventDestroy(e);
         if (graph) cudaGraphExecDestroy(graph);
         for (void *p : allocs) cudaFree(p);
         if (stream) cudaStreamDestroy(stream);
@@ -2774,22 +2780,97 @@ std::string GpuSolver::tuning() const {
     return s;
 }
 
+// ---- caller arrays <-> device through the pinned staging buffer
+// The arrays move in chunks of at least 1 MB: all host threads copy chunk k between the caller's
+// (pageable) memory and the staging buffer while the copy engine moves chunk k - 1.
+namespace {
+constexpr size_t STAGE_MIN = (size_t)1 << 17;   // doubles per chunk, at least
+constexpr int STAGE_EVENTS = 128;
+
+void par_copy(double *dst, const double *src, size_t n) {
+    const int nt = omp_get_max_threads();
+    if (n < ((size_t)1 << 15) || nt <= 1) {
+        std::memcpy(dst, src, n * sizeof(double));
+        return;
+    }
+    const size_t per = (n + nt - 1) / nt;
+#pragma omp parallel for schedule(static) num_threads(nt)
+    for (int t = 0; t < nt; ++t) {
+        const size_t b = (size_t)t * per;
+        if (b < n) std::memcpy(dst + b, src + b, std::min(per, n - b) * sizeof(double));
+    }
+}
+}  // namespace
+
+void GpuSolver::Impl::ensure_pinned(size_t n) {
+    n = std::max<size_t>(n, 1);
+    if (h_pinned_n >= n) return;
+    CUDA_CHECK(cudaStreamSynchronize(stream));   // no copy of the old buffer in flight
+    if (h_pinned) CUDA_CHECK(cudaFreeHost(h_pinned));
+    h_pinned = nullptr;
+    h_pinned_n = 0;
+    CUDA_CHECK(cudaMallocHost(&h_pinned, n * sizeof(double)));
+    h_pinned_n = n;
+}
+
+// columns j < ncols: dev[j * dev_pitch + i] = host[j * host_pitch + i], i < count (enqueued on the
+// stream; the caller's memory is free again on return)
+void GpuSolver::Impl::h2d_columns(double *dev, size_t dev_pitch, const double *host, size_t host_pitch, size_t count,
+                                  int ncols) {
+    if (count == 0 || ncols <= 0) return;
+    ensure_pinned(count * ncols);
+    const size_t chunk = std::max(STAGE_MIN, count * ncols / STAGE_EVENTS + 1);
+    for (int j = 0; j < ncols; ++j)
+        for (size_t c0 = 0; c0 < count; c0 += chunk) {
+            const size_t len = std::min(chunk, count - c0);
+            double *stg = h_pinned + (size_t)j * count + c0;
+            par_copy(stg, host + (size_t)j * host_pitch + c0, len);
+            CUDA_CHECK(cudaMemcpyAsync(dev + (size_t)j * dev_pitch + c0, stg, len * sizeof(double),
+                                       cudaMemcpyHostToDevice, stream));
+        }
+}
+
+// columns j < ncols: host[j * host_pitch + i] = dev[j * dev_pitch + i], i < count (after the work
+// enqueued before it; returns when the caller's memory holds the result)
+void GpuSolver::Impl::d2h_columns(double *host, size_t host_pitch, const double *dev, size_t dev_pitch, size_t count,
+                                  int ncols) {
+    if (count == 0 || ncols <= 0) {
+        CUDA_CHECK(cudaStreamSynchronize(stream));
+        return;
+    }
+    ensure_pinned(count * ncols);
+    const size_t chunk = std::max(STAGE_MIN, count * ncols / STAGE_EVENTS + 1);
+    struct Piece { size_t stg, host, dev, len; };
+    std::vector<Piece> pieces;
+    for (int j = 0; j < ncols; ++j)
+        for (size_t c0 = 0; c0 < count; c0 += chunk)
+            pieces.push_back({(size_t)j * count + c0, (size_t)j * host_pitch + c0, (size_t)j * dev_pitch + c0,
+                              std::min(chunk, count - c0)});
+    while (stage_ev.size() < pieces.size()) {
+        cudaEvent_t e;
+        CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        stage_ev.push_back(e);
+    }
+    for (size_t k = 0; k < pieces.size(); ++k) {
+        CUDA_CHECK(cudaMemcpyAsync(h_pinned + pieces[k].stg, dev + pieces[k].dev, pieces[k].len * sizeof(double),
+                                   cudaMemcpyDeviceToHost, stream));
+        CUDA_CHECK(cudaEventRecord(stage_ev[k], stream));
+    }
+    for (size_t k = 0; k < pieces.size(); ++k) {
+        CUDA_CHECK(cudaEventSynchronize(stage_ev[k]));
+        par_copy(host + pieces[k].host, h_pinned + pieces[k].stg, pieces[k].len);
+    }
+}
+
 void GpuSolver::solve_full(const double *rhs, int rhs_size, double *solution, int solution_size, SolveStats &stats,
                            bool upload_rhs) {
     Impl &I = *impl;
     DevProblem &P = I.P;
     const int nd = P.nd;
-    const size_t need = std::max<size_t>({(size_t)rhs_size, (size_t)solution_size, (size_t)1});
-    if (I.h_pinned_n < need) {
-        if (I.h_pinned) cudaFreeHost(I.h_pinned);
-        CUDA_CHECK(cudaMallocHost(&I.h_pinned, need * sizeof(double)));
-        I.h_pinned_n = need;
-    }
     if (upload_rhs) {
         CUDA_CHECK(cudaMemsetAsync(I.d_rhs, 0, sizeof(double) * std::max(1, I.n_caller), I.stream));
         const int ncp = std::min(rhs_size, I.n_caller);
-        std::memcpy(I.h_pinned, rhs, sizeof(double) * ncp);
-        CUDA_CHECK(cudaMemcpyAsync(I.d_rhs, I.h_pinned, sizeof(double) * ncp, cudaMemcpyHostToDevice, I.stream));
+        I.h2d_columns(I.d_rhs, 0, rhs, 0, (size_t)std::max(0, ncp), 1);
         split_rhs_kernel<<<(I.ntot + 255) / 256, 256, 0, I.stream>>>(I.d_rhs, I.d_gdof, I.d_invm, I.d_f, I.ntot);
         // Total FETI: b needs K^+ f at the touched DOFs only; the forward pass L^-1 f is kept for
         // the primal recovery
@@ -2811,9 +2892,7 @@ void GpuSolver::solve_full(const double *rhs, int rhs_size, double *solution, in
     primal_merge_kernel<<<nd, TPB, 0, I.stream>>>(P, I.d_doff, I.d_rdofs, I.d_Rd, I.d_kf, I.d_gdof, I.d_invm, I.d_sol);
     CUDA_CHECK(cudaGetLastError());
     const int ncp = std::min(solution_size, I.n_caller);
-    CUDA_CHECK(cudaMemcpyAsync(I.h_pinned, I.d_sol, sizeof(double) * std::max(0, ncp), cudaMemcpyDeviceToHost, I.stream));
-    CUDA_CHECK(cudaStreamSynchronize(I.stream));
-    std::memcpy(solution, I.h_pinned, sizeof(double) * std::max(0, ncp));
+    I.d2h_columns(solution, 0, I.d_sol, 0, (size_t)std::max(0, ncp), 1);
     for (int i = std::max(0, ncp); i < solution_size; ++i) solution[i] = 0.0;
     stats.kernel_launches += 10;
 }
@@ -4712,9 +4791,7 @@ void GpuSolver::solve_multi(const double *rhs, int nrhs, int rhs_size, double *s
     if (upload_rhs) {
         CUDA_CHECK(cudaMemsetAsync(I.blk.rhs, 0, sizeof(double) * (size_t)nc * nr, I.stream));
         const int ncp = std::min(rhs_size, I.n_caller);
-        for (int j = 0; j < nrhs; ++j)
-            CUDA_CHECK(cudaMemcpyAsync(I.blk.rhs + (size_t)j * nc, rhs + (size_t)j * rhs_size, sizeof(double) * ncp,
-                                       cudaMemcpyHostToDevice, I.stream));
+        I.h2d_columns(I.blk.rhs, nc, rhs, rhs_size, (size_t)std::max(0, ncp), nrhs);
         const long long tot = (long long)ntot * nr;
         bsplit_rhs_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, I.stream>>>(I.blk.rhs, nc, I.d_gdof, I.d_invm, I.blk.f,
                                                                               ntot, nr);
@@ -4801,11 +4878,7 @@ void GpuSolver::solve_multi(const double *rhs, int nrhs, int rhs_size, double *s
                                                            I.blk.sol, nc, ntot);
         CUDA_CHECK(cudaGetLastError());
         const int ncp = std::min(solution_size, I.n_caller);
-        for (int j = 0; j < nrhs; ++j) {
-            CUDA_CHECK(cudaMemcpyAsync(solutions + (size_t)j * solution_size, I.blk.sol + (size_t)j * nc,
-                                       sizeof(double) * ncp, cudaMemcpyDeviceToHost, I.stream));
-        }
-        CUDA_CHECK(cudaStreamSynchronize(I.stream));
+        I.d2h_columns(solutions, solution_size, I.blk.sol, nc, (size_t)std::max(0, ncp), nrhs);
         for (int j = 0; j < nrhs; ++j)
             for (int i = std::max(0, ncp); i < solution_size; ++i) solutions[(size_t)j * solution_size + i] = 0.0;
     }
