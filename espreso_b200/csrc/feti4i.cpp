@@ -628,6 +628,16 @@ void FETI4IApplyDualOperator(FETI4IInstance instance, FETI4IInt precision, FETI4
     });
 }
 
+void FETI4IApplyDualOperatorMulti(FETI4IInstance instance, FETI4IInt precision, FETI4IInt nrhs, FETI4IReal *x,
+                                  FETI4IReal *y) {
+    guarded([&] {
+        auto *I = check_instance(instance);
+        FETI_CHECK(I->gpu, "FETI4I: no device solver");
+        FETI_CHECK(x && y, "FETI4IApplyDualOperatorMulti: invalid arrays");
+        I->gpu->apply_F_multi(x, y, (int)nrhs, precision);
+    });
+}
+
 FETI4IReal FETI4ITimeDualOperator(FETI4IInstance instance, FETI4IInt precision, FETI4IInt reps) {
     double ms = -1.0;
     guarded([&] {

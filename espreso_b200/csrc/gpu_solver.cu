@@ -1757,10 +1757,12 @@ struct GpuSolver::Impl {
         int flat_grid = 1;
         int2 *units4 = nullptr;
         int nunits4 = 0;
+        float *pan = nullptr;          // K-major panels of the mixed blocks (asynchronous tensor-core SYMM)
         int2 *dunits = nullptr;   // SYMM units of the Dirichlet blocks (Dirichlet preconditioner)
         int ndunits = 0;
     } blk;
     void ensure_block(int nr);
+    void prepare_symm_panels();
     void launch_symm(const TileSetHost &T, bool src32, const double *x64, const float *x32, double *out, int slot,
                      int mode);
     void launch_block_iteration(int slot);
@@ -4332,6 +4334,312 @@ tile_symm_tc_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, d
     }
 }
 
+// ---- Tile SYMM on the tensor cores, asynchronous staging (32 right-hand sides)
+// Same units (four tile rows of one subdomain, M = 128) and results as tile_symm_tc_kernel<32>,
+// without register staging or transposes.  Every block column J of a unit arrives as raw FP32 by
+// cp.async (16-byte chunks placed at their swizzled positions) into a ring of S stages:
+//   * J >= I0 + 3: the stored tiles (I, J), K-major (128-byte swizzle);
+//   * J <  I0:     the stored tiles (J, I) as they are, MN-major (the MMA reads A transposed;
+//     128-byte swizzle with 32-byte atoms, the MN-major layout of 32-bit operands);
+//   * the three mixed blocks I0 <= J < I0 + 3: a K-major panel assembled once per unit
+//     (panel_kernel, before the first solve);
+//   * X_J: 32 rows of x, N-contiguous, MN-major (BMN) or transposed to K-major by the CTA.
+// The CTA splits the raw data in place, x = hi + lo with hi = x rounded to TF32 (the stage keeps
+// hi, the low parts go to a double buffer at the same positions; with BMN = false X_J is also
+// transposed there into K-major order), and one thread issues hi*hi + hi*lo + lo*hi
+// (tcgen05.mma kind::tf32) and commits to the stage's mbarrier, which frees both the stage and
+// the low-part buffer.  The copies of block t + S - 2 are
+// in flight while block t is converted and multiplied.  Units are claimed from the work queue S - 2
+// blocks ahead.  Every wait is bounded: on time-out the CTA records an error, drains its copies
+// and MMAs, frees its tensor memory and returns.
+namespace tc2 {
+constexpr int S = 8;                         // raw stages
+constexpr unsigned A_BYTES = 128 * 128;      // 128 rows x 32 FP32
+constexpr unsigned B_BYTES = 32 * 128;       // 32 k-rows x 32 FP32
+constexpr unsigned STAGE = A_BYTES + B_BYTES;
+constexpr unsigned LOW = A_BYTES + 2 * B_BYTES;   // low parts of A; X_J high and low parts when K-major
+constexpr unsigned SMEM = S * STAGE + 2 * LOW + 1024;
+constexpr int RING = 8;                      // claimed units in flight (>= S - 1)
+// MN-major TF32 operand: the 128-byte swizzle with 32-byte atoms (the only MN-major layout of
+// 32-bit operands), rows of 128 bytes (32 MN elements) along K; in row r the 32-byte granule g sits
+// at g ^ (r & 3).  32-element MN chunks LBO = 4096 bytes apart, 4-row K groups SBO = 512 bytes apart.
+__device__ __forceinline__ unsigned swz_mn(int row, int chunk) {
+    return (unsigned)(row * 128 + (((((chunk >> 1) ^ (row & 3)) << 1) | (chunk & 1)) << 4));
+}
+__device__ __forceinline__ uint64_t sdesc_mn(unsigned addr) {
+    return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)(4096 >> 4) << 16) | ((uint64_t)(512 >> 4) << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)1 << 61);
+}
+// kind::tf32, M = 128, N = 32, A and B K-major (0) or MN-major (1)
+__host__ __device__ constexpr uint32_t idesc(int a_mn, int b_mn) {
+    return tc::idesc<32>() | ((uint32_t)a_mn << 15) | ((uint32_t)b_mn << 16);
+}
+__device__ __forceinline__ void cp16(unsigned dst, const void *src, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+struct UnitInfo {
+    int u, m, I0, tn, n, voff, fb;   // fb: first block of the unit in the CTA's block stream
+    long long t0;
+};
+}  // namespace tc2
+
+// K-major panels of the mixed blocks: unit u (tile rows I0 .. I0+3 of matrix m), p = 0..2, block
+// column J = I0 + p: rows 32 q + r of S, columns 32 J .. 32 J + 31 (zero past the matrix)
+__global__ void panel_kernel(TileSetDev ts, const int2 *units, int nunits, float *pan) {
+    const int u = blockIdx.x / 3, p = blockIdx.x % 3;
+    if (u >= nunits) return;
+    const int m = units[u].x, I0 = 4 * units[u].y, J = I0 + p;
+    const int tn = ts.mat_tn[m];
+    const long long t0 = ts.mat_tile0[m];
+    const float *tiles = reinterpret_cast<const float *>(ts.tiles);
+    float *dst = pan + ((size_t)u * 3 + p) * 4096;
+    for (int e = threadIdx.x; e < 4096; e += blockDim.x) {
+        const int r = e >> 5, k = e & 31, q = r >> 5, rr = r & 31, I = I0 + q;
+        float v = 0.f;
+        if (J < tn && I < tn) {
+            if (I <= J) v = tiles[(size_t)(t0 + (long long)I * tn - (long long)I * (I - 1) / 2 + (J - I)) * 1024 + rr * 32 + k];
+            else v = tiles[(size_t)(t0 + (long long)J * tn - (long long)J * (J - 1) / 2 + (I - J)) * 1024 + k * 32 + rr];
+        }
+        dst[e] = v;
+    }
+}
+
+template <bool BMN>
+__global__ void __launch_bounds__(256, 1)
+tile_symm_tc2_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, const float *pan, double *out,
+                     const int2 *units, int nunits, int slot, int mode) {
+    pdl_enter();
+    constexpr int S = tc2::S, RING = tc2::RING;
+    extern __shared__ unsigned char tc2_smem[];
+    __shared__ unsigned long long bar[S];
+    __shared__ tc2::UnitInfo s_ring[RING];
+    __shared__ unsigned s_tmem;
+    __shared__ int s_nring, s_end, s_err, s_last;
+    __shared__ double s_dot[8][16];
+    if (mode != 0) {
+        const int iter = P.st->iter_base + slot;
+        if (skip_iter(P.st, iter)) return;
+    }
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const unsigned base = smem_u32(tc2_smem);
+    const unsigned pad = (1024u - (base & 1023u)) & 1023u;
+    unsigned char *buf = tc2_smem + pad;     // 1024-byte aligned: S raw stages, then 2 low-part buffers
+    const unsigned sbuf = base + pad;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(32u)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_nring = 0;
+        s_end = -1;
+        s_err = 0;
+    }
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const unsigned tmem = s_tmem;
+    const float *tiles = reinterpret_cast<const float *>(ts.tiles);
+    auto tidx = [](long long t0, int tn, int a, int b) -> long long {
+        return t0 + (long long)a * tn - (long long)a * (a - 1) / 2 + (b - a);
+    };
+    int pk = 0, pJ = 0;   // producer: ring counter of its unit, block column in the unit
+    int ck = 0, cJ = 0;   // consumer
+    int last_commit = -1;
+    bool ok = true;
+    for (int t = -(S - 2);; ++t) {
+        const int pb = t + S - 2;
+        if (tid == 0) {
+            // claim units until block pb of the stream is covered or the queue is empty
+            while (s_end < 0) {
+                const int nr_ = s_nring;
+                int endb = 0;
+                if (nr_ > 0) endb = s_ring[(nr_ - 1) % RING].fb + s_ring[(nr_ - 1) % RING].tn;
+                if (pb < endb) break;
+                const int u = atomicAdd(&B.queue[0], 1);
+                if (u >= nunits) {
+                    s_end = endb;
+                    break;
+                }
+                tc2::UnitInfo &N = s_ring[nr_ % RING];
+                N.u = u;
+                N.m = units[u].x;
+                N.I0 = 4 * units[u].y;
+                N.tn = ts.mat_tn[N.m];
+                N.n = ts.mat_n[N.m];
+                N.voff = ts.mat_voff[N.m];
+                N.t0 = ts.mat_tile0[N.m];
+                N.fb = endb;
+                s_nring = nr_ + 1;
+            }
+        }
+        if (!__syncthreads_and(ok)) break;
+        const int end = s_end;
+        if (end >= 0 && t >= end) break;
+        // stage pb % S last held block t - 2 (and low-part buffer t & 1 too): its MMAs must be done
+        if (t >= 2 && !mbar_wait(&bar[(t - 2) % S], (unsigned)(((t - 2) / S) & 1))) ok = false;
+        if (end < 0 || pb < end) {
+            const tc2::UnitInfo &U = s_ring[pk % RING];
+            const int J = pJ, I0 = U.I0, tn = U.tn;
+            const unsigned sa = sbuf + (unsigned)(pb % S) * tc2::STAGE, sb = sa + tc2::A_BYTES;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int q = tid + 256 * i, r = q >> 3, c = q & 7, qq = r >> 5, rr = r & 31, I = I0 + qq;
+                const float *src = tiles;
+                bool valid = true;
+                if (J >= I0 + 3) {
+                    valid = I < tn;
+                    if (valid) src = tiles + (size_t)tidx(U.t0, tn, I, J) * 1024 + rr * 32 + 4 * c;
+                } else if (J < I0) {
+                    valid = I < tn;
+                    if (valid) src = tiles + (size_t)tidx(U.t0, tn, J, I) * 1024 + rr * 32 + 4 * c;
+                    tc2::cp16(sa + tc2::swz_mn(r, c), src, valid);
+                    continue;
+                } else {
+                    src = pan + ((size_t)U.u * 3 + (J - I0)) * 4096 + r * 32 + 4 * c;
+                }
+                tc2::cp16(sa + tc::swz(r, c), src, valid);
+            }
+            {
+                const int kk = tid >> 3, c = tid & 7, row = TILE * J + kk;
+                const bool valid = row < U.n;
+                tc2::cp16(sb + (BMN ? tc2::swz_mn(kk, c) : tc::swz(kk, c)),
+                          valid ? (const void *)(x32 + (size_t)(U.voff + row) * 32 + 4 * c) : x32, valid);
+            }
+            if (++pJ == tn) {
+                ++pk;
+                pJ = 0;
+            }
+        }
+        tc2::cp_commit();
+        if (t < 0) continue;
+        // block t: this thread's copies, then everyone's
+        tc2::cp_wait<S - 2>();
+        __syncthreads();
+        const unsigned st = (unsigned)(t % S) * tc2::STAGE;
+        const unsigned lo = (unsigned)S * tc2::STAGE + (unsigned)(t & 1) * tc2::LOW;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {   // 1024 A chunks of 16 bytes, split in place
+            const unsigned off = (unsigned)(tid + 256 * i) * 16;
+            tc::split_store(buf + st, buf + lo, off, *reinterpret_cast<const float4 *>(buf + st + off));
+        }
+        if (BMN) {
+            const unsigned off = tc2::A_BYTES + (unsigned)tid * 16;
+            tc::split_store(buf + st, buf + lo, off, *reinterpret_cast<const float4 *>(buf + st + off));
+        } else {
+            // X_J chunk (k-row kk, n = 4c .. 4c + 3) -> K-major [n][k] high and low parts
+            const int kk = tid >> 3, c = tid & 7;
+            const float4 v = *reinterpret_cast<const float4 *>(buf + st + tc2::A_BYTES + tc::swz(kk, c));
+            const float xv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const float h = tc::tf32_hi(xv[e]);
+                const unsigned o = tc::swz(4 * c + e, kk >> 2) + 4u * (kk & 3);
+                *reinterpret_cast<float *>(buf + lo + tc2::A_BYTES + o) = h;
+                *reinterpret_cast<float *>(buf + lo + tc2::A_BYTES + tc2::B_BYTES + o) = xv[e] - h;
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        const tc2::UnitInfo U = s_ring[ck % RING];
+        if (tid == 0) {
+            tc::fence_after();
+            const bool amn = cJ < U.I0;       // stored tiles (J, I): A read transposed
+            const uint32_t id = tc2::idesc(amn ? 1 : 0, BMN ? 1 : 0);
+            const unsigned ahi = sbuf + st, alo = sbuf + lo;
+            const unsigned bhi = BMN ? ahi + tc2::A_BYTES : alo + tc2::A_BYTES;
+            const unsigned blo = BMN ? alo + tc2::A_BYTES : alo + tc2::A_BYTES + tc2::B_BYTES;
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) {
+                const uint64_t dah = amn ? tc2::sdesc_mn(ahi + 1024u * kk) : tc::sdesc(ahi + 32u * kk);
+                const uint64_t dal = amn ? tc2::sdesc_mn(alo + 1024u * kk) : tc::sdesc(alo + 32u * kk);
+                const uint64_t dbh = BMN ? tc2::sdesc_mn(bhi + 1024u * kk) : tc::sdesc(bhi + 32u * kk);
+                const uint64_t dbl = BMN ? tc2::sdesc_mn(blo + 1024u * kk) : tc::sdesc(blo + 32u * kk);
+                tc::mma(tmem, dah, dbh, id, (cJ > 0 || kk > 0) ? 1u : 0u);
+                tc::mma(tmem, dah, dbl, id, 1u);
+                tc::mma(tmem, dal, dbh, id, 1u);
+            }
+            tc::commit(&bar[t % S]);
+        }
+        last_commit = t;
+        if (cJ + 1 == U.tn) {
+            // unit complete: accumulator -> rows of the output, dots with x per column
+            if (!mbar_wait(&bar[t % S], (unsigned)((t / S) & 1))) ok = false;
+            tc::fence_after();
+            uint32_t r[16];
+            tc::ld16(tmem + ((unsigned)(32 * (warp & 3)) << 16) + (unsigned)((warp >> 2) * 16), r);
+            const int row = TILE * U.I0 + 32 * (warp & 3) + lane, c0 = (warp >> 2) * 16;
+            double dl[16];
+#pragma unroll
+            for (int c = 0; c < 16; ++c) {
+                dl[c] = 0.0;
+                if (row < U.n && ok) {
+                    const size_t o = (size_t)(U.voff + row) * 32 + c0 + c;
+                    const double y = (double)__uint_as_float(r[c]);
+                    out[o] = y;
+                    dl[c] = (double)x32[o] * y;
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < 16; ++c) {
+                double v = dl[c];
+#pragma unroll
+                for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+                if (lane == 0) s_dot[warp][c] = v;
+            }
+            tc::fence_before();
+            __syncthreads();
+            if (tid < 32) {
+                const int h = tid / 16, c = tid % 16;
+                double tsum = 0.0;
+                for (int w = 0; w < 4; ++w) tsum += s_dot[4 * h + w][c];
+                B.unit_dot[(size_t)U.u * 32 + tid] = tsum;
+            }
+        }
+        if (++cJ == U.tn) {
+            ++ck;
+            cJ = 0;
+        }
+    }
+    // drain: copies, then the MMAs of the last committed block
+    tc2::cp_wait_all();
+    if (last_commit >= 0 && !mbar_wait(&bar[last_commit % S], (unsigned)((last_commit / S) & 1))) ok = false;
+    if (!ok && lane == 0) s_err = 1;
+    tc::fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32u) : "memory");
+    if (tid == 0 && s_err) atomicExch(&P.st->error, 1);
+    if (tid == 0) {
+        __threadfence();
+        s_last = (atomicAdd(&B.queue[1], 1) == (int)gridDim.x - 1);
+    }
+    __syncthreads();
+    if (s_last) {
+        if (mode == 1) {
+            __threadfence();
+            if (tid < 32) {
+                double tsum = 0.0;
+                for (int q = 0; q < nunits; ++q) tsum += __ldcg(&B.unit_dot[(size_t)q * 32 + tid]);
+                B.scal[SC_PAP * 32 + tid] = tsum;
+            }
+        }
+        if (tid == 0) {
+            B.queue[0] = 0;
+            B.queue[1] = 0;
+            __threadfence();
+        }
+    }
+}
+
 // ---- Hybrid Total FETI cluster correction for nr columns ([row][rhs] layout)
 // z_i = V_i^T x_i: one warp per column of V_i, lane = (row group, rhs)
 __global__ void bhyb_vt_kernel(DevProblem P, HybDev H, BlockDev B, const double *x, double *z, int slot, int cond) {
@@ -4568,6 +4876,7 @@ void GpuSolver::Impl::ensure_block(int nr) {
         for (int I4 = 0; 4 * I4 < tn[m]; ++I4) units4.push_back(make_int2(m, I4));
     blk.units4 = upload(units4);
     blk.nunits4 = (int)units4.size();
+    blk.pan = nullptr;   // rebuilt for these units at the first asynchronous tensor-core SYMM
     size_t max_units = std::max(units.size(), units4.size());
     if (opt.precond == PREC_DIRICHLET) {
         // SYMM units of the Dirichlet blocks S_dir (T space)
@@ -4660,6 +4969,43 @@ static void symm_mma_launch(int nsm, int ncta, cudaStream_t st, TileSetDev td, D
     launch_pdl(tile_symm_mma_kernel<NR>, dim3(grid), dim3(256), 0, st, td, P, B, x64, out, units, nunits, slot, mode);
 }
 
+// The asynchronous variant is opt-in (FETI4I_SYMM_TC2=1): on the heat workload of 512 subdomains it
+// measured 71.1 ms per batch of 32 load cases against 57.1 ms with tile_symm_tc_kernel<32>.
+static bool symm_tc2_enabled() {
+    static const bool on = [] {
+        const char *e = getenv("FETI4I_SYMM_TC2");
+        return e && e[0] == '1';
+    }();
+    return on;
+}
+
+static bool symm_tc2_bmn() {
+    static const bool on = [] {
+        const char *e = getenv("FETI4I_TC2_BMN");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+static void symm_tc2_launch(int nsm, int nunits, cudaStream_t st, TileSetDev td, DevProblem P, BlockDev B,
+                            const float *x32, const float *pan, double *out, const int2 *units, int slot, int mode) {
+    static bool attr = false;
+    if (!attr) {
+        CUDA_CHECK(cudaFuncSetAttribute(tile_symm_tc2_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)tc2::SMEM));
+        CUDA_CHECK(cudaFuncSetAttribute(tile_symm_tc2_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)tc2::SMEM));
+        attr = true;
+    }
+    const int grid = std::max(1, std::min(nunits, nsm));
+    if (symm_tc2_bmn())
+        launch_pdl(tile_symm_tc2_kernel<true>, dim3(grid), dim3(256), (size_t)tc2::SMEM, st, td, P, B, x32, pan, out,
+                   units, nunits, slot, mode);
+    else
+        launch_pdl(tile_symm_tc2_kernel<false>, dim3(grid), dim3(256), (size_t)tc2::SMEM, st, td, P, B, x32, pan, out,
+                   units, nunits, slot, mode);
+}
+
 template <int NR>
 static void symm_tc_launch(int nsm, int nunits, cudaStream_t st, TileSetDev td, DevProblem P, BlockDev B,
                            const float *x32, double *out, const int2 *units, int slot, int mode) {
@@ -4683,6 +5029,13 @@ void GpuSolver::Impl::launch_symm(const TileSetHost &T, bool src32, const double
     const bool dir = &T == &Dir;
     const int2 *units = dir ? blk.dunits : blk.units;
     const int nunits = dir ? blk.ndunits : blk.nunits;
+    if (!dir && opt.symm_tensor && T.prec == SCHUR_FP32 && src32 && nr == 32 && symm_tc2_enabled()) {
+        TileSetDev td = T.dev();
+        FETI_CHECK(blk.pan != nullptr, "internal: tensor-core SYMM panels not built");
+        symm_tc2_launch(nsm, blk.nunits4, stream, td, P, blk.B, x32, blk.pan, out, blk.units4, slot, mode);
+        CUDA_CHECK(cudaGetLastError());
+        return;
+    }
     if (!dir && opt.symm_tensor && T.prec == SCHUR_FP32 && src32 && nr >= 8) {
         TileSetDev td = T.dev();
         switch (nr) {
@@ -4777,6 +5130,45 @@ void GpuSolver::Impl::launch_block_iteration(int slot) {
     launch_pdl(bupdate_kernel, dim3(nd), dim3(TPBB), 0, stream, P, B, slot);
 }
 
+// panels of the mixed blocks for the asynchronous tensor-core SYMM (built before any graph capture)
+void GpuSolver::Impl::prepare_symm_panels() {
+    if (blk.nr != 32 || !opt.symm_tensor || Flow.prec != SCHUR_FP32 || !symm_tc2_enabled() || blk.pan) return;
+    blk.pan = alloc<float>((size_t)blk.nunits4 * 3 * 4096);
+    panel_kernel<<<std::max(1, blk.nunits4 * 3), 256, 0, stream>>>(Flow.dev(), blk.units4, blk.nunits4, blk.pan);
+    CUDA_CHECK(cudaGetLastError());
+}
+
+// y_j = F x_j for nrhs dual vectors (column j at j * n_lambda) through the multi right-hand-side
+// F apply of the block PCG (tile SYMM in the given Schur precision, plus the HTFETI correction)
+void GpuSolver::apply_F_multi(const double *x, double *y, int nrhs, int precision) {
+    Impl &I = *impl;
+    DevProblem &P = I.P;
+    FETI_CHECK(nrhs >= 1 && nrhs <= 32, "FETI4IApplyDualOperatorMulti: 1..32 vectors per call");
+    const TileSetHost &T = precision == SCHUR_FP64 ? I.F64 : I.Flow;
+    FETI_CHECK(T.prec == precision, "FETI4I: the requested Schur precision was not prepared on the device");
+    int nr = 4;
+    while (nr < nrhs) nr *= 2;
+    I.ensure_block(nr);
+    I.prepare_symm_panels();
+    BlockDev &B = I.blk.B;
+    const int NL = P.NL;
+    std::vector<double> xb((size_t)NL * nr, 0.0), yb((size_t)NL * nr);
+    std::vector<float> xf((size_t)NL * nr);
+    for (int e = 0; e < NL; ++e)
+        for (int j = 0; j < nrhs; ++j) xb[(size_t)e * nr + j] = x[(size_t)j * I.n_lambda + I.h_lam[e]];
+    for (size_t i = 0; i < xb.size(); ++i) xf[i] = (float)xb[i];
+    CUDA_CHECK(cudaMemcpyAsync(B.p, xb.data(), xb.size() * sizeof(double), cudaMemcpyHostToDevice, I.stream));
+    CUDA_CHECK(cudaMemcpyAsync(B.p32, xf.data(), xf.size() * sizeof(float), cudaMemcpyHostToDevice, I.stream));
+    CUDA_CHECK(cudaMemsetAsync(B.Ap, 0, sizeof(double) * (size_t)NL * nr, I.stream));
+    I.launch_symm(T, precision != SCHUR_FP64, B.p, B.p32, B.Ap, 0, 0);
+    I.launch_block_hybrid(B.p, B.Ap, 0, 0, nullptr);
+    CUDA_CHECK(cudaMemcpyAsync(yb.data(), B.Ap, yb.size() * sizeof(double), cudaMemcpyDeviceToHost, I.stream));
+    CUDA_CHECK(cudaStreamSynchronize(I.stream));
+    for (size_t i = 0; i < (size_t)nrhs * I.n_lambda; ++i) y[i] = 0.0;
+    for (int e = 0; e < NL; ++e)
+        for (int j = 0; j < nrhs; ++j) y[(size_t)j * I.n_lambda + I.h_lam[e]] += yb[(size_t)e * nr + j];
+}
+
 void GpuSolver::solve_multi(const double *rhs, int nrhs, int rhs_size, double *solutions, int solution_size,
                             SolveStats &stats, bool upload_rhs) {
     Impl &I = *impl;
@@ -4785,6 +5177,7 @@ void GpuSolver::solve_multi(const double *rhs, int nrhs, int rhs_size, double *s
     int nr = 4;
     while (nr < nrhs) nr *= 2;
     I.ensure_block(nr);
+    I.prepare_symm_panels();
     BlockDev &B = I.blk.B;
     const int nd = P.nd, nc = std::max(1, I.n_caller), ntot = I.ntot;
     const int cgrid = (P.nK + CR - 1) / CR;

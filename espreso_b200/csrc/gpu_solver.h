@@ -70,6 +70,7 @@ public:
     void dual_rhs(const double *rhs, int rhs_size, double *b, double *e, int n_lambda, int n_kern);
     // y = F x in lambda space with the given operator precision (tests, benchmarks)
     void apply_F(const double *x_lambda, double *y_lambda, int precision);
+    void apply_F_multi(const double *x, double *y, int nrhs, int precision);
     // average device time of `reps` F applies (inputs resident), returns ms
     double time_F(int precision, int reps);
     double fapply_bytes(int precision) const;

@@ -37,7 +37,7 @@ EXPORTED = [
     "FETI4IGetLastError", "FETI4ISetSubdomainPartition", "FETI4IAddElements", "FETI4ISetExtendedOption",
     "FETI4IGetStats", "FETI4IGetDualSolution", "FETI4IGetSubdomainInfo", "FETI4IGetSubdomainMultipliers",
     "FETI4IGetSubdomainNodes", "FETI4IGetSubdomainSchur", "FETI4IGetSubdomainKernel", "FETI4IGetDualRhs",
-    "FETI4IApplySubdomainKplus", "FETI4IApplyDualOperator", "FETI4ITimeDualOperator", "FETI4ISolveResident", "FETI4ISetSolvePrecision",
+    "FETI4IApplySubdomainKplus", "FETI4IApplyDualOperator", "FETI4IApplyDualOperatorMulti", "FETI4ITimeDualOperator", "FETI4ISolveResident", "FETI4ISetSolvePrecision",
     "FETI4ITiledSymvNoAlloc", "FETI4IElementEnergies", "FETI4IGetTuning", "FETI4ISolveMulti",
     "FETI4ISolveMultiResident", "FETI4ISetClusterPartition", "FETI4IGetSubdomainCorners", "FETI4IGetClusterInfo",
 ]
@@ -87,6 +87,7 @@ def load(path: str = LIB_PATH):
         "FETI4IGetDualRhs": ([vp, pd, pd], None),
         "FETI4IApplySubdomainKplus": ([vp, i32, pd], None),
         "FETI4IApplyDualOperator": ([vp, i32, pd, pd], None),
+        "FETI4IApplyDualOperatorMulti": ([vp, i32, i32, pd, pd], None),
         "FETI4ITimeDualOperator": ([vp, i32, i32], f64),
         "FETI4ISolveResident": ([vp], f64),
         "FETI4ISetSolvePrecision": ([vp, i32], None),
@@ -345,6 +346,14 @@ class Instance:
         self.lib.FETI4IApplyDualOperator(self.h, int(precision), _dp(x), _dp(y))
         _check(self.lib)
         return y
+
+    def apply_F_multi(self, X, precision=FP64):
+        """F applied to the rows of X (nrhs x dual size) by the multi right-hand-side SYMM path."""
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        Y = np.zeros_like(X)
+        self.lib.FETI4IApplyDualOperatorMulti(self.h, int(precision), int(X.shape[0]), _dp(X), _dp(Y))
+        _check(self.lib)
+        return Y
 
     def time_F(self, precision=FP64, reps=10):
         ms = self.lib.FETI4ITimeDualOperator(self.h, int(precision), int(reps))

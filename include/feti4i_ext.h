@@ -126,6 +126,10 @@ void FETI4IGetDualRhs(FETI4IInstance instance, FETI4IReal *b, FETI4IReal *e);
 
 /* y = F x on the GPU with the Schur complements in the given precision (0/1/2). */
 void FETI4IApplyDualOperator(FETI4IInstance instance, FETI4IInt precision, FETI4IReal *x, FETI4IReal *y);
+/* y_j = F x_j for nrhs <= 32 dual vectors (vector j at j * dual size) through the multi right-hand-side
+   F apply of FETI4ISolveMulti (tile SYMM in the given Schur precision; introspection) */
+void FETI4IApplyDualOperatorMulti(FETI4IInstance instance, FETI4IInt precision, FETI4IInt nrhs, FETI4IReal *x,
+                                  FETI4IReal *y);
 /* Average device time in ms of one F apply over `reps` launches (inputs resident). */
 FETI4IReal FETI4ITimeDualOperator(FETI4IInstance instance, FETI4IInt precision, FETI4IInt reps);
 /* Several load cases at once (SURVEY of the reference: no multi-RHS path): nrhs right-hand

@@ -35,14 +35,21 @@ def direct(P, f):
                                                          ("elast", F.FP32, 8, F.PREC_LUMPED, 1),
                                                          ("heat", F.FP32, 32, F.PREC_LUMPED, 0),
                                                          ("heat", F.FP32, 32, F.PREC_LUMPED, 1),
+                                                         # Schur complements of 12-16 tiles: every block
+                                                         # kind of the 32-column tensor-core SYMM
+                                                         ("heat_big", F.FP32, 32, F.PREC_LUMPED, 1),
                                                          ("heat", F.FP32, 13, F.PREC_WEIGHT, 1),
                                                          ("heat", F.FP64, 3, F.PREC_NONE, 0),
                                                          ("elast", F.FP32, 8, F.PREC_DIRICHLET, 1),
                                                          ("heat", F.FP64, 6, F.PREC_DIRICHLET, 0)])
 def test_multi_rhs_matches_single_and_direct(kind, schur, nrhs, prec, tensor):
     """tensor=1: FP32 SYMM on the tensor cores (tcgen05, 3xTF32) inside FP64 residual replacement."""
-    P = (problems.elasticity_cube(domains=(3, 2, 2), elements=(3, 3, 3)) if kind == "elast"
-         else problems.heat_cube(domains=(3, 3, 2), elements=(4, 4, 4), seed=2))
+    if kind == "elast":
+        P = problems.elasticity_cube(domains=(3, 2, 2), elements=(3, 3, 3))
+    elif kind == "heat_big":
+        P = problems.heat_cube(domains=(2, 2, 2), elements=(10, 10, 10), seed=3)
+    else:
+        P = problems.heat_cube(domains=(3, 3, 2), elements=(4, 4, 4), seed=2)
     inst = problems.make_instance(P, iopts={F.PRECONDITIONER: prec, F.VERBOSE_LEVEL: 0, F.MAX_ITERATIONS: 3000},
                                   ropts={F.PRECISION: 1e-10},
                                   ext={F.EXT_SCHUR_PRECISION: schur, F.EXT_SYMM_TENSOR: tensor})
