@@ -1044,6 +1044,7 @@ struct KplusDev {
     const int *cbase;
     const int *cptr;
     const int *rows;
+    const long long *tpre;   // 32-blocks of the subdomains before d (vectors of kplus_mma_kernel in global memory)
 };
 
 // nz[t] = 1 when tile t holds a nonzero (one warp per tile)
@@ -1295,12 +1296,12 @@ __device__ __forceinline__ void dmma84(double (&c)[2], double a, double b) {
                  : "d"(a), "d"(b));
 }
 
-template <int NC>
+template <int NC, bool GL>
 __global__ void __launch_bounds__(256, 1) kplus_mma_kernel(KplusDev K, const double *in, double *out, int mode,
-                                                           int j0, long long stride, double *z) {
+                                                           int j0, long long stride, double *z, double *gvec) {
     static_assert(NC == 8 || NC == 16, "K+ MMA kernel: 8 or 16 columns");
     constexpr int NB = NC / 8;
-    extern __shared__ double vm[];                 // [NC][NP + KPM_PAD]
+    extern __shared__ double vm_s[];               // [NC][NP + KPM_PAD]
     __shared__ double part[8][4 * NB * 2 * 32];    // backward partials per warp, fragment order
     const int d = blockIdx.x;
     const int n = K.n[d], T = K.tn[d], o = K.doff[d];
@@ -1311,6 +1312,9 @@ __global__ void __launch_bounds__(256, 1) kplus_mma_kernel(KplusDev K, const dou
     const double *L = K.L + (size_t)K.tile0[d] * TILE * TILE;
     const int *cp = K.cptr + K.cbase[d];
     const int jt = mode == KPLUS_FULL ? 0 : K.jt[d];
+    // GL: the vectors of subdomains too large for shared memory live in a global (L2-resident)
+    // scratch, NC (32 T_d + KPM_PAD) doubles per subdomain; the block barriers order them as well
+    double *vm = GL ? gvec + (size_t)NC * ((size_t)TILE * K.tpre[d] + (size_t)KPM_PAD * d) : vm_s;
     for (int i = threadIdx.x; i < NC * NPp; i += blockDim.x) vm[i] = 0.0;
     __syncthreads();
     for (int c = 0; c < NC; ++c)
@@ -1716,6 +1720,9 @@ struct GpuSolver::Impl {
     // device K^+ and the right-hand-side / primal vectors
     KplusDev KP{};
     long long kplus_tiles_kept = 0, kplus_tiles_total = 0;   // factor tiles applied / stored
+    long long kp_tsum = 0;                                    // 32-blocks of all subdomains
+    double *kp_gvec = nullptr;                                // kplus_mma_kernel<NC, true> vectors
+    size_t kp_gvec_n = 0;
     int max_T = 0, ntot = 0, n_caller = 0;
     int *d_doff = nullptr, *d_rofs = nullptr, *d_gdof = nullptr, *d_rdof = nullptr, *d_tdof_g = nullptr;
     double *d_invm = nullptr, *d_R = nullptr, *d_rsign = nullptr, *d_rc = nullptr;
@@ -1854,10 +1861,25 @@ void GpuSolver::Impl::launch_kplus_multi(const double *in, double *out, int ncol
         // partial sums
         const size_t sm_mma = sizeof(double) * (size_t)nc * ((size_t)TILE * max_T + KPM_PAD);
         if (kplus_mma_enabled() && (nc == 16 || nc == 8) && sm_mma <= kplus_mma_smem(nc)) {
-            if (nc == 16) kplus_mma_kernel<16><<<P.nd, 256, sm_mma, stream>>>(KP, in, out, mode, j0, ntot, z);
-            else kplus_mma_kernel<8><<<P.nd, 256, sm_mma, stream>>>(KP, in, out, mode, j0, ntot, z);
+            if (nc == 16) kplus_mma_kernel<16, false><<<P.nd, 256, sm_mma, stream>>>(KP, in, out, mode, j0, ntot, z, nullptr);
+            else kplus_mma_kernel<8, false><<<P.nd, 256, sm_mma, stream>>>(KP, in, out, mode, j0, ntot, z, nullptr);
             CUDA_CHECK(cudaGetLastError());
             j0 += nc;
+            continue;
+        }
+        if (kplus_mma_enabled() && left >= 8) {
+            // subdomains too large for the vectors in shared memory: 16 (or 8) columns with the
+            // vectors in a global scratch instead of 2-4 columns per pass
+            const int ncg = left >= 16 ? 16 : 8;
+            const size_t need = (size_t)ncg * ((size_t)TILE * kp_tsum + (size_t)KPM_PAD * P.nd);
+            if (kp_gvec_n < need) {
+                kp_gvec = alloc<double>(need);
+                kp_gvec_n = need;
+            }
+            if (ncg == 16) kplus_mma_kernel<16, true><<<P.nd, 256, 0, stream>>>(KP, in, out, mode, j0, ntot, z, kp_gvec);
+            else kplus_mma_kernel<8, true><<<P.nd, 256, 0, stream>>>(KP, in, out, mode, j0, ntot, z, kp_gvec);
+            CUDA_CHECK(cudaGetLastError());
+            j0 += ncg;
             continue;
         }
         switch (nc) {
@@ -2001,6 +2023,10 @@ void GpuSolver::Impl::upload_kplus(const Decomposition &dec, const Prep &prep, c
         KP.cbase = upload(cbase);
         KP.cptr = upload(cptr);
         KP.rows = upload(rows);
+        std::vector<long long> tpre(nd + 1, 0);
+        for (int d = 0; d < nd; ++d) tpre[d + 1] = tpre[d] + tn[d];
+        KP.tpre = upload(tpre);
+        kp_tsum = tpre[nd];
         kplus_tiles_kept = kept;
         kplus_tiles_total = ntiles;
     }
@@ -2031,8 +2057,10 @@ void GpuSolver::Impl::upload_kplus(const Decomposition &dec, const Prep &prep, c
     CUDA_CHECK(cudaFuncSetAttribute(kplus_multi_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kplus_multi_smem(4)));
     CUDA_CHECK(cudaFuncSetAttribute(kplus_multi_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kplus_multi_smem(2)));
     CUDA_CHECK(cudaFuncSetAttribute(kplus_multi_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kplus_multi_smem(1)));
-    CUDA_CHECK(cudaFuncSetAttribute(kplus_mma_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kplus_mma_smem(16)));
-    CUDA_CHECK(cudaFuncSetAttribute(kplus_mma_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kplus_mma_smem(8)));
+    CUDA_CHECK(cudaFuncSetAttribute(kplus_mma_kernel<16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kplus_mma_smem(16)));
+    CUDA_CHECK(cudaFuncSetAttribute(kplus_mma_kernel<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kplus_mma_smem(8)));
 }
 
 void GpuSolver::Impl::upload_hybrid(const Decomposition &dec, const Prep &prep) {

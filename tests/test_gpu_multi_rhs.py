@@ -38,6 +38,9 @@ def direct(P, f):
                                                          # Schur complements of 12-16 tiles: every block
                                                          # kind of the 32-column tensor-core SYMM
                                                          ("heat_big", F.FP32, 32, F.PREC_LUMPED, 1),
+                                                         # subdomains of 3,993 DOFs: the multi-column K+
+                                                         # keeps its vectors in global memory
+                                                         ("elast_big", F.FP32, 16, F.PREC_LUMPED, 0),
                                                          ("heat", F.FP32, 13, F.PREC_WEIGHT, 1),
                                                          ("heat", F.FP64, 3, F.PREC_NONE, 0),
                                                          ("elast", F.FP32, 8, F.PREC_DIRICHLET, 1),
@@ -46,6 +49,8 @@ def test_multi_rhs_matches_single_and_direct(kind, schur, nrhs, prec, tensor):
     """tensor=1: FP32 SYMM on the tensor cores (tcgen05, 3xTF32) inside FP64 residual replacement."""
     if kind == "elast":
         P = problems.elasticity_cube(domains=(3, 2, 2), elements=(3, 3, 3))
+    elif kind == "elast_big":
+        P = problems.elasticity_cube(domains=(2, 1, 1), elements=(10, 10, 10))
     elif kind == "heat_big":
         P = problems.heat_cube(domains=(2, 2, 2), elements=(10, 10, 10), seed=3)
     else:
