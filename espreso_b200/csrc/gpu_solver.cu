@@ -1345,22 +1345,36 @@ __global__ void __launch_bounds__(256, 1) kplus_mma_kernel(KplusDev K, const dou
         __syncthreads();
     };
 
+    // Factor fragments come straight from global memory in fragment order; a warp's next tile is
+    // loaded while the MMAs of its current one run, and its first tile of the next block column
+    // before the barriers and the diagonal step of that column.
+    auto fload = [&](int J, int qx, double (&a)[4][8]) {
+        const double *tile = L + (size_t)ltile(T, K.rows[qx], J) * TILE * TILE + gr * TILE + gc;
+#pragma unroll
+        for (int mb = 0; mb < 4; ++mb)
+#pragma unroll
+            for (int ks = 0; ks < 8; ++ks) a[mb][ks] = __ldg(tile + 8 * mb * TILE + 4 * ks);
+    };
+    auto bload = [&](int J, int qx, double (&a)[4][8]) {   // A = L_IJ^T: A[m][k] = L_IJ[k][m]
+        const double *tile = L + (size_t)ltile(T, K.rows[qx], J) * TILE * TILE + gc * TILE + gr;
+#pragma unroll
+        for (int mb = 0; mb < 4; ++mb)
+#pragma unroll
+            for (int ks = 0; ks < 8; ++ks) a[mb][ks] = __ldg(tile + 4 * ks * TILE + 8 * mb);
+    };
+    double a0[4][8], a1[4][8];
     // forward: L y = f
-    for (int J = (mode == KPLUS_PRIMAL ? jt : 0); J < T; ++J) {
+    const int jf = mode == KPLUS_PRIMAL ? jt : 0;
+    if (jf < T && cp[jf] + 1 + warp < cp[jf + 1]) fload(jf, cp[jf] + 1 + warp, a0);
+    for (int J = jf; J < T; ++J) {
         diag(J, false);
         double bf[8][NB];
 #pragma unroll
         for (int ks = 0; ks < 8; ++ks)
 #pragma unroll
             for (int nb = 0; nb < NB; ++nb) bf[ks][nb] = vm[(size_t)(8 * nb + gr) * NPp + TILE * J + 4 * ks + gc];
-        for (int qi = cp[J] + 1 + warp; qi < cp[J + 1]; qi += 8) {
-            const int I = K.rows[qi];
-            const double *tile = L + (size_t)ltile(T, I, J) * TILE * TILE + gr * TILE + gc;
-            double af[4][8];
-#pragma unroll
-            for (int mb = 0; mb < 4; ++mb)
-#pragma unroll
-                for (int ks = 0; ks < 8; ++ks) af[mb][ks] = __ldg(tile + 8 * mb * TILE + 4 * ks);
+        auto fproc = [&](int qx, const double (&af)[4][8]) {
+            const int I = K.rows[qx];
             double acc[4][NB][2];
 #pragma unroll
             for (int mb = 0; mb < 4; ++mb)
@@ -1379,7 +1393,16 @@ __global__ void __launch_bounds__(256, 1) kplus_mma_kernel(KplusDev K, const dou
                     cc[0] -= acc[mb][nb][0];
                     cc[NPp] -= acc[mb][nb][1];
                 }
+        };
+        const int qe = cp[J + 1];
+        for (int qi = cp[J] + 1 + warp; qi < qe; qi += 16) {
+            if (qi + 8 < qe) fload(J, qi + 8, a1);
+            fproc(qi, a0);
+            if (qi + 8 >= qe) break;
+            if (qi + 16 < qe) fload(J, qi + 16, a0);
+            fproc(qi + 8, a1);
         }
+        if (J + 1 < T && cp[J + 1] + 1 + warp < cp[J + 2]) fload(J + 1, cp[J + 1] + 1 + warp, a0);
         __syncthreads();
     }
     if (mode == KPLUS_TOUCHED) {
@@ -1392,21 +1415,17 @@ __global__ void __launch_bounds__(256, 1) kplus_mma_kernel(KplusDev K, const dou
         __syncthreads();
     }
     // backward: L^T x = y (mode 1: down to block jt)
-    for (int J = T - 1; J >= (mode == KPLUS_TOUCHED ? jt : 0); --J) {
+    const int jb = mode == KPLUS_TOUCHED ? jt : 0;
+    if (T - 1 >= jb && cp[T - 1] + 1 + warp < cp[T]) bload(T - 1, cp[T - 1] + 1 + warp, a0);
+    for (int J = T - 1; J >= jb; --J) {
         double acc[4][NB][2];
 #pragma unroll
         for (int mb = 0; mb < 4; ++mb)
 #pragma unroll
             for (int nb = 0; nb < NB; ++nb) acc[mb][nb][0] = acc[mb][nb][1] = 0.0;
-        for (int qi = cp[J] + 1 + warp; qi < cp[J + 1]; qi += 8) {
-            const int I = K.rows[qi];
-            // A = L_IJ^T: A[m][k] = L_IJ[k][m]
-            const double *tile = L + (size_t)ltile(T, I, J) * TILE * TILE + gc * TILE + gr;
-            double af[4][8], bf[8][NB];
-#pragma unroll
-            for (int mb = 0; mb < 4; ++mb)
-#pragma unroll
-                for (int ks = 0; ks < 8; ++ks) af[mb][ks] = __ldg(tile + 4 * ks * TILE + 8 * mb);
+        auto bproc = [&](int qx, const double (&af)[4][8]) {
+            const int I = K.rows[qx];
+            double bf[8][NB];
 #pragma unroll
             for (int ks = 0; ks < 8; ++ks)
 #pragma unroll
@@ -1417,7 +1436,16 @@ __global__ void __launch_bounds__(256, 1) kplus_mma_kernel(KplusDev K, const dou
                 for (int nb = 0; nb < NB; ++nb)
 #pragma unroll
                     for (int ks = 0; ks < 8; ++ks) dmma84(acc[mb][nb], af[mb][ks], bf[ks][nb]);
+        };
+        const int qe = cp[J + 1];
+        for (int qi = cp[J] + 1 + warp; qi < qe; qi += 16) {
+            if (qi + 8 < qe) bload(J, qi + 8, a1);
+            bproc(qi, a0);
+            if (qi + 8 >= qe) break;
+            if (qi + 16 < qe) bload(J, qi + 16, a0);
+            bproc(qi + 8, a1);
         }
+        if (J - 1 >= jb && cp[J - 1] + 1 + warp < cp[J]) bload(J - 1, cp[J - 1] + 1 + warp, a0);
 #pragma unroll
         for (int mb = 0; mb < 4; ++mb)
 #pragma unroll
