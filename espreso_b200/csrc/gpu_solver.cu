@@ -3463,45 +3463,41 @@ __device__ __forceinline__ bool col_frozen(const BlockDev &B, int j, int iter) {
     return c == -2 || (c >= 0 && iter > c);
 }
 
-// out (nK x nr) = (GG^T)^-1 in: a CTA owns CR rows; 32-row blocks of `in` are staged in
-// shared memory and every thread keeps CR/8 rows of one column
-constexpr int CR = 16;
+// out (nK x nr) = (GG^T)^-1 in: a CTA owns CR rows; warp w takes one eighth of the inner dimension
+// for those rows (lane = column, independent loads in flight), and the eight partial sums meet
+// in shared memory in warp order
+constexpr int CR = 4;
 __global__ void __launch_bounds__(256) bcoarse_kernel(DevProblem P, BlockDev B, const double *in, double *out, int slot,
                                                       int looped) {
     pdl_enter();
     if (looped && skip_iter(P.st, P.st->iter_base + slot)) return;
-    __shared__ double xs[32][33];
-    __shared__ double ms[CR][33];
+    __shared__ double red[8][CR][32];
     const int nr = B.nr, nK = P.nK, nP = P.nP;
     const int r0 = blockIdx.x * CR;
-    const int j = threadIdx.x & 31, rg = threadIdx.x >> 5;   // column, row group (8 groups)
-    double acc[CR / 8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int per = (nP + 7) / 8, b_lo = w * per, b_hi = min(nP, b_lo + per);
+    const bool col = lane < nr;
+    double acc[CR];
 #pragma unroll
-    for (int q = 0; q < CR / 8; ++q) acc[q] = 0.0;
-    for (int b0 = 0; b0 < nP; b0 += 32) {
-        for (int t = threadIdx.x; t < 32 * 32; t += blockDim.x) {
-            const int b = t >> 5, c = t & 31;
-            xs[b][c] = (b0 + b < nP && c < nr) ? in[(size_t)(b0 + b) * nr + c] : 0.0;
-        }
-        for (int t = threadIdx.x; t < CR * 32; t += blockDim.x) {
-            const int r = t >> 5, c = t & 31;
-            ms[r][c] = (r0 + r < nK && b0 + c < nP) ? P.GGtinv[(size_t)(r0 + r) * nP + b0 + c] : 0.0;
-        }
-        __syncthreads();
+    for (int r = 0; r < CR; ++r) acc[r] = 0.0;
+    const double *g[CR];
 #pragma unroll
-        for (int q = 0; q < CR / 8; ++q) {
-            const int r = rg + 8 * q;
-            double sum = 0.0;
+    for (int r = 0; r < CR; ++r) g[r] = P.GGtinv + (size_t)min(r0 + r, nK - 1) * nP;
 #pragma unroll 8
-            for (int b = 0; b < 32; ++b) sum += ms[r][b] * xs[b][j];
-            acc[q] += sum;
-        }
-        __syncthreads();
+    for (int b = b_lo; b < b_hi; ++b) {
+        const double x = col ? in[(size_t)b * nr + lane] : 0.0;
+#pragma unroll
+        for (int r = 0; r < CR; ++r) acc[r] += g[r][b] * x;
     }
 #pragma unroll
-    for (int q = 0; q < CR / 8; ++q) {
-        const int r = r0 + rg + 8 * q;
-        if (r < nK && j < nr) out[(size_t)r * nr + j] = acc[q];
+    for (int r = 0; r < CR; ++r) red[w][r][lane] = acc[r];
+    __syncthreads();
+    if (threadIdx.x < CR * 32) {
+        const int r = threadIdx.x >> 5;
+        double sum = 0.0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) sum += red[q][r][lane];
+        if (r0 + r < nK && col) out[(size_t)(r0 + r) * nr + lane] = sum;
     }
 }
 
