@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 
 #include "common.h"
@@ -3210,8 +3211,12 @@ tile_symv_noalloc_kernel(const double *tiles, const long long *tile0, const int 
         const int m = s_m;
         if (m >= nmat) break;
         const int n = order[m];
-        if (n > max_order || n < 0) {   // violates the caller's stated bound: skip, output untouched
-            if (threadIdx.x == 0) scr->dots[m] = 0.0;
+        if (n > max_order || n < 0) {
+            // violates the caller's stated bound: no product is formed; its y range and the total
+            // dot are set to NaN so that the caller cannot mistake the result for a valid one
+            const int o = voff[m];
+            for (int i = threadIdx.x; i < n; i += blockDim.x) y[o + i] = __longlong_as_double(0x7ff8000000000000LL);
+            if (threadIdx.x == 0) scr->dots[m] = __longlong_as_double(0x7ff8000000000000LL);
             __syncthreads();
             continue;
         }
@@ -3278,16 +3283,22 @@ int tiled_symv_noalloc(const double *tiles, const long long *tile_offset, const 
     int dev = 0;
     CUDA_CHECK(cudaGetDevice(&dev));
     FETI_CHECK(dev >= 0 && dev < 256, "FETI4ITiledSymvNoAlloc: device index out of range");
-    if (!g_noalloc_ready[dev]) {
-        // first call on this device: resolve the device address of the scratch array
-        NoAllocScratch *p = nullptr;
-        cudaError_t rc = cudaGetSymbolAddress((void **)&p, g_noalloc_scratch);
-        FETI_CHECK(rc == cudaSuccess, std::string("FETI4ITiledSymvNoAlloc: cudaGetSymbolAddress failed: ") +
-                                          cudaGetErrorString(rc));
-        const int smem = (int)(2 * sizeof(double) * TILE * ((NOALLOC_MAX_ORDER + TILE - 1) / TILE));
-        CUDA_CHECK(cudaFuncSetAttribute(tile_symv_noalloc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        g_noalloc_ptr[dev] = p;
-        g_noalloc_ready[dev] = true;
+    {
+        // first call on this device: resolve the device address of the scratch array (under a lock, so
+        // that host threads making their first calls together do the set-up once)
+        static std::mutex setup_mutex;
+        std::lock_guard<std::mutex> lock(setup_mutex);
+        if (!g_noalloc_ready[dev]) {
+            NoAllocScratch *p = nullptr;
+            cudaError_t rc = cudaGetSymbolAddress((void **)&p, g_noalloc_scratch);
+            FETI_CHECK(rc == cudaSuccess, std::string("FETI4ITiledSymvNoAlloc: cudaGetSymbolAddress failed: ") +
+                                              cudaGetErrorString(rc));
+            const int smem = (int)(2 * sizeof(double) * TILE * ((NOALLOC_MAX_ORDER + TILE - 1) / TILE));
+            CUDA_CHECK(
+                cudaFuncSetAttribute(tile_symv_noalloc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            g_noalloc_ptr[dev] = p;
+            g_noalloc_ready[dev] = true;
+        }
     }
     cudaStream_t s = (cudaStream_t)stream;
     NoAllocScratch *scr = g_noalloc_ptr[dev];

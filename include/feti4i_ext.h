@@ -132,7 +132,7 @@ void FETI4IApplyDualOperatorMulti(FETI4IInstance instance, FETI4IInt precision, 
                                   FETI4IReal *y);
 /* Average device time in ms of one F apply over `reps` launches (inputs resident). */
 FETI4IReal FETI4ITimeDualOperator(FETI4IInstance instance, FETI4IInt precision, FETI4IInt reps);
-/* Several load cases at once (SURVEY of the reference: no multi-RHS path): nrhs right-hand
+/* Several load cases at once (the reference has no multi-RHS path): nrhs right-hand
  * sides (1..32) in rhs[j * size + i] are solved together by a block PCG whose F apply is a
  * tile SYMM; solutions[j * size + i].  LUMPED, WEIGHT_FUNCTION or no preconditioner. */
 void FETI4ISolveMulti(FETI4IInstance instance, FETI4IInt nrhs, FETI4IInt size, const FETI4IReal *rhs,
@@ -166,7 +166,8 @@ void FETI4IElementEnergies(FETI4IInstance instance, FETI4IInt size, const FETI4I
  * padding beyond the order.  x and y use vector_offset[m].  If `dot` is not
  * NULL the total x.y lands there (device memory).  Limits: nmatrices <= 16384
  * and max_order <= 3200; larger values are rejected with an error (return -1,
- * message in FETI4IGetLastError); matrices above max_order are skipped.  The
+ * message in FETI4IGetLastError).  A matrix whose order exceeds max_order (or is
+ * negative) gets no product: its y range is filled with NaN and *dot is NaN.  The
  * scratch (work-queue counters, one dot partial per matrix) is a static array
  * in device memory, held by every GPU that loads the library until exit; the
  * first call on a device looks up its address, so that call should come before

@@ -5,7 +5,7 @@ reference checkout (``benchmarks/**``) and stores the numbers, the case
 geometry and the monitor definitions as a small JSON fixture, so that the
 tests never need the reference tree at run time.
 
-    python tests/golden/make_emr_fixtures.py /root/reference
+    python tests/golden/make_emr_fixtures.py <path of the reference checkout>
 """
 import json
 import os
@@ -66,4 +66,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_emr_fixtures.py <path of the reference checkout>")
+    main(sys.argv[1])

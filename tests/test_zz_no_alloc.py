@@ -54,6 +54,20 @@ def test_tiled_symv_no_alloc_matches_dual_operator():
         ref = inst.apply_F(x, F.FP64)
         assert np.linalg.norm(y - ref) <= 1e-13 * np.linalg.norm(ref), call
         assert abs(t_dot.item() - float(xL @ yL)) <= 1e-12 * abs(float(xL @ yL))
+    # a caller that understates max_order gets no product for the larger matrices: NaN in their y
+    # range and in the dot, the others as before
+    lo = int(order.min()) if order.max() > order.min() else int(order.min()) - 1
+    F.tiled_symv_noalloc(t_tiles.data_ptr(), t_toff.data_ptr(), t_order.data_ptr(), t_voff.data_ptr(), nd, lo,
+                         t_x.data_ptr(), t_y.data_ptr(), t_dot.data_ptr(), 0)
+    torch.cuda.synchronize()
+    yS = t_y.cpu().numpy()
+    assert np.isnan(t_dot.item())
+    for d in range(nd):
+        seg = slice(voff[d], voff[d] + order[d])
+        if order[d] > lo:
+            assert np.all(np.isnan(yS[seg])), d
+        else:
+            assert np.allclose(yS[seg], yL[seg], rtol=1e-13, atol=1e-13 * np.abs(yL).max()), d
     with pytest.raises(F.FETI4IError, match="nmatrices"):
         F.tiled_symv_noalloc(t_tiles.data_ptr(), t_toff.data_ptr(), t_order.data_ptr(), t_voff.data_ptr(),
                              16385, int(order.max()), t_x.data_ptr(), t_y.data_ptr(), 0, 0)
