@@ -6,9 +6,11 @@ unit source; lumped preconditioner; Schur complements stored in FP32 inside FP64
 residual replacement (reliable updates); dual PCG to precision 1e-8.
 
 One step = one dual PCG solve on device-resident data (FETI4ISolveResident).
-``e2e`` = one FETI4ISolve call with host buffers (host b/e vectors, H2D, PCG,
-D2H, host primal recovery).  ``roofline`` is the tile SYMV (F apply) kernel:
-algorithmic bytes per launch / CUDA-event launch time on the library stream.
+``e2e`` = one FETI4ISolve call with host buffers (H2D right-hand side, device K+ f,
+b, e, PCG, device primal recovery, D2H solution).  ``roofline`` is the tile SYMV
+(F apply) kernel: algorithmic bytes per launch / CUDA-event launch time on the
+library stream.  ``parity`` states the error of every solution the line times
+against the oracle's FP64 solve and the primal residual on the assembled system.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -20,7 +22,6 @@ import os
 import statistics
 import subprocess
 import sys
-import threading
 import time
 
 import numpy as np
@@ -48,7 +49,7 @@ def parse():
     ap.add_argument("--nrhs", type=int, default=32, help="load cases of the batched (multi-RHS) leg, 0 to skip")
     ap.add_argument("--method", type=int, default=0, choices=[0, 1],
                     help="FETI_METHOD: 0 Total FETI, 1 Hybrid Total FETI on the config's clusters")
-    ap.add_argument("--loads", default="scaled", choices=["scaled", "traction"],
+    ap.add_argument("--loads", default="traction", choices=["scaled", "traction"],
                     help="batched leg load cases: scaled copies of the config load, or seeded N(0,1e6) "
                          "nodal tractions on the x=1 face")
     ap.add_argument("--symm-tensor", type=int, default=1, choices=[0, 1],
@@ -155,64 +156,58 @@ def dist_barrier(dist):
         dist.barrier()
 
 
-def cpu_reference_solver(cfg_name, precond):
-    """The oracle restatement of ESPRESO's FP64 dual PCG on the host cores."""
-    from espreso_b200 import problems
+def oracle_problem(P, precond):
+    """The oracle (numpy restatement of ESPRESO's Total FETI) on the same mesh, and its dual PCG
+    packed for the OpenMP C++ iteration (oracle/cpu_pcg.cpp) on all host cores."""
+    from oracle import cpu as OC
     from oracle import feti as OF
     from oracle import numbering as ON
-    P = problems.build_config(cfg_name)
     num = ON.Numbering(P.elem_nodes, P.elem_domain, P.n_nodes, P.dpn, P.dirichlet)
     OP = OF.FETIProblem(num, P.elem_nodes, P.elem_domain, P.Ke, P.fe, P.coords,
-                        build_dirichlet=(precond == OF.PREC_DIRICHLET))
-    return OP
+                        build_dirichlet=precond in (OF.PREC_DIRICHLET, OF.PREC_SUPER_DIRICHLET))
+    return OP, OC.CpuPCG(OP, precond, threads=os.cpu_count() or 1)
 
 
-def threaded_apply_F(OP, nthreads):
-    """F apply of the oracle with subdomains spread over host threads (numpy releases the GIL)."""
-    from concurrent.futures import ThreadPoolExecutor
-    pool = ThreadPoolExecutor(nthreads)
-
-    def apply(x):
-        parts = list(pool.map(lambda s: s.S @ x[s.lam], OP.sub))
-        y = np.zeros(OP.n_lambda)
-        for s, yi in zip(OP.sub, parts):
-            np.add.at(y, s.lam, yi)
-        return y
-    return apply
-
-
-def time_cpu_iterations(OP, precond, iters, nthreads, precision):
-    """Time a bounded sample of PCG iterations of the oracle (threaded F apply)."""
-    OP.apply_F = (lambda f: (lambda x, precision="f64": f(x)))(threaded_apply_F(OP, nthreads))
-    t0 = time.perf_counter()
-    OP.solve(precision=precision, max_it=iters, prec=precond)
-    return (time.perf_counter() - t0) / max(1, OP.iterations)
+def oracle_u(OP, C, P, precision, f=None):
+    """Displacements of the oracle's FP64 solve (global load ``f``, default the mesh's own)."""
+    if f is not None:
+        OP.set_rhs(f)
+    lam, alpha = C.solve(precision=precision, max_it=5000)
+    return OP.merge(OP.primal(lam, alpha), P.n_nodes).ravel()
 
 
 def run_reference(args):
+    """The reference arm: the oracle restatement of ESPRESO's FP64 CPU dual solve, timed as whole
+    solves (b, e -> lambda, alpha: every PCG iteration, projector and preconditioner) over all host
+    cores.  The preprocessing (factorisations, S_i, G, GG^T) is built once, untimed."""
     rank, world, local, dist = dist_init(args)
     if rank != 0:
         return
-    from threadpoolctl import threadpool_limits
+    from espreso_b200 import problems
     ncores = os.cpu_count() or 1
-    with threadpool_limits(1):
-        OP = cpu_reference_solver(args.config, args.precond)
-        # iteration count of the full solve (untimed), then bounded timed samples
-        hist = []
-        OP.solve(precision=args.precision, max_it=5000, prec=args.precond, history=hist)
-        n_it = OP.iterations
-        for _ in range(args.warmup):
-            time_cpu_iterations(OP, args.precond, 2, ncores, args.precision)
-        per_it = [time_cpu_iterations(OP, args.precond, 5, ncores, args.precision) for _ in range(args.steps)]
-    ms = 1e3 * statistics.median(per_it) * n_it
+    P = problems.build_config(args.config)
+    t0 = time.perf_counter()
+    OP, C = oracle_problem(P, args.precond)
+    setup_s = time.perf_counter() - t0
+    b, e = OP.vec_b(), OP.vec_e()
+    for _ in range(args.warmup):
+        C.solve(b, e, precision=args.precision, max_it=5000)
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        C.solve(b, e, precision=args.precision, max_it=5000)
+        times.append((time.perf_counter() - t) * 1e3)
+    ms = float(np.median(times))
     line = {"metric": METRIC, "value": ms, "unit": "ms", "impl": "reference", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": args.config, "precond": args.precond, "precision": args.precision,
-                       "pcg_iterations": n_it},
+                       "pcg_iterations": C.iterations, "setup_s": setup_s,
+                       "converged": bool(C.final_norm < C.tol)},
             "cpu_baseline": {"value": ms, "unit": "ms", "cores": ncores, "kind": "port",
-                             "sample": f"5 PCG iterations per step x {n_it} iterations of the full FP64 solve "
-                                       f"(oracle restatement, subdomain F apply over {ncores} threads)"},
+                             "sample": f"one whole FP64 dual PCG solve per step ({C.iterations} iterations: packed "
+                                       f"upper S_i SPMV, projector, preconditioner) by the OpenMP C++ restatement "
+                                       f"of the reference's CPU solver on {ncores} threads; preprocessing untimed"},
             "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -271,8 +266,14 @@ def run_ours(args):
         inst.solve(sol)
         e2e.append((time.perf_counter() - t) * 1e3)
     e2e_ms = dist_max(dist, float(np.median(e2e)))
+    u_mixed, conv_mixed = sol.copy(), bool(inst.stats()["converged"])
+    inst.set_solve_precision(0)
+    u_fp64 = inst.solve(np.zeros(P.ndofs))
+    conv_fp64 = bool(inst.stats()["converged"])
+    inst.set_solve_precision(SCHUR[args.schur])
     # batched leg: nrhs seeded load cases solved together (block PCG, tile SYMM)
     batched = None
+    R = U = U64 = None
     if args.nrhs > 0:
         rng = np.random.default_rng(1 + rank)
         if args.loads == "traction":
@@ -283,12 +284,14 @@ def run_ours(args):
         bms = [inst.solve_multi_resident(args.nrhs) for _ in range(max(1, args.steps))]
         stb = inst.stats()
         inst.set_solve_precision(0)
-        inst.solve_multi(R)
+        U64 = inst.solve_multi(R)
+        conv_b64 = bool(inst.stats()["converged"])
         b64 = inst.solve_multi_resident(args.nrhs)
         inst.set_solve_precision(SCHUR[args.schur])
         t = time.perf_counter()
-        inst.solve_multi(R)
+        U = inst.solve_multi(R)
         e2e_b = (time.perf_counter() - t) * 1e3
+        conv_b = bool(inst.stats()["converged"])
         bmed = float(np.median(bms))
         batched = {"nrhs": args.nrhs, "ms_per_batch": bmed, "ms_per_solve": bmed / args.nrhs,
                    "pcg_iterations": int(stb["iterations"]), "replacements": int(stb["replacements"]),
@@ -312,10 +315,37 @@ def run_ours(args):
             traffic = tj[key]["dram_bytes_per_launch"]
             traffic_src = tj[key]["source"]
     fp64_f = inst.time_F(0, 10)
-    # CPU baseline: oracle port on the host cores (rank 0, N=1 only)
+    # parity of every solution timed above: primal residual on the assembled system (every rank) and,
+    # on rank 0 at N=1, the error against the oracle's FP64 solve of the same mesh and loads
+    parity = {"precision": args.precision,
+              "mixed": {"residual": P.relative_residual(u_mixed, rhs), "converged": conv_mixed},
+              "fp64": {"residual": P.relative_residual(u_fp64, rhs), "converged": conv_fp64}}
+    if U is not None:
+        parity["batched"] = {"residual_max": max(P.relative_residual(U[j], R[j]) for j in range(len(R))),
+                             "converged": conv_b,
+                             "fp64_residual_max": max(P.relative_residual(U64[j], R[j]) for j in range(len(R))),
+                             "fp64_converged": conv_b64}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_from_library(inst, P, args)
+        cpu, uo, ucols = cpu_baseline_and_oracle(P, args, R)
+        rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+        parity["mixed"]["err_vs_oracle"] = rel(u_mixed, uo)
+        parity["fp64"]["err_vs_oracle"] = rel(u_fp64, uo)
+        if U is not None:
+            parity["batched"]["err_vs_oracle"] = {str(j): rel(U[j], uc) for j, uc in ucols.items()}
+            parity["batched"]["fp64_err_vs_oracle"] = {str(j): rel(U64[j], uc) for j, uc in ucols.items()}
+        parity["oracle"] = (f"oracle FP64 Total-FETI solve of the same mesh and loads (own factorisations and "
+                            f"S_i, OpenMP C++ PCG) to precision {ORACLE_PRECISION:g}; batched columns "
+                            f"{sorted(ucols)} checked")
+        errs = [parity["mixed"]["err_vs_oracle"], parity["fp64"]["err_vs_oracle"]]
+        if U is not None:
+            errs += list(parity["batched"]["err_vs_oracle"].values())
+            errs += list(parity["batched"]["fp64_err_vs_oracle"].values())
+        convs = [conv_mixed, conv_fp64] + ([conv_b, conv_b64] if U is not None else [])
+        parity["max_err_vs_oracle"] = max(errs)
+        parity["ok"] = bool(max(errs) <= args.precision and all(convs))
+        if not parity["ok"]:
+            print(f"PARITY FAILURE: max error vs oracle {max(errs):.3e}, converged {convs}", file=sys.stderr)
     clocks = clk.summary()
     launches = int(st["kernel_launches"]) * args.steps
     line = {
@@ -351,6 +381,7 @@ def run_ours(args):
                      "launch_ms": t_f, "peak_kind": peak_kind,
                      "alg_bytes_per_launch": alg},
         "cpu_baseline": cpu,
+        "parity": parity,
         "gpu_launches": launches,
         "clocks": clocks,
     }
@@ -361,42 +392,35 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def cpu_baseline_from_library(inst, P, args):
-    """Oracle FP64 PCG iterations on the host cores with the same S_i (bounded sample)."""
-    from threadpoolctl import threadpool_limits
+ORACLE_PRECISION = 1e-11
 
-    from oracle import feti as OF
-    from oracle import numbering as ON
+
+def cpu_baseline_and_oracle(P, args, R):
+    """CPU baseline and checker: the oracle's FP64 dual solve of the same mesh on all host cores.
+
+    The timed part is one whole dual PCG solve (b, e -> lambda, alpha) at the bench precision, by the
+    OpenMP C++ restatement of the reference's CPU solver (preprocessing untimed).  The same oracle
+    then solves to ORACLE_PRECISION, so that its own error is far below the one it checks, for the
+    mesh's load and for the first and last batched load case."""
     ncores = os.cpu_count() or 1
-    with threadpool_limits(1):
-        num = ON.Numbering(P.elem_nodes, P.elem_domain, P.n_nodes, P.dpn, P.dirichlet)
-        OP = OF.FETIProblem.__new__(OF.FETIProblem)
-        # light-weight oracle object on the library's operators (no oracle factorisation)
-        OP.num = num
-        OP.coords = P.coords
-        OP.n_lambda = num.n_lambda
-        OP.sub = []
-        for d in range(num.ndomains):
-            s = OF.Subdomain(K=None, f=None, R=inst.kernel(d), regmat=None, chol=None, lam=num.B[d]["lam"],
-                             dof=num.B[d]["dof"], sign=num.B[d]["sign"], c=num.B[d]["c"], w=None)
-            s.S = np.ascontiguousarray(inst.schur(d))
-            OP.sub.append(s)
-        OP._coarse()
-        apply = threaded_apply_F(OP, ncores)
-        rng = np.random.default_rng(0)
-        x = rng.standard_normal(OP.n_lambda)
-        apply(x)
-        reps = 3
-        t = time.perf_counter()
-        for _ in range(reps):
-            apply(x)
-        per_apply = (time.perf_counter() - t) / reps
-    iters = int(inst.stats()["iterations"])
-    # one PCG iteration = one F apply + projector/preconditioner work (counted as the F apply alone: lower bound)
-    ms = 1e3 * per_apply * iters
-    return {"value": ms, "unit": "ms", "cores": ncores, "kind": "port",
-            "sample": f"{reps} FP64 F applies of the oracle (subdomain S_i @ x over {ncores} threads) x "
-                      f"{iters} PCG iterations; projector and preconditioner not counted (lower bound)"}
+    t0 = time.perf_counter()
+    OP, C = oracle_problem(P, args.precond)
+    setup_s = time.perf_counter() - t0
+    b, e = OP.vec_b(), OP.vec_e()
+    t = time.perf_counter()
+    C.solve(b, e, precision=args.precision, max_it=5000)
+    ms = (time.perf_counter() - t) * 1e3
+    iters = C.iterations
+    uo = oracle_u(OP, C, P, ORACLE_PRECISION)
+    ucols = {}
+    if R is not None:
+        for j in sorted({0, len(R) - 1}):
+            ucols[j] = oracle_u(OP, C, P, ORACLE_PRECISION, f=R[j])
+    cpu = {"value": ms, "unit": "ms", "cores": ncores, "kind": "port",
+           "sample": f"one whole FP64 dual PCG solve ({iters} iterations: packed upper S_i SPMV, projector, "
+                     f"preconditioner) of the same workload by the OpenMP C++ restatement of the reference's CPU "
+                     f"solver on {ncores} threads; its preprocessing ({setup_s:.1f} s) untimed"}
+    return cpu, uo, ucols
 
 
 def run_adjoint(args):

@@ -57,6 +57,24 @@ class Problem:
         np.add.at(f, self.elem_dofs().ravel(), self.fe.ravel())
         return f
 
+    def relative_residual(self, u, f=None):
+        """||(K u - f)_free|| / ||f_free|| over the DOFs that are not Dirichlet-fixed, with the
+        assembled global stiffness K (the primal residual check of the reference's
+        src/solver/specific/itersolver.cpp:171-370, on the caller's assembled system)."""
+        import scipy.sparse as sp
+        if getattr(self, "_K", None) is None:
+            dofs = self.elem_dofs()
+            nd = dofs.shape[1]
+            rows = np.repeat(dofs, nd, axis=1).ravel()
+            cols = np.tile(dofs, (1, nd)).ravel()
+            self._K = sp.csr_matrix((self.Ke.reshape(-1), (rows, cols)), shape=(self.ndofs, self.ndofs))
+            free = np.ones(self.ndofs, dtype=bool)
+            free[self.dirichlet_dofs()[0]] = False
+            self._free = free
+        f = self.rhs() if f is None else np.asarray(f)
+        r = (self._K @ np.asarray(u).ravel() - f)[self._free]
+        return float(np.linalg.norm(r) / np.linalg.norm(f[self._free]))
+
     def dirichlet_dofs(self):
         dofs, vals = [], []
         for c, (nodes, v) in sorted(self.dirichlet.items()):

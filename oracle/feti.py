@@ -14,6 +14,8 @@ import scipy.sparse as sp
 from .numbering import Numbering
 
 PREC_NONE, PREC_LUMPED, PREC_WEIGHT, PREC_DIRICHLET = 0, 1, 2, 3
+# src/config/ecf/solver/feti.h:45-47
+PREC_SUPER_DIRICHLET, PREC_MAGIC = 4, 5
 
 
 @dataclass
@@ -30,6 +32,7 @@ class Subdomain:
     w: np.ndarray               # B1 scale (duplicity) per local row
     S: np.ndarray = None        # B K+ B^T (n_i x n_i)
     Sdir: np.ndarray = None     # Dirichlet preconditioner on sorted touched DOFs
+    Ssd: sp.csr_matrix = None   # SUPER_DIRICHLET preconditioner on the same DOFs
     tdofs: np.ndarray = None    # sorted touched DOFs
     trow: np.ndarray = None     # local row -> index into tdofs
     extra: dict = field(default_factory=dict)
@@ -120,6 +123,22 @@ def dirichlet_schur(K, tdofs):
     return Kbb - Kib.T @ sla.cho_solve(sla.cho_factor(Kii), Kib)
 
 
+def super_dirichlet_schur(K, tdofs):
+    """SUPER_DIRICHLET preconditioner: S_sd = K_ss - K_sr diag(K_rr)^-1 K_rs on the touched DOFs s,
+    with r the remaining DOFs (src/solver/specific/cpu/clustercpu.cpp:254-311, branch
+    diagonalized_K_rr: K_rs scaled by 1/diag(K_rr) in place of K_rr^-1).  K is the unregularised
+    stiffness (K_modif = K_reg - RegMat, :191-192).  Symmetric, sparse."""
+    n = K.shape[0]
+    inner = np.setdiff1d(np.arange(n), tdofs)
+    K = sp.csr_matrix(K)
+    Kss = K[tdofs][:, tdofs]
+    if inner.size == 0:
+        return sp.csr_matrix(Kss)
+    Krs = K[inner][:, tdofs]
+    dinv = 1.0 / K.diagonal()[inner]
+    return sp.csr_matrix(Kss - Krs.T @ sp.diags(dinv) @ Krs)
+
+
 class FETIProblem:
     """Total-FETI problem built the reference's way on a single cluster."""
 
@@ -140,14 +159,27 @@ class FETIProblem:
         diags = [s.K.diagonal() for s in self.sub] if scaling else None
         for s, w in zip(self.sub, num.weights(diags)):
             s.w = w
-        self.n_lambda = num.n_lambda
         for s in self.sub:
             self._schur(s)
             if build_dirichlet:
                 s.tdofs = np.unique(s.dof)
                 s.trow = np.searchsorted(s.tdofs, s.dof)
                 s.Sdir = dirichlet_schur(s.K, s.tdofs)
+                s.Ssd = super_dirichlet_schur(s.K, s.tdofs)
+        self.n_lambda = num.n_lambda
         self._coarse()
+
+    def set_rhs(self, f_global):
+        """Subdomain loads from a global DOF vector, split over the subdomains that share a node
+        (value / multiplicity, src/assembler/physics/precomputed.cpp:61-65)."""
+        num, dpn = self.num, self.num.dpn
+        mult = np.zeros(int(max(n.max() for n in num.dom_nodes)) + 1)
+        for nodes in num.dom_nodes:
+            mult[nodes] += 1
+        f_global = np.asarray(f_global, dtype=np.float64).reshape(-1, dpn)
+        for d, s in enumerate(self.sub):
+            nodes = num.dom_nodes[d]
+            s.f = (f_global[nodes] / mult[nodes, None]).ravel()
 
     # -- explicit Schur complement (SparseSolverMKL.cpp:1207-1428: S = B K_reg^-1 B^T)
     def _schur(self, s: Subdomain):
@@ -205,23 +237,25 @@ class FETIProblem:
         return x - self.G.T @ a
 
     def precondition(self, x, kind):
-        """Apply_Prec (itersolvercpu.cpp:520-602): scaled B (K | S_dir) B^T."""
+        """Apply_Prec (itersolvercpu.cpp:520-602): scaled B (K | S_dir) B^T.  MAGIC applies the
+        stored K - RegMat (cluster.cpp:413-433), the same operator as LUMPED's K x - RegMat x;
+        SUPER_DIRICHLET applies the sparse S_sd of ``super_dirichlet_schur`` on the touched DOFs."""
         y = np.zeros(self.n_lambda)
         if kind == PREC_NONE:
             return x.copy()
         for s in self.sub:
             xi = x[s.lam] * s.w
-            if kind == PREC_LUMPED:
+            if kind in (PREC_LUMPED, PREC_MAGIC):
                 u = np.zeros(s.K.shape[0])
                 np.add.at(u, s.dof, s.sign * xi)
                 v = s.K @ u
                 yi = s.sign * v[s.dof]
             elif kind == PREC_WEIGHT:
                 yi = xi.copy()
-            elif kind == PREC_DIRICHLET:
+            elif kind in (PREC_DIRICHLET, PREC_SUPER_DIRICHLET):
                 u = np.zeros(s.tdofs.size)
                 np.add.at(u, s.trow, s.sign * xi)
-                v = s.Sdir @ u
+                v = (s.Sdir if kind == PREC_DIRICHLET else s.Ssd) @ u
                 yi = s.sign * v[s.trow]
             else:
                 raise ValueError(kind)
