@@ -113,7 +113,7 @@ void build(FETI4IStructInstance *I, bool keep_decomposition = false) {
                    " is not supported (0 TOTAL_FETI, 1 HYBRID_FETI)");
     FETI_CHECK(io[FETI4I_CGSOLVER] == 0, "FETI4I: only CGSOLVER 0 (PCG) is supported by this build");
     int prec = io[FETI4I_PRECONDITIONER];
-    FETI_CHECK(prec >= 0 && prec <= 3, "FETI4I: PRECONDITIONER " + std::to_string(prec) + " is not supported (0..3)");
+    FETI_CHECK(prec >= 0 && prec <= 5, "FETI4I: PRECONDITIONER " + std::to_string(prec) + " is not supported (0..5)");
     FETI_CHECK(I->ropt[FETI4I_PRECISION] > 0, "FETI4I: PRECISION must be positive");
     FETI_CHECK(io[FETI4I_MAX_ITERATIONS] > 0, "FETI4I: MAX_ITERATIONS must be positive");
     double t0 = now_s();
@@ -147,7 +147,9 @@ void build(FETI4IStructInstance *I, bool keep_decomposition = false) {
     SolveOptions &so = I->sopt;
     so.precision = I->ropt[FETI4I_PRECISION];
     so.max_iterations = io[FETI4I_MAX_ITERATIONS];
-    so.precond = prec;
+    // SUPER_DIRICHLET and MAGIC apply a sparse matrix on the touched DOFs, as LUMPED does: the
+    // device iteration runs them through the LUMPED kernels with the matrix the preparation built
+    so.precond = (prec == PREC_SUPER_DIRICHLET || prec == PREC_MAGIC) ? (int)PREC_LUMPED : prec;
     so.schur_precision = (int)I->ext[FETI4I_EXT_SCHUR_PRECISION];
     FETI_CHECK(so.schur_precision >= 0 && so.schur_precision <= 2, "FETI4I: invalid Schur precision");
     so.tiles_per_item = std::max(1, (int)I->ext[FETI4I_EXT_TILES_PER_ITEM]);

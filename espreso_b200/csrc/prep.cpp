@@ -193,6 +193,9 @@ static void prep_symbolic(const ElementData &el, const Decomposition &dec, int d
     std::vector<double> diag(n, 0.0);
     S.f.assign(n, 0.0);
     std::vector<std::vector<std::pair<int, double>>> KT(S.t);
+    // SUPER_DIRICHLET: the columns K_rT of the untouched DOFs r (r -> (T index, value))
+    const bool super_dir = opt.precond == PREC_SUPER_DIRICHLET;
+    std::vector<std::vector<std::pair<int, double>>> KrT(super_dir ? n1 : 0);
     if (device) {
         W.eldof.clear();
         W.Kfix.assign((size_t)n * ns, 0.0);
@@ -208,6 +211,7 @@ static void prep_symbolic(const ElementData &el, const Decomposition &dec, int d
                 for (int b = 0; b < nd; ++b) {
                     int pb = S.pos[eldof[b]];
                     if (pb >= n1) KT[pa - n1].emplace_back(pb - n1, Ke[(size_t)a * nd + b]);
+                    else if (super_dir) KrT[pb].emplace_back(pa - n1, Ke[(size_t)a * nd + b]);
                 }
         }
         if (device) {
@@ -221,7 +225,28 @@ static void prep_symbolic(const ElementData &el, const Decomposition &dec, int d
         }
     }
     W.rho = *std::max_element(diag.begin(), diag.end());
-    if (opt.precond == PREC_LUMPED) {
+    if (super_dir) {
+        // S_sd = K_TT - K_Tr diag(K_rr)^-1 K_rT (clustercpu.cpp:254-311, diagonalized_K_rr): every
+        // untouched DOF r adds -K_ir K_jr / K_rr to the T pairs (i, j) it couples
+        std::vector<int> rdof(n1);
+        for (int i = 0; i < n; ++i) if (S.pos[i] < n1) rdof[S.pos[i]] = i;
+        for (int r = 0; r < n1; ++r) {
+            auto &col = KrT[r];
+            if (col.empty()) continue;
+            std::sort(col.begin(), col.end(), [](auto &x, auto &y) { return x.first < y.first; });
+            size_t m = 0;   // sum duplicates (element contributions)
+            for (size_t k = 0; k < col.size(); ++k) {
+                if (m > 0 && col[m - 1].first == col[k].first) col[m - 1].second += col[k].second;
+                else col[m++] = col[k];
+            }
+            col.resize(m);
+            const double inv = 1.0 / diag[rdof[r]];
+            for (auto &ci : col)
+                for (auto &cj : col) KT[ci.first].emplace_back(cj.first, -ci.second * cj.second * inv);
+        }
+    }
+    if (opt.precond == PREC_LUMPED || opt.precond == PREC_MAGIC || super_dir) {
+        // MAGIC stores K - RegMat (cluster.cpp:413-433): on T the same entries as LUMPED's K
         S.KT_ptr.assign(S.t + 1, 0);
         for (int i = 0; i < S.t; ++i) {
             auto &row = KT[i];

@@ -13,7 +13,9 @@ namespace feti {
 
 struct DevPrepStore;
 
-enum Precond { PREC_NONE = 0, PREC_LUMPED = 1, PREC_WEIGHT = 2, PREC_DIRICHLET = 3 };
+// FETI4I_PRECONDITIONER values (src/config/ecf/solver/feti.h:40-47 of the reference)
+enum Precond { PREC_NONE = 0, PREC_LUMPED = 1, PREC_WEIGHT = 2, PREC_DIRICHLET = 3, PREC_SUPER_DIRICHLET = 4,
+               PREC_MAGIC = 5 };
 
 struct SubPrep {
     int n = 0;              // local DOFs
@@ -27,7 +29,9 @@ struct SubPrep {
     std::vector<double> R;  // n x nk, local DOF order, orthonormal columns
     std::vector<double> S;  // ni x ni, column-major, B K_reg^-1 B^T
     std::vector<double> Sdir;  // t x t Schur complement of K onto T (Dirichlet preconditioner)
-    std::vector<int> KT_ptr, KT_col;  // K restricted to T (lumped preconditioner), CSR in T order
+    // sparse preconditioner matrix on T, CSR in T order: K restricted to T (LUMPED, MAGIC), or
+    // S_sd = K_TT - K_Tr diag(K_rr)^-1 K_rT over the untouched DOFs r (SUPER_DIRICHLET)
+    std::vector<int> KT_ptr, KT_col;
     std::vector<double> KT_val;
     std::vector<double> f;  // subdomain right-hand side
     std::vector<double> G;  // nk x ni, row-major: G_i = -(B_i R_i)^T

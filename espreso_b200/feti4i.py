@@ -19,7 +19,7 @@ LIB_PATH = os.path.join(HERE, "libfeti4i_b200.so")
 SUBDOMAINS, MAX_ITERATIONS, FETI_METHOD, PRECONDITIONER, CGSOLVER, N_MICS, VERBOSE_LEVEL, MEASURE_LEVEL, \
     PRINT_MATRICES, SC_SIZE, INTEGER_OPTIONS_SIZE = range(11)
 PRECISION, REAL_OPTIONS_SIZE = 0, 1
-PREC_NONE, PREC_LUMPED, PREC_WEIGHT, PREC_DIRICHLET = 0, 1, 2, 3
+PREC_NONE, PREC_LUMPED, PREC_WEIGHT, PREC_DIRICHLET, PREC_SUPER_DIRICHLET, PREC_MAGIC = 0, 1, 2, 3, 4, 5
 # extended options (include/feti4i_ext.h)
 EXT_SCHUR_PRECISION, EXT_SCALING, EXT_HOST_ONLY, EXT_TILES_PER_ITEM, EXT_GRAPH_CHUNK, EXT_RELIABLE_DELTA, \
     EXT_HOST_THREADS, EXT_TILE_KERNEL, EXT_AUTOTUNE, EXT_SYMM_TENSOR, EXT_DEVICE_PREP = range(11)

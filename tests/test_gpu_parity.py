@@ -80,7 +80,8 @@ def test_fapply_edge_sizes():
 
 
 @pytest.mark.parametrize("prec,tile_kernel", [(OF.PREC_NONE, 1), (OF.PREC_LUMPED, 1), (OF.PREC_WEIGHT, 1),
-                                               (OF.PREC_DIRICHLET, 1), (OF.PREC_LUMPED, 0), (OF.PREC_DIRICHLET, 0)])
+                                               (OF.PREC_DIRICHLET, 1), (OF.PREC_LUMPED, 0), (OF.PREC_DIRICHLET, 0),
+                                               (OF.PREC_SUPER_DIRICHLET, 0), (OF.PREC_MAGIC, 0)])
 def test_solve_elasticity(elast, prec, tile_kernel):
     inst = gpu_instance(elast, prec=prec, tile_kernel=tile_kernel)
     sol = inst.solve()
@@ -102,8 +103,9 @@ def test_solve_elasticity(elast, prec, tile_kernel):
     inst.destroy()
 
 
-def test_solve_heat_dirichlet(heat):
-    inst = gpu_instance(heat, prec=F.PREC_DIRICHLET)
+@pytest.mark.parametrize("prec", [F.PREC_DIRICHLET, F.PREC_SUPER_DIRICHLET])
+def test_solve_heat_dirichlet(heat, prec):
+    inst = gpu_instance(heat, prec=prec)
     u = inst.solve().reshape(-1, 1)
     ud = direct_u(heat)
     assert np.linalg.norm(u - ud) <= 1e-8 * np.linalg.norm(ud)

@@ -84,7 +84,8 @@ def test_kernel_and_projected_operator(case):
 
 
 @pytest.mark.parametrize("case,prec", [("elast_2x2x2", OF.PREC_LUMPED), ("heat_3x3x2", OF.PREC_DIRICHLET),
-                                       ("elast_3x2x1", OF.PREC_NONE)])
+                                       ("elast_3x2x1", OF.PREC_NONE), ("heat_3x3x2", OF.PREC_SUPER_DIRICHLET),
+                                       ("elast_2x2x2", OF.PREC_MAGIC)])
 def test_host_operators_reproduce_solution(case, prec):
     P = CASES[case]()
     inst = host_instance(P, prec=prec)
@@ -111,7 +112,7 @@ def test_error_paths():
     with pytest.raises(F.FETI4IError, match="PCG"):
         problems.make_instance(P, iopts={F.CGSOLVER: 3, F.VERBOSE_LEVEL: 0}, ext={F.EXT_HOST_ONLY: 1})
     with pytest.raises(F.FETI4IError, match="PRECONDITIONER"):
-        problems.make_instance(P, iopts={F.PRECONDITIONER: 5, F.VERBOSE_LEVEL: 0}, ext={F.EXT_HOST_ONLY: 1})
+        problems.make_instance(P, iopts={F.PRECONDITIONER: 6, F.VERBOSE_LEVEL: 0}, ext={F.EXT_HOST_ONLY: 1})
     inst = host_instance(P)
     with pytest.raises(F.FETI4IError, match="HOST_ONLY"):
         inst.solve()
