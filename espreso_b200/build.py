@@ -14,6 +14,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libfeti4i_b200.so")
+# the same library with the FETI4I_INT_WIDTH 64 ABI (FETI4IInt = long)
+LIB64 = os.path.join(HERE, "libfeti4i_b200_i64.so")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -34,14 +36,16 @@ def _newer(target, deps):
 def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", h)
-                                                      for h in ("feti4i.h", "feti4i_ext.h")]
+                                                      for h in ("feti4i.h", "feti4i_ext.h", "mpi.h")]
     objs = []
-    for src in SOURCES:
+    units = [(src, os.path.splitext(src)[0] + ".o", []) for src in SOURCES]
+    units.append(("feti4i.cpp", "feti4i_i64.o", ["-DFETI4I_INT_WIDTH=64"]))
+    for src, obj, defs in units:
         s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, os.path.splitext(src)[0] + ".o")
+        o = os.path.join(BUILD, obj)
         objs.append(o)
         if force or _newer(o, [s] + hdrs):
-            cmd = [NVCC] + COMMON + ARCH + ["-c", s, "-o", o]
+            cmd = [NVCC] + COMMON + defs + ARCH + ["-c", s, "-o", o]
             if src.endswith(".cu"):
                 cmd += ["-Xptxas", "-v"] if verbose else []
             if verbose:
@@ -51,11 +55,15 @@ def build(force: bool = False, verbose: bool = False) -> str:
                 raise RuntimeError(f"compilation of {src} failed:\n{r.stdout}\n{r.stderr}")
             if verbose and r.stderr:
                 print(r.stderr)
-    if force or _newer(LIB, objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-Xcompiler", "-fopenmp", "-o", LIB] + objs + ["-lgomp"]
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    shared = [o for o in objs if not os.path.basename(o).startswith("feti4i")]
+    abi32 = os.path.join(BUILD, "feti4i.o")
+    abi64 = os.path.join(BUILD, "feti4i_i64.o")
+    for lib, abi in ((LIB, abi32), (LIB64, abi64)):
+        if force or _newer(lib, shared + [abi]):
+            cmd = [NVCC] + ARCH + ["-shared", "-Xcompiler", "-fopenmp", "-o", lib] + shared + [abi, "-lgomp"]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
     return LIB
 
 

@@ -2,6 +2,7 @@
 // reference is the interface being replaced).
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdlib>
 #include <cstring>
 #include <list>
@@ -82,7 +83,20 @@ FETI4IStructMatrix *check_matrix(FETI4IMatrix m) {
     return m;
 }
 
-void add_element(ElementData &el, int type, int nn, const int *nodes, int nd, const int *dofs, const double *values) {
+// Caller integers (FETI4IInt: 32 or 64 bit, by FETI4I_INT_WIDTH) -> the library's 32-bit indices.
+int narrow(FETI4IInt v, const char *what) {
+    FETI_CHECK(v >= (FETI4IInt)INT32_MIN && v <= (FETI4IInt)INT32_MAX,
+               std::string("FETI4I: ") + what + " does not fit the library's 32-bit indices");
+    return (int)v;
+}
+std::vector<int> narrow_all(const FETI4IInt *v, size_t n, const char *what) {
+    std::vector<int> out(n);
+    for (size_t i = 0; i < n; ++i) out[i] = narrow(v[i], what);
+    return out;
+}
+
+void add_element(ElementData &el, int type, int nn, const FETI4IInt *nodes, int nd, const FETI4IInt *dofs,
+                 const double *values) {
     // elements whose first dofsSize values are all zero are skipped, as in the
     // reference (src/app/apiwrapper/wrapper.cpp:151)
     bool zero = true;
@@ -90,8 +104,8 @@ void add_element(ElementData &el, int type, int nn, const int *nodes, int nd, co
     if (zero) return;
     if (el.node_ptr.empty()) { el.node_ptr.push_back(0); el.dof_ptr.push_back(0); el.val_ptr.push_back(0); }
     el.etype.push_back(type);
-    for (int i = 0; i < nn; ++i) el.nodes.push_back(nodes[i] - el.index_base);
-    for (int i = 0; i < nd; ++i) el.dofs.push_back(dofs[i] - el.index_base);
+    for (int i = 0; i < nn; ++i) el.nodes.push_back(narrow(nodes[i] - el.index_base, "a node index"));
+    for (int i = 0; i < nd; ++i) el.dofs.push_back(narrow(dofs[i] - el.index_base, "a DOF index"));
     el.vals.insert(el.vals.end(), values, values + (size_t)nd * nd);
     el.node_ptr.push_back((int64_t)el.nodes.size());
     el.dof_ptr.push_back((int64_t)el.dofs.size());
@@ -204,8 +218,8 @@ void FETI4ICreateStiffnessMatrix(FETI4IMatrix *matrix, FETI4IInt type, FETI4IInt
         FETI_CHECK(type == FETI4I_REAL_SYMMETRIC_POSITIVE_DEFINITE,
                    "FETI4I: only REAL_SYMMETRIC_POSITIVE_DEFINITE matrices are supported by the explicit-Schur solver");
         auto *m = new FETI4IStructMatrix();
-        m->el.type = type;
-        m->el.index_base = indexBase;
+        m->el.type = (int)type;
+        m->el.index_base = narrow(indexBase, "indexBase");
         g_matrices.push_back(m);
         *matrix = m;
     });
@@ -216,7 +230,8 @@ void FETI4IAddElement(FETI4IMatrix matrix, FETI4IInt type, FETI4IInt nodesSize, 
     guarded([&] {
         auto *m = check_matrix(matrix);
         FETI_CHECK(nodesSize > 0 && dofsSize > 0 && nodes && dofs && values, "FETI4I: invalid element data");
-        add_element(m->el, type, nodesSize, nodes, dofsSize, dofs, values);
+        add_element(m->el, (int)type, narrow(nodesSize, "nodesSize"), nodes, narrow(dofsSize, "dofsSize"), dofs,
+                    values);
     });
 }
 
@@ -227,9 +242,10 @@ void FETI4IAddElements(FETI4IMatrix matrix, FETI4IInt type, FETI4IInt nelems, FE
         FETI_CHECK(nelems >= 0 && nodesSize > 0 && dofsSize > 0 && nodes && dofs && values, "FETI4I: invalid element data");
         m->el.etype.reserve(m->el.etype.size() + nelems);
         m->el.vals.reserve(m->el.vals.size() + (size_t)nelems * dofsSize * dofsSize);
+        const int nn = narrow(nodesSize, "nodesSize"), nd = narrow(dofsSize, "dofsSize");
         for (FETI4IInt e = 0; e < nelems; ++e)
-            add_element(m->el, type, nodesSize, nodes + (size_t)e * nodesSize, dofsSize, dofs + (size_t)e * dofsSize,
-                        values + (size_t)e * dofsSize * dofsSize);
+            add_element(m->el, (int)type, nn, nodes + (size_t)e * nn, nd, dofs + (size_t)e * nd,
+                        values + (size_t)e * nd * nd);
     });
 }
 
@@ -237,7 +253,7 @@ void FETI4ISetSubdomainPartition(FETI4IMatrix matrix, FETI4IInt size, FETI4IInt 
     guarded([&] {
         auto *m = check_matrix(matrix);
         FETI_CHECK(size == (FETI4IInt)m->el.nelem(), "FETI4I: partition size differs from the number of added elements");
-        m->el.partition.assign(elem2sub, elem2sub + size);
+        m->el.partition = narrow_all(elem2sub, (size_t)size, "a subdomain index");
     });
 }
 
@@ -245,7 +261,7 @@ void FETI4ISetClusterPartition(FETI4IMatrix matrix, FETI4IInt nsubdomains, const
     guarded([&] {
         auto *m = check_matrix(matrix);
         FETI_CHECK(nsubdomains >= 0 && (nsubdomains == 0 || sub2cluster), "FETI4I: invalid cluster partition");
-        m->el.sub_cluster.assign(sub2cluster, sub2cluster + nsubdomains);
+        m->el.sub_cluster = narrow_all(sub2cluster, (size_t)nsubdomains, "a cluster index");
     });
 }
 
@@ -253,6 +269,26 @@ void FETI4ISetExtendedOption(FETI4IInt key, FETI4IReal value) {
     guarded([&] {
         FETI_CHECK(key >= 0 && key < FETI4I_EXT_OPTIONS_SIZE, "FETI4I: unknown extended option");
         g_ext[key] = value;
+    });
+}
+
+void FETI4ISetExtendedOptions(FETI4IInstance instance, FETI4IInt key, FETI4IReal value) {
+    guarded([&] {
+        auto *I = check_instance(instance);
+        FETI_CHECK(key >= 0 && key < FETI4I_EXT_OPTIONS_SIZE, "FETI4I: unknown extended option");
+        if (I->ext[key] == value) return;
+        I->ext[key] = value;
+        if (I->gpu && (key == FETI4I_EXT_RELIABLE_DELTA || key == FETI4I_EXT_GRAPH_CHUNK ||
+                       key == FETI4I_EXT_SYMM_TENSOR)) {
+            SolveOptions so = I->sopt;
+            so.reliable_delta = I->ext[FETI4I_EXT_RELIABLE_DELTA];
+            so.chunk = std::max(1, (int)I->ext[FETI4I_EXT_GRAPH_CHUNK]);
+            so.symm_tensor = I->ext[FETI4I_EXT_SYMM_TENSOR] != 0.0;
+            I->gpu->set_options(so);
+            I->sopt = so;
+            return;
+        }
+        build(I, true);   // preprocessing-dependent option: same decomposition, new preparation
     });
 }
 
@@ -269,12 +305,12 @@ void FETI4ICreateInstance(FETI4IInstance *instance, FETI4IMatrix matrix, FETI4II
         std::unique_ptr<FETI4IStructInstance> I(new FETI4IStructInstance());
         I->el = m->el;
         I->rhs.assign(rhs, rhs + size);
-        if (l2g) I->l2g.assign(l2g, l2g + size);
+        if (l2g) I->l2g = narrow_all(l2g, (size_t)size, "an l2g entry");
         for (FETI4IInt i = 0; i < dirichlet_size; ++i) {
-            I->dir_idx.push_back(dirichlet_indices[i] - m->el.index_base);
+            I->dir_idx.push_back(narrow(dirichlet_indices[i] - m->el.index_base, "a Dirichlet index"));
             I->dir_val.push_back(dirichlet_values[i]);
         }
-        std::memcpy(I->iopt, integer_options, sizeof(I->iopt));
+        for (int k = 0; k < FETI4I_INTEGER_OPTIONS_SIZE; ++k) I->iopt[k] = narrow(integer_options[k], "an option");
         std::memcpy(I->ropt, real_options, sizeof(I->ropt));
         std::memcpy(I->ext, g_ext, sizeof(I->ext));
         (void)neighbours;
@@ -434,7 +470,7 @@ void FETI4IUpdateDirichlet(FETI4IInstance instance, FETI4IInt size, FETI4IInt *i
         std::vector<int> idx;
         std::vector<double> val;
         for (FETI4IInt i = 0; i < size; ++i) {
-            idx.push_back(indices[i] - I->el.index_base);
+            idx.push_back(narrow(indices[i] - I->el.index_base, "a Dirichlet index"));
             val.push_back(values[i]);
         }
         std::vector<int> a = idx, b = I->dir_idx;
@@ -645,7 +681,7 @@ FETI4IReal FETI4ITimeDualOperator(FETI4IInstance instance, FETI4IInt precision, 
     guarded([&] {
         auto *I = check_instance(instance);
         FETI_CHECK(I->gpu, "FETI4I: no device solver");
-        ms = I->gpu->time_F(precision, std::max(1, reps));
+        ms = I->gpu->time_F((int)precision, std::max(1, (int)reps));
     });
     return ms;
 }
@@ -665,7 +701,14 @@ int FETI4ITiledSymvNoAlloc(const FETI4IReal *tiles, const long long *tile_offset
                            const FETI4IReal *x, FETI4IReal *y, FETI4IReal *dot, void *stream) {
     int rc = -1;
     guarded([&] {
+#if FETI4I_INT_WIDTH == 32
         rc = tiled_symv_noalloc(tiles, tile_offset, order, vector_offset, nmatrices, max_order, x, y, dot, stream);
+#else
+        (void)tiles; (void)tile_offset; (void)order; (void)vector_offset; (void)nmatrices; (void)max_order;
+        (void)x; (void)y; (void)dot; (void)stream;
+        FETI_CHECK(false, "FETI4ITiledSymvNoAlloc reads 32-bit device index arrays: call it through the "
+                          "FETI4I_INT_WIDTH 32 library");
+#endif
     });
     return rc;
 }

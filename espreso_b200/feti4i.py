@@ -34,7 +34,7 @@ EXPORTED = [
     "FETI4IAddElement", "FETI4ICreateInstance", "FETI4ISolve", "FETI4IUpdateStiffnessMatrix",
     "FETI4IUpdateStiffnessMatrixScaled",
     "FETI4IUpdateRhs", "FETI4IUpdateDirichlet", "FETI4IDestroy",
-    "FETI4IGetLastError", "FETI4ISetSubdomainPartition", "FETI4IAddElements", "FETI4ISetExtendedOption",
+    "FETI4IGetLastError", "FETI4ISetSubdomainPartition", "FETI4IAddElements", "FETI4ISetExtendedOption", "FETI4ISetExtendedOptions",
     "FETI4IGetStats", "FETI4IGetDualSolution", "FETI4IGetSubdomainInfo", "FETI4IGetSubdomainMultipliers",
     "FETI4IGetSubdomainNodes", "FETI4IGetSubdomainSchur", "FETI4IGetSubdomainKernel", "FETI4IGetDualRhs",
     "FETI4IApplySubdomainKplus", "FETI4IApplyDualOperator", "FETI4IApplyDualOperatorMulti", "FETI4ITimeDualOperator", "FETI4ISolveResident", "FETI4ISetSolvePrecision",
@@ -77,6 +77,7 @@ def load(path: str = LIB_PATH):
         "FETI4ISetSubdomainPartition": ([vp, i32, pi], None),
         "FETI4IAddElements": ([vp, i32, i32, i32, pi, i32, pi, pd], None),
         "FETI4ISetExtendedOption": ([i32, f64], None),
+        "FETI4ISetExtendedOptions": ([vp, i32, f64], None),
         "FETI4IGetStats": ([vp, i32, pd], None),
         "FETI4IGetDualSolution": ([vp, pd, pd], None),
         "FETI4IGetSubdomainInfo": ([vp, i32, pi], None),
@@ -372,6 +373,11 @@ class Instance:
         self.lib.FETI4IElementEnergies(self.h, u.size, _dp(u), _dp(v), _dp(out))
         _check(self.lib)
         return out
+
+    def set_extended(self, key, value):
+        """Extended option of this instance only (FETI4ISetExtendedOptions)."""
+        self.lib.FETI4ISetExtendedOptions(self.h, int(key), float(value))
+        _check(self.lib)
 
     def update_rhs(self, rhs):
         r = np.ascontiguousarray(rhs, dtype=np.float64)

@@ -9,7 +9,12 @@
  *
  * Differences in behaviour, all additive:
  *   - no MPI: one process, one GPU; FETI4IMPIInt stays a plain int and
- *     neighbours_size must be 0;
+ *     neighbours_size must be 0.  "mpi.h" is included as in the reference
+ *     (include/feti4i.h:5); without a real MPI the single-process stand-in
+ *     include/mpi.h serves it;
+ *   - FETI4I_INT_WIDTH 64 (FETI4IInt = long, include/feti4i.h:25-30) is the
+ *     ABI of libfeti4i_b200_i64.so; the default 32 that of libfeti4i_b200.so.
+ *     Indices must still fit 32 bits (larger ones are rejected);
  *   - errors never terminate the process: a failing call records a message
  *     that FETI4IGetLastError() (feti4i_ext.h) returns;
  *   - FETI4IUpdateStiffnessMatrix/Rhs/Dirichlet, declared but not defined in
@@ -17,6 +22,8 @@
  */
 #ifndef FETI4I_H_
 #define FETI4I_H_
+
+#include "mpi.h"
 
 /* integer/real widths: include/feti4i.h:7-39 */
 #ifndef FETI4I_INT_WIDTH
@@ -28,8 +35,10 @@
 
 #if FETI4I_INT_WIDTH == 32
 typedef int FETI4IInt;
+#elif FETI4I_INT_WIDTH == 64
+typedef long FETI4IInt;
 #else
-#error "this build supports FETI4I_INT_WIDTH 32 only"
+#error "Incorrect user-supplied value of FETI4I_INT_WIDTH"
 #endif
 
 typedef int FETI4IMPIInt;

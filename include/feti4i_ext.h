@@ -68,6 +68,12 @@ typedef enum {
 } FETI4IExtOptions;
 void FETI4ISetExtendedOption(FETI4IInt key, FETI4IReal value);
 
+/* Extended option of one instance (the per-instance form of FETI4ISetExtendedOption, which only
+ * sets the defaults of instances created afterwards).  FETI4I_EXT_RELIABLE_DELTA, GRAPH_CHUNK and
+ * SYMM_TENSOR apply to the next solve; the others (Schur precision, scaling, tiles, device or host
+ * preprocessing) redo the instance's preprocessing and upload with its decomposition kept. */
+void FETI4ISetExtendedOptions(FETI4IInstance instance, FETI4IInt key, FETI4IReal value);
+
 /* Statistics of an instance (indices of FETI4IStatIndex). */
 typedef enum {
     FETI4I_STAT_ITERATIONS,

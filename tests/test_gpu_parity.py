@@ -156,3 +156,16 @@ def test_max_iterations_stop(elast):
     st = inst.stats()
     assert st["converged"] == 0.0 and st["iterations"] == 5
     inst.destroy()
+
+
+def test_per_instance_schur_precision(elast):
+    """Two instances in one process with different Schur storage (FETI4ISetExtendedOptions)."""
+    a = gpu_instance(elast)
+    b = gpu_instance(elast)
+    b.set_extended(F.EXT_SCHUR_PRECISION, F.FP32)
+    assert b.stats()["fapply_bytes"] < 0.6 * a.stats()["fapply_bytes"]
+    ua, ub = a.solve(), b.solve()
+    assert b.stats()["converged"] == 1.0 and b.stats()["replacements"] > 0
+    assert np.linalg.norm(ua - ub) <= 1e-8 * np.linalg.norm(ua)
+    a.destroy()
+    b.destroy()

@@ -178,3 +178,24 @@ def test_update_matrix_scaled():
     unit.destroy()
     inst.destroy()
     ref.destroy()
+
+
+def test_per_instance_extended_options():
+    """FETI4ISetExtendedOptions changes one instance only; the process-wide defaults stay."""
+    P = CASES["elast_3x2x1"]()
+    a = host_instance(P)
+    b = host_instance(P)
+    b.set_extended(F.EXT_SCALING, 0)      # preparation-dependent: redone with the decomposition kept
+    OP = oracle_problem(P, scaling=False)
+    OS = oracle_problem(P, scaling=True)
+    for d in range(OP.num.ndomains):
+        np.testing.assert_allclose(b.multipliers(d)["w"], OP.sub[d].w, rtol=1e-15)
+        np.testing.assert_allclose(a.multipliers(d)["w"], OS.sub[d].w, rtol=1e-14)
+    b.set_extended(F.EXT_RELIABLE_DELTA, 0.05)   # solve-only option (no device solver on a host-only instance)
+    with pytest.raises(F.FETI4IError, match="unknown extended option"):
+        b.set_extended(99, 1)
+    c = host_instance(P)                  # new instances still take the defaults
+    for d in range(OP.num.ndomains):
+        np.testing.assert_allclose(c.multipliers(d)["w"], OS.sub[d].w, rtol=1e-14)
+    for i in (a, b, c):
+        i.destroy()
