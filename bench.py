@@ -61,6 +61,9 @@ def parse():
                     help="adjoint leg: DOMAINS^3 subdomains of ELEMENTS^3 HEXA8")
     ap.add_argument("--device-prep", type=int, default=1, choices=[0, 1],
                     help="subdomain eliminations and Schur complements on the GPU (1) or on the host (0)")
+    ap.add_argument("--explicit", type=int, default=1, choices=[0, 1],
+                    help="0: F applied through the subdomain K+ factors with no Schur complements stored "
+                         "(FP64, single right-hand side)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -213,6 +216,8 @@ def run_reference(args):
 
 
 def run_ours(args):
+    if args.explicit == 0:
+        args.schur, args.nrhs = "fp64", 0
     rank, world, local, dist = dist_init(args)
     import torch
     torch.cuda.set_device(local)
@@ -229,7 +234,8 @@ def run_ours(args):
                                        F.EXT_AUTOTUNE: 1 if args.tile_kernel < 0 else 0,
                                        F.EXT_RELIABLE_DELTA: args.delta,
                                        F.EXT_SYMM_TENSOR: args.symm_tensor,
-                                       F.EXT_DEVICE_PREP: args.device_prep},
+                                       F.EXT_DEVICE_PREP: args.device_prep,
+                                       F.EXT_SCHUR_EXPLICIT: args.explicit},
                                   clusters=P.sub_cluster() if args.method == 1 else None)
     setup_s = time.time() - t0
     st0 = inst.stats()
@@ -308,7 +314,7 @@ def run_ours(args):
     traffic = None
     traffic_src = None
     tp = os.path.join(ROOT, "profiles", "fapply_traffic.json")
-    if os.path.exists(tp):
+    if args.explicit and os.path.exists(tp):
         tj = json.load(open(tp))
         key = f"{args.config}:{args.schur}"
         if key in tj:
@@ -369,7 +375,9 @@ def run_ours(args):
                                           if st0["prep_device_ms"] > 0 else None),
                    "tuning": inst.tuning(),
                    "kplus_tiles_applied": st0["kplus_tiles"],
-                   "reliable_delta": args.delta},
+                   "reliable_delta": args.delta,
+                   "f_apply": "explicit S_i tiles" if args.explicit else "implicit through the K+ factors",
+                   "device_bytes": st["device_bytes"]},
         "fp64_gpu": {"ms": fp64_ms, "pcg_iterations": int(st64["iterations"]), "speedup_mixed": fp64_ms / step_ms,
                      "fapply_ms": fp64_f},
         "solves_per_s": world * 1e3 / step_ms,
@@ -377,7 +385,8 @@ def run_ours(args):
         "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": int(rhs.nbytes),
                 "d2h_bytes_per_step": int(sol.nbytes)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "traffic_source": traffic_src, "kernel": "tile_symv_kernel",
+                     "traffic": traffic, "traffic_source": traffic_src,
+                     "kernel": "tile_symv_kernel" if args.explicit else "kplus_dual_kernel",
                      "launch_ms": t_f, "peak_kind": peak_kind,
                      "alg_bytes_per_launch": alg},
         "cpu_baseline": cpu,

@@ -58,7 +58,7 @@ namespace {
 std::mutex g_mutex;
 std::list<FETI4IStructMatrix *> g_matrices;
 std::list<FETI4IStructInstance *> g_instances;
-double g_ext[FETI4I_EXT_OPTIONS_SIZE] = {0, 1, 0, 48, 16, 0.01, 0, 0, 1, 1, 1};
+double g_ext[FETI4I_EXT_OPTIONS_SIZE] = {0, 1, 0, 48, 16, 0.01, 0, 0, 1, 1, 1, 1};
 
 template <typename F>
 void guarded(F &&f) {
@@ -172,6 +172,7 @@ void build(FETI4IStructInstance *I, bool keep_decomposition = false) {
     so.tile_kernel = (int)I->ext[FETI4I_EXT_TILE_KERNEL];
     so.autotune = I->ext[FETI4I_EXT_AUTOTUNE] != 0.0;
     so.symm_tensor = I->ext[FETI4I_EXT_SYMM_TENSOR] != 0.0;
+    so.schur_explicit = I->ext[FETI4I_EXT_SCHUR_EXPLICIT] != 0.0;
     I->gpu.reset();
     I->rhs_on_device = false;
     if (I->ext[FETI4I_EXT_HOST_ONLY] == 0.0) {

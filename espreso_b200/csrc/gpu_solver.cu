@@ -114,7 +114,7 @@ struct BlockDev {
     int *queue;          // SYMM work queue [2]
     int n_conv_target;
 };
-enum { DONE_W = 0, DONE_RHO = 1, DONE_B = 2, DONE_PN = 3, DONE_COUNT = 8 };
+enum { DONE_W = 0, DONE_RHO = 1, DONE_B = 2, DONE_PN = 3, DONE_PAP_IMPLICIT = 4, DONE_COUNT = 8 };
 
 // Hybrid Total FETI cluster correction: F_c = sum_i B_i S_i B_i^T - V M V^T with, per subdomain,
 // V_i = [B_i K_i^+ B0_i^T | G_i^T] (n_i x m_i, column-major) and, per cluster, the dense
@@ -1164,6 +1164,118 @@ __global__ void __launch_bounds__(256) kplus_kernel(KplusDev K, const double *in
     for (int i = threadIdx.x; i < n; i += blockDim.x) out[o + i] = v[pos[i]];
 }
 
+// Implicit F apply (the reference's default without explicit Schur complements,
+// src/solver/specific/cpu/itersolvercpu.cpp:73-106 with Domain::multKplusLocal, Domain.cpp:271-338):
+// (S_i x)_r = s_r (K_i^+ B_i^T x)[dof_r] through the device Cholesky factor instead of stored S_i.
+// B_i^T x is zero at the untouched DOFs, which the factor order puts first, and only the touched
+// DOFs are read back, so the forward pass starts and the backward pass stops at the first touched
+// 32-block: both passes read only the factor's trailing touched part L_TT (its tiles that are not
+// all zero).  One CTA per subdomain writes the unassembled local product, as the tile SYMV does.
+// MODE 0: x = src, out += S x.  MODE 1 (PCG loop): x = src + beta src2 (direction p = y + beta p),
+// out = S x and p.Ap into SC_PAP.
+template <int MODE>
+__global__ void __launch_bounds__(256) kplus_dual_kernel(KplusDev K, DevProblem P, const int *rdof,
+                                                         const double *rsign, const double *src, const double *src2,
+                                                         double *out, int slot) {
+    pdl_enter();
+    extern __shared__ double v[];
+    __shared__ double part[8][32];
+    __shared__ double sh[32];
+    double beta = 0.0;
+    if (MODE == 1) {
+        const int iter = P.st->iter_base + slot;
+        if (skip_iter(P.st, iter)) return;
+        beta = (iter == 0) ? 0.0 : P.scal[SC_RHO] / P.rho_hist[iter - 1];
+    }
+    const int d = blockIdx.x;
+    const int T = K.tn[d], o = K.doff[d];
+    const int e0 = P.loff[d], e1 = P.loff[d + 1];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int *pos = K.pos + o;
+    const uint4 *tiles = reinterpret_cast<const uint4 *>(K.L) + (size_t)K.tile0[d] * (TILE * 16);
+    const double *dtiles = K.L + (size_t)K.tile0[d] * TILE * TILE;
+    const int *cp = K.cptr + K.cbase[d];
+    const int jt = K.jt[d];
+    for (int i = TILE * jt + threadIdx.x; i < TILE * T; i += blockDim.x) v[i] = 0.0;
+    __syncthreads();
+    // B^T x: several multipliers (Dirichlet and gluing rows) may share a DOF
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+        const double xv = (MODE == 1) ? src[e] + beta * src2[e] : src[e];
+        atomicAdd(&v[pos[rdof[e] - o]], rsign[e] * xv);
+    }
+    __syncthreads();
+    const int cq = lane % 16, h = lane / 16, idx = 2 * cq + h;
+    for (int J = jt; J < T; ++J) {   // forward: L y = B^T x
+        if (warp == 0) {
+            const double *row = dtiles + (size_t)ltile(T, J, J) * TILE * TILE + lane * TILE;
+            const double vr = v[TILE * J + lane];
+            double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+            for (int k = 0; k < TILE; k += 2) {
+                s0 += row[k] * __shfl_sync(FULL, vr, k);
+                s1 += row[k + 1] * __shfl_sync(FULL, vr, k + 1);
+            }
+            v[TILE * J + lane] = s0 + s1;
+        }
+        __syncthreads();
+        for (int q = cp[J] + 1 + warp; q < cp[J + 1]; q += nw) {
+            const int I = K.rows[q];
+            const uint4 *tp = tiles + (size_t)ltile(T, I, J) * (TILE * 16);
+            double rs[16];
+            const double x0 = v[TILE * J + 2 * cq], x1 = v[TILE * J + 2 * cq + 1];
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+                const uint4 u = ld_stream(tp + k * 32 + lane);
+                rs[k] = __hiloint2double(u.y, u.x) * x0 + __hiloint2double(u.w, u.z) * x1;
+            }
+            v[TILE * I + idx] -= reduce_scatter<16, 0>(rs, lane);
+        }
+        __syncthreads();
+    }
+    for (int J = T - 1; J >= jt; --J) {   // backward: L^T z = y, down to the first touched block
+        double cpart = 0.0;
+        for (int q = cp[J] + 1 + warp; q < cp[J + 1]; q += nw) {
+            const int I = K.rows[q];
+            const uint4 *tp = tiles + (size_t)ltile(T, I, J) * (TILE * 16);
+            double cs[2] = {0.0, 0.0};
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+                const uint4 u = ld_stream(tp + k * 32 + lane);
+                const double xr = v[TILE * I + 2 * k + h];
+                cs[0] += __hiloint2double(u.y, u.x) * xr;
+                cs[1] += __hiloint2double(u.w, u.z) * xr;
+            }
+            cpart += reduce_scatter<2, 4>(cs, lane);
+        }
+        part[warp][idx] = cpart;
+        __syncthreads();
+        if (warp == 0) {
+            double vc = v[TILE * J + lane];
+            for (int w = 0; w < nw; ++w) vc -= part[w][lane];
+            const double *tile = dtiles + (size_t)ltile(T, J, J) * TILE * TILE;
+            double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+            for (int k = 0; k < TILE; k += 2) {
+                s0 += tile[k * TILE + lane] * __shfl_sync(FULL, vc, k);
+                s1 += tile[(k + 1) * TILE + lane] * __shfl_sync(FULL, vc, k + 1);
+            }
+            v[TILE * J + lane] = s0 + s1;
+        }
+        __syncthreads();
+    }
+    double dot = 0.0;
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+        const double yv = rsign[e] * v[pos[rdof[e] - o]];
+        if (MODE == 1) {
+            out[e] = yv;
+            dot += (src[e] + beta * src2[e]) * yv;
+        } else {
+            out[e] += yv;
+        }
+    }
+    if (MODE == 1) grid_total(block_sum(dot, sh), P.part_w + P.nd, P.done + DONE_PAP_IMPLICIT, P.scal + SC_PAP, sh);
+}
+
 // K^+ on NC right-hand sides at once (columns j0 .. j0+NC-1 of in/out, `stride` doubles apart):
 // every factor tile is loaded once per pass and applied to all NC columns, so the factor is read
 // once for NC load cases.  Same tile walk and modes as kplus_kernel; z (mode 1/2) holds the
@@ -1738,6 +1850,10 @@ struct GpuSolver::Impl {
     DevProblem P{};
     DevState *st = nullptr;
     TileSetHost F64, Flow, Dir;
+    bool implicit = false;        // F64 applies run through the K^+ factor (kplus_dual_kernel), no S_i tiles
+    long long implicit_tiles = 0; // factor tiles one implicit pass applies (touched block columns, not all zero)
+    void launch_implicit(int mode, const double *src, const double *src2, double *out, int slot);
+    void release(void *p);        // frees one allocation of `allocs` before the solver goes
     int max_tn = 0, max_tn_dir = 0, max_nt = 0, max_ni = 0;
     std::vector<int> h_lam;       // L row -> lambda
     std::vector<int> h_loff;
@@ -1821,9 +1937,16 @@ struct GpuSolver::Impl {
         if (n == 0) n = 1;
         CUDA_CHECK(cudaMalloc(&p, n * sizeof(T)));
         allocs.push_back(p);
+        alloc_sizes.push_back(n * sizeof(T));
         bytes += n * sizeof(T);
         return (T *)p;
     }
+    size_t alloc_bytes_of(void *p) const {
+        for (size_t i = 0; i < allocs.size(); ++i)
+            if (allocs[i] == p) return alloc_sizes[i];
+        return 0;
+    }
+    std::vector<size_t> alloc_sizes;
     template <typename T>
     T *upload(const std::vector<T> &v) {
         T *p = alloc<T>(v.size());
@@ -1849,6 +1972,7 @@ struct GpuSolver::Impl {
         T *q = p;
         p = nullptr;
         allocs.push_back(q);
+        alloc_sizes.push_back(n * sizeof(T));
         bytes += n * sizeof(T);
         return q;
     }
@@ -2048,6 +2172,11 @@ void GpuSolver::Impl::upload_kplus(const Decomposition &dec, const Prep &prep, c
         }
         kept = (long long)rows.size();
         cbase[nd] = (int)cptr.size();
+        implicit_tiles = 0;
+        for (int d = 0; d < nd; ++d) {
+            const int jt_d = (prep.sub[d].n - prep.sub[d].t) / TILE;
+            implicit_tiles += cptr[cbase[d] + tn[d]] - cptr[cbase[d] + jt_d];
+        }
         FETI_CHECK(kept < (1LL << 31), "FETI4I: too many factor tiles");
         KP.cbase = upload(cbase);
         KP.cptr = upload(cptr);
@@ -2081,6 +2210,8 @@ void GpuSolver::Impl::upload_kplus(const Decomposition &dec, const Prep &prep, c
     d_rhs = alloc<double>(std::max(1, n_caller));
     d_sol = alloc<double>(std::max(1, n_caller));
     cudaFuncSetAttribute(kplus_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(kplus_dual_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(kplus_dual_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     CUDA_CHECK(cudaFuncSetAttribute(kplus_multi_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kplus_multi_smem(16)));
     CUDA_CHECK(cudaFuncSetAttribute(kplus_multi_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kplus_multi_smem(8)));
     CUDA_CHECK(cudaFuncSetAttribute(kplus_multi_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kplus_multi_smem(4)));
@@ -2440,8 +2571,35 @@ static size_t tile_smem(int prec, int max_tn) {
     return 2 * acc * (size_t)max_tn * TILE;
 }
 
+void GpuSolver::Impl::release(void *p) {
+    for (size_t i = 0; i < allocs.size(); ++i)
+        if (allocs[i] == p) {
+            CUDA_CHECK(cudaFree(p));
+            bytes -= alloc_sizes[i];
+            allocs.erase(allocs.begin() + i);
+            alloc_sizes.erase(alloc_sizes.begin() + i);
+            return;
+        }
+}
+
+void GpuSolver::Impl::launch_implicit(int mode, const double *src, const double *src2, double *out, int slot) {
+    FETI_CHECK(mode == 0 || mode == 1, "internal: implicit F apply in an unsupported mode");
+    const size_t sm = sizeof(double) * TILE * (size_t)max_T;
+    if (mode == 0)
+        launch_pdl(kplus_dual_kernel<0>, dim3(P.nd), dim3(256), sm, stream, KP, P, (const int *)d_rdof,
+                   (const double *)d_rsign, src, src2, out, slot);
+    else
+        launch_pdl(kplus_dual_kernel<1>, dim3(P.nd), dim3(256), sm, stream, KP, P, (const int *)d_rdof,
+                   (const double *)d_rsign, src, src2, out, slot);
+    CUDA_CHECK(cudaGetLastError());
+}
+
 void GpuSolver::Impl::launch_tiles(const TileSetHost &T, int mode, const double *src, const double *src2, double *out,
                                    int slot) {
+    if (implicit && &T == &F64) {
+        launch_implicit(mode, src, src2, out, slot);
+        return;
+    }
     int mtn = (&T == &Dir) ? max_tn_dir : max_tn;
     TileSetDev td = T.dev();
     FETI_CHECK(mode != 1 || src2 != nullptr, "internal: PCG direction update without a previous direction");
@@ -2593,6 +2751,8 @@ double GpuSolver::kplus_tile_fraction() const {
 }
 int GpuSolver::device_id() const { return impl->device; }
 void GpuSolver::set_options(const SolveOptions &opt) {
+    FETI_CHECK(opt.schur_explicit == impl->opt.schur_explicit,
+               "FETI4I: explicit or implicit F apply is fixed at instance creation");
     FETI_CHECK(opt.schur_precision == SCHUR_FP64 || impl->Flow.prec == opt.schur_precision,
                "FETI4I: the requested Schur precision was not prepared on the device");
     FETI_CHECK(opt.precond == impl->opt.precond, "FETI4I: the preconditioner is fixed at instance creation");
@@ -2768,7 +2928,7 @@ void GpuSolver::upload(const Decomposition &dec, const Prep &prep, const SolveOp
     P.alpha = I.alloc<double>(prep.n_kern + KS);
     CUDA_CHECK(cudaMemset(P.alpha, 0, sizeof(double) * (prep.n_kern + KS)));
     I.e_dev = I.alloc<double>(P.nP);
-    P.part_w = I.alloc<double>(nd); P.part_rho = I.alloc<double>(nd); P.part_b = I.alloc<double>(nd);
+    P.part_w = I.alloc<double>(2 * nd); P.part_rho = I.alloc<double>(nd); P.part_b = I.alloc<double>(nd);
     P.rho_hist = I.alloc<double>((size_t)opt.max_iterations + 64);
     I.st = I.alloc<DevState>(1);
     P.st = I.st;
@@ -2791,10 +2951,23 @@ void GpuSolver::upload(const Decomposition &dec, const Prep &prep, const SolveOp
     FETI_CHECK(tile_smem(SCHUR_FP64, I.max_tn) <= 200 * 1024, "FETI4I: a Schur complement is too large for the tile kernel");
     DevPrepStore *ds = prep.dstore.get();
     FETI_CHECK(!ds || (ds->nd == nd && ds->s_tiles && ds->kp_tiles), "FETI4I: device preprocessing store missing");
-    double *s64 = ds ? I.adopt(ds->s_tiles, (size_t)ds->s_tile0[nd] * TILE * TILE) : nullptr;
-    I.build_tiles(I.F64, SCHUR_FP64, mats, ns, voffs, opt.tiles_per_item, s64);
-    if (opt.schur_precision != SCHUR_FP64)
-        I.build_tiles(I.Flow, opt.schur_precision, mats, ns, voffs, opt.tiles_per_item, s64);
+    I.implicit = !opt.schur_explicit;
+    if (I.implicit) {
+        // F through the K^+ factor: no S_i tiles on the device (those of the device preprocessing are freed)
+        FETI_CHECK(prep.method == 0, "FETI4I: the implicit F apply (no explicit Schur complements) is Total FETI only");
+        FETI_CHECK(opt.schur_precision == SCHUR_FP64,
+                   "FETI4I: the implicit F apply runs in FP64 (the Schur precision applies to explicit S_i)");
+        if (ds && ds->s_tiles) {
+            CUDA_CHECK(cudaFree(ds->s_tiles));
+            ds->s_tiles = nullptr;
+        }
+        I.F64.prec = SCHUR_FP64;
+    } else {
+        double *s64 = ds ? I.adopt(ds->s_tiles, (size_t)ds->s_tile0[nd] * TILE * TILE) : nullptr;
+        I.build_tiles(I.F64, SCHUR_FP64, mats, ns, voffs, opt.tiles_per_item, s64);
+        if (opt.schur_precision != SCHUR_FP64)
+            I.build_tiles(I.Flow, opt.schur_precision, mats, ns, voffs, opt.tiles_per_item, s64);
+    }
     if (opt.precond == PREC_DIRICHLET) {
         std::vector<const double *> dm(nd);
         std::vector<int> dn(nd), dv(nd);
@@ -2812,7 +2985,7 @@ void GpuSolver::upload(const Decomposition &dec, const Prep &prep, const SolveOp
     }
     if (opt.autotune) {
         CUDA_CHECK(cudaMemset(P.w, 0, sizeof(double) * NL));
-        I.autotune(I.F64, P.w, I.Ax64, NL);
+        if (!I.implicit) I.autotune(I.F64, P.w, I.Ax64, NL);
         if (opt.schur_precision != SCHUR_FP64) I.autotune(I.Flow, P.w, I.Ax64, NL);
         if (opt.precond == PREC_DIRICHLET) {
             CUDA_CHECK(cudaMemset(P.uT, 0, sizeof(double) * NT));
@@ -2822,6 +2995,11 @@ void GpuSolver::upload(const Decomposition &dec, const Prep &prep, const SolveOp
     const double tu2 = now_s();
     I.upload_kplus(dec, prep, loff, toff);
     I.upload_hybrid(dec, prep);
+    if (I.implicit) {
+        // algorithmic bytes of one implicit apply: the touched factor tiles that are not all zero, read by the
+        // forward and the backward pass, plus the vectors (index, sign, x in, y out per local multiplier)
+        I.F64.alg_bytes = 2.0 * (double)I.implicit_tiles * TILE * TILE * sizeof(double) + (double)NL * (4 + 8 + 8 + 8);
+    }
     CUDA_CHECK(cudaDeviceSynchronize());
     FETI_LOG(2, "FETI4I: upload: dual layout %.3f s, tiles and autotuning %.3f s, K+ and clusters %.3f s\n",
              tu1 - tu0, tu2 - tu1, now_s() - tu2);
@@ -3046,6 +3224,7 @@ void GpuSolver::get_solution(std::vector<double> &lambda, std::vector<double> &a
 }
 
 void GpuSolver::subdomain_schur(int d, double *S) {
+    FETI_CHECK(!impl->implicit, "FETI4I: no Schur complements are stored with the implicit F apply");
     Impl &I = *impl;
     const TileSetHost &T = I.F64;
     FETI_CHECK(d >= 0 && d < (int)T.h_tn.size(), "FETI4I: subdomain index out of range");
@@ -5204,6 +5383,7 @@ void GpuSolver::Impl::prepare_symm_panels() {
 // y_j = F x_j for nrhs dual vectors (column j at j * n_lambda) through the multi right-hand-side
 // F apply of the block PCG (tile SYMM in the given Schur precision, plus the HTFETI correction)
 void GpuSolver::apply_F_multi(const double *x, double *y, int nrhs, int precision) {
+    FETI_CHECK(!impl->implicit, "FETI4I: the multi right-hand-side F apply needs the explicit Schur complements");
     Impl &I = *impl;
     DevProblem &P = I.P;
     FETI_CHECK(nrhs >= 1 && nrhs <= 32, "FETI4IApplyDualOperatorMulti: 1..32 vectors per call");
@@ -5234,6 +5414,7 @@ void GpuSolver::apply_F_multi(const double *x, double *y, int nrhs, int precisio
 
 void GpuSolver::solve_multi(const double *rhs, int nrhs, int rhs_size, double *solutions, int solution_size,
                             SolveStats &stats, bool upload_rhs) {
+    FETI_CHECK(!impl->implicit, "FETI4ISolveMulti needs the explicit Schur complements (FETI4I_EXT_SCHUR_EXPLICIT 1)");
     Impl &I = *impl;
     DevProblem &P = I.P;
     FETI_CHECK(nrhs >= 1 && nrhs <= 32, "FETI4ISolveMulti: 1..32 right-hand sides per call");

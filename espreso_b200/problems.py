@@ -307,6 +307,7 @@ def make_instance(problem: Problem, iopts=None, ropts=None, ext=None, batched=Tr
             F.set_extended(F.EXT_SYMM_TENSOR, 1)
             F.set_extended(F.EXT_DEVICE_PREP, 1)
             F.set_extended(F.EXT_RELIABLE_DELTA, 0.01)
+            F.set_extended(F.EXT_SCHUR_EXPLICIT, 1)
     return inst
 
 

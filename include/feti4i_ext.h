@@ -64,6 +64,10 @@ typedef enum {
                                     (batched FP64 partial Cholesky of [K_reg B^T; B 0]); 0, or HOST_ONLY: host
                                     dense path.  The reference assembles S_i on the host
                                     (SparseSolverMKL.cpp:1207) */
+    FETI4I_EXT_SCHUR_EXPLICIT,   /* 1 (default): F applied through stored Schur complements S_i (the reference's
+                                    use_schur_complement); 0: through the subdomains' K^+ factors, with no S_i stored
+                                    (the reference's default, itersolvercpu.cpp:73-106; FP64, Total FETI, one
+                                    right-hand side) */
     FETI4I_EXT_OPTIONS_SIZE
 } FETI4IExtOptions;
 void FETI4ISetExtendedOption(FETI4IInt key, FETI4IReal value);

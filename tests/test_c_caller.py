@@ -90,4 +90,6 @@ def test_c_caller_solve(setup, width):
     ref = inst.solve()
     inst.destroy()
     got = np.fromfile(out, dtype=np.float64)
-    assert np.linalg.norm(got - ref) <= 1e-12 * np.linalg.norm(ref)
+    # two solves of the same instance data agree to the solver precision (the F apply sums with
+    # atomics, so the last bits differ from run to run)
+    assert np.linalg.norm(got - ref) <= 1e-10 * np.linalg.norm(ref)
