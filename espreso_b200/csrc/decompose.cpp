@@ -333,4 +333,13 @@ void compute_weights(Decomposition &dec, const std::vector<std::vector<double>> 
     }
 }
 
+void restrict_subdomains(Decomposition &dec, int first, int count) {
+    FETI_CHECK(first >= 0 && count > 0 && first + count <= dec.ndom,
+               "FETI4I: the owned subdomain range [" + std::to_string(first) + ", " + std::to_string(first + count) +
+                   ") is outside the " + std::to_string(dec.ndom) + " subdomains");
+    dec.dom = std::vector<DomainRows>(dec.dom.begin() + first, dec.dom.begin() + first + count);
+    dec.g2l = std::vector<std::unordered_map<int, int>>(dec.g2l.begin() + first, dec.g2l.begin() + first + count);
+    dec.ndom = count;
+}
+
 }  // namespace feti

@@ -60,4 +60,8 @@ Decomposition decompose(const ElementData &el, int ndomains_hint, const std::vec
 // Duplicity weights: 1/ndomains, or with scaling K-diagonal ratios; diags[d] in local DOF order.
 void compute_weights(Decomposition &dec, const std::vector<std::vector<double>> *diags);
 
+// Keep subdomains [first, first + count) only (a partitioned dual problem: the subdomain block of one
+// process).  Multiplier indices, weights, multiplicities and the caller-DOF maps stay global.
+void restrict_subdomains(Decomposition &dec, int first, int count);
+
 }  // namespace feti

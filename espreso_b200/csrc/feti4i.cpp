@@ -42,7 +42,8 @@ struct FETI4IStructInstance {
     int iopt[FETI4I_INTEGER_OPTIONS_SIZE];
     double ropt[FETI4I_REAL_OPTIONS_SIZE];
     double ext[FETI4I_EXT_OPTIONS_SIZE];
-    Decomposition dec;
+    Decomposition dec_full;      // numbering of the whole problem
+    Decomposition dec;           // the subdomains this instance prepares (all, or the owned block)
     Prep prep;
     std::unique_ptr<GpuSolver> gpu;
     SolveOptions sopt;
@@ -58,7 +59,7 @@ namespace {
 std::mutex g_mutex;
 std::list<FETI4IStructMatrix *> g_matrices;
 std::list<FETI4IStructInstance *> g_instances;
-double g_ext[FETI4I_EXT_OPTIONS_SIZE] = {0, 1, 0, 48, 16, 0.01, 0, 0, 1, 1, 1, 1};
+double g_ext[FETI4I_EXT_OPTIONS_SIZE] = {0, 1, 0, 48, 16, 0.01, 0, 0, 1, 1, 1, 1, 0, 0};
 
 template <typename F>
 void guarded(F &&f) {
@@ -132,9 +133,10 @@ void build(FETI4IStructInstance *I, bool keep_decomposition = false) {
     FETI_CHECK(io[FETI4I_MAX_ITERATIONS] > 0, "FETI4I: MAX_ITERATIONS must be positive");
     double t0 = now_s();
     if (!keep_decomposition) {
-        I->dec = decompose(I->el, io[FETI4I_SUBDOMAINS], I->dir_idx, I->dir_val);
+        I->dec_full = decompose(I->el, io[FETI4I_SUBDOMAINS], I->dir_idx, I->dir_val);
         FETI_LOG(2, "FETI4I: decomposition %.3f s\n", now_s() - t0);
     }
+    I->dec = I->dec_full;   // preprocess keeps the owned subdomains of a partitioned problem
     PrepOptions po;
     po.method = io[FETI4I_FETI_METHOD];
     if (po.method == 1 && !I->el.sub_cluster.empty()) {
@@ -144,6 +146,10 @@ void build(FETI4IStructInstance *I, bool keep_decomposition = false) {
         po.sub_cluster = I->el.sub_cluster;
     }
     po.precond = prec;
+    po.owned_first = (int)I->ext[FETI4I_EXT_OWNED_FIRST];
+    po.owned_count = (int)I->ext[FETI4I_EXT_OWNED_COUNT];
+    FETI_CHECK(po.owned_count == 0 || io[FETI4I_FETI_METHOD] == 0,
+               "FETI4I: a partitioned dual problem (FETI4I_EXT_OWNED_COUNT > 0) is Total FETI only");
     po.scaling = I->ext[FETI4I_EXT_SCALING] != 0.0;
     po.threads = (int)I->ext[FETI4I_EXT_HOST_THREADS];
     // the device preprocessing runs with the GPU path; HOST_ONLY instances preprocess on the host
@@ -321,6 +327,15 @@ void FETI4ICreateInstance(FETI4IInstance *instance, FETI4IMatrix matrix, FETI4II
     });
 }
 
+// The internal dual PCG needs the whole dual problem; a partitioned instance (one process's block of
+// subdomains) is driven through the device-operator entry points instead.
+static void check_whole(FETI4IStructInstance *I) {
+    FETI_CHECK(I->ext[FETI4I_EXT_OWNED_COUNT] == 0.0,
+               "FETI4I: this instance holds a block of the subdomains (FETI4I_EXT_OWNED_COUNT); it is solved by a "
+               "partitioned driver through FETI4IApplyDualOperatorDevice, FETI4IApplyPreconditionerDevice and "
+               "FETI4IPrimalFromDual");
+}
+
 static void solve_instance(FETI4IStructInstance *I) {
     FETI_CHECK(I->gpu, "FETI4I: instance was created with FETI4I_EXT_HOST_ONLY; no device solver");
     make_rhs_vectors(I->dec, I->prep, I->b, I->e);
@@ -336,6 +351,7 @@ static void solve_instance(FETI4IStructInstance *I) {
 void FETI4ISolve(FETI4IInstance instance, FETI4IInt solution_size, FETI4IReal *solution) {
     guarded([&] {
         auto *I = check_instance(instance);
+        check_whole(I);
         FETI_CHECK(solution_size >= 0 && (solution_size == 0 || solution), "FETI4I: invalid solution array");
         FETI_CHECK(I->gpu, "FETI4I: instance was created with FETI4I_EXT_HOST_ONLY; no device solver");
         double t0 = now_s();
@@ -353,6 +369,7 @@ void FETI4ISolveMulti(FETI4IInstance instance, FETI4IInt nrhs, FETI4IInt size, c
                       FETI4IReal *solutions) {
     guarded([&] {
         auto *I = check_instance(instance);
+        check_whole(I);
         FETI_CHECK(I->gpu, "FETI4I: instance was created with FETI4I_EXT_HOST_ONLY; no device solver");
         FETI_CHECK(rhs && solutions && size > 0, "FETI4ISolveMulti: invalid arrays");
         double t0 = now_s();
@@ -366,6 +383,7 @@ FETI4IReal FETI4ISolveMultiResident(FETI4IInstance instance, FETI4IInt nrhs) {
     double ms = -1.0;
     guarded([&] {
         auto *I = check_instance(instance);
+        check_whole(I);
         FETI_CHECK(I->gpu && I->multi_on_device == nrhs, "FETI4ISolveMultiResident: call FETI4ISolveMulti first");
         I->gpu->solve_multi(nullptr, nrhs, 0, nullptr, 0, I->stats, false);
         ms = I->stats.t_solve_ms;
@@ -377,6 +395,7 @@ FETI4IReal FETI4ISolveResident(FETI4IInstance instance) {
     double ms = -1.0;
     guarded([&] {
         auto *I = check_instance(instance);
+        check_whole(I);
         FETI_CHECK(I->gpu && I->rhs_on_device, "FETI4I: no right-hand side on the device (call FETI4ISolve first)");
         I->gpu->solve(I->stats);
         I->lambda.clear();
@@ -485,9 +504,10 @@ void FETI4IUpdateDirichlet(FETI4IInstance instance, FETI4IInt size, FETI4IInt *i
             std::vector<double> byk((size_t)I->dec.n_nodes * dpn, 0.0);
             for (size_t i = 0; i < idx.size(); ++i)
                 byk[(size_t)I->dec.dof_node[idx[i]] * dpn + I->dec.dof_comp[idx[i]]] = val[i];
-            for (auto &D : I->dec.dom)
-                for (size_t r = 0; r < D.lam.size(); ++r)
-                    if (D.other[r] < 0) D.c[r] = byk[(size_t)D.node[r] * dpn + D.comp[r]];
+            for (Decomposition *dc : {&I->dec, &I->dec_full})
+                for (auto &D : dc->dom)
+                    for (size_t r = 0; r < D.lam.size(); ++r)
+                        if (D.other[r] < 0) D.c[r] = byk[(size_t)D.node[r] * dpn + D.comp[r]];
             I->rhs_on_device = false;
         } else {
             build(I);
@@ -694,6 +714,36 @@ void FETI4IElementEnergies(FETI4IInstance instance, FETI4IInt size, const FETI4I
         FETI_CHECK(I->gpu, "FETI4I: no device solver");
         FETI_CHECK(size > 0 && u && v && out, "FETI4I: invalid vectors");
         I->gpu->element_energies(I->el, u, v, size, out);
+    });
+}
+
+void FETI4IApplyDualOperatorDevice(FETI4IInstance instance, FETI4IInt precision, const FETI4IReal *x, FETI4IReal *y,
+                                   void *stream) {
+    guarded([&] {
+        auto *I = check_instance(instance);
+        FETI_CHECK(I->gpu, "FETI4I: no device solver");
+        FETI_CHECK(x && y, "FETI4IApplyDualOperatorDevice: null vector");
+        I->gpu->apply_F_device(x, y, (int)precision, stream);
+    });
+}
+
+void FETI4IApplyPreconditionerDevice(FETI4IInstance instance, const FETI4IReal *x, FETI4IReal *y, void *stream) {
+    guarded([&] {
+        auto *I = check_instance(instance);
+        FETI_CHECK(I->gpu, "FETI4I: no device solver");
+        FETI_CHECK(x && y, "FETI4IApplyPreconditionerDevice: null vector");
+        I->gpu->apply_prec_device(x, y, stream);
+    });
+}
+
+void FETI4IPrimalFromDual(FETI4IInstance instance, const FETI4IReal *lambda, const FETI4IReal *amplitudes,
+                          FETI4IInt solution_size, FETI4IReal *solution) {
+    guarded([&] {
+        auto *I = check_instance(instance);
+        FETI_CHECK(I->gpu, "FETI4I: no device solver");
+        FETI_CHECK(lambda && amplitudes && solution_size >= 0 && (solution_size == 0 || solution),
+                   "FETI4IPrimalFromDual: invalid arrays");
+        I->gpu->primal_from_dual(I->rhs.data(), (int)I->rhs.size(), lambda, amplitudes, solution, (int)solution_size);
     });
 }
 

@@ -1023,6 +1023,54 @@ __global__ void chunk_end_kernel(DevProblem P, int chunk) {
 
 
 // ---------------------------------------------------------------------------------------------
+// Partitioned dual problem: operators between caller vectors in the whole problem's multiplier
+// numbering and this instance's local rows.
+__global__ void gather_lambda_kernel(const int *lam, const double *x, double *xl, int NL) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < NL) xl[e] = x[lam[e]];
+}
+// y[lambda] += yl (two local rows of one multiplier add both), yl cleared for the next accumulation
+__global__ void scatter_lambda_kernel(const int *lam, double *yl, double *y, int NL) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < NL) {
+        atomicAdd(&y[lam[e]], yl[e]);
+        yl[e] = 0.0;
+    }
+}
+// u_T = B^T W x on the touched DOFs (x in the whole numbering); WEIGHT also v_T = u_T
+template <int PRECOND>
+__global__ void prec_gather_kernel(DevProblem P, const int *lam, const double *x) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.NT) return;
+    double s = 0.0;
+    for (int q = P.trow_ptr[t]; q < P.trow_ptr[t + 1]; ++q) {
+        const int e = P.trow_idx[q];
+        s += P.ws[e] * x[lam[e]];
+    }
+    P.uT[t] = s;
+    if (PRECOND == PREC_WEIGHT) P.vT[t] = s;
+}
+// v_T = K_TT u_T (sliced ELL; LUMPED, MAGIC and SUPER_DIRICHLET matrices)
+__global__ void prec_ell_kernel(DevProblem P) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.NT) return;
+    const int t0 = P.tbase[t], ts = P.tslot[t];
+    const int sl = ts >> 5, ln = ts & 31;
+    const int base = P.ell_ptr[sl], wd = P.ell_w[sl];
+    double s = 0.0;
+    for (int q = 0; q < wd; ++q) {
+        const int o = base + q * 32 + ln;
+        s += P.ell_val[o] * P.uT[t0 + P.ell_col[o]];
+    }
+    P.vT[t] = s;
+}
+// y[lambda] += W B v_T
+__global__ void prec_scatter_kernel(DevProblem P, const int *lam, double *y) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < P.NL) atomicAdd(&y[lam[e]], P.ws[e] * P.vT[P.tidx[e]]);
+}
+
+// ---------------------------------------------------------------------------------------------
 // K^+ on the device: forward/backward substitution with the Cholesky factor of
 // K_reg (factor order), stored as 32x32 lower tiles (I >= J), block column by
 // block column; the diagonal tiles hold the inverse of their 32x32 triangular block,
@@ -1856,6 +1904,7 @@ struct GpuSolver::Impl {
     void release(void *p);        // frees one allocation of `allocs` before the solver goes
     int max_tn = 0, max_tn_dir = 0, max_nt = 0, max_ni = 0;
     std::vector<int> h_lam;       // L row -> lambda
+    int *d_lam = nullptr;         // the same on the device
     std::vector<int> h_loff;
     std::vector<int> h_doff;      // local-DOF offsets of the subdomains (K^+ vectors)
     int n_lambda = 0;
@@ -2826,6 +2875,7 @@ void GpuSolver::upload(const Decomposition &dec, const Prep &prep, const SolveOp
             for (int k = 0; k < S.dnk; ++k) Gl[(size_t)e * KS + k] = S.Gd[(size_t)k * S.ni + r];
         }
     }
+    I.d_lam = I.upload(I.h_lam);
     // partner data of every row (shortens the dependent-load chains of the assembly)
     std::vector<int> ptidx(NL, -1), pkof(NL, 0), pnk(NL, 0);
     std::vector<double> pws(NL, 0.0), Gp((size_t)NL * KS, 0.0);
@@ -3320,6 +3370,98 @@ double GpuSolver::time_F(int precision, int reps) {
     zero_kernel<<<(NL + 255) / 256, 256, 0, I.stream>>>(I.Ax64, NL);
     CUDA_CHECK(cudaStreamSynchronize(I.stream));
     return total / reps;
+}
+
+// caller stream -> library stream -> caller stream ordering of a device-operator call
+namespace {
+struct StreamJoin {
+    cudaStream_t caller, lib;
+    cudaEvent_t ev;
+    StreamJoin(cudaStream_t c, cudaStream_t l) : caller(c), lib(l) {
+        CUDA_CHECK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        CUDA_CHECK(cudaEventRecord(ev, caller));
+        CUDA_CHECK(cudaStreamWaitEvent(lib, ev, 0));
+    }
+    void done() {
+        CUDA_CHECK(cudaEventRecord(ev, lib));
+        CUDA_CHECK(cudaStreamWaitEvent(caller, ev, 0));
+        CUDA_CHECK(cudaEventDestroy(ev));
+    }
+};
+}  // namespace
+
+void GpuSolver::apply_F_device(const double *x, double *y, int precision, void *stream) {
+    Impl &I = *impl;
+    const TileSetHost &T = precision == SCHUR_FP64 ? I.F64 : I.Flow;
+    FETI_CHECK(T.prec == precision, "FETI4I: the requested Schur precision was not prepared on the device");
+    FETI_CHECK(!I.hybrid, "FETI4I: the device-operator entry points are Total FETI only");
+    const int NL = I.P.NL;
+    StreamJoin j((cudaStream_t)stream, I.stream);
+    if (NL > 0) {
+        gather_lambda_kernel<<<(NL + 255) / 256, 256, 0, I.stream>>>(I.d_lam, x, I.P.w, NL);
+        I.launch_tiles(T, 0, I.P.w, nullptr, I.Ax64, 0);
+        scatter_lambda_kernel<<<(NL + 255) / 256, 256, 0, I.stream>>>(I.d_lam, I.Ax64, y, NL);
+        CUDA_CHECK(cudaGetLastError());
+    }
+    j.done();
+}
+
+void GpuSolver::apply_prec_device(const double *x, double *y, void *stream) {
+    Impl &I = *impl;
+    DevProblem &P = I.P;
+    FETI_CHECK(!I.hybrid, "FETI4I: the device-operator entry points are Total FETI only");
+    FETI_CHECK(I.opt.precond != PREC_NONE, "FETI4I: the instance has no preconditioner (PRECONDITIONER 0)");
+    StreamJoin j((cudaStream_t)stream, I.stream);
+    const int tg = (P.NT + 255) / 256, rg = (P.NL + 255) / 256;
+    if (P.NL > 0) {
+        switch (I.opt.precond) {
+        case PREC_WEIGHT:
+            prec_gather_kernel<PREC_WEIGHT><<<tg, 256, 0, I.stream>>>(P, I.d_lam, x);
+            prec_scatter_kernel<<<rg, 256, 0, I.stream>>>(P, I.d_lam, y);
+            break;
+        case PREC_LUMPED:
+            prec_gather_kernel<PREC_LUMPED><<<tg, 256, 0, I.stream>>>(P, I.d_lam, x);
+            prec_ell_kernel<<<tg, 256, 0, I.stream>>>(P);
+            prec_scatter_kernel<<<rg, 256, 0, I.stream>>>(P, I.d_lam, y);
+            break;
+        default:   // DIRICHLET: S_dir tiles
+            prec_gather_kernel<PREC_DIRICHLET><<<tg, 256, 0, I.stream>>>(P, I.d_lam, x);
+            zero_kernel<<<tg, 256, 0, I.stream>>>(P.vT, P.NT);
+            I.launch_tiles(I.Dir, 0, P.uT, nullptr, P.vT, 0);
+            prec_scatter_kernel<<<rg, 256, 0, I.stream>>>(P, I.d_lam, y);
+            break;
+        }
+        CUDA_CHECK(cudaGetLastError());
+    }
+    j.done();
+}
+
+void GpuSolver::primal_from_dual(const double *rhs, int rhs_size, const double *lambda, const double *alpha,
+                                 double *solution, int solution_size) {
+    Impl &I = *impl;
+    DevProblem &P = I.P;
+    FETI_CHECK(!I.hybrid, "FETI4I: the device-operator entry points are Total FETI only");
+    // f_i, and the forward pass L^-1 f kept for the primal (as in solve_full)
+    CUDA_CHECK(cudaMemsetAsync(I.d_rhs, 0, sizeof(double) * std::max(1, I.n_caller), I.stream));
+    const int ncp = std::min(rhs_size, I.n_caller);
+    I.h2d_columns(I.d_rhs, 0, rhs, 0, (size_t)std::max(0, ncp), 1);
+    split_rhs_kernel<<<(I.ntot + 255) / 256, 256, 0, I.stream>>>(I.d_rhs, I.d_gdof, I.d_invm, I.d_f, I.ntot);
+    I.launch_kplus(I.d_f, I.d_kf, KPLUS_TOUCHED);
+    // lambda at the local rows, the amplitudes of the instance's kernels
+    std::vector<double> xL(P.NL);
+    for (int e = 0; e < P.NL; ++e) xL[e] = lambda[I.h_lam[e]];
+    CUDA_CHECK(cudaMemcpyAsync(P.x, xL.data(), sizeof(double) * P.NL, cudaMemcpyHostToDevice, I.stream));
+    CUDA_CHECK(cudaMemcpyAsync(P.alpha, alpha, sizeof(double) * P.nK, cudaMemcpyHostToDevice, I.stream));
+    primal_rhs_kernel<<<std::max(1, std::min(4096, (I.ntot + 255) / 256)), 256, 0, I.stream>>>(
+        P, I.d_tdof_g, I.d_rsign, nullptr, I.d_g, I.ntot);
+    primal_bt_kernel<<<(P.NT + 255) / 256, 256, 0, I.stream>>>(P, I.d_tdof_g, I.d_rsign, I.d_g);
+    I.launch_kplus(I.d_g, I.d_kf, KPLUS_PRIMAL);
+    CUDA_CHECK(cudaMemsetAsync(I.d_sol, 0, sizeof(double) * std::max(1, I.n_caller), I.stream));
+    primal_merge_kernel<<<P.nd, TPB, 0, I.stream>>>(P, I.d_doff, I.d_rdofs, I.d_Rd, I.d_kf, I.d_gdof, I.d_invm, I.d_sol);
+    CUDA_CHECK(cudaGetLastError());
+    const int nco = std::min(solution_size, I.n_caller);
+    I.d2h_columns(solution, 0, I.d_sol, 0, (size_t)std::max(0, nco), 1);
+    for (int i = std::max(0, nco); i < solution_size; ++i) solution[i] = 0.0;
 }
 
 double GpuSolver::fapply_bytes(int precision) const {

@@ -72,6 +72,13 @@ public:
     // y = F x in lambda space with the given operator precision (tests, benchmarks)
     void apply_F(const double *x_lambda, double *y_lambda, int precision);
     void apply_F_multi(const double *x, double *y, int nrhs, int precision);
+    // partitioned dual problem, caller device vectors in the whole problem's multiplier numbering:
+    // y += sum over the instance's subdomains of B S B^T x (precision of S), or of W B M B^T W x
+    void apply_F_device(const double *x, double *y, int precision, void *stream);
+    void apply_prec_device(const double *x, double *y, void *stream);
+    // primal recovery from host lambda (whole numbering) and amplitudes (the instance's kernel numbering)
+    void primal_from_dual(const double *rhs, int rhs_size, const double *lambda, const double *alpha, double *solution,
+                          int solution_size);
     // average device time of `reps` F applies (inputs resident), returns ms
     double time_F(int precision, int reps);
     double fapply_bytes(int precision) const;

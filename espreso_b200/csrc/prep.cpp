@@ -561,6 +561,11 @@ void preprocess(const ElementData &el, Decomposition &dec, const std::vector<dou
         }
     }
     compute_weights(dec, opt.scaling ? &diags : nullptr);
+    // partitioned dual problem: the weights need every subdomain's diagonal; the rest only the owned block
+    if (opt.owned_count > 0) {
+        FETI_CHECK(opt.method == 0, "FETI4I: a partitioned dual problem (owned subdomain range) is Total FETI only");
+        restrict_subdomains(dec, opt.owned_first, opt.owned_count);
+    }
 
     out.sub.assign(dec.ndom, SubPrep());
     out.n_lambda = dec.n_lambda;

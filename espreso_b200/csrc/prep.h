@@ -99,6 +99,7 @@ struct PrepOptions {
     int threads = 0;
     bool device = false;            // subdomain eliminations and S_i on the current CUDA device
     size_t device_mem = 0;          // bytes for one batch of dense subdomain matrices (0: half the free memory)
+    int owned_first = 0, owned_count = 0;   // partitioned dual problem: prepare these subdomains only (count 0: all)
 };
 
 // rhs: caller DOF vector (size >= max DOF + 1); split per subdomain by multiplicity.

@@ -22,7 +22,8 @@ PRECISION, REAL_OPTIONS_SIZE = 0, 1
 PREC_NONE, PREC_LUMPED, PREC_WEIGHT, PREC_DIRICHLET, PREC_SUPER_DIRICHLET, PREC_MAGIC = 0, 1, 2, 3, 4, 5
 # extended options (include/feti4i_ext.h)
 EXT_SCHUR_PRECISION, EXT_SCALING, EXT_HOST_ONLY, EXT_TILES_PER_ITEM, EXT_GRAPH_CHUNK, EXT_RELIABLE_DELTA, \
-    EXT_HOST_THREADS, EXT_TILE_KERNEL, EXT_AUTOTUNE, EXT_SYMM_TENSOR, EXT_DEVICE_PREP, EXT_SCHUR_EXPLICIT = range(12)
+    EXT_HOST_THREADS, EXT_TILE_KERNEL, EXT_AUTOTUNE, EXT_SYMM_TENSOR, EXT_DEVICE_PREP, EXT_SCHUR_EXPLICIT, \
+    EXT_OWNED_FIRST, EXT_OWNED_COUNT = range(14)
 FP64, FP32, BF16 = 0, 1, 2
 STAT_NAMES = ["iterations", "converged", "dual_size", "kernel_size", "subdomains", "prep_seconds",
               "upload_seconds", "solve_ms", "solve_wall_ms", "fapply_bytes", "replacements",
@@ -38,7 +39,8 @@ EXPORTED = [
     "FETI4IGetStats", "FETI4IGetDualSolution", "FETI4IGetSubdomainInfo", "FETI4IGetSubdomainMultipliers",
     "FETI4IGetSubdomainNodes", "FETI4IGetSubdomainSchur", "FETI4IGetSubdomainKernel", "FETI4IGetDualRhs",
     "FETI4IApplySubdomainKplus", "FETI4IApplyDualOperator", "FETI4IApplyDualOperatorMulti", "FETI4ITimeDualOperator", "FETI4ISolveResident", "FETI4ISetSolvePrecision",
-    "FETI4ITiledSymvNoAlloc", "FETI4IElementEnergies", "FETI4IGetTuning", "FETI4ISolveMulti",
+    "FETI4ITiledSymvNoAlloc", "FETI4IApplyDualOperatorDevice", "FETI4IApplyPreconditionerDevice",
+    "FETI4IPrimalFromDual", "FETI4IElementEnergies", "FETI4IGetTuning", "FETI4ISolveMulti",
     "FETI4ISolveMultiResident", "FETI4ISetClusterPartition", "FETI4IGetSubdomainCorners", "FETI4IGetClusterInfo",
 ]
 
@@ -93,6 +95,9 @@ def load(path: str = LIB_PATH):
         "FETI4ISolveResident": ([vp], f64),
         "FETI4ISetSolvePrecision": ([vp, i32], None),
         "FETI4ITiledSymvNoAlloc": ([vp, vp, vp, vp, i32, i32, vp, vp, vp, vp], i32),
+        "FETI4IApplyDualOperatorDevice": ([vp, i32, vp, vp, vp], None),
+        "FETI4IApplyPreconditionerDevice": ([vp, vp, vp, vp], None),
+        "FETI4IPrimalFromDual": ([vp, pd, pd, i32, pd], None),
         "FETI4IElementEnergies": ([vp, i32, pd, pd, pd], None),
         "FETI4IGetTuning": ([vp], C.c_char_p),
         "FETI4ISolveMulti": ([vp, i32, i32, pd, pd], None),
@@ -371,6 +376,24 @@ class Instance:
         v = np.ascontiguousarray(v, dtype=np.float64)
         out = np.zeros(int(self.stats()["elements"]))
         self.lib.FETI4IElementEnergies(self.h, u.size, _dp(u), _dp(v), _dp(out))
+        _check(self.lib)
+        return out
+
+    def apply_F_device(self, x_ptr, y_ptr, precision=FP64, stream=0):
+        """y += (this instance's subdomains' part of F) x on caller device memory (partitioned problems)."""
+        self.lib.FETI4IApplyDualOperatorDevice(self.h, int(precision), x_ptr, y_ptr, stream)
+        _check(self.lib)
+
+    def apply_prec_device(self, x_ptr, y_ptr, stream=0):
+        self.lib.FETI4IApplyPreconditionerDevice(self.h, x_ptr, y_ptr, stream)
+        _check(self.lib)
+
+    def primal_from_dual(self, lam, alpha):
+        """This instance's part of the solution from the whole problem's lambda and its own amplitudes."""
+        lam = np.ascontiguousarray(lam, dtype=np.float64)
+        alpha = np.ascontiguousarray(alpha, dtype=np.float64)
+        out = np.zeros(self.n)
+        self.lib.FETI4IPrimalFromDual(self.h, _dp(lam), _dp(alpha), out.size, _dp(out))
         _check(self.lib)
         return out
 

@@ -68,6 +68,12 @@ typedef enum {
                                     use_schur_complement); 0: through the subdomains' K^+ factors, with no S_i stored
                                     (the reference's default, itersolvercpu.cpp:73-106; FP64, Total FETI, one
                                     right-hand side) */
+    FETI4I_EXT_OWNED_FIRST,      /* partitioned dual problem: first subdomain of this process's block */
+    FETI4I_EXT_OWNED_COUNT,      /* ... and its size (0, default: all subdomains).  The reference splits the
+                                    subdomains over MPI processes and sums the shared multipliers between them
+                                    (itersolver.cpp:6373-6406); here every process numbers the whole problem,
+                                    prepares and uploads only its block, and a driver (espreso_b200.partitioned)
+                                    runs the dual PCG with the operators below and one allreduce per apply. */
     FETI4I_EXT_OPTIONS_SIZE
 } FETI4IExtOptions;
 void FETI4ISetExtendedOption(FETI4IInt key, FETI4IReal value);
@@ -140,6 +146,22 @@ void FETI4IApplyDualOperator(FETI4IInstance instance, FETI4IInt precision, FETI4
    F apply of FETI4ISolveMulti (tile SYMM in the given Schur precision; introspection) */
 void FETI4IApplyDualOperatorMulti(FETI4IInstance instance, FETI4IInt precision, FETI4IInt nrhs, FETI4IReal *x,
                                   FETI4IReal *y);
+/* Partitioned dual problem (FETI4I_EXT_OWNED_COUNT > 0), device memory of the caller, dual vectors in the
+ * whole problem's multiplier numbering (dual size entries): y += sum over this instance's subdomains of
+ * B_i S_i B_i^T x (the F apply of itersolvercpu.cpp:9-114 before All_Reduce_lambdas_compB), and
+ * y += sum of W_i B_i M_i B_i^T W_i x (Apply_Prec, itersolvercpu.cpp:520-602, before its allreduce).  The
+ * caller sums y over the processes.  stream: a cudaStream_t the calls are ordered after and before,
+ * or NULL for the default stream. */
+void FETI4IApplyDualOperatorDevice(FETI4IInstance instance, FETI4IInt precision, const FETI4IReal *x, FETI4IReal *y,
+                                   void *stream);
+void FETI4IApplyPreconditionerDevice(FETI4IInstance instance, const FETI4IReal *x, FETI4IReal *y, void *stream);
+/* Primal recovery u_i = K_i^+ (f_i - B_i^T lambda) + R_i alpha_i of this instance's subdomains
+ * (itersolver.cpp:372-431) from host lambda (whole problem's numbering) and the amplitudes of its own
+ * kernel numbering (FETI4IGetStats kernel size entries), averaged into caller DOFs with the weights of
+ * the whole problem: summed over the processes it is the solution. */
+void FETI4IPrimalFromDual(FETI4IInstance instance, const FETI4IReal *lambda, const FETI4IReal *amplitudes,
+                          FETI4IInt solution_size, FETI4IReal *solution);
+
 /* Average device time in ms of one F apply over `reps` launches (inputs resident). */
 FETI4IReal FETI4ITimeDualOperator(FETI4IInstance instance, FETI4IInt precision, FETI4IInt reps);
 /* Several load cases at once (the reference has no multi-RHS path): nrhs right-hand
