@@ -64,6 +64,9 @@ def parse():
     ap.add_argument("--explicit", type=int, default=1, choices=[0, 1],
                     help="0: F applied through the subdomain K+ factors with no Schur complements stored "
                          "(FP64, single right-hand side)")
+    ap.add_argument("--mode", default="replicas", choices=["replicas", "partitioned"],
+                    help="N > 1: one independent load case per GPU (replicas), or one dual problem whose "
+                         "subdomains are split into blocks over the GPUs (partitioned; NCCL allreduce per apply)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -404,6 +407,57 @@ def run_ours(args):
 ORACLE_PRECISION = 1e-11
 
 
+def run_partitioned(args):
+    """One dual problem split over the ranks: rank r prepares the r-th contiguous block of the
+    subdomains on its GPU; the PCG runs replicated with one NCCL allreduce of the dual vector per F
+    apply and per preconditioner apply (espreso_b200.partitioned).  Total work is fixed: strong scaling."""
+    rank, world, local, dist = dist_init(args)
+    import torch
+    torch.cuda.set_device(local)
+    from espreso_b200 import feti4i as F
+    from espreso_b200 import problems
+    from espreso_b200.partitioned import LibraryBlock, PartitionedSolver, owned_range
+    P = problems.build_config(args.config)
+    nsub = int(P.elem_domain.max()) + 1
+    first, count = owned_range(nsub, rank, world)
+    t0 = time.time()
+    blk = LibraryBlock(P, first, count,
+                       iopts={F.PRECONDITIONER: args.precond, F.VERBOSE_LEVEL: 0, F.MAX_ITERATIONS: 5000},
+                       ropts={F.PRECISION: args.precision}, ext={F.EXT_DEVICE_PREP: args.device_prep})
+    group = dist.group.WORLD if dist is not None else None
+    S = PartitionedSolver(blk, group=group)
+    setup_s = time.time() - t0
+    for _ in range(args.warmup):
+        S.solve(precision=args.precision, max_it=5000, prec=args.precond)
+    dist_barrier(dist)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        ev0.record()
+        for _ in range(args.steps):
+            S.solve(precision=args.precision, max_it=5000, prec=args.precond)
+        ev1.record()
+        torch.cuda.synchronize()
+    dist_barrier(dist)
+    ms = dist_max(dist, ev0.elapsed_time(ev1) / args.steps)
+    u = S.primal()
+    res = P.relative_residual(u)
+    line = {"metric": METRIC, "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": False, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": args.config, "subdomains": nsub, "dual_size": S.n_lambda, "kernel_size": S.n_kern,
+                       "precond": args.precond, "precision": args.precision, "pcg_iterations": S.iterations,
+                       "parallelism": f"subdomain-blocks{world}", "setup_s": setup_s,
+                       "collectives_per_solve": S.collectives // max(1, args.warmup + args.steps)},
+            "parity": {"residual": res, "converged": bool(S.converged)},
+            "clocks": clk.summary()}
+    if rank == 0:
+        print(json.dumps(line))
+    blk.destroy()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 def cpu_baseline_and_oracle(P, args, R):
     """CPU baseline and checker: the oracle's FP64 dual solve of the same mesh on all host cores.
 
@@ -508,5 +562,7 @@ if __name__ == "__main__":
         run_prep(a)
     elif a.impl == "reference":
         run_reference(a)
+    elif a.mode == "partitioned":
+        run_partitioned(a)
     else:
         run_ours(a)
