@@ -227,6 +227,26 @@ __device__ void block_sum_k(double (&v)[KMAX], double *sh /* >= 32*KMAX */) {
 }
 
 
+// block-wide sum of KC values at once (KC = the kernel width of the problem)
+template <int KC>
+__device__ void block_sum_kc(double (&v)[KC], double *sh /* >= 32*KC */) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < KC; ++k) v[k] = warp_sum(v[k]);
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < KC; ++k) sh[wid * KC + k] = v[k];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < KC; ++k) {
+        double s = 0.0;
+        for (int i = 0; i < nw; ++i) s += sh[i * KC + k];
+        v[k] = s;
+    }
+    __syncthreads();
+}
+
 __device__ __forceinline__ bool skip_iter(const DevState *st, int iter) {
     int c = st->conv_iter;
     return (c >= 0 && iter > c) || iter >= st->max_it;
@@ -235,11 +255,11 @@ __device__ __forceinline__ bool skip_iter(const DevState *st, int iter) {
 // (G^T a) at local row e: own coefficients plus the partner's
 template <int KC>
 __device__ __forceinline__ double gt_alpha_fixed(const DevProblem &P, int e, const double *a) {
-    const int ko = P.rkof[e], po = P.pkof[e];
+    const int ko = __ldg(P.rkof + e), po = __ldg(P.pkof + e);
     const double *g = P.Gl + (size_t)e * KC, *gp = P.Gp + (size_t)e * KC;
     double s = 0.0;
 #pragma unroll
-    for (int k = 0; k < KC; ++k) s += g[k] * a[ko + k] + gp[k] * a[po + k];
+    for (int k = 0; k < KC; ++k) s += __ldg(g + k) * a[ko + k] + __ldg(gp + k) * a[po + k];
     return s;
 }
 // The common kernel widths 1 (heat) and 6 (elasticity) take fixed-width loads: coefficients
@@ -279,8 +299,29 @@ __device__ void grid_total(double v, double *partials, int *counter, double *out
     }
 }
 
-// G_i v over the rows [e0, e1) of one subdomain, written to d[kof..]
+// G_i v over the rows [e0, e1) of one subdomain, written to d[kof..]; KC = the row stride KS of the
+// coefficients (zero-padded rows), so only the problem's kernel width is reduced
+template <int KC>
+__device__ void g_dot_kc(const DevProblem &P, int dsub, const double *v, double *sh) {
+    const int e0 = P.loff[dsub], e1 = P.loff[dsub + 1];
+    const int nk = P.kof[dsub + 1] - P.kof[dsub];
+    double gk[KC];
+#pragma unroll
+    for (int k = 0; k < KC; ++k) gk[k] = 0.0;
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+        const double ve = v[e - e0];
+        const double *g = P.Gl + (size_t)e * KC;
+#pragma unroll
+        for (int k = 0; k < KC; ++k) gk[k] += __ldg(g + k) * ve;
+    }
+    block_sum_kc<KC>(gk, sh);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < nk; ++k) P.d[P.kof[dsub] + k] = gk[k];
+}
+
 __device__ void g_dot(const DevProblem &P, int dsub, const double *v, double *sh) {
+    if (P.KS == 1) { g_dot_kc<1>(P, dsub, v, sh); return; }
+    if (P.KS == 6) { g_dot_kc<6>(P, dsub, v, sh); return; }
     const int e0 = P.loff[dsub], e1 = P.loff[dsub + 1];
     const int nk = P.kof[dsub + 1] - P.kof[dsub];
     double gk[KMAX];
@@ -790,9 +831,17 @@ __global__ void coarse_kernel(DevProblem P, const double *in, double *out, int s
     int lane = threadIdx.x & 31;
     if (row >= P.nK) return;
     const double *col = P.GGtinv + (size_t)row * P.nP;
-    double s = 0.0;
-    for (int b = lane; b < P.nP; b += 32) s += col[b] * in[b];
-    s = warp_sum(s);
+    // four independent partial sums: the loads of four steps are in flight together
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    int b = lane;
+    for (; b + 96 < P.nP; b += 128) {
+        s0 += __ldg(col + b) * __ldg(in + b);
+        s1 += __ldg(col + b + 32) * __ldg(in + b + 32);
+        s2 += __ldg(col + b + 64) * __ldg(in + b + 64);
+        s3 += __ldg(col + b + 96) * __ldg(in + b + 96);
+    }
+    for (; b < P.nP; b += 32) s0 += __ldg(col + b) * __ldg(in + b);
+    double s = warp_sum((s0 + s1) + (s2 + s3));
     if (lane == 0) out[row] = s;
 }
 
@@ -814,7 +863,7 @@ __global__ void zero2_kernel(double *a, double *b, int n) {
 }
 
 // r = b - assemble(Ax); d = G r per subdomain; ||b||^2 total (initial call).  One CTA per subdomain.
-__global__ void r0_kernel(DevProblem P, double *Ax, int replace_mode, int slot) {
+__global__ void __launch_bounds__(1024) r0_kernel(DevProblem P, double *Ax, int replace_mode, int slot) {
     pdl_enter();
     extern __shared__ double rv_s[];
     __shared__ double sh[32 * KMAX];
@@ -875,11 +924,11 @@ __global__ void __launch_bounds__(TPB1) w_prec_kernel(DevProblem P, int slot) {
     double *u = sm + (e1 - e0);    // B^T W w on the touched DOFs
     double ww = 0.0;
     for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-        const double wv = P.r[e] - gt_alpha(P, e, P.alpha);
+        const double wv = __ldg(P.r + e) - gt_alpha(P, e, P.alpha);
         P.w[e] = wv;
         wsm[e - e0] = wv;
         if (PRECOND == PREC_NONE) P.y[e] = wv;
-        ww += wv * wv * P.minv[e];
+        ww += wv * wv * __ldg(P.minv + e);
     }
     ww = block_sum(ww, sh);  // also a barrier for wsm
     grid_total(ww, P.part_w, P.done + DONE_W, P.scal + SC_WN2, sh);
@@ -889,9 +938,9 @@ __global__ void __launch_bounds__(TPB1) w_prec_kernel(DevProblem P, int slot) {
     }
     for (int t = threadIdx.x; t < nt; t += blockDim.x) {
         double s = 0.0;
-        for (int j = P.trow_ptr[t0 + t]; j < P.trow_ptr[t0 + t + 1]; ++j) {
-            const int e = P.trow_idx[j];
-            s += P.ws[e] * wsm[e - e0];
+        for (int j = __ldg(P.trow_ptr + t0 + t); j < __ldg(P.trow_ptr + t0 + t + 1); ++j) {
+            const int e = __ldg(P.trow_idx + j);
+            s += __ldg(P.ws + e) * wsm[e - e0];
         }
         if (PRECOND == PREC_LUMPED) u[t] = s;
         else P.uT[t0 + t] = s;
@@ -902,18 +951,31 @@ __global__ void __launch_bounds__(TPB1) w_prec_kernel(DevProblem P, int slot) {
     const int sl0 = P.slice0[dsub];
     for (int t = threadIdx.x; t < nt; t += blockDim.x) {
         const int sl = sl0 + (t >> 5), ln = t & 31;
-        const int base = P.ell_ptr[sl], wd = P.ell_w[sl];
-        double s = 0.0;
-        for (int j = 0; j < wd; ++j) {
+        const int base = __ldg(P.ell_ptr + sl), wd = __ldg(P.ell_w + sl);
+        // four independent entries per step: their loads are in flight together
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        int j = 0;
+        for (; j + 3 < wd; j += 4) {
             const int o = base + j * 32 + ln;
-            s += P.ell_val[o] * u[P.ell_col[o]];
+            const double v0 = __ldg(P.ell_val + o), v1 = __ldg(P.ell_val + o + 32), v2 = __ldg(P.ell_val + o + 64),
+                         v3 = __ldg(P.ell_val + o + 96);
+            const int c0 = __ldg(P.ell_col + o), c1 = __ldg(P.ell_col + o + 32), c2 = __ldg(P.ell_col + o + 64),
+                      c3 = __ldg(P.ell_col + o + 96);
+            s0 += v0 * u[c0];
+            s1 += v1 * u[c1];
+            s2 += v2 * u[c2];
+            s3 += v3 * u[c3];
         }
-        P.vT[t0 + t] = s;
+        for (; j < wd; ++j) {
+            const int o = base + j * 32 + ln;
+            s0 += __ldg(P.ell_val + o) * u[__ldg(P.ell_col + o)];
+        }
+        P.vT[t0 + t] = (s0 + s1) + (s2 + s3);
     }
 }
 
 // z = assemble(W B v_T); d = G z.  One CTA per subdomain.
-__global__ void z_kernel(DevProblem P, int slot) {
+__global__ void __launch_bounds__(1024) z_kernel(DevProblem P, int slot) {
     pdl_enter();
     extern __shared__ double zs[];
     __shared__ double sh[32 * KMAX];
@@ -922,9 +984,9 @@ __global__ void z_kernel(DevProblem P, int slot) {
     const int dsub = blockIdx.x;
     const int e0 = P.loff[dsub], e1 = P.loff[dsub + 1];
     for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-        const int pt = P.ptidx[e];
-        double zv = P.ws[e] * P.vT[P.tidx[e]];
-        if (pt >= 0) zv += P.pws[e] * P.vT[pt];
+        const int pt = __ldg(P.ptidx + e);
+        double zv = __ldg(P.ws + e) * __ldg(P.vT + __ldg(P.tidx + e));
+        if (pt >= 0) zv += __ldg(P.pws + e) * __ldg(P.vT + pt);
         P.z[e] = zv;
         zs[e - e0] = zv;
     }
@@ -933,7 +995,7 @@ __global__ void z_kernel(DevProblem P, int slot) {
 }
 
 // y = z - G^T alpha, rho = y.w total; clear the F apply accumulators.
-__global__ void y_kernel(DevProblem P, double *Ax64, int slot) {
+__global__ void __launch_bounds__(1024) y_kernel(DevProblem P, double *Ax64, int slot) {
     pdl_enter();
     __shared__ double sh[32];
     const int iter = P.st->iter_base + slot;
@@ -941,9 +1003,9 @@ __global__ void y_kernel(DevProblem P, double *Ax64, int slot) {
     const int dsub = blockIdx.x;
     double s = 0.0;
     for (int e = P.loff[dsub] + threadIdx.x; e < P.loff[dsub + 1]; e += blockDim.x) {
-        const double yv = P.z[e] - gt_alpha(P, e, P.alpha);
+        const double yv = __ldg(P.z + e) - gt_alpha(P, e, P.alpha);
         P.y[e] = yv;
-        s += yv * P.w[e] * P.minv[e];
+        s += yv * __ldg(P.w + e) * __ldg(P.minv + e);
         P.Ap[e] = 0.0;
         Ax64[e] = 0.0;
     }
@@ -958,7 +1020,7 @@ __global__ void zero_vT_kernel(DevProblem P, int slot) {
 }
 
 // p = y + beta p, x += alpha p, r -= alpha assemble(Ap), d = G r, convergence check.
-__global__ void update_kernel(DevProblem P, int slot) {
+__global__ void __launch_bounds__(1024) update_kernel(DevProblem P, int slot) {
     pdl_enter();
     extern __shared__ double rs_s[];
     __shared__ double sh[32 * KMAX];
@@ -972,12 +1034,12 @@ __global__ void update_kernel(DevProblem P, int slot) {
     const int dsub = blockIdx.x;
     const int e0 = P.loff[dsub], e1 = P.loff[dsub + 1];
     for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-        const double pv = P.y[e] + beta * P.p[e];
+        const int q = __ldg(P.partner + e);
+        const double ap = __ldg(P.Ap + e) + (q >= 0 ? __ldg(P.Ap + q) : 0.0);
+        const double pv = __ldg(P.y + e) + beta * P.p[e];
         P.p[e] = pv;
         P.x[e] += alpha * pv;
-        const int q = P.partner[e];
-        const double a = P.Ap[e] + (q >= 0 ? P.Ap[q] : 0.0);
-        const double rv = P.r[e] - alpha * a;
+        const double rv = P.r[e] - alpha * ap;
         P.r[e] = rv;
         rs_s[e - e0] = rv;
     }
@@ -1903,6 +1965,9 @@ struct GpuSolver::Impl {
     void launch_implicit(int mode, const double *src, const double *src2, double *out, int slot);
     void release(void *p);        // frees one allocation of `allocs` before the solver goes
     int max_tn = 0, max_tn_dir = 0, max_nt = 0, max_ni = 0;
+    // threads of the per-subdomain vector kernels of the PCG loop: as many as keep every subdomain's
+    // CTA resident in one wave (2048 threads per SM), so that each thread has about one row
+    int tpbv = 256;
     std::vector<int> h_lam;       // L row -> lambda
     int *d_lam = nullptr;         // the same on the device
     std::vector<int> h_loff;
@@ -2739,7 +2804,7 @@ void GpuSolver::Impl::launch_iteration(int slot) {
         // residual replacement r = b - F64 x when the previous update asked for it
         launch_tiles(F64, 3, P.x, nullptr, Ax64, slot);
         launch_hybrid_F(P.x, Ax64, slot, 3, nullptr);
-        launch_pdl(r0_kernel, dim3(nd), dim3(TPB), sizeof(double) * max_ni, stream, P, Ax64, 1, slot);
+        launch_pdl(r0_kernel, dim3(nd), dim3(tpbv), sizeof(double) * max_ni, stream, P, Ax64, 1, slot);
     }
     launch_pdl(coarse_kernel, dim3(cgrid), dim3(256), 0, stream, P, P.d, P.alpha, slot, 1);
     const size_t tsm = sizeof(double) * (size_t)(max_ni + max_nt);
@@ -2755,15 +2820,15 @@ void GpuSolver::Impl::launch_iteration(int slot) {
                        slot);
             launch_tiles(Dir, 2, P.uT, nullptr, P.vT, slot);
         }
-        launch_pdl(z_kernel, dim3(nd), dim3(TPB), sizeof(double) * max_ni, stream, P, slot);
+        launch_pdl(z_kernel, dim3(nd), dim3(tpbv), sizeof(double) * max_ni, stream, P, slot);
         launch_pdl(coarse_kernel, dim3(cgrid), dim3(256), 0, stream, P, P.d, P.alpha, slot, 1);
-        launch_pdl(y_kernel, dim3(nd), dim3(TPB), 0, stream, P, Ax64, slot);
+        launch_pdl(y_kernel, dim3(nd), dim3(tpbv), 0, stream, P, Ax64, slot);
     } else {
         launch_pdl(zero2_kernel, dim3((P.NL + 255) / 256), dim3(256), 0, stream, P.Ap, Ax64, P.NL);
     }
     launch_tiles(Fop, 1, P.y, P.p, P.Ap, slot);
     launch_hybrid_F(nullptr, P.Ap, slot, 1, P.scal + SC_PAP);   // p = y + beta p formed on the fly
-    launch_pdl(update_kernel, dim3(nd), dim3(TPB), sizeof(double) * max_ni, stream, P, slot);
+    launch_pdl(update_kernel, dim3(nd), dim3(tpbv), sizeof(double) * max_ni, stream, P, slot);
 }
 
 int GpuSolver::Impl::kernels_per_iteration() const {
@@ -2850,6 +2915,10 @@ void GpuSolver::upload(const Decomposition &dec, const Prep &prep, const SolveOp
     const int NL = loff[nd], NT = toff[nd];
     I.n_lambda = dec.n_lambda;
     I.h_loff = loff;
+    {
+        const int per_sm = std::max(1, (nd + I.nsm - 1) / I.nsm);
+        I.tpbv = std::max(128, std::min(1024, (2048 / per_sm) / 32 * 32));
+    }
     I.h_lam.resize(NL);
     int KS = 1;
     for (int d = 0; d < nd; ++d) KS = std::max(KS, prep.sub[d].dnk);
