@@ -3775,6 +3775,9 @@ namespace {
 
 
 constexpr int UNR = 4;   // rows in flight per thread in the block vector kernels
+// resident CTAs per SM of the flat block vector kernels: the register cap that keeps 4 x 256 threads
+// per SM (the uncapped kernels took up to 94 registers, 2 CTAs per SM, and stalled on latency)
+constexpr int FLAT_MIN_BLOCKS = 4;
 
 // per-column sum over a CTA: threads with the same column (tid % nr) are combined
 __device__ void block_sum_cols(double v, int nr, double *sh /* >= 8*32 */, double *out_col /* nr */) {
@@ -3996,7 +3999,7 @@ __global__ void __launch_bounds__(TPBB) bz_kernel(DevProblem P, BlockDev B, int 
 
 // u_T = B^T W w over all touched DOFs (v_T = u_T for the weight-function preconditioner)
 template <int PRECOND>
-__global__ void __launch_bounds__(256) bu_flat_kernel(DevProblem P, BlockDev B, int slot) {
+__global__ void __launch_bounds__(256, FLAT_MIN_BLOCKS) bu_flat_kernel(DevProblem P, BlockDev B, int slot) {
     pdl_enter();
     const int iter = P.st->iter_base + slot;
     if (skip_iter(P.st, iter)) return;
@@ -4058,7 +4061,7 @@ __device__ __forceinline__ double2 gt_alpha_colk2(const DevProblem &P, int e, in
     return r;
 }
 
-__global__ void __launch_bounds__(256) bell_flat2_kernel(DevProblem P, BlockDev B, int slot) {
+__global__ void __launch_bounds__(256, FLAT_MIN_BLOCKS) bell_flat2_kernel(DevProblem P, BlockDev B, int slot) {
     pdl_enter();
     const int iter = P.st->iter_base + slot;
     if (skip_iter(P.st, iter)) return;
@@ -4095,7 +4098,7 @@ __global__ void __launch_bounds__(256) bell_flat2_kernel(DevProblem P, BlockDev 
 // w = r - G^T alpha, |w_j|^2 (and y = w, rho_j = |w_j|^2 without a preconditioner); two columns
 // per thread, as in bell_flat2_kernel
 template <int PRECOND, int KC>
-__global__ void __launch_bounds__(256) bw_flat2_kernel(DevProblem P, BlockDev B, int slot) {
+__global__ void __launch_bounds__(256, FLAT_MIN_BLOCKS) bw_flat2_kernel(DevProblem P, BlockDev B, int slot) {
     pdl_enter();
     __shared__ double sh[8 * 32];
     __shared__ double cols[32];
@@ -4137,7 +4140,7 @@ __global__ void __launch_bounds__(256) bw_flat2_kernel(DevProblem P, BlockDev B,
 }
 
 template <int KC>
-__global__ void __launch_bounds__(256) by_flat2_kernel(DevProblem P, BlockDev B, int slot) {
+__global__ void __launch_bounds__(256, FLAT_MIN_BLOCKS) by_flat2_kernel(DevProblem P, BlockDev B, int slot) {
     pdl_enter();
     __shared__ double sh[8 * 32];
     __shared__ double cols[32];
@@ -4195,7 +4198,10 @@ __global__ void bp_kernel(DevProblem P, BlockDev B, int slot) {
     }
 }
 
-__global__ void __launch_bounds__(TPBB) bupdate_kernel(DevProblem P, BlockDev B, int slot) {
+// Two CTAs of 1024 threads per SM (32 registers, two rows in flight per thread): with 60 registers
+// only one fitted, and the 512 subdomains of the heat workload ran in four waves.
+__global__ void __launch_bounds__(TPBB, 2) bupdate_kernel(DevProblem P, BlockDev B, int slot) {
+    constexpr int UNR = 2;
     pdl_enter();
     __shared__ double sh[32 * 32];
     const int iter = P.st->iter_base + slot;
@@ -5302,7 +5308,8 @@ void GpuSolver::Impl::ensure_block(int nr) {
     B.e = alloc<double>((size_t)P.nP * nr);
     CUDA_CHECK(cudaMemset(B.alpha, 0, sizeof(double) * (size_t)(nK + P.KS) * nr));
     // persistent grid of the flat block kernels: rows of all subdomains, UNR per thread in flight
-    blk.flat_grid = std::max(1, std::min(nsm * 8, (int)(((long long)NL * nr + 256LL * UNR - 1) / (256LL * UNR))));
+    blk.flat_grid =
+        std::max(1, std::min(nsm * FLAT_MIN_BLOCKS, (int)(((long long)NL * nr + 256LL * UNR - 1) / (256LL * UNR))));
     B.part = alloc<double>((size_t)2 * std::max(nd, blk.flat_grid) * nr);
     B.scal = alloc<double>((size_t)SC_COUNT * nr);
     B.rho_hist = alloc<double>((size_t)(opt.max_iterations + 64) * nr);
