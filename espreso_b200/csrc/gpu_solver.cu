@@ -1040,7 +1040,7 @@ struct LoopCtl {
     cudaGraphConditionalHandle h_loop, h_repl;
 };
 
-__global__ void __launch_bounds__(1024) update_kernel(DevProblem P, int slot, LoopCtl lc) {
+__global__ void __launch_bounds__(1024) update_kernel(DevProblem P, int slot) {
     pdl_enter();
     extern __shared__ double rs_s[];
     __shared__ double sh[32 * KMAX];
@@ -1094,7 +1094,6 @@ __global__ void __launch_bounds__(1024) update_kernel(DevProblem P, int slot, Lo
                 st->replacements += 1;
             }
         }
-        if (lc.on) cudaGraphSetConditional(lc.h_repl, st->replace_iter == iter + 1 ? 1u : 0u);
     }
 }
 
@@ -1103,14 +1102,17 @@ __global__ void chunk_end_kernel(DevProblem P, int chunk) {
     if (threadIdx.x == 0 && blockIdx.x == 0) P.st->iter_base += chunk;
 }
 
-// End of one pass of the loop graph: always runs (no skip test), advances the iteration and keeps
-// the WHILE node going only while the solve has neither converged, nor reached max_iterations, nor
-// recorded a pipeline error, so the loop ends after at most max_iterations passes.
+// End of one pass of the loop graph: always runs (no skip test), advances the iteration, asks for the
+// residual replacement that the update requested for the next iteration, and keeps the WHILE node
+// going only while the solve has neither converged, nor reached max_iterations, nor recorded a
+// pipeline error, so the loop ends after at most max_iterations passes.  (A separate kernel, so that
+// the kernels of the chunked graphs make no device-runtime call.)
 __global__ void loop_end_kernel(DevProblem P, LoopCtl lc) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         DevState *st = P.st;
         const int done = ++st->iter_base;
         const bool more = st->conv_iter < 0 && done < st->max_it && st->error == 0;
+        cudaGraphSetConditional(lc.h_repl, (more && st->replace_iter == done) ? 1u : 0u);
         cudaGraphSetConditional(lc.h_loop, more ? 1u : 0u);
     }
 }
@@ -2874,7 +2876,8 @@ void GpuSolver::Impl::launch_iteration(int slot, bool with_replacement, LoopCtl 
     }
     launch_tiles(Fop, 1, P.y, P.p, P.Ap, slot);
     launch_hybrid_F(nullptr, P.Ap, slot, 1, P.scal + SC_PAP);   // p = y + beta p formed on the fly
-    launch_pdl(update_kernel, dim3(nd), dim3(tpbv), sizeof(double) * max_ni, stream, P, slot, lc);
+    launch_pdl(update_kernel, dim3(nd), dim3(tpbv), sizeof(double) * max_ni, stream, P, slot);
+    (void)lc;
 }
 
 int GpuSolver::Impl::kernels_per_iteration() const {
