@@ -4117,7 +4117,7 @@ __global__ void __launch_bounds__(TPBB) bz_kernel(DevProblem P, BlockDev B, int 
 
 // u_T = B^T W w over all touched DOFs (v_T = u_T for the weight-function preconditioner)
 template <int PRECOND>
-__global__ void __launch_bounds__(256, FLAT_MIN_BLOCKS) bu_flat_kernel(DevProblem P, BlockDev B, int slot) {
+__global__ void __launch_bounds__(256) bu_flat_kernel(DevProblem P, BlockDev B, int slot) {
     pdl_enter();
     const int iter = P.st->iter_base + slot;
     if (skip_iter(P.st, iter)) return;
@@ -5666,6 +5666,8 @@ void GpuSolver::Impl::launch_block_iteration(int slot) {
     }
     launch_pdl(bcoarse_kernel, dim3(cgrid), dim3(256), 0, stream, P, B, B.d, B.alpha, slot, 1);
     const int fgrid = blk.flat_grid;
+    // the T-space gather has no register pressure (50 registers): twice the CTAs of the capped kernels
+    const int ugrid = 2 * blk.flat_grid;
 #define BW(PC)                                                                              \
     switch (P.KS) {                                                                         \
     case 1: launch_pdl(bw_flat2_kernel<PC, 1>, dim3(fgrid), dim3(256), 0, stream, P, B, slot); break;  \
@@ -5676,18 +5678,18 @@ void GpuSolver::Impl::launch_block_iteration(int slot) {
     case PREC_NONE: BW(PREC_NONE) break;
     case PREC_LUMPED:
         BW(PREC_LUMPED)
-        launch_pdl(bu_flat_kernel<PREC_LUMPED>, dim3(fgrid), dim3(256), 0, stream, P, B, slot);
+        launch_pdl(bu_flat_kernel<PREC_LUMPED>, dim3(ugrid), dim3(256), 0, stream, P, B, slot);
         launch_pdl(bell_flat2_kernel, dim3(fgrid), dim3(256), 0, stream, P, B, slot);
         break;
     case PREC_DIRICHLET:
         // u_T = B^T W w, then v_T = S_dir u_T (FP64 SYMM over the Dirichlet blocks)
         BW(PREC_WEIGHT)
-        launch_pdl(bu_flat_kernel<PREC_LUMPED>, dim3(fgrid), dim3(256), 0, stream, P, B, slot);
+        launch_pdl(bu_flat_kernel<PREC_LUMPED>, dim3(ugrid), dim3(256), 0, stream, P, B, slot);
         launch_symm(Dir, false, B.uT, nullptr, B.vT, slot, 2);
         break;
     default:
         BW(PREC_WEIGHT)
-        launch_pdl(bu_flat_kernel<PREC_WEIGHT>, dim3(fgrid), dim3(256), 0, stream, P, B, slot);
+        launch_pdl(bu_flat_kernel<PREC_WEIGHT>, dim3(ugrid), dim3(256), 0, stream, P, B, slot);
         break;
     }
 #undef BW
