@@ -3956,6 +3956,23 @@ __device__ void g_dot_cols(const DevProblem &P, const BlockDev &B, int dsub, con
     }
 }
 
+// G_i v per column from per-thread partial sums gk[k] = sum over the thread's elements of
+// G[e, k] v[e, j] (every thread of the CTA on one column j = threadIdx.x & (nr - 1)): one pass over
+// the rows instead of one per kernel vector
+template <int KC>
+__device__ void g_cols_reduce(const DevProblem &P, const BlockDev &B, int dsub, double (&gk)[KC], double *sh) {
+    __shared__ double cols[32];
+    const int nk = P.kof[dsub + 1] - P.kof[dsub];
+#pragma unroll
+    for (int k = 0; k < KC; ++k) {
+        if (k < nk) {   // uniform over the CTA
+            block_sum_cols(gk[k], B.nr, sh, cols);
+            if (threadIdx.x < B.nr) B.d[(size_t)(P.kof[dsub] + k) * B.nr + threadIdx.x] = cols[threadIdx.x];
+            __syncthreads();
+        }
+    }
+}
+
 __device__ __forceinline__ double gt_alpha_col(const DevProblem &P, int e, int j, int nr, const double *a) {
     double s = 0.0;
     const int nk = P.rnk[e], ko = P.rkof[e], pn = P.pnk[e], po = P.pkof[e];
@@ -4081,6 +4098,9 @@ __global__ void btol_kernel(DevProblem P, BlockDev B) {
     }
 }
 
+// KC: the kernel width (1, 6: G z accumulated in registers while z is formed; 0: per-row counts,
+// a second pass over z)
+template <int KC>
 __global__ void __launch_bounds__(TPBB) bz_kernel(DevProblem P, BlockDev B, int slot) {
     pdl_enter();
     __shared__ double sh[32 * 32];
@@ -4089,6 +4109,10 @@ __global__ void __launch_bounds__(TPBB) bz_kernel(DevProblem P, BlockDev B, int 
     const int nr = B.nr, dsub = blockIdx.x;
     const int e0 = P.loff[dsub], e1 = P.loff[dsub + 1];
     const int cnt = (e1 - e0) * nr;
+    constexpr int NG = KC > 0 ? KC : 1;
+    double gk[NG];
+#pragma unroll
+    for (int k = 0; k < NG; ++k) gk[k] = 0.0;
     for (int i0 = threadIdx.x; i0 < cnt; i0 += UNR * blockDim.x) {
         double zv[UNR];
 #pragma unroll
@@ -4104,11 +4128,19 @@ __global__ void __launch_bounds__(TPBB) bz_kernel(DevProblem P, BlockDev B, int 
 #pragma unroll
         for (int u = 0; u < UNR; ++u) {
             const int i = i0 + u * blockDim.x;
-            if (i < cnt) B.z[(size_t)e0 * nr + i] = zv[u];
+            if (i < cnt) {
+                B.z[(size_t)e0 * nr + i] = zv[u];
+                if (KC > 0) {
+                    const double *g = P.Gl + (size_t)(e0 + (i >> B.lg)) * NG;
+#pragma unroll
+                    for (int k = 0; k < NG; ++k) gk[k] += __ldg(g + k) * zv[u];
+                }
+            }
         }
     }
     __syncthreads();
-    g_dot_cols(P, B, dsub, B.z + (size_t)e0 * nr, sh);
+    if (KC > 0) g_cols_reduce<NG>(P, B, dsub, gk, sh);
+    else g_dot_cols(P, B, dsub, B.z + (size_t)e0 * nr, sh);
 }
 
 // ---- flat block kernels: a persistent grid over all rows (no per-subdomain reduction needed)
@@ -4318,8 +4350,13 @@ __global__ void bp_kernel(DevProblem P, BlockDev B, int slot) {
 
 // Two CTAs of 1024 threads per SM (32 registers, two rows in flight per thread): with 60 registers
 // only one fitted, and the 512 subdomains of the heat workload ran in four waves.
+template <int KC>
 __global__ void __launch_bounds__(TPBB, 2) bupdate_kernel(DevProblem P, BlockDev B, int slot) {
     constexpr int UNR = 2;
+    constexpr int NG = KC > 0 ? KC : 1;
+    double gk[NG];
+#pragma unroll
+    for (int k = 0; k < NG; ++k) gk[k] = 0.0;
     pdl_enter();
     __shared__ double sh[32 * 32];
     const int iter = P.st->iter_base + slot;
@@ -4353,12 +4390,27 @@ __global__ void __launch_bounds__(TPBB, 2) bupdate_kernel(DevProblem P, BlockDev
                 if (i < cnt) {
                     const size_t o = (size_t)e0 * nr + i;
                     B.x[o] = xv[u] + alpha * pv[u];
-                    B.r[o] = rv[u] - alpha * av[u];
+                    const double rn = rv[u] - alpha * av[u];
+                    B.r[o] = rn;
+                    if (KC > 0) {
+                        const double *g = P.Gl + (size_t)(e0 + (i >> B.lg)) * NG;
+#pragma unroll
+                        for (int k = 0; k < NG; ++k) gk[k] += __ldg(g + k) * rn;
+                    }
                 }
             }
         }
+    else if (KC > 0)
+        // a converged column keeps its r: its G r is still the coarse input of the next iteration
+        for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+            const double *g = P.Gl + (size_t)(e0 + (i >> B.lg)) * NG;
+            const double rv = B.r[(size_t)e0 * nr + i];
+#pragma unroll
+            for (int k = 0; k < NG; ++k) gk[k] += __ldg(g + k) * rv;
+        }
     __syncthreads();
-    g_dot_cols(P, B, dsub, B.r + (size_t)e0 * nr, sh);
+    if (KC > 0) g_cols_reduce<NG>(P, B, dsub, gk, sh);
+    else g_dot_cols(P, B, dsub, B.r + (size_t)e0 * nr, sh);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         DevState *st = P.st;
         bool replace = false;
@@ -5694,7 +5746,11 @@ void GpuSolver::Impl::launch_block_iteration(int slot) {
     }
 #undef BW
     if (opt.precond != PREC_NONE) {
-        launch_pdl(bz_kernel, dim3(nd), dim3(TPBB), 0, stream, P, B, slot);
+        switch (P.KS) {
+        case 1: launch_pdl(bz_kernel<1>, dim3(nd), dim3(TPBB), 0, stream, P, B, slot); break;
+        case 6: launch_pdl(bz_kernel<6>, dim3(nd), dim3(TPBB), 0, stream, P, B, slot); break;
+        default: launch_pdl(bz_kernel<0>, dim3(nd), dim3(TPBB), 0, stream, P, B, slot); break;
+        }
         launch_pdl(bcoarse_kernel, dim3(cgrid), dim3(256), 0, stream, P, B, B.d, B.alpha, slot, 1);
         switch (P.KS) {
         case 1: launch_pdl(by_flat2_kernel<1>, dim3(fgrid), dim3(256), 0, stream, P, B, slot); break;
@@ -5707,7 +5763,11 @@ void GpuSolver::Impl::launch_block_iteration(int slot) {
     if (mixed) launch_symm(Flow, true, nullptr, B.p32, B.Ap, slot, 1);
     else launch_symm(F64, false, B.p, nullptr, B.Ap, slot, 1);
     launch_block_hybrid(B.p, B.Ap, slot, 1, B.scal + SC_PAP * blk.nr);
-    launch_pdl(bupdate_kernel, dim3(nd), dim3(TPBB), 0, stream, P, B, slot);
+    switch (P.KS) {
+    case 1: launch_pdl(bupdate_kernel<1>, dim3(nd), dim3(TPBB), 0, stream, P, B, slot); break;
+    case 6: launch_pdl(bupdate_kernel<6>, dim3(nd), dim3(TPBB), 0, stream, P, B, slot); break;
+    default: launch_pdl(bupdate_kernel<0>, dim3(nd), dim3(TPBB), 0, stream, P, B, slot); break;
+    }
 }
 
 // panels of the mixed blocks for the asynchronous tensor-core SYMM (built before any graph capture)
