@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--precision", type=float, default=1e-8)
     ap.add_argument("--tile-kernel", type=int, default=-1,
                     help="-1 autotuned (default), 0 register prefetch, 1 TMA bulk pipeline")
-    ap.add_argument("--delta", type=float, default=0.01, help="residual replacement threshold")
+    ap.add_argument("--delta", type=float, default=0.003, help="residual replacement threshold")
     ap.add_argument("--nrhs", type=int, default=32, help="load cases of the batched (multi-RHS) leg, 0 to skip")
     ap.add_argument("--method", type=int, default=0, choices=[0, 1],
                     help="FETI_METHOD: 0 Total FETI, 1 Hybrid Total FETI on the config's clusters")

@@ -59,7 +59,7 @@ namespace {
 std::mutex g_mutex;
 std::list<FETI4IStructMatrix *> g_matrices;
 std::list<FETI4IStructInstance *> g_instances;
-double g_ext[FETI4I_EXT_OPTIONS_SIZE] = {0, 1, 0, 48, 16, 0.01, 0, 0, 1, 1, 1, 1, 0, 0};
+double g_ext[FETI4I_EXT_OPTIONS_SIZE] = {0, 1, 0, 48, 16, 0.003, 0, 0, 1, 1, 1, 1, 0, 0};
 
 template <typename F>
 void guarded(F &&f) {

@@ -28,7 +28,7 @@ struct SolveOptions {
     bool autotune = true;              // time the variants and item granularities per size class at upload
     bool symm_tensor = true;           // multi-RHS FP32 SYMM on the tensor cores (3xTF32) instead of CUDA cores
     bool schur_explicit = true;        // false: F applied through the K^+ factor (no stored S_i; FP64, Total FETI)
-    double reliable_delta = 0.01;      // residual replacement threshold (mixed precision)
+    double reliable_delta = 0.003;     // residual replacement threshold (mixed precision)
     bool use_graph = true;
 };
 

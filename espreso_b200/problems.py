@@ -306,7 +306,7 @@ def make_instance(problem: Problem, iopts=None, ropts=None, ext=None, batched=Tr
             F.set_extended(F.EXT_AUTOTUNE, 1)
             F.set_extended(F.EXT_SYMM_TENSOR, 1)
             F.set_extended(F.EXT_DEVICE_PREP, 1)
-            F.set_extended(F.EXT_RELIABLE_DELTA, 0.01)
+            F.set_extended(F.EXT_RELIABLE_DELTA, 0.003)
             F.set_extended(F.EXT_SCHUR_EXPLICIT, 1)
             F.set_extended(F.EXT_OWNED_FIRST, 0)
             F.set_extended(F.EXT_OWNED_COUNT, 0)

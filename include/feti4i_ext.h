@@ -54,7 +54,7 @@ typedef enum {
     FETI4I_EXT_HOST_ONLY,        /* 1: run the host preprocessing only (no GPU; FETI4ISolve fails) */
     FETI4I_EXT_TILES_PER_ITEM,   /* work-queue granularity of the Schur SYMV (autotuned default 48) */
     FETI4I_EXT_GRAPH_CHUNK,      /* PCG iterations per captured CUDA graph (default 16) */
-    FETI4I_EXT_RELIABLE_DELTA,   /* mixed precision: residual replacement threshold (default 0.01) */
+    FETI4I_EXT_RELIABLE_DELTA,   /* mixed precision: residual replacement threshold (default 0.003) */
     FETI4I_EXT_HOST_THREADS,     /* OpenMP threads of the preprocessing (0: all) */
     FETI4I_EXT_TILE_KERNEL,      /* Schur SYMV: 0 register-prefetch loads, 1 TMA bulk-copy pipeline */
     FETI4I_EXT_AUTOTUNE,         /* 1 (default): time both SYMV variants and the work-item sizes per size class */
