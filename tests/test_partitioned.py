@@ -90,11 +90,14 @@ def test_partitioned_matches_one_process(two_ranks, prec):
     ud = direct_u(P).ravel()
     for rank in (0, 1):
         lam, alpha, it, u, coll = two_ranks[rank][prec]
-        assert it == it1
+        # the allreduce adds the blocks' parts in another order than one process does, so the
+        # last bits differ and the stop test may pass one iteration apart
+        assert abs(it - it1) <= 1
         assert np.linalg.norm(lam - lam1) <= 1e-10 * np.linalg.norm(lam1)
         assert np.linalg.norm(u - ud) <= 1e-8 * np.linalg.norm(ud)
         # one allreduce of the dual vector per F apply (and per preconditioner apply), b and u once
         per_it = 1 if prec == OF.PREC_NONE else 2
         assert coll == 1 + 1 + per_it * it + 1
+    assert two_ranks[0][prec][2] == two_ranks[1][prec][2]   # the processes take the same iterations
     # both processes hold the same replicated iterates
     assert np.array_equal(two_ranks[0][prec][0], two_ranks[1][prec][0])
