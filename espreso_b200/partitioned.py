@@ -114,10 +114,10 @@ class PartitionedSolver:
         r = torch.from_numpy(np.concatenate(rows))
         c = torch.from_numpy(np.concatenate(cols))
         v = torch.from_numpy(np.concatenate(vals))
-        Gd = torch.sparse_coo_tensor(torch.stack([r, c]), v, (self.n_kern, self.n_lambda),
-                                     check_invariants=True).coalesce()
         with warnings.catch_warnings():
-            warnings.simplefilter("ignore", UserWarning)   # torch marks sparse CSR as beta
+            warnings.simplefilter("ignore", UserWarning)   # torch marks its sparse tensors as beta
+            Gd = torch.sparse_coo_tensor(torch.stack([r, c]), v, (self.n_kern, self.n_lambda),
+                                         check_invariants=True).coalesce()
             self.G = Gd.to_sparse_csr().to(self.device)
             self.Gt = Gd.t().coalesce().to_sparse_csr().to(self.device)
         GGt = (Gd.to_dense() @ Gd.to_dense().t()).to(self.device)
