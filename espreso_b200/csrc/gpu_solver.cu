@@ -4289,6 +4289,44 @@ __global__ void __launch_bounds__(256, FLAT_MIN_BLOCKS) bw_flat2_kernel(DevProbl
         grid_total_cols(cols, B.part + (size_t)gridDim.x * nr, nr, B.done + DONE_RHO, B.scal + SC_RHO * nr);
 }
 
+// w = r - G^T alpha and u_T = B^T W w in one pass over the touched DOFs: a thread takes one T entry
+// and two columns, forms w at the (one to three) rows of that DOF, writes them, and adds
+// ws_e w_e into u_T; |w_j|^2 as in bw_flat2_kernel.  Every row carries exactly one T entry, so every
+// w is formed once.  WEIGHT also writes v_T = u_T.  Replaces bw_flat2 + bu_flat: w is not read back.
+template <int PRECOND, int KC>
+__global__ void __launch_bounds__(256, FLAT_MIN_BLOCKS) bwu_flat2_kernel(DevProblem P, BlockDev B, int slot) {
+    pdl_enter();
+    __shared__ double sh[8 * 32];
+    __shared__ double cols[32];
+    const int iter = P.st->iter_base + slot;
+    if (skip_iter(P.st, iter)) return;
+    const int nr = B.nr, lh = B.lg - 1;
+    const long long cnt = (long long)P.NT * (nr >> 1), stride = (long long)gridDim.x * blockDim.x;
+    double s0 = 0.0, s1 = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += stride) {
+        const int t = (int)(i >> lh), j = 2 * (int)(i & ((nr >> 1) - 1));
+        const int q0 = __ldg(P.trow_ptr + t), q1 = __ldg(P.trow_ptr + t + 1);
+        double2 u = make_double2(0.0, 0.0);
+        for (int q = q0; q < q1; ++q) {
+            const int e = __ldg(P.trow_idx + q);
+            const size_t o = (size_t)e * nr + j;
+            const double2 rv = *reinterpret_cast<const double2 *>(B.r + o);
+            const double2 ga = gt_alpha_colk2<KC>(P, e, j, nr, B.alpha);
+            const double2 wv = make_double2(rv.x - ga.x, rv.y - ga.y);
+            *reinterpret_cast<double2 *>(B.w + o) = wv;
+            const double mv = __ldg(P.minv + e), ws = __ldg(P.ws + e);
+            s0 += wv.x * wv.x * mv;
+            s1 += wv.y * wv.y * mv;
+            u.x += ws * wv.x;
+            u.y += ws * wv.y;
+        }
+        *reinterpret_cast<double2 *>(B.uT + (size_t)t * nr + j) = u;
+        if (PRECOND == PREC_WEIGHT) *reinterpret_cast<double2 *>(B.vT + (size_t)t * nr + j) = u;
+    }
+    block_sum_cols2(s0, s1, nr, sh, cols);
+    grid_total_cols(cols, B.part, nr, B.done + DONE_W, B.scal + SC_WN2 * nr);
+}
+
 template <int KC>
 __global__ void __launch_bounds__(256, FLAT_MIN_BLOCKS) by_flat2_kernel(DevProblem P, BlockDev B, int slot) {
     pdl_enter();
@@ -5577,6 +5615,16 @@ static void symm_launch(int nsm, int ncta, size_t sm, cudaStream_t st, TileSetDe
                mode);
 }
 
+// w and u_T of the block PCG in one kernel (bwu_flat2_kernel); FETI4I_BLOCK_BWU=0 runs the two
+// kernels it replaces
+static bool bwu_enabled() {
+    static const bool on = [] {
+        const char *e = getenv("FETI4I_BLOCK_BWU");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 static bool symm_mma_enabled() {
     static const bool on = [] {
         const char *e = getenv("FETI4I_SYMM_MMA");
@@ -5726,24 +5774,41 @@ void GpuSolver::Impl::launch_block_iteration(int slot) {
     case 6: launch_pdl(bw_flat2_kernel<PC, 6>, dim3(fgrid), dim3(256), 0, stream, P, B, slot); break;  \
     default: launch_pdl(bw_flat2_kernel<PC, 0>, dim3(fgrid), dim3(256), 0, stream, P, B, slot); break; \
     }
+#define BWU(PC)                                                                              \
+    switch (P.KS) {                                                                          \
+    case 1: launch_pdl(bwu_flat2_kernel<PC, 1>, dim3(fgrid), dim3(256), 0, stream, P, B, slot); break;  \
+    case 6: launch_pdl(bwu_flat2_kernel<PC, 6>, dim3(fgrid), dim3(256), 0, stream, P, B, slot); break;  \
+    default: launch_pdl(bwu_flat2_kernel<PC, 0>, dim3(fgrid), dim3(256), 0, stream, P, B, slot); break; \
+    }
+    const bool fused = bwu_enabled();
     switch (opt.precond) {
     case PREC_NONE: BW(PREC_NONE) break;
     case PREC_LUMPED:
-        BW(PREC_LUMPED)
-        launch_pdl(bu_flat_kernel<PREC_LUMPED>, dim3(ugrid), dim3(256), 0, stream, P, B, slot);
+        if (fused) { BWU(PREC_LUMPED) }
+        else {
+            BW(PREC_LUMPED)
+            launch_pdl(bu_flat_kernel<PREC_LUMPED>, dim3(ugrid), dim3(256), 0, stream, P, B, slot);
+        }
         launch_pdl(bell_flat2_kernel, dim3(fgrid), dim3(256), 0, stream, P, B, slot);
         break;
     case PREC_DIRICHLET:
         // u_T = B^T W w, then v_T = S_dir u_T (FP64 SYMM over the Dirichlet blocks)
-        BW(PREC_WEIGHT)
-        launch_pdl(bu_flat_kernel<PREC_LUMPED>, dim3(ugrid), dim3(256), 0, stream, P, B, slot);
+        if (fused) { BWU(PREC_LUMPED) }
+        else {
+            BW(PREC_WEIGHT)
+            launch_pdl(bu_flat_kernel<PREC_LUMPED>, dim3(ugrid), dim3(256), 0, stream, P, B, slot);
+        }
         launch_symm(Dir, false, B.uT, nullptr, B.vT, slot, 2);
         break;
     default:
-        BW(PREC_WEIGHT)
-        launch_pdl(bu_flat_kernel<PREC_WEIGHT>, dim3(ugrid), dim3(256), 0, stream, P, B, slot);
+        if (fused) { BWU(PREC_WEIGHT) }
+        else {
+            BW(PREC_WEIGHT)
+            launch_pdl(bu_flat_kernel<PREC_WEIGHT>, dim3(ugrid), dim3(256), 0, stream, P, B, slot);
+        }
         break;
     }
+#undef BWU
 #undef BW
     if (opt.precond != PREC_NONE) {
         switch (P.KS) {
