@@ -4219,29 +4219,35 @@ __global__ void __launch_bounds__(256, FLAT_MIN_BLOCKS) bell_flat2_kernel(DevPro
     const long long cnt = (long long)P.NT * (nr >> 1), stride = (long long)gridDim.x * blockDim.x;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += stride) {
         const int t = (int)(i >> lh), j = 2 * (int)(i & ((nr >> 1) - 1));
-        const int t0 = P.tbase[t], ts = P.tslot[t];
+        const int t0 = __ldg(P.tbase + t), ts = __ldg(P.tslot + t);
         const int sl = ts >> 5, ln = ts & 31;
-        const int base = P.ell_ptr[sl], wd = P.ell_w[sl];
-        double2 s0 = make_double2(0.0, 0.0), s1 = make_double2(0.0, 0.0);
+        const int base = __ldg(P.ell_ptr + sl), wd = __ldg(P.ell_w + sl);
+        const double2 *uT = reinterpret_cast<const double2 *>(B.uT);
+        const size_t hn = (size_t)(nr >> 1), jh = (size_t)(j >> 1);
+        // four entries in flight: the gathered u_T rows come from L2, one latency per four entries
+        double2 s0 = make_double2(0.0, 0.0), s1 = s0, s2 = s0, s3 = s0;
         int q = 0;
-        for (; q + 1 < wd; q += 2) {
+        for (; q + 3 < wd; q += 4) {
             const int o = base + q * 32 + ln;
-            const double v0 = P.ell_val[o], v1 = P.ell_val[o + 32];
-            const double2 u0 = *reinterpret_cast<const double2 *>(B.uT + (size_t)(t0 + P.ell_col[o]) * nr + j);
-            const double2 u1 = *reinterpret_cast<const double2 *>(B.uT + (size_t)(t0 + P.ell_col[o + 32]) * nr + j);
-            s0.x += v0 * u0.x;
-            s0.y += v0 * u0.y;
-            s1.x += v1 * u1.x;
-            s1.y += v1 * u1.y;
+            const double v0 = __ldg(P.ell_val + o), v1 = __ldg(P.ell_val + o + 32), v2 = __ldg(P.ell_val + o + 64),
+                         v3 = __ldg(P.ell_val + o + 96);
+            const double2 u0 = __ldg(uT + (size_t)(t0 + __ldg(P.ell_col + o)) * hn + jh);
+            const double2 u1 = __ldg(uT + (size_t)(t0 + __ldg(P.ell_col + o + 32)) * hn + jh);
+            const double2 u2 = __ldg(uT + (size_t)(t0 + __ldg(P.ell_col + o + 64)) * hn + jh);
+            const double2 u3 = __ldg(uT + (size_t)(t0 + __ldg(P.ell_col + o + 96)) * hn + jh);
+            s0.x += v0 * u0.x; s0.y += v0 * u0.y;
+            s1.x += v1 * u1.x; s1.y += v1 * u1.y;
+            s2.x += v2 * u2.x; s2.y += v2 * u2.y;
+            s3.x += v3 * u3.x; s3.y += v3 * u3.y;
         }
-        if (q < wd) {
+        for (; q < wd; ++q) {
             const int o = base + q * 32 + ln;
-            const double v0 = P.ell_val[o];
-            const double2 u0 = *reinterpret_cast<const double2 *>(B.uT + (size_t)(t0 + P.ell_col[o]) * nr + j);
-            s0.x += v0 * u0.x;
-            s0.y += v0 * u0.y;
+            const double v0 = __ldg(P.ell_val + o);
+            const double2 u0 = __ldg(uT + (size_t)(t0 + __ldg(P.ell_col + o)) * hn + jh);
+            s0.x += v0 * u0.x; s0.y += v0 * u0.y;
         }
-        *reinterpret_cast<double2 *>(B.vT + (size_t)t * nr + j) = make_double2(s0.x + s1.x, s0.y + s1.y);
+        *reinterpret_cast<double2 *>(B.vT + (size_t)t * nr + j) =
+            make_double2((s0.x + s1.x) + (s2.x + s3.x), (s0.y + s1.y) + (s2.y + s3.y));
     }
 }
 
