@@ -5,7 +5,7 @@ Tolerances:
     (re-association of the FP64 sums only);
   * F apply, FP32 tiles: 1e-6; BF16 tiles with per-tile scale: 1e-2 (storage precision);
   * solves: displacements within 1e-8 relative of the oracle's FP64 solve and of
-    a direct solve (the north-star bar), for FP64 and for FP32 storage inside
+    a direct solve, for FP64 and for FP32 storage inside
     FP64 residual replacement.
 """
 import numpy as np
