@@ -59,7 +59,7 @@ namespace {
 std::mutex g_mutex;
 std::list<FETI4IStructMatrix *> g_matrices;
 std::list<FETI4IStructInstance *> g_instances;
-double g_ext[FETI4I_EXT_OPTIONS_SIZE] = {0, 1, 0, 48, 16, 0.003, 0, 0, 1, 1, 1, 1, 0, 0};
+double g_ext[FETI4I_EXT_OPTIONS_SIZE] = {0, 1, 0, 48, 16, 0.003, 0, 0, 1, 1, 1, 1, 0, 0, 0};
 
 template <typename F>
 void guarded(F &&f) {
@@ -285,6 +285,7 @@ void FETI4ISetExtendedOptions(FETI4IInstance instance, FETI4IInt key, FETI4IReal
         FETI_CHECK(key >= 0 && key < FETI4I_EXT_OPTIONS_SIZE, "FETI4I: unknown extended option");
         if (I->ext[key] == value) return;
         I->ext[key] = value;
+        if (key == FETI4I_EXT_TRUNCATE) return;   // read by the next solve
         if (I->gpu && (key == FETI4I_EXT_RELIABLE_DELTA || key == FETI4I_EXT_GRAPH_CHUNK ||
                        key == FETI4I_EXT_SYMM_TENSOR)) {
             SolveOptions so = I->sopt;
@@ -336,6 +337,19 @@ static void check_whole(FETI4IStructInstance *I) {
                "FETI4IPrimalFromDual");
 }
 
+// The reference's output formatting (FETISolver.cpp:130-147): every value truncated to
+// dplaces = 1 / precision / max(1, 10^ceil(log10 max|u|)) places.  The reference applies it to the
+// subdomain primal values before they are gathered; here it is applied to the caller's (averaged)
+// solution vector, so values on subdomain interfaces may differ from the reference's by one unit of
+// 1 / dplaces.
+static void truncate_like_reference(double *u, size_t n, double precision) {
+    double gmax = 0.0;
+    for (size_t i = 0; i < n; ++i) gmax = std::max(gmax, std::fabs(u[i]));
+    if (gmax == 0.0) return;
+    const double dplaces = 1.0 / precision / std::max(1.0, std::pow(10.0, std::ceil(std::log10(gmax))));
+    for (size_t i = 0; i < n; ++i) u[i] = std::trunc(dplaces * u[i]) / dplaces;
+}
+
 static void solve_instance(FETI4IStructInstance *I) {
     FETI_CHECK(I->gpu, "FETI4I: instance was created with FETI4I_EXT_HOST_ONLY; no device solver");
     make_rhs_vectors(I->dec, I->prep, I->b, I->e);
@@ -356,6 +370,8 @@ void FETI4ISolve(FETI4IInstance instance, FETI4IInt solution_size, FETI4IReal *s
         FETI_CHECK(I->gpu, "FETI4I: instance was created with FETI4I_EXT_HOST_ONLY; no device solver");
         double t0 = now_s();
         I->gpu->solve_full(I->rhs.data(), (int)I->rhs.size(), solution, solution_size, I->stats, true);
+        if (I->ext[FETI4I_EXT_TRUNCATE] != 0.0)
+            truncate_like_reference(solution, (size_t)solution_size, I->ropt[FETI4I_PRECISION]);
         I->rhs_on_device = true;
         I->t_solve_wall = (now_s() - t0) * 1e3;
         I->lambda.clear();
@@ -374,6 +390,9 @@ void FETI4ISolveMulti(FETI4IInstance instance, FETI4IInt nrhs, FETI4IInt size, c
         FETI_CHECK(rhs && solutions && size > 0, "FETI4ISolveMulti: invalid arrays");
         double t0 = now_s();
         I->gpu->solve_multi(rhs, nrhs, size, solutions, size, I->stats, true);
+        if (I->ext[FETI4I_EXT_TRUNCATE] != 0.0)
+            for (FETI4IInt j = 0; j < nrhs; ++j)
+                truncate_like_reference(solutions + (size_t)j * size, (size_t)size, I->ropt[FETI4I_PRECISION]);
         I->t_solve_wall = (now_s() - t0) * 1e3;
         I->multi_on_device = nrhs;
     });

@@ -23,7 +23,7 @@ PREC_NONE, PREC_LUMPED, PREC_WEIGHT, PREC_DIRICHLET, PREC_SUPER_DIRICHLET, PREC_
 # extended options (include/feti4i_ext.h)
 EXT_SCHUR_PRECISION, EXT_SCALING, EXT_HOST_ONLY, EXT_TILES_PER_ITEM, EXT_GRAPH_CHUNK, EXT_RELIABLE_DELTA, \
     EXT_HOST_THREADS, EXT_TILE_KERNEL, EXT_AUTOTUNE, EXT_SYMM_TENSOR, EXT_DEVICE_PREP, EXT_SCHUR_EXPLICIT, \
-    EXT_OWNED_FIRST, EXT_OWNED_COUNT = range(14)
+    EXT_OWNED_FIRST, EXT_OWNED_COUNT, EXT_TRUNCATE = range(15)
 FP64, FP32, BF16 = 0, 1, 2
 STAT_NAMES = ["iterations", "converged", "dual_size", "kernel_size", "subdomains", "prep_seconds",
               "upload_seconds", "solve_ms", "solve_wall_ms", "fapply_bytes", "replacements",

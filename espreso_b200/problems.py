@@ -310,6 +310,7 @@ def make_instance(problem: Problem, iopts=None, ropts=None, ext=None, batched=Tr
             F.set_extended(F.EXT_SCHUR_EXPLICIT, 1)
             F.set_extended(F.EXT_OWNED_FIRST, 0)
             F.set_extended(F.EXT_OWNED_COUNT, 0)
+            F.set_extended(F.EXT_TRUNCATE, 0)
     return inst
 
 

@@ -74,12 +74,15 @@ typedef enum {
                                     (itersolver.cpp:6373-6406); here every process numbers the whole problem,
                                     prepares and uploads only its block, and a driver (espreso_b200.partitioned)
                                     runs the dual PCG with the operators below and one allreduce per apply. */
+    FETI4I_EXT_TRUNCATE,         /* 1: FETI4ISolve / FETI4ISolveMulti return the solution truncated as the reference's
+                                    FETISolver::solve does (FETISolver.cpp:130-147): to 1 / PRECISION places relative
+                                    to 10^ceil(log10 max|u|), per load case; 0 (default): the full FP64 solution */
     FETI4I_EXT_OPTIONS_SIZE
 } FETI4IExtOptions;
 void FETI4ISetExtendedOption(FETI4IInt key, FETI4IReal value);
 
 /* Extended option of one instance (the per-instance form of FETI4ISetExtendedOption, which only
- * sets the defaults of instances created afterwards).  FETI4I_EXT_RELIABLE_DELTA, GRAPH_CHUNK and
+ * sets the defaults of instances created afterwards).  FETI4I_EXT_RELIABLE_DELTA, GRAPH_CHUNK, TRUNCATE and
  * SYMM_TENSOR apply to the next solve; the others (Schur precision, scaling, tiles, device or host
  * preprocessing) redo the instance's preprocessing and upload with its decomposition kept. */
 void FETI4ISetExtendedOptions(FETI4IInstance instance, FETI4IInt key, FETI4IReal value);

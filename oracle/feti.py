@@ -359,3 +359,14 @@ def direct_solve(K, f, fixed_dofs, fixed_vals):
     rhs = f[free] - K[free][:, fixed_dofs] @ u[fixed_dofs]
     u[free] = spla.spsolve(K[free][:, free].tocsc(), rhs)
     return u
+
+
+def espreso_truncate(u, precision):
+    """The reference's output formatting (src/solver/generic/FETISolver.cpp:130-147): every value
+    truncated to dplaces = 1 / precision / max(1, 10^ceil(log10 max|u|)) places."""
+    u = np.asarray(u, dtype=np.float64)
+    gmax = np.abs(u).max()
+    if gmax == 0.0:
+        return u.copy()
+    dplaces = 1.0 / precision / max(1.0, 10.0 ** np.ceil(np.log10(gmax)))
+    return np.trunc(dplaces * u) / dplaces

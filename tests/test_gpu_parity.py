@@ -169,3 +169,22 @@ def test_per_instance_schur_precision(elast):
     assert np.linalg.norm(ua - ub) <= 1e-8 * np.linalg.norm(ua)
     a.destroy()
     b.destroy()
+
+
+def test_reference_truncated_output(heat):
+    """FETI4I_EXT_TRUNCATE: the solution formatted as the reference's FETISolver returns it (the
+    oracle's espreso_truncate of the full solution, up to one truncation unit where two solves of the
+    same instance differ in their last bits)."""
+    inst = gpu_instance(heat, precision=1e-6)
+    u = inst.solve()
+    assert np.abs(u).max() > 1e-4          # several significant places survive the truncation
+    inst.set_extended(F.EXT_TRUNCATE, 1)
+    ut = inst.solve()
+    ref = OF.espreso_truncate(u, 1e-6)
+    unit = 1.0 / (1e6 / max(1.0, 10.0 ** np.ceil(np.log10(np.abs(u).max()))))
+    assert np.all(np.abs(ut - ref) <= unit * (1 + 1e-9))
+    assert np.mean(ut == ref) > 0.99
+    assert np.all(np.abs(ut - u) <= unit)
+    inst.set_extended(F.EXT_TRUNCATE, 0)
+    assert np.linalg.norm(inst.solve() - u) <= 1e-9 * np.linalg.norm(u)
+    inst.destroy()

@@ -79,3 +79,14 @@ def test_global_load_split(case):
     u = OP.merge(OP.primal(lam, alpha), P.n_nodes)
     ud = direct_u(P)
     assert np.linalg.norm(u - ud) <= 1e-8 * np.linalg.norm(ud)
+
+
+def test_espreso_truncate():
+    """FETISolver.cpp:130-147: 1 / precision places relative to 10^ceil(log10 max|u|)."""
+    dp = 1.0 / 1e-5          # the reference divides by the precision in double, as here
+    u = np.array([0.123456789, -0.0004567, 0.0])
+    np.testing.assert_array_equal(OF.espreso_truncate(u, 1e-5), np.trunc(dp * u) / dp)
+    v = np.array([123.456789, -0.5])
+    dv = dp / 1000.0         # max|v| = 123.5: 10^ceil(log10) = 1000
+    np.testing.assert_array_equal(OF.espreso_truncate(v, 1e-5), np.trunc(dv * v) / dv)
+    assert abs(OF.espreso_truncate(v, 1e-5)[0] - 123.45) < 1e-12
