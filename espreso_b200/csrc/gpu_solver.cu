@@ -2059,6 +2059,9 @@ struct GpuSolver::Impl {
         int2 *units4 = nullptr;
         int nunits4 = 0;
         float *pan = nullptr;          // K-major panels of the mixed blocks (asynchronous tensor-core SYMM)
+        float *xs = nullptr;           // split X blocks of the warp-specialised tensor-core SYMM (8 KB each)
+        int *blk0 = nullptr, *blkm = nullptr;   // first 32-row block of every subdomain; subdomain of every block
+        int nblk = 0;
         int2 *dunits = nullptr;   // SYMM units of the Dirichlet blocks (Dirichlet preconditioner)
         int ndunits = 0;
     } blk;
@@ -5313,6 +5316,345 @@ tile_symm_tc2_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, 
     }
 }
 
+// ---- Tile SYMM on the tensor cores, warp-specialised (32 right-hand sides)
+// Same units (four tile rows of one subdomain, M = 128) and results as tile_symm_tc_kernel<32>.
+// The roles of a CTA (one per SM) hand 32-column blocks over through a ring of NS stages:
+//   * producer (one lane): per block J, one 4 KB bulk copy (cp.async.bulk) of every stored tile the
+//     unit needs, (I, J) for J >= I and (J, I) for J < I, row-major as stored, into the tile's 4 KB
+//     slice of the stage, and one 8 KB copy of X_J already split (xsplit_kernel);
+//   * four converter warps, warp q for tile row I0 + q: read the raw tile into registers (vector
+//     loads for a stored tile, transposing scalar loads for the transposed one), then write its
+//     TF32 high part in place, at the swizzled K-major position, and its low part to the stage's
+//     low buffer;
+//   * one MMA lane: hi*hi + hi*lo + lo*hi (tcgen05.mma kind::tf32, M = 128, N = 32, K = 8, four K
+//     steps) into one of two FP32 accumulators in tensor memory, commits that free the stage and,
+//     after the unit's last block, hand the accumulator to
+//   * four epilogue warps (tensor-memory lane quadrants 0..3): y rows to `out`; each lane keeps its
+//     column's share of x.y over the CTA's units and writes it to unit_dot[4 CTA + warp] at the end.
+// Units go to CTAs round-robin in the order of the unit list (longest rows first), so every role
+// derives the same unit and block sequence.  Every wait is bounded and gives up at once when
+// another role has given up: the CTA then records an error, drains its copies and MMAs in flight,
+// frees its tensor memory and returns.
+namespace tc3 {
+constexpr int NS = 4;                            // stages
+constexpr int CONV = 4, EPI = 4;                 // converter warps, epilogue warps
+constexpr int PROD_WARP = CONV + EPI, MMA_WARP = CONV + EPI + 1;
+constexpr int THREADS = (CONV + EPI + 2) * 32;
+constexpr unsigned A_BYTES = 128 * 128;          // 128 rows x 32 FP32
+constexpr unsigned B_BYTES = 32 * 128;           // 32 rows (right-hand sides) x 32 FP32
+constexpr unsigned STAGE = 2 * A_BYTES + 2 * B_BYTES;
+constexpr unsigned SMEM = NS * STAGE + 1024;
+constexpr unsigned TMEM_COLS = 64;               // two accumulators of 32 columns
+__device__ __forceinline__ void bulk(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+// bounded wait that also gives up when another role has set *abort
+__device__ __forceinline__ bool wait(unsigned long long *bar, unsigned parity, volatile int *abort) {
+    for (long long i = 0; i < WAIT_LIMIT; ++i) {
+        if (mbar_try(bar, parity)) return true;
+        if (*abort) return false;
+        if (i > 64) __nanosleep(64);
+    }
+    return false;
+}
+__device__ __forceinline__ void ld32(unsigned taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ long long tile_index(long long t0, int tn, int I, int J) {   // stored tile (I, J), I <= J
+    return t0 + (long long)I * tn - (long long)I * (I - 1) / 2 + (J - I);
+}
+}  // namespace tc3
+
+// X_J of every 32-row block J of every subdomain, split once per F apply for tile_symm_tc3_kernel:
+// block b (subdomain blkm[b], J = b - blk0[m]) holds 8 KB, the TF32 high and then the low part of
+// X_J^T (32 right-hand sides x 32 rows) in the swizzled K-major operand layout; rows past the
+// subdomain are zero.  A CTA reads the block's 32 rows of x coalesced into shared memory and
+// writes the 16-byte chunks of the operand in address order.
+__global__ void __launch_bounds__(256) xsplit_kernel(TileSetDev ts, DevProblem P, const float *x32, const int *blkm,
+                                                     const int *blk0, int nblk, float *xs, int slot, int mode) {
+    pdl_enter();
+    if (mode != 0) {
+        const int iter = P.st->iter_base + slot;
+        if (skip_iter(P.st, iter)) return;
+    }
+    __shared__ float xt[32][33];
+    const int t = threadIdx.x;
+    const int rr = t >> 3, cq = t & 7;                          // load: row, 4-column group
+    const int p8 = (t >> 3) & 7;                                // store: chunk t of the operand
+    const int nn = (t >> 6) * 8 + p8, c = (t & 7) ^ p8;         //   holds rows 4c..4c+3 of column nn
+    for (int b = blockIdx.x; b < nblk; b += gridDim.x) {
+        const int m = blkm[b], J = b - blk0[m];
+        const int n = ts.mat_n[m], voff = ts.mat_voff[m];
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (TILE * J + rr < n) v = *reinterpret_cast<const float4 *>(x32 + (size_t)(voff + TILE * J + rr) * 32 + 4 * cq);
+        xt[rr][4 * cq + 0] = v.x;
+        xt[rr][4 * cq + 1] = v.y;
+        xt[rr][4 * cq + 2] = v.z;
+        xt[rr][4 * cq + 3] = v.w;
+        __syncthreads();
+        const float4 w = make_float4(xt[4 * c + 0][nn], xt[4 * c + 1][nn], xt[4 * c + 2][nn], xt[4 * c + 3][nn]);
+        unsigned char *dst = reinterpret_cast<unsigned char *>(xs + (size_t)b * 2048);
+        tc::split_store(dst, dst + tc3::B_BYTES, (unsigned)t * 16u, w);
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(tc3::THREADS, 1)
+tile_symm_tc3_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, const float *xs, const int *blk0,
+                     double *out, const int2 *units, int nunits, int slot, int mode) {
+    pdl_enter();
+    constexpr int NS = tc3::NS, NR = 32;
+    extern __shared__ unsigned char tc3_smem[];
+    __shared__ __align__(8) unsigned long long full[NS], conv[NS], empty[NS], accf[2], acce[2];
+    __shared__ unsigned s_tmem;
+    __shared__ volatile int s_abort;
+    __shared__ int s_last;
+    __shared__ double s_red[tc3::THREADS / 32][32];
+    if (mode != 0) {
+        const int iter = P.st->iter_base + slot;
+        if (skip_iter(P.st, iter)) return;
+    }
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const unsigned base = smem_u32(tc3_smem);
+    unsigned char *buf = tc3_smem + ((1024u - (base & 1023u)) & 1023u);   // 1024-byte aligned stages
+    if (warp == tc3::MMA_WARP) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(tc3::TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int s = 0; s < NS; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&conv[s], tc3::CONV);
+            mbar_init(&empty[s], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&accf[a], 1);
+            mbar_init(&acce[a], tc3::EPI);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_abort = 0;
+    }
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const unsigned tmem = s_tmem;
+    const float *tiles = reinterpret_cast<const float *>(ts.tiles);
+    bool ok = true;
+
+    if (warp == tc3::PROD_WARP) {
+        if (lane == 0) {
+            long long t = 0, last[NS];
+            for (int s = 0; s < NS; ++s) last[s] = -1;
+            for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+                const int m = units[u].x, I0 = 4 * units[u].y, tn = ts.mat_tn[m];
+                const long long t0 = ts.mat_tile0[m];
+                const int nq = min(4, tn - I0);
+                const float *xb = xs + (size_t)blk0[m] * 2048;
+                for (int J = 0; J < tn; ++J, ++t) {
+                    const int s = (int)(t % NS);
+                    if (t >= NS && !tc3::wait(&empty[s], (unsigned)(((t / NS) - 1) & 1), &s_abort)) {
+                        ok = false;
+                        break;
+                    }
+                    unsigned char *stg = buf + (size_t)s * tc3::STAGE;
+                    mbar_arrive_tx(&full[s], 4096u * (unsigned)nq + 2u * tc3::B_BYTES);
+                    for (int q = 0; q < nq; ++q) {
+                        const int I = I0 + q;
+                        const long long idx = (I <= J) ? tc3::tile_index(t0, tn, I, J) : tc3::tile_index(t0, tn, J, I);
+                        tc3::bulk(stg + q * 4096, tiles + (size_t)idx * (TILE * TILE), 4096u, &full[s]);
+                    }
+                    tc3::bulk(stg + 2 * tc3::A_BYTES, xb + (size_t)J * 2048, 2u * tc3::B_BYTES, &full[s]);
+                    last[s] = t;
+                }
+            }
+            if (!ok) s_abort = 1;
+            // every copy this lane issued has landed before the CTA can leave (bounded waits)
+            for (int s = 0; s < NS; ++s)
+                if (last[s] >= 0) mbar_wait(&full[s], (unsigned)((last[s] / NS) & 1));
+        }
+    } else if (warp == tc3::MMA_WARP) {
+        if (lane == 0) {
+            constexpr uint32_t ID = tc::idesc<NR>();
+            long long t = 0, lastc = -1;
+            int k = 0;
+            for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++k) {
+                const int m = units[u].x, tn = ts.mat_tn[m];
+                const int a = k & 1;
+                if (k >= 2 && !tc3::wait(&acce[a], (unsigned)(((k >> 1) - 1) & 1), &s_abort)) {
+                    ok = false;
+                    break;
+                }
+                tc::fence_after();
+                const unsigned d = tmem + (unsigned)(a * NR);
+                for (int J = 0; J < tn; ++J, ++t) {
+                    const int s = (int)(t % NS);
+                    if (!tc3::wait(&conv[s], (unsigned)((t / NS) & 1), &s_abort)) {
+                        ok = false;
+                        break;
+                    }
+                    tc::fence_after();
+                    const unsigned a_hi = smem_u32(buf + (size_t)s * tc3::STAGE), a_lo = a_hi + tc3::A_BYTES,
+                                   b_hi = a_hi + 2 * tc3::A_BYTES, b_lo = b_hi + tc3::B_BYTES;
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk) {
+                        const unsigned off = 32u * kk;
+                        tc::mma(d, tc::sdesc(a_hi + off), tc::sdesc(b_hi + off), ID, (J > 0 || kk > 0) ? 1u : 0u);
+                        tc::mma(d, tc::sdesc(a_hi + off), tc::sdesc(b_lo + off), ID, 1u);
+                        tc::mma(d, tc::sdesc(a_lo + off), tc::sdesc(b_hi + off), ID, 1u);
+                    }
+                    tc::commit(&empty[s]);
+                    if (J == tn - 1) tc::commit(&accf[a]);
+                    lastc = t;
+                }
+            }
+            if (!ok) s_abort = 1;
+            // every MMA issued has completed before the stages and the tensor memory are released
+            if (lastc >= 0) mbar_wait(&empty[lastc % NS], (unsigned)((lastc / NS) & 1));
+        }
+    } else if (warp < tc3::CONV) {
+        const int q = warp;
+        long long t = 0;
+        for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+            const int m = units[u].x, I = 4 * units[u].y + q, tn = ts.mat_tn[m];
+            for (int J = 0; J < tn; ++J, ++t) {
+                const int s = (int)(t % NS);
+                ok = __all_sync(FULL, tc3::wait(&full[s], (unsigned)((t / NS) & 1), &s_abort));
+                if (!ok) break;
+                if (I < tn) {   // rows of a missing tile row only reach accumulator rows that are not read
+                    unsigned char *hi = buf + (size_t)s * tc3::STAGE + q * 4096, *lo = hi + tc3::A_BYTES;
+                    float4 v[8];
+                    if (I <= J) {
+                        const float4 *src = reinterpret_cast<const float4 *>(hi);
+#pragma unroll
+                        for (int it = 0; it < 8; ++it) v[it] = src[it * 32 + lane];
+                        __syncwarp();
+#pragma unroll
+                        for (int it = 0; it < 8; ++it) {
+                            const int p = it * 32 + lane;
+                            tc::split_store(hi, lo, tc::swz(p >> 3, p & 7), v[it]);
+                        }
+                    } else {
+                        // stored tile (J, I): row `lane` of S_IJ is column `lane` of the stored tile
+                        const float *src = reinterpret_cast<const float *>(hi);
+#pragma unroll
+                        for (int it = 0; it < 8; ++it)
+                            v[it] = make_float4(src[(4 * it + 0) * 32 + lane], src[(4 * it + 1) * 32 + lane],
+                                                src[(4 * it + 2) * 32 + lane], src[(4 * it + 3) * 32 + lane]);
+                        __syncwarp();
+#pragma unroll
+                        for (int it = 0; it < 8; ++it) tc::split_store(hi, lo, tc::swz(lane, it), v[it]);
+                    }
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&conv[s]);
+            }
+        }
+        if (!ok && lane == 0) s_abort = 1;
+    } else {
+        // epilogue: warp 4 + e reads tensor-memory lanes 32 e .. 32 e + 31 (rows of tile row I0 + e)
+        const int e = warp - tc3::CONV;
+        int k = 0;
+        double dot = 0.0;   // lane l: this warp's share of x_l . y_l over the CTA's units
+        for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++k) {
+            const int m = units[u].x, I0 = 4 * units[u].y;
+            const int n = ts.mat_n[m], voff = ts.mat_voff[m];
+            const int a = k & 1;
+            ok = __all_sync(FULL, tc3::wait(&accf[a], (unsigned)((k >> 1) & 1), &s_abort));
+            if (!ok) break;
+            tc::fence_after();
+            uint32_t r[32];
+            tc3::ld32(tmem + ((unsigned)(32 * e) << 16) + (unsigned)(a * NR), r);
+            tc::fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acce[a]);
+            const int row = TILE * I0 + 32 * e + lane;
+            double v[32];
+            if (row < n) {
+                const float4 *xr = reinterpret_cast<const float4 *>(x32 + (size_t)(voff + row) * NR);
+                double2 *orow = reinterpret_cast<double2 *>(out + (size_t)(voff + row) * NR);
+#pragma unroll
+                for (int c4 = 0; c4 < 8; ++c4) {
+                    const float4 xv = xr[c4];
+                    const double y0 = (double)__uint_as_float(r[4 * c4 + 0]), y1 = (double)__uint_as_float(r[4 * c4 + 1]),
+                                 y2 = (double)__uint_as_float(r[4 * c4 + 2]), y3 = (double)__uint_as_float(r[4 * c4 + 3]);
+                    orow[2 * c4] = make_double2(y0, y1);
+                    orow[2 * c4 + 1] = make_double2(y2, y3);
+                    v[4 * c4 + 0] = (double)xv.x * y0;
+                    v[4 * c4 + 1] = (double)xv.y * y1;
+                    v[4 * c4 + 2] = (double)xv.z * y2;
+                    v[4 * c4 + 3] = (double)xv.w * y3;
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < 32; ++c) v[c] = 0.0;
+            }
+            // reduce-scatter over the lanes: afterwards lane l holds the warp's sum of column l
+#pragma unroll
+            for (int o = 16; o >= 1; o >>= 1) {
+                const bool upper = (lane & o) != 0;
+#pragma unroll
+                for (int i = 0; i < o; ++i) {
+                    const double send = upper ? v[i] : v[i + o];
+                    const double keep = upper ? v[i + o] : v[i];
+                    v[i] = keep + __shfl_xor_sync(FULL, send, o);
+                }
+            }
+            dot += v[0];
+        }
+        if (!ok && lane == 0) s_abort = 1;
+        B.unit_dot[((size_t)blockIdx.x * tc3::EPI + e) * NR + lane] = dot;
+        __threadfence();
+    }
+    if (!ok) atomicExch(&P.st->error, 1);
+    tc::fence_before();
+    __syncthreads();
+    if (warp == tc3::MMA_WARP) {
+        __syncwarp();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tc3::TMEM_COLS)
+                     : "memory");
+    }
+    if (tid == 0) {
+        __threadfence();
+        s_last = (atomicAdd(&B.queue[1], 1) == (int)gridDim.x - 1);
+    }
+    __syncthreads();
+    if (s_last) {
+        if (mode == 1) {
+            // p.Ap of every column: the CTAs' partials, summed in a fixed order by all warps
+            __threadfence();
+            double tsum = 0.0;
+            for (int q = warp; q < tc3::EPI * (int)gridDim.x; q += tc3::THREADS / 32)
+                tsum += __ldcg(&B.unit_dot[(size_t)q * NR + lane]);
+            s_red[warp][lane] = tsum;
+            __syncthreads();
+            if (tid < NR) {
+                double t2 = 0.0;
+                for (int w = 0; w < tc3::THREADS / 32; ++w) t2 += s_red[w][tid];
+                B.scal[SC_PAP * NR + tid] = t2;
+            }
+        }
+        if (tid == 0) {
+            B.queue[0] = 0;
+            B.queue[1] = 0;
+            __threadfence();
+        }
+    }
+}
+
 // ---- Hybrid Total FETI cluster correction for nr columns ([row][rhs] layout)
 // z_i = V_i^T x_i: one warp per column of V_i, lane = (row group, rhs)
 __global__ void bhyb_vt_kernel(DevProblem P, HybDev H, BlockDev B, const double *x, double *z, int slot, int cond) {
@@ -5551,7 +5893,25 @@ void GpuSolver::Impl::ensure_block(int nr) {
     blk.units4 = upload(units4);
     blk.nunits4 = (int)units4.size();
     blk.pan = nullptr;   // rebuilt for these units at the first asynchronous tensor-core SYMM
-    size_t max_units = std::max(units.size(), units4.size());
+    // 32-row blocks of the subdomains for the split X of the warp-specialised tensor-core SYMM
+    blk.xs = nullptr;
+    blk.blk0 = blk.blkm = nullptr;
+    blk.nblk = 0;
+    if (nr == 32) {
+        std::vector<int> b0(tn.size()), bm;
+        for (size_t m = 0; m < tn.size(); ++m) {
+            b0[m] = (int)bm.size();
+            for (int J = 0; J < tn[m]; ++J) bm.push_back((int)m);
+        }
+        blk.nblk = (int)bm.size();
+        if (blk.nblk > 0) {
+            blk.blk0 = upload(b0);
+            blk.blkm = upload(bm);
+            blk.xs = alloc<float>((size_t)blk.nblk * 2048);
+        }
+    }
+    // per-unit dot products: one per unit, or four (one per epilogue warp) for the tensor-core units
+    size_t max_units = std::max(units.size(), 4 * units4.size());
     if (opt.precond == PREC_DIRICHLET) {
         // SYMM units of the Dirichlet blocks S_dir (T space)
         std::vector<int2> du;
@@ -5663,6 +6023,33 @@ static bool symm_tc2_enabled() {
     return on;
 }
 
+// The warp-specialised tensor-core SYMM (tile_symm_tc3_kernel) serves 32 right-hand sides unless
+// FETI4I_SYMM_TC3=0 selects tile_symm_tc_kernel<32>.
+static bool symm_tc3_enabled() {
+    static const bool on = [] {
+        const char *e = getenv("FETI4I_SYMM_TC3");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+static void symm_tc3_launch(int nsm, cudaStream_t st, TileSetDev td, DevProblem P, BlockDev B, const float *x32,
+                            float *xs, const int *blk0, const int *blkm, int nblk, double *out, const int2 *units,
+                            int nunits, int slot, int mode) {
+    static bool attr = false;
+    if (!attr) {
+        CUDA_CHECK(cudaFuncSetAttribute(tile_symm_tc3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)tc3::SMEM));
+        attr = true;
+    }
+    launch_pdl(xsplit_kernel, dim3(std::max(1, std::min(nblk, nsm * 8))), dim3(256), 0, st, td, P, x32, blkm, blk0,
+               nblk, xs, slot, mode);
+    // one CTA per SM (its shared memory); CTAs never wait for one another
+    const int grid = std::max(1, std::min(nunits, nsm));
+    launch_pdl(tile_symm_tc3_kernel, dim3(grid), dim3(tc3::THREADS), (size_t)tc3::SMEM, st, td, P, B, x32,
+               (const float *)xs, blk0, out, units, nunits, slot, mode);
+}
+
 static bool symm_tc2_bmn() {
     static const bool on = [] {
         const char *e = getenv("FETI4I_TC2_BMN");
@@ -5713,6 +6100,13 @@ void GpuSolver::Impl::launch_symm(const TileSetHost &T, bool src32, const double
     const bool dir = &T == &Dir;
     const int2 *units = dir ? blk.dunits : blk.units;
     const int nunits = dir ? blk.ndunits : blk.nunits;
+    if (!dir && opt.symm_tensor && T.prec == SCHUR_FP32 && src32 && nr == 32 && blk.xs && symm_tc3_enabled() &&
+        !symm_tc2_enabled()) {
+        symm_tc3_launch(nsm, stream, T.dev(), P, blk.B, x32, blk.xs, blk.blk0, blk.blkm, blk.nblk, out, blk.units4,
+                        blk.nunits4, slot, mode);
+        CUDA_CHECK(cudaGetLastError());
+        return;
+    }
     if (!dir && opt.symm_tensor && T.prec == SCHUR_FP32 && src32 && nr == 32 && symm_tc2_enabled()) {
         TileSetDev td = T.dev();
         FETI_CHECK(blk.pan != nullptr, "internal: tensor-core SYMM panels not built");

@@ -2,10 +2,11 @@
 
 FETI4IApplyDualOperatorMulti runs the F apply of FETI4ISolveMulti on up to 32 dual vectors at once:
   * FP64 tiles: tile_symm_mma_kernel (FP64 tensor-core MMA), to 1e-12;
-  * FP32 tiles on the tensor cores (3xTF32): tile_symm_tc_kernel at 8, 16 and 32 vectors, and the
-    asynchronous tile_symm_tc2_kernel at 32 vectors (FETI4I_SYMM_TC2=1, run in a child process),
-    with every kind of 32-column block (stored tiles, their transposes read MN-major, assembled
-    diagonal panels);
+  * FP32 tiles on the tensor cores (3xTF32): the warp-specialised tile_symm_tc3_kernel at 32
+    vectors, tile_symm_tc_kernel at 8 and 16 (and at 32 with FETI4I_SYMM_TC3=0, run in a child
+    process), and the asynchronous tile_symm_tc2_kernel at 32 vectors (FETI4I_SYMM_TC2=1, child
+    process), with every kind of 32-column block (stored tiles, their transposes, the blocks that
+    mix both);
   * FP32 tiles on the CUDA cores (FETI4I_EXT_SYMM_TENSOR = 0).
 FP32 Schur storage rounds S_i to 2^-24 relative and accumulates in FP32, so the FP32 paths agree
 with the FP64 apply to 2e-5 (norm-wise per vector).  A single subdomain makes every dual row one
@@ -72,6 +73,15 @@ def test_symm_matches_single_apply(problems_, name, tensor):
 def test_symm_async_variant():
     """The same checks with the asynchronous tensor-core SYMM selected (read once per process)."""
     env = dict(os.environ, FETI4I_SYMM_TC2="1")
+    r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-m", "gpu", "-p", "no:cacheprovider",
+                        __file__ + "::test_symm_matches_single_apply"],
+                       env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+
+
+def test_symm_register_staged_variant():
+    """The same checks with tile_symm_tc_kernel serving 32 vectors (FETI4I_SYMM_TC3=0)."""
+    env = dict(os.environ, FETI4I_SYMM_TC3="0")
     r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-m", "gpu", "-p", "no:cacheprovider",
                         __file__ + "::test_symm_matches_single_apply"],
                        env=env, capture_output=True, text=True, timeout=600)
