@@ -5319,17 +5319,23 @@ tile_symm_tc2_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, 
 // ---- Tile SYMM on the tensor cores, warp-specialised (32 right-hand sides)
 // Same units (four tile rows of one subdomain, M = 128) and results as tile_symm_tc_kernel<32>.
 // The roles of a CTA (one per SM) hand 32-column blocks over through a ring of NS stages:
-//   * producer (one lane): per block J, one 4 KB bulk copy (cp.async.bulk) of every stored tile the
-//     unit needs, (I, J) for J >= I and (J, I) for J < I, row-major as stored, into the tile's 4 KB
-//     slice of the stage, and one 8 KB copy of X_J already split (xsplit_kernel);
+//   * two producer lanes (warps 8 and 10, even and odd blocks: a lane's copy issue, not the copies,
+//     limits one): per block J, one 4 KB bulk copy (cp.async.bulk) of every stored tile the unit
+//     needs, (I, J) for J >= I and (J, I) for J < I, row-major as stored, into the tile's 4 KB slice
+//     of the stage (one 16 KB copy when all four are transposed: they are adjacent in tile row J),
+//     and one 8 KB copy of X_J already split (xsplit_kernel);
 //   * four converter warps, warp q for tile row I0 + q: read the raw tile into registers (vector
 //     loads for a stored tile, transposing scalar loads for the transposed one), then write its
 //     TF32 high part in place, at the swizzled K-major position, and its low part to the stage's
 //     low buffer;
-//   * one MMA lane: hi*hi + hi*lo + lo*hi (tcgen05.mma kind::tf32, M = 128, N = 32, K = 8, four K
-//     steps) into one of two FP32 accumulators in tensor memory, commits that free the stage and,
-//     after the unit's last block, hand the accumulator to
-//   * four epilogue warps (tensor-memory lane quadrants 0..3): y rows to `out`; each lane keeps its
+//   * one MMA lane: per K step (K = 8, four per block) A_hi [X_hi | X_lo] as one N = 64 product
+//     (the two halves of X are adjacent in the stage) and A_lo X_hi (N = 32), tcgen05.mma kind::tf32,
+//     M = 128, into one of two FP32 accumulators of 64 columns in tensor memory (columns 0..31 hold
+//     hi*hi + lo*hi, 32..63 hi*lo; an MMA of N <= 128 takes the same time, so the stacking saves a
+//     third of the MMAs); commits that free the stage and, after the unit's last block, hand the
+//     accumulator to
+//   * four epilogue warps (tensor-memory lane quadrants 0..3): y = the two halves summed in FP64,
+//     rows to `out`; each lane keeps its
 //     column's share of x.y over the CTA's units and writes it to unit_dot[4 CTA + warp] at the end.
 // Units go to CTAs round-robin in the order of the unit list (longest rows first), so every role
 // derives the same unit and block sequence.  Every wait is bounded and gives up at once when
@@ -5338,13 +5344,14 @@ tile_symm_tc2_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, 
 namespace tc3 {
 constexpr int NS = 4;                            // stages
 constexpr int CONV = 4, EPI = 4;                 // converter warps, epilogue warps
-constexpr int PROD_WARP = CONV + EPI, MMA_WARP = CONV + EPI + 1;
-constexpr int THREADS = (CONV + EPI + 2) * 32;
+constexpr int PROD_WARP = CONV + EPI, MMA_WARP = CONV + EPI + 1, PROD_WARP2 = CONV + EPI + 2;
+constexpr int THREADS = (CONV + EPI + 3) * 32;
 constexpr unsigned A_BYTES = 128 * 128;          // 128 rows x 32 FP32
 constexpr unsigned B_BYTES = 32 * 128;           // 32 rows (right-hand sides) x 32 FP32
 constexpr unsigned STAGE = 2 * A_BYTES + 2 * B_BYTES;
 constexpr unsigned SMEM = NS * STAGE + 1024;
-constexpr unsigned TMEM_COLS = 64;               // two accumulators of 32 columns
+static_assert(NS % 2 == 0, "the two producer lanes own the even and the odd stages");
+constexpr unsigned TMEM_COLS = 128;              // two accumulators of 64 columns (hi*hi + lo*hi | hi*lo)
 __device__ __forceinline__ void bulk(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                      smem_u32(dst)),
@@ -5454,8 +5461,9 @@ tile_symm_tc3_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, 
     const float *tiles = reinterpret_cast<const float *>(ts.tiles);
     bool ok = true;
 
-    if (warp == tc3::PROD_WARP) {
+    if (warp == tc3::PROD_WARP || warp == tc3::PROD_WARP2) {
         if (lane == 0) {
+            const int par = (warp == tc3::PROD_WARP) ? 0 : 1;   // this lane's blocks: t % 2 == par
             long long t = 0, last[NS];
             for (int s = 0; s < NS; ++s) last[s] = -1;
             for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
@@ -5464,6 +5472,7 @@ tile_symm_tc3_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, 
                 const int nq = min(4, tn - I0);
                 const float *xb = xs + (size_t)blk0[m] * 2048;
                 for (int J = 0; J < tn; ++J, ++t) {
+                    if ((int)(t & 1) != par) continue;
                     const int s = (int)(t % NS);
                     if (t >= NS && !tc3::wait(&empty[s], (unsigned)(((t / NS) - 1) & 1), &s_abort)) {
                         ok = false;
@@ -5471,10 +5480,16 @@ tile_symm_tc3_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, 
                     }
                     unsigned char *stg = buf + (size_t)s * tc3::STAGE;
                     mbar_arrive_tx(&full[s], 4096u * (unsigned)nq + 2u * tc3::B_BYTES);
-                    for (int q = 0; q < nq; ++q) {
-                        const int I = I0 + q;
-                        const long long idx = (I <= J) ? tc3::tile_index(t0, tn, I, J) : tc3::tile_index(t0, tn, J, I);
-                        tc3::bulk(stg + q * 4096, tiles + (size_t)idx * (TILE * TILE), 4096u, &full[s]);
+                    if (J < I0) {
+                        // the stored tiles (J, I0 .. I0 + nq - 1) are adjacent in tile row J
+                        tc3::bulk(stg, tiles + (size_t)tc3::tile_index(t0, tn, J, I0) * (TILE * TILE), 4096u * (unsigned)nq,
+                                  &full[s]);
+                    } else {
+                        for (int q = 0; q < nq; ++q) {
+                            const int I = I0 + q;
+                            const long long idx = (I <= J) ? tc3::tile_index(t0, tn, I, J) : tc3::tile_index(t0, tn, J, I);
+                            tc3::bulk(stg + q * 4096, tiles + (size_t)idx * (TILE * TILE), 4096u, &full[s]);
+                        }
                     }
                     tc3::bulk(stg + 2 * tc3::A_BYTES, xb + (size_t)J * 2048, 2u * tc3::B_BYTES, &full[s]);
                     last[s] = t;
@@ -5487,7 +5502,7 @@ tile_symm_tc3_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, 
         }
     } else if (warp == tc3::MMA_WARP) {
         if (lane == 0) {
-            constexpr uint32_t ID = tc::idesc<NR>();
+            constexpr uint32_t ID64 = tc::idesc<2 * NR>(), ID32 = tc::idesc<NR>();
             long long t = 0, lastc = -1;
             int k = 0;
             for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++k) {
@@ -5498,7 +5513,7 @@ tile_symm_tc3_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, 
                     break;
                 }
                 tc::fence_after();
-                const unsigned d = tmem + (unsigned)(a * NR);
+                const unsigned d = tmem + (unsigned)(a * 2 * NR);
                 for (int J = 0; J < tn; ++J, ++t) {
                     const int s = (int)(t % NS);
                     if (!tc3::wait(&conv[s], (unsigned)((t / NS) & 1), &s_abort)) {
@@ -5507,13 +5522,12 @@ tile_symm_tc3_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, 
                     }
                     tc::fence_after();
                     const unsigned a_hi = smem_u32(buf + (size_t)s * tc3::STAGE), a_lo = a_hi + tc3::A_BYTES,
-                                   b_hi = a_hi + 2 * tc3::A_BYTES, b_lo = b_hi + tc3::B_BYTES;
+                                   b_hi = a_hi + 2 * tc3::A_BYTES;   // X_lo follows X_hi: rows 32..63 of B
 #pragma unroll
                     for (int kk = 0; kk < 4; ++kk) {
                         const unsigned off = 32u * kk;
-                        tc::mma(d, tc::sdesc(a_hi + off), tc::sdesc(b_hi + off), ID, (J > 0 || kk > 0) ? 1u : 0u);
-                        tc::mma(d, tc::sdesc(a_hi + off), tc::sdesc(b_lo + off), ID, 1u);
-                        tc::mma(d, tc::sdesc(a_lo + off), tc::sdesc(b_hi + off), ID, 1u);
+                        tc::mma(d, tc::sdesc(a_hi + off), tc::sdesc(b_hi + off), ID64, (J > 0 || kk > 0) ? 1u : 0u);
+                        tc::mma(d, tc::sdesc(a_lo + off), tc::sdesc(b_hi + off), ID32, 1u);
                     }
                     tc::commit(&empty[s]);
                     if (J == tn - 1) tc::commit(&accf[a]);
@@ -5576,8 +5590,9 @@ tile_symm_tc3_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, 
             ok = __all_sync(FULL, tc3::wait(&accf[a], (unsigned)((k >> 1) & 1), &s_abort));
             if (!ok) break;
             tc::fence_after();
-            uint32_t r[32];
-            tc3::ld32(tmem + ((unsigned)(32 * e) << 16) + (unsigned)(a * NR), r);
+            uint32_t r[32], r2[32];
+            tc3::ld32(tmem + ((unsigned)(32 * e) << 16) + (unsigned)(a * 2 * NR), r);
+            tc3::ld32(tmem + ((unsigned)(32 * e) << 16) + (unsigned)(a * 2 * NR + NR), r2);
             tc::fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&acce[a]);
@@ -5589,8 +5604,10 @@ tile_symm_tc3_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, 
 #pragma unroll
                 for (int c4 = 0; c4 < 8; ++c4) {
                     const float4 xv = xr[c4];
-                    const double y0 = (double)__uint_as_float(r[4 * c4 + 0]), y1 = (double)__uint_as_float(r[4 * c4 + 1]),
-                                 y2 = (double)__uint_as_float(r[4 * c4 + 2]), y3 = (double)__uint_as_float(r[4 * c4 + 3]);
+                    const double y0 = (double)__uint_as_float(r[4 * c4 + 0]) + (double)__uint_as_float(r2[4 * c4 + 0]),
+                                 y1 = (double)__uint_as_float(r[4 * c4 + 1]) + (double)__uint_as_float(r2[4 * c4 + 1]),
+                                 y2 = (double)__uint_as_float(r[4 * c4 + 2]) + (double)__uint_as_float(r2[4 * c4 + 2]),
+                                 y3 = (double)__uint_as_float(r[4 * c4 + 3]) + (double)__uint_as_float(r2[4 * c4 + 3]);
                     orow[2 * c4] = make_double2(y0, y1);
                     orow[2 * c4 + 1] = make_double2(y2, y3);
                     v[4 * c4 + 0] = (double)xv.x * y0;
