@@ -2059,9 +2059,6 @@ struct GpuSolver::Impl {
         int2 *units4 = nullptr;
         int nunits4 = 0;
         float *pan = nullptr;          // K-major panels of the mixed blocks (asynchronous tensor-core SYMM)
-        float *xs = nullptr;           // split X blocks of the warp-specialised tensor-core SYMM (8 KB each)
-        int *blk0 = nullptr, *blkm = nullptr;   // first 32-row block of every subdomain; subdomain of every block
-        int nblk = 0;
         int2 *dunits = nullptr;   // SYMM units of the Dirichlet blocks (Dirichlet preconditioner)
         int ndunits = 0;
     } blk;
@@ -5318,29 +5315,31 @@ tile_symm_tc2_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, 
 
 // ---- Tile SYMM on the tensor cores, warp-specialised (32 right-hand sides)
 // Same units (four tile rows of one subdomain, M = 128) and results as tile_symm_tc_kernel<32>.
-// The roles of a CTA (one per SM) hand 32-column blocks over through a ring of NS stages:
-//   * two producer lanes (warps 8 and 10, even and odd blocks: a lane's copy issue, not the copies,
-//     limits one): per block J, one 4 KB bulk copy (cp.async.bulk) of every stored tile the unit
-//     needs, (I, J) for J >= I and (J, I) for J < I, row-major as stored, into the tile's 4 KB slice
-//     of the stage (one 16 KB copy when all four are transposed: they are adjacent in tile row J),
-//     and one 8 KB copy of X_J already split (xsplit_kernel);
+// The roles of a CTA (one per SM) hand 32-column blocks J over through a ring of NS stages (the
+// bulk copies, at about 24 bytes per cycle and SM, and the ring's round-trip latency bound it):
+//   * two producer lanes (warps 8 and 10, even and odd blocks: a lane's copy issue limits one): one
+//     4 KB bulk copy (cp.async.bulk) of every stored tile the block needs, (I, J) for J >= I and
+//     (J, I) for J < I, row-major as stored, into the tile's 4 KB slice of the stage (one 16 KB copy
+//     when all four are transposed: they are adjacent in tile row J), and one 4 KB copy of the 32
+//     rows of x (32 right-hand sides each);
 //   * four converter warps, warp q for tile row I0 + q: read the raw tile into registers (vector
-//     loads for a stored tile, transposing scalar loads for the transposed one), then write its
-//     TF32 high part in place, at the swizzled K-major position, and its low part to the stage's
-//     low buffer;
-//   * one MMA lane: per K step (K = 8, four per block) A_hi [X_hi | X_lo] as one N = 64 product
-//     (the two halves of X are adjacent in the stage) and A_lo X_hi (N = 32), tcgen05.mma kind::tf32,
-//     M = 128, into one of two FP32 accumulators of 64 columns in tensor memory (columns 0..31 hold
-//     hi*hi + lo*hi, 32..63 hi*lo; an MMA of N <= 128 takes the same time, so the stacking saves a
-//     third of the MMAs); commits that free the stage and, after the unit's last block, hand the
-//     accumulator to
+//     loads for a stored tile, transposing scalar loads for the transposed one), write its TF32
+//     high part in place at the swizzled K-major position and its low part to the stage's low
+//     buffer; warp q also splits columns 8q .. 8q + 7 of X_J^T (rows past the subdomain zero) into
+//     the stage's X_hi | X_lo, the N = 64 operand;
+//   * one MMA lane: per K step (K = 8, four per block) A_hi [X_hi | X_lo] as one N = 64 product and
+//     A_lo X_hi (N = 32), tcgen05.mma kind::tf32, M = 128, into one of two FP32 accumulators of 64
+//     columns in tensor memory (columns 0..31 hold hi*hi + lo*hi, 32..63 hi*lo; an MMA of N <= 128
+//     takes the same time, so the stacking saves a third of the MMAs); commits free the stage and,
+//     after the unit's last block, hand the accumulator to
 //   * four epilogue warps (tensor-memory lane quadrants 0..3): y = the two halves summed in FP64,
-//     rows to `out`; each lane keeps its
-//     column's share of x.y over the CTA's units and writes it to unit_dot[4 CTA + warp] at the end.
+//     rows to `out`; each lane keeps its column's share of x.y over the CTA's units and writes it
+//     to unit_dot[4 CTA + warp] at the end.
 // Units go to CTAs round-robin in the order of the unit list (longest rows first), so every role
 // derives the same unit and block sequence.  Every wait is bounded and gives up at once when
 // another role has given up: the CTA then records an error, drains its copies and MMAs in flight,
-// frees its tensor memory and returns.
+// frees its tensor memory and returns.  x32 carries 32 rows past the last subdomain: the copy of a
+// subdomain's last block may read them (they are zeroed before use).
 namespace tc3 {
 constexpr int NS = 4;                            // stages
 constexpr int CONV = 4, EPI = 4;                 // converter warps, epilogue warps
@@ -5348,9 +5347,12 @@ constexpr int PROD_WARP = CONV + EPI, MMA_WARP = CONV + EPI + 1, PROD_WARP2 = CO
 constexpr int THREADS = (CONV + EPI + 3) * 32;
 constexpr unsigned A_BYTES = 128 * 128;          // 128 rows x 32 FP32
 constexpr unsigned B_BYTES = 32 * 128;           // 32 rows (right-hand sides) x 32 FP32
-constexpr unsigned STAGE = 2 * A_BYTES + 2 * B_BYTES;
+// stage: A (raw, then high part) | A low part | X_hi | X_lo | raw x rows
+constexpr unsigned ALO = A_BYTES, XS = 2 * A_BYTES, XRAW = 2 * A_BYTES + 2 * B_BYTES;
+constexpr unsigned STAGE = 2 * A_BYTES + 3 * B_BYTES;
 constexpr unsigned SMEM = NS * STAGE + 1024;
 static_assert(NS % 2 == 0, "the two producer lanes own the even and the odd stages");
+static_assert(STAGE % 1024 == 0, "stages start on 1024-byte boundaries (128-byte swizzle atoms)");
 constexpr unsigned TMEM_COLS = 128;              // two accumulators of 64 columns (hi*hi + lo*hi | hi*lo)
 __device__ __forceinline__ void bulk(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
@@ -5383,43 +5385,9 @@ __device__ __forceinline__ long long tile_index(long long t0, int tn, int I, int
 }
 }  // namespace tc3
 
-// X_J of every 32-row block J of every subdomain, split once per F apply for tile_symm_tc3_kernel:
-// block b (subdomain blkm[b], J = b - blk0[m]) holds 8 KB, the TF32 high and then the low part of
-// X_J^T (32 right-hand sides x 32 rows) in the swizzled K-major operand layout; rows past the
-// subdomain are zero.  A CTA reads the block's 32 rows of x coalesced into shared memory and
-// writes the 16-byte chunks of the operand in address order.
-__global__ void __launch_bounds__(256) xsplit_kernel(TileSetDev ts, DevProblem P, const float *x32, const int *blkm,
-                                                     const int *blk0, int nblk, float *xs, int slot, int mode) {
-    pdl_enter();
-    if (mode != 0) {
-        const int iter = P.st->iter_base + slot;
-        if (skip_iter(P.st, iter)) return;
-    }
-    __shared__ float xt[32][33];
-    const int t = threadIdx.x;
-    const int rr = t >> 3, cq = t & 7;                          // load: row, 4-column group
-    const int p8 = (t >> 3) & 7;                                // store: chunk t of the operand
-    const int nn = (t >> 6) * 8 + p8, c = (t & 7) ^ p8;         //   holds rows 4c..4c+3 of column nn
-    for (int b = blockIdx.x; b < nblk; b += gridDim.x) {
-        const int m = blkm[b], J = b - blk0[m];
-        const int n = ts.mat_n[m], voff = ts.mat_voff[m];
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (TILE * J + rr < n) v = *reinterpret_cast<const float4 *>(x32 + (size_t)(voff + TILE * J + rr) * 32 + 4 * cq);
-        xt[rr][4 * cq + 0] = v.x;
-        xt[rr][4 * cq + 1] = v.y;
-        xt[rr][4 * cq + 2] = v.z;
-        xt[rr][4 * cq + 3] = v.w;
-        __syncthreads();
-        const float4 w = make_float4(xt[4 * c + 0][nn], xt[4 * c + 1][nn], xt[4 * c + 2][nn], xt[4 * c + 3][nn]);
-        unsigned char *dst = reinterpret_cast<unsigned char *>(xs + (size_t)b * 2048);
-        tc::split_store(dst, dst + tc3::B_BYTES, (unsigned)t * 16u, w);
-        __syncthreads();
-    }
-}
-
 __global__ void __launch_bounds__(tc3::THREADS, 1)
-tile_symm_tc3_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, const float *xs, const int *blk0,
-                     double *out, const int2 *units, int nunits, int slot, int mode) {
+tile_symm_tc3_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, double *out, const int2 *units,
+                     int nunits, int slot, int mode) {
     pdl_enter();
     constexpr int NS = tc3::NS, NR = 32;
     extern __shared__ unsigned char tc3_smem[];
@@ -5470,7 +5438,7 @@ tile_symm_tc3_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, 
                 const int m = units[u].x, I0 = 4 * units[u].y, tn = ts.mat_tn[m];
                 const long long t0 = ts.mat_tile0[m];
                 const int nq = min(4, tn - I0);
-                const float *xb = xs + (size_t)blk0[m] * 2048;
+                const float *xm = x32 + (size_t)ts.mat_voff[m] * NR;
                 for (int J = 0; J < tn; ++J, ++t) {
                     if ((int)(t & 1) != par) continue;
                     const int s = (int)(t % NS);
@@ -5479,7 +5447,7 @@ tile_symm_tc3_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, 
                         break;
                     }
                     unsigned char *stg = buf + (size_t)s * tc3::STAGE;
-                    mbar_arrive_tx(&full[s], 4096u * (unsigned)nq + 2u * tc3::B_BYTES);
+                    mbar_arrive_tx(&full[s], 4096u * (unsigned)nq + tc3::B_BYTES);
                     if (J < I0) {
                         // the stored tiles (J, I0 .. I0 + nq - 1) are adjacent in tile row J
                         tc3::bulk(stg, tiles + (size_t)tc3::tile_index(t0, tn, J, I0) * (TILE * TILE), 4096u * (unsigned)nq,
@@ -5491,7 +5459,7 @@ tile_symm_tc3_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, 
                             tc3::bulk(stg + q * 4096, tiles + (size_t)idx * (TILE * TILE), 4096u, &full[s]);
                         }
                     }
-                    tc3::bulk(stg + 2 * tc3::A_BYTES, xb + (size_t)J * 2048, 2u * tc3::B_BYTES, &full[s]);
+                    tc3::bulk(stg + tc3::XRAW, xm + (size_t)TILE * J * NR, tc3::B_BYTES, &full[s]);
                     last[s] = t;
                 }
             }
@@ -5521,8 +5489,8 @@ tile_symm_tc3_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, 
                         break;
                     }
                     tc::fence_after();
-                    const unsigned a_hi = smem_u32(buf + (size_t)s * tc3::STAGE), a_lo = a_hi + tc3::A_BYTES,
-                                   b_hi = a_hi + 2 * tc3::A_BYTES;   // X_lo follows X_hi: rows 32..63 of B
+                    const unsigned a_hi = smem_u32(buf + (size_t)s * tc3::STAGE), a_lo = a_hi + tc3::ALO,
+                                   b_hi = a_hi + tc3::XS;   // X_lo follows X_hi: rows 32..63 of B
 #pragma unroll
                     for (int kk = 0; kk < 4; ++kk) {
                         const unsigned off = 32u * kk;
@@ -5542,37 +5510,66 @@ tile_symm_tc3_kernel(TileSetDev ts, DevProblem P, BlockDev B, const float *x32, 
         const int q = warp;
         long long t = 0;
         for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
-            const int m = units[u].x, I = 4 * units[u].y + q, tn = ts.mat_tn[m];
+            const int m = units[u].x, I = 4 * units[u].y + q, tn = ts.mat_tn[m], n = ts.mat_n[m];
             for (int J = 0; J < tn; ++J, ++t) {
                 const int s = (int)(t % NS);
                 ok = __all_sync(FULL, tc3::wait(&full[s], (unsigned)((t / NS) & 1), &s_abort));
                 if (!ok) break;
+                unsigned char *stg = buf + (size_t)s * tc3::STAGE;
+                // X_J^T: columns 8q .. 8q + 7 (chunks 2q, 2q + 1) of every right-hand side `lane`
+                {
+                    const float *xr = reinterpret_cast<const float *>(stg + tc3::XRAW);
+                    const int rows = n - TILE * J;   // rows of the block inside the subdomain
+                    float4 xv[2];
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int c = 2 * q + h;
+                        xv[h].x = (4 * c + 0 < rows) ? xr[(4 * c + 0) * NR + lane] : 0.f;
+                        xv[h].y = (4 * c + 1 < rows) ? xr[(4 * c + 1) * NR + lane] : 0.f;
+                        xv[h].z = (4 * c + 2 < rows) ? xr[(4 * c + 2) * NR + lane] : 0.f;
+                        xv[h].w = (4 * c + 3 < rows) ? xr[(4 * c + 3) * NR + lane] : 0.f;
+                    }
+#pragma unroll
+                    for (int h = 0; h < 2; ++h)
+                        tc::split_store(stg + tc3::XS, stg + tc3::XS + tc3::B_BYTES, tc::swz(lane, 2 * q + h), xv[h]);
+                }
                 if (I < tn) {   // rows of a missing tile row only reach accumulator rows that are not read
-                    unsigned char *hi = buf + (size_t)s * tc3::STAGE + q * 4096, *lo = hi + tc3::A_BYTES;
-                    float4 v[8];
+                    unsigned char *hi = stg + q * 4096, *lo = stg + tc3::ALO + q * 4096;
+                    float4 v[8], h4[8];
+                    unsigned off[8];
                     if (I <= J) {
                         const float4 *src = reinterpret_cast<const float4 *>(hi);
 #pragma unroll
                         for (int it = 0; it < 8; ++it) v[it] = src[it * 32 + lane];
-                        __syncwarp();
 #pragma unroll
                         for (int it = 0; it < 8; ++it) {
                             const int p = it * 32 + lane;
-                            tc::split_store(hi, lo, tc::swz(p >> 3, p & 7), v[it]);
+                            off[it] = tc::swz(p >> 3, p & 7);
                         }
                     } else {
                         // stored tile (J, I): row `lane` of S_IJ is column `lane` of the stored tile
                         const float *src = reinterpret_cast<const float *>(hi);
 #pragma unroll
-                        for (int it = 0; it < 8; ++it)
+                        for (int it = 0; it < 8; ++it) {
                             v[it] = make_float4(src[(4 * it + 0) * 32 + lane], src[(4 * it + 1) * 32 + lane],
                                                 src[(4 * it + 2) * 32 + lane], src[(4 * it + 3) * 32 + lane]);
-                        __syncwarp();
-#pragma unroll
-                        for (int it = 0; it < 8; ++it) tc::split_store(hi, lo, tc::swz(lane, it), v[it]);
+                            off[it] = tc::swz(lane, it);
+                        }
                     }
-                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    __syncwarp();
+                    // high parts in place, low parts to the stage's low buffer
+#pragma unroll
+                    for (int it = 0; it < 8; ++it) {
+                        h4[it].x = tc::tf32_hi(v[it].x);
+                        h4[it].y = tc::tf32_hi(v[it].y);
+                        h4[it].z = tc::tf32_hi(v[it].z);
+                        h4[it].w = tc::tf32_hi(v[it].w);
+                        *reinterpret_cast<float4 *>(hi + off[it]) = h4[it];
+                        *reinterpret_cast<float4 *>(lo + off[it]) =
+                            make_float4(v[it].x - h4[it].x, v[it].y - h4[it].y, v[it].z - h4[it].z, v[it].w - h4[it].w);
+                    }
                 }
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&conv[s]);
             }
@@ -5874,7 +5871,8 @@ void GpuSolver::Impl::ensure_block(int nr) {
     B.x = alloc<double>((size_t)NL * nr); B.r = alloc<double>((size_t)NL * nr); B.w = alloc<double>((size_t)NL * nr);
     B.z = alloc<double>((size_t)NL * nr); B.y = alloc<double>((size_t)NL * nr); B.p = alloc<double>((size_t)NL * nr);
     B.Ap = alloc<double>((size_t)NL * nr); B.Ax = alloc<double>((size_t)NL * nr); B.bL = alloc<double>((size_t)NL * nr);
-    B.p32 = alloc<float>((size_t)NL * nr);
+    // 32 rows past the last subdomain: the warp-specialised tensor-core SYMM copies whole 32-row blocks
+    B.p32 = alloc<float>((size_t)(NL + TILE) * nr);
     B.uT = alloc<double>((size_t)NT * nr); B.vT = alloc<double>((size_t)NT * nr);
     // alpha carries KS zero rows past nK for the fixed-width G^T alpha loads
     B.d = alloc<double>((size_t)P.nP * nr); B.alpha = alloc<double>((size_t)(nK + P.KS) * nr);
@@ -5910,23 +5908,6 @@ void GpuSolver::Impl::ensure_block(int nr) {
     blk.units4 = upload(units4);
     blk.nunits4 = (int)units4.size();
     blk.pan = nullptr;   // rebuilt for these units at the first asynchronous tensor-core SYMM
-    // 32-row blocks of the subdomains for the split X of the warp-specialised tensor-core SYMM
-    blk.xs = nullptr;
-    blk.blk0 = blk.blkm = nullptr;
-    blk.nblk = 0;
-    if (nr == 32) {
-        std::vector<int> b0(tn.size()), bm;
-        for (size_t m = 0; m < tn.size(); ++m) {
-            b0[m] = (int)bm.size();
-            for (int J = 0; J < tn[m]; ++J) bm.push_back((int)m);
-        }
-        blk.nblk = (int)bm.size();
-        if (blk.nblk > 0) {
-            blk.blk0 = upload(b0);
-            blk.blkm = upload(bm);
-            blk.xs = alloc<float>((size_t)blk.nblk * 2048);
-        }
-    }
     // per-unit dot products: one per unit, or four (one per epilogue warp) for the tensor-core units
     size_t max_units = std::max(units.size(), 4 * units4.size());
     if (opt.precond == PREC_DIRICHLET) {
@@ -6051,20 +6032,17 @@ static bool symm_tc3_enabled() {
 }
 
 static void symm_tc3_launch(int nsm, cudaStream_t st, TileSetDev td, DevProblem P, BlockDev B, const float *x32,
-                            float *xs, const int *blk0, const int *blkm, int nblk, double *out, const int2 *units,
-                            int nunits, int slot, int mode) {
+                            double *out, const int2 *units, int nunits, int slot, int mode) {
     static bool attr = false;
     if (!attr) {
         CUDA_CHECK(cudaFuncSetAttribute(tile_symm_tc3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)tc3::SMEM));
         attr = true;
     }
-    launch_pdl(xsplit_kernel, dim3(std::max(1, std::min(nblk, nsm * 8))), dim3(256), 0, st, td, P, x32, blkm, blk0,
-               nblk, xs, slot, mode);
     // one CTA per SM (its shared memory); CTAs never wait for one another
     const int grid = std::max(1, std::min(nunits, nsm));
-    launch_pdl(tile_symm_tc3_kernel, dim3(grid), dim3(tc3::THREADS), (size_t)tc3::SMEM, st, td, P, B, x32,
-               (const float *)xs, blk0, out, units, nunits, slot, mode);
+    launch_pdl(tile_symm_tc3_kernel, dim3(grid), dim3(tc3::THREADS), (size_t)tc3::SMEM, st, td, P, B, x32, out, units,
+               nunits, slot, mode);
 }
 
 static bool symm_tc2_bmn() {
@@ -6117,10 +6095,9 @@ void GpuSolver::Impl::launch_symm(const TileSetHost &T, bool src32, const double
     const bool dir = &T == &Dir;
     const int2 *units = dir ? blk.dunits : blk.units;
     const int nunits = dir ? blk.ndunits : blk.nunits;
-    if (!dir && opt.symm_tensor && T.prec == SCHUR_FP32 && src32 && nr == 32 && blk.xs && symm_tc3_enabled() &&
+    if (!dir && opt.symm_tensor && T.prec == SCHUR_FP32 && src32 && nr == 32 && symm_tc3_enabled() &&
         !symm_tc2_enabled()) {
-        symm_tc3_launch(nsm, stream, T.dev(), P, blk.B, x32, blk.xs, blk.blk0, blk.blkm, blk.nblk, out, blk.units4,
-                        blk.nunits4, slot, mode);
+        symm_tc3_launch(nsm, stream, T.dev(), P, blk.B, x32, out, blk.units4, blk.nunits4, slot, mode);
         CUDA_CHECK(cudaGetLastError());
         return;
     }
