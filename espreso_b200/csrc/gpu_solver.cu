@@ -4377,18 +4377,42 @@ __global__ void __launch_bounds__(256, FLAT_MIN_BLOCKS) by_flat2_kernel(DevProbl
 
 // y = z - G^T alpha, rho_j = y.w
 
-// p = y + beta_j p (and its FP32 copy)
-__global__ void bp_kernel(DevProblem P, BlockDev B, int slot) {
+// p = y + beta_j p (and its FP32 copy).  Two columns per thread (16-byte loads and stores), UNR
+// rows in flight; the grid stride is a multiple of nr / 2, so every thread keeps its columns and
+// computes their beta once.
+__global__ void __launch_bounds__(256, FLAT_MIN_BLOCKS) bp_kernel(DevProblem P, BlockDev B, int slot) {
     pdl_enter();
     const int iter = P.st->iter_base + slot;
     if (skip_iter(P.st, iter)) return;
-    const int nr = B.nr;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.NL * nr; i += gridDim.x * blockDim.x) {
-        const int j = (i & (nr - 1));
-        const double beta = (iter == 0) ? 0.0 : B.scal[SC_RHO * nr + j] / B.rho_hist[(size_t)(iter - 1) * nr + j];
-        const double pv = col_frozen(B, j, iter) ? 0.0 : B.y[i] + beta * B.p[i];
-        B.p[i] = pv;
-        B.p32[i] = (float)pv;
+    const int nr = B.nr, hn = nr >> 1;
+    const long long cnt = (long long)P.NL * hn, stride = (long long)gridDim.x * blockDim.x;
+    const long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 2 * (int)(i0 & (hn - 1));
+    const bool f0 = col_frozen(B, j, iter), f1 = col_frozen(B, j + 1, iter);
+    const double b0 = (iter == 0) ? 0.0 : B.scal[SC_RHO * nr + j] / B.rho_hist[(size_t)(iter - 1) * nr + j];
+    const double b1 = (iter == 0) ? 0.0 : B.scal[SC_RHO * nr + j + 1] / B.rho_hist[(size_t)(iter - 1) * nr + j + 1];
+    const double2 *y = reinterpret_cast<const double2 *>(B.y);
+    double2 *p = reinterpret_cast<double2 *>(B.p);
+    float2 *p32 = reinterpret_cast<float2 *>(B.p32);
+    for (long long i = i0; i < cnt; i += UNR * stride) {
+        double2 yv[UNR], pv[UNR];
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            const long long k = i + u * stride;
+            if (k < cnt) {
+                yv[u] = __ldg(y + k);
+                pv[u] = p[k];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            const long long k = i + u * stride;
+            if (k < cnt) {
+                const double2 r = make_double2(f0 ? 0.0 : yv[u].x + b0 * pv[u].x, f1 ? 0.0 : yv[u].y + b1 * pv[u].y);
+                p[k] = r;
+                p32[k] = make_float2((float)r.x, (float)r.y);
+            }
+        }
     }
 }
 
@@ -6217,8 +6241,7 @@ void GpuSolver::Impl::launch_block_iteration(int slot) {
         default: launch_pdl(by_flat2_kernel<0>, dim3(fgrid), dim3(256), 0, stream, P, B, slot); break;
         }
     }
-    launch_pdl(bp_kernel, dim3(std::max(1, std::min(4096, (P.NL * blk.nr + 255) / 256))), dim3(256), 0, stream, P, B,
-               slot);
+    launch_pdl(bp_kernel, dim3(blk.flat_grid), dim3(256), 0, stream, P, B, slot);
     if (mixed) launch_symm(Flow, true, nullptr, B.p32, B.Ap, slot, 1);
     else launch_symm(F64, false, B.p, nullptr, B.Ap, slot, 1);
     launch_block_hybrid(B.p, B.Ap, slot, 1, B.scal + SC_PAP * blk.nr);
